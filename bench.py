@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Traversal benchmark of the B200 hot path (one JSON line on rank 0).
+
+Workload (the reference's traversal microbenchmark configuration): a 1M-triangle soup (centroids
+uniform in the unit cube, edge lengths lognormal(ln 0.002, 0.5), random orientations, FP32,
+seed 0), LBVH with SAH treelet restructuring collapsed to 4-wide nodes, 16M coherent primary rays
+(4096 x 4096 pinhole) and 16M incoherent rays (origins uniform in the cube, directions uniform on
+the sphere). One step = closest hit of both sets + any hit of both sets (shadow tmax per ray),
+64M ray queries. `value` = ray queries per second over the whole job (Mrays/s), inputs resident
+in HBM; `e2e` = the same through the C-ABI host-buffer entry points, host<->device copies inside
+the timed region.
+
+--impl reference: the reference's own CPU path (its binned-SAH 4-wide build and 4-wide
+traversal, restated in C++ by the oracle since the Swift/Metal reference cannot run here), on all
+host threads, over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "traversal Mrays/s"
+UNIT = "Mrays/s"
+L2_NOTE = "inputs larger than L2 (1 GiB of rays read per step); BVH + triangles (~88 MB) L2-resident by design"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--faces", type=int, default=1_000_000)
+    p.add_argument("--res", type=int, default=4096, help="coherent set is res x res")
+    p.add_argument("--incoherent", type=int, default=1 << 24)
+    p.add_argument("--leaf", type=int, default=2)
+    p.add_argument("--cpu-sample", type=int, default=1 << 18, help="rays per set in the CPU sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--profile", action="store_true", help="small run for ncu: no e2e, no CPU leg")
+    return p.parse_args()
+
+
+def workload_config(a) -> dict:
+    return {
+        "workload": ("bvh traversal microbenchmark: %d-triangle soup (lognormal edges ln 0.002 / 0.5, seed 0), "
+                     "LBVH + SAH treelet restructuring -> 4-wide nodes, %dx%d coherent + %d incoherent rays, "
+                     "closest-hit + any-hit" % (a.faces, a.res, a.res, a.incoherent)),
+        "faces": a.faces,
+        "coherent_rays": a.res * a.res,
+        "incoherent_rays": a.incoherent,
+        "queries_per_step": 2 * (a.res * a.res + a.incoherent),
+        "leaf_size": a.leaf,
+        "l2": L2_NOTE,
+    }
+
+
+# ---- clocks during the timed region ----------------------------------------------------------
+class ClockSampler:
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= int(self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+            except Exception:
+                pass
+            time.sleep(0.05)
+
+    def __enter__(self):
+        if self.nv is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        names = [n for bit, n in self.REASONS.items() if self.reasons & bit and n != "gpu_idle"]
+        return {"sm_mhz": float(np.median(self.samples)), "sm_max_mhz": self.max_mhz, "reasons": names,
+                "samples": len(self.samples)}
+
+
+# ---- CPU legs (oracle: test infrastructure, used here only as the timed CPU baseline) ----------
+def cpu_sample_rays(a, rank_seed=0):
+    from metal_vibe_tracer_b200 import scenes
+    s = a.cpu_sample
+    stride = max(1, a.res // int(math.sqrt(s)))
+    coh = scenes.coherent_rays_np(a.res, a.res, rows=slice(0, a.res, stride))
+    coh = coh.reshape(-1, a.res, 8)[:, ::stride].reshape(-1, 8)[:s]
+    inc = scenes.incoherent_rays_np(s, seed=1 + rank_seed)
+    return coh, inc, scenes.shadow_tmax_np(coh, True), scenes.shadow_tmax_np(inc, False)
+
+
+def time_cpu(bvh, sets, threads):
+    t0 = time.perf_counter()
+    n = 0
+    bvh.closest(sets[0], nthreads=threads); n += len(sets[0])
+    bvh.closest(sets[1], nthreads=threads); n += len(sets[1])
+    bvh.occluded(sets[2], nthreads=threads); n += len(sets[2])
+    bvh.occluded(sets[3], nthreads=threads); n += len(sets[3])
+    return n, time.perf_counter() - t0
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from metal_vibe_tracer_b200 import scenes
+    from oracle import vt_oracle as O
+    threads = O.threads()
+    faces, verts = scenes.triangle_soup(a.faces, seed=0)
+    bvh = O.Bvh.widebvh(faces, verts, leaf_size=2)
+    sets = cpu_sample_rays(a)
+    for _ in range(min(a.warmup, 1)):
+        time_cpu(bvh, [s[:4096] for s in sets], threads)
+    total_n, total_t = 0, 0.0
+    per = []
+    for _ in range(a.steps):
+        n, t = time_cpu(bvh, sets, threads)
+        total_n += n
+        total_t += t
+        per.append(t)
+    value = total_n / total_t / 1e6
+    sample = ("reference WideBVH binned-SAH build (leaf 2) + 4-wide traversal restated in C++ (fp32), "
+              "%d rays per set (strided coherent subset + first incoherent rays), 4 query sets per step" % len(sets[0]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * total_t / a.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+        "config": workload_config(a),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm ----------------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.profile:
+        a.no_e2e = True
+        a.no_cpu_baseline = True
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import torch
+    import torch.distributed as dist
+
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        print(json.dumps({"metric": METRIC, "error": "no CUDA device"}))
+        return 1
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    ctx = vt.Context(local)
+    faces, verts = scenes.triangle_soup(a.faces, seed=0)
+    mesh = vt.Mesh(ctx, faces, verts, leaf_size=a.leaf)
+    info = mesh.info()
+
+    # Inputs resident in HBM; each rank traces its own incoherent rays (weak scaling).
+    coh = scenes.coherent_rays_torch(a.res, a.res, dev)
+    inc = scenes.incoherent_rays_torch(a.incoherent, dev, seed=1 + rank)
+    coh_s = scenes.shadow_tmax_torch(coh, True, seed=2 + rank)
+    inc_s = scenes.shadow_tmax_torch(inc, False, seed=3 + rank)
+    hits_c = torch.empty((coh.shape[0], 4), dtype=torch.float32, device=dev)
+    hits_i = torch.empty((inc.shape[0], 4), dtype=torch.float32, device=dev)
+    occ_c = torch.empty((coh.shape[0],), dtype=torch.uint8, device=dev)
+    occ_i = torch.empty((inc.shape[0],), dtype=torch.uint8, device=dev)
+    queries = 2 * (coh.shape[0] + inc.shape[0])
+    stream = torch.cuda.current_stream(dev)
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+
+    def step(record=None):
+        # record: list of 8 events bracketing each launch (per-kernel durations), or None.
+        launches = ((mesh.closest, coh, hits_c), (mesh.closest, inc, hits_i),
+                    (mesh.occluded, coh_s, occ_c), (mesh.occluded, inc_s, occ_i))
+        for k, (fn, rays, out) in enumerate(launches):
+            if record:
+                record[2 * k].record(stream)
+            fn(rays, out)
+            if record:
+                record[2 * k + 1].record(stream)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # Per-kernel durations (one instrumented step, events on the launching stream).
+    step(ev)
+    torch.cuda.synchronize()
+    kernel_ms = [ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(4)]
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for _ in range(a.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * queries * a.steps / (ms_max / 1e3) / 1e6
+
+    # Traversal counts for the roofline (instrumented kernel, outside the timed region).
+    counts = {}
+    names = ["closest_coherent", "closest_incoherent", "any_coherent", "any_incoherent"]
+    sets = [(coh, True), (inc, True), (coh_s, False), (inc_s, False)]
+    for name, (rays, closest) in zip(names, sets):
+        counts[name] = mesh.count(rays, closest=closest)
+
+    # Roofline for the dominant launch: algorithmic bytes = node fetches x 128 B + triangle tests
+    # x 48 B + ray record 32 B + result (16 B hit / 1 B flag), per launch, over its event duration.
+    dom = int(np.argmax(kernel_ms))
+    nv, nt = counts[names[dom]]
+    n_rays = sets[dom][0].shape[0]
+    out_b = 16 if sets[dom][1] else 1
+    alg_bytes = nv * 128 + nt * 48 + n_rays * (32 + out_b)
+    achieved = alg_bytes / (kernel_ms[dom] / 1e3) / 1e9
+    peaks_path = ROOT / "MEASURED_PEAKS.json"
+    peak, peak_src = 6650.0, "fallback"
+    if peaks_path.exists():
+        try:
+            peak = float(json.loads(peaks_path.read_text())["hbm_gbs"])
+            peak_src = "measured"
+        except Exception:
+            pass
+    traffic = None
+    tpath = ROOT / "profiles" / "traffic.json"
+    if tpath.exists():
+        try:
+            traffic = json.loads(tpath.read_text()).get(names[dom])
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "traffic": traffic, "kernel": names[dom], "peak_source": peak_src,
+        "algorithmic_bytes_per_launch": alg_bytes,
+        "note": "algorithmic bytes are node/triangle fetches served mostly by L1/L2 (structure is L2-resident); "
+                "HBM carries the ray stream",
+    }
+
+    # End to end through the C-ABI host-buffer entry points (pinned host memory).
+    e2e = None
+    if not a.no_e2e:
+        h_coh = torch.empty_like(coh, device="cpu").pin_memory()
+        h_inc = torch.empty_like(inc, device="cpu").pin_memory()
+        h_cohs = torch.empty_like(coh_s, device="cpu").pin_memory()
+        h_incs = torch.empty_like(inc_s, device="cpu").pin_memory()
+        for h, d in ((h_coh, coh), (h_inc, inc), (h_cohs, coh_s), (h_incs, inc_s)):
+            h.copy_(d)
+        o_c = torch.empty((coh.shape[0], 4), dtype=torch.float32).pin_memory()
+        o_i = torch.empty((inc.shape[0], 4), dtype=torch.float32).pin_memory()
+        oc_c = torch.empty((coh.shape[0],), dtype=torch.uint8).pin_memory()
+        oc_i = torch.empty((inc.shape[0],), dtype=torch.uint8).pin_memory()
+        as_np = lambda t, dt: t.numpy().view(dt).reshape(-1)
+
+        def e2e_step():
+            mesh.closest(as_np(h_coh, vt.RAY_DTYPE), as_np(o_c, vt.HIT_DTYPE))
+            mesh.closest(as_np(h_inc, vt.RAY_DTYPE), as_np(o_i, vt.HIT_DTYPE))
+            mesh.occluded(as_np(h_cohs, vt.RAY_DTYPE), oc_c.numpy())
+            mesh.occluded(as_np(h_incs, vt.RAY_DTYPE), oc_i.numpy())
+
+        for _ in range(max(1, min(a.warmup, 2))):
+            e2e_step()
+        e2e_steps = max(1, min(a.steps, 5))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t
+        e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
+        e2e_s = float(e_t.item())
+        e2e = {"value": world * queries * e2e_steps / e2e_s / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": 32 * queries, "d2h_bytes_per_step": 16 * (coh.shape[0] + inc.shape[0]) + (coh.shape[0] + inc.shape[0]),
+               "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls"}
+        # Parity spot check of the host path against the device path.
+        torch.cuda.synchronize()
+        assert torch.equal(o_i[:4096], hits_i[:4096].cpu()), "host path differs from device path"
+
+    # CPU baseline (rank 0, N = 1 only): the oracle port on the same BVH, bounded sample.
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import vt_oracle as O
+        threads = O.threads()
+        ref = O.Bvh.lbvh(faces, verts, leaf_size=a.leaf)
+        sets_cpu = cpu_sample_rays(a)
+        n, t = time_cpu(ref, sets_cpu, threads)
+        cpu = {"value": n / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": "oracle fp32 traversal of the same LBVH, %d rays per set x 4 sets (%.1f s)" % (len(sets_cpu[0]), t)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators; no dataset)",
+            "config": workload_config(a),
+            "e2e": e2e, "gpu_launches": 4 * a.steps, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "kernel_ms": dict(zip(names, kernel_ms)),
+            "per_set_mrays": {n: (sets[k][0].shape[0] / (kernel_ms[k] / 1e3) / 1e6) for k, n in enumerate(names)},
+            "traversal_counts_per_ray": {n: [c[0] / sets[k][0].shape[0], c[1] / sets[k][0].shape[0]]
+                                         for k, (n, c) in enumerate(counts.items())},
+            "build": {"ms": info.build_ms, "sah_cost": info.sah_cost, "wide_nodes": info.wide_nodes, "depth": info.depth},
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    mesh.close()
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

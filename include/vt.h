@@ -1,0 +1,151 @@
+/*
+ * vt.h — C ABI of the B200 rendering hot path (libvt_b200.so).
+ *
+ * The reference renderer is a Swift host that builds its acceleration structures on the CPU
+ * and dispatches Metal kernels. Each entry point below replaces one reference interface; the
+ * comment above it names the reference file:line it stands in for. Signatures carry plain
+ * pointers, sizes and POD structs only: no CUDA, torch or C++ types. A stream argument is a
+ * cudaStream_t passed as `void *` (NULL = the context's own stream).
+ *
+ * Errors: every call returns a vt_status. A non-zero status leaves a human-readable message in
+ * vt_last_error(ctx) (the role of MaterialLibrary.error(String), Sources/Acceleration.swift:733,
+ * and of renderFrame's onError callback, main.swift:11199-11202). A context is single-threaded,
+ * like the reference's @MainActor renderer.
+ */
+#ifndef VT_H
+#define VT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VT_ABI_VERSION 1u
+
+typedef int32_t vt_status;
+enum {
+  VT_OK = 0,
+  VT_ERR_INVALID = 1,   /* bad argument (null pointer, out-of-range index, bad size) */
+  VT_ERR_CUDA = 2,      /* a CUDA runtime call failed; the message holds cudaGetErrorString */
+  VT_ERR_MEMORY = 3,    /* device allocation failed or the scene exceeds the memory budget */
+  VT_ERR_LIMIT = 4,     /* a structural limit was exceeded (BVH depth vs traversal stack, sizes) */
+  VT_ERR_DEVICE = 5     /* a kernel reported an error status (bounded wait expired, stack overflow) */
+};
+
+typedef struct vt_ctx vt_ctx;
+typedef struct vt_mesh vt_mesh;
+
+/* MSL MeshFace (main.swift:616, Sources/Acceleration.swift:62): three absolute vertex indices
+ * and the stored tag (material slot / subset). 16 bytes. */
+typedef struct vt_face { uint32_t a, b, c, tag; } vt_face;
+
+/* MSL MeshVertex (main.swift:615, Sources/Acceleration.swift:61): position, normal, uv. 32 B. */
+typedef struct vt_vertex { float px, py, pz, nx, ny, nz, u, v; } vt_vertex;
+
+/* MSL MeshWideNode (main.swift:617, Sources/Acceleration.swift:23-30): 4-wide node, 128 bytes.
+ * Child k is an inner node (> 0, index of the node), a leaf (< 0: -(first + 1) with count[k]
+ * triangles starting at `first` in BVH order) or empty (0). Node 0 is the root. */
+typedef struct vt_wide_node {
+  float lox[4], loy[4], loz[4], hix[4], hiy[4], hiz[4];
+  int32_t child[4];
+  int32_t count[4];
+} vt_wide_node;
+
+/* A ray with its parametric interval [tmin, tmax). 32 bytes, two 16-byte vectors. */
+typedef struct vt_ray { float ox, oy, oz, tmin, dx, dy, dz, tmax; } vt_ray;
+
+/* Closest-hit record (the MSL MeshHit, main.swift:1843): t, barycentrics b1/b2 weighting
+ * vertices b and c, and the hit face's index in the caller's input order (-1 = miss). 16 B. */
+typedef struct vt_hit { float t, b1, b2; int32_t prim; } vt_hit;
+
+/* Build options. Zero-initialised fields take the defaults noted. */
+typedef struct vt_build_options {
+  int32_t leaf_size;          /* triangles per wide-BVH leaf, 1..8 (default 2, the reference BLAS
+                                 leaf size, Sources/Acceleration.swift:692) */
+  int32_t treelet_size;       /* SAH treelet restructuring: leaves per treelet, 0 = default 7,
+                                 -1 = plain LBVH (no refinement) */
+  int32_t refine_rounds;      /* restructuring rounds (default 2) */
+  int32_t max_depth;          /* reject trees deeper than this (default 31; stack bound) */
+} vt_build_options;
+
+typedef struct vt_mesh_info {
+  uint32_t faces;             /* triangles in the mesh */
+  uint32_t wide_nodes;        /* 4-wide nodes (vt_mesh_get_nodes count) */
+  uint32_t binary_nodes;      /* internal nodes of the binary LBVH (faces - 1) */
+  uint32_t depth;             /* 4-wide depth, root = 1 */
+  float sah_cost;             /* SAH cost of the 4-wide tree (node cost 1, triangle cost 1) */
+  float build_ms;             /* device time of the last build, ms */
+  float lo[3], hi[3];         /* scene bounds */
+} vt_mesh_info;
+
+/* ---- context ---------------------------------------------------------------------------- */
+
+/* Creates a context on CUDA device `device` with its own stream. Replaces PathTracerRenderer's
+ * init(device:) (main.swift:9513) for the traversal and build paths. */
+vt_status vt_ctx_create(int32_t device, vt_ctx **out);
+vt_status vt_ctx_destroy(vt_ctx *ctx);
+/* Message of the last failing call on `ctx` ("" if none). Valid until the next call. */
+const char *vt_last_error(const vt_ctx *ctx);
+uint32_t vt_abi_version(void);
+/* Blocks until the context's stream has drained. */
+vt_status vt_sync(vt_ctx *ctx);
+
+/* ---- mesh publish / BVH build ------------------------------------------------------------- */
+
+/* Builds a mesh's acceleration structure on the device from caller-owned HOST arrays (copied).
+ * Replaces MaterialLibrary.setMesh -> publishTwoLevel (Sources/Acceleration.swift:652-782) and
+ * WideBVH.build(bounds:count:leafSize:depth:) (Sources/Acceleration.swift:296) for one asset:
+ * a GPU LBVH (30-bit Morton codes, radix sort, Karras hierarchy), SAH treelet restructuring and
+ * a collapse to the reference's 4-wide node layout. Face indices must be < nverts. */
+vt_status vt_mesh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, const vt_build_options *opts, vt_mesh **out);
+/* The same from DEVICE arrays (no host copy). */
+vt_status vt_mesh_build_device(vt_ctx *ctx, const vt_face *faces_dev, uint32_t nfaces,
+                               const vt_vertex *verts_dev, uint32_t nverts,
+                               const vt_build_options *opts, vt_mesh **out);
+vt_status vt_mesh_destroy(vt_ctx *ctx, vt_mesh *mesh);
+vt_status vt_mesh_get_info(vt_ctx *ctx, const vt_mesh *mesh, vt_mesh_info *out);
+/* BVH leaf order (WideBVH.Result.order, Sources/Acceleration.swift:107-110): order[i] is the input
+ * face stored at BVH position i. `n` must equal the face count. Host output. */
+vt_status vt_mesh_get_order(vt_ctx *ctx, const vt_mesh *mesh, int32_t *order, uint32_t n);
+/* The 4-wide nodes (WideBVH.Result.nodes). `n` must equal info.wide_nodes. Host output. */
+vt_status vt_mesh_get_nodes(vt_ctx *ctx, const vt_mesh *mesh, vt_wide_node *nodes, uint32_t n);
+/* Sorted 30-bit Morton codes of the face centroids (parity of the LBVH's first stage), and the
+ * sorted face indices they belong to (before restructuring). Host outputs of `n` = face count. */
+vt_status vt_mesh_get_morton(vt_ctx *ctx, const vt_mesh *mesh, uint32_t *codes, int32_t *sorted,
+                             uint32_t n);
+/* Binary LBVH after refinement: per internal node its two children (>= 0 internal index,
+ * < 0 leaf -(sorted position + 1)) and its box (lo xyz, hi xyz). `n` = faces - 1. Host outputs. */
+vt_status vt_mesh_get_binary(vt_ctx *ctx, const vt_mesh *mesh, int32_t *children /* 2n */,
+                             float *boxes /* 6n */, uint32_t n);
+
+/* ---- traversal ----------------------------------------------------------------------------- */
+
+/* Closest hit of `n` DEVICE rays; writes `n` DEVICE hits. Replaces mesh_closest/blas_closest
+ * (main.swift:1788-1812, 1843-1901): watertight triangle test (main.swift:1536-1582), conservative
+ * 4-wide slab test (main.swift:1758-1785), nearest child first. Stream-ordered, asynchronous. */
+vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                           vt_hit *hits_dev, void *stream);
+/* Any hit in [tmin, tmax) of `n` DEVICE rays; writes one byte per ray (1 = occluded). Replaces
+ * mesh_occluded/blas_any (main.swift:1815-1838, 1902-1984) without endpoint slack. */
+vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                       uint8_t *occluded_dev, void *stream);
+/* The same from HOST arrays: copies in, traces and copies out in pipelined chunks on the
+ * context's streams, then synchronises. Pinned host memory gives overlapped copies. */
+vt_status vt_trace_closest_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
+                                vt_hit *hits);
+vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
+                            uint8_t *occluded);
+
+/* Per-ray traversal counters for the roofline: wide nodes fetched and triangles tested, summed
+ * over `n` DEVICE rays into two host uint64 values. A separate instrumented kernel; it does not
+ * slow the traversal entry points. closest = 1 counts closest-hit traversal, 0 any-hit. */
+vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                         int32_t closest, uint64_t *nodes_visited, uint64_t *tris_tested);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VT_H */

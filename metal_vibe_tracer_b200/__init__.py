@@ -1,0 +1,14 @@
+"""B200-native rendering hot path of Metal Vibe Tracer: LBVH build and watertight traversal.
+
+The kernels live in libvt_b200.so (C ABI: include/vt.h); this package is the host side that
+mirrors the reference's acceleration-structure interface. Nothing here computes a result on the
+CPU: a missing library raises.
+"""
+from ._lib import (FACE_DTYPE, HIT_DTYPE, RAY_DTYPE, VERTEX_DTYPE, WIDE_NODE_DTYPE, LIB_PATH,
+                   exported_symbols, load)
+from .accel import Context, MaterialLibraryError, Mesh, WideBVHResult
+
+__all__ = [
+    "Context", "Mesh", "MaterialLibraryError", "WideBVHResult", "FACE_DTYPE", "VERTEX_DTYPE",
+    "RAY_DTYPE", "HIT_DTYPE", "WIDE_NODE_DTYPE", "LIB_PATH", "exported_symbols", "load",
+]

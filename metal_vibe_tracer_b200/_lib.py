@@ -1,0 +1,92 @@
+"""ctypes binding of libvt_b200.so (the C ABI declared in include/vt.h).
+
+The library is loaded from the package's ``lib/`` folder. There is no fallback: if the library is
+missing or fails to load, every entry point raises, so no result can silently come from anything
+but the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvt_b200.so"
+
+# ---- record layouts (numpy dtypes mirror the C structs byte for byte) -------------------------
+FACE_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("tag", "<u4")])
+VERTEX_DTYPE = np.dtype([("p", "<f4", 3), ("n", "<f4", 3), ("uv", "<f4", 2)])
+WIDE_NODE_DTYPE = np.dtype([
+    ("lox", "<f4", 4), ("loy", "<f4", 4), ("loz", "<f4", 4),
+    ("hix", "<f4", 4), ("hiy", "<f4", 4), ("hiz", "<f4", 4),
+    ("child", "<i4", 4), ("count", "<i4", 4),
+])
+RAY_DTYPE = np.dtype([("o", "<f4", 3), ("tmin", "<f4"), ("d", "<f4", 3), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("b1", "<f4"), ("b2", "<f4"), ("prim", "<i4")])
+assert FACE_DTYPE.itemsize == 16 and VERTEX_DTYPE.itemsize == 32
+assert WIDE_NODE_DTYPE.itemsize == 128 and RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
+
+
+class BuildOptions(C.Structure):
+    _fields_ = [("leaf_size", C.c_int32), ("treelet_size", C.c_int32),
+                ("refine_rounds", C.c_int32), ("max_depth", C.c_int32)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("faces", C.c_uint32), ("wide_nodes", C.c_uint32), ("binary_nodes", C.c_uint32),
+                ("depth", C.c_uint32), ("sah_cost", C.c_float), ("build_ms", C.c_float),
+                ("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+
+VT_OK = 0
+STATUS_NAMES = {0: "VT_OK", 1: "VT_ERR_INVALID", 2: "VT_ERR_CUDA", 3: "VT_ERR_MEMORY",
+                4: "VT_ERR_LIMIT", 5: "VT_ERR_DEVICE"}
+
+# Every symbol include/vt.h declares, with (restype, argtypes).
+_P = C.c_void_p
+_U32 = C.c_uint32
+_I32 = C.c_int32
+SIGNATURES = {
+    "vt_abi_version": (_U32, []),
+    "vt_ctx_create": (_I32, [_I32, C.POINTER(_P)]),
+    "vt_ctx_destroy": (_I32, [_P]),
+    "vt_last_error": (C.c_char_p, [_P]),
+    "vt_sync": (_I32, [_P]),
+    "vt_mesh_build": (_I32, [_P, _P, _U32, _P, _U32, C.POINTER(BuildOptions), C.POINTER(_P)]),
+    "vt_mesh_build_device": (_I32, [_P, _P, _U32, _P, _U32, C.POINTER(BuildOptions), C.POINTER(_P)]),
+    "vt_mesh_destroy": (_I32, [_P, _P]),
+    "vt_mesh_get_info": (_I32, [_P, _P, C.POINTER(MeshInfo)]),
+    "vt_mesh_get_order": (_I32, [_P, _P, _P, _U32]),
+    "vt_mesh_get_nodes": (_I32, [_P, _P, _P, _U32]),
+    "vt_mesh_get_morton": (_I32, [_P, _P, _P, _P, _U32]),
+    "vt_mesh_get_binary": (_I32, [_P, _P, _P, _P, _U32]),
+    "vt_trace_closest": (_I32, [_P, _P, _P, _U32, _P, _P]),
+    "vt_trace_any": (_I32, [_P, _P, _P, _U32, _P, _P]),
+    "vt_trace_closest_host": (_I32, [_P, _P, _P, _U32, _P]),
+    "vt_trace_any_host": (_I32, [_P, _P, _P, _U32, _P]),
+    "vt_trace_count": (_I32, [_P, _P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def load() -> C.CDLL:
+    """Load libvt_b200.so (once) and declare every C-ABI signature. Raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m metal_vibe_tracer_b200.build` "
+            "(or __graft_entry__.build()). There is no CPU fallback.")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)

@@ -1,0 +1,633 @@
+// lbvh.cu — GPU acceleration-structure build: LBVH (30-bit Morton codes, stable radix sort,
+// Karras hierarchy), bottom-up refit, SAH treelet restructuring and the collapse to the
+// reference's 4-wide node layout (MeshWideNode, main.swift:617; Sources/Acceleration.swift:23-30).
+//
+// Replaces the reference's CPU binned-SAH WideBVH.build (Sources/Acceleration.swift:106-352).
+// Every arithmetic step that decides topology is written with explicitly rounded intrinsics
+// (__fadd_rn, __fmul_rn, __fdiv_rn) so the CPU oracle (oracle/vt_oracle.cpp, built with
+// -ffp-contract=off) reproduces Morton codes, sorted order and topology bit for bit.
+#include <cfloat>
+#include <vector>
+
+#include "vt_internal.cuh"
+
+namespace {
+
+constexpr float kCi = 1.2f, kCt = 1.0f;  // treelet costs: internal node, triangle
+constexpr int kMaxTreelet = 8;
+
+struct Box { float3 lo, hi; };
+
+__device__ __forceinline__ float box_area(float3 lo, float3 hi) {
+  float ex = fmaxf(__fsub_rn(hi.x, lo.x), 0.0f), ey = fmaxf(__fsub_rn(hi.y, lo.y), 0.0f),
+        ez = fmaxf(__fsub_rn(hi.z, lo.z), 0.0f);
+  return __fadd_rn(__fadd_rn(__fmul_rn(ex, ey), __fmul_rn(ey, ez)), __fmul_rn(ez, ex));
+}
+__device__ __forceinline__ Box box_union(const Box &a, const Box &b) {
+  return {make_float3(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z)),
+          make_float3(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z))};
+}
+// Boxes live as two float4 (lo.xyz, hi.xyz). L2 loads (.cg) because other threads of the same
+// launch write them in the bottom-up passes.
+__device__ __forceinline__ Box load_box_cg(const float4 *b, int i) {
+  float4 l = __ldcg(b + 2 * i), h = __ldcg(b + 2 * i + 1);
+  return {make_float3(l.x, l.y, l.z), make_float3(h.x, h.y, h.z)};
+}
+__device__ __forceinline__ void store_box(float4 *b, int i, const Box &x) {
+  __stcg(b + 2 * i, make_float4(x.lo.x, x.lo.y, x.lo.z, 0.0f));
+  __stcg(b + 2 * i + 1, make_float4(x.hi.x, x.hi.y, x.hi.z, 0.0f));
+}
+
+// Order-preserving float <-> uint map for atomic min/max of the scene bounds.
+__device__ __forceinline__ uint32_t f2ord(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ inline float ord2f(uint32_t u) {
+  uint32_t b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+#endif
+}
+
+// ---- stage 1: face boxes, centroid bounds, scene bounds, validation ---------------------------
+// bounds[0..5] = centroid lo xyz, hi xyz; bounds[6..11] = scene lo xyz, hi xyz (ordered uints).
+__global__ void k_init_bounds(uint32_t *bounds) {
+  int i = threadIdx.x;
+  if (i < 12) bounds[i] = (i % 6) < 3 ? 0xffffffffu : 0u;
+}
+
+__global__ void __launch_bounds__(256) k_face_boxes(const vt_face *faces, uint32_t nfaces,
+                                                      const vt_vertex *verts, uint32_t nverts,
+                                                      float4 *boxes, uint32_t *bounds,
+                                                      uint32_t *status) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float3 clo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), chi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  float3 slo = clo, shi = chi;
+  if (i < nfaces) {
+    vt_face f = faces[i];
+    Box b{make_float3(0, 0, 0), make_float3(0, 0, 0)};
+    if (f.a >= nverts || f.b >= nverts || f.c >= nverts) {
+      atomicOr(status, (uint32_t)VT_DEV_BAD_INDEX);
+    } else {
+      const vt_vertex &va = verts[f.a], &vb = verts[f.b], &vc = verts[f.c];
+      float3 a = make_float3(va.px, va.py, va.pz), p = make_float3(vb.px, vb.py, vb.pz),
+             q = make_float3(vc.px, vc.py, vc.pz);
+      bool finite = isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(p.x) &&
+                    isfinite(p.y) && isfinite(p.z) && isfinite(q.x) && isfinite(q.y) && isfinite(q.z);
+      if (!finite) {
+        atomicOr(status, (uint32_t)VT_DEV_NONFINITE);
+      } else {
+        b.lo = make_float3(fminf(fminf(a.x, p.x), q.x), fminf(fminf(a.y, p.y), q.y), fminf(fminf(a.z, p.z), q.z));
+        b.hi = make_float3(fmaxf(fmaxf(a.x, p.x), q.x), fmaxf(fmaxf(a.y, p.y), q.y), fmaxf(fmaxf(a.z, p.z), q.z));
+      }
+    }
+    boxes[2 * i] = make_float4(b.lo.x, b.lo.y, b.lo.z, 0.0f);
+    boxes[2 * i + 1] = make_float4(b.hi.x, b.hi.y, b.hi.z, 0.0f);
+    float3 c = make_float3(__fmul_rn(__fadd_rn(b.lo.x, b.hi.x), 0.5f), __fmul_rn(__fadd_rn(b.lo.y, b.hi.y), 0.5f),
+                           __fmul_rn(__fadd_rn(b.lo.z, b.hi.z), 0.5f));
+    clo = chi = c;
+    slo = b.lo;
+    shi = b.hi;
+  }
+  // Warp then block reduction of the 12 bounds, one atomic per block per bound.
+  float v[12] = {clo.x, clo.y, clo.z, chi.x, chi.y, chi.z, slo.x, slo.y, slo.z, shi.x, shi.y, shi.z};
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    const bool isMin = (k % 6) < 3;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      float u = __shfl_xor_sync(0xffffffffu, v[k], o);
+      v[k] = isMin ? fminf(v[k], u) : fmaxf(v[k], u);
+    }
+  }
+  __shared__ float red[8][12];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 12; ++k) red[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < 12) {
+    const int k = threadIdx.x;
+    const bool isMin = (k % 6) < 3;
+    float x = red[0][k];
+    for (int w = 1; w < (int)(blockDim.x / 32); ++w) x = isMin ? fminf(x, red[w][k]) : fmaxf(x, red[w][k]);
+    if (isMin) atomicMin(&bounds[k], f2ord(x));
+    else atomicMax(&bounds[k], f2ord(x));
+  }
+}
+
+// ---- stage 2: Morton codes --------------------------------------------------------------------
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+// q = min(uint((c - clo) * (1024 / (chi - clo))), 1023), 0 on a flat axis.
+__device__ __forceinline__ uint32_t quantize(float c, float clo, float chi) {
+  float ext = __fsub_rn(chi, clo);
+  if (!(ext > 0.0f)) return 0u;
+  float scale = __fdiv_rn(1024.0f, ext);
+  float f = __fmul_rn(__fsub_rn(c, clo), scale);
+  return f >= 1023.0f ? 1023u : (uint32_t)f;
+}
+
+__global__ void k_morton(const float4 *boxes, uint32_t n, const uint32_t *bounds, uint32_t *codes,
+                         uint32_t *vals) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 l = boxes[2 * i], h = boxes[2 * i + 1];
+  float cx = __fmul_rn(__fadd_rn(l.x, h.x), 0.5f), cy = __fmul_rn(__fadd_rn(l.y, h.y), 0.5f),
+        cz = __fmul_rn(__fadd_rn(l.z, h.z), 0.5f);
+  uint32_t qx = quantize(cx, ord2f(bounds[0]), ord2f(bounds[3]));
+  uint32_t qy = quantize(cy, ord2f(bounds[1]), ord2f(bounds[4]));
+  uint32_t qz = quantize(cz, ord2f(bounds[2]), ord2f(bounds[5]));
+  codes[i] = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
+  vals[i] = i;
+}
+
+// ---- stage 3: Karras hierarchy (HPG 2012) -----------------------------------------------------
+// Children: internal index >= 0, leaf = -(sorted position + 1). parent[] holds internal nodes at
+// [0, n-1) and leaves at n - 1 + position; the root's parent is -1.
+__device__ __forceinline__ int delta(const uint32_t *codes, int n, int i, int j) {
+  if (j < 0 || j > n - 1) return -1;
+  uint32_t a = codes[i], b = codes[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+}
+
+__global__ void k_karras(const uint32_t *codes, int n, int2 *child, int32_t *parent) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) parent[0] = -1;
+  if (i >= n - 1) return;
+  const int d = delta(codes, n, i, i + 1) - delta(codes, n, i, i - 1) > 0 ? 1 : -1;
+  const int dmin = delta(codes, n, i, i - d);
+  int lmax = 2;
+  while (delta(codes, n, i, i + lmax * d) > dmin) lmax *= 2;
+  int l = 0;
+  for (int s = lmax / 2; s >= 1; s /= 2)
+    if (delta(codes, n, i, i + (l + s) * d) > dmin) l += s;
+  const int j = i + l * d;
+  const int dnode = delta(codes, n, i, j);
+  int s = 0;
+  for (int div = 2;; div *= 2) {
+    const int step = (l + div - 1) / div;
+    if (delta(codes, n, i, i + (s + step) * d) > dnode) s += step;
+    if (step == 1) break;
+  }
+  const int gamma = i + s * d + min(d, 0);
+  const int lo = min(i, j), hi = max(i, j);
+  const int left = lo == gamma ? -(gamma + 1) : gamma;
+  const int right = hi == gamma + 1 ? -(gamma + 2) : gamma + 1;
+  child[i] = make_int2(left, right);
+  parent[left >= 0 ? left : (n - 1 + gamma)] = i;
+  parent[right >= 0 ? right : (n - 1 + gamma + 1)] = i;
+}
+
+__global__ void k_leaf_boxes(const float4 *boxes, const uint32_t *sorted, uint32_t n, float4 *leaf) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t f = sorted[i];
+  leaf[2 * i] = boxes[2 * f];
+  leaf[2 * i + 1] = boxes[2 * f + 1];
+}
+
+// ---- bottom-up passes ---------------------------------------------------------------------------
+struct TreeView {
+  int n;
+  int2 *child;
+  int32_t *parent;
+  const float4 *leafBox;
+  float4 *nodeBox;
+  uint32_t *count;
+  float *cost;
+};
+
+__device__ __forceinline__ int2 load_child(const TreeView &t, int i) {
+  return __ldcg(t.child + i);
+}
+__device__ __forceinline__ Box child_box(const TreeView &t, int c) {
+  return c >= 0 ? load_box_cg(t.nodeBox, c) : load_box_cg(t.leafBox, -c - 1);
+}
+__device__ __forceinline__ float child_cost(const TreeView &t, int c) {
+  if (c >= 0) return __ldcg(t.cost + c);
+  Box b = load_box_cg(t.leafBox, -c - 1);
+  return __fmul_rn(kCt, box_area(b.lo, b.hi));
+}
+__device__ __forceinline__ uint32_t child_count(const TreeView &t, int c) {
+  return c >= 0 ? __ldcg(t.count + c) : 1u;
+}
+__device__ __forceinline__ void refit_node(const TreeView &t, int i) {
+  int2 ch = load_child(t, i);
+  Box b = box_union(child_box(t, ch.x), child_box(t, ch.y));
+  store_box(t.nodeBox, i, b);
+  __stcg(t.count + i, child_count(t, ch.x) + child_count(t, ch.y));
+  __stcg(t.cost + i, __fadd_rn(__fmul_rn(kCi, box_area(b.lo, b.hi)),
+                               __fadd_rn(child_cost(t, ch.x), child_cost(t, ch.y))));
+}
+
+// Treelet restructuring at internal node `root` (Karras and Aila, HPG 2013), in the
+// deterministic form the oracle restates: grow the treelet by opening its largest-area internal
+// leaf (first in list order on ties; opened node replaced in place by its left child, right child
+// appended), DP over subsets (partitions p = (p - 1) & s downwards, strict improvement), rebuild
+// only on a strict cost improvement, internal nodes reassigned depth first, left = the side with
+// the lowest leaf bit.
+__device__ void restructure_node(const TreeView &t, int root, int size, uint32_t *status) {
+  int leaves[kMaxTreelet], internals[kMaxTreelet];
+  int nl = 0, ni = 0;
+  internals[ni++] = root;
+  int2 rc = load_child(t, root);
+  leaves[nl++] = rc.x;
+  leaves[nl++] = rc.y;
+  while (nl < size) {
+    int best = -1;
+    float bestA = -1.0f;
+    for (int k = 0; k < nl; ++k) {
+      int c = leaves[k];
+      if (c < 0) continue;
+      Box b = load_box_cg(t.nodeBox, c);
+      float a = box_area(b.lo, b.hi);
+      if (a > bestA) { bestA = a; best = k; }
+    }
+    if (best < 0) break;
+    int c = leaves[best];
+    internals[ni++] = c;
+    int2 cc = load_child(t, c);
+    leaves[best] = cc.x;
+    leaves[nl++] = cc.y;
+  }
+  const int k = nl;
+  if (k < 3) return;
+  const int full = (1 << k) - 1;
+  float area[1 << kMaxTreelet], copt[1 << kMaxTreelet];
+  uint8_t part[1 << kMaxTreelet];
+  Box lb[kMaxTreelet];
+  for (int q = 0; q < k; ++q) {
+    lb[q] = child_box(t, leaves[q]);
+    copt[1 << q] = child_cost(t, leaves[q]);
+  }
+  for (int s = 1; s <= full; ++s) {
+    int low = __ffs(s) - 1;
+    Box b = lb[low];
+    for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, lb[__ffs(r) - 1]);
+    area[s] = box_area(b.lo, b.hi);
+  }
+  for (int sz = 2; sz <= k; ++sz) {
+    for (int s = 1; s <= full; ++s) {
+      if (__popc(s) != sz) continue;
+      float best = FLT_MAX;
+      int bp = 0;
+      for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+        float c = __fadd_rn(copt[p], copt[s ^ p]);
+        if (c < best) { best = c; bp = p; }
+      }
+      copt[s] = __fadd_rn(__fmul_rn(kCi, area[s]), best);
+      part[s] = (uint8_t)bp;
+    }
+  }
+  if (!(copt[full] < __ldcg(t.cost + root))) return;
+  int next = 0;
+  int st_s[kMaxTreelet * 2], st_n[kMaxTreelet * 2];
+  int top = 0;
+  st_s[top] = full; st_n[top] = internals[next++]; ++top;
+  while (top) {
+    --top;
+    const int s = st_s[top], node = st_n[top];
+    const int p = part[s], q = s ^ p;
+    const int lowbit = s & -s;
+    const int subs[2] = {(p & lowbit) ? p : q, (p & lowbit) ? q : p};
+    int kids[2];
+    for (int c = 0; c < 2; ++c) {
+      const int x = subs[c];
+      if ((x & (x - 1)) == 0) kids[c] = leaves[__ffs(x) - 1];
+      else {
+        if (next >= ni) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
+        kids[c] = internals[next++];
+      }
+    }
+    __stcg(t.child + node, make_int2(kids[0], kids[1]));
+    for (int c = 1; c >= 0; --c)
+      if ((subs[c] & (subs[c] - 1)) != 0) { st_s[top] = subs[c]; st_n[top] = kids[c]; ++top; }
+  }
+  for (int i = ni - 1; i >= 0; --i) {
+    const int nd = internals[i];
+    refit_node(t, nd);
+    int2 ch = load_child(t, nd);
+    __stcg(t.parent + (ch.x >= 0 ? ch.x : (t.n - 1 + (-ch.x - 1))), nd);
+    __stcg(t.parent + (ch.y >= 0 ? ch.y : (t.n - 1 + (-ch.y - 1))), nd);
+  }
+}
+
+// One thread per leaf walks to the root; the second thread to reach a node owns it (its two
+// subtrees are final) and refits it (mode 0) or restructures it (mode 1: subtrees with >= size
+// leaves). flags[] must be zero on entry.
+__global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, int mode, int size,
+                                                    uint32_t *status) {
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= t.n) return;
+  int node = __ldcg(t.parent + (t.n - 1 + leaf));
+  while (node >= 0) {
+    __threadfence();
+    if (atomicAdd(&flags[node], 1u) == 0u) return;
+    __threadfence();
+    if (mode == 0) refit_node(t, node);
+    else if (__ldcg(t.count + node) >= (uint32_t)size) restructure_node(t, node, size, status);
+    __threadfence();
+    node = __ldcg(t.parent + node);
+  }
+}
+
+// ---- collapse to 4-wide -------------------------------------------------------------------------
+// A wide node rooted at binary node b starts with children [b] and splits the child of largest
+// area among those with more than leafSize leaves (the reference's rule,
+// Sources/Acceleration.swift:255-263) until four children.
+__global__ void k_collapse_count(TreeView t, const int32_t *level, uint32_t L, int leafSize,
+                                 int4 *chOut, uint32_t *nInner, uint32_t *nPrims) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= L) return;
+  int ch[4] = {level[w], 0, 0, 0};
+  int m = 1;
+  while (m < 4) {
+    int best = -1;
+    float bestA = 0.0f;
+    for (int k = 0; k < m; ++k) {
+      if (child_count(t, ch[k]) <= (uint32_t)leafSize) continue;
+      Box b = child_box(t, ch[k]);
+      float a = box_area(b.lo, b.hi);
+      if (best < 0 || a > bestA) { best = k; bestA = a; }
+    }
+    if (best < 0) break;
+    const int c = ch[best];
+    for (int k = m; k > best + 1; --k) ch[k] = ch[k - 1];
+    int2 cc = load_child(t, c);
+    ch[best] = cc.x;
+    ch[best + 1] = cc.y;
+    ++m;
+  }
+  uint32_t inner = 0, prims = 0;
+  for (int k = 0; k < m; ++k) {
+    uint32_t cnt = child_count(t, ch[k]);
+    if (cnt <= (uint32_t)leafSize) prims += cnt;
+    else ++inner;
+  }
+  // Unused slots marked INT_MIN (a valid leaf encoding never reaches it).
+  int4 out = make_int4(ch[0], m > 1 ? ch[1] : INT_MIN, m > 2 ? ch[2] : INT_MIN, m > 3 ? ch[3] : INT_MIN);
+  chOut[w] = out;
+  nInner[w] = inner;
+  nPrims[w] = prims;
+}
+
+__global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4 *chIn,
+                                const uint32_t *offInner, const uint32_t *offPrims, uint32_t base,
+                                uint32_t nextBase, uint32_t primBase, vt_wide_node *nodes,
+                                int32_t *nextLevel, const uint32_t *sorted, const vt_face *faces,
+                                const vt_vertex *verts, int32_t *order, float4 *tris) {
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= L) return;
+  int4 c4 = chIn[w];
+  int ch[4] = {c4.x, c4.y, c4.z, c4.w};
+  vt_wide_node nd;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    nd.lox[k] = nd.loy[k] = nd.loz[k] = nd.hix[k] = nd.hiy[k] = nd.hiz[k] = 0.0f;
+    nd.child[k] = 0;
+    nd.count[k] = 0;
+  }
+  uint32_t inner = offInner[w], prim = primBase + offPrims[w];
+  for (int k = 0; k < 4; ++k) {
+    if (ch[k] == INT_MIN) break;
+    Box b = child_box(t, ch[k]);
+    nd.lox[k] = b.lo.x; nd.loy[k] = b.lo.y; nd.loz[k] = b.lo.z;
+    nd.hix[k] = b.hi.x; nd.hiy[k] = b.hi.y; nd.hiz[k] = b.hi.z;
+    uint32_t cnt = child_count(t, ch[k]);
+    if (cnt <= (uint32_t)leafSize) {
+      nd.child[k] = -(int32_t)(prim + 1);
+      nd.count[k] = (int32_t)cnt;
+      // Leaves of the binary subtree, depth first, left first.
+      int st[2 * 8 + 2];
+      int top = 0;
+      st[top++] = ch[k];
+      while (top) {
+        int c = st[--top];
+        if (c < 0) {
+          uint32_t f = sorted[-c - 1];
+          order[prim] = (int32_t)f;
+          vt_face fc = faces[f];
+          const vt_vertex &va = verts[fc.a], &vb = verts[fc.b], &vc = verts[fc.c];
+          tris[3 * prim] = make_float4(va.px, va.py, va.pz, __int_as_float((int)f));
+          tris[3 * prim + 1] = make_float4(vb.px, vb.py, vb.pz, 0.0f);
+          tris[3 * prim + 2] = make_float4(vc.px, vc.py, vc.pz, 0.0f);
+          ++prim;
+          continue;
+        }
+        int2 cc = load_child(t, c);
+        st[top++] = cc.y;
+        st[top++] = cc.x;
+      }
+    } else {
+      nd.child[k] = (int32_t)(nextBase + inner);
+      nextLevel[inner] = ch[k];
+      ++inner;
+    }
+  }
+  nodes[base + w] = nd;
+}
+
+// SAH cost of the wide tree (node cost 1, triangle cost 1, areas over the root box's area).
+__global__ void k_sah(const vt_wide_node *nodes, uint32_t nn, double *acc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const vt_wide_node &r = nodes[0];
+  float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  for (int k = 0; k < 4; ++k) {
+    if (r.child[k] == 0) continue;
+    lo = make_float3(fminf(lo.x, r.lox[k]), fminf(lo.y, r.loy[k]), fminf(lo.z, r.loz[k]));
+    hi = make_float3(fmaxf(hi.x, r.hix[k]), fmaxf(hi.y, r.hiy[k]), fmaxf(hi.z, r.hiz[k]));
+  }
+  auto dA = [](double lx, double ly, double lz, double hx, double hy, double hz) {
+    double ex = fmax(0.0, hx - lx), ey = fmax(0.0, hy - ly), ez = fmax(0.0, hz - lz);
+    return ex * ey + ey * ez + ez * ex;
+  };
+  double A0 = dA(lo.x, lo.y, lo.z, hi.x, hi.y, hi.z);
+  if (!(A0 > 0.0)) A0 = 1.0;
+  double v = 0.0;
+  if (i < nn) {
+    if (i == 0) v += 1.0;
+    const vt_wide_node &nd = nodes[i];
+    for (int k = 0; k < 4; ++k) {
+      if (nd.child[k] == 0) continue;
+      double a = dA(nd.lox[k], nd.loy[k], nd.loz[k], nd.hix[k], nd.hiy[k], nd.hiz[k]) / A0;
+      v += nd.child[k] > 0 ? a : a * nd.count[k];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(acc, v);
+}
+
+struct DeviceArena {
+  std::vector<void *> ptrs;
+  ~DeviceArena() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <typename T> cudaError_t alloc(T **p, size_t count) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(T) + 16);
+    if (e == cudaSuccess) {
+      ptrs.push_back(q);
+      *p = static_cast<T *>(q);
+    }
+    return e;
+  }
+};
+
+inline uint32_t blocks(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+}  // namespace
+
+vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, const vt_build_options &opt, vt_mesh *mesh) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t n = nfaces;
+  mesh->nfaces = n;
+  if (n == 0) { mesh->nnodes = 0; mesh->depth = 0; return VT_OK; }
+  int leafSize = opt.leaf_size > 0 ? opt.leaf_size : 2;
+  int treelet = opt.treelet_size == 0 ? 7 : opt.treelet_size;
+  int rounds = opt.refine_rounds > 0 ? opt.refine_rounds : 2;
+  int maxDepth = opt.max_depth > 0 ? opt.max_depth : 31;
+  if (leafSize > 8) return vt_fail(ctx, VT_ERR_INVALID, "leaf_size must be in 1..8");
+  if (treelet > kMaxTreelet) treelet = kMaxTreelet;
+  if (treelet > 0 && treelet < 3) treelet = 3;
+
+  DeviceArena tmp;
+  float4 *boxes, *leafBox, *nodeBox;
+  uint32_t *bounds, *codes, *vals, *codesAlt, *valsAlt, *sortTemp, *flags, *count;
+  int2 *child;
+  int32_t *parent;
+  float *cost;
+  const uint32_t ni = n > 1 ? n - 1 : 1;
+  VT_CUDA(ctx, tmp.alloc(&boxes, 2 * (size_t)n));
+  VT_CUDA(ctx, tmp.alloc(&leafBox, 2 * (size_t)n));
+  VT_CUDA(ctx, tmp.alloc(&nodeBox, 2 * (size_t)ni));
+  VT_CUDA(ctx, tmp.alloc(&bounds, 16));
+  VT_CUDA(ctx, tmp.alloc(&codesAlt, n));
+  VT_CUDA(ctx, tmp.alloc(&valsAlt, n));
+  VT_CUDA(ctx, tmp.alloc(&sortTemp, vt_radix_temp_words(n)));
+  VT_CUDA(ctx, tmp.alloc(&flags, ni));
+  VT_CUDA(ctx, tmp.alloc(&count, ni));
+  VT_CUDA(ctx, tmp.alloc(&child, ni));
+  VT_CUDA(ctx, tmp.alloc(&parent, 2 * (size_t)n));
+  VT_CUDA(ctx, tmp.alloc(&cost, ni));
+  // Outputs kept by the mesh.
+  VT_CUDA(ctx, cudaMalloc(&mesh->d_codes, n * sizeof(uint32_t)));
+  VT_CUDA(ctx, cudaMalloc(&mesh->d_sorted, n * sizeof(int32_t)));
+  VT_CUDA(ctx, cudaMalloc(&mesh->d_order, n * sizeof(int32_t)));
+  VT_CUDA(ctx, cudaMalloc(&mesh->d_tris, 3 * (size_t)n * sizeof(float4)));
+  codes = mesh->d_codes;
+  vals = reinterpret_cast<uint32_t *>(mesh->d_sorted);
+
+  VT_CUDA(ctx, cudaEventRecord(ctx->ev0, s));
+  VT_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), s));
+  k_init_bounds<<<1, 32, 0, s>>>(bounds);
+  k_face_boxes<<<blocks(n, 256), 256, 0, s>>>(faces, n, verts, nverts, boxes, bounds, ctx->d_status);
+  k_morton<<<blocks(n, 256), 256, 0, s>>>(boxes, n, bounds, codes, vals);
+  vt_radix_sort_pairs(codes, vals, codesAlt, valsAlt, n, 30, sortTemp, s);
+  k_leaf_boxes<<<blocks(n, 256), 256, 0, s>>>(boxes, vals, n, leafBox);
+  TreeView t{(int)n, child, parent, leafBox, nodeBox, count, cost};
+  if (n >= 2) {
+    k_karras<<<blocks(n - 1, 256), 256, 0, s>>>(codes, (int)n, child, parent);
+    VT_CUDA(ctx, cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), s));
+    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, flags, 0, 0, ctx->d_status);
+    if (treelet > 0 && n >= 3) {
+      for (int r = 0; r < rounds; ++r) {
+        VT_CUDA(ctx, cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), s));
+        k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, flags, 1, treelet, ctx->d_status);
+      }
+    }
+  }
+  VT_CUDA(ctx, cudaGetLastError());
+
+  // Collapse, level by level. Per-level arrays are sized by the level (at most n wide nodes per
+  // level, fewer in practice); totals come back to the host to size the next level.
+  int32_t *levelA, *levelB;
+  int4 *chBuf;
+  uint32_t *nInner, *nPrims, *scanTemp, *totals;
+  VT_CUDA(ctx, tmp.alloc(&levelA, n));
+  VT_CUDA(ctx, tmp.alloc(&levelB, n));
+  VT_CUDA(ctx, tmp.alloc(&chBuf, n));
+  VT_CUDA(ctx, tmp.alloc(&nInner, n));
+  VT_CUDA(ctx, tmp.alloc(&nPrims, n));
+  VT_CUDA(ctx, tmp.alloc(&scanTemp, vt_scan_temp_words(n)));
+  VT_CUDA(ctx, tmp.alloc(&totals, 4));
+  // Wide node count is bounded by the binary internal count (each wide inner node consumes at
+  // least one binary internal node) plus the root.
+  const uint32_t maxNodes = ni + 1;
+  vt_wide_node *nodes;
+  VT_CUDA(ctx, cudaMalloc(&nodes, maxNodes * sizeof(vt_wide_node)));
+  mesh->d_nodes = nodes;
+  const int32_t rootRef = n >= 2 ? 0 : -1;
+  VT_CUDA(ctx, cudaMemcpyAsync(levelA, &rootRef, sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  uint32_t L = 1, base = 0, primBase = 0, depth = 0;
+  uint32_t host_tot[2];
+  while (L > 0) {
+    ++depth;
+    if ((int)depth > maxDepth) {
+      return vt_fail(ctx, VT_ERR_LIMIT, "BVH depth exceeds max_depth (" + std::to_string(maxDepth) + ")");
+    }
+    k_collapse_count<<<blocks(L, 128), 128, 0, s>>>(t, levelA, L, leafSize, chBuf, nInner, nPrims);
+    vt_scan_exclusive(nInner, nInner, L, scanTemp, totals, s);
+    vt_scan_exclusive(nPrims, nPrims, L, scanTemp, totals + 1, s);
+    const uint32_t nextBase = base + L;
+    k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, chBuf, nInner, nPrims, base,
+                                                   nextBase, primBase, nodes, levelB, vals, faces,
+                                                   verts, mesh->d_order, mesh->d_tris);
+    VT_CUDA(ctx, cudaMemcpyAsync(host_tot, totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VT_CUDA(ctx, cudaStreamSynchronize(s));
+    primBase += host_tot[1];
+    base = nextBase;
+    L = host_tot[0];
+    if (base + L > maxNodes) return vt_fail(ctx, VT_ERR_LIMIT, "wide node count exceeds its bound");
+    int32_t *x = levelA; levelA = levelB; levelB = x;
+  }
+  mesh->nnodes = base;
+  mesh->depth = depth;
+  if (primBase != n) return vt_fail(ctx, VT_ERR_DEVICE, "collapse emitted " + std::to_string(primBase) + " of " + std::to_string(n) + " triangles");
+
+  // Keep the refined binary tree for parity checks.
+  if (n >= 2) {
+    VT_CUDA(ctx, cudaMalloc(&mesh->d_bin_child, 2 * (size_t)(n - 1) * sizeof(int32_t)));
+    VT_CUDA(ctx, cudaMalloc(&mesh->d_bin_box, 8 * (size_t)(n - 1) * sizeof(float)));
+    VT_CUDA(ctx, cudaMemcpyAsync(mesh->d_bin_child, child, 2 * (size_t)(n - 1) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    VT_CUDA(ctx, cudaMemcpyAsync(mesh->d_bin_box, nodeBox, 8 * (size_t)(n - 1) * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  }
+  double *sah;
+  VT_CUDA(ctx, tmp.alloc(&sah, 1));
+  VT_CUDA(ctx, cudaMemsetAsync(sah, 0, sizeof(double), s));
+  k_sah<<<blocks(mesh->nnodes, 256), 256, 0, s>>>(nodes, mesh->nnodes, sah);
+  VT_CUDA(ctx, cudaEventRecord(ctx->ev1, s));
+  uint32_t hb[12], status = 0;
+  double hsah = 0.0;
+  VT_CUDA(ctx, cudaMemcpyAsync(hb, bounds + 0, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  VT_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  VT_CUDA(ctx, cudaMemcpyAsync(&hsah, sah, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VT_CUDA(ctx, cudaStreamSynchronize(s));
+  if (status & VT_DEV_BAD_INDEX) return vt_fail(ctx, VT_ERR_INVALID, "a face indexes past the vertex array");
+  if (status & VT_DEV_NONFINITE) return vt_fail(ctx, VT_ERR_INVALID, "a vertex position is not finite");
+  if (status & VT_DEV_TREELET) return vt_fail(ctx, VT_ERR_DEVICE, "treelet restructuring inconsistency");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  mesh->build_ms = ms;
+  mesh->sah = (float)hsah;
+  float m = 0.0f;
+  for (int k = 0; k < 3; ++k) {
+    mesh->lo[k] = ord2f(hb[6 + k]);
+    mesh->hi[k] = ord2f(hb[9 + k]);
+    m = fmaxf(m, fmaxf(fabsf(mesh->lo[k]), fabsf(mesh->hi[k])));
+  }
+  mesh->root_max = m;
+  return VT_OK;
+}

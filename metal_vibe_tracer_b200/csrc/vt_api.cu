@@ -1,0 +1,341 @@
+// vt_api.cu — the C ABI (include/vt.h): contexts, mesh publish, traversal entry points.
+#include <cstring>
+#include <string>
+
+#include "vt_internal.cuh"
+
+vt_status vt_fail(vt_ctx *ctx, vt_status code, const std::string &msg) {
+  if (ctx) ctx->error = msg;
+  return code;
+}
+
+vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(err);
+  return vt_fail(ctx, err == cudaErrorMemoryAllocation ? VT_ERR_MEMORY : VT_ERR_CUDA, m);
+}
+
+namespace {
+
+thread_local std::string g_no_ctx_error;
+
+void free_mesh(vt_mesh *m) {
+  if (!m) return;
+  cudaFree(m->d_nodes);
+  cudaFree(m->d_tris);
+  cudaFree(m->d_order);
+  cudaFree(m->d_codes);
+  cudaFree(m->d_sorted);
+  cudaFree(m->d_bin_child);
+  cudaFree(m->d_bin_box);
+  delete m;
+}
+
+vt_build_options defaults(const vt_build_options *o) {
+  vt_build_options r;
+  std::memset(&r, 0, sizeof r);
+  if (o) r = *o;
+  return r;
+}
+
+// Device-side copy of the chunk buffers for host pipelining.
+vt_status ensure_chunks(vt_ctx *ctx, size_t in_bytes, size_t out_bytes) {
+  if (in_bytes > ctx->chunk_in_bytes) {
+    for (int k = 0; k < 2; ++k) {
+      cudaFree(ctx->d_chunk_in[k]);
+      ctx->d_chunk_in[k] = nullptr;
+      VT_CUDA(ctx, cudaMalloc(&ctx->d_chunk_in[k], in_bytes));
+    }
+    ctx->chunk_in_bytes = in_bytes;
+  }
+  if (out_bytes > ctx->chunk_out_bytes) {
+    for (int k = 0; k < 2; ++k) {
+      cudaFree(ctx->d_chunk_out[k]);
+      ctx->d_chunk_out[k] = nullptr;
+      VT_CUDA(ctx, cudaMalloc(&ctx->d_chunk_out[k], out_bytes));
+    }
+    ctx->chunk_out_bytes = out_bytes;
+  }
+  return VT_OK;
+}
+
+vt_status check_trace_args(vt_ctx *ctx, const vt_mesh *mesh, const void *rays, const void *out, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh) return vt_fail(ctx, VT_ERR_INVALID, "mesh is null");
+  if (n > 0 && (!rays || !out)) return vt_fail(ctx, VT_ERR_INVALID, "rays or output is null");
+  if (n > 0 && mesh->nfaces > 0 && !mesh->d_nodes) return vt_fail(ctx, VT_ERR_INVALID, "mesh has no nodes");
+  return VT_OK;
+}
+
+// Chunk of rays per pipeline stage: 2^22 rays = 128 MB in, 64 MB out.
+constexpr uint32_t kChunk = 1u << 22;
+
+__global__ void k_fill_miss(int4 *hits, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) hits[i] = make_int4(0, 0, 0, -1);
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vt_abi_version(void) { return VT_ABI_VERSION; }
+
+vt_status vt_ctx_create(int32_t device, vt_ctx **out) {
+  if (!out) return VT_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    g_no_ctx_error = std::string("no CUDA device: ") + cudaGetErrorString(e);
+    return VT_ERR_CUDA;
+  }
+  if (device < 0 || device >= count) return VT_ERR_INVALID;
+  vt_ctx *c = new vt_ctx();
+  c->device = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->pipe[0], cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->pipe[1], cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
+      (e = cudaMalloc(&c->d_status, 64)) != cudaSuccess || (e = cudaMalloc(&c->d_counters, 256)) != cudaSuccess) {
+    g_no_ctx_error = std::string("context creation: ") + cudaGetErrorString(e);
+    vt_ctx_destroy(c);
+    return VT_ERR_CUDA;
+  }
+  cudaMemset(c->d_status, 0, 64);
+  *out = c;
+  return VT_OK;
+}
+
+vt_status vt_ctx_destroy(vt_ctx *ctx) {
+  if (!ctx) return VT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->pipe[k]) cudaStreamSynchronize(ctx->pipe[k]);
+    cudaFree(ctx->d_chunk_in[k]);
+    cudaFree(ctx->d_chunk_out[k]);
+    if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
+  }
+  cudaFree(ctx->d_status);
+  cudaFree(ctx->d_counters);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return VT_OK;
+}
+
+const char *vt_last_error(const vt_ctx *ctx) { return ctx ? ctx->error.c_str() : g_no_ctx_error.c_str(); }
+
+vt_status vt_sync(vt_ctx *ctx) {
+  if (!ctx) return VT_ERR_INVALID;
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return VT_OK;
+}
+
+vt_status vt_mesh_build_device(vt_ctx *ctx, const vt_face *faces_dev, uint32_t nfaces,
+                               const vt_vertex *verts_dev, uint32_t nverts,
+                               const vt_build_options *opts, vt_mesh **out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!out) return vt_fail(ctx, VT_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (nfaces > 0 && (!faces_dev || !verts_dev)) return vt_fail(ctx, VT_ERR_INVALID, "faces or vertices is null");
+  if (nfaces > (1u << 30)) return vt_fail(ctx, VT_ERR_LIMIT, "more than 2^30 faces");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  vt_mesh *m = new vt_mesh();
+  vt_build_options o = defaults(opts);
+  vt_status st = vt_lbvh_build(ctx, faces_dev, nfaces, verts_dev, nverts, o, m);
+  if (st != VT_OK) {
+    cudaStreamSynchronize(ctx->stream);
+    free_mesh(m);
+    return st;
+  }
+  *out = m;
+  return VT_OK;
+}
+
+vt_status vt_mesh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, const vt_build_options *opts, vt_mesh **out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (nfaces > 0 && (!faces || !verts)) return vt_fail(ctx, VT_ERR_INVALID, "faces or vertices is null");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  vt_face *df = nullptr;
+  vt_vertex *dv = nullptr;
+  if (nfaces > 0) {
+    VT_CUDA(ctx, cudaMalloc(&df, (size_t)nfaces * sizeof(vt_face)));
+    cudaError_t e = cudaMalloc(&dv, (size_t)(nverts ? nverts : 1) * sizeof(vt_vertex));
+    if (e != cudaSuccess) { cudaFree(df); return vt_cuda_fail(ctx, e, "cudaMalloc(vertices)"); }
+    e = cudaMemcpyAsync(df, faces, (size_t)nfaces * sizeof(vt_face), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && nverts)
+      e = cudaMemcpyAsync(dv, verts, (size_t)nverts * sizeof(vt_vertex), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) { cudaFree(df); cudaFree(dv); return vt_cuda_fail(ctx, e, "cudaMemcpyAsync(mesh)"); }
+  }
+  vt_status st = vt_mesh_build_device(ctx, df, nfaces, dv, nverts, opts, out);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(df);
+  cudaFree(dv);
+  return st;
+}
+
+vt_status vt_mesh_destroy(vt_ctx *ctx, vt_mesh *mesh) {
+  if (ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  free_mesh(mesh);
+  return VT_OK;
+}
+
+vt_status vt_mesh_get_info(vt_ctx *ctx, const vt_mesh *mesh, vt_mesh_info *out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh || !out) return vt_fail(ctx, VT_ERR_INVALID, "mesh or out is null");
+  out->faces = mesh->nfaces;
+  out->wide_nodes = mesh->nnodes;
+  out->binary_nodes = mesh->nfaces > 1 ? mesh->nfaces - 1 : 0;
+  out->depth = mesh->depth;
+  out->sah_cost = mesh->sah;
+  out->build_ms = mesh->build_ms;
+  for (int k = 0; k < 3; ++k) { out->lo[k] = mesh->lo[k]; out->hi[k] = mesh->hi[k]; }
+  return VT_OK;
+}
+
+vt_status vt_mesh_get_order(vt_ctx *ctx, const vt_mesh *mesh, int32_t *order, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh || (n && !order)) return vt_fail(ctx, VT_ERR_INVALID, "mesh or order is null");
+  if (n != mesh->nfaces) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the face count");
+  if (n) VT_CUDA(ctx, cudaMemcpy(order, mesh->d_order, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return VT_OK;
+}
+
+vt_status vt_mesh_get_nodes(vt_ctx *ctx, const vt_mesh *mesh, vt_wide_node *nodes, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh || (n && !nodes)) return vt_fail(ctx, VT_ERR_INVALID, "mesh or nodes is null");
+  if (n != mesh->nnodes) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the wide node count");
+  if (n) VT_CUDA(ctx, cudaMemcpy(nodes, mesh->d_nodes, n * sizeof(vt_wide_node), cudaMemcpyDeviceToHost));
+  return VT_OK;
+}
+
+vt_status vt_mesh_get_morton(vt_ctx *ctx, const vt_mesh *mesh, uint32_t *codes, int32_t *sorted, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh || (n && (!codes || !sorted))) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  if (n != mesh->nfaces) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the face count");
+  if (n) {
+    VT_CUDA(ctx, cudaMemcpy(codes, mesh->d_codes, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    VT_CUDA(ctx, cudaMemcpy(sorted, mesh->d_sorted, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  }
+  return VT_OK;
+}
+
+vt_status vt_mesh_get_binary(vt_ctx *ctx, const vt_mesh *mesh, int32_t *children, float *boxes, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!mesh || (n && (!children || !boxes))) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  uint32_t expect = mesh->nfaces > 1 ? mesh->nfaces - 1 : 0;
+  if (n != expect) return vt_fail(ctx, VT_ERR_INVALID, "n must equal faces - 1");
+  if (n) {
+    VT_CUDA(ctx, cudaMemcpy(children, mesh->d_bin_child, 2 * (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    // Device boxes are (lo xyz, pad, hi xyz, pad); the ABI packs 6 floats.
+    float *tmp = new float[8 * (size_t)n];
+    cudaError_t e = cudaMemcpy(tmp, mesh->d_bin_box, 8 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { delete[] tmp; return vt_cuda_fail(ctx, e, "cudaMemcpy(binary boxes)"); }
+    for (size_t i = 0; i < n; ++i) {
+      boxes[6 * i + 0] = tmp[8 * i + 0]; boxes[6 * i + 1] = tmp[8 * i + 1]; boxes[6 * i + 2] = tmp[8 * i + 2];
+      boxes[6 * i + 3] = tmp[8 * i + 4]; boxes[6 * i + 4] = tmp[8 * i + 5]; boxes[6 * i + 5] = tmp[8 * i + 6];
+    }
+    delete[] tmp;
+  }
+  return VT_OK;
+}
+
+vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                           vt_hit *hits_dev, void *stream) {
+  vt_status st = check_trace_args(ctx, mesh, rays_dev, hits_dev, n);
+  if (st) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  if (mesh->nfaces == 0) {
+    if (n) k_fill_miss<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<int4 *>(hits_dev), n);
+  } else {
+    vt_launch_closest(mesh, rays_dev, n, hits_dev, ctx->sm_count, s);
+  }
+  VT_CUDA(ctx, cudaGetLastError());
+  return VT_OK;
+}
+
+vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                       uint8_t *occluded_dev, void *stream) {
+  vt_status st = check_trace_args(ctx, mesh, rays_dev, occluded_dev, n);
+  if (st) return st;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  if (mesh->nfaces == 0) {
+    if (n) VT_CUDA(ctx, cudaMemsetAsync(occluded_dev, 0, n, s));
+  } else {
+    vt_launch_any(mesh, rays_dev, n, occluded_dev, ctx->sm_count, s);
+  }
+  VT_CUDA(ctx, cudaGetLastError());
+  return VT_OK;
+}
+
+// Host pipeline: chunk c goes on stream c % 2 as copy-in, trace, copy-out; the two streams let
+// chunk c + 1's copy-in and chunk c - 1's copy-out overlap chunk c's traversal.
+static vt_status trace_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
+                            void *out, size_t out_stride, bool closest) {
+  vt_status st = check_trace_args(ctx, mesh, rays, out, n);
+  if (st) return st;
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (n == 0) return VT_OK;
+  const uint32_t chunk = n < kChunk ? n : kChunk;
+  st = ensure_chunks(ctx, (size_t)chunk * sizeof(vt_ray), (size_t)chunk * out_stride);
+  if (st) return st;
+  // The previous user of these buffers may still be in flight on the other stream.
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[0]));
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[1]));
+  for (uint32_t c = 0, first = 0; first < n; ++c, first += chunk) {
+    const uint32_t m = n - first < chunk ? n - first : chunk;
+    const int k = c & 1;
+    cudaStream_t s = ctx->pipe[k];
+    VT_CUDA(ctx, cudaMemcpyAsync(ctx->d_chunk_in[k], rays + first, (size_t)m * sizeof(vt_ray),
+                                 cudaMemcpyHostToDevice, s));
+    const vt_ray *dr = static_cast<const vt_ray *>(ctx->d_chunk_in[k]);
+    if (closest) st = vt_trace_closest(ctx, mesh, dr, m, static_cast<vt_hit *>(ctx->d_chunk_out[k]), s);
+    else st = vt_trace_any(ctx, mesh, dr, m, static_cast<uint8_t *>(ctx->d_chunk_out[k]), s);
+    if (st) return st;
+    VT_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(out) + (size_t)first * out_stride, ctx->d_chunk_out[k],
+                                 (size_t)m * out_stride, cudaMemcpyDeviceToHost, s));
+  }
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[0]));
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[1]));
+  return VT_OK;
+}
+
+vt_status vt_trace_closest_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
+                                vt_hit *hits) {
+  return trace_host(ctx, mesh, rays, n, hits, sizeof(vt_hit), true);
+}
+
+vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
+                            uint8_t *occluded) {
+  return trace_host(ctx, mesh, rays, n, occluded, 1, false);
+}
+
+vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                         int32_t closest, uint64_t *nodes_visited, uint64_t *tris_tested) {
+  vt_status st = check_trace_args(ctx, mesh, rays_dev, nodes_visited, n);
+  if (st) return st;
+  if (!tris_tested) return vt_fail(ctx, VT_ERR_INVALID, "tris_tested is null");
+  *nodes_visited = 0;
+  *tris_tested = 0;
+  if (n == 0 || mesh->nfaces == 0) return VT_OK;
+  unsigned long long *acc = reinterpret_cast<unsigned long long *>(ctx->d_counters);
+  VT_CUDA(ctx, cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  vt_launch_count(mesh, rays_dev, n, closest, acc, ctx->stream);
+  VT_CUDA(ctx, cudaGetLastError());
+  unsigned long long h[2];
+  VT_CUDA(ctx, cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *nodes_visited = h[0];
+  *tris_tested = h[1];
+  return VT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// vt_internal.cuh — shared device/host definitions of libvt_b200 (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/vt.h"
+
+// ---------------------------------------------------------------------------------------------
+// Context and mesh objects behind the opaque C handles.
+
+struct vt_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;        // the context's own stream
+  cudaStream_t pipe[2] = {nullptr, nullptr};  // host-buffer pipelining (copy in, trace, copy out)
+  std::string error;
+  uint32_t *d_status = nullptr;         // device-side error word (build validation, kernels)
+  uint32_t *d_counters = nullptr;       // scratch counters for kernels (work queues)
+  // Host-pipeline device buffers (allocated on first use, grown as needed).
+  void *d_chunk_in[2] = {nullptr, nullptr};
+  void *d_chunk_out[2] = {nullptr, nullptr};
+  size_t chunk_in_bytes = 0, chunk_out_bytes = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct vt_mesh {
+  uint32_t nfaces = 0;
+  uint32_t nnodes = 0;       // 4-wide nodes
+  uint32_t depth = 0;        // 4-wide depth (root = 1)
+  float root_max = 0.0f;     // max |coordinate| over the scene bounds (slab enlargement)
+  float sah = 0.0f;
+  float build_ms = 0.0f;
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  vt_wide_node *d_nodes = nullptr;   // nnodes, reference layout (128 B, 16-B vector loads)
+  float4 *d_tris = nullptr;          // 3 per BVH position: (a, face id bits), (b, 0), (c, 0)
+  int32_t *d_order = nullptr;        // BVH position -> input face
+  uint32_t *d_codes = nullptr;       // sorted Morton codes
+  int32_t *d_sorted = nullptr;       // sorted position -> input face
+  int32_t *d_bin_child = nullptr;    // 2 per binary internal node (refined)
+  float *d_bin_box = nullptr;        // 8 per binary internal node (lo xyz, -, hi xyz, -)
+};
+
+// ---------------------------------------------------------------------------------------------
+// Error plumbing.
+
+vt_status vt_fail(vt_ctx *ctx, vt_status code, const std::string &msg);
+vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what);
+
+#define VT_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return vt_cuda_fail(ctx, _e, #call); \
+  } while (0)
+
+// Device error word bits (ctx->d_status).
+enum : uint32_t {
+  VT_DEV_BAD_INDEX = 1u,       // a face indexes past the vertex array
+  VT_DEV_NONFINITE = 2u,       // a vertex position is NaN or infinite
+  VT_DEV_STACK = 4u,           // traversal stack overflow
+  VT_DEV_TREELET = 8u          // treelet restructuring hit an internal inconsistency
+};
+
+// ---------------------------------------------------------------------------------------------
+// Build helpers implemented in scan_sort.cu / lbvh.cu.
+
+// Exclusive prefix sum of n uint32 values (in place allowed). `temp` must hold
+// vt_scan_temp_words(n) words. Returns the total through *total_dev if non-null (device word).
+size_t vt_scan_temp_words(uint32_t n);
+void vt_scan_exclusive(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *temp,
+                       uint32_t *total_dev, cudaStream_t s);
+
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of the keys.
+// keys/vals are sorted in place using the alternate buffers; temp is vt_radix_temp_words(n).
+size_t vt_radix_temp_words(uint32_t n);
+void vt_radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt, uint32_t *vals_alt,
+                         uint32_t n, int bits, uint32_t *temp, cudaStream_t s);
+
+vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, const vt_build_options &opt, vt_mesh *mesh);
+
+// Traversal launches (traverse.cu).
+void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits,
+                       int sm_count, cudaStream_t s);
+void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t *occ,
+                   int sm_count, cudaStream_t s);
+void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int closest,
+                     unsigned long long *acc /* 2 device words */, cudaStream_t s);

@@ -1,0 +1,139 @@
+"""Seeded synthetic workloads for the traversal path.
+
+Triangle soup: ``n`` triangles whose centroids are uniform in the unit cube, with edge lengths
+lognormal(mu = ln 0.002, sigma = 0.5) and uniformly random orientations; each triangle is
+equilateral with that edge length, rotated by a uniform random rotation about its centroid. FP32
+vertices, unwelded (three vertices per face).
+
+Ray sets (32-byte records: origin, tmin, direction, tmax):
+  * coherent: one primary ray per pixel of a W x H pinhole camera at (0.5, 0.5, -1.2) looking at
+    the cube centre (vertical field of view 45 degrees), tmin 0, tmax inf;
+  * incoherent: origins uniform in the cube, directions uniform on the sphere, tmin 0, tmax inf.
+Any-hit sets use the same rays with a finite tmax per ray (shadow-ray style): uniform in
+[1.0, 2.2] for the camera rays (the cube spans t in about [1.2, 2.4]) and in [0.05, 1.0] for the
+incoherent ones.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from ._lib import FACE_DTYPE, VERTEX_DTYPE
+
+
+def triangle_soup(n: int, seed: int = 0, mu: float = math.log(0.002), sigma: float = 0.5):
+    """(faces FACE_DTYPE[n], vertices VERTEX_DTYPE[3n]) of the soup described above."""
+    rng = np.random.default_rng(seed)
+    centre = rng.random((n, 3))
+    edge = rng.lognormal(mean=mu, sigma=sigma, size=n)
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    # Rotation matrix rows of unit quaternion (w, x, y, z).
+    R = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], axis=1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], axis=1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], axis=1),
+    ], axis=1)  # (n, 3, 3)
+    radius = edge / math.sqrt(3.0)
+    verts = np.empty((n, 3, 3))
+    for k in range(3):
+        a = 2.0 * math.pi * k / 3.0
+        local = np.array([math.cos(a), math.sin(a), 0.0])
+        verts[:, k, :] = centre + radius[:, None] * (R @ local)
+    v = np.zeros(3 * n, VERTEX_DTYPE)
+    v["p"] = verts.reshape(-1, 3).astype(np.float32)
+    f = np.zeros(n, FACE_DTYPE)
+    idx = np.arange(n, dtype=np.uint32)
+    f["a"], f["b"], f["c"] = 3 * idx, 3 * idx + 1, 3 * idx + 2
+    return f, v
+
+
+def _camera_dirs(xs, ys, width, height, fov_deg, lib):
+    eye = (0.5, 0.5, -1.2)
+    # Looking down +z at the cube centre; right = +x, up = +y.
+    th = math.tan(math.radians(fov_deg) * 0.5)
+    aspect = width / height
+    u = (2.0 * (xs + 0.5) / width - 1.0) * th * aspect
+    v = (1.0 - 2.0 * (ys + 0.5) / height) * th
+    d = lib.stack([u, v, lib.ones_like(u)], -1) if lib is not np else np.stack([u, v, np.ones_like(u)], -1)
+    norm = (d * d).sum(-1, keepdims=True) ** 0.5
+    return eye, d / norm
+
+
+def coherent_rays_np(width: int, height: int, rows: slice | None = None, fov_deg: float = 45.0):
+    """Camera rays (n, 8) float32 for the pixel rows in `rows` (all rows by default)."""
+    ys_all = np.arange(height, dtype=np.float64)
+    if rows is not None:
+        ys_all = ys_all[rows]
+    ys, xs = np.meshgrid(ys_all, np.arange(width, dtype=np.float64), indexing="ij")
+    eye, d = _camera_dirs(xs.reshape(-1), ys.reshape(-1), width, height, fov_deg, np)
+    out = np.empty((d.shape[0], 8), np.float32)
+    out[:, 0:3] = eye
+    out[:, 3] = 0.0
+    out[:, 4:7] = d
+    out[:, 7] = np.inf
+    return out
+
+
+def incoherent_rays_np(n: int, seed: int = 1):
+    rng = np.random.default_rng(seed)
+    o = rng.random((n, 3))
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out = np.empty((n, 8), np.float32)
+    out[:, 0:3] = o
+    out[:, 3] = 0.0
+    out[:, 4:7] = d
+    out[:, 7] = np.inf
+    return out
+
+
+def shadow_tmax_np(rays: np.ndarray, coherent: bool, seed: int = 2) -> np.ndarray:
+    """Copy of `rays` with the any-hit tmax distribution of the set."""
+    rng = np.random.default_rng(seed)
+    out = rays.copy()
+    lo, hi = (1.0, 2.2) if coherent else (0.05, 1.0)
+    out[:, 7] = (lo + (hi - lo) * rng.random(rays.shape[0])).astype(np.float32)
+    return out
+
+
+def coherent_rays_torch(width: int, height: int, device, fov_deg: float = 45.0):
+    import torch
+    ys, xs = torch.meshgrid(torch.arange(height, device=device, dtype=torch.float64),
+                            torch.arange(width, device=device, dtype=torch.float64), indexing="ij")
+    eye, d = _camera_dirs(xs.reshape(-1), ys.reshape(-1), width, height, fov_deg, torch)
+    out = torch.empty((d.shape[0], 8), dtype=torch.float32, device=device)
+    out[:, 0] = eye[0]
+    out[:, 1] = eye[1]
+    out[:, 2] = eye[2]
+    out[:, 3] = 0.0
+    out[:, 4:7] = d.float()
+    out[:, 7] = float("inf")
+    return out
+
+
+def incoherent_rays_torch(n: int, device, seed: int = 1):
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    o = torch.rand((n, 3), generator=g, device=device, dtype=torch.float32)
+    d = torch.randn((n, 3), generator=g, device=device, dtype=torch.float32)
+    d = d / d.norm(dim=1, keepdim=True)
+    out = torch.empty((n, 8), dtype=torch.float32, device=device)
+    out[:, 0:3] = o
+    out[:, 3] = 0.0
+    out[:, 4:7] = d
+    out[:, 7] = float("inf")
+    return out
+
+
+def shadow_tmax_torch(rays, coherent: bool, seed: int = 2):
+    import torch
+    g = torch.Generator(device=rays.device)
+    g.manual_seed(seed)
+    out = rays.clone()
+    lo, hi = (1.0, 2.2) if coherent else (0.05, 1.0)
+    out[:, 7] = lo + (hi - lo) * torch.rand((rays.shape[0],), generator=g, device=rays.device)
+    return out

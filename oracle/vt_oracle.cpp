@@ -1,0 +1,1043 @@
+// vt_oracle.cpp — CPU restatement of the reference's traversal and BVH-build arithmetic.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA path (tests, smoke check, bench CPU
+// baseline). Built by oracle/Makefile with -ffp-contract=off so every float product and sum
+// rounds on its own, exactly as the CUDA kernels' __fmul_rn/__fadd_rn sequence does.
+// See vt_oracle.h for the list of reference functions restated here.
+#include "vt_oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// ------------------------------------------------------------------------------------------
+// PCG hash stream (main.swift:91-101): pcg_hash and the 24-bit float draw of rand_f.
+uint32_t pcg_hash(uint32_t input) {
+  uint32_t state = input * 747796405u + 2891336453u;
+  uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+  return (word >> 22u) ^ word;
+}
+
+// ------------------------------------------------------------------------------------------
+// Small vector helpers.
+struct F3 { float x, y, z; };
+inline float comp(const F3 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+inline F3 fmin3(F3 a, F3 b) { return {std::fmin(a.x, b.x), std::fmin(a.y, b.y), std::fmin(a.z, b.z)}; }
+inline F3 fmax3(F3 a, F3 b) { return {std::fmax(a.x, b.x), std::fmax(a.y, b.y), std::fmax(a.z, b.z)}; }
+
+// Surface-area measure of the reference's WideBVH.area (Sources/Acceleration.swift:125-128):
+// e = max(hi - lo, 0); e.x e.y + e.y e.z + e.z e.x, each product and sum rounded on its own.
+inline float box_area(F3 lo, F3 hi) {
+  float ex = std::fmax(hi.x - lo.x, 0.0f), ey = std::fmax(hi.y - lo.y, 0.0f),
+        ez = std::fmax(hi.z - lo.z, 0.0f);
+  return (ex * ey + ey * ez) + ez * ex;
+}
+
+struct Box { F3 lo, hi; };
+inline Box box_union(const Box &a, const Box &b) { return {fmin3(a.lo, b.lo), fmax3(a.hi, b.hi)}; }
+const float kBig = 3.4028234663852886e38f;
+inline Box empty_box() { return {{kBig, kBig, kBig}, {-kBig, -kBig, -kBig}}; }
+
+inline F3 vpos(const vt_vertex &v) { return {v.px, v.py, v.pz}; }
+
+// Triangle bounds of face i (Sources/Acceleration.swift:466-473, MeshSceneLayout.bounds).
+inline Box face_box(const vt_face &f, const vt_vertex *v) {
+  F3 a = vpos(v[f.a]), b = vpos(v[f.b]), c = vpos(v[f.c]);
+  return {fmin3(fmin3(a, b), c), fmax3(fmax3(a, b), c)};
+}
+
+// ------------------------------------------------------------------------------------------
+// Watertight ray/triangle test (main.swift:1536-1582). The ray is translated to the origin and
+// sheared/scaled onto +z once; each vertex maps to (A[kx] - Sx A[kz], A[ky] - Sy A[kz], Sz A[kz]);
+// edge functions are fl(fl(p.x q.y) - fl(p.y q.x)) with the exact FMA tie fallback; a hit needs
+// all edge signs to agree (0 counts for both), det != 0 and t in [tMin, tMax).
+template <typename T> struct WRay {
+  T o[3];
+  int kx, ky, kz;
+  T Sx, Sy, Sz;
+};
+template <typename T> WRay<T> make_wray(const T o[3], const T d[3]) {
+  WRay<T> w;
+  T ax = std::fabs(d[0]), ay = std::fabs(d[1]), az = std::fabs(d[2]);
+  int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+  // Swapping x and y for a negative z direction preserves the winding.
+  if (d[kz] < T(0)) std::swap(kx, ky);
+  w.kx = kx; w.ky = ky; w.kz = kz;
+  w.Sx = d[kx] / d[kz];
+  w.Sy = d[ky] / d[kz];
+  w.Sz = T(1) / d[kz];
+  for (int k = 0; k < 3; ++k) w.o[k] = o[k];
+  return w;
+}
+template <typename T> inline T edge_fn(T px, T py, T qx, T qy) {
+  T x = px * qy, y = py * qx, e = x - y;
+  if (e == T(0)) e = std::fma(px, qy, -x) - std::fma(py, qx, -y);
+  return e;
+}
+template <typename T>
+bool intersect_tri(const WRay<T> &r, const T a[3], const T b[3], const T c[3], T tMin, T tMax, T &t,
+                   T &b1, T &b2) {
+  T A[3], B[3], C[3];
+  for (int k = 0; k < 3; ++k) { A[k] = a[k] - r.o[k]; B[k] = b[k] - r.o[k]; C[k] = c[k] - r.o[k]; }
+  T ax = A[r.kx] - r.Sx * A[r.kz], ay = A[r.ky] - r.Sy * A[r.kz];
+  T bx = B[r.kx] - r.Sx * B[r.kz], by = B[r.ky] - r.Sy * B[r.kz];
+  T cx = C[r.kx] - r.Sx * C[r.kz], cy = C[r.ky] - r.Sy * C[r.kz];
+  T U = edge_fn(cx, cy, bx, by), V = edge_fn(ax, ay, cx, cy);
+  if ((U < 0 && V > 0) || (U > 0 && V < 0)) return false;
+  T W = edge_fn(bx, by, ax, ay);
+  if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
+  T det = (U + V) + W;
+  if (det == T(0)) return false;
+  T az = r.Sz * A[r.kz], bz = r.Sz * B[r.kz], cz = r.Sz * C[r.kz];
+  T Tn = (U * az + V * bz) + W * cz;
+  T inv = T(1) / det;
+  t = Tn * inv;
+  b1 = V * inv;
+  b2 = W * inv;
+  return t >= tMin && t < tMax;
+}
+
+// ------------------------------------------------------------------------------------------
+// A built 4-wide BVH: nodes in the reference layout plus the triangles in BVH order.
+struct BinNode { int32_t child[2]; Box box; };
+
+}  // namespace
+
+struct vto_bvh {
+  std::vector<vt_wide_node> nodes;
+  std::vector<int32_t> order;       // order[i] = input face at BVH position i
+  std::vector<float> tris;          // 9 floats per BVH position
+  uint32_t faces = 0, depth = 0;
+  float root_max = 0.0f;            // max |coordinate| over the scene bounds
+  Box bounds = empty_box();
+  // LBVH-only stages
+  std::vector<uint32_t> codes;      // sorted Morton codes
+  std::vector<int32_t> sorted;      // face index per sorted position
+  std::vector<BinNode> binary;      // refined binary tree (n - 1 internal nodes)
+  double sah = 0.0;
+};
+
+namespace {
+
+void finish_bvh(vto_bvh *h, const vt_face *faces, const vt_vertex *verts) {
+  size_t n = h->order.size();
+  h->tris.resize(9 * n);
+  for (size_t i = 0; i < n; ++i) {
+    const vt_face &f = faces[h->order[i]];
+    const vt_vertex *p[3] = {&verts[f.a], &verts[f.b], &verts[f.c]};
+    for (int k = 0; k < 3; ++k) {
+      h->tris[9 * i + 3 * k + 0] = p[k]->px;
+      h->tris[9 * i + 3 * k + 1] = p[k]->py;
+      h->tris[9 * i + 3 * k + 2] = p[k]->pz;
+    }
+  }
+  Box b = empty_box();
+  for (uint32_t i = 0; i < h->faces; ++i) b = box_union(b, face_box(faces[i], verts));
+  h->bounds = b;
+  float m = 0.0f;
+  if (h->faces) {
+    m = std::fmax(std::fmax(std::fabs(b.lo.x), std::fabs(b.lo.y)), std::fabs(b.lo.z));
+    m = std::fmax(m, std::fmax(std::fmax(std::fabs(b.hi.x), std::fabs(b.hi.y)), std::fabs(b.hi.z)));
+  }
+  h->root_max = m;
+  // SAH cost: wide node cost 1, triangle cost 1, areas relative to the root box.
+  double sah = 0.0;
+  if (!h->nodes.empty()) {
+    std::vector<double> area(h->nodes.size(), 0.0);
+    Box root = empty_box();
+    const vt_wide_node &r = h->nodes[0];
+    for (int k = 0; k < 4; ++k)
+      if (r.child[k] != 0) root = box_union(root, Box{{r.lox[k], r.loy[k], r.loz[k]}, {r.hix[k], r.hiy[k], r.hiz[k]}});
+    auto dA = [](Box x) {
+      double ex = std::max(0.0, double(x.hi.x) - x.lo.x), ey = std::max(0.0, double(x.hi.y) - x.lo.y),
+             ez = std::max(0.0, double(x.hi.z) - x.lo.z);
+      return ex * ey + ey * ez + ez * ex;
+    };
+    double A0 = dA(root);
+    if (A0 <= 0) A0 = 1.0;
+    area[0] = A0;
+    for (size_t i = 0; i < h->nodes.size(); ++i) {
+      const vt_wide_node &nd = h->nodes[i];
+      sah += area[i] / A0;
+      for (int k = 0; k < 4; ++k) {
+        Box cb{{nd.lox[k], nd.loy[k], nd.loz[k]}, {nd.hix[k], nd.hiy[k], nd.hiz[k]}};
+        if (nd.child[k] > 0) area[nd.child[k]] = dA(cb);
+        else if (nd.child[k] < 0) sah += dA(cb) / A0 * nd.count[k];
+      }
+    }
+  }
+  h->sah = sah;
+}
+
+// ------------------------------------------------------------------------------------------
+// LBVH (the GPU build's definition; no reference counterpart).
+//
+// Morton code of a centroid c = (lo + hi) * 0.5 inside the centroid bounds [clo, chi]: per axis
+// q = min(uint((c - clo) * (1024 / (chi - clo))), 1023) (0 on a flat axis), bits interleaved
+// x2 y1 z0. Faces sort by (code, face index). The binary hierarchy is Karras' (HPG 2012) over
+// the sorted keys with the face index breaking code ties.
+inline uint32_t expand_bits(uint32_t v) {
+  v = (v * 0x00010001u) & 0xFF0000FFu;
+  v = (v * 0x00000101u) & 0x0F00F00Fu;
+  v = (v * 0x00000011u) & 0xC30C30C3u;
+  v = (v * 0x00000005u) & 0x49249249u;
+  return v;
+}
+inline uint32_t quantize(float c, float clo, float chi) {
+  float ext = chi - clo;
+  if (!(ext > 0.0f)) return 0u;
+  float scale = 1024.0f / ext;
+  float f = (c - clo) * scale;
+  uint32_t q = f >= 1023.0f ? 1023u : (uint32_t)f;
+  return q;
+}
+
+inline int clz32(uint32_t v) { return v ? __builtin_clz(v) : 32; }
+
+struct Karras {
+  const uint32_t *codes;
+  int n;
+  int delta(int i, int j) const {
+    if (j < 0 || j > n - 1) return -1;
+    uint32_t a = codes[i], b = codes[j];
+    if (a != b) return clz32(a ^ b);
+    return 32 + clz32((uint32_t)i ^ (uint32_t)j);
+  }
+};
+
+// Leaf encoding in the binary tree: internal node index >= 0, leaf = -(sorted position + 1).
+struct LbvhTree {
+  int n;
+  std::vector<BinNode> nodes;      // n - 1 internal nodes
+  std::vector<Box> leafBox;        // per sorted position
+  std::vector<int32_t> parent;     // internal nodes then leaves (index n - 1 + pos)
+  std::vector<uint32_t> count;     // leaves under each internal node
+  std::vector<float> cost;         // SAH cost of each internal node's subtree
+};
+
+const float kCi = 1.2f, kCt = 1.0f;  // treelet restructuring costs (internal node, triangle)
+
+inline Box child_box(const LbvhTree &t, int c) { return c >= 0 ? t.nodes[c].box : t.leafBox[-c - 1]; }
+inline float child_cost(const LbvhTree &t, int c) {
+  return c >= 0 ? t.cost[c] : kCt * box_area(t.leafBox[-c - 1].lo, t.leafBox[-c - 1].hi);
+}
+inline uint32_t child_count(const LbvhTree &t, int c) { return c >= 0 ? t.count[c] : 1u; }
+
+// Bottom-up boxes, leaf counts and SAH costs (post-order, so children are final first).
+void lbvh_refit(LbvhTree &t) {
+  if (t.n < 2) return;
+  std::vector<int> stack{0}, post;
+  while (!stack.empty()) {
+    int i = stack.back(); stack.pop_back();
+    post.push_back(i);
+    for (int k = 0; k < 2; ++k) if (t.nodes[i].child[k] >= 0) stack.push_back(t.nodes[i].child[k]);
+  }
+  for (auto it = post.rbegin(); it != post.rend(); ++it) {
+    int i = *it;
+    int l = t.nodes[i].child[0], r = t.nodes[i].child[1];
+    Box b = box_union(child_box(t, l), child_box(t, r));
+    t.nodes[i].box = b;
+    t.count[i] = child_count(t, l) + child_count(t, r);
+    t.cost[i] = kCi * box_area(b.lo, b.hi) + (child_cost(t, l) + child_cost(t, r));
+  }
+}
+
+// Treelet restructuring (Karras and Aila, HPG 2013), deterministic form shared with the GPU:
+// at an internal node whose subtree holds >= gamma leaves, grow a treelet by repeatedly opening
+// the treelet leaf (an internal node) of largest area (first in list order on ties; the opened
+// node is replaced in place by its left child and its right child is appended) until `size`
+// leaves; find the SAH-optimal topology over those leaves by dynamic programming over subsets
+// (partitions enumerated p = (p - 1) & s downwards, strict improvement keeps the first); if its
+// cost is strictly below the current subtree cost, rebuild the treelet with the same internal
+// nodes (root first, then in the order they were opened), assigning them depth-first, left
+// partition (the one holding the lowest set leaf bit) first.
+struct Treelet {
+  int size;
+  int leaves[8];
+  int internals[8];
+  int nl = 0, ni = 0;
+};
+
+void restructure_node(LbvhTree &t, int root, int size) {
+  Treelet tl;
+  tl.size = size;
+  tl.internals[tl.ni++] = root;
+  tl.leaves[tl.nl++] = t.nodes[root].child[0];
+  tl.leaves[tl.nl++] = t.nodes[root].child[1];
+  while (tl.nl < size) {
+    int best = -1;
+    float bestA = -1.0f;
+    for (int k = 0; k < tl.nl; ++k) {
+      int c = tl.leaves[k];
+      if (c < 0) continue;
+      float a = box_area(t.nodes[c].box.lo, t.nodes[c].box.hi);
+      if (a > bestA) { bestA = a; best = k; }
+    }
+    if (best < 0) break;
+    int c = tl.leaves[best];
+    tl.internals[tl.ni++] = c;
+    tl.leaves[best] = t.nodes[c].child[0];
+    tl.leaves[tl.nl++] = t.nodes[c].child[1];
+  }
+  int k = tl.nl;
+  if (k < 3) return;
+  int full = (1 << k) - 1;
+  float area[256], copt[256];
+  uint8_t part[256];
+  Box sb[256];
+  for (int s = 1; s <= full; ++s) {
+    int low = __builtin_ctz(s);
+    Box b = child_box(t, tl.leaves[low]);
+    if (s != (1 << low)) b = box_union(sb[s & (s - 1)], b);
+    sb[s] = b;
+    area[s] = box_area(b.lo, b.hi);
+  }
+  for (int i = 0; i < k; ++i) copt[1 << i] = child_cost(t, tl.leaves[i]);
+  // Subsets by increasing size so every proper subset is final first.
+  for (int sz = 2; sz <= k; ++sz) {
+    for (int s = 1; s <= full; ++s) {
+      if (__builtin_popcount(s) != sz) continue;
+      float best = kBig;
+      int bp = 0;
+      for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+        float c = copt[p] + copt[s ^ p];
+        if (c < best) { best = c; bp = p; }
+      }
+      copt[s] = kCi * area[s] + best;
+      part[s] = (uint8_t)bp;
+    }
+  }
+  if (!(copt[full] < t.cost[root])) return;
+  // Rebuild: assign internal nodes depth-first from the root.
+  int next = 0;
+  struct Item { int s, node; };
+  Item stack[16];
+  int top = 0;
+  stack[top++] = {full, tl.internals[next++]};
+  while (top) {
+    Item it = stack[--top];
+    int p = part[it.s], q = it.s ^ p;
+    // Left = the side holding the lowest leaf bit of the subset.
+    int lowbit = it.s & -it.s;
+    int L = (p & lowbit) ? p : q, R = (p & lowbit) ? q : p;
+    int kids[2];
+    int subs[2] = {L, R};
+    for (int c = 0; c < 2; ++c) {
+      int s = subs[c];
+      if ((s & (s - 1)) == 0) kids[c] = tl.leaves[__builtin_ctz(s)];
+      else kids[c] = tl.internals[next++];
+    }
+    t.nodes[it.node].child[0] = kids[0];
+    t.nodes[it.node].child[1] = kids[1];
+    // Push right then left so the left subtree is assigned first.
+    for (int c = 1; c >= 0; --c) if ((subs[c] & (subs[c] - 1)) != 0) stack[top++] = {subs[c], kids[c]};
+  }
+  // Refit the treelet's internal nodes bottom-up (reverse assignment order is a valid order:
+  // every node was assigned after its parent).
+  for (int i = tl.ni - 1; i >= 0; --i) {
+    int nd = tl.internals[i];
+    int l = t.nodes[nd].child[0], r = t.nodes[nd].child[1];
+    Box b = box_union(child_box(t, l), child_box(t, r));
+    t.nodes[nd].box = b;
+    t.count[nd] = child_count(t, l) + child_count(t, r);
+    t.cost[nd] = kCi * box_area(b.lo, b.hi) + (child_cost(t, l) + child_cost(t, r));
+    for (int c = 0; c < 2; ++c) {
+      int ch = t.nodes[nd].child[c];
+      t.parent[ch >= 0 ? ch : (t.n - 1 + (-ch - 1))] = nd;
+    }
+  }
+}
+
+// One restructuring round: nodes in post-order (children before parents), as the GPU's
+// bottom-up pass finalises them.
+void restructure_round(LbvhTree &t, int size) {
+  if (t.n < 2) return;
+  std::vector<int> stack{0}, post;
+  while (!stack.empty()) {
+    int i = stack.back(); stack.pop_back();
+    post.push_back(i);
+    for (int k = 0; k < 2; ++k) if (t.nodes[i].child[k] >= 0) stack.push_back(t.nodes[i].child[k]);
+  }
+  for (auto it = post.rbegin(); it != post.rend(); ++it)
+    if (t.count[*it] >= (uint32_t)size) restructure_node(t, *it, size);
+}
+
+// Collapse to the 4-wide layout, numbered level by level (breadth first): a wide node rooted at
+// binary node b starts with children [b] and repeatedly splits the child of largest area among
+// those with more than leafSize leaves (the reference's rule, Sources/Acceleration.swift:255-263);
+// children with <= leafSize leaves become leaves whose triangles (depth-first, left first) are
+// numbered in (node, slot) order; the others become the next level's nodes in (node, slot) order.
+void lbvh_collapse(const LbvhTree &t, const std::vector<int32_t> &sorted, int leafSize, vto_bvh *h) {
+  int n = t.n;
+  h->nodes.clear();
+  h->order.clear();
+  if (n == 0) { h->depth = 0; return; }
+  int rootRef = n >= 2 ? 0 : -1;
+  std::vector<int> level{rootRef};
+  uint32_t depth = 0;
+  while (!level.empty()) {
+    ++depth;
+    size_t base = h->nodes.size();
+    size_t nextBase = base + level.size();
+    std::vector<int> next;
+    for (size_t w = 0; w < level.size(); ++w) {
+      int ch[4];
+      int m = 0;
+      ch[m++] = level[w];
+      while (m < 4) {
+        int best = -1;
+        float bestA = 0.0f;
+        for (int k = 0; k < m; ++k) {
+          if (child_count(t, ch[k]) <= (uint32_t)leafSize) continue;
+          Box b = child_box(t, ch[k]);
+          float a = box_area(b.lo, b.hi);
+          if (best < 0 || a > bestA) { best = k; bestA = a; }
+        }
+        if (best < 0) break;
+        int c = ch[best];
+        for (int k = m; k > best + 1; --k) ch[k] = ch[k - 1];
+        ch[best] = t.nodes[c].child[0];
+        ch[best + 1] = t.nodes[c].child[1];
+        ++m;
+      }
+      vt_wide_node nd;
+      std::memset(&nd, 0, sizeof nd);
+      for (int k = 0; k < m; ++k) {
+        Box b = child_box(t, ch[k]);
+        nd.lox[k] = b.lo.x; nd.loy[k] = b.lo.y; nd.loz[k] = b.lo.z;
+        nd.hix[k] = b.hi.x; nd.hiy[k] = b.hi.y; nd.hiz[k] = b.hi.z;
+        uint32_t cnt = child_count(t, ch[k]);
+        if (cnt <= (uint32_t)leafSize) {
+          nd.child[k] = -(int32_t)(h->order.size() + 1);
+          nd.count[k] = (int32_t)cnt;
+          // Leaves of the binary subtree, depth first, left first.
+          int st[64];
+          int top = 0;
+          st[top++] = ch[k];
+          while (top) {
+            int c = st[--top];
+            if (c < 0) { h->order.push_back(sorted[-c - 1]); continue; }
+            st[top++] = t.nodes[c].child[1];
+            st[top++] = t.nodes[c].child[0];
+          }
+        } else {
+          nd.child[k] = (int32_t)(nextBase + next.size());
+          nd.count[k] = 0;
+          next.push_back(ch[k]);
+        }
+      }
+      h->nodes.push_back(nd);
+    }
+    level.swap(next);
+  }
+  h->depth = depth;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vto_pcg_hash(uint32_t v) { return pcg_hash(v); }
+float vto_rand_f(uint32_t *seed) {
+  *seed = pcg_hash(*seed);
+  return float(*seed >> 8u) * (1.0f / 16777216.0f);
+}
+
+int32_t vto_intersect_f32(const vt_ray *ray, const float *tri, float *t, float *b1, float *b2) {
+  float o[3] = {ray->ox, ray->oy, ray->oz}, d[3] = {ray->dx, ray->dy, ray->dz};
+  WRay<float> w = make_wray(o, d);
+  return intersect_tri<float>(w, tri, tri + 3, tri + 6, ray->tmin, ray->tmax, *t, *b1, *b2) ? 1 : 0;
+}
+int32_t vto_intersect_f64(const double *ray, const double *tri, double tmin, double tmax, double *t,
+                          double *b1, double *b2) {
+  WRay<double> w = make_wray(ray, ray + 3);
+  return intersect_tri<double>(w, tri, tri + 3, tri + 6, tmin, tmax, *t, *b1, *b2) ? 1 : 0;
+}
+
+vto_bvh *vto_lbvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, int32_t leaf_size, int32_t treelet_size, int32_t rounds) {
+  (void)nverts;
+  vto_bvh *h = new vto_bvh();
+  h->faces = nfaces;
+  int n = (int)nfaces;
+  if (leaf_size < 1) leaf_size = 2;
+  std::vector<Box> boxes(n);
+  std::vector<F3> cent(n);
+  Box cb = empty_box();
+  for (int i = 0; i < n; ++i) {
+    boxes[i] = face_box(faces[i], verts);
+    F3 c = {(boxes[i].lo.x + boxes[i].hi.x) * 0.5f, (boxes[i].lo.y + boxes[i].hi.y) * 0.5f,
+            (boxes[i].lo.z + boxes[i].hi.z) * 0.5f};
+    cent[i] = c;
+    cb.lo = fmin3(cb.lo, c);
+    cb.hi = fmax3(cb.hi, c);
+  }
+  std::vector<uint64_t> keys(n);
+  for (int i = 0; i < n; ++i) {
+    uint32_t qx = quantize(cent[i].x, cb.lo.x, cb.hi.x), qy = quantize(cent[i].y, cb.lo.y, cb.hi.y),
+             qz = quantize(cent[i].z, cb.lo.z, cb.hi.z);
+    uint32_t code = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
+    keys[i] = (uint64_t(code) << 32) | uint32_t(i);
+  }
+  std::sort(keys.begin(), keys.end());
+  h->codes.resize(n);
+  h->sorted.resize(n);
+  for (int i = 0; i < n; ++i) {
+    h->codes[i] = uint32_t(keys[i] >> 32);
+    h->sorted[i] = int32_t(keys[i] & 0xffffffffu);
+  }
+  LbvhTree t;
+  t.n = n;
+  t.nodes.resize(n > 1 ? n - 1 : 0);
+  t.count.assign(t.nodes.size(), 0);
+  t.cost.assign(t.nodes.size(), 0.0f);
+  t.parent.assign(n > 0 ? 2 * n - 1 : 0, -1);
+  t.leafBox.resize(n);
+  for (int i = 0; i < n; ++i) t.leafBox[i] = boxes[h->sorted[i]];
+  Karras K{h->codes.data(), n};
+  for (int i = 0; i < n - 1; ++i) {
+    int d = K.delta(i, i + 1) - K.delta(i, i - 1) > 0 ? 1 : -1;
+    int dmin = K.delta(i, i - d);
+    int lmax = 2;
+    while (K.delta(i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int s = lmax / 2; s >= 1; s /= 2)
+      if (K.delta(i, i + (l + s) * d) > dmin) l += s;
+    int j = i + l * d;
+    int dnode = K.delta(i, j);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+      int step = (l + div - 1) / div;
+      if (K.delta(i, i + (s + step) * d) > dnode) s += step;
+      if (step == 1) break;
+    }
+    int gamma = i + s * d + std::min(d, 0);
+    int lo = std::min(i, j), hi = std::max(i, j);
+    int left = lo == gamma ? -(gamma + 1) : gamma;
+    int right = hi == gamma + 1 ? -(gamma + 2) : gamma + 1;
+    t.nodes[i].child[0] = left;
+    t.nodes[i].child[1] = right;
+    t.parent[left >= 0 ? left : (n - 1 + gamma)] = i;
+    t.parent[right >= 0 ? right : (n - 1 + gamma + 1)] = i;
+  }
+  lbvh_refit(t);
+  if (treelet_size == 0) treelet_size = 7;
+  if (rounds <= 0) rounds = 2;
+  if (treelet_size > 0 && n >= 3) {
+    if (treelet_size < 3) treelet_size = 3;
+    if (treelet_size > 8) treelet_size = 8;
+    for (int r = 0; r < rounds; ++r) restructure_round(t, treelet_size);
+  }
+  h->binary = t.nodes;
+  lbvh_collapse(t, h->sorted, leaf_size, h);
+  finish_bvh(h, faces, verts);
+  return h;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Reference binned-SAH 4-wide build (WideBVH, Sources/Acceleration.swift:106-352), restated:
+// 16 bins on each axis with a non-zero finite scale, SAH cost area x count of both sides, the
+// in-place two-pointer partition, coincident-centroid / balanced fallback to an object median on
+// the widest centroid axis, each node splitting its largest-area child (most populous in median
+// mode) until four children, depth-first numbering with subtrees below n/16 deferred and appended
+// in order (n >= 65536), and a median rebuild past the depth limit.
+namespace {
+
+struct Range {
+  int start, end;
+  F3 lo, hi, clo, chi;
+  int count() const { return end - start; }
+  float area() const { return box_area(lo, hi); }
+};
+
+struct WideBuilder {
+  const float *bounds;  // 6 per item
+  int32_t *order;
+  int leafSize;
+  bool median;
+  static const int kBins = 16;
+  F3 binLo[3 * kBins], binHi[3 * kBins], binCLo[3 * kBins], binCHi[3 * kBins];
+  int binCount[3 * kBins];
+  float suffix[kBins];
+
+  F3 lo(int i) const { return {bounds[6 * i], bounds[6 * i + 1], bounds[6 * i + 2]}; }
+  F3 hi(int i) const { return {bounds[6 * i + 3], bounds[6 * i + 4], bounds[6 * i + 5]}; }
+  Range measure(int start, int end) const {
+    Range r{start, end, {kBig, kBig, kBig}, {-kBig, -kBig, -kBig}, {kBig, kBig, kBig}, {-kBig, -kBig, -kBig}};
+    for (int k = start; k < end; ++k) {
+      int i = order[k];
+      F3 l = lo(i), h = hi(i), c = {(l.x + h.x) * 0.5f, (l.y + h.y) * 0.5f, (l.z + h.z) * 0.5f};
+      r.lo = fmin3(r.lo, l); r.hi = fmax3(r.hi, h); r.clo = fmin3(r.clo, c); r.chi = fmax3(r.chi, c);
+    }
+    return r;
+  }
+  static float bin_scale(float e) {
+    float s = float(kBins) / e;
+    return e > 0 && std::isfinite(s) ? s : 0.0f;
+  }
+  static int to_bin(float f) {
+    // Swift Int(Float) truncates toward zero; clamp to [0, bins - 1].
+    long v = (long)f;
+    return (int)std::min<long>(kBins - 1, std::max<long>(0, v));
+  }
+  void split(const Range &r, Range &left, Range &right) {
+    F3 ext = {r.chi.x - r.clo.x, r.chi.y - r.clo.y, r.chi.z - r.clo.z};
+    float emax = std::fmax(ext.x, std::fmax(ext.y, ext.z));
+    F3 big = {kBig, kBig, kBig}, nbig = {-kBig, -kBig, -kBig};
+    if (!median && emax > 0) {
+      float scale[3] = {bin_scale(ext.x), bin_scale(ext.y), bin_scale(ext.z)};
+      for (int k = 0; k < 3 * kBins; ++k) { binLo[k] = big; binHi[k] = nbig; binCLo[k] = big; binCHi[k] = nbig; binCount[k] = 0; }
+      for (int k = r.start; k < r.end; ++k) {
+        int i = order[k];
+        F3 l = lo(i), h = hi(i), c = {(l.x + h.x) * 0.5f, (l.y + h.y) * 0.5f, (l.z + h.z) * 0.5f};
+        float f[3] = {(c.x - r.clo.x) * scale[0], (c.y - r.clo.y) * scale[1], (c.z - r.clo.z) * scale[2]};
+        for (int a = 0; a < 3; ++a) {
+          int s = a * kBins + to_bin(f[a]);
+          binCount[s] += 1;
+          binLo[s] = fmin3(binLo[s], l); binHi[s] = fmax3(binHi[s], h);
+          binCLo[s] = fmin3(binCLo[s], c); binCHi[s] = fmax3(binCHi[s], c);
+        }
+      }
+      float bestCost = kBig;
+      int best = -1, bin = 0;
+      for (int a = 0; a < 3; ++a) {
+        if (!(scale[a] > 0)) continue;
+        F3 l = big, h = nbig;
+        int count = 0;
+        for (int b = kBins - 1; b > 0; --b) {
+          int k = a * kBins + b;
+          if (binCount[k] > 0) { l = fmin3(l, binLo[k]); h = fmax3(h, binHi[k]); }
+          count += binCount[k];
+          suffix[b] = count > 0 ? box_area(l, h) * float(count) : 0.0f;
+        }
+        l = big; h = nbig; count = 0;
+        for (int b = 0; b < kBins - 1; ++b) {
+          int k = a * kBins + b;
+          if (binCount[k] > 0) { l = fmin3(l, binLo[k]); h = fmax3(h, binHi[k]); }
+          count += binCount[k];
+          if (count == 0 || count == r.count()) continue;
+          float cost = box_area(l, h) * float(count) + suffix[b + 1];
+          if (cost < bestCost) { bestCost = cost; best = a; bin = b; }
+        }
+      }
+      if (best >= 0) {
+        float s = scale[best], origin = comp(r.clo, best);
+        int i = r.start, j = r.end - 1;
+        while (i <= j) {
+          int tt = order[i];
+          float c = (bounds[6 * tt + best] + bounds[6 * tt + 3 + best]) * 0.5f;
+          if (to_bin((c - origin) * s) <= bin) ++i;
+          else { std::swap(order[i], order[j]); --j; }
+        }
+        if (i > r.start && i < r.end) {
+          left = Range{r.start, i, big, nbig, big, nbig};
+          right = Range{i, r.end, big, nbig, big, nbig};
+          for (int b = 0; b < kBins; ++b) {
+            int k = best * kBins + b;
+            if (binCount[k] <= 0) continue;
+            Range &x = b <= bin ? left : right;
+            x.lo = fmin3(x.lo, binLo[k]); x.hi = fmax3(x.hi, binHi[k]);
+            x.clo = fmin3(x.clo, binCLo[k]); x.chi = fmax3(x.chi, binCHi[k]);
+          }
+          return;
+        }
+      }
+    }
+    int middle = (r.start + r.end) / 2;
+    if (emax > 0) {
+      int a = ext.x > ext.y ? (ext.x > ext.z ? 0 : 2) : (ext.y > ext.z ? 1 : 2);
+      const float *b = bounds;
+      std::sort(order + r.start, order + r.end, [b, a](int32_t x, int32_t y) {
+        float cx = b[6 * x + a] + b[6 * x + 3 + a], cy = b[6 * y + a] + b[6 * y + 3 + a];
+        return cx == cy ? x < y : cx < cy;
+      });
+    }
+    left = measure(r.start, middle);
+    right = measure(middle, r.end);
+  }
+  struct Work { Range r; int parent, slot, level; };
+  int run(const Range &root, int depth, std::vector<vt_wide_node> &nodes, int deferThreshold,
+          std::vector<Work> &deferred) {
+    int reached = depth;
+    std::vector<Work> work{{root, -1, 0, depth}};
+    while (!work.empty()) {
+      Work wk = work.back(); work.pop_back();
+      reached = std::max(reached, wk.level);
+      std::vector<Range> children{wk.r};
+      while (children.size() < 4) {
+        int best = -1;
+        for (size_t k = 0; k < children.size(); ++k) {
+          const Range &c = children[k];
+          if (c.count() <= leafSize) continue;
+          if (best < 0 || (median ? c.count() > children[best].count() : c.area() > children[best].area())) best = (int)k;
+        }
+        if (best < 0) break;
+        Range a, b;
+        split(children[best], a, b);
+        children[best] = a;
+        children.insert(children.begin() + best + 1, b);
+      }
+      vt_wide_node nd;
+      std::memset(&nd, 0, sizeof nd);
+      int index = (int)nodes.size();
+      if (wk.parent >= 0) nodes[wk.parent].child[wk.slot] = index;
+      for (size_t k = 0; k < children.size(); ++k) {
+        const Range &c = children[k];
+        nd.lox[k] = c.lo.x; nd.loy[k] = c.lo.y; nd.loz[k] = c.lo.z;
+        nd.hix[k] = c.hi.x; nd.hiy[k] = c.hi.y; nd.hiz[k] = c.hi.z;
+        if (c.count() <= leafSize) { nd.child[k] = -(c.start + 1); nd.count[k] = c.count(); }
+      }
+      nodes.push_back(nd);
+      for (int k = (int)children.size() - 1; k >= 0; --k) {
+        if (children[k].count() <= leafSize) continue;
+        if (children[k].count() < deferThreshold) deferred.push_back({children[k], index, k, wk.level + 1});
+        else work.push_back({children[k], index, k, wk.level + 1});
+      }
+    }
+    return reached;
+  }
+};
+
+int wide_build(const float *bounds, int n, int leafSize, bool median, int threads,
+               std::vector<int32_t> &order, std::vector<vt_wide_node> &nodes) {
+  order.resize(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  nodes.clear();
+  if (n <= 0) return 0;
+  WideBuilder *b = new WideBuilder{bounds, order.data(), leafSize, median};
+  std::vector<WideBuilder::Work> deferred;
+  int threshold = n >= 65536 ? n / 16 : 0;
+  int depth = b->run(b->measure(0, n), 1, nodes, threshold, deferred);
+  delete b;
+  if (!deferred.empty()) {
+    size_t T = deferred.size();
+    std::vector<std::vector<vt_wide_node>> parts(T);
+    std::vector<int> depths(T, 0);
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+      WideBuilder *local = new WideBuilder{bounds, order.data(), leafSize, median};
+      for (size_t t; (t = next.fetch_add(1)) < T;) {
+        std::vector<WideBuilder::Work> none;
+        depths[t] = local->run(deferred[t].r, deferred[t].level, parts[t], 0, none);
+      }
+      delete local;
+    };
+    int nt = std::max(1, std::min<int>(threads, (int)T));
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nt; ++i) pool.emplace_back(worker);
+    for (auto &th : pool) th.join();
+    for (size_t t = 0; t < T; ++t) {
+      int32_t offset = (int32_t)nodes.size();
+      nodes[deferred[t].parent].child[deferred[t].slot] = offset;
+      for (vt_wide_node nd : parts[t]) {
+        for (int k = 0; k < 4; ++k) if (nd.child[k] > 0) nd.child[k] += offset;
+        nodes.push_back(nd);
+      }
+      depth = std::max(depth, depths[t]);
+    }
+  }
+  return depth;
+}
+
+}  // namespace
+
+extern "C" {
+
+vto_bvh *vto_widebvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                           uint32_t nverts, int32_t leaf_size, int32_t max_depth, int32_t threads) {
+  (void)nverts;
+  vto_bvh *h = new vto_bvh();
+  h->faces = nfaces;
+  int n = (int)nfaces;
+  if (leaf_size < 1) leaf_size = 2;
+  if (max_depth <= 0) max_depth = 20;
+  if (threads <= 0) threads = 1;
+  std::vector<float> bounds(6 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    Box b = face_box(faces[i], verts);
+    bounds[6 * i] = b.lo.x; bounds[6 * i + 1] = b.lo.y; bounds[6 * i + 2] = b.lo.z;
+    bounds[6 * i + 3] = b.hi.x; bounds[6 * i + 4] = b.hi.y; bounds[6 * i + 5] = b.hi.z;
+  }
+  int depth = wide_build(bounds.data(), n, leaf_size, false, threads, h->order, h->nodes);
+  if (depth > max_depth) depth = wide_build(bounds.data(), n, leaf_size, true, threads, h->order, h->nodes);
+  h->depth = (uint32_t)depth;
+  finish_bvh(h, faces, verts);
+  return h;
+}
+
+void vto_bvh_free(vto_bvh *h) { delete h; }
+
+void vto_bvh_get_info(const vto_bvh *h, vto_bvh_info *out) {
+  out->faces = h->faces;
+  out->wide_nodes = (uint32_t)h->nodes.size();
+  out->binary_nodes = (uint32_t)h->binary.size();
+  out->depth = h->depth;
+  out->sah_cost = (float)h->sah;
+  out->lo[0] = h->bounds.lo.x; out->lo[1] = h->bounds.lo.y; out->lo[2] = h->bounds.lo.z;
+  out->hi[0] = h->bounds.hi.x; out->hi[1] = h->bounds.hi.y; out->hi[2] = h->bounds.hi.z;
+}
+void vto_bvh_get_nodes(const vto_bvh *h, vt_wide_node *out) {
+  if (!h->nodes.empty()) std::memcpy(out, h->nodes.data(), h->nodes.size() * sizeof(vt_wide_node));
+}
+void vto_bvh_get_order(const vto_bvh *h, int32_t *out) {
+  if (!h->order.empty()) std::memcpy(out, h->order.data(), h->order.size() * sizeof(int32_t));
+}
+void vto_bvh_get_morton(const vto_bvh *h, uint32_t *codes, int32_t *sorted) {
+  if (!h->codes.empty()) std::memcpy(codes, h->codes.data(), h->codes.size() * sizeof(uint32_t));
+  if (!h->sorted.empty()) std::memcpy(sorted, h->sorted.data(), h->sorted.size() * sizeof(int32_t));
+}
+void vto_bvh_get_binary(const vto_bvh *h, int32_t *children, float *boxes) {
+  for (size_t i = 0; i < h->binary.size(); ++i) {
+    const BinNode &b = h->binary[i];
+    children[2 * i] = b.child[0];
+    children[2 * i + 1] = b.child[1];
+    float v[6] = {b.box.lo.x, b.box.lo.y, b.box.lo.z, b.box.hi.x, b.box.hi.y, b.box.hi.z};
+    std::memcpy(boxes + 6 * i, v, sizeof v);
+  }
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Traversal (main.swift:1758-1838): conservative slab test with origins shifted by
+// e = 2^-23 (|o|max + rootMax) (wide_ray, main.swift:1758-1763), near-to-far insertion order
+// (wide_order, :1780-1785), closest hit popping the nearest inner child first (blas_closest),
+// any hit in child-slot order (blas_any, without endpoint slack).
+namespace {
+
+template <typename T> struct TraceRay {
+  T o[3], d[3], tmin, tmax;
+};
+
+template <typename T> struct SlabRay {
+  T low[3], high[3], inv[3];
+  bool parallel[3];
+};
+
+template <typename T> SlabRay<T> make_slab(const TraceRay<T> &r, T rootMax) {
+  SlabRay<T> s;
+  T om = std::fmax(std::fmax(std::fabs(r.o[0]), std::fabs(r.o[1])), std::fabs(r.o[2]));
+  // fp64 needs no enlargement for its own rounding but keeps the fp32 one (it is conservative).
+  T e = T(1.1920929e-6) * (om + rootMax);
+  for (int k = 0; k < 3; ++k) {
+    s.low[k] = r.o[k] + e;
+    s.high[k] = r.o[k] - e;
+    s.parallel[k] = std::fabs(r.d[k]) < T(1e-8);
+    s.inv[k] = T(1) / (s.parallel[k] ? T(1) : r.d[k]);
+  }
+  return s;
+}
+
+template <typename T>
+int node_hits(const vt_wide_node &n, const SlabRay<T> &w, T tMin, T tMax, T nearT[4]) {
+  int mask = 0;
+  const float *lo[3] = {n.lox, n.loy, n.loz}, *hi[3] = {n.hix, n.hiy, n.hiz};
+  for (int k = 0; k < 4; ++k) {
+    if (n.child[k] == 0) continue;
+    T nt = tMin, ft = tMax;
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      if (w.parallel[a]) {
+        if (w.low[a] < T(lo[a][k]) || w.high[a] > T(hi[a][k])) ok = false;
+        continue;
+      }
+      T x = (T(lo[a][k]) - w.low[a]) * w.inv[a], y = (T(hi[a][k]) - w.high[a]) * w.inv[a];
+      // Plain comparisons (no NaN can arise: every operand is finite).
+      T mn = x < y ? x : y, mx = x < y ? y : x;
+      nt = nt < mn ? mn : nt;
+      ft = ft < mx ? ft : mx;
+    }
+    nearT[k] = nt;
+    if (ok && nt <= ft) mask |= 1 << k;
+  }
+  return mask;
+}
+
+template <typename T>
+bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &hb1, T &hb2,
+                 uint64_t *nodes = nullptr, uint64_t *tests = nullptr) {
+  if (h.nodes.empty()) return false;
+  WRay<T> w = make_wray(r.o, r.d);
+  SlabRay<T> s = make_slab(r, T(h.root_max));
+  T closest = r.tmax;
+  bool found = false;
+  int stack[128];
+  int top = 0;
+  stack[top++] = 0;
+  while (top > 0) {
+    const vt_wide_node &nd = h.nodes[stack[--top]];
+    if (nodes) ++*nodes;
+    T nearT[4];
+    int mask = node_hits(nd, s, r.tmin, closest, nearT);
+    int order[4];
+    T key[4];
+    int m = 0;
+    for (int k = 0; k < 4; ++k) {
+      if (!(mask >> k & 1)) continue;
+      int j = m++;
+      while (j > 0 && key[j - 1] > nearT[k]) { key[j] = key[j - 1]; order[j] = order[j - 1]; --j; }
+      key[j] = nearT[k];
+      order[j] = k;
+    }
+    for (int j = 0; j < m; ++j) {
+      int k = order[j];
+      if (nd.child[k] > 0 || key[j] > closest) continue;
+      int first = -nd.child[k] - 1;
+      for (int q = 0; q < nd.count[k]; ++q) {
+        const float *tf = &h.tris[9 * (size_t)(first + q)];
+        T a[3] = {T(tf[0]), T(tf[1]), T(tf[2])}, b[3] = {T(tf[3]), T(tf[4]), T(tf[5])},
+          c[3] = {T(tf[6]), T(tf[7]), T(tf[8])};
+        T t, b1, b2;
+        if (tests) ++*tests;
+        if (!intersect_tri<T>(w, a, b, c, r.tmin, closest, t, b1, b2)) continue;
+        closest = t; prim = h.order[first + q]; hb1 = b1; hb2 = b2; found = true;
+      }
+    }
+    for (int j = m - 1; j >= 0; --j) {
+      int k = order[j];
+      if (nd.child[k] > 0 && key[j] <= closest && top < 128) stack[top++] = nd.child[k];
+    }
+  }
+  best = closest;
+  return found;
+}
+
+template <typename T>
+bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, uint64_t *tests = nullptr) {
+  if (h.nodes.empty()) return false;
+  WRay<T> w = make_wray(r.o, r.d);
+  SlabRay<T> s = make_slab(r, T(h.root_max));
+  int stack[128];
+  int top = 0;
+  stack[top++] = 0;
+  while (top > 0) {
+    const vt_wide_node &nd = h.nodes[stack[--top]];
+    if (nodes) ++*nodes;
+    T nearT[4];
+    int mask = node_hits(nd, s, r.tmin, r.tmax, nearT);
+    for (int k = 0; k < 4; ++k) {
+      if (!(mask >> k & 1)) continue;
+      if (nd.child[k] > 0) { if (top < 128) stack[top++] = nd.child[k]; continue; }
+      int first = -nd.child[k] - 1;
+      for (int q = 0; q < nd.count[k]; ++q) {
+        const float *tf = &h.tris[9 * (size_t)(first + q)];
+        T a[3] = {T(tf[0]), T(tf[1]), T(tf[2])}, b[3] = {T(tf[3]), T(tf[4]), T(tf[5])},
+          c[3] = {T(tf[6]), T(tf[7]), T(tf[8])};
+        T t, b1, b2;
+        if (tests) ++*tests;
+        if (intersect_tri<T>(w, a, b, c, r.tmin, r.tmax, t, b1, b2)) return true;
+      }
+    }
+  }
+  return false;
+}
+
+template <typename T> TraceRay<T> load_ray(const vt_ray &r) {
+  TraceRay<T> x;
+  x.o[0] = r.ox; x.o[1] = r.oy; x.o[2] = r.oz;
+  x.d[0] = r.dx; x.d[1] = r.dy; x.d[2] = r.dz;
+  x.tmin = r.tmin; x.tmax = r.tmax;
+  return x;
+}
+
+template <typename F> void parallel_for(uint32_t n, int threads, F f) {
+  if (threads <= 1 || n < 2048) { for (uint32_t i = 0; i < n; ++i) f(i); return; }
+  std::atomic<uint32_t> next{0};
+  const uint32_t chunk = 512;
+  auto worker = [&]() {
+    for (uint32_t s; (s = next.fetch_add(chunk)) < n;) {
+      uint32_t e = std::min(n, s + chunk);
+      for (uint32_t i = s; i < e; ++i) f(i);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 0; i < threads; ++i) pool.emplace_back(worker);
+  for (auto &t : pool) t.join();
+}
+
+}  // namespace
+
+extern "C" {
+
+void vto_trace_closest(const vto_bvh *h, const vt_ray *rays, uint32_t n, vt_hit *hits,
+                       int32_t precision, int32_t threads) {
+  parallel_for(n, threads, [&](uint32_t i) {
+    vt_hit out{0.0f, 0.0f, 0.0f, -1};
+    int prim = -1;
+    if (precision == 64) {
+      TraceRay<double> r = load_ray<double>(rays[i]);
+      double t, b1 = 0, b2 = 0;
+      if (closest_hit<double>(*h, r, t, prim, b1, b2)) out = {float(t), float(b1), float(b2), prim};
+    } else {
+      TraceRay<float> r = load_ray<float>(rays[i]);
+      float t, b1 = 0, b2 = 0;
+      if (closest_hit<float>(*h, r, t, prim, b1, b2)) out = {t, b1, b2, prim};
+    }
+    hits[i] = out;
+  });
+}
+
+void vto_trace_any(const vto_bvh *h, const vt_ray *rays, uint32_t n, uint8_t *occluded,
+                   int32_t precision, int32_t threads) {
+  parallel_for(n, threads, [&](uint32_t i) {
+    bool hit = precision == 64 ? any_hit<double>(*h, load_ray<double>(rays[i]))
+                               : any_hit<float>(*h, load_ray<float>(rays[i]));
+    occluded[i] = hit ? 1 : 0;
+  });
+}
+
+void vto_brute_closest(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                       const vt_ray *rays, uint32_t n, vt_hit *hits, int32_t precision,
+                       int32_t threads) {
+  parallel_for(n, threads, [&](uint32_t i) {
+    vt_hit out{0.0f, 0.0f, 0.0f, -1};
+    if (precision == 64) {
+      TraceRay<double> r = load_ray<double>(rays[i]);
+      WRay<double> w = make_wray(r.o, r.d);
+      double best = r.tmax;
+      for (uint32_t f = 0; f < nfaces; ++f) {
+        const vt_vertex *p[3] = {&verts[faces[f].a], &verts[faces[f].b], &verts[faces[f].c]};
+        double a[3] = {p[0]->px, p[0]->py, p[0]->pz}, b[3] = {p[1]->px, p[1]->py, p[1]->pz},
+               c[3] = {p[2]->px, p[2]->py, p[2]->pz};
+        double t, b1, b2;
+        if (intersect_tri<double>(w, a, b, c, r.tmin, best, t, b1, b2)) { best = t; out = {float(t), float(b1), float(b2), int32_t(f)}; }
+      }
+    } else {
+      TraceRay<float> r = load_ray<float>(rays[i]);
+      WRay<float> w = make_wray(r.o, r.d);
+      float best = r.tmax;
+      for (uint32_t f = 0; f < nfaces; ++f) {
+        const vt_vertex *p[3] = {&verts[faces[f].a], &verts[faces[f].b], &verts[faces[f].c]};
+        float a[3] = {p[0]->px, p[0]->py, p[0]->pz}, b[3] = {p[1]->px, p[1]->py, p[1]->pz},
+              c[3] = {p[2]->px, p[2]->py, p[2]->pz};
+        float t, b1, b2;
+        if (intersect_tri<float>(w, a, b, c, r.tmin, best, t, b1, b2)) { best = t; out = {t, b1, b2, int32_t(f)}; }
+      }
+    }
+    hits[i] = out;
+  });
+}
+
+void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t closest,
+                     uint64_t *nodes_visited, uint64_t *tris_tested, int32_t threads) {
+  std::atomic<uint64_t> nv{0}, tt{0};
+  parallel_for(n, threads, [&](uint32_t i) {
+    uint64_t a = 0, b = 0;
+    TraceRay<float> r = load_ray<float>(rays[i]);
+    if (closest) { float t, b1 = 0, b2 = 0; int p = -1; closest_hit<float>(*h, r, t, p, b1, b2, &a, &b); }
+    else any_hit<float>(*h, r, &a, &b);
+    nv += a; tt += b;
+  });
+  *nodes_visited = nv;
+  *tris_tested = tt;
+}
+
+}  // extern "C"

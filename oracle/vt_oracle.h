@@ -1,0 +1,78 @@
+/*
+ * vt_oracle.h — CPU restatement of the reference's traversal and BVH-build arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path: the tests, the smoke
+ * check and bench.py's CPU-baseline leg load it; the product library never links or calls it.
+ *
+ * What it restates (reference file:line):
+ *   - PCG hash stream: main.swift:91-101 (pcg_hash, rand_f).
+ *   - Watertight ray/triangle test: main.swift:1536-1582 (watertight_ray, watertight_edge,
+ *     intersect_mesh_triangle), in two precisions:
+ *       fp32: the op order fixed for the CUDA kernels (every product and sum rounded on its own,
+ *             the exact-tie FMA fallback of watertight_edge), so GPU hits compare bit for bit;
+ *       fp64: the same algorithm in double precision, the accuracy judge (hit IDs, t error).
+ *   - Conservative 4-wide slab test and near-to-far order: main.swift:1758-1785.
+ *   - Closest-hit / any-hit 4-wide traversal: main.swift:1788-1838.
+ *   - Binned-SAH 4-wide build (WideBVH): Sources/Acceleration.swift:106-352, with its deferred
+ *     subtree numbering (:302-350) and the median rebuild past the depth limit (:296-300).
+ *   - The LBVH that replaces it on the GPU (no reference counterpart; restated from the CUDA
+ *     build's own definition so Morton codes, order and topology compare bit for bit).
+ */
+#ifndef VT_ORACLE_H
+#define VT_ORACLE_H
+#include <stdint.h>
+#include "../include/vt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct vto_bvh vto_bvh;
+
+typedef struct vto_bvh_info {
+  uint32_t faces, wide_nodes, binary_nodes, depth;
+  float sah_cost;
+  float lo[3], hi[3];
+} vto_bvh_info;
+
+uint32_t vto_pcg_hash(uint32_t v);
+float vto_rand_f(uint32_t *seed);
+
+/* One watertight test (fp32 op order of the CUDA kernels). tri = 9 floats (a, b, c). Returns
+ * 1 on a hit in [tmin, tmax) and writes t, b1, b2. */
+int32_t vto_intersect_f32(const vt_ray *ray, const float *tri, float *t, float *b1, float *b2);
+int32_t vto_intersect_f64(const double *ray /* o xyz, d xyz */, const double *tri, double tmin,
+                          double tmax, double *t, double *b1, double *b2);
+
+/* LBVH restatement. treelet_size < 0 disables the SAH restructuring. */
+vto_bvh *vto_lbvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                        uint32_t nverts, int32_t leaf_size, int32_t treelet_size,
+                        int32_t rounds);
+/* Reference binned-SAH 4-wide build (WideBVH.build with leafSize and depth limit). */
+vto_bvh *vto_widebvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                           uint32_t nverts, int32_t leaf_size, int32_t max_depth, int32_t threads);
+void vto_bvh_free(vto_bvh *h);
+void vto_bvh_get_info(const vto_bvh *h, vto_bvh_info *out);
+void vto_bvh_get_nodes(const vto_bvh *h, vt_wide_node *out);
+void vto_bvh_get_order(const vto_bvh *h, int32_t *out);
+/* LBVH only: sorted codes/faces and the refined binary tree (children 2n, boxes 6n). */
+void vto_bvh_get_morton(const vto_bvh *h, uint32_t *codes, int32_t *sorted);
+void vto_bvh_get_binary(const vto_bvh *h, int32_t *children, float *boxes);
+
+/* Traversal over an oracle BVH. precision = 32 (bit-exact CUDA op order) or 64. */
+void vto_trace_closest(const vto_bvh *h, const vt_ray *rays, uint32_t n, vt_hit *hits,
+                       int32_t precision, int32_t threads);
+void vto_trace_any(const vto_bvh *h, const vt_ray *rays, uint32_t n, uint8_t *occluded,
+                   int32_t precision, int32_t threads);
+/* Brute force over all faces (input order ids). */
+void vto_brute_closest(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                       const vt_ray *rays, uint32_t n, vt_hit *hits, int32_t precision,
+                       int32_t threads);
+/* Traversal statistics of closest (1) or any-hit (0) traversal, fp32 order. */
+void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t closest,
+                     uint64_t *nodes_visited, uint64_t *tris_tested, int32_t threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

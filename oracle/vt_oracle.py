@@ -1,0 +1,206 @@
+"""ctypes binding of the oracle library (oracle/lib/libvt_oracle.so).
+
+Test infrastructure only: the checker for the CUDA path (see vt_oracle.h for the reference
+functions each routine restates, with file:line).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "lib" / "libvt_oracle.so"
+
+FACE_DTYPE = np.dtype([("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("tag", "<u4")])
+VERTEX_DTYPE = np.dtype([("p", "<f4", 3), ("n", "<f4", 3), ("uv", "<f4", 2)])
+WIDE_NODE_DTYPE = np.dtype([
+    ("lox", "<f4", 4), ("loy", "<f4", 4), ("loz", "<f4", 4),
+    ("hix", "<f4", 4), ("hiy", "<f4", 4), ("hiz", "<f4", 4),
+    ("child", "<i4", 4), ("count", "<i4", 4),
+])
+RAY_DTYPE = np.dtype([("o", "<f4", 3), ("tmin", "<f4"), ("d", "<f4", 3), ("tmax", "<f4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("b1", "<f4"), ("b2", "<f4"), ("prim", "<i4")])
+
+
+class BvhInfo(C.Structure):
+    _fields_ = [("faces", C.c_uint32), ("wide_nodes", C.c_uint32), ("binary_nodes", C.c_uint32),
+                ("depth", C.c_uint32), ("sah_cost", C.c_float), ("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+
+_P, _U32, _I32 = C.c_void_p, C.c_uint32, C.c_int32
+_SIGS = {
+    "vto_pcg_hash": (_U32, [_U32]),
+    "vto_rand_f": (C.c_float, [C.POINTER(_U32)]),
+    "vto_intersect_f32": (_I32, [_P, _P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "vto_intersect_f64": (_I32, [_P, _P, C.c_double, C.c_double, C.POINTER(C.c_double),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "vto_lbvh_build": (_P, [_P, _U32, _P, _U32, _I32, _I32, _I32]),
+    "vto_widebvh_build": (_P, [_P, _U32, _P, _U32, _I32, _I32, _I32]),
+    "vto_bvh_free": (None, [_P]),
+    "vto_bvh_get_info": (None, [_P, C.POINTER(BvhInfo)]),
+    "vto_bvh_get_nodes": (None, [_P, _P]),
+    "vto_bvh_get_order": (None, [_P, _P]),
+    "vto_bvh_get_morton": (None, [_P, _P, _P]),
+    "vto_bvh_get_binary": (None, [_P, _P, _P]),
+    "vto_trace_closest": (None, [_P, _P, _U32, _P, _I32, _I32]),
+    "vto_trace_any": (None, [_P, _P, _U32, _P, _I32, _I32]),
+    "vto_brute_closest": (None, [_P, _U32, _P, _P, _U32, _P, _I32, _I32]),
+    "vto_trace_count": (None, [_P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _I32]),
+}
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle with its Makefile (g++, -ffp-contract=off)."""
+    res = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        lib = C.CDLL(str(LIB))
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1)
+
+
+def _faces(f):
+    f = np.ascontiguousarray(f)
+    assert f.dtype == FACE_DTYPE
+    return f
+
+
+def _verts(v):
+    v = np.ascontiguousarray(v)
+    assert v.dtype == VERTEX_DTYPE
+    return v
+
+
+def _rays(r):
+    r = np.ascontiguousarray(r)
+    if r.dtype != RAY_DTYPE:
+        r = np.ascontiguousarray(r, dtype=np.float32).view(RAY_DTYPE).reshape(-1)
+    return r
+
+
+def pcg_hash(v: int) -> int:
+    return int(load().vto_pcg_hash(v & 0xFFFFFFFF))
+
+
+def rand_f(seed: int) -> tuple[float, int]:
+    s = C.c_uint32(seed & 0xFFFFFFFF)
+    x = load().vto_rand_f(C.byref(s))
+    return float(x), int(s.value)
+
+
+def intersect_f32(ray, tri) -> tuple[bool, float, float, float]:
+    r = _rays(np.asarray(ray, np.float32).reshape(1, 8))
+    t9 = np.ascontiguousarray(tri, np.float32).reshape(9)
+    t, b1, b2 = C.c_float(), C.c_float(), C.c_float()
+    hit = load().vto_intersect_f32(r.ctypes.data, t9.ctypes.data, C.byref(t), C.byref(b1), C.byref(b2))
+    return bool(hit), t.value, b1.value, b2.value
+
+
+def intersect_f64(o, d, tri, tmin=0.0, tmax=np.inf) -> tuple[bool, float, float, float]:
+    r = np.ascontiguousarray(np.concatenate([o, d]), np.float64)
+    t9 = np.ascontiguousarray(tri, np.float64).reshape(9)
+    t, b1, b2 = C.c_double(), C.c_double(), C.c_double()
+    hit = load().vto_intersect_f64(r.ctypes.data, t9.ctypes.data, tmin, tmax, C.byref(t), C.byref(b1), C.byref(b2))
+    return bool(hit), t.value, b1.value, b2.value
+
+
+class Bvh:
+    """An oracle BVH (LBVH restatement or the reference's binned-SAH WideBVH)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def lbvh(cls, faces, verts, leaf_size=2, treelet_size=7, rounds=2):
+        f, v = _faces(faces), _verts(verts)
+        return cls(load().vto_lbvh_build(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0],
+                                         leaf_size, treelet_size, rounds))
+
+    @classmethod
+    def widebvh(cls, faces, verts, leaf_size=2, max_depth=20, nthreads=None):
+        f, v = _faces(faces), _verts(verts)
+        return cls(load().vto_widebvh_build(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0],
+                                            leaf_size, max_depth, nthreads or threads()))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            load().vto_bvh_free(self._h)
+            self._h = None
+
+    def info(self) -> BvhInfo:
+        out = BvhInfo()
+        load().vto_bvh_get_info(self._h, C.byref(out))
+        return out
+
+    def nodes(self) -> np.ndarray:
+        out = np.empty(self.info().wide_nodes, WIDE_NODE_DTYPE)
+        load().vto_bvh_get_nodes(self._h, out.ctypes.data)
+        return out
+
+    def order(self) -> np.ndarray:
+        out = np.empty(self.info().faces, np.int32)
+        load().vto_bvh_get_order(self._h, out.ctypes.data)
+        return out
+
+    def morton(self):
+        n = self.info().faces
+        codes, sorted_ = np.empty(n, np.uint32), np.empty(n, np.int32)
+        load().vto_bvh_get_morton(self._h, codes.ctypes.data, sorted_.ctypes.data)
+        return codes, sorted_
+
+    def binary(self):
+        n = self.info().binary_nodes
+        ch, boxes = np.empty((n, 2), np.int32), np.empty((n, 6), np.float32)
+        load().vto_bvh_get_binary(self._h, ch.ctypes.data, boxes.ctypes.data)
+        return ch, boxes
+
+    def closest(self, rays, precision=32, nthreads=None):
+        r = _rays(rays)
+        out = np.empty(r.shape[0], HIT_DTYPE)
+        load().vto_trace_closest(self._h, r.ctypes.data, r.shape[0], out.ctypes.data, precision,
+                                 nthreads or threads())
+        return out
+
+    def occluded(self, rays, precision=32, nthreads=None):
+        r = _rays(rays)
+        out = np.empty(r.shape[0], np.uint8)
+        load().vto_trace_any(self._h, r.ctypes.data, r.shape[0], out.ctypes.data, precision,
+                             nthreads or threads())
+        return out
+
+    def count(self, rays, closest=True, nthreads=None):
+        r = _rays(rays)
+        a, b = C.c_uint64(), C.c_uint64()
+        load().vto_trace_count(self._h, r.ctypes.data, r.shape[0], 1 if closest else 0, C.byref(a), C.byref(b),
+                               nthreads or threads())
+        return int(a.value), int(b.value)
+
+
+def brute_closest(faces, verts, rays, precision=32, nthreads=None):
+    f, v, r = _faces(faces), _verts(verts), _rays(rays)
+    out = np.empty(r.shape[0], HIT_DTYPE)
+    load().vto_brute_closest(f.ctypes.data, f.shape[0], v.ctypes.data, r.ctypes.data, r.shape[0],
+                             out.ctypes.data, precision, nthreads or threads())
+    return out
