@@ -337,7 +337,7 @@ def main():
                "steps": e2e_steps, "timing": "host wall clock around synchronous C-ABI calls"}
         # Parity spot check of the host path against the device path.
         torch.cuda.synchronize()
-        assert torch.equal(o_i[:4096], hits_i[:4096].cpu()), "host path differs from device path"
+        assert torch.equal(o_i[:4096].view(torch.int32), hits_i[:4096].cpu().view(torch.int32)), "host path differs from device path"
 
     # CPU baseline (rank 0, N = 1 only): the oracle port on the same BVH, bounded sample.
     cpu = None

@@ -5,7 +5,8 @@
  * and dispatches Metal kernels. Each entry point below replaces one reference interface; the
  * comment above it names the reference file:line it stands in for. Signatures carry plain
  * pointers, sizes and POD structs only: no CUDA, torch or C++ types. A stream argument is a
- * cudaStream_t passed as `void *` (NULL = the context's own stream).
+ * cudaStream_t passed as `void *` (NULL = the CUDA default stream, as in the CUDA runtime).
+ * Builds run on the context's own stream and return only when the structure is complete.
  *
  * Errors: every call returns a vt_status. A non-zero status leaves a human-readable message in
  * vt_last_error(ctx) (the role of MaterialLibrary.error(String), Sources/Acceleration.swift:733,

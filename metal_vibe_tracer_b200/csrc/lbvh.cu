@@ -332,7 +332,9 @@ __global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, 
   const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
   if (leaf >= t.n) return;
   int node = __ldcg(t.parent + (t.n - 1 + leaf));
-  while (node >= 0) {
+  // A walk longer than the node count means a corrupted parent chain: stop and report.
+  for (int guard = 0; node >= 0; ++guard) {
+    if (guard >= t.n) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
     __threadfence();
     if (atomicAdd(&flags[node], 1u) == 0u) return;
     __threadfence();
@@ -387,7 +389,8 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
                                 const uint32_t *offInner, const uint32_t *offPrims, uint32_t base,
                                 uint32_t nextBase, uint32_t primBase, vt_wide_node *nodes,
                                 int32_t *nextLevel, const uint32_t *sorted, const vt_face *faces,
-                                const vt_vertex *verts, int32_t *order, float4 *tris) {
+                                const vt_vertex *verts, int32_t *order, float4 *tris,
+                                uint32_t *status) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= L) return;
   int4 c4 = chIn[w];
@@ -416,6 +419,7 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
       while (top) {
         int c = st[--top];
         if (c < 0) {
+          if (prim >= (uint32_t)t.n) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
           uint32_t f = sorted[-c - 1];
           order[prim] = (int32_t)f;
           vt_face fc = faces[f];
@@ -426,6 +430,7 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
           ++prim;
           continue;
         }
+        if (top + 2 > 2 * 8 + 2) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
         int2 cc = load_child(t, c);
         st[top++] = cc.y;
         st[top++] = cc.x;
@@ -584,9 +589,13 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
     const uint32_t nextBase = base + L;
     k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, chBuf, nInner, nPrims, base,
                                                    nextBase, primBase, nodes, levelB, vals, faces,
-                                                   verts, mesh->d_order, mesh->d_tris);
+                                                   verts, mesh->d_order, mesh->d_tris, ctx->d_status);
+    uint32_t st_level = 0;
     VT_CUDA(ctx, cudaMemcpyAsync(host_tot, totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VT_CUDA(ctx, cudaMemcpyAsync(&st_level, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     VT_CUDA(ctx, cudaStreamSynchronize(s));
+    if (st_level & VT_DEV_TREELET) return vt_fail(ctx, VT_ERR_DEVICE, "hierarchy inconsistency during the collapse");
+    if (st_level & (VT_DEV_BAD_INDEX | VT_DEV_NONFINITE)) break;
     primBase += host_tot[1];
     base = nextBase;
     L = host_tot[0];
@@ -595,6 +604,12 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
   }
   mesh->nnodes = base;
   mesh->depth = depth;
+  {
+    uint32_t st0 = 0;
+    VT_CUDA(ctx, cudaMemcpy(&st0, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (st0 & VT_DEV_BAD_INDEX) return vt_fail(ctx, VT_ERR_INVALID, "a face indexes past the vertex array");
+    if (st0 & VT_DEV_NONFINITE) return vt_fail(ctx, VT_ERR_INVALID, "a vertex position is not finite");
+  }
   if (primBase != n) return vt_fail(ctx, VT_ERR_DEVICE, "collapse emitted " + std::to_string(primBase) + " of " + std::to_string(n) + " triangles");
 
   // Keep the refined binary tree for parity checks.

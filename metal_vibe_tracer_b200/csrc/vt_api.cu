@@ -252,7 +252,7 @@ vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_
                            vt_hit *hits_dev, void *stream) {
   vt_status st = check_trace_args(ctx, mesh, rays_dev, hits_dev, n);
   if (st) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL = the default stream
   if (mesh->nfaces == 0) {
     if (n) k_fill_miss<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<int4 *>(hits_dev), n);
   } else {
@@ -266,7 +266,7 @@ vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev,
                        uint8_t *occluded_dev, void *stream) {
   vt_status st = check_trace_args(ctx, mesh, rays_dev, occluded_dev, n);
   if (st) return st;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL = the default stream
   if (mesh->nfaces == 0) {
     if (n) VT_CUDA(ctx, cudaMemsetAsync(occluded_dev, 0, n, s));
   } else {

@@ -145,9 +145,12 @@ class Bvh:
                                             leaf_size, max_depth, nthreads or threads()))
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            load().vto_bvh_free(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None):
+                load().vto_bvh_free(self._h)
+                self._h = None
+        except Exception:
+            pass
 
     def info(self) -> BvhInfo:
         out = BvhInfo()
