@@ -60,7 +60,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
             print(res.stdout + res.stderr, file=sys.stderr)
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", str(tmp), *map(str, objs)]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
