@@ -146,6 +146,30 @@ vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays
 vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
                          int32_t closest, uint64_t *nodes_visited, uint64_t *tris_tested);
 
+/* ---- allocation-free build --------------------------------------------------------------- */
+
+/* No counterpart in the reference. The same GPU build as vt_mesh_build_device, for callers that
+ * cannot call cudaMalloc: hosts running under a fixed device-memory budget owned elsewhere (their
+ * own arena, or a framework's caching allocator holding the GPU memory), and loops that must not
+ * pay cudaMalloc/cudaFree's implicit device synchronisation. It needs no vt_ctx and allocates
+ * nothing: the caller passes DEVICE faces and vertices and DEVICE outputs, and every temporary
+ * comes from a 6 MiB static device array that each GPU loading the library holds until exit.
+ *   nodes: nodes_capacity >= nfaces 4-wide nodes (16-byte aligned); info->wide_nodes are written.
+ *   tris:  12 floats per face (three float4 per BVH position: a with the input face index's bits
+ *          in .w, b, c; 16-byte aligned).  order: nfaces int32 (BVH position -> input face).
+ *   info:  host output (build_ms is host wall time).  stream: NULL = the CUDA default stream;
+ *          the call returns when the build on that stream is complete.
+ *   error: optional host buffer of error_capacity bytes for the failure message.
+ * Meshes over VT_NOALLOC_MAX_FACES faces are rejected with VT_ERR_LIMIT. The first call on each
+ * device looks up the static array's address (with that device current), so make that first call
+ * before any stream capture. Every call shares the one array: calls that overlap on the GPU (on
+ * other streams or from other host threads) race on it. */
+#define VT_NOALLOC_MAX_FACES 32768u
+vt_status vt_mesh_build_noalloc(const vt_face *faces_dev, uint32_t nfaces, const vt_vertex *verts_dev,
+                                uint32_t nverts, const vt_build_options *opts, vt_wide_node *nodes_dev,
+                                uint32_t nodes_capacity, float *tris_dev, int32_t *order_dev,
+                                vt_mesh_info *info, void *stream, char *error, uint32_t error_capacity);
+
 #ifdef __cplusplus
 }
 #endif

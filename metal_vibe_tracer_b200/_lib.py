@@ -65,7 +65,10 @@ SIGNATURES = {
     "vt_trace_closest_host": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_trace_any_host": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_trace_count": (_I32, [_P, _P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "vt_mesh_build_noalloc": (_I32, [_P, _U32, _P, _U32, C.POINTER(BuildOptions), _P, _U32, _P, _P,
+                                     C.POINTER(MeshInfo), _P, C.c_char_p, _U32]),
 }
+NOALLOC_MAX_FACES = 32768
 
 _lib: C.CDLL | None = None
 

@@ -646,3 +646,222 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
   mesh->root_max = m;
   return VT_OK;
 }
+
+// =============================================================================================
+// Allocation-free build (vt_mesh_build_noalloc). No counterpart in the reference.
+//
+// For callers that cannot call cudaMalloc: hosts that run under a fixed device-memory budget
+// owned elsewhere (their own arena, or a framework's caching allocator holding the GPU memory),
+// and loops that must not pay cudaMalloc/cudaFree's implicit device synchronisation. The caller
+// passes the faces, vertices and the output buffers; every temporary of the build comes from
+// g_build_scratch, a file-scope device array of kNoAllocScratchBytes that every GPU loading this
+// library holds until the process exits. It fits VT_NOALLOC_MAX_FACES faces; larger meshes are
+// rejected. The first call on a device looks the array's address up (cudaGetSymbolAddress, with
+// that device current) and caches it, so that first call should come before any stream capture.
+// All calls share the one array and find the previous call's contents in it: every region the
+// build needs zeroed is cleared on the call's stream, and two calls overlapping on the GPU (other
+// streams or other host threads) race on it.
+#include <chrono>
+#include <cstring>
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(6) << 20;  // 6 MiB per GPU
+static __device__ __align__(256) unsigned char g_build_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_scratch_mutex;
+unsigned char *g_scratch_addr[kNoAllocMaxDevices] = {};
+
+// Bump allocator over the scratch array (256-byte aligned regions). With base == nullptr it only
+// measures.
+struct ScratchCarve {
+  unsigned char *base;
+  size_t off = 0;
+  template <typename T> T *take(size_t count) {
+    size_t bytes = (count * sizeof(T) + 16 + 255) & ~size_t(255);
+    T *p = base ? reinterpret_cast<T *>(base + off) : nullptr;
+    off += bytes;
+    return p;
+  }
+};
+
+struct NoAllocBuffers {
+  float4 *boxes, *leafBox, *nodeBox;
+  uint32_t *bounds, *codes, *vals, *codesAlt, *valsAlt, *sortTemp, *flags, *count, *status;
+  int2 *child;
+  int32_t *parent, *levelA, *levelB;
+  float *cost;
+  int4 *chBuf;
+  uint32_t *nInner, *nPrims, *scanTemp, *totals;
+  double *sah;
+};
+
+size_t carve_noalloc(unsigned char *base, uint32_t n, NoAllocBuffers &b) {
+  ScratchCarve c{base};
+  const uint32_t ni = n > 1 ? n - 1 : 1;
+  b.boxes = c.take<float4>(2 * (size_t)n);
+  b.leafBox = c.take<float4>(2 * (size_t)n);
+  b.nodeBox = c.take<float4>(2 * (size_t)ni);
+  b.bounds = c.take<uint32_t>(16);
+  b.codes = c.take<uint32_t>(n);
+  b.vals = c.take<uint32_t>(n);
+  b.codesAlt = c.take<uint32_t>(n);
+  b.valsAlt = c.take<uint32_t>(n);
+  b.sortTemp = c.take<uint32_t>(vt_radix_temp_words(n));
+  b.flags = c.take<uint32_t>(ni);
+  b.count = c.take<uint32_t>(ni);
+  b.child = c.take<int2>(ni);
+  b.parent = c.take<int32_t>(2 * (size_t)n);
+  b.cost = c.take<float>(ni);
+  b.levelA = c.take<int32_t>(n);
+  b.levelB = c.take<int32_t>(n);
+  b.chBuf = c.take<int4>(n);
+  b.nInner = c.take<uint32_t>(n);
+  b.nPrims = c.take<uint32_t>(n);
+  b.scanTemp = c.take<uint32_t>(vt_scan_temp_words(n));
+  b.totals = c.take<uint32_t>(4);
+  b.status = c.take<uint32_t>(4);
+  b.sah = c.take<double>(1);
+  return c.off;
+}
+
+vt_status noalloc_fail(char *error, uint32_t capacity, vt_status code, const std::string &msg) {
+  if (error && capacity) {
+    std::strncpy(error, msg.c_str(), capacity - 1);
+    error[capacity - 1] = '\0';
+  }
+  return code;
+}
+
+}  // namespace
+
+extern "C" vt_status vt_mesh_build_noalloc(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
+                                           uint32_t nverts, const vt_build_options *opts,
+                                           vt_wide_node *nodes, uint32_t nodes_capacity, float *tris,
+                                           int32_t *order, vt_mesh_info *info, void *stream,
+                                           char *error, uint32_t error_capacity) {
+  auto t_start = std::chrono::steady_clock::now();
+  if (error && error_capacity) error[0] = '\0';
+  auto fail = [&](vt_status code, const std::string &msg) { return noalloc_fail(error, error_capacity, code, msg); };
+  if (nfaces > VT_NOALLOC_MAX_FACES)
+    return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: " + std::to_string(nfaces) + " faces exceed the limit of " +
+                                  std::to_string(VT_NOALLOC_MAX_FACES) + " (the library's static build scratch)");
+  if (!info) return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: info is null");
+  std::memset(info, 0, sizeof *info);
+  if (nfaces == 0) return VT_OK;
+  if (!faces || !verts || !nodes || !tris || !order)
+    return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: null input or output pointer");
+  if (nodes_capacity < nfaces)
+    return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: nodes_capacity must be at least nfaces");
+  if ((reinterpret_cast<uintptr_t>(nodes) | reinterpret_cast<uintptr_t>(tris)) & 15u)
+    return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: nodes and tris must be 16-byte aligned");
+  vt_build_options o;
+  std::memset(&o, 0, sizeof o);
+  if (opts) o = *opts;
+  const int leafSize = o.leaf_size > 0 ? o.leaf_size : 2;
+  int treelet = o.treelet_size == 0 ? 7 : o.treelet_size;
+  const int rounds = o.refine_rounds > 0 ? o.refine_rounds : 2;
+  const int maxDepth = o.max_depth > 0 ? o.max_depth : 31;
+  if (leafSize > 8) return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: leaf_size must be in 1..8");
+  if (treelet > kMaxTreelet) treelet = kMaxTreelet;
+  if (treelet > 0 && treelet < 3) treelet = 3;
+
+  // Per-device set-up: the scratch array's device address, looked up once with the device current.
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(VT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: device index too large");
+  unsigned char *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+      void *p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_build_scratch);
+      if (e != cudaSuccess) return fail(VT_ERR_CUDA, std::string("cudaGetSymbolAddress(build scratch): ") + cudaGetErrorString(e));
+      NoAllocBuffers probe;
+      if (carve_noalloc(nullptr, VT_NOALLOC_MAX_FACES, probe) > kNoAllocScratchBytes)
+        return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: static scratch smaller than the face limit needs");
+      g_scratch_addr[dev] = static_cast<unsigned char *>(p);
+    }
+    scratch = g_scratch_addr[dev];
+  }
+  NoAllocBuffers b;
+  carve_noalloc(scratch, nfaces, b);
+
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const uint32_t n = nfaces, ni = n > 1 ? n - 1 : 1;
+#define VT_NA(call)                                                                  \
+  do {                                                                               \
+    cudaError_t _e = (call);                                                         \
+    if (_e != cudaSuccess) return fail(VT_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
+  } while (0)
+  VT_NA(cudaMemsetAsync(b.status, 0, 4 * sizeof(uint32_t), s));
+  k_init_bounds<<<1, 32, 0, s>>>(b.bounds);
+  k_face_boxes<<<blocks(n, 256), 256, 0, s>>>(faces, n, verts, nverts, b.boxes, b.bounds, b.status);
+  k_morton<<<blocks(n, 256), 256, 0, s>>>(b.boxes, n, b.bounds, b.codes, b.vals);
+  vt_radix_sort_pairs(b.codes, b.vals, b.codesAlt, b.valsAlt, n, 30, b.sortTemp, s);
+  k_leaf_boxes<<<blocks(n, 256), 256, 0, s>>>(b.boxes, b.vals, n, b.leafBox);
+  TreeView t{(int)n, b.child, b.parent, b.leafBox, b.nodeBox, b.count, b.cost};
+  if (n >= 2) {
+    k_karras<<<blocks(n - 1, 256), 256, 0, s>>>(b.codes, (int)n, b.child, b.parent);
+    VT_NA(cudaMemsetAsync(b.flags, 0, ni * sizeof(uint32_t), s));
+    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, 0, 0, b.status);
+    if (treelet > 0 && n >= 3) {
+      for (int r = 0; r < rounds; ++r) {
+        VT_NA(cudaMemsetAsync(b.flags, 0, ni * sizeof(uint32_t), s));
+        k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, 1, treelet, b.status);
+      }
+    }
+  }
+  VT_NA(cudaGetLastError());
+  // Root reference of the first level: binary node 0, or leaf 0 (-1, all bits set) for one face.
+  VT_NA(cudaMemsetAsync(b.levelA, n >= 2 ? 0 : 0xff, sizeof(int32_t), s));
+  uint32_t L = 1, base = 0, primBase = 0, depth = 0;
+  int32_t *levelA = b.levelA, *levelB = b.levelB;
+  while (L > 0) {
+    ++depth;
+    if ((int)depth > maxDepth) return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: BVH depth exceeds max_depth");
+    k_collapse_count<<<blocks(L, 128), 128, 0, s>>>(t, levelA, L, leafSize, b.chBuf, b.nInner, b.nPrims);
+    vt_scan_exclusive(b.nInner, b.nInner, L, b.scanTemp, b.totals, s);
+    vt_scan_exclusive(b.nPrims, b.nPrims, L, b.scanTemp, b.totals + 1, s);
+    const uint32_t nextBase = base + L;
+    k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, b.chBuf, b.nInner, b.nPrims, base, nextBase,
+                                                   primBase, nodes, levelB, b.vals, faces, verts, order,
+                                                   reinterpret_cast<float4 *>(tris), b.status);
+    uint32_t tot[2] = {0, 0}, st = 0;
+    VT_NA(cudaMemcpyAsync(tot, b.totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VT_NA(cudaMemcpyAsync(&st, b.status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    VT_NA(cudaStreamSynchronize(s));
+    if (st & VT_DEV_BAD_INDEX) return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: a face indexes past the vertex array");
+    if (st & VT_DEV_NONFINITE) return fail(VT_ERR_INVALID, "vt_mesh_build_noalloc: a vertex position is not finite");
+    if (st & VT_DEV_TREELET) return fail(VT_ERR_DEVICE, "vt_mesh_build_noalloc: hierarchy inconsistency");
+    primBase += tot[1];
+    base = nextBase;
+    L = tot[0];
+    if (base + L > nodes_capacity) return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: wide nodes exceed nodes_capacity");
+    int32_t *x = levelA; levelA = levelB; levelB = x;
+  }
+  if (primBase != n) return fail(VT_ERR_DEVICE, "vt_mesh_build_noalloc: collapse emitted too few triangles");
+  VT_NA(cudaMemsetAsync(b.sah, 0, sizeof(double), s));
+  k_sah<<<blocks(base, 256), 256, 0, s>>>(nodes, base, b.sah);
+  VT_NA(cudaGetLastError());
+  uint32_t hb[12];
+  double hsah = 0.0;
+  VT_NA(cudaMemcpyAsync(hb, b.bounds, 12 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  VT_NA(cudaMemcpyAsync(&hsah, b.sah, sizeof(double), cudaMemcpyDeviceToHost, s));
+  VT_NA(cudaStreamSynchronize(s));
+#undef VT_NA
+  info->faces = n;
+  info->wide_nodes = base;
+  info->binary_nodes = n - 1;
+  info->depth = depth;
+  info->sah_cost = (float)hsah;
+  for (int k = 0; k < 3; ++k) {
+    info->lo[k] = ord2f(hb[6 + k]);
+    info->hi[k] = ord2f(hb[9 + k]);
+  }
+  info->build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  return VT_OK;
+}
