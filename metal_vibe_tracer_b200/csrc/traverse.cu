@@ -13,6 +13,8 @@
 // The watertight arithmetic is written with explicitly rounded intrinsics in one fixed order
 // (each product and sum rounded on its own; the exact FMA fallback on edge ties), which the CPU
 // oracle reproduces, so hits compare bit for bit.
+#include <algorithm>
+
 #include "vt_internal.cuh"
 
 namespace {
@@ -232,31 +234,199 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
   return false;
 }
 
-__global__ void __launch_bounds__(128) k_closest(const float4 *__restrict__ nodes,
-                                                  const float4 *__restrict__ tris, float rootMax,
-                                                  const float4 *__restrict__ rays, uint32_t n,
-                                                  int4 *__restrict__ hits) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 r0 = __ldg(rays + 2 * (size_t)i), r1 = __ldg(rays + 2 * (size_t)i + 1);
-  float t = 0.0f, b1 = 0.0f, b2 = 0.0f;
-  int prim = -1;
-  uint32_t nv = 0, nt = 0;
-  int4 out = make_int4(0, 0, 0, -1);
-  if (trace_closest<false>(nodes, tris, rootMax, r0, r1, t, b1, b2, prim, nv, nt))
-    out = make_int4(__float_as_int(t), __float_as_int(b1), __float_as_int(b2), prim);
-  hits[i] = out;
+// ---- persistent traversal -----------------------------------------------------------------------
+// Rays vary a lot in length (65 node visits on average for the incoherent set, with a long tail), so
+// a thread-per-ray grid leaves most lanes of a warp idle while its longest ray finishes. Here each
+// warp stays resident and refills idle lanes from a global ray counter: one warp-aggregated
+// atomicAdd hands out as many rays as there are idle lanes, whenever at least kRefill lanes are
+// idle. Each loop iteration visits one node per active lane with the reference's per-ray algorithm
+// (leaves tested at the node visit in near-to-far order, inner children pushed far to near), so
+// the hits are those of the thread-per-ray form bit for bit. Rays are read and hits written with
+// streaming cache hints so that the ray stream does not evict the BVH from L2.
+#ifndef VT_TRACE_REFILL
+#define VT_TRACE_REFILL 8
+#endif
+#ifndef VT_TRACE_MIN_BLOCKS
+#define VT_TRACE_MIN_BLOCKS 6
+#endif
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kRefill = VT_TRACE_REFILL;      // refill once this many lanes are idle
+constexpr int kBlock = 128;
+constexpr int kMinBlocks = VT_TRACE_MIN_BLOCKS;  // register budget: 65536 / (kBlock * kMinBlocks)
+
+struct RayState {
+  WRay wr;
+  SlabRay sr;
+  float tMin, tMax;
+};
+
+__device__ __forceinline__ void load_ray(const float4 *__restrict__ rays, uint32_t r, RayState &s,
+                                         float rootMax) {
+  const float4 r0 = __ldcs(rays + 2 * (size_t)r), r1 = __ldcs(rays + 2 * (size_t)r + 1);
+  s.wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+  s.sr = make_slab(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
+  s.tMin = r0.w;
+  s.tMax = r1.w;
 }
 
-__global__ void __launch_bounds__(128) k_any(const float4 *__restrict__ nodes,
-                                              const float4 *__restrict__ tris, float rootMax,
-                                              const float4 *__restrict__ rays, uint32_t n,
-                                              uint8_t *__restrict__ occ) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float4 r0 = __ldg(rays + 2 * (size_t)i), r1 = __ldg(rays + 2 * (size_t)i + 1);
-  uint32_t nv = 0, nt = 0;
-  occ[i] = trace_any<false>(nodes, tris, rootMax, r0, r1, nv, nt) ? 1 : 0;
+// Hands rays [base, base + idle lanes) to the idle lanes of the warp. Returns the lane's ray
+// index, or n if it got none; *exhausted is set (warp-uniformly) once the pool is empty.
+__device__ __forceinline__ uint32_t refill(unsigned idle, uint32_t *counter, uint32_t n, bool &exhausted) {
+  const unsigned lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(counter, (uint32_t)__popc(idle));
+  base = __shfl_sync(kFull, base, 0);
+  if (base + (uint32_t)__popc(idle) >= n) exhausted = true;
+  const uint32_t r = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+  return (idle >> lane & 1u) && r < n ? r : n;
+}
+
+// Children of a node in near-to-far order, in registers. A 4-element sorting network on
+// (entry distance, slot) gives exactly the order of the reference's stable insertion sort
+// (wide_order, main.swift:1780-1785), since slots break distance ties; missed children sort last.
+struct Sorted4 {
+  float key[4];
+  int child[4], count[4];
+  int m;  // number of hit children (the first m entries)
+};
+__device__ __forceinline__ void cswap(float &ka, int &sa, int &ca, int &na, float &kb, int &sb, int &cb, int &nb) {
+  const bool sw = ka > kb || (ka == kb && sa > sb);
+  const float k = sw ? kb : ka; kb = sw ? ka : kb; ka = k;
+  const int sl = sw ? sb : sa; sb = sw ? sa : sb; sa = sl;
+  const int c = sw ? cb : ca; cb = sw ? ca : cb; ca = c;
+  const int n = sw ? nb : na; nb = sw ? na : nb; na = n;
+}
+__device__ __forceinline__ Sorted4 sort_children(const Node4 &nd, int mask, const float nearT[4]) {
+  Sorted4 o;
+  float k0 = (mask & 1) ? nearT[0] : __int_as_float(0x7f800000), k1 = (mask & 2) ? nearT[1] : __int_as_float(0x7f800000);
+  float k2 = (mask & 4) ? nearT[2] : __int_as_float(0x7f800000), k3 = (mask & 8) ? nearT[3] : __int_as_float(0x7f800000);
+  int s0 = (mask & 1) ? 0 : 4, s1 = (mask & 2) ? 1 : 5, s2 = (mask & 4) ? 2 : 6, s3 = (mask & 8) ? 3 : 7;
+  int c0 = nd.child.x, c1 = nd.child.y, c2 = nd.child.z, c3 = nd.child.w;
+  int n0 = nd.count.x, n1 = nd.count.y, n2 = nd.count.z, n3 = nd.count.w;
+  cswap(k0, s0, c0, n0, k1, s1, c1, n1);
+  cswap(k2, s2, c2, n2, k3, s3, c3, n3);
+  cswap(k0, s0, c0, n0, k2, s2, c2, n2);
+  cswap(k1, s1, c1, n1, k3, s3, c3, n3);
+  cswap(k1, s1, c1, n1, k2, s2, c2, n2);
+  o.key[0] = k0; o.key[1] = k1; o.key[2] = k2; o.key[3] = k3;
+  o.child[0] = c0; o.child[1] = c1; o.child[2] = c2; o.child[3] = c3;
+  o.count[0] = n0; o.count[1] = n1; o.count[2] = n2; o.count[3] = n3;
+  o.m = __popc(mask);
+  return o;
+}
+
+// The traversal stack lives in shared memory, one column per thread: entry d of thread t is
+// word d * kBlock + t, so every lane of a warp hits its own bank whatever its stack depth.
+__device__ __forceinline__ int *stack_slot(int *sstack, int d) { return sstack + d * kBlock + threadIdx.x; }
+
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__restrict__ nodes,
+                                                        const float4 *__restrict__ tris, float rootMax,
+                                                        const float4 *__restrict__ rays, uint32_t n,
+                                                        int4 *__restrict__ hits, uint32_t *counter,
+                                                        const uint32_t *__restrict__ perm, int stackSize,
+                                                        uint32_t *status) {
+  extern __shared__ int sstack[];
+  int top = 0;  // 0: the lane holds no ray
+  uint32_t rid = 0;
+  RayState s;
+  float closest = 0.0f, hb1 = 0.0f, hb2 = 0.0f;
+  int prim = -1;
+  bool exhausted = false;  // warp-uniform
+  while (true) {
+    const unsigned idle = __ballot_sync(kFull, top == 0);
+    if (!exhausted && __popc(idle) >= kRefill) {
+      const uint32_t r = refill(idle, counter, n, exhausted);
+      if (r < n) {
+        rid = perm ? __ldcs(perm + r) : r;
+        load_ray(rays, rid, s, rootMax);
+        closest = s.tMax;
+        prim = -1;
+        *stack_slot(sstack, 0) = 0;
+        top = 1;
+      }
+    }
+    if (exhausted && !__any_sync(kFull, top > 0)) break;
+    if (top == 0) continue;
+    Node4 nd;
+    load_node(nodes, *stack_slot(sstack, --top), nd);
+    float nearT[4];
+    const int mask = node_hits(nd, s.sr, s.tMin, closest, nearT);
+    const Sorted4 o = sort_children(nd, mask, nearT);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j >= o.m || o.child[j] > 0 || o.key[j] > closest) continue;
+      const int first = -o.child[j] - 1, cnt = o.count[j];
+      for (int q = 0; q < cnt; ++q) {
+        const float4 *tp = tris + 3 * (size_t)(first + q);
+        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+        float t, b1, b2;
+        if (!intersect_tri(s.wr, a, b, cc, s.tMin, closest, t, b1, b2)) continue;
+        closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w);
+      }
+    }
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+      if (j >= o.m || o.child[j] <= 0 || o.key[j] > closest) continue;
+      if (top < stackSize) *stack_slot(sstack, top++) = o.child[j];
+      else atomicOr(status, (uint32_t)VT_DEV_STACK);
+    }
+    if (top == 0) {
+      const int4 out = prim >= 0 ? make_int4(__float_as_int(closest), __float_as_int(hb1), __float_as_int(hb2), prim)
+                                 : make_int4(0, 0, 0, -1);
+      __stcs(hits + rid, out);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock, kMinBlocks) k_any(const float4 *__restrict__ nodes,
+                                                    const float4 *__restrict__ tris, float rootMax,
+                                                    const float4 *__restrict__ rays, uint32_t n,
+                                                    uint8_t *__restrict__ occ, uint32_t *counter,
+                                                    const uint32_t *__restrict__ perm, int stackSize,
+                                                    uint32_t *status) {
+  extern __shared__ int sstack[];
+  int top = 0;
+  uint32_t rid = 0;
+  RayState s;
+  bool exhausted = false;
+  while (true) {
+    const unsigned idle = __ballot_sync(kFull, top == 0);
+    if (!exhausted && __popc(idle) >= kRefill) {
+      const uint32_t r = refill(idle, counter, n, exhausted);
+      if (r < n) {
+        rid = perm ? __ldcs(perm + r) : r;
+        load_ray(rays, rid, s, rootMax);
+        *stack_slot(sstack, 0) = 0;
+        top = 1;
+      }
+    }
+    if (exhausted && !__any_sync(kFull, top > 0)) break;
+    if (top == 0) continue;
+    Node4 nd;
+    load_node(nodes, *stack_slot(sstack, --top), nd);
+    float nearT[4];
+    const int mask = node_hits(nd, s.sr, s.tMin, s.tMax, nearT);
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (hit || !(mask >> k & 1)) continue;
+      const int c = i4(nd.child, k);
+      if (c > 0) {
+        if (top < stackSize) *stack_slot(sstack, top++) = c;
+        else atomicOr(status, (uint32_t)VT_DEV_STACK);
+        continue;
+      }
+      const int first = -c - 1, cnt = i4(nd.count, k);
+      for (int q = 0; q < cnt; ++q) {
+        const float4 *tp = tris + 3 * (size_t)(first + q);
+        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
+        float t, b1, b2;
+        if (intersect_tri(s.wr, a, b, cc, s.tMin, s.tMax, t, b1, b2)) { hit = true; break; }
+      }
+    }
+    if (hit) top = 0;
+    if (top == 0) occ[rid] = hit ? 1 : 0;
+  }
 }
 
 __global__ void __launch_bounds__(128) k_count(const float4 *__restrict__ nodes,
@@ -288,21 +458,113 @@ __global__ void __launch_bounds__(128) k_count(const float4 *__restrict__ nodes,
 
 }  // namespace
 
-void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits,
-                       int sm_count, cudaStream_t s) {
-  (void)sm_count;
+// ---- ray ordering ----------------------------------------------------------------------------------
+// Large ray batches are traced in the order of a 30-bit key of origin and direction, so that the
+// rays of a warp follow similar paths (fewer idle lanes at divergent branches, shared cache lines).
+// The key is computed per ray, sorted with the LBVH's radix sort, and the persistent kernels read
+// ray perm[q] at queue position q; results still go to each ray's own slot.
+#ifndef VT_TRACE_SORT
+#define VT_TRACE_SORT 0
+#endif
+constexpr uint32_t kSortMinRays = 1u << 20;
+
+__device__ __forceinline__ uint32_t quant(float x, float lo, float inv, uint32_t bits) {
+  float f = (x - lo) * inv;
+  const float top = (float)((1u << bits) - 1u);
+  f = fminf(fmaxf(f, 0.0f), top);
+  return (uint32_t)f;
+}
+// Octahedral map of a unit direction to [0, 1]^2.
+__device__ __forceinline__ float2 octahedral(float dx, float dy, float dz) {
+  const float sum = fabsf(dx) + fabsf(dy) + fabsf(dz);
+  float u = dx / sum, v = dy / sum;
+  if (dz < 0.0f) {
+    const float uu = (1.0f - fabsf(v)) * (u >= 0.0f ? 1.0f : -1.0f);
+    const float vv = (1.0f - fabsf(u)) * (v >= 0.0f ? 1.0f : -1.0f);
+    u = uu; v = vv;
+  }
+  return make_float2(u * 0.5f + 0.5f, v * 0.5f + 0.5f);
+}
+
+__global__ void k_ray_keys(const float4 *__restrict__ rays, uint32_t n, float3 lo, float3 inv,
+                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, int mode) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 r0 = __ldcs(rays + 2 * (size_t)i), r1 = __ldcs(rays + 2 * (size_t)i + 1);
+  uint32_t key = 0;
+  if (mode == 1 || mode == 2) {
+    // Origin Morton code (10 bits per axis), or octant + 9 bits per axis.
+    const uint32_t b = mode == 1 ? 10u : 9u;
+    const float sc = (float)(1u << b);
+    uint32_t q[3] = {quant(r0.x, lo.x, inv.x * sc, b), quant(r0.y, lo.y, inv.y * sc, b), quant(r0.z, lo.z, inv.z * sc, b)};
+    for (uint32_t bit = 0; bit < b; ++bit)
+      for (int a = 0; a < 3; ++a) key |= ((q[a] >> bit) & 1u) << (3 * bit + (2 - a));
+    if (mode == 2) key |= ((r1.x < 0.0f ? 4u : 0u) | (r1.y < 0.0f ? 2u : 0u) | (r1.z < 0.0f ? 1u : 0u)) << 27;
+  } else if (mode == 3) {
+    // 5-D Morton code: 6 bits each of origin x, y, z and octahedral direction u, v.
+    const float2 o = octahedral(r1.x, r1.y, r1.z);
+    uint32_t q[5] = {quant(r0.x, lo.x, inv.x * 64.0f, 6), quant(r0.y, lo.y, inv.y * 64.0f, 6),
+                     quant(r0.z, lo.z, inv.z * 64.0f, 6), quant(o.x, 0.0f, 64.0f, 6), quant(o.y, 0.0f, 64.0f, 6)};
+    for (uint32_t bit = 0; bit < 6; ++bit)
+      for (int a = 0; a < 5; ++a) key |= ((q[a] >> bit) & 1u) << (5 * bit + (4 - a));
+  } else {
+    // Direction major (5 + 5 octahedral bits), origin Morton minor (20 bits).
+    const float2 o = octahedral(r1.x, r1.y, r1.z);
+    const uint32_t du = quant(o.x, 0.0f, 32.0f, 5), dv = quant(o.y, 0.0f, 32.0f, 5);
+    uint32_t q[3] = {quant(r0.x, lo.x, inv.x * 128.0f, 7), quant(r0.y, lo.y, inv.y * 128.0f, 7), quant(r0.z, lo.z, inv.z * 64.0f, 6)};
+    uint32_t m = 0, pos = 0;
+    for (uint32_t bit = 0; bit < 7; ++bit)
+      for (int a = 0; a < 3; ++a)
+        if (bit < (a == 2 ? 6u : 7u)) m |= ((q[a] >> bit) & 1u) << pos++;
+    key = (du << 25) | (dv << 20) | m;
+  }
+  keys[i] = key;
+  vals[i] = i;
+}
+
+namespace {
+// Stack entries a traversal of a tree of `depth` levels needs: the root, then at most 3 net pushes
+// per level below it (a visit pops one node and pushes up to four).
+inline int stack_entries(uint32_t depth) { return depth <= 1 ? 1 : 3 * (int)(depth - 1) + 1; }
+
+// Resident blocks per SM for a persistent kernel with `smem` bytes of dynamic shared memory.
+template <typename K> int resident_blocks(K kernel, size_t smem) {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kBlock, smem) != cudaSuccess || b < 1) b = 1;
+  return b;
+}
+
+template <typename K> void prepare(K kernel, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+}  // namespace
+
+void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits, int sm_count,
+                       uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s) {
   if (n == 0) return;
-  k_closest<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
-                                           mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
-                                           reinterpret_cast<int4 *>(hits));
+  const int S = stack_entries(mesh->depth);
+  const size_t smem = (size_t)S * kBlock * sizeof(int);
+  prepare(k_closest, smem);
+  const uint32_t want = (n + kBlock - 1) / kBlock;
+  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_closest, smem) * sm_count));
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  k_closest<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
+                                       mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
+                                       reinterpret_cast<int4 *>(hits), counter, perm, S, status);
 }
 
 void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t *occ, int sm_count,
-                   cudaStream_t s) {
-  (void)sm_count;
+                   uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s) {
   if (n == 0) return;
-  k_any<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
-                                       mesh->root_max, reinterpret_cast<const float4 *>(rays), n, occ);
+  const int S = stack_entries(mesh->depth);
+  const size_t smem = (size_t)S * kBlock * sizeof(int);
+  prepare(k_any, smem);
+  const uint32_t want = (n + kBlock - 1) / kBlock;
+  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_any, smem) * sm_count));
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  k_any<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
+                                   mesh->root_max, reinterpret_cast<const float4 *>(rays), n, occ, counter, perm,
+                                   S, status);
 }
 
 void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int closest,
@@ -311,4 +573,21 @@ void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int cl
   k_count<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
                                          mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
                                          closest, acc);
+}
+
+size_t vt_ray_order_words(uint32_t n) { return 4 * (((size_t)n + 63) & ~size_t(63)) + vt_radix_temp_words(n) + 64; }
+
+const uint32_t *vt_ray_order(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint32_t *scratch,
+                             cudaStream_t s) {
+  if (VT_TRACE_SORT == 0 || n < kSortMinRays) return nullptr;
+  // Each array starts on a 256-byte boundary: the sort reads them with 16-byte vector loads.
+  const size_t stride = ((size_t)n + 63) & ~size_t(63);
+  uint32_t *keys = scratch, *vals = keys + stride, *keysAlt = vals + stride, *valsAlt = keysAlt + stride;
+  uint32_t *temp = valsAlt + stride;
+  float3 lo = make_float3(mesh->lo[0], mesh->lo[1], mesh->lo[2]);
+  float ex = mesh->hi[0] - mesh->lo[0], ey = mesh->hi[1] - mesh->lo[1], ez = mesh->hi[2] - mesh->lo[2];
+  float3 inv = make_float3(ex > 0 ? 1.0f / ex : 0.0f, ey > 0 ? 1.0f / ey : 0.0f, ez > 0 ? 1.0f / ez : 0.0f);
+  k_ray_keys<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4 *>(rays), n, lo, inv, keys, vals, VT_TRACE_SORT);
+  vt_radix_sort_pairs(keys, vals, keysAlt, valsAlt, n, 30, temp, s);
+  return vals;
 }

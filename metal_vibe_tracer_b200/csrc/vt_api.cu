@@ -58,6 +58,20 @@ vt_status ensure_chunks(vt_ctx *ctx, size_t in_bytes, size_t out_bytes) {
   return VT_OK;
 }
 
+// Ray-ordering scratch of `slot` (0: caller streams, 1-2: the host pipeline's streams).
+vt_status order_scratch(vt_ctx *ctx, int slot, uint32_t n, uint32_t **out) {
+  size_t words = vt_ray_order_words(n);
+  if (words > ctx->order_words[slot]) {
+    cudaFree(ctx->d_order[slot]);
+    ctx->d_order[slot] = nullptr;
+    ctx->order_words[slot] = 0;
+    VT_CUDA(ctx, cudaMalloc(&ctx->d_order[slot], words * sizeof(uint32_t)));
+    ctx->order_words[slot] = words;
+  }
+  *out = ctx->d_order[slot];
+  return VT_OK;
+}
+
 vt_status check_trace_args(vt_ctx *ctx, const vt_mesh *mesh, const void *rays, const void *out, uint32_t n) {
   if (!ctx) return VT_ERR_INVALID;
   if (!mesh) return vt_fail(ctx, VT_ERR_INVALID, "mesh is null");
@@ -98,7 +112,7 @@ vt_status vt_ctx_create(int32_t device, vt_ctx **out) {
       (e = cudaStreamCreateWithFlags(&c->pipe[0], cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->pipe[1], cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreate(&c->ev0)) != cudaSuccess || (e = cudaEventCreate(&c->ev1)) != cudaSuccess ||
-      (e = cudaMalloc(&c->d_status, 64)) != cudaSuccess || (e = cudaMalloc(&c->d_counters, 256)) != cudaSuccess) {
+      (e = cudaMalloc(&c->d_status, 64)) != cudaSuccess || (e = cudaMalloc(&c->d_counters, kCounterWords * sizeof(uint32_t))) != cudaSuccess) {
     g_no_ctx_error = std::string("context creation: ") + cudaGetErrorString(e);
     vt_ctx_destroy(c);
     return VT_ERR_CUDA;
@@ -112,6 +126,7 @@ vt_status vt_ctx_destroy(vt_ctx *ctx) {
   if (!ctx) return VT_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int k = 0; k < 3; ++k) cudaFree(ctx->d_order[k]);
   for (int k = 0; k < 2; ++k) {
     if (ctx->pipe[k]) cudaStreamSynchronize(ctx->pipe[k]);
     cudaFree(ctx->d_chunk_in[k]);
@@ -248,32 +263,36 @@ vt_status vt_mesh_get_binary(vt_ctx *ctx, const vt_mesh *mesh, int32_t *children
   return VT_OK;
 }
 
-vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
-                           vt_hit *hits_dev, void *stream) {
-  vt_status st = check_trace_args(ctx, mesh, rays_dev, hits_dev, n);
+// Shared body of the device-buffer entry points; `slot` picks the ray-ordering scratch.
+static vt_status trace_device(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n, void *out,
+                              bool closest, cudaStream_t s, int slot) {
+  vt_status st = check_trace_args(ctx, mesh, rays_dev, out, n);
   if (st) return st;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL = the default stream
+  if (n == 0) return VT_OK;
   if (mesh->nfaces == 0) {
-    if (n) k_fill_miss<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<int4 *>(hits_dev), n);
+    if (closest) k_fill_miss<<<(n + 255) / 256, 256, 0, s>>>(static_cast<int4 *>(out), n);
+    else VT_CUDA(ctx, cudaMemsetAsync(out, 0, n, s));
   } else {
-    vt_launch_closest(mesh, rays_dev, n, hits_dev, ctx->sm_count, s);
+    uint32_t *scratch = nullptr;
+    st = order_scratch(ctx, slot, n, &scratch);
+    if (st) return st;
+    const uint32_t *perm = vt_ray_order(mesh, rays_dev, n, scratch, s);
+    if (closest) vt_launch_closest(mesh, rays_dev, n, static_cast<vt_hit *>(out), ctx->sm_count, vt_queue_slot(ctx), perm, ctx->d_status + 1, s);
+    else vt_launch_any(mesh, rays_dev, n, static_cast<uint8_t *>(out), ctx->sm_count, vt_queue_slot(ctx), perm, ctx->d_status + 1, s);
   }
   VT_CUDA(ctx, cudaGetLastError());
   return VT_OK;
 }
 
+vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
+                           vt_hit *hits_dev, void *stream) {
+  // NULL stream = the CUDA default stream.
+  return trace_device(ctx, mesh, rays_dev, n, hits_dev, true, static_cast<cudaStream_t>(stream), 0);
+}
+
 vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
                        uint8_t *occluded_dev, void *stream) {
-  vt_status st = check_trace_args(ctx, mesh, rays_dev, occluded_dev, n);
-  if (st) return st;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL = the default stream
-  if (mesh->nfaces == 0) {
-    if (n) VT_CUDA(ctx, cudaMemsetAsync(occluded_dev, 0, n, s));
-  } else {
-    vt_launch_any(mesh, rays_dev, n, occluded_dev, ctx->sm_count, s);
-  }
-  VT_CUDA(ctx, cudaGetLastError());
-  return VT_OK;
+  return trace_device(ctx, mesh, rays_dev, n, occluded_dev, false, static_cast<cudaStream_t>(stream), 0);
 }
 
 // Host pipeline: chunk c goes on stream c % 2 as copy-in, trace, copy-out; the two streams let
@@ -297,8 +316,7 @@ static vt_status trace_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays
     VT_CUDA(ctx, cudaMemcpyAsync(ctx->d_chunk_in[k], rays + first, (size_t)m * sizeof(vt_ray),
                                  cudaMemcpyHostToDevice, s));
     const vt_ray *dr = static_cast<const vt_ray *>(ctx->d_chunk_in[k]);
-    if (closest) st = vt_trace_closest(ctx, mesh, dr, m, static_cast<vt_hit *>(ctx->d_chunk_out[k]), s);
-    else st = vt_trace_any(ctx, mesh, dr, m, static_cast<uint8_t *>(ctx->d_chunk_out[k]), s);
+    st = trace_device(ctx, mesh, dr, m, ctx->d_chunk_out[k], closest, s, 1 + k);
     if (st) return st;
     VT_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(out) + (size_t)first * out_stride, ctx->d_chunk_out[k],
                                  (size_t)m * out_stride, cudaMemcpyDeviceToHost, s));
@@ -326,7 +344,7 @@ vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_de
   *nodes_visited = 0;
   *tris_tested = 0;
   if (n == 0 || mesh->nfaces == 0) return VT_OK;
-  unsigned long long *acc = reinterpret_cast<unsigned long long *>(ctx->d_counters);
+  unsigned long long *acc = vt_count_words(ctx);
   VT_CUDA(ctx, cudaMemsetAsync(acc, 0, 2 * sizeof(unsigned long long), ctx->stream));
   vt_launch_count(mesh, rays_dev, n, closest, acc, ctx->stream);
   VT_CUDA(ctx, cudaGetLastError());

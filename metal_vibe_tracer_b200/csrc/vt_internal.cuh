@@ -18,11 +18,17 @@ struct vt_ctx {
   cudaStream_t pipe[2] = {nullptr, nullptr};  // host-buffer pipelining (copy in, trace, copy out)
   std::string error;
   uint32_t *d_status = nullptr;         // device-side error word (build validation, kernels)
-  uint32_t *d_counters = nullptr;       // scratch counters for kernels (work queues)
+  uint32_t *d_counters = nullptr;       // scratch: ray-queue heads (kQueueSlots words, one per
+                                        // launch in rotation) then the count accumulators
+  uint32_t next_slot = 0;               // next ray-queue slot
   // Host-pipeline device buffers (allocated on first use, grown as needed).
   void *d_chunk_in[2] = {nullptr, nullptr};
   void *d_chunk_out[2] = {nullptr, nullptr};
   size_t chunk_in_bytes = 0, chunk_out_bytes = 0;
+  // Ray-ordering scratch (keys, permutation, sort buffers), grown on demand. One per pipeline
+  // stream plus one for caller streams, so concurrent launches do not share it.
+  uint32_t *d_order[3] = {nullptr, nullptr, nullptr};
+  size_t order_words[3] = {0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -55,6 +61,19 @@ vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what);
     if (_e != cudaSuccess) return vt_cuda_fail(ctx, _e, #call); \
   } while (0)
 
+// Ray-queue slots: consecutive traversal launches take slots in rotation (32 bytes apart), so up
+// to kQueueSlots launches of one context may run concurrently on different streams.
+constexpr uint32_t kQueueSlots = 16;
+constexpr uint32_t kCounterWords = kQueueSlots * 8 + 8;  // + two uint64 count accumulators
+inline uint32_t *vt_queue_slot(vt_ctx *ctx) {
+  uint32_t *p = ctx->d_counters + 8 * (ctx->next_slot % kQueueSlots);
+  ++ctx->next_slot;
+  return p;
+}
+inline unsigned long long *vt_count_words(vt_ctx *ctx) {
+  return reinterpret_cast<unsigned long long *>(ctx->d_counters + kQueueSlots * 8);
+}
+
 // Device error word bits (ctx->d_status).
 enum : uint32_t {
   VT_DEV_BAD_INDEX = 1u,       // a face indexes past the vertex array
@@ -82,9 +101,20 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
                         uint32_t nverts, const vt_build_options &opt, vt_mesh *mesh);
 
 // Traversal launches (traverse.cu).
+// Persistent kernels; `counter` is one device word of scratch (the ray queue head), reset by the
+// launch on stream s.
+// `status` receives VT_DEV_STACK if a traversal stack would overflow (it cannot for a tree within
+// the mesh's recorded depth; the check keeps a corrupted tree from writing out of bounds).
 void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits,
-                       int sm_count, cudaStream_t s);
+                       int sm_count, uint32_t *counter, const uint32_t *perm, uint32_t *status,
+                       cudaStream_t s);
 void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t *occ,
-                   int sm_count, cudaStream_t s);
+                   int sm_count, uint32_t *counter, const uint32_t *perm, uint32_t *status,
+                   cudaStream_t s);
+// Ray ordering for large batches: returns the device permutation (inside `scratch`, which must
+// hold vt_ray_order_words(n) words) or nullptr when the batch is traced in input order.
+size_t vt_ray_order_words(uint32_t n);
+const uint32_t *vt_ray_order(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint32_t *scratch,
+                             cudaStream_t s);
 void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int closest,
                      unsigned long long *acc /* 2 device words */, cudaStream_t s);
