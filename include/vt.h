@@ -146,6 +146,75 @@ vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays
 vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
                          int32_t closest, uint64_t *nodes_visited, uint64_t *tris_tested);
 
+/* ---- path tracing (integrator) ------------------------------------------------------------- */
+
+typedef struct vt_scene vt_scene;
+
+/* Material types: the reference's MaterialType values (main.swift:316-322). */
+enum { VT_MAT_DIFFUSE = 0, VT_MAT_EMISSIVE = 3 };
+
+/* A constant material slot (the role of SurfaceSettings / MaterialResources, main.swift:2253-2263,
+ * 628-654, for constant Lambert and emissive surfaces). A face's tag selects its slot. 32 bytes. */
+typedef struct vt_material {
+  int32_t type;        /* VT_MAT_DIFFUSE or VT_MAT_EMISSIVE */
+  float albedo[3];     /* linear sRGB reflectance (Lambert) */
+  float emission[3];   /* linear sRGB radiance (emissive) */
+  float pad;
+} vt_material;
+
+/* The procedural area light of the reference's scenes 1/3/4 (sample_direct_light, main.swift:
+ * 2957-2978; eval_light_pdf, main.swift:3046-3050): a parallelogram corner + u su + v sv emitting
+ * towards `normal`. The scene's emissive faces should cover the same quad. 64 bytes. */
+typedef struct vt_quad_light {
+  float corner[3], su[3], sv[3], normal[3];
+  float emission[3];   /* radiance, linear sRGB (the light tint applied) */
+  float pad;
+} vt_quad_light;
+
+/* Spectral transport tables (1 nm bins from lambda_min): linear-sRGB colour-matching functions,
+ * the emitters' illuminant (luminance 1) and the wavelength inverse CDF (segments + 1 nodes); the
+ * roles of the spectral sampling buffer written by spectral_icdf_kernel (main.swift:8117-8185). */
+typedef struct vt_spectral_tables {
+  const float *cmf_rgb;     /* nbins x 3 */
+  const float *illuminant;  /* nbins */
+  const float *icdf;        /* segments + 1 */
+  uint32_t nbins, segments;
+  float lambda_min;
+  uint32_t pad;
+} vt_spectral_tables;
+
+/* Per-frame parameters: the subset of Uniforms (main.swift:393-420) the integrator reads. */
+typedef struct vt_frame_params {
+  float camera_pos[3];
+  float fov_deg;            /* vertical field of view (Uniforms.cameraPos.w) */
+  float camera_target[3];
+  uint32_t max_depth;       /* path depth, 1 = direct light only (Uniforms.cameraTarget.w) */
+  float camera_up[3];
+  uint32_t sampling_mode;   /* 1 = NEE + BSDF with power-heuristic MIS, 2 = light sampling (NEE),
+                               3 = BSDF sampling (Uniforms.samplingMode 1-3) */
+  uint32_t width, height;
+  uint32_t first_sample;    /* sample index of the first frame (>= 1, Uniforms.sampleIndex) */
+  uint32_t spectral;        /* 1 = four hero wavelengths, 0 = RGB transport */
+} vt_frame_params;
+
+/* A renderable scene: the mesh, its material slots, the area light and (optionally) the spectral
+ * tables, plus the FP64 accumulation. Replaces MaterialLibrary.bind + the renderer's resources
+ * (main.swift:9432-9449, 11016-11154). Host arrays are copied. */
+vt_status vt_scene_create(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
+                          const vt_quad_light *light, const vt_spectral_tables *tables, vt_scene **out);
+vt_status vt_scene_destroy(vt_ctx *ctx, vt_scene *scene);
+/* Renders `spp` frames (sample indices first_sample .. first_sample + spp - 1, one sample per pixel
+ * each, jittered by the reference's frameJitter) and adds them to the scene's FP64 accumulation.
+ * Replaces renderFrame(output:samples:) / encodeSample (main.swift:10978, 11214-11708) for the
+ * MIS integrator: camera ray, closest hit, NEE with MIS, BSDF continuation, Russian roulette
+ * (shading_kernel, main.swift:7370-7914). Resizing (a new width/height) resets the accumulation.
+ * Stream-ordered; NULL = the CUDA default stream. */
+vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *params, uint32_t spp, void *stream);
+vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene);
+/* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3)
+ * and the number of samples accumulated. Synchronises. */
+vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t n, uint32_t *samples);
+
 /* ---- allocation-free build --------------------------------------------------------------- */
 
 /* No counterpart in the reference. The same GPU build as vt_mesh_build_device, for callers that
@@ -156,7 +225,8 @@ vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_de
  * comes from a 6 MiB static device array that each GPU loading the library holds until exit.
  *   nodes: nodes_capacity >= nfaces 4-wide nodes (16-byte aligned); info->wide_nodes are written.
  *   tris:  12 floats per face (three float4 per BVH position: a with the input face index's bits
- *          in .w, b, c; 16-byte aligned).  order: nfaces int32 (BVH position -> input face).
+ *          in .w, b with the face's tag bits in .w, c; 16-byte aligned).
+ *   order: nfaces int32 (BVH position -> input face).
  *   info:  host output (build_ms is host wall time).  stream: NULL = the CUDA default stream;
  *          the call returns when the build on that stream is complete.
  *   error: optional host buffer of error_capacity bytes for the failure message.

@@ -67,6 +67,11 @@ SIGNATURES = {
     "vt_trace_count": (_I32, [_P, _P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "vt_mesh_build_noalloc": (_I32, [_P, _U32, _P, _U32, C.POINTER(BuildOptions), _P, _U32, _P, _P,
                                      C.POINTER(MeshInfo), _P, C.c_char_p, _U32]),
+    "vt_scene_create": (_I32, [_P, _P, _P, _U32, _P, _P, C.POINTER(_P)]),
+    "vt_scene_destroy": (_I32, [_P, _P]),
+    "vt_render": (_I32, [_P, _P, _P, _U32, _P]),
+    "vt_accum_reset": (_I32, [_P, _P]),
+    "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
 }
 NOALLOC_MAX_FACES = 32768
 

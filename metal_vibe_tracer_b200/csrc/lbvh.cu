@@ -425,7 +425,7 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
           vt_face fc = faces[f];
           const vt_vertex &va = verts[fc.a], &vb = verts[fc.b], &vc = verts[fc.c];
           tris[3 * prim] = make_float4(va.px, va.py, va.pz, __int_as_float((int)f));
-          tris[3 * prim + 1] = make_float4(vb.px, vb.py, vb.pz, 0.0f);
+          tris[3 * prim + 1] = make_float4(vb.px, vb.py, vb.pz, __uint_as_float(fc.tag));
           tris[3 * prim + 2] = make_float4(vc.px, vc.py, vc.pz, 0.0f);
           ++prim;
           continue;

@@ -41,12 +41,29 @@ struct vt_mesh {
   float build_ms = 0.0f;
   float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
   vt_wide_node *d_nodes = nullptr;   // nnodes, reference layout (128 B, 16-B vector loads)
-  float4 *d_tris = nullptr;          // 3 per BVH position: (a, face id bits), (b, 0), (c, 0)
+  float4 *d_tris = nullptr;          // 3 per BVH position: (a, face id bits), (b, face tag bits), (c, 0)
   int32_t *d_order = nullptr;        // BVH position -> input face
   uint32_t *d_codes = nullptr;       // sorted Morton codes
   int32_t *d_sorted = nullptr;       // sorted position -> input face
   int32_t *d_bin_child = nullptr;    // 2 per binary internal node (refined)
   float *d_bin_box = nullptr;        // 8 per binary internal node (lo xyz, -, hi xyz, -)
+};
+
+struct vt_scene {
+  const vt_mesh *mesh = nullptr;
+  vt_material *d_mats = nullptr;
+  uint32_t nmat = 0;
+  vt_quad_light light;
+  // Spectral tables: per 1 nm bin (cmf r, g, b, illuminant), the inverse CDF.
+  float4 *d_spec = nullptr;
+  float *d_icdf = nullptr;
+  uint32_t nbins = 0, segments = 0;
+  float lambda_min = 0.0f;
+  // FP64 accumulation (3 doubles per pixel) and its sample count.
+  double *d_accum = nullptr;
+  uint32_t width = 0, height = 0, samples = 0;
+  float2 *d_jitter = nullptr;
+  uint32_t jitter_cap = 0;
 };
 
 // ---------------------------------------------------------------------------------------------

@@ -1,0 +1,123 @@
+"""Path tracing on the B200: scenes, frames and the FP64 accumulation (host side of include/vt.h).
+
+The roles of the reference's renderer: `MaterialLibrary` resources and bind (main.swift:9432-9449),
+`renderFrame(output:samples:)` / `encodeSample` (main.swift:10978, 11214-11708) for the MIS
+integrator (shading_kernel, main.swift:7370-7914), and the accumulation read back as linear sRGB.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .accel import Context, MaterialLibraryError, Mesh, _check
+
+VT_MAT_DIFFUSE, VT_MAT_EMISSIVE = 0, 3
+
+
+class Material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("albedo", C.c_float * 3), ("emission", C.c_float * 3), ("pad", C.c_float)]
+
+
+class QuadLight(C.Structure):
+    _fields_ = [("corner", C.c_float * 3), ("su", C.c_float * 3), ("sv", C.c_float * 3), ("normal", C.c_float * 3),
+                ("emission", C.c_float * 3), ("pad", C.c_float)]
+
+
+class SpectralTables(C.Structure):
+    _fields_ = [("cmf_rgb", C.c_void_p), ("illuminant", C.c_void_p), ("icdf", C.c_void_p),
+                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float), ("pad", C.c_uint32)]
+
+
+class FrameParams(C.Structure):
+    _fields_ = [("camera_pos", C.c_float * 3), ("fov_deg", C.c_float), ("camera_target", C.c_float * 3),
+                ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
+                ("spectral", C.c_uint32)]
+
+
+assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 64
+
+
+def make_materials(materials) -> C.Array:
+    arr = (Material * len(materials))()
+    for i, m in enumerate(materials):
+        arr[i].type = int(m["type"])
+        arr[i].albedo[:] = [float(x) for x in m["albedo"]]
+        arr[i].emission[:] = [float(x) for x in m["emission"]]
+    return arr
+
+
+def make_light(light) -> QuadLight:
+    q = QuadLight()
+    for k in ("corner", "su", "sv", "normal", "emission"):
+        getattr(q, k)[:] = [float(x) for x in light[k]]
+    return q
+
+
+def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1) -> FrameParams:
+    p = FrameParams()
+    p.camera_pos[:] = [float(x) for x in camera["pos"]]
+    p.camera_target[:] = [float(x) for x in camera["target"]]
+    p.camera_up[:] = [float(x) for x in camera["up"]]
+    p.fov_deg = float(camera["fov"])
+    p.max_depth = int(max_depth)
+    p.sampling_mode = int(mode)  # 1 MIS, 2 light sampling, 3 BSDF sampling (Uniforms.samplingMode)
+    p.width, p.height = int(width), int(height)
+    p.first_sample = int(first_sample)
+    p.spectral = 1 if spectral else 0
+    return p
+
+
+class Scene:
+    """A renderable scene on the device (vt_scene): mesh, material slots, area light, spectral
+    tables and the FP64 accumulation."""
+
+    def __init__(self, ctx: Context, mesh: Mesh, materials, light, spectral: dict | None = None):
+        lib = _lib.load()
+        self.ctx, self.mesh = ctx, mesh
+        self._mats = make_materials(materials)
+        self._light = make_light(light)
+        tables = None
+        if spectral is not None:
+            self._cmf = np.ascontiguousarray(spectral["cmf_rgb"], np.float32)
+            self._illum = np.ascontiguousarray(spectral["illum"], np.float32)
+            self._icdf = np.ascontiguousarray(spectral["icdf"], np.float32)
+            tables = SpectralTables(self._cmf.ctypes.data, self._illum.ctypes.data, self._icdf.ctypes.data,
+                                    self._cmf.shape[0], self._icdf.shape[0] - 1, float(spectral["lambda_min"]), 0)
+        p = C.c_void_p()
+        st = lib.vt_scene_create(ctx.handle, mesh._p, self._mats, len(materials), C.byref(self._light),
+                                 C.byref(tables) if tables is not None else None, C.byref(p))
+        _check(ctx.handle, st, "vt_scene_create")
+        self._p = p
+        self.width = self.height = 0
+
+    def render(self, params: FrameParams, spp: int, stream=None) -> None:
+        """Adds `spp` frames (one sample per pixel each) to the accumulation; stream-ordered."""
+        self.width, self.height = params.width, params.height
+        _check(self.ctx.handle, _lib.load().vt_render(self.ctx.handle, self._p, C.byref(params), int(spp), stream),
+               "vt_render")
+
+    def reset(self) -> None:
+        _check(self.ctx.handle, _lib.load().vt_accum_reset(self.ctx.handle, self._p), "vt_accum_reset")
+
+    def readback(self) -> tuple[np.ndarray, int]:
+        """(height, width, 3) float64 mean radiance and the sample count."""
+        n = 3 * self.width * self.height
+        out = np.empty(n, np.float64)
+        samples = C.c_uint32()
+        _check(self.ctx.handle, _lib.load().vt_accum_readback(self.ctx.handle, self._p, out.ctypes.data, n,
+                                                              C.byref(samples)), "vt_accum_readback")
+        return out.reshape(self.height, self.width, 3), int(samples.value)
+
+    def close(self) -> None:
+        if getattr(self, "_p", None) is not None and self.ctx._p is not None:
+            _lib.load().vt_scene_destroy(self.ctx.handle, self._p)
+        self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

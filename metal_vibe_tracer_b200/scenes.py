@@ -1,4 +1,4 @@
-"""Seeded synthetic workloads for the traversal path.
+"""Seeded synthetic workloads: the traversal microbenchmark and the integrator's Cornell box.
 
 Triangle soup: ``n`` triangles whose centroids are uniform in the unit cube, with edge lengths
 lognormal(mu = ln 0.002, sigma = 0.5) and uniformly random orientations; each triangle is
@@ -137,3 +137,77 @@ def shadow_tmax_torch(rays, coherent: bool, seed: int = 2):
     lo, hi = (1.0, 2.2) if coherent else (0.05, 1.0)
     out[:, 7] = lo + (hi - lo) * torch.rand((rays.shape[0],), generator=g, device=rays.device)
     return out
+
+
+# ---- procedural Cornell box (the integrator's workload) ------------------------------------------
+def _pcg_hash(v: int) -> int:
+    state = (v * 747796405 + 2891336453) & 0xFFFFFFFF
+    word = (((state >> ((state >> 28) + 4)) ^ state) * 277803737) & 0xFFFFFFFF
+    return ((word >> 22) ^ word) & 0xFFFFFFFF
+
+
+def cornell_box(light_radiance: float = 17.0, seed: int = 0):
+    """Procedural Cornell box of the reference's scene 1 (main.swift:1421-1438) as triangles.
+
+    Five walls of the cube [-1, 1]^3, open at -z toward the camera (10 triangles), two axis-aligned
+    boxes at scene 1's centres and half extents (tall (-0.33, -0.4, 0.35) +- (0.3, 0.6, 0.3), short
+    (0.33, -0.7, -0.25) +- (0.3, 0.3, 0.3); 24 triangles), and a 0.25 x 0.25 emitter quad under the
+    ceiling at y = 0.999, facing down (2 triangles). Surfaces are grey Lambert: surface s (floor,
+    ceiling, back, left, right, tall box, short box) has albedo 0.2 + 0.6 u with u the first PCG
+    draw of state (seed * 7 + s) (main.swift:91-101). The emitter has grey radiance
+    `light_radiance` (CIE D65 spectrum in spectral transport, luminance = radiance).
+    Returns faces, vertices, materials (list of dicts), the quad light (dict) and the camera
+    (scene 1's default view, main.swift:10749-10755: yaw 0.45, pitch 0.25, distance 3.4, target
+    (0, -0.1, 0), fov 42 degrees).
+    """
+    quads = [  # corner, u, v (scene 1's walls)
+        ((-1, -1, -1), (2, 0, 0), (0, 0, 2)),     # floor
+        ((-1, 1, -1), (2, 0, 0), (0, 0, 2)),      # ceiling
+        ((1, 1, 1), (-2, 0, 0), (0, -2, 0)),      # back
+        ((-1, 1, 1), (0, 0, -2), (0, -2, 0)),     # left
+        ((1, 1, -1), (0, 0, 2), (0, -2, 0)),      # right
+    ]
+    tris, tags = [], []
+
+    def quad(c, u, v, tag):
+        c, u, v = np.array(c, float), np.array(u, float), np.array(v, float)
+        tris.extend([(c, c + u, c + u + v), (c, c + u + v, c + v)])
+        tags.extend([tag, tag])
+
+    for s, (c, u, v) in enumerate(quads):
+        quad(c, u, v, s)
+
+    def box(center, half, tag):
+        lo, hi = np.array(center) - np.array(half), np.array(center) + np.array(half)
+        x0, y0, z0 = lo
+        x1, y1, z1 = hi
+        quad((x0, y0, z0), (x1 - x0, 0, 0), (0, y1 - y0, 0), tag)   # -z
+        quad((x0, y0, z1), (0, y1 - y0, 0), (x1 - x0, 0, 0), tag)   # +z
+        quad((x0, y0, z0), (0, y1 - y0, 0), (0, 0, z1 - z0), tag)   # -x
+        quad((x1, y0, z0), (0, 0, z1 - z0), (0, y1 - y0, 0), tag)   # +x
+        quad((x0, y0, z0), (0, 0, z1 - z0), (x1 - x0, 0, 0), tag)   # -y
+        quad((x0, y1, z0), (x1 - x0, 0, 0), (0, 0, z1 - z0), tag)   # +y
+
+    box((-0.33, -0.4, 0.35), (0.3, 0.6, 0.3), 5)
+    box((0.33, -0.7, -0.25), (0.3, 0.3, 0.3), 6)
+    lc, lsu, lsv = (-0.125, 0.999, -0.125), (0.25, 0, 0), (0, 0, 0.25)
+    quad(lc, lsu, lsv, 7)
+    n = len(tris)
+    verts = np.zeros(3 * n, VERTEX_DTYPE)
+    verts["p"] = np.array(tris, np.float64).reshape(-1, 3).astype(np.float32)
+    faces = np.zeros(n, FACE_DTYPE)
+    i = np.arange(n, dtype=np.uint32)
+    faces["a"], faces["b"], faces["c"] = 3 * i, 3 * i + 1, 3 * i + 2
+    faces["tag"] = np.array(tags, np.uint32)
+    materials = []
+    for s in range(7):
+        state = _pcg_hash((seed * 7 + s) & 0xFFFFFFFF)
+        a = np.float32(0.2) + np.float32(0.6) * (np.float32(state >> 8) * np.float32(1.0 / 16777216.0))
+        materials.append({"type": 0, "albedo": (float(a),) * 3, "emission": (0.0, 0.0, 0.0)})
+    materials.append({"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (light_radiance,) * 3})
+    light = {"corner": lc, "su": lsu, "sv": lsv, "normal": (0, -1, 0), "emission": (light_radiance,) * 3}
+    yaw, pitch, dist, target = 0.45, 0.25, 3.4, np.array([0.0, -0.1, 0.0])
+    eye = target + dist * np.array([math.cos(pitch) * math.sin(yaw), math.sin(pitch), -math.cos(pitch) * math.cos(yaw)])
+    camera = {"pos": tuple(float(x) for x in eye.astype(np.float32)), "target": tuple(float(x) for x in target), "up": (0.0, 1.0, 0.0),
+              "fov": 42.0}
+    return faces, verts, materials, light, camera

@@ -1,0 +1,160 @@
+"""Spectral transport tables: CIE 1931 CMFs as linear sRGB, the D65 illuminant and the wavelength
+inverse CDF (restating scripts/generate_spectral_tables.py: `Data` :142-181, `sampling_density`
+:490-500, `inverse_cdf` :510-530).
+
+The CIE datasets are CC BY-SA 4.0 and are not part of this repository. `generate()` reads them
+at build time from the reference's vendored copies (Vendor/Spectral/CIE) and writes the derived
+tables to `data/spectral_<lo>_<hi>.bin` (git-ignored, shipped with the built library); `load()`
+reads that file at run time. Every table is a 1 nm table over [lambda_min, lambda_max]:
+
+* cmf_rgb[i]  linear-sRGB colour-matching functions M xyz(lambda_i), with M the XYZ -> linear sRGB
+              matrix whose white point is the computed XYZ of D65 (so D65 maps to rgb (1, 1, 1));
+* illum[i]    D65, normalised to luminance Y = 1 (1 nm sums over the range);
+* icdf[n]     1025 nodes: lambda at u = n / 1024 of the piecewise-linear density
+              0.9 D65 s / int(D65 s) + 0.1 s / int(s), s = |r| + |g| + |b| of the sRGB CMFs.
+
+The renderer's default range is 380-780 nm (the traversal-path configs ask for four hero
+wavelengths over 380-780 nm); the reference tabulates 360-830 nm, which `generate(360, 830)`
+reproduces for the golden-vector check.
+"""
+from __future__ import annotations
+
+import csv
+import math
+import struct
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+DATA_DIR = PKG / "data"
+REFERENCE_CIE = Path("/root/reference/Vendor/Spectral/CIE")
+SRGB_PRIMARIES = ((0.64, 0.33), (0.30, 0.60), (0.15, 0.06))
+ICDF_SEGMENTS = 1024
+DEFENSIVE = 0.1
+MAGIC = b"VTSPEC01"
+
+
+def _read(path: Path):
+    with open(path, newline="") as f:
+        return [[float(v) for v in row] for row in csv.reader(f) if row]
+
+
+def _resample(rows, col, wavelengths):
+    pts = [(r[0], r[col]) for r in rows]
+    out, j = [], 0
+    for lam in wavelengths:
+        if lam < pts[0][0] or lam > pts[-1][0]:
+            out.append(0.0)
+            continue
+        while pts[j + 1][0] < lam:
+            j += 1
+        (x0, y0), (x1, y1) = pts[j], pts[j + 1]
+        out.append(y0 + (y1 - y0) * (lam - x0) / (x1 - x0))
+    return out
+
+
+def _inv3(m):
+    (a, b, c), (d, e, f), (g, h, i) = m
+    det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g)
+    return [[(e * i - f * h) / det, (c * h - b * i) / det, (b * f - c * e) / det],
+            [(f * g - d * i) / det, (a * i - c * g) / det, (c * d - a * f) / det],
+            [(d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det]]
+
+
+def _apply(m, v):
+    return [m[r][0] * v[0] + m[r][1] * v[1] + m[r][2] * v[2] for r in range(3)]
+
+
+def compute(lambda_min: int, lambda_max: int, cie_dir: Path = REFERENCE_CIE) -> dict:
+    """All tables in float64 (lists), from the CIE CSVs."""
+    wl = list(range(lambda_min, lambda_max + 1))
+    cmf_rows = _read(cie_dir / "CIE_xyz_1931_2deg.csv")
+    cmf = [tuple(r[1:4]) for r in cmf_rows if lambda_min <= r[0] <= lambda_max]
+    assert len(cmf) == len(wl)
+    spd = _resample(_read(cie_dir / "CIE_std_illum_D65.csv"), 1, wl)
+    y = sum(s * c[1] for s, c in zip(spd, cmf))
+    d65 = [s / y for s in spd]
+    white = [sum(s * c[k] for s, c in zip(d65, cmf)) for k in range(3)]
+    primaries = [[x / yy for x, yy in SRGB_PRIMARIES], [1.0, 1.0, 1.0],
+                 [(1 - x - yy) / yy for x, yy in SRGB_PRIMARIES]]
+    scale = _apply(_inv3(primaries), white)
+    rgb_to_xyz = [[primaries[r][k] * scale[k] for k in range(3)] for r in range(3)]
+    xyz_to_rgb = _inv3(rgb_to_xyz)
+    cmf_rgb = [_apply(xyz_to_rgb, c) for c in cmf]
+    s = [abs(v[0]) + abs(v[1]) + abs(v[2]) for v in cmf_rgb]
+
+    def normalized(values):
+        total = sum(0.5 * (values[i] + values[i + 1]) for i in range(len(values) - 1))
+        return [v / total for v in values]
+    a, b = normalized([p * q for p, q in zip(d65, s)]), normalized(s)
+    density = [(1.0 - DEFENSIVE) * x + DEFENSIVE * yv for x, yv in zip(a, b)]
+    icdf = inverse_cdf(density, lambda_min, lambda_max)
+    return {"lambda_min": lambda_min, "lambda_max": lambda_max, "cmf_xyz": cmf, "cmf_rgb": cmf_rgb,
+            "illum": d65, "icdf": icdf, "xyz_to_rgb": xyz_to_rgb, "density": density}
+
+
+def inverse_cdf(density, lambda_min, lambda_max, segments=ICDF_SEGMENTS):
+    """Wavelengths at u = i / segments of the CDF of a piecewise-linear 1 nm density (exact)."""
+    cdf = [0.0]
+    for i in range(len(density) - 1):
+        cdf.append(cdf[-1] + 0.5 * (density[i] + density[i + 1]))
+    total = cdf[-1]
+    out = [float(lambda_min)]
+    j = 0
+    for n in range(1, segments):
+        yv = total * n / segments
+        while cdf[j + 1] < yv:
+            j += 1
+        p0, p1, rest = density[j], density[j + 1], yv - cdf[j]
+        dp = p1 - p0
+        if abs(dp) < 1e-12 * max(p0, 1e-30):
+            t = rest / p0
+        else:
+            t = (-p0 + math.sqrt(max(p0 * p0 + 2.0 * dp * rest, 0.0))) / dp
+        out.append(lambda_min + j + min(max(t, 0.0), 1.0))
+    out.append(float(lambda_max))
+    for i in range(1, len(out)):
+        if out[i] <= out[i - 1]:
+            out[i] = math.nextafter(out[i - 1], math.inf)
+    return out
+
+
+def path(lambda_min: int = 380, lambda_max: int = 780) -> Path:
+    return DATA_DIR / f"spectral_{lambda_min}_{lambda_max}.bin"
+
+
+def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path = REFERENCE_CIE) -> Path:
+    """Write the float32 table file (build time; needs the CIE CSVs)."""
+    t = compute(lambda_min, lambda_max, cie_dir)
+    n = lambda_max - lambda_min + 1
+    DATA_DIR.mkdir(parents=True, exist_ok=True)
+    out = path(lambda_min, lambda_max)
+    blob = MAGIC + struct.pack("<iiii", lambda_min, lambda_max, n, ICDF_SEGMENTS)
+    blob += np.asarray(t["cmf_rgb"], np.float32).tobytes()
+    blob += np.asarray(t["illum"], np.float32).tobytes()
+    blob += np.asarray(t["icdf"], np.float32).tobytes()
+    blob += np.asarray(t["xyz_to_rgb"], np.float64).tobytes()
+    tmp = out.with_suffix(".tmp")
+    tmp.write_bytes(blob)
+    tmp.replace(out)
+    return out
+
+
+def load(lambda_min: int = 380, lambda_max: int = 780) -> dict:
+    """float32 tables from the generated file (no CIE input needed)."""
+    p = path(lambda_min, lambda_max)
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: it is generated at build time from the CIE datasets "
+                           "(metal_vibe_tracer_b200.spectral_tables.generate)")
+    b = p.read_bytes()
+    if b[:8] != MAGIC:
+        raise RuntimeError(f"{p}: bad header")
+    lo, hi, n, seg = struct.unpack("<iiii", b[8:24])
+    off = 24
+    cmf_rgb = np.frombuffer(b, np.float32, 3 * n, off).reshape(n, 3); off += 12 * n
+    illum = np.frombuffer(b, np.float32, n, off); off += 4 * n
+    icdf = np.frombuffer(b, np.float32, seg + 1, off); off += 4 * (seg + 1)
+    m = np.frombuffer(b, np.float64, 9, off).reshape(3, 3)
+    return {"lambda_min": lo, "lambda_max": hi, "n": n, "segments": seg, "cmf_rgb": cmf_rgb.copy(),
+            "illum": illum.copy(), "icdf": icdf.copy(), "xyz_to_rgb": m.copy()}

@@ -1041,3 +1041,298 @@ void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t c
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Path tracer: FP64 restatement of the MIS integrator (shading_kernel, main.swift:7370-7914, with
+// the primary hit of restir_temporal_kernel, main.swift:4842-4893), PCG sampler. The stream
+// consumption order is the reference's: wavelength numbers from a hashed copy
+// (wavelength_numbers, main.swift:2222-2231), decorrelate_shading_seed (main.swift:109-111)
+// after the camera ray, then per vertex NEE (2 draws, main.swift:2957-2978), Lambert sampling
+// (3 draws, the last two used, main.swift:3354-3360) and, after bounce 3, Russian roulette
+// (1 draw, main.swift:7819-7827).
+namespace {
+
+struct D3 { double x, y, z; };
+inline D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline D3 operator-(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline D3 cross(D3 a, D3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline D3 normalize(D3 a) { return a * (1.0 / std::sqrt(dot(a, a))); }
+inline D3 d3(const float *v) { return {v[0], v[1], v[2]}; }
+
+const double kPi = 3.14159265358979323846;
+const double kEpsPt = 0.001;  // ray_epsilon / ray_t_min of the procedural scenes
+
+inline double rand_d(uint32_t &seed) {
+  seed = pcg_hash(seed);
+  return double(seed >> 8u) * (1.0 / 16777216.0);
+}
+
+// frameJitter (main.swift:8773-8785) in float, as the host computes it.
+float halton_f(uint32_t index, uint32_t base) {
+  uint32_t n = index;
+  float fraction = 1.0f, result = 0.0f;
+  while (n > 0) {
+    fraction /= float(base);
+    result += fraction * float(n % base);
+    n /= base;
+  }
+  return result;
+}
+
+struct Spec4 { double v[4]; };
+
+struct PtContext {
+  const vto_pt_inputs *in;
+  const vt_frame_params *p;
+  vto_bvh *bvh;
+  D3 cam, fwd, right, up;
+  double aspect, fovScale, larea;
+  bool spectral;
+};
+
+struct PtLanes { int bin[4]; double w[4]; };
+
+PtLanes make_lanes(const PtContext &C, uint32_t state) {
+  PtLanes L;
+  const uint32_t h = pcg_hash(state ^ 0x5bd1e995u);
+  const double u = double(h >> 8u) * (1.0 / 16777216.0);
+  const uint32_t seg = C.in->segments;
+  for (int k = 0; k < 4; ++k) {
+    const double x = (u + k) * 0.25 * seg;
+    const uint32_t i = std::min((uint32_t)x, seg - 1u);
+    const double low = C.in->icdf[i], width = double(C.in->icdf[i + 1]) - low;
+    L.w[k] = 0.25 * seg * width;
+    const double lambda = low + (x - i) * width;
+    const double b = std::min(std::max(lambda - C.in->lambda_min + 0.5, 0.0), double(C.in->nbins - 1u));
+    L.bin[k] = (int)std::min((uint32_t)b, C.in->nbins - 1u);
+  }
+  return L;
+}
+
+D3 to_rgb(const PtContext &C, const PtLanes &L, const Spec4 &s) {
+  if (!C.spectral) return {s.v[0], s.v[1], s.v[2]};
+  D3 rgb{0, 0, 0};
+  for (int k = 0; k < 4; ++k) {
+    const float *c = C.in->cmf_rgb + 3 * L.bin[k];
+    const double a = s.v[k] * L.w[k];
+    rgb = rgb + D3{a * c[0], a * c[1], a * c[2]};
+  }
+  return rgb;
+}
+
+Spec4 reflectance(const PtContext &C, const vt_material &m) {
+  if (C.spectral) { const double g = (double(m.albedo[0]) + m.albedo[1] + m.albedo[2]) / 3.0; return {{g, g, g, g}}; }
+  return {{m.albedo[0], m.albedo[1], m.albedo[2], 0.0}};
+}
+Spec4 emission(const PtContext &C, const PtLanes &L, const float e[3]) {
+  if (C.spectral) {
+    Spec4 s;
+    for (int k = 0; k < 4; ++k) s.v[k] = double(e[0]) * C.in->illum[L.bin[k]];
+    return s;
+  }
+  return {{e[0], e[1], e[2], 0.0}};
+}
+inline Spec4 mul(const Spec4 &a, const Spec4 &b) { return {{a.v[0] * b.v[0], a.v[1] * b.v[1], a.v[2] * b.v[2], a.v[3] * b.v[3]}}; }
+inline Spec4 scale(const Spec4 &a, double s) { return {{a.v[0] * s, a.v[1] * s, a.v[2] * s, a.v[3] * s}}; }
+inline double smax(const PtContext &C, const Spec4 &a) {
+  double m = std::max(std::max(a.v[0], a.v[1]), a.v[2]);
+  return C.spectral ? std::max(m, a.v[3]) : m;
+}
+
+struct PtHit { D3 pos, gn; uint32_t slot; };
+
+bool pt_closest(const PtContext &C, D3 o, D3 d, PtHit &h) {
+  TraceRay<double> r;
+  r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
+  r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
+  r.tmin = kEpsPt; r.tmax = INFINITY;
+  double t, b1, b2;
+  int prim = -1;
+  if (!closest_hit<double>(*C.bvh, r, t, prim, b1, b2)) return false;
+  const vt_face &f = C.in->faces[prim];
+  const D3 a = d3(&C.in->verts[f.a].px), b = d3(&C.in->verts[f.b].px), c = d3(&C.in->verts[f.c].px);
+  h.pos = o + d * t;
+  const D3 ng = normalize(cross(b - a, c - a));
+  h.gn = dot(ng, d) < 0.0 ? ng : ng * -1.0;
+  h.slot = f.tag;
+  return true;
+}
+
+bool pt_occluded(const PtContext &C, D3 o, D3 d, double tmax) {
+  TraceRay<double> r;
+  r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
+  r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
+  r.tmin = kEpsPt; r.tmax = tmax;
+  return any_hit<double>(*C.bvh, r);
+}
+
+vt_material pt_material(const PtContext &C, uint32_t slot) {
+  if (slot < C.in->nmat) return C.in->materials[slot];
+  vt_material m;
+  std::memset(&m, 0, sizeof m);
+  return m;
+}
+
+inline D3 ray_origin_d(D3 p, D3 gn, D3 dir) { return p + gn * (dot(dir, gn) >= 0.0 ? kEpsPt : -kEpsPt); }
+
+double power_heuristic_d(double pf, double pg) {
+  const double s = std::max(pf, pg);
+  if (s <= 0.0) return 0.0;
+  const double f = pf / s, g = pg / s;
+  return f * f / (f * f + g * g);
+}
+
+struct PtLight { D3 pos, wi; double dist, pdf; };
+
+PtLight sample_light_d(const PtContext &C, D3 p, uint32_t &seed) {
+  PtLight ls{};
+  const vt_quad_light &l = C.in->light;
+  const double u = rand_d(seed), v = rand_d(seed);
+  const D3 lp = d3(l.corner) + d3(l.su) * u + d3(l.sv) * v;
+  D3 dir = lp - p;
+  const double dist = std::sqrt(dot(dir, dir));
+  dir = dir * (1.0 / dist);
+  const double cos_l = std::max(0.0, -dot(dir, d3(l.normal)));
+  if (cos_l > 1e-4) { ls.pos = lp; ls.wi = dir; ls.dist = dist; ls.pdf = dist * dist / (C.larea * cos_l); }
+  return ls;
+}
+
+double light_pdf_d(const PtContext &C, D3 p, D3 hit) {
+  D3 dir = hit - p;
+  const double dist = std::sqrt(dot(dir, dir));
+  dir = dir * (1.0 / dist);
+  const double cos_l = std::max(0.0, -dot(dir, d3(C.in->light.normal)));
+  return cos_l <= 0.0 ? 0.0 : dist * dist / (C.larea * cos_l);
+}
+
+bool visible_d(const PtContext &C, D3 p, D3 gn, const PtLight &ls) {
+  if (!(ls.pdf > 0.0)) return false;
+  const D3 o = ray_origin_d(p, gn, ls.wi);
+  D3 delta = ls.pos - o;
+  const double d = std::sqrt(dot(delta, delta)), tol = 2.0 * kEpsPt;
+  if (d <= tol) return false;
+  return !pt_occluded(C, o, delta * (1.0 / d), d - tol);
+}
+
+D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 wo, const Spec4 &T, const Spec4 &albedo,
+            bool useMIS, uint32_t &seed, bool requirePdf) {
+  const PtLight ls = sample_light_d(C, p, seed);
+  if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
+  if (!visible_d(C, p, n, ls)) return {0, 0, 0};
+  const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
+  double f = 0.0, bpdf = 0.0;
+  if (no > 0.0) {
+    bpdf = std::max(0.0, ni) / kPi;
+    if (ni > 0.0 && cosine >= 1e-7) f = 1.0 / kPi;
+  }
+  const double w = useMIS ? power_heuristic_d(ls.pdf, bpdf) : 1.0;
+  return to_rgb(C, L, scale(mul(mul(T, albedo), emission(C, L, C.in->light.emission)), f * cosine * w / ls.pdf));
+}
+
+void make_basis_d(D3 n, D3 &u, D3 &v) {
+  const D3 up = std::fabs(n.z) < 0.999 ? D3{0, 0, 1} : D3{1, 0, 0};
+  u = normalize(cross(up, n));
+  v = cross(n, u);
+}
+
+D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float jx_f, float jy_f) {
+  uint32_t seed = (y * C.p->width + x) ^ (si * 1999999973u);
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, seed);
+  const double jx = double(jx_f) + 0.5, jy = double(jy_f) + 0.5;
+  double u = ((x + jx) / C.p->width) * 2.0 - 1.0, v = ((y + jy) / C.p->height) * 2.0 - 1.0;
+  v = -v;
+  u *= C.aspect * C.fovScale;
+  v *= C.fovScale;
+  const D3 dir0 = normalize(C.fwd + C.right * u + C.up * v);
+  PtHit h;
+  const bool hit0 = pt_closest(C, C.cam, dir0, h);
+  seed = pcg_hash(seed ^ 0x27d4eb2fu);
+  if (!hit0) return {0, 0, 0};
+  vt_material m = pt_material(C, h.slot);
+  if (m.type == VT_MAT_EMISSIVE) return {m.emission[0], m.emission[1], m.emission[2]};
+  const int limit = std::max(0, (int)C.p->max_depth - 1);
+  const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode == 1u;
+  Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
+  D3 R{0, 0, 0};
+  if (nee) R = direct_d(C, L, h.pos, h.gn, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
+  int scattering = 0;
+  bool emissionOnly = false;
+  for (int bounce = 1;; ++bounce) {
+    if (scattering >= limit) {
+      if (nee || emissionOnly) break;
+      emissionOnly = true;
+    }
+    ++scattering;
+    rand_d(seed);
+    const double r1 = rand_d(seed), r2 = rand_d(seed);
+    const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
+    const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
+    D3 bu, bv;
+    make_basis_d(h.gn, bu, bv);
+    const D3 nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.gn * cos_th);
+    const double bpdf = std::max(0.0, dot(h.gn, nd)) / kPi;
+    if (!(bpdf > 0.0) || !(dot(nd, h.gn) > 0.0)) break;
+    T = mul(T, reflectance(C, m));
+    bool finite = true;
+    for (double t : T.v) finite = finite && std::isfinite(t);
+    if (!finite || smax(C, T) <= 0.0) break;
+    const D3 prev = h.pos;
+    const D3 o = ray_origin_d(h.pos, h.gn, nd);
+    if (!pt_closest(C, o, nd, h)) break;
+    m = pt_material(C, h.slot);
+    if (m.type == VT_MAT_EMISSIVE) {
+      const double lpdf = light_pdf_d(C, prev, h.pos);
+      const double w = !nee || lpdf <= 0.0 ? 1.0 : (mis ? power_heuristic_d(bpdf, lpdf) : 0.0);
+      R = R + to_rgb(C, L, scale(mul(T, emission(C, L, m.emission)), w));
+      break;
+    }
+    if (emissionOnly) break;
+    if (nee) R = R + direct_d(C, L, h.pos, h.gn, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
+    if (bounce > 3) {
+      const double survival = std::min(std::max(smax(C, T), 0.05), 0.95);
+      if (rand_d(seed) >= survival) break;
+      T = scale(T, 1.0 / survival);
+    }
+  }
+  if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
+  return R;
+}
+
+}  // namespace
+
+extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, uint32_t spp, double *out_rgb,
+                           int32_t threads) {
+  PtContext C;
+  C.in = in;
+  C.p = p;
+  C.bvh = vto_lbvh_build(in->faces, in->nfaces, in->verts, in->nverts, 2, 7, 2);
+  C.spectral = p->spectral != 0 && in->cmf_rgb != nullptr;
+  const D3 pos = d3(p->camera_pos), target = d3(p->camera_target), upv = d3(p->camera_up);
+  C.cam = pos;
+  C.fwd = normalize(target - pos);
+  C.right = normalize(cross(C.fwd, upv));
+  C.up = cross(C.right, C.fwd);
+  C.aspect = double(p->width) / p->height;
+  C.fovScale = std::tan(p->fov_deg * 0.5 * kPi / 180.0);
+  C.larea = std::sqrt(dot(cross(d3(in->light.su), d3(in->light.sv)), cross(d3(in->light.su), d3(in->light.sv))));
+  std::vector<float> jx(spp), jy(spp);
+  for (uint32_t k = 0; k < spp; ++k) {
+    const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
+    jx[k] = halton_f(n, 2) - 0.5f;
+    jy[k] = halton_f(n, 3) - 0.5f;
+  }
+  const uint32_t npix = p->width * p->height;
+  parallel_for(npix, threads, [&](uint32_t i) {
+    const uint32_t x = i % p->width, y = i / p->width;
+    double s[3] = {0, 0, 0};
+    for (uint32_t k = 0; k < spp; ++k) {
+      const D3 c = path_sample_d(C, x, y, p->first_sample + k, jx[k], jy[k]);
+      s[0] += c.x; s[1] += c.y; s[2] += c.z;
+    }
+    for (int c = 0; c < 3; ++c) out_rgb[3 * (size_t)i + c] = spp ? s[c] / spp : 0.0;
+  });
+  vto_bvh_free(C.bvh);
+}

@@ -72,6 +72,30 @@ void vto_brute_closest(const vt_face *faces, uint32_t nfaces, const vt_vertex *v
 void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t closest,
                      uint64_t *nodes_visited, uint64_t *tris_tested, int32_t threads);
 
+/* ---- path tracer (FP64 restatement of the MIS integrator) ------------------------------------ */
+/* shading_kernel (main.swift:7370-7914) in MIS mode with the PCG sampler, on a triangle scene whose
+ * faces' tags select material slots, the procedural quad light (main.swift:2957-2978, 3046-3050)
+ * and, when `spectral`, four hero wavelengths from the tables (main.swift:755-848, 945-959). All
+ * arithmetic in double; random numbers are the reference's exact 24-bit PCG draws. */
+typedef struct vto_pt_inputs {
+  const vt_face *faces;
+  uint32_t nfaces;
+  const vt_vertex *verts;
+  uint32_t nverts;
+  const vt_material *materials;
+  uint32_t nmat;
+  vt_quad_light light;
+  const float *cmf_rgb;   /* nbins x 3 (may be null for RGB transport) */
+  const float *illum;     /* nbins */
+  const float *icdf;      /* segments + 1 */
+  uint32_t nbins, segments;
+  float lambda_min;
+} vto_pt_inputs;
+
+/* Mean linear-sRGB radiance per pixel over `spp` frames starting at params->first_sample. */
+void vto_render(const vto_pt_inputs *in, const vt_frame_params *params, uint32_t spp, double *out_rgb,
+                int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -207,3 +207,68 @@ def brute_closest(faces, verts, rays, precision=32, nthreads=None):
     load().vto_brute_closest(f.ctypes.data, f.shape[0], v.ctypes.data, r.ctypes.data, r.shape[0],
                              out.ctypes.data, precision, nthreads or threads())
     return out
+
+
+# ---- path tracer -------------------------------------------------------------------------------
+class Material(C.Structure):
+    _fields_ = [("type", C.c_int32), ("albedo", C.c_float * 3), ("emission", C.c_float * 3), ("pad", C.c_float)]
+
+
+class QuadLight(C.Structure):
+    _fields_ = [("corner", C.c_float * 3), ("su", C.c_float * 3), ("sv", C.c_float * 3), ("normal", C.c_float * 3),
+                ("emission", C.c_float * 3), ("pad", C.c_float)]
+
+
+class FrameParams(C.Structure):
+    _fields_ = [("camera_pos", C.c_float * 3), ("fov_deg", C.c_float), ("camera_target", C.c_float * 3),
+                ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
+                ("spectral", C.c_uint32)]
+
+
+class PtInputs(C.Structure):
+    _fields_ = [("faces", C.c_void_p), ("nfaces", C.c_uint32), ("verts", C.c_void_p), ("nverts", C.c_uint32),
+                ("materials", C.c_void_p), ("nmat", C.c_uint32), ("light", QuadLight),
+                ("cmf_rgb", C.c_void_p), ("illum", C.c_void_p), ("icdf", C.c_void_p),
+                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float)]
+
+
+_SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
+
+
+def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
+           spectral=None, nthreads=None, mode=1):
+    """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames."""
+    lib = load()
+    if not hasattr(lib.vto_render, "_typed"):
+        lib.vto_render.restype, lib.vto_render.argtypes = _SIGS["vto_render"]
+        lib.vto_render._typed = True
+    f, v = _faces(faces), _verts(verts)
+    mats = (Material * len(materials))()
+    for i, m in enumerate(materials):
+        mats[i].type = int(m["type"])
+        mats[i].albedo[:] = [float(x) for x in m["albedo"]]
+        mats[i].emission[:] = [float(x) for x in m["emission"]]
+    q = QuadLight()
+    for k in ("corner", "su", "sv", "normal", "emission"):
+        getattr(q, k)[:] = [float(x) for x in light[k]]
+    inp = PtInputs(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0], C.cast(mats, C.c_void_p), len(materials), q,
+                   None, None, None, 0, 0, 0.0)
+    keep = []
+    if spectral is not None:
+        cmf = np.ascontiguousarray(spectral["cmf_rgb"], np.float32)
+        ill = np.ascontiguousarray(spectral["illum"], np.float32)
+        icdf = np.ascontiguousarray(spectral["icdf"], np.float32)
+        keep += [cmf, ill, icdf]
+        inp.cmf_rgb, inp.illum, inp.icdf = cmf.ctypes.data, ill.ctypes.data, icdf.ctypes.data
+        inp.nbins, inp.segments, inp.lambda_min = cmf.shape[0], icdf.shape[0] - 1, float(spectral["lambda_min"])
+    p = FrameParams()
+    p.camera_pos[:] = [float(x) for x in camera["pos"]]
+    p.camera_target[:] = [float(x) for x in camera["target"]]
+    p.camera_up[:] = [float(x) for x in camera["up"]]
+    p.fov_deg = float(camera["fov"])
+    p.max_depth, p.sampling_mode, p.width, p.height = max_depth, mode, width, height
+    p.first_sample, p.spectral = first_sample, 1 if spectral is not None else 0
+    out = np.empty(3 * width * height, np.float64)
+    lib.vto_render(C.byref(inp), C.byref(p), spp, out.ctypes.data, nthreads or threads())
+    return out.reshape(height, width, 3)

@@ -49,6 +49,7 @@ def expected_tris(faces, verts, order):
     out = np.zeros((len(order), 12), np.float32)
     out[:, 0:3], out[:, 4:7], out[:, 8:11] = p[f["a"]], p[f["b"]], p[f["c"]]
     out[:, 3] = order.view(np.float32)
+    out[:, 7] = f["tag"].view(np.float32)
     return out
 
 
