@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--profile", action="store_true", help="small run for ncu: no e2e, no CPU leg")
+    p.add_argument("--no-cornell", action="store_true", help="skip the integrator measurement")
+    p.add_argument("--reference-spp", type=int, default=65536, help="spp of the FP64 reference image")
     return p.parse_args()
 
 
@@ -173,12 +175,92 @@ def run_reference(a):
     return 0
 
 
+def rel_mse(img, ref) -> float:
+    """Relative MSE of luminance (scripts/compare_mitsuba.py:353-354): mean squared luminance error
+    over the squared mean luminance of the reference."""
+    w = np.array([0.2126, 0.7152, 0.0722])
+    li, lr = img @ w, ref @ w
+    return float(np.mean((li - lr) ** 2) / np.mean(lr) ** 2)
+
+
+def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
+    """Spectral Cornell box (256 x 256, 16 spp, depth 8): device time per 16-spp image, paths/s, and
+    the plain path tracer's time to relMSE 1e-3 against an FP64 reference of `reference_spp`."""
+    import torch
+
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes, spectral_tables
+
+    W = H = 256
+    spp, depth = 16, 8
+    faces, verts, mats, light, cam = scenes.cornell_box()
+    tables = spectral_tables.load()
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, light, tables)
+    cs = stream.cuda_stream
+    params = lambda first, n=spp: vt.make_params(cam, W, H, depth, first, True)
+    for k in range(2):
+        scene.render(params(1 + spp * k), spp, cs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(stream)
+    for k in range(reps):
+        scene.render(params(1 + spp * k), spp, cs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out = {"workload": "spectral Cornell box, 36 triangles, 256x256, 16 spp, depth 8, 4 hero wavelengths 380-780 nm, "
+                       "MIS, FP64 accumulation", "ms_per_image": ms, "paths_per_s": W * H * spp / (ms / 1e3),
+           "gpu_launches_per_image": 1}
+    # FP64 reference: reference_spp samples from independent sample indices.
+    ref_scene = vt.Scene(ctx, mesh, mats, light, tables)
+    chunk = 1024
+    t0 = time.perf_counter()
+    for k in range(a.reference_spp // chunk):
+        ref_scene.render(params(10_000_001 + chunk * k, chunk), chunk, cs)
+    ref, nref = ref_scene.readback()
+    ref_s = time.perf_counter() - t0
+    # Plain path tracing, progressively in 16-spp steps, until relMSE <= 1e-3 (device time of the
+    # renders only; the readback and error between steps are not timed).
+    scene.reset()
+    total_ms, done, err = 0.0, 0, None
+    while done < 16384:
+        e0.record(stream)
+        scene.render(params(1 + done, spp), spp, cs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        done += spp
+        img, _ = scene.readback()
+        err = rel_mse(img, ref)
+        if err <= 1e-3:
+            break
+    out["time_to_relmse_1e-3"] = {
+        "plain_pt_s": total_ms / 1e3 if err is not None and err <= 1e-3 else None, "spp": done, "relmse": err,
+        "reference_spp": nref, "reference_wall_s": ref_s,
+        "definition": "relMSE of luminance vs the FP64-accumulated reference (scripts/compare_mitsuba.py:353-354)",
+        "nrc": "not built (neural radiance cache is later work): the NRC arm of the metric is unmeasured"}
+    if cpu_leg:
+        from oracle import vt_oracle as O
+        t0 = time.perf_counter()
+        O.render(faces, verts, mats, light, cam, W, H, spp, max_depth=depth, spectral=tables)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": W * H * spp / t, "unit": "paths/s", "cores": O.threads(), "kind": "port",
+                               "sample": "FP64 oracle path tracer, the full 256x256x16 image (%.2f s)" % t}
+    scene.close()
+    ref_scene.close()
+    mesh.close()
+    return out
+
+
 # ---- our arm ----------------------------------------------------------------------------------
 def main():
     a = parse()
     if a.profile:
         a.no_e2e = True
         a.no_cpu_baseline = True
+        a.no_cornell = True
     if a.impl == "reference":
         return run_reference(a)
 
@@ -350,6 +432,12 @@ def main():
         cpu = {"value": n / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": "oracle fp32 traversal of the same LBVH, %d rays per set x 4 sets (%.1f s)" % (len(sets_cpu[0]), t)}
 
+    # The integrator (N = 1 only): the spectral Cornell box at 256 x 256, 16 spp, depth 8, and the
+    # plain path tracer's time to relMSE 1e-3 against a 65,536-spp FP64-accumulated reference.
+    cornell = None
+    if world == 1 and not a.no_cornell:
+        cornell = bench_cornell(a, ctx, dev, stream, cpu_leg=(rank == 0 and not a.no_cpu_baseline))
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
@@ -363,6 +451,7 @@ def main():
             "traversal_counts_per_ray": {n: [c[0] / sets[k][0].shape[0], c[1] / sets[k][0].shape[0]]
                                          for k, (n, c) in enumerate(counts.items())},
             "build": {"ms": info.build_ms, "sah_cost": info.sah_cost, "wide_nodes": info.wide_nodes, "depth": info.depth},
+            "cornell_pt": cornell,
         }
         print(json.dumps(line))
     if world > 1:

@@ -20,9 +20,10 @@
 // spectral_lagrange treats greys, main.swift:905-910) and grey emitters under the illuminant
 // (spectral_emission's white term, main.swift:945-959).
 //
-// Layout: one persistent thread per pixel runs all of the call's samples in order and adds their
-// FP64 sum to the pixel's accumulator, so the accumulation is deterministic. Traversal is the
-// 4-wide watertight traversal of traverse.cu with a per-thread local stack.
+// Layout: a grid-stride loop over (sample group, pixel) items; an item runs its group's samples of
+// one pixel in order and adds their FP64 sum to the pixel's accumulator (FP64 atomics when a call's
+// samples are split into several groups to fill the GPU). Traversal is the 4-wide watertight
+// traversal of traverse.cu with a per-thread local stack.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -401,21 +402,30 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   return R;
 }
 
-__global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A) {
+// Work item i = (sample group g, pixel p), pixel-major within a group so that a warp traces
+// neighbouring pixels; a group covers `per` consecutive samples of the call. Each item adds its
+// FP64 sum to the pixel with one atomic per channel (groups > 1) or a plain add (groups = 1).
+__global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t groups, uint32_t per) {
   int stack[kRenderStack];
   const uint32_t npix = A.W * A.H;
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+  const uint64_t items = (uint64_t)npix * groups;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < items; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = (uint32_t)(i % npix), g = (uint32_t)(i / npix);
     const uint32_t x = p % A.W, y = p / A.W;
+    const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
-    for (uint32_t k = 0; k < A.spp; ++k) {
+    for (uint32_t k = k0; k < k1; ++k) {
       const float3 c = path_sample(A, x, y, A.first + k, A.jitter[k], stack);
       sr += c.x;
       sg += c.y;
       sb += c.z;
     }
-    A.accum[3 * (size_t)p] += sr;
-    A.accum[3 * (size_t)p + 1] += sg;
-    A.accum[3 * (size_t)p + 2] += sb;
+    double *acc = A.accum + 3 * (size_t)p;
+    if (groups == 1) {
+      acc[0] += sr; acc[1] += sg; acc[2] += sb;
+    } else {
+      atomicAdd(acc, sr); atomicAdd(acc + 1, sg); atomicAdd(acc + 2, sb);
+    }
   }
 }
 
@@ -599,9 +609,15 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.mode = p->sampling_mode;
   A.jitter = scene->d_jitter;
   A.accum = scene->d_accum;
+  // Enough (pixel, sample group) items to fill the GPU about four times over.
   const uint32_t npix = p->width * p->height;
-  const uint32_t grid = std::min<uint32_t>((npix + kRenderBlock - 1) / kRenderBlock, (uint32_t)ctx->sm_count * 16u);
-  k_render<<<grid, kRenderBlock, 0, s>>>(A);
+  const uint64_t target = (uint64_t)ctx->sm_count * 2048u * 4u;
+  uint32_t groups = (uint32_t)std::min<uint64_t>(spp, std::max<uint64_t>(1, (target + npix - 1) / npix));
+  const uint32_t per = (spp + groups - 1) / groups;
+  groups = (spp + per - 1) / per;
+  const uint64_t items = (uint64_t)npix * groups;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((items + kRenderBlock - 1) / kRenderBlock, (uint64_t)ctx->sm_count * 32u);
+  k_render<<<grid, kRenderBlock, 0, s>>>(A, groups, per);
   VT_CUDA(ctx, cudaGetLastError());
   scene->samples += spp;
   return VT_OK;
