@@ -195,6 +195,11 @@ typedef struct vt_frame_params {
   uint32_t width, height;
   uint32_t first_sample;    /* sample index of the first frame (>= 1, Uniforms.sampleIndex) */
   uint32_t spectral;        /* 1 = four hero wavelengths, 0 = RGB transport */
+  uint32_t sampler;         /* 0 = PCG streams, 1 = Z++ sampler (Uniforms.indirectReuse bit 6) */
+  uint32_t z_temporal;      /* Z++ temporal model 0-3 (bits 7-8; the reference's default is 3) */
+  uint32_t first_frame;     /* accumulation frame of the first sample (Uniforms.frameIndex, >= 1);
+                               0 = continue the scene's accumulation */
+  uint32_t pad;
 } vt_frame_params;
 
 /* A renderable scene: the mesh, its material slots, the area light and (optionally) the spectral
@@ -214,6 +219,14 @@ vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene);
 /* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3)
  * and the number of samples accumulated. Synchronises. */
 vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t n, uint32_t *samples);
+
+/* Per pixel the first draws of one sampling event (vertex, stream) of the pixel's sampler: rand_f,
+ * rand_f2 and rand_f3, 6 floats per pixel into the HOST array `out` (width * height * 6). The
+ * role of the reference's z_frame test kernel (tests/Fix_zsampling.swift:58-66), for checking the
+ * sampler against a CPU restatement. sampler 0 = PCG, 1 = Z++ with temporal model z_temporal. */
+vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_t sampler, uint32_t z_temporal,
+                           uint32_t sample_index, uint32_t frame_index, uint32_t vertex, uint32_t stream,
+                           float *out);
 
 /* ---- allocation-free build --------------------------------------------------------------- */
 

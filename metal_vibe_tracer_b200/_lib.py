@@ -72,6 +72,7 @@ SIGNATURES = {
     "vt_render": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_accum_reset": (_I32, [_P, _P]),
     "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
+    "vt_sampler_frame": (_I32, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _P]),
 }
 NOALLOC_MAX_FACES = 32768
 

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <vector>
 
+#include "sampler.cuh"
 #include "trace_common.cuh"
 #include "vt_internal.cuh"
 
@@ -39,16 +40,6 @@ constexpr float kTwoPi = 6.28318530717958647692f;
 constexpr float kEps = 0.001f;            // ray_epsilon / ray_t_min of the procedural scenes
 constexpr int kRenderStack = 96;
 constexpr int kRenderBlock = 128;
-
-__device__ __forceinline__ uint32_t pcg_hash(uint32_t input) {
-  uint32_t state = input * 747796405u + 2891336453u;
-  uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
-  return (word >> 22u) ^ word;
-}
-__device__ __forceinline__ float rand_f(uint32_t &seed) {
-  seed = pcg_hash(seed);
-  return float(seed >> 8u) * (1.0f / 16777216.0f);
-}
 
 struct RenderArgs {
   const float4 *nodes, *tris;
@@ -66,6 +57,7 @@ struct RenderArgs {
   float aspect, fovScale;
   uint32_t W, H, maxDepth, first, spp;
   uint32_t mode;  // Uniforms.samplingMode: 1 MIS, 2 light sampling, 3 BSDF sampling
+  uint32_t zSampler, zModel, firstFrame;  // Z++ sampler on/off, its temporal model, frame of `first`
   const float2 *jitter;
   double *accum;
 };
@@ -178,10 +170,8 @@ struct Lanes {
   float w[4];
 };
 
-__device__ __forceinline__ Lanes make_lanes(const RenderArgs &A, uint32_t state) {
+__device__ __forceinline__ Lanes make_lanes(const RenderArgs &A, float u) {
   Lanes L;
-  const uint32_t h = pcg_hash(state ^ 0x5bd1e995u);
-  const float u = float(h >> 8u) * (1.0f / 16777216.0f);
   const float seg = float(A.segments);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -220,10 +210,11 @@ struct LightSample {
 };
 
 // Quad light sample (2 draws).
-__device__ __forceinline__ LightSample sample_light(const RenderArgs &A, float3 p, uint32_t &seed) {
+__device__ __forceinline__ LightSample sample_light(const RenderArgs &A, float3 p, Sampler &seed) {
   LightSample ls;
   ls.pdf = 0.0f;
-  const float u = rand_f(seed), v = rand_f(seed);
+  const float2 uv = rand_f2(seed);
+  const float u = uv.x, v = uv.y;
   const float3 lp = add(A.lc, add(mul(A.lsu, u), mul(A.lsv, v)));
   float3 dir = sub(lp, p);
   const float dist = sqrtf(dot3(dir, dir));
@@ -312,7 +303,7 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
 
 // NEE at a Lambert vertex: the contribution's rgb (2 draws).
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 wo,
-                                               float4 T, float4 albedo, bool useMIS, uint32_t &seed, int *stack,
+                                               float4 T, float4 albedo, bool useMIS, Sampler &seed, int *stack,
                                                bool requirePdf) {
   const LightSample ls = sample_light(A, p, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
@@ -332,10 +323,11 @@ __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes 
   return to_rgb(A, L, s);
 }
 
-__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, float2 jit, int *stack) {
-  uint32_t seed = (y * A.W + x) ^ (si * 1999999973u);
+__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
+                              int *stack) {
+  Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
   Lanes L;
-  if (A.spectral) L = make_lanes(A, seed);
+  if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
   // Camera ray (restir_temporal_kernel, main.swift:4874-4893).
   const float jx = jit.x + 0.5f, jy = jit.y + 0.5f;
   float u = ((float(x) + jx) / float(A.W)) * 2.0f - 1.0f;
@@ -346,7 +338,7 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   const float3 dir0 = normalize3(add(A.fwd, add(mul(A.right, u), mul(A.up, v))));
   Hit h;
   const bool hit0 = rt_closest(A, A.cam, dir0, kEps, __int_as_float(0x7f800000), h, stack);
-  seed = pcg_hash(seed ^ 0x27d4eb2fu);  // decorrelate_shading_seed
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   if (!hit0) return f3(0.0f, 0.0f, 0.0f);
   Surface S = surface_at(A, h, A.cam, dir0);
   vt_material m = material(A, S.slot);
@@ -355,7 +347,10 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   const bool nee = A.mode != 3u, mis = A.mode == 1u;
   float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
   float3 R = f3(0.0f, 0.0f, 0.0f);
-  if (nee) R = direct_light(A, L, S.pos, S.gn, mul(dir0, -1.0f), T, reflectance(A, m), mis && limit > 0, seed, stack, true);
+  if (nee) {
+    sampler_event(seed, 1u, kZNee);
+    R = direct_light(A, L, S.pos, S.gn, mul(dir0, -1.0f), T, reflectance(A, m), mis && limit > 0, seed, stack, true);
+  }
   float3 dir = dir0;
   int scattering = 0;
   bool emissionOnly = false;
@@ -366,10 +361,10 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
       emissionOnly = true;
     }
     ++scattering;
-    // sample_bsdf, Lambert: three draws, the direction from the last two.
-    rand_f(seed);
-    const float r1 = rand_f(seed), r2 = rand_f(seed);
-    const float3 nd = cosine_hemisphere(S.gn, r1, r2);
+    // sample_bsdf, Lambert: one 3D draw (three PCG draws), the direction from the last two.
+    sampler_event(seed, (uint32_t)bounce, kZBsdf);
+    const float3 r = rand_f3(seed);
+    const float3 nd = cosine_hemisphere(S.gn, r.y, r.z);
     const float bpdf = fmaxf(0.0f, dot3(S.gn, nd)) * kInvPi;
     if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
     T = mul4(T, reflectance(A, m));
@@ -389,11 +384,14 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
       break;
     }
     if (emissionOnly) break;
-    if (nee)
+    if (nee) {
+      sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
       R = add(R, direct_light(A, L, S.pos, S.gn, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit, seed,
                               stack, false));
+    }
     if (bounce > 3) {
       const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+      sampler_event(seed, (uint32_t)bounce + 1u, kZRoulette);
       if (rand_f(seed) >= survival) break;
       T = scale4(T, 1.0f / survival);
     }
@@ -415,7 +413,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t 
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
-      const float3 c = path_sample(A, x, y, A.first + k, A.jitter[k], stack);
+      const float3 c = path_sample(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack);
       sr += c.x;
       sg += c.y;
       sb += c.z;
@@ -533,6 +531,7 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
     return vt_fail(ctx, VT_ERR_INVALID, "sampling_mode must be 1 (MIS), 2 (light) or 3 (BSDF)");
   if (p->spectral && !scene->d_spec) return vt_fail(ctx, VT_ERR_INVALID, "spectral transport needs spectral tables");
   if (p->first_sample == 0) return vt_fail(ctx, VT_ERR_INVALID, "first_sample starts at 1");
+  if (p->sampler > 1 || p->z_temporal > 3) return vt_fail(ctx, VT_ERR_INVALID, "sampler must be 0 (PCG) or 1 (Z++), z_temporal 0-3");
   const vt_mesh *mesh = scene->mesh;
   if (mesh->nfaces > 0 && mesh->depth > 32) return vt_fail(ctx, VT_ERR_LIMIT, "BVH deeper than the render stack");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -607,6 +606,9 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.first = p->first_sample;
   A.spp = spp;
   A.mode = p->sampling_mode;
+  A.zSampler = p->sampler;
+  A.zModel = p->z_temporal;
+  A.firstFrame = p->first_frame ? p->first_frame : scene->samples + 1u;
   A.jitter = scene->d_jitter;
   A.accum = scene->d_accum;
   // Enough (pixel, sample group) items to fill the GPU about four times over.
@@ -637,3 +639,40 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
 }
 
 }  // extern "C"
+
+// ---- sampler draws (diagnostic entry point) -----------------------------------------------------
+namespace {
+__global__ void k_sampler_frame(uint32_t width, uint32_t height, uint32_t z, uint32_t model, uint32_t sampleIndex,
+                                uint32_t frameIndex, uint32_t vertex, uint32_t stream, float *out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= width * height) return;
+  const uint32_t x = i % width, y = i / width;
+  Sampler s = pixel_sampler(x, y, width, sampleIndex, z != 0u, model, frameIndex);
+  sampler_event(s, vertex, stream);
+  const float a = rand_f(s);
+  const float2 b = rand_f2(s);
+  const float3 c = rand_f3(s);
+  float *o = out + 6 * (size_t)i;
+  o[0] = a; o[1] = b.x; o[2] = b.y; o[3] = c.x; o[4] = c.y; o[5] = c.z;
+}
+}  // namespace
+
+extern "C" vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_t sampler,
+                                      uint32_t z_temporal, uint32_t sample_index, uint32_t frame_index,
+                                      uint32_t vertex, uint32_t stream, float *out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!out || width == 0 || height == 0 || (uint64_t)width * height > (1u << 24) || sampler > 1 || z_temporal > 3)
+    return vt_fail(ctx, VT_ERR_INVALID, "bad sampler_frame arguments");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t n = (size_t)width * height;
+  float *d = nullptr;
+  VT_CUDA(ctx, cudaMalloc(&d, 6 * n * sizeof(float)));
+  k_sampler_frame<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(width, height, sampler, z_temporal, sample_index,
+                                                                          frame_index, vertex, stream, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, 6 * n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return vt_cuda_fail(ctx, e, "vt_sampler_frame");
+  return VT_OK;
+}

@@ -34,10 +34,11 @@ class FrameParams(C.Structure):
     _fields_ = [("camera_pos", C.c_float * 3), ("fov_deg", C.c_float), ("camera_target", C.c_float * 3),
                 ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
-                ("spectral", C.c_uint32)]
+                ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
+                ("first_frame", C.c_uint32), ("pad", C.c_uint32)]
 
 
-assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 64
+assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 80
 
 
 def make_materials(materials) -> C.Array:
@@ -56,7 +57,8 @@ def make_light(light) -> QuadLight:
     return q
 
 
-def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1) -> FrameParams:
+def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1, sampler=0, z_temporal=3,
+                first_frame=0) -> FrameParams:
     p = FrameParams()
     p.camera_pos[:] = [float(x) for x in camera["pos"]]
     p.camera_target[:] = [float(x) for x in camera["target"]]
@@ -67,6 +69,9 @@ def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=Tru
     p.width, p.height = int(width), int(height)
     p.first_sample = int(first_sample)
     p.spectral = 1 if spectral else 0
+    p.sampler = int(sampler)          # 0 PCG, 1 Z++
+    p.z_temporal = int(z_temporal)    # Z++ temporal model (the reference's default: 3, reshuffled)
+    p.first_frame = int(first_frame)  # 0: continue the scene's accumulation
     return p
 
 
@@ -121,3 +126,13 @@ class Scene:
             self.close()
         except Exception:
             pass
+
+
+def sampler_frame(ctx: Context, width: int, height: int, z: bool, model: int, sample_index: int, frame_index: int,
+                  vertex: int, stream: int) -> np.ndarray:
+    """(height, width, 6) float32: rand_f, rand_f2, rand_f3 of one sampling event per pixel, drawn on
+    the device (the sampler's diagnostic entry point)."""
+    out = np.empty((height, width, 6), np.float32)
+    _check(ctx.handle, _lib.load().vt_sampler_frame(ctx.handle, width, height, 1 if z else 0, model, sample_index,
+                                                    frame_index, vertex, stream, out.ctypes.data), "vt_sampler_frame")
+    return out

@@ -1043,6 +1043,180 @@ void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t c
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------
+// Z++ sampler (main.swift:122-305, 497-515), restated: per-pixel keys from a shuffled Morton code
+// and a temporal index, sampling events of 32 dimensions, van der Corput / Sobol' / O2m3
+// constituents under Owen scrambling, frame offsets from the pixel's own sequence. Integer
+// arithmetic throughout: every draw equals the GPU's bit for bit.
+namespace {
+
+inline uint32_t rev32(uint32_t v) {
+  v = ((v >> 1) & 0x55555555u) | ((v & 0x55555555u) << 1);
+  v = ((v >> 2) & 0x33333333u) | ((v & 0x33333333u) << 2);
+  v = ((v >> 4) & 0x0F0F0F0Fu) | ((v & 0x0F0F0F0Fu) << 4);
+  v = ((v >> 8) & 0x00FF00FFu) | ((v & 0x00FF00FFu) << 8);
+  return (v >> 16) | (v << 16);
+}
+inline uint32_t zmix(uint32_t v) {
+  v ^= v >> 16; v *= 0x7feb352du; v ^= v >> 15; v *= 0x846ca68bu; v ^= v >> 16;
+  return v;
+}
+const uint64_t kZPerm = 0x6c9c78d8b4e4ull;
+uint32_t zshuffle(uint32_t index, uint32_t dimension) {
+  const uint32_t seed = zmix(dimension * 0x9e3779b9u + 0x632be5abu);
+  uint32_t result = index & ~((1u << 24) - 1u);
+  for (int d = 11; d >= 0; --d) {
+    const uint32_t shift = 2u * d, digit = (index >> shift) & 3u;
+    const uint32_t h = zmix((index >> (shift + 2u)) ^ seed);
+    const uint32_t sigma = ((h >> 16) * 6u) >> 16;
+    const uint32_t image = (uint32_t)(kZPerm >> (8u * sigma + 2u * digit)) & 3u;
+    result |= (image ^ (h & 3u)) << shift;
+  }
+  return result;
+}
+uint32_t zowen(uint32_t v, uint32_t seed) {
+  v = rev32(v);
+  v ^= v * 0x3d20adeau;
+  v += seed;
+  v *= (seed >> 16) | 1u;
+  v ^= v * 0x05526c56u;
+  v ^= v * 0x53a22864u;
+  return rev32(v);
+}
+uint32_t zowen_seed(uint32_t dimension, uint32_t axis) {
+  const uint32_t h = (dimension ^ (axis << 24)) * 0x9e3779b9u;
+  return (h ^ (h >> 16)) * 0x85ebca6bu;
+}
+uint32_t zsobol1(uint32_t i) {
+  i ^= (i & 0xAAAAAAAAu) >> 1; i ^= (i & 0xCCCCCCCCu) >> 2; i ^= (i & 0xF0F0F0F0u) >> 4;
+  i ^= (i & 0xFF00FF00u) >> 8; i ^= (i & 0xFFFF0000u) >> 16;
+  return rev32(i);
+}
+uint32_t zo2m3x(uint32_t V) {
+  V ^= ((V << 2) & 0xF3CF3CF3u) ^ ((V << 3) & 0x41041041u);
+  V ^= (V << 4) & 0x3F03F03Fu;
+  V ^= (V << 8) & 0x0FFF000Fu;
+  V ^= (V << 16) & 0x00FFFFFFu;
+  return V;
+}
+uint32_t zo2m3y(uint32_t V) { return zo2m3x(((V >> 1) & 0x45145145u) ^ (V & 0xB5EB5EB5u) ^ ((V << 1) & 0x8A28A28Au)); }
+uint32_t zo2m3z(uint32_t V) { return zo2m3x(((V >> 1) & 0x45145145u) ^ (V & 0x7AD7AD7Au) ^ ((V << 1) & 0x8A28A28Au)); }
+inline double zfloat(uint32_t v) { return double(v >> 8) * (1.0 / 16777216.0); }
+uint32_t zmorton(uint32_t x, uint32_t y) {
+  auto spread = [](uint32_t v) {
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu; v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u; v = (v | (v << 1)) & 0x55555555u;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1);
+}
+
+struct ZSampler {
+  uint32_t state = 0, key = 0, dimension = 0, sub = 0, subBits = 0;
+  bool z = false;
+
+  static ZSampler pixel(uint32_t x, uint32_t y, uint32_t width, uint32_t sampleIndex, bool z, uint32_t model,
+                        uint32_t frameIndex) {
+    ZSampler s;
+    s.state = (y * width + x) ^ (sampleIndex * 1999999973u);
+    s.z = z;
+    if (z) {
+      const uint32_t j = std::max(frameIndex, 1u) - 1u, s0 = sampleIndex - j;
+      uint32_t t = model == 1u || model == 2u ? s0 ^ ((s0 & 0xAAAAAAAAu) << 1) : model == 3u ? zmix(s0 ^ 0x2c1b3c6du) : s0;
+      uint32_t k = zshuffle(zmorton(x, y), 0xffffffffu);
+      if (model == 2u) k ^= k << 2;
+      if ((j >> 14) != 0u) t ^= zmix(j >> 14);
+      s.key = ((k ^ t) << 14) | (j & 0x3FFFu);
+    }
+    return s;
+  }
+  uint32_t code() const { return key >> 14; }
+  uint32_t frame() const { return ((key & 0x3FFFu) << subBits) | sub; }
+  uint32_t index(uint32_t d) const { return zowen(code(), zowen_seed(d, 3u)); }
+  uint32_t next_dimension() { return dimension++ | ((code() >> 12) << 17); }
+  static uint32_t frame_index(uint32_t J, uint32_t d) {
+    const uint32_t seed = zowen_seed(d, 4u);
+    return zowen(J, seed) ^ zowen(0u, seed);
+  }
+  uint32_t frame_offset(uint32_t v, uint32_t d, uint32_t axis) const {
+    const uint32_t seed = zowen_seed(d, axis) ^ zmix(code() ^ 0x68e31da4u);
+    return ((zowen(v, seed) ^ zowen(0u, seed)) & 0x3FFFFFFFu) | (v & 0xC0000000u);
+  }
+  double pcg() { state = pcg_hash(state); return double(state >> 8u) * (1.0 / 16777216.0); }
+  double f1() {
+    if (!z) return pcg();
+    const uint32_t d = next_dimension(), J = frame();
+    uint32_t x = zowen(rev32(index(d)), zowen_seed(d, 0u));
+    if (J) x ^= frame_offset(rev32(frame_index(J, d)), d, 0u);
+    return zfloat(x);
+  }
+  void f2(double &a, double &b) {
+    if (!z) { a = pcg(); b = pcg(); return; }
+    const uint32_t d = next_dimension(), i = index(d), J = frame();
+    uint32_t x = zowen(rev32(i), zowen_seed(d, 0u)), y = zowen(zsobol1(i), zowen_seed(d, 1u));
+    if (J) {
+      const uint32_t k = frame_index(J, d);
+      x ^= frame_offset(rev32(k), d, 0u);
+      y ^= frame_offset(zsobol1(k), d, 1u);
+    }
+    a = zfloat(x); b = zfloat(y);
+  }
+  void f3(double &a, double &b, double &c) {
+    if (!z) { a = pcg(); b = pcg(); c = pcg(); return; }
+    const uint32_t d = next_dimension(), V = rev32(index(d)), J = frame();
+    uint32_t x = zowen(zo2m3x(V), zowen_seed(d, 0u)), y = zowen(zo2m3y(V), zowen_seed(d, 1u)), w = zowen(zo2m3z(V), zowen_seed(d, 2u));
+    if (J) {
+      const uint32_t W = rev32(frame_index(J, d));
+      x ^= frame_offset(zo2m3x(W), d, 0u);
+      y ^= frame_offset(zo2m3y(W), d, 1u);
+      w ^= frame_offset(zo2m3z(W), d, 2u);
+    }
+    a = zfloat(x); b = zfloat(y); c = zfloat(w);
+  }
+  void event(uint32_t vertex, uint32_t stream) { dimension = (vertex * 16u + stream) * 32u; sub = 0u; subBits = 0u; }
+  // wavelength_numbers: from a copy.
+  double wavelength_u() const {
+    if (z) { ZSampler c = *this; c.event(0u, 12u); return c.f1(); }
+    const uint32_t h = pcg_hash(state ^ 0x5bd1e995u);
+    return double(h >> 8u) * (1.0 / 16777216.0);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+void vto_z_sequences(uint32_t seed, uint32_t n, uint32_t *o2m3, uint32_t *sobol) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t V = rev32(i);
+    uint32_t p[3] = {zo2m3x(V), zo2m3y(V), zo2m3z(V)}, q[2] = {V, zsobol1(i)};
+    if (seed) {
+      for (int a = 0; a < 3; ++a) p[a] = zowen(p[a], zowen_seed(seed, a));
+      for (int a = 0; a < 2; ++a) q[a] = zowen(q[a], zowen_seed(seed, a));
+    }
+    for (int a = 0; a < 3; ++a) o2m3[3 * i + a] = p[a];
+    for (int a = 0; a < 2; ++a) sobol[2 * i + a] = q[a];
+  }
+}
+void vto_z_shuffles(uint32_t base, uint32_t dimension, uint32_t n, uint32_t *out) {
+  for (uint32_t i = 0; i < n; ++i) out[i] = zshuffle(base + i, dimension);
+}
+// Per pixel: rand_f, rand_f2 and rand_f3 of one sampling event (vertex, stream).
+void vto_sampler_frame(uint32_t width, uint32_t height, int32_t z, uint32_t model, uint32_t sampleIndex,
+                       uint32_t frameIndex, uint32_t vertex, uint32_t stream, float *out) {
+  for (uint32_t y = 0; y < height; ++y)
+    for (uint32_t x = 0; x < width; ++x) {
+      ZSampler s = ZSampler::pixel(x, y, width, sampleIndex, z != 0, model, frameIndex);
+      s.event(vertex, stream);
+      double v[6];
+      v[0] = s.f1();
+      s.f2(v[1], v[2]);
+      s.f3(v[3], v[4], v[5]);
+      for (int k = 0; k < 6; ++k) out[6 * ((size_t)y * width + x) + k] = (float)v[k];
+    }
+}
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
 // Path tracer: FP64 restatement of the MIS integrator (shading_kernel, main.swift:7370-7914, with
 // the primary hit of restir_temporal_kernel, main.swift:4842-4893), PCG sampler. The stream
 // consumption order is the reference's: wavelength numbers from a hashed copy
@@ -1064,10 +1238,6 @@ inline D3 d3(const float *v) { return {v[0], v[1], v[2]}; }
 const double kPi = 3.14159265358979323846;
 const double kEpsPt = 0.001;  // ray_epsilon / ray_t_min of the procedural scenes
 
-inline double rand_d(uint32_t &seed) {
-  seed = pcg_hash(seed);
-  return double(seed >> 8u) * (1.0 / 16777216.0);
-}
 
 // frameJitter (main.swift:8773-8785) in float, as the host computes it.
 float halton_f(uint32_t index, uint32_t base) {
@@ -1094,10 +1264,8 @@ struct PtContext {
 
 struct PtLanes { int bin[4]; double w[4]; };
 
-PtLanes make_lanes(const PtContext &C, uint32_t state) {
+PtLanes make_lanes(const PtContext &C, double u) {
   PtLanes L;
-  const uint32_t h = pcg_hash(state ^ 0x5bd1e995u);
-  const double u = double(h >> 8u) * (1.0 / 16777216.0);
   const uint32_t seg = C.in->segments;
   for (int k = 0; k < 4; ++k) {
     const double x = (u + k) * 0.25 * seg;
@@ -1186,10 +1354,11 @@ double power_heuristic_d(double pf, double pg) {
 
 struct PtLight { D3 pos, wi; double dist, pdf; };
 
-PtLight sample_light_d(const PtContext &C, D3 p, uint32_t &seed) {
+PtLight sample_light_d(const PtContext &C, D3 p, ZSampler &seed) {
   PtLight ls{};
   const vt_quad_light &l = C.in->light;
-  const double u = rand_d(seed), v = rand_d(seed);
+  double u, v;
+  seed.f2(u, v);
   const D3 lp = d3(l.corner) + d3(l.su) * u + d3(l.sv) * v;
   D3 dir = lp - p;
   const double dist = std::sqrt(dot(dir, dir));
@@ -1217,7 +1386,7 @@ bool visible_d(const PtContext &C, D3 p, D3 gn, const PtLight &ls) {
 }
 
 D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 wo, const Spec4 &T, const Spec4 &albedo,
-            bool useMIS, uint32_t &seed, bool requirePdf) {
+            bool useMIS, ZSampler &seed, bool requirePdf) {
   const PtLight ls = sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
   if (!visible_d(C, p, n, ls)) return {0, 0, 0};
@@ -1237,10 +1406,10 @@ void make_basis_d(D3 n, D3 &u, D3 &v) {
   v = cross(n, u);
 }
 
-D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float jx_f, float jy_f) {
-  uint32_t seed = (y * C.p->width + x) ^ (si * 1999999973u);
+D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx_f, float jy_f) {
+  ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
   PtLanes L{};
-  if (C.spectral) L = make_lanes(C, seed);
+  if (C.spectral) L = make_lanes(C, seed.wavelength_u());
   const double jx = double(jx_f) + 0.5, jy = double(jy_f) + 0.5;
   double u = ((x + jx) / C.p->width) * 2.0 - 1.0, v = ((y + jy) / C.p->height) * 2.0 - 1.0;
   v = -v;
@@ -1249,7 +1418,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float 
   const D3 dir0 = normalize(C.fwd + C.right * u + C.up * v);
   PtHit h;
   const bool hit0 = pt_closest(C, C.cam, dir0, h);
-  seed = pcg_hash(seed ^ 0x27d4eb2fu);
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
   if (!hit0) return {0, 0, 0};
   vt_material m = pt_material(C, h.slot);
   if (m.type == VT_MAT_EMISSIVE) return {m.emission[0], m.emission[1], m.emission[2]};
@@ -1257,7 +1426,10 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float 
   const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode == 1u;
   Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
   D3 R{0, 0, 0};
-  if (nee) R = direct_d(C, L, h.pos, h.gn, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
+  if (nee) {
+    seed.event(1u, 1u);
+    R = direct_d(C, L, h.pos, h.gn, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
+  }
   int scattering = 0;
   bool emissionOnly = false;
   for (int bounce = 1;; ++bounce) {
@@ -1266,8 +1438,9 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float 
       emissionOnly = true;
     }
     ++scattering;
-    rand_d(seed);
-    const double r1 = rand_d(seed), r2 = rand_d(seed);
+    seed.event((uint32_t)bounce, 0u);
+    double r0, r1, r2;
+    seed.f3(r0, r1, r2);
     const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
     const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
     D3 bu, bv;
@@ -1290,10 +1463,14 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, float 
       break;
     }
     if (emissionOnly) break;
-    if (nee) R = R + direct_d(C, L, h.pos, h.gn, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
+    if (nee) {
+      seed.event((uint32_t)bounce + 1u, 1u);
+      R = R + direct_d(C, L, h.pos, h.gn, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
+    }
     if (bounce > 3) {
       const double survival = std::min(std::max(smax(C, T), 0.05), 0.95);
-      if (rand_d(seed) >= survival) break;
+      seed.event((uint32_t)bounce + 1u, 2u);
+      if (seed.f1() >= survival) break;
       T = scale(T, 1.0 / survival);
     }
   }
@@ -1329,7 +1506,7 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
     const uint32_t x = i % p->width, y = i / p->width;
     double s[3] = {0, 0, 0};
     for (uint32_t k = 0; k < spp; ++k) {
-      const D3 c = path_sample_d(C, x, y, p->first_sample + k, jx[k], jy[k]);
+      const D3 c = path_sample_d(C, x, y, p->first_sample + k, std::max(1u, p->first_frame) + k, jx[k], jy[k]);
       s[0] += c.x; s[1] += c.y; s[2] += c.z;
     }
     for (int c = 0; c < 3; ++c) out_rgb[3 * (size_t)i + c] = spp ? s[c] / spp : 0.0;

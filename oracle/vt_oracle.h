@@ -92,7 +92,16 @@ typedef struct vto_pt_inputs {
   float lambda_min;
 } vto_pt_inputs;
 
-/* Mean linear-sRGB radiance per pixel over `spp` frames starting at params->first_sample. */
+/* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences
+ * (Owen-scrambled under `seed` unless 0), `n` quadrant shuffles of base + i, and per pixel the
+ * rand_f, rand_f2, rand_f3 draws (6 floats) of one sampling event. */
+void vto_z_sequences(uint32_t seed, uint32_t n, uint32_t *o2m3, uint32_t *sobol);
+void vto_z_shuffles(uint32_t base, uint32_t dimension, uint32_t n, uint32_t *out);
+void vto_sampler_frame(uint32_t width, uint32_t height, int32_t z, uint32_t model, uint32_t sampleIndex,
+                       uint32_t frameIndex, uint32_t vertex, uint32_t stream, float *out);
+
+/* Mean linear-sRGB radiance per pixel over `spp` frames starting at params->first_sample
+ * (accumulation frames from max(1, params->first_frame)). */
 void vto_render(const vto_pt_inputs *in, const vt_frame_params *params, uint32_t spp, double *out_rgb,
                 int32_t threads);
 

@@ -223,7 +223,8 @@ class FrameParams(C.Structure):
     _fields_ = [("camera_pos", C.c_float * 3), ("fov_deg", C.c_float), ("camera_target", C.c_float * 3),
                 ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
-                ("spectral", C.c_uint32)]
+                ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
+                ("first_frame", C.c_uint32), ("pad", C.c_uint32)]
 
 
 class PtInputs(C.Structure):
@@ -237,7 +238,7 @@ _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32,
 
 
 def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
-           spectral=None, nthreads=None, mode=1):
+           spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1):
     """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames."""
     lib = load()
     if not hasattr(lib.vto_render, "_typed"):
@@ -269,6 +270,39 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
     p.fov_deg = float(camera["fov"])
     p.max_depth, p.sampling_mode, p.width, p.height = max_depth, mode, width, height
     p.first_sample, p.spectral = first_sample, 1 if spectral is not None else 0
+    p.sampler, p.z_temporal, p.first_frame = sampler, z_temporal, first_frame
     out = np.empty(3 * width * height, np.float64)
     lib.vto_render(C.byref(inp), C.byref(p), spp, out.ctypes.data, nthreads or threads())
     return out.reshape(height, width, 3)
+
+
+_SIGS["vto_z_sequences"] = (None, [_U32, _U32, _P, _P])
+_SIGS["vto_z_shuffles"] = (None, [_U32, _U32, _U32, _P])
+_SIGS["vto_sampler_frame"] = (None, [_U32, _U32, _I32, _U32, _U32, _U32, _U32, _U32, _P])
+
+
+def _fn(name):
+    fn = getattr(load(), name)
+    fn.restype, fn.argtypes = _SIGS[name]
+    return fn
+
+
+def z_sequences(seed: int, n: int):
+    """(O2m3 points (n, 3) uint32, Sobol' points (n, 2) uint32) as 0.32 fixed point."""
+    o, q = np.empty((n, 3), np.uint32), np.empty((n, 2), np.uint32)
+    _fn("vto_z_sequences")(seed, n, o.ctypes.data, q.ctypes.data)
+    return o, q
+
+
+def z_shuffles(base: int, dimension: int, n: int):
+    out = np.empty(n, np.uint32)
+    _fn("vto_z_shuffles")(base & 0xFFFFFFFF, dimension & 0xFFFFFFFF, n, out.ctypes.data)
+    return out
+
+
+def sampler_frame(width, height, z, model, sample_index, frame_index, vertex, stream):
+    """(height, width, 6): rand_f, rand_f2 (2), rand_f3 (3) of one event per pixel."""
+    out = np.empty((height, width, 6), np.float32)
+    _fn("vto_sampler_frame")(width, height, 1 if z else 0, model, sample_index, frame_index, vertex, stream,
+                             out.ctypes.data)
+    return out

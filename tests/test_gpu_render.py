@@ -97,3 +97,20 @@ def test_render_rejects_unsupported_input(ctx, cornell):
     with pytest.raises(vt.MaterialLibraryError, match="spectral tables"):
         scene.render(vt.make_params(cam, 8, 8, 8, 1, True), 1)
     scene.close()
+
+
+@pytest.mark.parametrize("model", [0, 3])
+def test_cornell_z_sampler_matches_oracle(ctx, oracle, cornell, model):
+    faces, verts, mats, light, cam, mesh = cornell
+    tables = spectral_tables.load()
+    scene = vt.Scene(ctx, mesh, mats, light, tables)
+    scene.render(vt.make_params(cam, 128, 128, 8, 1, True, sampler=1, z_temporal=model), 16)
+    gpu, n = scene.readback()
+    scene.close()
+    ref = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, spectral=tables, sampler=1, z_temporal=model)
+    assert np.all(np.abs(gpu.reshape(-1, 3).mean(0) / ref.reshape(-1, 3).mean(0) - 1) < MEAN_REL)
+    same = np.all(np.abs(gpu - ref) <= 1e-4 * np.maximum(np.abs(ref), 1e-3), axis=-1)
+    assert same.mean() > 0.9, same.mean()
+    # Z++ and PCG estimate the same image.
+    pcg = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, spectral=tables)
+    assert abs(gpu.mean() / pcg.mean() - 1) < 0.02
