@@ -93,7 +93,7 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
     const Sorted4 s = sort_children(nd, mask, nearT);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      if (j >= s.m || s.child[j] > 0 || s.key[j] > closest) continue;
+      if (j >= s.m || s.child[j] > 0 || beyond(s.key[j], closest)) continue;
       const int first = -s.child[j] - 1;
       for (int q = 0; q < s.count[j]; ++q) {
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
@@ -105,7 +105,7 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
     }
 #pragma unroll
     for (int j = 3; j >= 0; --j)
-      if (j < s.m && s.child[j] > 0 && s.key[j] <= closest && top < kRenderStack) stack[top++] = s.child[j];
+      if (j < s.m && s.child[j] > 0 && !beyond(s.key[j], closest) && top < kRenderStack) stack[top++] = s.child[j];
   }
   h.t = closest;
   h.pos = best;

@@ -15,12 +15,31 @@ struct Node4 {
   int4 child, count;
 };
 
+#ifndef VT_NODE_LD256
+#define VT_NODE_LD256 1
+#endif
+// A node is fetched through the read-only path as four 32-byte vector loads (sm_100 ld.global.v8;
+// nodes are 128-byte records in a 256-byte aligned buffer): half the load instructions, and so half
+// the L1 wavefronts, of eight 16-byte loads when the lanes of a warp fetch different nodes.
+__device__ __forceinline__ void ld256(const float4 *p, float4 &a, float4 &b) {
+#if VT_NODE_LD256
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+               : "l"(p));
+#else
+  a = __ldg(p);
+  b = __ldg(p + 1);
+#endif
+}
 __device__ __forceinline__ void load_node(const float4 *__restrict__ nodes, int i, Node4 &n) {
   const float4 *p = nodes + 8 * (size_t)i;
-  n.lox = __ldg(p + 0); n.loy = __ldg(p + 1); n.loz = __ldg(p + 2);
-  n.hix = __ldg(p + 3); n.hiy = __ldg(p + 4); n.hiz = __ldg(p + 5);
-  n.child = __ldg(reinterpret_cast<const int4 *>(p + 6));
-  n.count = __ldg(reinterpret_cast<const int4 *>(p + 7));
+  float4 c, d;
+  ld256(p + 0, n.lox, n.loy);
+  ld256(p + 2, n.loz, n.hix);
+  ld256(p + 4, n.hiy, n.hiz);
+  ld256(p + 6, c, d);
+  n.child = make_int4(__float_as_int(c.x), __float_as_int(c.y), __float_as_int(c.z), __float_as_int(c.w));
+  n.count = make_int4(__float_as_int(d.x), __float_as_int(d.y), __float_as_int(d.z), __float_as_int(d.w));
 }
 
 __device__ __forceinline__ float f4(const float4 &v, int k) {
@@ -89,11 +108,18 @@ __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b,
 }
 
 // Conservative slab ray (wide_ray, main.swift:1758-1763): origins shifted by the per-ray bound
-// e = 2^-23 (max|o| + rootMax) so traversal never culls a triangle the edge test would hit.
+// e = 2^-23 (max|o| + rootMax) so traversal never culls a triangle the edge test would hit. An axis
+// the ray runs parallel to (|d| < 1e-8) gets the inverse +-1e30 instead of the reference's separate
+// inside-slab test: the slab distances are then -huge/+huge inside the shifted slab and cull outside
+// it (the same decisions except where the origin lies exactly on a shifted face, where this form
+// keeps the child), so the per-child test needs no parallel-axis branches.
 struct SlabRay {
   float lowx, lowy, lowz, highx, highy, highz, invx, invy, invz;
-  bool px, py, pz;
 };
+
+__device__ __forceinline__ float slab_inverse(float d) {
+  return fabsf(d) < 1e-8f ? copysignf(1e30f, d) : __fdiv_rn(1.0f, d);
+}
 
 __device__ __forceinline__ SlabRay make_slab(float ox, float oy, float oz, float dx, float dy, float dz,
                                              float rootMax) {
@@ -103,10 +129,9 @@ __device__ __forceinline__ SlabRay make_slab(float ox, float oy, float oz, float
   float e = __fmul_rn(1.1920929e-6f, __fadd_rn(om, rootMax));
   s.lowx = __fadd_rn(ox, e); s.lowy = __fadd_rn(oy, e); s.lowz = __fadd_rn(oz, e);
   s.highx = __fsub_rn(ox, e); s.highy = __fsub_rn(oy, e); s.highz = __fsub_rn(oz, e);
-  s.px = fabsf(dx) < 1e-8f; s.py = fabsf(dy) < 1e-8f; s.pz = fabsf(dz) < 1e-8f;
-  s.invx = __fdiv_rn(1.0f, s.px ? 1.0f : dx);
-  s.invy = __fdiv_rn(1.0f, s.py ? 1.0f : dy);
-  s.invz = __fdiv_rn(1.0f, s.pz ? 1.0f : dz);
+  s.invx = slab_inverse(dx);
+  s.invy = slab_inverse(dy);
+  s.invz = slab_inverse(dz);
   return s;
 }
 
@@ -116,56 +141,65 @@ __device__ __forceinline__ int node_hits(const Node4 &n, const SlabRay &w, float
   int mask = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    float ax = __fmul_rn(__fsub_rn(f4(n.lox, k), w.lowx), w.invx), bx = __fmul_rn(__fsub_rn(f4(n.hix, k), w.highx), w.invx);
-    float ay = __fmul_rn(__fsub_rn(f4(n.loy, k), w.lowy), w.invy), by = __fmul_rn(__fsub_rn(f4(n.hiy, k), w.highy), w.invy);
-    float az = __fmul_rn(__fsub_rn(f4(n.loz, k), w.lowz), w.invz), bz = __fmul_rn(__fsub_rn(f4(n.hiz, k), w.highz), w.invz);
-    float lx = w.px ? -1e30f : fminf(ax, bx), hx = w.px ? 1e30f : fmaxf(ax, bx);
-    float ly = w.py ? -1e30f : fminf(ay, by), hy = w.py ? 1e30f : fmaxf(ay, by);
-    float lz = w.pz ? -1e30f : fminf(az, bz), hz = w.pz ? 1e30f : fmaxf(az, bz);
-    float nt = fmaxf(fmaxf(lx, ly), fmaxf(lz, tMin));
-    float ft = fminf(fminf(hx, hy), fminf(hz, tMax));
-    bool hit = nt <= ft && i4(n.child, k) != 0;
-    if (w.px) hit = hit && !(w.lowx < f4(n.lox, k) || w.highx > f4(n.hix, k));
-    if (w.py) hit = hit && !(w.lowy < f4(n.loy, k) || w.highy > f4(n.hiy, k));
-    if (w.pz) hit = hit && !(w.lowz < f4(n.loz, k) || w.highz > f4(n.hiz, k));
+    const float ax = __fmul_rn(__fsub_rn(f4(n.lox, k), w.lowx), w.invx), bx = __fmul_rn(__fsub_rn(f4(n.hix, k), w.highx), w.invx);
+    const float ay = __fmul_rn(__fsub_rn(f4(n.loy, k), w.lowy), w.invy), by = __fmul_rn(__fsub_rn(f4(n.hiy, k), w.highy), w.invy);
+    const float az = __fmul_rn(__fsub_rn(f4(n.loz, k), w.lowz), w.invz), bz = __fmul_rn(__fsub_rn(f4(n.hiz, k), w.highz), w.invz);
+    const float nt = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tMin));
+    const float ft = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tMax));
     nearT[k] = nt;
-    mask |= hit ? (1 << k) : 0;
+    mask |= (nt <= ft && i4(n.child, k) != 0) ? (1 << k) : 0;
   }
   return mask;
 }
 
-// Children of a node in near-to-far order, in registers. A 4-element sorting network on
-// (entry distance, slot) gives exactly the order of the reference's stable insertion sort
-// (wide_order, main.swift:1780-1785), since slots break distance ties; missed children sort last.
+// Order-preserving map of a float to an unsigned integer.
+__device__ __forceinline__ uint32_t ord32(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Hit children near to far, in registers. Each hit child gets the key (ord32(entry + 0), so -0 and +0
+// agree, with its two low bits replaced by the slot): a 5-comparator network of unsigned min/max sorts them by entry distance
+// with slots breaking ties (the reference's stable insertion sort, wide_order, main.swift:1780-1785,
+// up to entry distances equal in all but their two lowest bits); missed children sort last. A child
+// is culled against the closest hit when (key & ~3) > ord32(closest), i.e. only when its entry
+// distance is certainly beyond it.
 struct Sorted4 {
-  float key[4];
+  uint32_t key[4];
   int child[4], count[4];
   int m;  // number of hit children (the first m entries)
 };
-__device__ __forceinline__ void cswap(float &ka, int &sa, int &ca, int &na, float &kb, int &sb, int &cb, int &nb) {
-  const bool sw = ka > kb || (ka == kb && sa > sb);
-  const float k = sw ? kb : ka; kb = sw ? ka : kb; ka = k;
-  const int sl = sw ? sb : sa; sb = sw ? sa : sb; sa = sl;
-  const int c = sw ? cb : ca; cb = sw ? ca : cb; ca = c;
-  const int n = sw ? nb : na; nb = sw ? na : nb; na = n;
+__device__ __forceinline__ void ucswap(uint32_t &a, uint32_t &b) {
+  const uint32_t lo = min(a, b), hi = max(a, b);
+  a = lo; b = hi;
+}
+__device__ __forceinline__ int pick4(const int4 &v, uint32_t slot) {
+  const int lo = (slot & 1u) ? v.y : v.x, hi = (slot & 1u) ? v.w : v.z;
+  return (slot & 2u) ? hi : lo;
 }
 __device__ __forceinline__ Sorted4 sort_children(const Node4 &nd, int mask, const float nearT[4]) {
+  uint32_t k[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    k[c] = (mask >> c & 1) ? ((ord32(__fadd_rn(nearT[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
+  ucswap(k[0], k[1]);
+  ucswap(k[2], k[3]);
+  ucswap(k[0], k[2]);
+  ucswap(k[1], k[3]);
+  ucswap(k[1], k[2]);
   Sorted4 o;
-  float k0 = (mask & 1) ? nearT[0] : __int_as_float(0x7f800000), k1 = (mask & 2) ? nearT[1] : __int_as_float(0x7f800000);
-  float k2 = (mask & 4) ? nearT[2] : __int_as_float(0x7f800000), k3 = (mask & 8) ? nearT[3] : __int_as_float(0x7f800000);
-  int s0 = (mask & 1) ? 0 : 4, s1 = (mask & 2) ? 1 : 5, s2 = (mask & 4) ? 2 : 6, s3 = (mask & 8) ? 3 : 7;
-  int c0 = nd.child.x, c1 = nd.child.y, c2 = nd.child.z, c3 = nd.child.w;
-  int n0 = nd.count.x, n1 = nd.count.y, n2 = nd.count.z, n3 = nd.count.w;
-  cswap(k0, s0, c0, n0, k1, s1, c1, n1);
-  cswap(k2, s2, c2, n2, k3, s3, c3, n3);
-  cswap(k0, s0, c0, n0, k2, s2, c2, n2);
-  cswap(k1, s1, c1, n1, k3, s3, c3, n3);
-  cswap(k1, s1, c1, n1, k2, s2, c2, n2);
-  o.key[0] = k0; o.key[1] = k1; o.key[2] = k2; o.key[3] = k3;
-  o.child[0] = c0; o.child[1] = c1; o.child[2] = c2; o.child[3] = c3;
-  o.count[0] = n0; o.count[1] = n1; o.count[2] = n2; o.count[3] = n3;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    o.key[j] = k[j];
+    o.child[j] = pick4(nd.child, k[j] & 3u);
+    o.count[j] = pick4(nd.count, k[j] & 3u);
+  }
   o.m = __popc(mask);
   return o;
+}
+// Whether sorted entry j lies certainly beyond the closest hit.
+__device__ __forceinline__ bool beyond(uint32_t key, float closest) {
+  return (key & ~3u) > ord32(__fadd_rn(closest, 0.0f));
 }
 
 }  // namespace vtd

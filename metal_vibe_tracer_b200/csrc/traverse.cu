@@ -40,23 +40,11 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
     if (kCount) ++nv;
     float nearT[4];
     const int mask = node_hits(nd, sr, tMin, closest, nearT);
-    // Near-to-far insertion sort of the hit children (wide_order, main.swift:1780-1785).
-    int order[4];
-    float key[4];
-    int m = 0;
+    const Sorted4 o = sort_children(nd, mask, nearT);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (!(mask >> k & 1)) continue;
-      int j = m++;
-      while (j > 0 && key[j - 1] > nearT[k]) { key[j] = key[j - 1]; order[j] = order[j - 1]; --j; }
-      key[j] = nearT[k];
-      order[j] = k;
-    }
-    for (int j = 0; j < m; ++j) {
-      const int k = order[j];
-      const int c = i4(nd.child, k);
-      if (c > 0 || key[j] > closest) continue;
-      const int first = -c - 1, cnt = i4(nd.count, k);
+    for (int j = 0; j < 4; ++j) {
+      if (j >= o.m || o.child[j] > 0 || beyond(o.key[j], closest)) continue;
+      const int first = -o.child[j] - 1, cnt = o.count[j];
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
@@ -66,11 +54,9 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
         closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w); found = true;
       }
     }
-    for (int j = m - 1; j >= 0; --j) {
-      const int k = order[j];
-      const int c = i4(nd.child, k);
-      if (c > 0 && key[j] <= closest && top < kStack) stack[top++] = c;
-    }
+#pragma unroll
+    for (int j = 3; j >= 0; --j)
+      if (j < o.m && o.child[j] > 0 && !beyond(o.key[j], closest) && top < kStack) stack[top++] = o.child[j];
   }
   best = closest;
   return found;
@@ -196,7 +182,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
     const Sorted4 o = sort_children(nd, mask, nearT);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      if (j >= o.m || o.child[j] > 0 || o.key[j] > closest) continue;
+      if (j >= o.m || o.child[j] > 0 || beyond(o.key[j], closest)) continue;
       const int first = -o.child[j] - 1, cnt = o.count[j];
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
@@ -208,7 +194,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
     }
 #pragma unroll
     for (int j = 3; j >= 0; --j) {
-      if (j >= o.m || o.child[j] <= 0 || o.key[j] > closest) continue;
+      if (j >= o.m || o.child[j] <= 0 || beyond(o.key[j], closest)) continue;
       if (top < stackSize) *stack_slot(sstack, top++) = o.child[j];
       else atomicOr(status, (uint32_t)VT_DEV_STACK);
     }

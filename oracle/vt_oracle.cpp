@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstring>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -830,11 +831,59 @@ template <typename T> SlabRay<T> make_slab(const TraceRay<T> &r, T rootMax) {
   for (int k = 0; k < 3; ++k) {
     s.low[k] = r.o[k] + e;
     s.high[k] = r.o[k] - e;
-    s.parallel[k] = std::fabs(r.d[k]) < T(1e-8);
-    s.inv[k] = T(1) / (s.parallel[k] ? T(1) : r.d[k]);
+    if (std::is_same<T, float>::value) {
+      // The CUDA kernels' form: a parallel axis gets the inverse +-1e30 (no separate inside test).
+      s.parallel[k] = false;
+      s.inv[k] = std::fabs(r.d[k]) < T(1e-8) ? std::copysign(T(1e30f), r.d[k]) : T(1) / r.d[k];
+    } else {
+      // The reference's form (wide_ray / wide_node_hit, main.swift:1758-1779).
+      s.parallel[k] = std::fabs(r.d[k]) < T(1e-8);
+      s.inv[k] = T(1) / (s.parallel[k] ? T(1) : r.d[k]);
+    }
   }
   return s;
 }
+
+inline uint32_t ord32(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Near-to-far order of the hit children. fp32 (the CUDA kernels' order): keys ord32(entry + 0)
+// with the two low bits replaced by the slot, sorted ascending; a child is skipped when
+// (key & ~3) > ord32(closest + 0). fp64: the reference's stable insertion sort on the entry
+// distance (wide_order, main.swift:1780-1785), skipped when the entry exceeds the closest hit.
+template <typename T> struct ChildOrder {
+  int order[4];
+  uint32_t key[4];
+  T dist[4];
+  int m = 0;
+  ChildOrder(int mask, const T nearT[4]) {
+    if (std::is_same<T, float>::value) {
+      for (int k = 0; k < 4; ++k) {
+        if (!(mask >> k & 1)) continue;
+        const float z = float(nearT[k]) + 0.0f;
+        key[m] = (ord32(z) & ~3u) | (uint32_t)k;
+        ++m;
+      }
+      std::sort(key, key + m);
+      for (int j = 0; j < m; ++j) order[j] = key[j] & 3u;
+    } else {
+      for (int k = 0; k < 4; ++k) {
+        if (!(mask >> k & 1)) continue;
+        int j = m++;
+        while (j > 0 && dist[j - 1] > nearT[k]) { dist[j] = dist[j - 1]; order[j] = order[j - 1]; --j; }
+        dist[j] = nearT[k];
+        order[j] = k;
+      }
+    }
+  }
+  bool beyond(int j, T closest) const {
+    if (std::is_same<T, float>::value) return (key[j] & ~3u) > ord32(float(closest) + 0.0f);
+    return dist[j] > closest;
+  }
+};
 
 template <typename T>
 int node_hits(const vt_wide_node &n, const SlabRay<T> &w, T tMin, T tMax, T nearT[4]) {
@@ -877,19 +926,11 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
     if (nodes) ++*nodes;
     T nearT[4];
     int mask = node_hits(nd, s, r.tmin, closest, nearT);
-    int order[4];
-    T key[4];
-    int m = 0;
-    for (int k = 0; k < 4; ++k) {
-      if (!(mask >> k & 1)) continue;
-      int j = m++;
-      while (j > 0 && key[j - 1] > nearT[k]) { key[j] = key[j - 1]; order[j] = order[j - 1]; --j; }
-      key[j] = nearT[k];
-      order[j] = k;
-    }
+    const ChildOrder<T> co(mask, nearT);
+    const int m = co.m;
     for (int j = 0; j < m; ++j) {
-      int k = order[j];
-      if (nd.child[k] > 0 || key[j] > closest) continue;
+      int k = co.order[j];
+      if (nd.child[k] > 0 || co.beyond(j, closest)) continue;
       int first = -nd.child[k] - 1;
       for (int q = 0; q < nd.count[k]; ++q) {
         const float *tf = &h.tris[9 * (size_t)(first + q)];
@@ -902,8 +943,8 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
       }
     }
     for (int j = m - 1; j >= 0; --j) {
-      int k = order[j];
-      if (nd.child[k] > 0 && key[j] <= closest && top < 128) stack[top++] = nd.child[k];
+      int k = co.order[j];
+      if (nd.child[k] > 0 && !co.beyond(j, closest) && top < 128) stack[top++] = nd.child[k];
     }
   }
   best = closest;
