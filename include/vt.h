@@ -228,6 +228,73 @@ vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_
                            uint32_t sample_index, uint32_t frame_index, uint32_t vertex, uint32_t stream,
                            float *out);
 
+/* ---- emitter lights: light tree and emitter list ----------------------------------------- */
+
+/* One emitter triangle (LightTree.Emitter, Sources/LightTree.swift:11-16): world corners, power
+ * (area x selection weight) and the cosine of the emission half-angle (0 = one-sided Lambertian).
+ * 56 bytes. */
+typedef struct vt_emitter {
+  float a[3], b[3], c[3];
+  float pad;
+  double power;
+  double cos_emission;
+} vt_emitter;
+
+/* A light BVH built on the host (LightTree.Built, Sources/LightTree.swift:100-108). */
+typedef struct vt_light_tree vt_light_tree;
+typedef struct vt_light_tree_info {
+  uint32_t node_count, depth, count, pad;
+  float grid_lo[3], grid_hi[3];   /* the box node bounds are quantised in */
+} vt_light_tree_info;
+
+/* LightTree.build(_:maxLeaf:leafRatio:) (Sources/LightTree.swift:112): 8 words per node in
+ * depth-first order (LightTree.node, :190-203), `order` mapping leaf positions to input emitters
+ * and each leaf position's node. The reference's defaults are max_leaf 8, leaf_ratio 0.75.
+ * Host only, no device work: ctx may be NULL (errors then go to vt_last_error(NULL)), as for the
+ * getters and vt_emitter_list_pack. */
+vt_status vt_light_tree_build(vt_ctx *ctx, const vt_emitter *emitters, uint32_t n, uint32_t max_leaf,
+                              double leaf_ratio, vt_light_tree **out);
+vt_status vt_light_tree_destroy(vt_ctx *ctx, vt_light_tree *tree);
+vt_status vt_light_tree_get_info(vt_ctx *ctx, const vt_light_tree *tree, vt_light_tree_info *info);
+/* n = 8 * node_count */
+vt_status vt_light_tree_get_words(vt_ctx *ctx, const vt_light_tree *tree, uint32_t *words, uint32_t n);
+/* n = emitter count: order[leaf position] = input emitter, leaf_nodes[leaf position] = its node */
+vt_status vt_light_tree_get_order(vt_ctx *ctx, const vt_light_tree *tree, int32_t *order, uint32_t *leaf_nodes,
+                                  uint32_t n);
+
+/* The packed emitter list the integrator reads (MaterialLibrary's list, main.swift:9313-9345, and
+ * lightTreeList, :9374-9401) for emitters with strictly increasing ids. Power sampling:
+ * [count, ids, cdf, total, 0]; with light_tree = 1 (more than one emitter, and a tree the build
+ * splits and the GPU can walk): [count, ids, leaf positions, total, node count, node offset,
+ * leaf offset, grid lo/hi, padding to 16 bytes, nodes, per leaf position (id, power, leaf node)].
+ * `count` receives the word count; words may be NULL to query it. Host only. */
+vt_status vt_emitter_list_pack(vt_ctx *ctx, const uint32_t *ids, const vt_emitter *emitters, uint32_t n,
+                               uint32_t light_tree, uint32_t *words, uint32_t capacity, uint32_t *count);
+
+/* A scene lit by its emissive triangles: the reference's imported scenes (sceneIndex 6 with a scene
+ * graph), replacing vt_scene_create's quad light. Every face whose slot is VT_MAT_EMISSIVE with
+ * non-zero emission is an emitter with the selection weight max(1e-8, luminance) (main.swift:
+ * 9300-9309); the emitter ids are input face indices. NEE chooses an emitter by power or, with
+ * light_tree = 1, by walking the light tree (sample_direct_light / light_tree_sample, main.swift:
+ * 2892-2912, 2807-2833); BSDF hits on emitters weigh with the matching density (light_tree_pmf,
+ * imported_emitter_area_pdf, :2835-2850, 2871-2881). Emitters emit from their front face
+ * (cross(b - a, c - a)). Offsets and tolerances are the reference's imported-scene rounding bounds
+ * (ray_epsilon, mesh_hit_error, endpoint_tolerance, ray_t_min, main.swift:1343-1364). */
+vt_status vt_scene_create_imported(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
+                                   const vt_spectral_tables *tables, uint32_t light_tree, vt_scene **out);
+/* The scene's packed emitter list (see vt_emitter_list_pack); words may be NULL to query the
+ * count. */
+vt_status vt_scene_emitter_words(vt_ctx *ctx, const vt_scene *scene, uint32_t *words, uint32_t capacity,
+                                 uint32_t *count);
+/* The reference's light-selection check (lt_estimate, tests/Fix_light-tree.swift:66-93) on an
+ * imported scene: thread i takes the receiver points[i / per_point] (4 floats, xyz used), seeds
+ * pcg_hash(i * 7919 + 3) and draws `samples` light samples. It writes 8 floats per thread to the
+ * HOST array out: the sum and sum of squares of luminance / pdf, the samples whose traced ray hit
+ * the sampled triangle, those with a zero BSDF-hit pdf, the largest relative pdf difference, the
+ * samples that chose a back-facing emitter, 0, 0. */
+vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *points, uint32_t npoints,
+                            uint32_t per_point, uint32_t samples, float *out);
+
 /* ---- allocation-free build --------------------------------------------------------------- */
 
 /* No counterpart in the reference. The same GPU build as vt_mesh_build_device, for callers that

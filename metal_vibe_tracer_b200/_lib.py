@@ -23,6 +23,9 @@ WIDE_NODE_DTYPE = np.dtype([
 ])
 RAY_DTYPE = np.dtype([("o", "<f4", 3), ("tmin", "<f4"), ("d", "<f4", 3), ("tmax", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("b1", "<f4"), ("b2", "<f4"), ("prim", "<i4")])
+EMITTER_DTYPE = np.dtype([("a", "<f4", 3), ("b", "<f4", 3), ("c", "<f4", 3), ("pad", "<f4"),
+                          ("power", "<f8"), ("cos_emission", "<f8")])
+assert EMITTER_DTYPE.itemsize == 56
 assert FACE_DTYPE.itemsize == 16 and VERTEX_DTYPE.itemsize == 32
 assert WIDE_NODE_DTYPE.itemsize == 128 and RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
 
@@ -36,6 +39,11 @@ class MeshInfo(C.Structure):
     _fields_ = [("faces", C.c_uint32), ("wide_nodes", C.c_uint32), ("binary_nodes", C.c_uint32),
                 ("depth", C.c_uint32), ("sah_cost", C.c_float), ("build_ms", C.c_float),
                 ("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+
+class LightTreeInfo(C.Structure):
+    _fields_ = [("node_count", C.c_uint32), ("depth", C.c_uint32), ("count", C.c_uint32), ("pad", C.c_uint32),
+                ("grid_lo", C.c_float * 3), ("grid_hi", C.c_float * 3)]
 
 
 VT_OK = 0
@@ -73,6 +81,15 @@ SIGNATURES = {
     "vt_accum_reset": (_I32, [_P, _P]),
     "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_sampler_frame": (_I32, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _P]),
+    "vt_light_tree_build": (_I32, [_P, _P, _U32, _U32, C.c_double, C.POINTER(_P)]),
+    "vt_light_tree_destroy": (_I32, [_P, _P]),
+    "vt_light_tree_get_info": (_I32, [_P, _P, C.POINTER(LightTreeInfo)]),
+    "vt_light_tree_get_words": (_I32, [_P, _P, _P, _U32]),
+    "vt_light_tree_get_order": (_I32, [_P, _P, _P, _P, _U32]),
+    "vt_emitter_list_pack": (_I32, [_P, _P, _P, _U32, _U32, _P, _U32, C.POINTER(_U32)]),
+    "vt_scene_create_imported": (_I32, [_P, _P, _P, _U32, _P, _U32, C.POINTER(_P)]),
+    "vt_scene_emitter_words": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
+    "vt_light_estimate": (_I32, [_P, _P, _P, _U32, _U32, _U32, _P]),
 }
 NOALLOC_MAX_FACES = 32768
 

@@ -60,6 +60,16 @@ struct RenderArgs {
   uint32_t zSampler, zModel, firstFrame;  // Z++ sampler on/off, its temporal model, frame of `first`
   const float2 *jitter;
   double *accum;
+  // Imported scenes (sceneIndex 6): emitter triangles instead of the quad light.
+  uint32_t imported;
+  const uint32_t *emitters;  // packed list (vt_emitter_list_pack layout)
+  const float4 *emissions;   // per slot: emission rgb, selection weight
+  const int32_t *facePos;    // input face -> BVH position
+  uint32_t ecount, treeNodes;
+  float etotal;
+  const uint4 *ltNodes;
+  const uint32_t *ltLeaves;
+  float3 ltLo, ltScale;
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -74,14 +84,14 @@ __device__ __forceinline__ float3 normalize3(float3 a) { return mul(a, rsqrtf(do
 
 // ---- traversal (the 4-wide watertight traversal with a local stack) ---------------------------
 struct Hit {
-  float t;
+  float t, b1, b2;
   int pos;  // BVH position of the triangle
 };
 
 __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, Hit &h, int *stack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
-  float closest = tMax;
+  float closest = tMax, bb1 = 0.0f, bb2 = 0.0f;
   int best = -1;
   int top = 0;
   stack[top++] = 0;
@@ -100,6 +110,8 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
         float t, b1, b2;
         if (!intersect_tri(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
         closest = t;
+        bb1 = b1;
+        bb2 = b2;
         best = first + q;
       }
     }
@@ -108,11 +120,24 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
       if (j < s.m && s.child[j] > 0 && !beyond(s.key[j], closest) && top < kRenderStack) stack[top++] = s.child[j];
   }
   h.t = closest;
+  h.b1 = bb1;
+  h.b2 = bb2;
   h.pos = best;
   return best >= 0;
 }
 
-__device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, int *stack) {
+__device__ __forceinline__ float max_abs3(float x, float y, float z) { return fmaxf(fabsf(x), fmaxf(fabsf(y), fabsf(z))); }
+__device__ __forceinline__ float max_abs(float3 p) { return max_abs3(p.x, p.y, p.z); }
+
+// mesh_hit_error (main.swift:1353-1355) of an imported triangle: its vertices' rounding bound.
+__device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) {
+  return fmaxf(1e-7f, 1.907349e-6f * fmaxf(max_abs3(a.x, a.y, a.z), fmaxf(max_abs3(b.x, b.y, b.z), max_abs3(c.x, c.y, c.z))));
+}
+
+// Any hit in [tMin, tMax); with `slack` (imported scenes) each triangle's own rounding bound is
+// taken off tMax, so the endpoint surface does not occlude itself (scene_occluded, main.swift:
+// 2066-2069).
+__device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, int *stack, bool slack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
   int top = 0;
@@ -130,8 +155,9 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
       const int first = -c - 1, cnt = i4(nd.count, k);
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
+        const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
         float t, b1, b2;
-        if (intersect_tri(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, tMax, t, b1, b2)) return true;
+        if (intersect_tri(wr, ta, tb, tc, tMin, slack ? tMax - mesh_hit_error(ta, tb, tc) : tMax, t, b1, b2)) return true;
       }
     }
   }
@@ -141,17 +167,41 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
 // ---- surfaces, lights, spectra -----------------------------------------------------------------
 struct Surface {
   float3 pos, gn;  // position, geometric normal facing the incoming ray (the shading normal)
-  uint32_t slot;
+  float err;       // HitRecord.error: the position's rounding bound
+  uint32_t slot, face;
+  bool front;      // the ray meets the side cross(b - a, c - a) points to
 };
 
+// ray_epsilon (main.swift:1343-1345): the procedural scenes' 0.001, or for imported scenes a bound
+// that scales with the coordinates' magnitude.
+__device__ __forceinline__ float ray_eps(const RenderArgs &A, float3 p) {
+  return A.imported ? fmaxf(1e-7f, 9.536743e-7f * max_abs(p)) : kEps;
+}
+// ray_t_min (main.swift:1362-1364).
+__device__ __forceinline__ float ray_tmin(const RenderArgs &A, float3 o) {
+  return A.imported ? ray_eps(A, o) * 0.25f : kEps;
+}
+
+// The hit record (trace_scene and mesh_hit_attributes, main.swift:1587-1592, 2025-2032): imported
+// scenes rebuild the point from barycentrics and take the triangle's rounding bound as its error.
 __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h, float3 o, float3 d) {
   Surface s;
   const float4 a = __ldg(A.tris + 3 * (size_t)h.pos), b = __ldg(A.tris + 3 * (size_t)h.pos + 1),
                c = __ldg(A.tris + 3 * (size_t)h.pos + 2);
-  s.pos = add(o, mul(d, h.t));
-  float3 ng = normalize3(cross3(f3(b.x - a.x, b.y - a.y, b.z - a.z), f3(c.x - a.x, c.y - a.y, c.z - a.z)));
-  s.gn = dot3(ng, d) < 0.0f ? ng : mul(ng, -1.0f);
+  const float3 e1 = f3(b.x - a.x, b.y - a.y, b.z - a.z), e2 = f3(c.x - a.x, c.y - a.y, c.z - a.z);
+  const float3 ng = normalize3(cross3(e1, e2));
+  s.front = dot3(ng, d) < 0.0f;
+  s.gn = s.front ? ng : mul(ng, -1.0f);
   s.slot = __float_as_uint(b.w);
+  s.face = __float_as_uint(a.w);
+  if (A.imported) {
+    const float b0 = 1.0f - h.b1 - h.b2;
+    s.pos = add(add(mul(f3(a.x, a.y, a.z), b0), mul(f3(b.x, b.y, b.z), h.b1)), mul(f3(c.x, c.y, c.z), h.b2));
+    s.err = mesh_hit_error(a, b, c);
+  } else {
+    s.pos = add(o, mul(d, h.t));
+    s.err = kEps;
+  }
   return s;
 }
 
@@ -205,14 +255,17 @@ __device__ __forceinline__ float4 lanes_emission(const RenderArgs &A, const Lane
 }
 
 struct LightSample {
-  float3 pos, wi;
+  float3 pos, wi, emission;
   float dist, pdf;
+  uint32_t face;  // sampled emitter triangle (imported scenes), else 0xffffffff
 };
 
 // Quad light sample (2 draws).
 __device__ __forceinline__ LightSample sample_light(const RenderArgs &A, float3 p, Sampler &seed) {
   LightSample ls;
   ls.pdf = 0.0f;
+  ls.face = 0xffffffffu;
+  ls.emission = A.le;
   const float2 uv = rand_f2(seed);
   const float u = uv.x, v = uv.y;
   const float3 lp = add(A.lc, add(mul(A.lsu, u), mul(A.lsv, v)));
@@ -237,23 +290,256 @@ __device__ __forceinline__ float light_pdf(const RenderArgs &A, float3 p, float3
   return cos_l <= 0.0f ? 0.0f : dist * dist / (A.larea * cos_l);
 }
 
-// ray_origin (main.swift:1366-1369) with the procedural scenes' epsilon.
-__device__ __forceinline__ float3 ray_origin(float3 p, float3 gn, float3 dir) {
-  return add(p, mul(gn, dot3(dir, gn) >= 0.0f ? kEps : -kEps));
+// ---- emitter triangles: power sampling and the light tree (imported scenes) -------------------
+struct Tri {
+  float3 a, b, c;
+  uint32_t slot;
+};
+
+__device__ __forceinline__ Tri scene_triangle(const RenderArgs &A, uint32_t face) {
+  const float4 *t = A.tris + 3 * (size_t)__ldg(A.facePos + face);
+  const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+  return Tri{f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), __float_as_uint(b.w)};
+}
+
+// imported_geometry (main.swift:2721-2725): cos at the emitter (front side) over d^2.
+__device__ __forceinline__ float imported_geometry(float3 p, float3 position, const Tri &t) {
+  const float3 d = sub(position, p);
+  const float d2 = dot3(d, d);
+  const float3 n = cross3(sub(t.b, t.a), sub(t.c, t.a));
+  return d2 > 1e-12f && dot3(n, n) > 1e-20f ? fmaxf(0.0f, dot3(normalize3(n), mul(d, -rsqrtf(d2)))) / d2 : 0.0f;
+}
+
+__device__ __forceinline__ float triangle_area(const Tri &t) {
+  const float3 n = cross3(sub(t.b, t.a), sub(t.c, t.a));
+  return 0.5f * sqrtf(dot3(n, n));
+}
+
+struct LtNode {
+  float3 lo, hi, w;
+  float phi, cosO, cosE;
+  uint32_t child, parent, count;
+};
+
+// light_tree_axis (main.swift:2751-2756): the octahedral cone axis.
+__device__ __forceinline__ float3 lt_axis(uint32_t q) {
+  const float fx = float(q & 0xffffu) / 65535.0f * 2.0f - 1.0f, fy = float(q >> 16) / 65535.0f * 2.0f - 1.0f;
+  float3 v = f3(fx, fy, 1.0f - fabsf(fx) - fabsf(fy));
+  if (v.z < 0.0f) {
+    const float vx = (1.0f - fabsf(v.y)) * (v.x >= 0.0f ? 1.0f : -1.0f);
+    const float vy = (1.0f - fabsf(v.x)) * (v.y >= 0.0f ? 1.0f : -1.0f);
+    v.x = vx;
+    v.y = vy;
+  }
+  return normalize3(v);
+}
+
+// light_tree_node (main.swift:2768-2778).
+__device__ __forceinline__ LtNode lt_node(const RenderArgs &A, uint32_t i) {
+  const uint4 a = __ldg(A.ltNodes + 2 * (size_t)i), b = __ldg(A.ltNodes + 2 * (size_t)i + 1);
+  LtNode n;
+  n.w = lt_axis(a.x);
+  n.phi = __uint_as_float(a.y);
+  n.cosO = float(a.z & 0xffffu) / 65535.0f * 2.0f - 1.0f;
+  n.cosE = float(a.z >> 16) / 65535.0f * 2.0f - 1.0f;
+  n.lo = add(A.ltLo, f3(float(a.w & 0xffffu) * A.ltScale.x, float(a.w >> 16) * A.ltScale.y, float(b.x & 0xffffu) * A.ltScale.z));
+  n.hi = add(A.ltLo, f3(float(b.x >> 16) * A.ltScale.x, float(b.y & 0xffffu) * A.ltScale.y, float(b.y >> 16) * A.ltScale.z));
+  n.child = b.z;
+  n.parent = b.w & 0x7ffffffu;
+  n.count = b.w >> 27;
+  return n;
+}
+
+__device__ __forceinline__ uint32_t lt_leaf_word(const RenderArgs &A, uint32_t position, uint32_t k) {
+  return __ldg(A.ltLeaves + 3 * (size_t)position + k);
+}
+__device__ __forceinline__ float lt_leaf_sum(const RenderArgs &A, const LtNode &n) {
+  float sum = 0.0f;
+  for (uint32_t i = 0; i < n.count; ++i) sum += __uint_as_float(lt_leaf_word(A, n.child + i, 1u));
+  return sum;
+}
+
+__device__ __forceinline__ float cos_sub_clamped(float sinA, float cosA, float sinB, float cosB) {
+  return cosA > cosB ? 1.0f : cosA * cosB + sinA * sinB;
+}
+__device__ __forceinline__ float sin_sub_clamped(float sinA, float cosA, float sinB, float cosB) {
+  return cosA > cosB ? 0.0f : sinA * cosB - cosA * sinB;
+}
+
+// light_tree_importance (main.swift:2788-2805): pbrt-v4's bound without the receiver normal.
+__device__ float lt_importance(const LtNode &n, float3 p) {
+  if (!(n.phi > 0.0f)) return 0.0f;
+  const float3 pc = mul(add(n.lo, n.hi), 0.5f);
+  const float3 dp = sub(p, pc), ext = sub(n.hi, n.lo);
+  const float dist2 = dot3(dp, dp);
+  const float d2 = fmaxf(dist2, fmaxf(0.5f * sqrtf(dot3(ext, ext)), 1e-20f));
+  if (p.x >= n.lo.x && p.y >= n.lo.y && p.z >= n.lo.z && p.x <= n.hi.x && p.y <= n.hi.y && p.z <= n.hi.z)
+    return n.phi / d2;
+  const float3 wi = mul(dp, rsqrtf(dist2));
+  const float cosW = dot3(n.w, wi), sinW = sqrtf(fmaxf(0.0f, 1.0f - cosW * cosW));
+  const float3 dh = sub(pc, n.hi);
+  const float s2 = dot3(dh, dh) / dist2;
+  const float cosB = s2 >= 1.0f ? -1.0f : sqrtf(fmaxf(0.0f, 1.0f - s2)), sinB = sqrtf(fmaxf(0.0f, 1.0f - cosB * cosB));
+  const float sinO = sqrtf(fmaxf(0.0f, 1.0f - n.cosO * n.cosO));
+  const float cosX = cos_sub_clamped(sinW, cosW, sinO, n.cosO), sinX = sin_sub_clamped(sinW, cosW, sinO, n.cosO);
+  const float cosP = cos_sub_clamped(sinX, cosX, sinB, cosB);
+  return cosP <= n.cosE ? 0.0f : n.phi * cosP / d2;
+}
+
+// light_tree_sample (main.swift:2809-2833): walk from the root with one number, rescaled at each
+// choice, then choose within the leaf by power. Returns the leaf position, or 0xffffffff.
+__device__ uint32_t lt_sample(const RenderArgs &A, float3 p, float u, float &pmf) {
+  pmf = 1.0f;
+  uint32_t index = 0;
+  for (uint32_t depth = 0; depth <= 64u; ++depth) {
+    const LtNode n = lt_node(A, index);
+    if (n.count != 0u) {
+      const float sum = lt_leaf_sum(A, n), target = u * sum;
+      float cumulative = 0.0f, chosen = 0.0f;
+      uint32_t position = 0xffffffffu;
+      for (uint32_t i = 0; i < n.count && sum > 0.0f; ++i) {
+        const float power = __uint_as_float(lt_leaf_word(A, n.child + i, 1u));
+        if (!(power > 0.0f)) continue;
+        position = n.child + i;
+        chosen = power;
+        cumulative += power;
+        if (target < cumulative) break;
+      }
+      if (position == 0xffffffffu) break;
+      pmf *= chosen / sum;
+      return position;
+    }
+    const float l = lt_importance(lt_node(A, index + 1u), p), r = lt_importance(lt_node(A, n.child), p);
+    if (!(l + r > 0.0f)) break;
+    const float pl = l / (l + r);
+    if (u < pl) {
+      u = fminf(u / pl, 0x1.fffffep-1f);
+      index = index + 1u;
+      pmf *= pl;
+    } else {
+      u = fminf((u - pl) / (1.0f - pl), 0x1.fffffep-1f);
+      index = n.child;
+      pmf *= r / (l + r);
+    }
+  }
+  pmf = 0.0f;
+  return 0xffffffffu;
+}
+
+// light_tree_pmf (main.swift:2835-2850): the same choices from the leaf up to the root.
+__device__ float lt_pmf(const RenderArgs &A, float3 p, uint32_t position) {
+  uint32_t index = lt_leaf_word(A, position, 2u);
+  LtNode node = lt_node(A, index);
+  const float sum = lt_leaf_sum(A, node);
+  float pmf = sum > 0.0f ? __uint_as_float(lt_leaf_word(A, position, 1u)) / sum : 0.0f;
+  for (uint32_t depth = 0; depth <= 64u && pmf > 0.0f; ++depth) {
+    const uint32_t parent = node.parent;
+    if (parent == 0x7ffffffu) return pmf;
+    const LtNode up = lt_node(A, parent);
+    const float l = lt_importance(lt_node(A, parent + 1u), p), r = lt_importance(lt_node(A, up.child), p);
+    const float mine = index == parent + 1u ? l : r;
+    if (!(l + r > 0.0f) || !(mine > 0.0f)) return 0.0f;
+    pmf *= mine / (l + r);
+    index = parent;
+    node = up;
+  }
+  return 0.0f;
+}
+
+// imported_emitter_position (main.swift:2852-2856): a face's leaf position, by binary search of
+// the sorted ids.
+__device__ __forceinline__ uint32_t emitter_position(const RenderArgs &A, uint32_t face) {
+  uint32_t low = 0, high = A.ecount;
+  while (low < high) {
+    const uint32_t middle = (low + high) / 2;
+    if (__ldg(A.emitters + 1 + middle) < face) low = middle + 1; else high = middle;
+  }
+  return low < A.ecount && __ldg(A.emitters + 1 + low) == face ? __ldg(A.emitters + 1 + A.ecount + low) : 0xffffffffu;
+}
+
+// imported_emitter_area_pdf (main.swift:2859-2869): density per unit area of choosing the face.
+__device__ __forceinline__ float emitter_area_pdf(const RenderArgs &A, uint32_t face, float3 p, const Tri &t) {
+  if (A.ecount == 0u) return 0.0f;
+  if (A.treeNodes > 0u) {
+    const uint32_t position = emitter_position(A, face);
+    const float area = triangle_area(t);
+    return position != 0xffffffffu && area > 0.0f ? lt_pmf(A, p, position) / area : 0.0f;
+  }
+  return A.etotal > 0.0f ? __ldg(A.emissions + t.slot).w / A.etotal : 0.0f;
+}
+
+// sample_direct_light's emitter branch (main.swift:2892-2920), with the emitter probability 1 (no
+// environment): the choice draw, then one 3D draw (emitter, point on it).
+__device__ LightSample sample_emitters(const RenderArgs &A, float3 p, Sampler &seed) {
+  LightSample ls;
+  ls.pdf = 0.0f;
+  ls.face = 0xffffffffu;
+  ls.emission = f3(0.0f, 0.0f, 0.0f);
+  if (A.ecount == 0u) return ls;
+  (void)rand_f(seed);  // rand_f(seed) < importedProbability (= 1)
+  const float3 q = rand_f3(seed);
+  const bool tree = A.treeNodes > 0u;
+  float pmf = 0.0f;
+  uint32_t face;
+  if (tree) {
+    const uint32_t position = lt_sample(A, p, q.x, pmf);
+    if (position == 0xffffffffu) return ls;
+    face = lt_leaf_word(A, position, 0u);
+  } else {
+    uint32_t low = 0, high = A.ecount - 1u;
+    while (low < high) {
+      const uint32_t middle = (low + high) / 2;
+      if (__uint_as_float(__ldg(A.emitters + 1 + A.ecount + middle)) >= q.x) high = middle; else low = middle + 1;
+    }
+    face = __ldg(A.emitters + 1 + low);
+  }
+  const Tri t = scene_triangle(A, face);
+  const float root = sqrtf(q.y);
+  ls.pos = add(add(mul(t.a, 1.0f - root), mul(t.b, root * (1.0f - q.z))), mul(t.c, root * q.z));
+  const float3 delta = sub(ls.pos, p);
+  ls.dist = sqrtf(dot3(delta, delta));
+  ls.wi = mul(delta, 1.0f / fmaxf(ls.dist, 1e-8f));
+  const float geometry = imported_geometry(p, ls.pos, t);
+  const float4 e = __ldg(A.emissions + t.slot);
+  ls.emission = f3(e.x, e.y, e.z);
+  ls.face = face;
+  const float area = tree ? triangle_area(t) : 0.0f;
+  const float areaPdf = !tree ? emitter_area_pdf(A, face, p, t) : (area > 0.0f ? pmf / area : 0.0f);
+  ls.pdf = geometry > 1e-12f ? areaPdf / geometry : 0.0f;
+  return ls;
+}
+
+// eval_light_pdf for imported emitters (main.swift:3066-3071): the BSDF hit's own triangle.
+__device__ __forceinline__ float emitter_pdf(const RenderArgs &A, float3 p, float3 hitPos, uint32_t face) {
+  if (A.ecount == 0u) return 0.0f;
+  const Tri t = scene_triangle(A, face);
+  const float g = imported_geometry(p, hitPos, t);
+  return g > 1e-12f ? emitter_area_pdf(A, face, p, t) / g : 0.0f;
+}
+
+__device__ __forceinline__ LightSample sample_direct(const RenderArgs &A, float3 p, Sampler &seed) {
+  return A.imported ? sample_emitters(A, p, seed) : sample_light(A, p, seed);
+}
+
+// ray_origin (main.swift:1366-1369): offset along the geometric normal by max(error, epsilon).
+__device__ __forceinline__ float3 ray_origin(const RenderArgs &A, float3 p, float3 gn, float3 dir, float err) {
+  const float offset = fmaxf(err, ray_eps(A, p));
+  return add(p, mul(gn, dot3(dir, gn) >= 0.0f ? offset : -offset));
 }
 
 // light_visible (main.swift:3254-3264): shadow ray from the offset origin to the sample, shortened
-// by the endpoint tolerance 2 epsilon.
-__device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, const LightSample &ls,
-                                              int *stack) {
+// by the endpoint tolerance (endpoint_tolerance, main.swift:1358-1361).
+__device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
+                                              const LightSample &ls, int *stack) {
   if (ls.pdf <= 0.0f) return false;
-  const float3 o = ray_origin(p, gn, ls.wi);
+  const float3 o = ray_origin(A, p, gn, ls.wi, err);
   float3 delta = sub(ls.pos, o);
   const float d = sqrtf(dot3(delta, delta));
-  const float tol = 2.0f * kEps;
+  const float legacy = 2.0f * ray_eps(A, ls.pos);
+  const float tol = A.imported ? fmaxf(legacy, 1.907349e-6f * (max_abs(o) + max_abs(ls.pos) + d)) : legacy;
   if (d <= tol) return false;
   delta = mul(delta, 1.0f / d);
-  return !rt_any(A, o, delta, kEps, d - tol, stack);
+  return !rt_any(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
 }
 
 __device__ __forceinline__ float power_heuristic(float pf, float pg) {
@@ -301,13 +587,13 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
   return A.spectral ? fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)) : fmaxf(fmaxf(a.x, a.y), a.z);
 }
 
-// NEE at a Lambert vertex: the contribution's rgb (2 draws).
-__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 wo,
-                                               float4 T, float4 albedo, bool useMIS, Sampler &seed, int *stack,
-                                               bool requirePdf) {
-  const LightSample ls = sample_light(A, p, seed);
+// NEE at a Lambert vertex: the contribution's rgb (quad: 2 draws; emitters: 4).
+__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float err,
+                                               float3 wo, float4 T, float4 albedo, bool useMIS, Sampler &seed,
+                                               int *stack, bool requirePdf) {
+  const LightSample ls = sample_direct(A, p, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
-  if (!light_visible(A, p, n, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
+  if (!light_visible(A, p, n, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
   const float cosine = fabsf(dot3(n, ls.wi));
   // eval_bsdf / eval_bsdf_pdf for DIFFUSE (main.swift:2665-2686), shading normal = geometric.
   float f = 0.0f, bpdf = 0.0f;
@@ -317,7 +603,7 @@ __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes 
     if (ni > 0.0f && cosine >= 1e-7f) f = kInvPi;
   }
   const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
-  const float le[3] = {A.le.x, A.le.y, A.le.z};
+  const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
   const float4 Le = emission(A, L, le);
   const float4 s = scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
   return to_rgb(A, L, s);
@@ -337,19 +623,26 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   v *= A.fovScale;
   const float3 dir0 = normalize3(add(A.fwd, add(mul(A.right, u), mul(A.up, v))));
   Hit h;
-  const bool hit0 = rt_closest(A, A.cam, dir0, kEps, __int_as_float(0x7f800000), h, stack);
+  const bool hit0 = rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   if (!hit0) return f3(0.0f, 0.0f, 0.0f);
   Surface S = surface_at(A, h, A.cam, dir0);
   vt_material m = material(A, S.slot);
-  if (m.type == VT_MAT_EMISSIVE) return f3(m.emission[0], m.emission[1], m.emission[2]);
+  if (m.type == VT_MAT_EMISSIVE) {
+    // The camera sees the emitter's radiance, in spectral transport its four-wavelength estimate
+    // (emitter_rgb, main.swift:7467-7468); imported emitters emit from their front face only
+    // (trace_scene, main.swift:2031).
+    if (A.imported && !S.front) return f3(0.0f, 0.0f, 0.0f);
+    return to_rgb(A, L, emission(A, L, m.emission));
+  }
   const int limit = max(0, (int)A.maxDepth - 1);
   const bool nee = A.mode != 3u, mis = A.mode == 1u;
   float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
   float3 R = f3(0.0f, 0.0f, 0.0f);
   if (nee) {
     sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.gn, mul(dir0, -1.0f), T, reflectance(A, m), mis && limit > 0, seed, stack, true);
+    R = direct_light(A, L, S.pos, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), mis && limit > 0, seed, stack,
+                     true);
   }
   float3 dir = dir0;
   int scattering = 0;
@@ -370,24 +663,24 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     T = mul4(T, reflectance(A, m));
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
     const float3 prev = S.pos;
-    const float3 o = ray_origin(S.pos, S.gn, nd);
+    const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
-    if (!rt_closest(A, o, dir, kEps, __int_as_float(0x7f800000), h, stack)) break;
+    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       // emission_weight (main.swift:3462-3466): 1 without NEE or without a light pdf, else the
       // power heuristic (MIS) or 0 (light sampling).
-      const float lpdf = light_pdf(A, prev, S.pos);
+      const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
       const float w = !nee || lpdf <= 0.0f ? 1.0f : (mis ? power_heuristic(bpdf, lpdf) : 0.0f);
-      R = add(R, to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w)));
+      if (!A.imported || S.front) R = add(R, to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w)));
       break;
     }
     if (emissionOnly) break;
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light(A, L, S.pos, S.gn, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit, seed,
-                              stack, false));
+      R = add(R, direct_light(A, L, S.pos, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit,
+                              seed, stack, false));
     }
     if (bounce > 3) {
       const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
@@ -427,6 +720,63 @@ __global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t 
   }
 }
 
+// ---- imported scenes: emitter collection and the light-selection check --------------------------
+__global__ void k_face_positions(const int32_t *__restrict__ order, uint32_t n, int32_t *__restrict__ facePos) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) facePos[order[i]] = (int32_t)i;
+}
+
+// Emitter faces: those whose slot has a positive selection weight. Pass 1 counts, pass 2 writes
+// (face, a, b, c) records in arbitrary order (the host sorts them by face).
+__global__ void k_collect_emitters(const float4 *__restrict__ tris, uint32_t n, const float4 *__restrict__ emissions,
+                                   uint32_t nslots, uint32_t *counter, float4 *out, uint32_t capacity) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 b = tris[3 * (size_t)i + 1];
+  const uint32_t slot = __float_as_uint(b.w);
+  if (slot >= nslots || !(emissions[slot].w > 0.0f)) return;
+  const uint32_t k = atomicAdd(counter, 1u);
+  if (!out || k >= capacity) return;
+  out[3 * (size_t)k] = tris[3 * (size_t)i];
+  out[3 * (size_t)k + 1] = b;
+  out[3 * (size_t)k + 2] = tris[3 * (size_t)i + 2];
+}
+
+// lt_estimate (tests/Fix_light-tree.swift:66-93) on the scene's emitter list.
+__global__ void k_light_estimate(RenderArgs A, const float4 *__restrict__ points, uint32_t npoints, uint32_t perPoint,
+                                 uint32_t samples, float *out) {
+  int stack[kRenderStack];
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= npoints * perPoint) return;
+  const float4 pp = points[tid / perPoint];
+  const float3 p = f3(pp.x, pp.y, pp.z);
+  Sampler seed;
+  seed.state = pcg_hash(tid * 7919u + 3u);
+  seed.z = false;
+  seed.key = seed.dimension = seed.sub = seed.subBits = 0u;
+  float sum = 0.0f, squares = 0.0f, hits = 0.0f, zero = 0.0f, error = 0.0f, backFacing = 0.0f;
+  for (uint32_t i = 0; i < samples; ++i) {
+    const LightSample ls = sample_emitters(A, p, seed);
+    if (ls.face == 0xffffffffu) continue;
+    const Tri t = scene_triangle(A, ls.face);
+    if (dot3(cross3(sub(t.b, t.a), sub(t.c, t.a)), sub(p, ls.pos)) <= 0.0f) backFacing += 1.0f;
+    if (!(ls.pdf > 0.0f)) continue;
+    const float c = (0.2126f * ls.emission.x + 0.7152f * ls.emission.y + 0.0722f * ls.emission.z) / ls.pdf;
+    sum += c;
+    squares += c * c;
+    Hit h;
+    if (!rt_closest(A, p, ls.wi, ray_tmin(A, p), __int_as_float(0x7f800000), h, stack)) continue;
+    const Surface S = surface_at(A, h, p, ls.wi);
+    if (material(A, S.slot).type != VT_MAT_EMISSIVE || S.face != ls.face) continue;
+    hits += 1.0f;
+    const float pdf = emitter_pdf(A, p, S.pos, S.face);
+    if (!(pdf > 0.0f)) zero += 1.0f; else error = fmaxf(error, fabsf(pdf - ls.pdf) / ls.pdf);
+  }
+  float *o = out + 8 * (size_t)tid;
+  o[0] = sum; o[1] = squares; o[2] = hits; o[3] = zero;
+  o[4] = error; o[5] = backFacing; o[6] = 0.0f; o[7] = 0.0f;
+}
+
 // frameJitter (main.swift:8773-8785): base-2/base-3 Halton, 1024-frame period, minus 0.5.
 float halton(uint32_t index, uint32_t base) {
   uint32_t n = index;
@@ -446,14 +796,11 @@ void host_normalize(float v[3]) {
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-vt_status vt_scene_create(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
-                          const vt_quad_light *light, const vt_spectral_tables *tables, vt_scene **out) {
-  if (!ctx) return VT_ERR_INVALID;
-  if (!out || !mesh || !light || (nmat && !materials)) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
-  *out = nullptr;
-  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+// Shared by both scene kinds: validation, material slots, spectral tables.
+vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
+                       const float *lightEmission, const vt_spectral_tables *tables, vt_scene *sc) {
   if (tables) {
     if (!tables->cmf_rgb || !tables->illuminant || !tables->icdf || tables->nbins < 2 || tables->segments < 1)
       return vt_fail(ctx, VT_ERR_INVALID, "incomplete spectral tables");
@@ -463,24 +810,17 @@ vt_status vt_scene_create(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *m
       if (std::fabs(c[0] - c[1]) > 1e-4f || std::fabs(c[1] - c[2]) > 1e-4f)
         return vt_fail(ctx, VT_ERR_INVALID, "spectral transport supports grey materials only (slot " + std::to_string(i) + ")");
     }
-    const float *e = light->emission;
-    if (std::fabs(e[0] - e[1]) > 1e-4f || std::fabs(e[1] - e[2]) > 1e-4f)
-      return vt_fail(ctx, VT_ERR_INVALID, "spectral transport supports a grey light emission only");
+    if (lightEmission) {
+      const float *e = lightEmission;
+      if (std::fabs(e[0] - e[1]) > 1e-4f || std::fabs(e[1] - e[2]) > 1e-4f)
+        return vt_fail(ctx, VT_ERR_INVALID, "spectral transport supports a grey light emission only");
+    }
   }
-  vt_scene *sc = new vt_scene();
   sc->mesh = mesh;
   sc->nmat = nmat;
-  sc->light = *light;
-  auto fail = [&](cudaError_t err, const char *what) {
-    cudaFree(sc->d_mats); cudaFree(sc->d_spec); cudaFree(sc->d_icdf);
-    delete sc;
-    return vt_cuda_fail(ctx, err, what);
-  };
-  cudaError_t e;
   if (nmat) {
-    if ((e = cudaMalloc(&sc->d_mats, nmat * sizeof(vt_material))) != cudaSuccess) return fail(e, "cudaMalloc(materials)");
-    if ((e = cudaMemcpy(sc->d_mats, materials, nmat * sizeof(vt_material), cudaMemcpyHostToDevice)) != cudaSuccess)
-      return fail(e, "cudaMemcpy(materials)");
+    VT_CUDA(ctx, cudaMalloc(&sc->d_mats, nmat * sizeof(vt_material)));
+    VT_CUDA(ctx, cudaMemcpy(sc->d_mats, materials, nmat * sizeof(vt_material), cudaMemcpyHostToDevice));
   }
   if (tables) {
     std::vector<float4> spec(tables->nbins);
@@ -489,14 +829,209 @@ vt_status vt_scene_create(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *m
     sc->nbins = tables->nbins;
     sc->segments = tables->segments;
     sc->lambda_min = tables->lambda_min;
-    if ((e = cudaMalloc(&sc->d_spec, spec.size() * sizeof(float4))) != cudaSuccess) return fail(e, "cudaMalloc(spectral)");
-    if ((e = cudaMemcpy(sc->d_spec, spec.data(), spec.size() * sizeof(float4), cudaMemcpyHostToDevice)) != cudaSuccess)
-      return fail(e, "cudaMemcpy(spectral)");
-    if ((e = cudaMalloc(&sc->d_icdf, (tables->segments + 1) * sizeof(float))) != cudaSuccess) return fail(e, "cudaMalloc(icdf)");
-    if ((e = cudaMemcpy(sc->d_icdf, tables->icdf, (tables->segments + 1) * sizeof(float), cudaMemcpyHostToDevice)) != cudaSuccess)
-      return fail(e, "cudaMemcpy(icdf)");
+    VT_CUDA(ctx, cudaMalloc(&sc->d_spec, spec.size() * sizeof(float4)));
+    VT_CUDA(ctx, cudaMemcpy(sc->d_spec, spec.data(), spec.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    VT_CUDA(ctx, cudaMalloc(&sc->d_icdf, (tables->segments + 1) * sizeof(float)));
+    VT_CUDA(ctx, cudaMemcpy(sc->d_icdf, tables->icdf, (tables->segments + 1) * sizeof(float), cudaMemcpyHostToDevice));
   }
+  return VT_OK;
+}
+
+void scene_free(vt_scene *scene) {
+  cudaFree(scene->d_mats);
+  cudaFree(scene->d_spec);
+  cudaFree(scene->d_icdf);
+  cudaFree(scene->d_accum);
+  cudaFree(scene->d_jitter);
+  cudaFree(scene->d_emitters);
+  cudaFree(scene->d_emissions);
+  cudaFree(scene->d_face_pos);
+  delete scene;
+}
+
+// Selection weight of an emission slot (main.swift:9303-9306): the float luminance, at least 1e-8.
+float selection_weight(const float e[3]) {
+  const float lum = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2];
+  return std::max(1e-8f, lum);
+}
+
+// Emitter list of an imported scene: collect emitter faces on the device, compute their power on
+// the host (area in double from float edges, times the float weight, main.swift:9318-9323), sort
+// by face id and pack.
+vt_status build_emitters(vt_ctx *ctx, vt_scene *sc, const vt_material *materials, uint32_t nmat, bool lightTree) {
+  const vt_mesh *mesh = sc->mesh;
+  std::vector<float4> emis(std::max(1u, nmat), make_float4(0, 0, 0, 0));
+  for (uint32_t i = 0; i < nmat; ++i) {
+    const vt_material &m = materials[i];
+    if (m.type != VT_MAT_EMISSIVE) continue;
+    const double l2 = double(m.emission[0]) * m.emission[0] + double(m.emission[1]) * m.emission[1] +
+                      double(m.emission[2]) * m.emission[2];
+    emis[i] = make_float4(m.emission[0], m.emission[1], m.emission[2], l2 > 0 ? selection_weight(m.emission) : 0.0f);
+  }
+  VT_CUDA(ctx, cudaMalloc(&sc->d_emissions, emis.size() * sizeof(float4)));
+  VT_CUDA(ctx, cudaMemcpy(sc->d_emissions, emis.data(), emis.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  const uint32_t n = mesh->nfaces;
+  VT_CUDA(ctx, cudaMalloc(&sc->d_face_pos, std::max(1u, n) * sizeof(int32_t)));
+  std::vector<float4> recs;
+  if (n) {
+    const unsigned blocks = (n + 255) / 256;
+    k_face_positions<<<blocks, 256, 0, ctx->stream>>>(mesh->d_order, n, sc->d_face_pos);
+    uint32_t *counter = vt_scratch_word(ctx);
+    VT_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), ctx->stream));
+    k_collect_emitters<<<blocks, 256, 0, ctx->stream>>>(mesh->d_tris, n, sc->d_emissions, nmat, counter, nullptr, 0);
+    uint32_t count = 0;
+    VT_CUDA(ctx, cudaMemcpyAsync(&count, counter, sizeof count, cudaMemcpyDeviceToHost, ctx->stream));
+    VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (count) {
+      float4 *d_recs = nullptr;
+      VT_CUDA(ctx, cudaMalloc(&d_recs, 3 * (size_t)count * sizeof(float4)));
+      cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), ctx->stream);
+      if (e == cudaSuccess) {
+        k_collect_emitters<<<blocks, 256, 0, ctx->stream>>>(mesh->d_tris, n, sc->d_emissions, nmat, counter, d_recs, count);
+        e = cudaGetLastError();
+      }
+      recs.resize(3 * (size_t)count);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(recs.data(), d_recs, recs.size() * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+      cudaFree(d_recs);
+      if (e != cudaSuccess) return vt_cuda_fail(ctx, e, "collecting emitters");
+    }
+  }
+  const uint32_t count = (uint32_t)(recs.size() / 3);
+  std::vector<uint32_t> idx(count), ids(count);
+  for (uint32_t i = 0; i < count; ++i) idx[i] = i;
+  auto face_of = [&](uint32_t i) { uint32_t f; std::memcpy(&f, &recs[3 * (size_t)i].w, 4); return f; };
+  std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return face_of(x) < face_of(y); });
+  std::vector<vt_emitter> em(count);
+  for (uint32_t j = 0; j < count; ++j) {
+    const float4 a = recs[3 * (size_t)idx[j]], b = recs[3 * (size_t)idx[j] + 1], c = recs[3 * (size_t)idx[j] + 2];
+    ids[j] = face_of(idx[j]);
+    vt_emitter &e = em[j];
+    std::memset(&e, 0, sizeof e);
+    const float av[3] = {a.x, a.y, a.z}, bv[3] = {b.x, b.y, b.z}, cv[3] = {c.x, c.y, c.z};
+    for (int k = 0; k < 3; ++k) { e.a[k] = av[k]; e.b[k] = bv[k]; e.c[k] = cv[k]; }
+    const double e1[3] = {double(bv[0] - av[0]), double(bv[1] - av[1]), double(bv[2] - av[2])};
+    const double e2[3] = {double(cv[0] - av[0]), double(cv[1] - av[1]), double(cv[2] - av[2])};
+    const double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+    uint32_t slot;
+    std::memcpy(&slot, &b.w, 4);
+    e.power = 0.5 * std::sqrt((cx * cx + cy * cy) + cz * cz) * double(emis[slot].w);
+    e.cos_emission = 0.0;
+  }
+  const vt_status st = vt_emitter_list_compute(ids.data(), em.data(), count, lightTree, sc->emitter_words, nullptr);
+  if (st != VT_OK) return vt_fail(ctx, st, "light tree exceeds 2^27 - 1 nodes");
+  VT_CUDA(ctx, cudaMalloc(&sc->d_emitters, sc->emitter_words.size() * sizeof(uint32_t)));
+  VT_CUDA(ctx, cudaMemcpy(sc->d_emitters, sc->emitter_words.data(), sc->emitter_words.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice));
+  return VT_OK;
+}
+
+// The emitter fields of the kernel arguments, from the packed list.
+void emitter_args(const vt_scene *sc, RenderArgs &A) {
+  A.imported = sc->imported ? 1u : 0u;
+  if (!sc->imported) return;
+  const std::vector<uint32_t> &w = sc->emitter_words;
+  A.emitters = sc->d_emitters;
+  A.emissions = sc->d_emissions;
+  A.facePos = sc->d_face_pos;
+  A.ecount = w[0];
+  if (A.ecount == 0) return;
+  const uint32_t c = A.ecount;
+  float total;
+  std::memcpy(&total, &w[2 * c + 1], 4);
+  A.etotal = total;
+  A.treeNodes = w[2 * c + 2];
+  if (A.treeNodes) {
+    A.ltNodes = reinterpret_cast<const uint4 *>(sc->d_emitters + w[2 * c + 3]);
+    A.ltLeaves = sc->d_emitters + w[2 * c + 4];
+    float g[6];
+    std::memcpy(g, &w[2 * c + 5], sizeof g);
+    A.ltLo = make_float3(g[0], g[1], g[2]);
+    A.ltScale = make_float3((g[3] - g[0]) / 65535.0f, (g[4] - g[1]) / 65535.0f, (g[5] - g[2]) / 65535.0f);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_status vt_scene_create(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
+                          const vt_quad_light *light, const vt_spectral_tables *tables, vt_scene **out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!out || !mesh || !light || (nmat && !materials)) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  *out = nullptr;
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  vt_scene *sc = new vt_scene();
+  sc->light = *light;
+  const vt_status st = scene_common(ctx, mesh, materials, nmat, light->emission, tables, sc);
+  if (st != VT_OK) { scene_free(sc); return st; }
   *out = sc;
+  return VT_OK;
+}
+
+vt_status vt_scene_create_imported(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
+                                   const vt_spectral_tables *tables, uint32_t light_tree, vt_scene **out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!out || !mesh || (nmat && !materials)) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  *out = nullptr;
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  vt_scene *sc = new vt_scene();
+  std::memset(&sc->light, 0, sizeof sc->light);
+  sc->imported = true;
+  vt_status st = scene_common(ctx, mesh, materials, nmat, nullptr, tables, sc);
+  if (st == VT_OK) st = build_emitters(ctx, sc, materials, nmat, light_tree != 0);
+  if (st != VT_OK) { scene_free(sc); return st; }
+  *out = sc;
+  return VT_OK;
+}
+
+vt_status vt_scene_emitter_words(vt_ctx *ctx, const vt_scene *scene, uint32_t *words, uint32_t capacity,
+                                 uint32_t *count) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !count) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  if (!scene->imported) return vt_fail(ctx, VT_ERR_INVALID, "the scene has a quad light, not an emitter list");
+  *count = (uint32_t)scene->emitter_words.size();
+  if (words) {
+    if (capacity < scene->emitter_words.size()) return vt_fail(ctx, VT_ERR_INVALID, "capacity below the word count");
+    std::copy(scene->emitter_words.begin(), scene->emitter_words.end(), words);
+  }
+  return VT_OK;
+}
+
+vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *points, uint32_t npoints,
+                            uint32_t per_point, uint32_t samples, float *out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !points || !out) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  if (!scene->imported) return vt_fail(ctx, VT_ERR_INVALID, "vt_light_estimate needs an imported scene");
+  const uint64_t threads = (uint64_t)npoints * per_point;
+  if (threads == 0 || threads > (1u << 24)) return vt_fail(ctx, VT_ERR_INVALID, "npoints * per_point must be 1 .. 2^24");
+  const vt_mesh *mesh = scene->mesh;
+  if (mesh->nfaces == 0) return vt_fail(ctx, VT_ERR_INVALID, "empty mesh");
+  if (mesh->depth > 32) return vt_fail(ctx, VT_ERR_LIMIT, "BVH deeper than the render stack");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RenderArgs A;
+  std::memset(&A, 0, sizeof A);
+  A.nodes = reinterpret_cast<const float4 *>(mesh->d_nodes);
+  A.tris = mesh->d_tris;
+  A.rootMax = mesh->root_max;
+  A.mats = scene->d_mats;
+  A.nmat = scene->nmat;
+  emitter_args(scene, A);
+  float4 *d_points = nullptr;
+  float *d_out = nullptr;
+  VT_CUDA(ctx, cudaMalloc(&d_points, npoints * sizeof(float4)));
+  cudaError_t e = cudaMalloc(&d_out, 8 * threads * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_points, points, npoints * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    k_light_estimate<<<(unsigned)((threads + 63) / 64), 64, 0, ctx->stream>>>(A, d_points, npoints, per_point, samples, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, 8 * threads * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d_points);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return vt_cuda_fail(ctx, e, "vt_light_estimate");
   return VT_OK;
 }
 
@@ -504,12 +1039,7 @@ vt_status vt_scene_destroy(vt_ctx *ctx, vt_scene *scene) {
   if (!scene) return VT_OK;
   if (ctx) cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
-  cudaFree(scene->d_mats);
-  cudaFree(scene->d_spec);
-  cudaFree(scene->d_icdf);
-  cudaFree(scene->d_accum);
-  cudaFree(scene->d_jitter);
-  delete scene;
+  scene_free(scene);
   return VT_OK;
 }
 
@@ -611,6 +1141,7 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.firstFrame = p->first_frame ? p->first_frame : scene->samples + 1u;
   A.jitter = scene->d_jitter;
   A.accum = scene->d_accum;
+  emitter_args(scene, A);
   // Enough (pixel, sample group) items to fill the GPU about four times over.
   const uint32_t npix = p->width * p->height;
   const uint64_t target = (uint64_t)ctx->sm_count * 2048u * 4u;

@@ -4,8 +4,11 @@
 
 #include "vt_internal.cuh"
 
+// The error of calls made without a context (context creation, host-only entry points).
+thread_local std::string g_no_ctx_error;
+
 vt_status vt_fail(vt_ctx *ctx, vt_status code, const std::string &msg) {
-  if (ctx) ctx->error = msg;
+  if (ctx) ctx->error = msg; else g_no_ctx_error = msg;
   return code;
 }
 
@@ -15,8 +18,6 @@ vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what) {
 }
 
 namespace {
-
-thread_local std::string g_no_ctx_error;
 
 void free_mesh(vt_mesh *m) {
   if (!m) return;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/vt.h"
 
@@ -49,8 +50,28 @@ struct vt_mesh {
   float *d_bin_box = nullptr;        // 8 per binary internal node (lo xyz, -, hi xyz, -)
 };
 
+// Light BVH (host words, LightTree.Built).
+struct vt_light_tree {
+  std::vector<uint32_t> words;
+  std::vector<int32_t> order;
+  std::vector<uint32_t> leaf_node;
+  uint32_t node_count = 0, depth = 0;
+  float grid_lo[3] = {0, 0, 0}, grid_hi[3] = {0, 0, 0};
+};
+vt_status vt_light_tree_compute(const vt_emitter *emitters, uint32_t count, uint32_t maxLeaf, double leafRatio,
+                                vt_light_tree &out);
+vt_status vt_emitter_list_compute(const uint32_t *ids, const vt_emitter *emitters, uint32_t count, bool lightTree,
+                                  std::vector<uint32_t> &words, vt_light_tree *treeOut);
+
 struct vt_scene {
   const vt_mesh *mesh = nullptr;
+  // Imported scenes (emissive triangles, no quad light): the packed emitter list, per slot
+  // (emission rgb, selection weight), and face -> BVH position.
+  bool imported = false;
+  uint32_t *d_emitters = nullptr;
+  std::vector<uint32_t> emitter_words;
+  float4 *d_emissions = nullptr;
+  int32_t *d_face_pos = nullptr;
   vt_material *d_mats = nullptr;
   uint32_t nmat = 0;
   vt_quad_light light;
@@ -90,6 +111,8 @@ inline uint32_t *vt_queue_slot(vt_ctx *ctx) {
 inline unsigned long long *vt_count_words(vt_ctx *ctx) {
   return reinterpret_cast<unsigned long long *>(ctx->d_counters + kQueueSlots * 8);
 }
+// A spare counter word after the accumulators (host-synchronised uses on the context stream).
+inline uint32_t *vt_scratch_word(vt_ctx *ctx) { return ctx->d_counters + kQueueSlots * 8 + 4; }
 
 // Device error word bits (ctx->d_status).
 enum : uint32_t {

@@ -76,14 +76,21 @@ def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=Tru
 
 
 class Scene:
-    """A renderable scene on the device (vt_scene): mesh, material slots, area light, spectral
-    tables and the FP64 accumulation."""
+    """A renderable scene on the device (vt_scene): mesh, material slots, the lights, spectral
+    tables and the FP64 accumulation.
 
-    def __init__(self, ctx: Context, mesh: Mesh, materials, light, spectral: dict | None = None):
+    With a quad `light` the scene is lit as the reference's procedural scenes (sample_direct_light's
+    quad branch). With light=None it is an imported scene (sceneIndex 6): every face whose slot is
+    emissive is an emitter, chosen by power or, with light_tree=True (the reference's default), by
+    walking the light tree."""
+
+    def __init__(self, ctx: Context, mesh: Mesh, materials, light=None, spectral: dict | None = None,
+                 light_tree: bool = True):
         lib = _lib.load()
         self.ctx, self.mesh = ctx, mesh
         self._mats = make_materials(materials)
-        self._light = make_light(light)
+        self.imported = light is None
+        self._light = None if light is None else make_light(light)
         tables = None
         if spectral is not None:
             self._cmf = np.ascontiguousarray(spectral["cmf_rgb"], np.float32)
@@ -92,11 +99,39 @@ class Scene:
             tables = SpectralTables(self._cmf.ctypes.data, self._illum.ctypes.data, self._icdf.ctypes.data,
                                     self._cmf.shape[0], self._icdf.shape[0] - 1, float(spectral["lambda_min"]), 0)
         p = C.c_void_p()
-        st = lib.vt_scene_create(ctx.handle, mesh._p, self._mats, len(materials), C.byref(self._light),
-                                 C.byref(tables) if tables is not None else None, C.byref(p))
-        _check(ctx.handle, st, "vt_scene_create")
+        tp = C.byref(tables) if tables is not None else None
+        if self.imported:
+            st = lib.vt_scene_create_imported(ctx.handle, mesh._p, self._mats, len(materials), tp,
+                                              1 if light_tree else 0, C.byref(p))
+            _check(ctx.handle, st, "vt_scene_create_imported")
+        else:
+            st = lib.vt_scene_create(ctx.handle, mesh._p, self._mats, len(materials), C.byref(self._light), tp,
+                                     C.byref(p))
+            _check(ctx.handle, st, "vt_scene_create")
         self._p = p
         self.width = self.height = 0
+
+    def emitter_words(self) -> np.ndarray:
+        """The packed emitter list of an imported scene (uint32 words)."""
+        lib = _lib.load()
+        n = C.c_uint32()
+        _check(self.ctx.handle, lib.vt_scene_emitter_words(self.ctx.handle, self._p, None, 0, C.byref(n)),
+               "vt_scene_emitter_words")
+        out = np.empty(n.value, np.uint32)
+        _check(self.ctx.handle, lib.vt_scene_emitter_words(self.ctx.handle, self._p, out.ctypes.data, n.value,
+                                                           C.byref(n)), "vt_scene_emitter_words")
+        return out
+
+    def light_estimate(self, points, per_point: int, samples: int = 64) -> np.ndarray:
+        """The reference's lt_estimate check on the device: (npoints * per_point, 8) float32 per
+        thread (sum, squares, hits, zero pdfs, max pdf error, back-facing choices, 0, 0)."""
+        pts = np.zeros((len(points), 4), np.float32)
+        pts[:, :3] = np.asarray(points, np.float32)[:, :3]
+        out = np.empty((len(points) * per_point, 8), np.float32)
+        _check(self.ctx.handle, _lib.load().vt_light_estimate(self.ctx.handle, self._p, pts.ctypes.data, len(points),
+                                                              int(per_point), int(samples), out.ctypes.data),
+               "vt_light_estimate")
+        return out
 
     def render(self, params: FrameParams, spp: int, stream=None) -> None:
         """Adds `spp` frames (one sample per pixel each) to the accumulation; stream-ordered."""

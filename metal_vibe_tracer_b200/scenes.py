@@ -211,3 +211,77 @@ def cornell_box(light_radiance: float = 17.0, seed: int = 0):
     camera = {"pos": tuple(float(x) for x in eye.astype(np.float32)), "target": tuple(float(x) for x in target), "up": (0.0, 1.0, 0.0),
               "fov": 42.0}
     return faces, verts, materials, light, camera
+
+
+def _mesh_from_triangles(tris, tags):
+    n = len(tris)
+    verts = np.zeros(3 * n, VERTEX_DTYPE)
+    verts["p"] = np.array(tris, np.float64).reshape(-1, 3).astype(np.float32)
+    faces = np.zeros(n, FACE_DTYPE)
+    i = np.arange(n, dtype=np.uint32)
+    faces["a"], faces["b"], faces["c"] = 3 * i, 3 * i + 1, 3 * i + 2
+    faces["tag"] = np.array(tags, np.uint32)
+    return faces, verts
+
+
+def ceiling_lights(rows: int = 24, up_row: int = 12):
+    """The light-tree check's emitters (tests/Fix_light-tree.swift:38-51): a rows x rows grid of
+    0.3-sided right triangles at y = 3 facing down (x = -24 + 2i, z = -24 + 2j; slot 1 where
+    (i + j) % 3 == 0, else slot 0) and a row of `up_row` facing up (x = -23 + 4i, z = 0.9, slot 0).
+    Slot 0 emits (5, 5, 5), slot 1 (1, 4, 2). Returns faces, vertices, materials."""
+    s = 0.3
+    tris, tags = [], []
+
+    def emitter(x, z, slot, down):
+        a, b, c = (x, 3.0, z), (x + s, 3.0, z), (x, 3.0, z + s)
+        tris.append((a, b, c) if down else (a, c, b))
+        tags.append(slot)
+
+    for i in range(rows):
+        for j in range(rows):
+            emitter(-24 + 2 * i, -24 + 2 * j, 1 if (i + j) % 3 == 0 else 0, True)
+    for i in range(up_row):
+        emitter(-23 + 4 * i, 0.9, 0, False)
+    faces, verts = _mesh_from_triangles(tris, tags)
+    materials = [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (5.0, 5.0, 5.0)},
+                 {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (1.0, 4.0, 2.0)}]
+    return faces, verts, materials
+
+
+def lamp(count: int = 6):
+    """One lamp: `count` coincident downward triangles at (1, 3, 1) (tests/Fix_light-tree.swift:170)."""
+    s = 0.3
+    tris = [((1.0, 3.0, 1.0), (1.0 + s, 3.0, 1.0), (1.0, 3.0, 1.0 + s))] * count
+    faces, verts = _mesh_from_triangles(tris, [0] * count)
+    return faces, verts, [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (5.0, 5.0, 5.0)}]
+
+
+def cornell_emitters(grid: int = 4, seed: int = 0, lamps: bool = True):
+    """The Cornell box lit by emitter triangles (an imported scene): the ceiling light split into a
+    grid x grid array of quads (radiance 17) plus, with `lamps`, two small lamps on the back wall
+    facing the camera (radiance 6 and 40, each 0.1 x 0.1). All emitters are grey. Returns faces,
+    vertices, materials and the camera."""
+    faces, verts, materials, light, camera = cornell_box(seed=seed)
+    p = verts["p"].reshape(-1, 3, 3).astype(np.float64)
+    keep = faces["tag"] != 7
+    tris = [tuple(map(tuple, t)) for t in p[keep]]
+    tags = list(faces["tag"][keep])
+
+    def quad(c, u, v, tag):
+        c, u, v = np.array(c, float), np.array(u, float), np.array(v, float)
+        tris.extend([(tuple(c), tuple(c + u), tuple(c + u + v)), (tuple(c), tuple(c + u + v), tuple(c + v))])
+        tags.extend([tag, tag])
+
+    step = 0.25 / grid
+    for i in range(grid):
+        for j in range(grid):
+            quad((-0.125 + i * step, 0.999, -0.125 + j * step), (step, 0, 0), (0, 0, step), 7)
+    if lamps:
+        quad((0.5, 0.2, 0.999), (0, 0.1, 0), (0.1, 0, 0), 8)     # facing -z
+        quad((-0.7, -0.3, 0.999), (0, 0.1, 0), (0.1, 0, 0), 9)
+    faces, verts = _mesh_from_triangles(tris, tags)
+    materials = materials[:7] + [
+        {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (17.0,) * 3},
+        {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (6.0,) * 3},
+        {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (40.0,) * 3}]
+    return faces, verts, materials, camera

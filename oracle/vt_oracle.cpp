@@ -7,6 +7,7 @@
 #include "vt_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -952,7 +953,8 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
 }
 
 template <typename T>
-bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, uint64_t *tests = nullptr) {
+bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, uint64_t *tests = nullptr,
+             bool slack = false) {
   if (h.nodes.empty()) return false;
   WRay<T> w = make_wray(r.o, r.d);
   SlabRay<T> s = make_slab(r, T(h.root_max));
@@ -974,7 +976,15 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
           c[3] = {T(tf[6]), T(tf[7]), T(tf[8])};
         T t, b1, b2;
         if (tests) ++*tests;
-        if (intersect_tri<T>(w, a, b, c, r.tmin, r.tmax, t, b1, b2)) return true;
+        // Imported scenes take each triangle's rounding bound off tMax (scene_occluded,
+        // main.swift:2066-2069; mesh_hit_error, :1353-1355).
+        T tmax = r.tmax;
+        if (slack) {
+          T m = 0;
+          for (int k = 0; k < 3; ++k) m = std::max(m, std::max(std::fabs(a[k]), std::max(std::fabs(b[k]), std::fabs(c[k]))));
+          tmax = r.tmax - std::max(T(1e-7), T(1.907349e-6) * m);
+        }
+        if (intersect_tri<T>(w, a, b, c, r.tmin, tmax, t, b1, b2)) return true;
       }
     }
   }
@@ -1301,7 +1311,21 @@ struct PtContext {
   D3 cam, fwd, right, up;
   double aspect, fovScale, larea;
   bool spectral;
+  // Imported scenes: per slot (emission rgb, selection weight), the packed emitter list.
+  bool imported = false;
+  std::vector<std::array<double, 4>> emis;
+  const uint32_t *E = nullptr;
+  uint32_t ecount = 0, treeNodes = 0;
+  double etotal = 0;
+  const uint32_t *ltNodes = nullptr, *ltLeaves = nullptr;
+  double ltLo[3] = {0, 0, 0}, ltScale[3] = {0, 0, 0};
 };
+
+inline double fword(uint32_t w) { float f; std::memcpy(&f, &w, 4); return f; }
+inline double max_abs_d(D3 p) { return std::max(std::fabs(p.x), std::max(std::fabs(p.y), std::fabs(p.z))); }
+// ray_epsilon / ray_t_min (main.swift:1343-1345, 1362-1364).
+inline double ray_eps_d(const PtContext &C, D3 p) { return C.imported ? std::max(1e-7, 9.536743e-7 * max_abs_d(p)) : kEpsPt; }
+inline double ray_tmin_d(const PtContext &C, D3 o) { return C.imported ? ray_eps_d(C, o) * 0.25 : kEpsPt; }
 
 struct PtLanes { int bin[4]; double w[4]; };
 
@@ -1350,22 +1374,40 @@ inline double smax(const PtContext &C, const Spec4 &a) {
   return C.spectral ? std::max(m, a.v[3]) : m;
 }
 
-struct PtHit { D3 pos, gn; uint32_t slot; };
+struct PtHit { D3 pos, gn; double err; uint32_t slot, face; bool front; };
 
+struct PtTri { D3 a, b, c; uint32_t slot; };
+PtTri pt_triangle(const PtContext &C, uint32_t face) {
+  const vt_face &f = C.in->faces[face];
+  return {d3(&C.in->verts[f.a].px), d3(&C.in->verts[f.b].px), d3(&C.in->verts[f.c].px), f.tag};
+}
+// mesh_hit_error (main.swift:1353-1355).
+double mesh_hit_error_d(const PtTri &t) {
+  return std::max(1e-7, 1.907349e-6 * std::max(max_abs_d(t.a), std::max(max_abs_d(t.b), max_abs_d(t.c))));
+}
+
+// The hit record: imported scenes rebuild the point from barycentrics (main.swift:2025-2028).
 bool pt_closest(const PtContext &C, D3 o, D3 d, PtHit &h) {
   TraceRay<double> r;
   r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
   r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
-  r.tmin = kEpsPt; r.tmax = INFINITY;
-  double t, b1, b2;
+  r.tmin = ray_tmin_d(C, o); r.tmax = INFINITY;
+  double t = 0, b1 = 0, b2 = 0;
   int prim = -1;
   if (!closest_hit<double>(*C.bvh, r, t, prim, b1, b2)) return false;
-  const vt_face &f = C.in->faces[prim];
-  const D3 a = d3(&C.in->verts[f.a].px), b = d3(&C.in->verts[f.b].px), c = d3(&C.in->verts[f.c].px);
-  h.pos = o + d * t;
-  const D3 ng = normalize(cross(b - a, c - a));
-  h.gn = dot(ng, d) < 0.0 ? ng : ng * -1.0;
-  h.slot = f.tag;
+  const PtTri tri = pt_triangle(C, (uint32_t)prim);
+  const D3 ng = normalize(cross(tri.b - tri.a, tri.c - tri.a));
+  h.front = dot(ng, d) < 0.0;
+  h.gn = h.front ? ng : ng * -1.0;
+  h.slot = tri.slot;
+  h.face = (uint32_t)prim;
+  if (C.imported) {
+    h.pos = tri.a * (1.0 - b1 - b2) + tri.b * b1 + tri.c * b2;
+    h.err = mesh_hit_error_d(tri);
+  } else {
+    h.pos = o + d * t;
+    h.err = kEpsPt;
+  }
   return true;
 }
 
@@ -1373,8 +1415,8 @@ bool pt_occluded(const PtContext &C, D3 o, D3 d, double tmax) {
   TraceRay<double> r;
   r.o[0] = o.x; r.o[1] = o.y; r.o[2] = o.z;
   r.d[0] = d.x; r.d[1] = d.y; r.d[2] = d.z;
-  r.tmin = kEpsPt; r.tmax = tmax;
-  return any_hit<double>(*C.bvh, r);
+  r.tmin = ray_tmin_d(C, o); r.tmax = tmax;
+  return any_hit<double>(*C.bvh, r, nullptr, nullptr, C.imported);
 }
 
 vt_material pt_material(const PtContext &C, uint32_t slot) {
@@ -1384,7 +1426,11 @@ vt_material pt_material(const PtContext &C, uint32_t slot) {
   return m;
 }
 
-inline D3 ray_origin_d(D3 p, D3 gn, D3 dir) { return p + gn * (dot(dir, gn) >= 0.0 ? kEpsPt : -kEpsPt); }
+// ray_origin (main.swift:1366-1369).
+inline D3 ray_origin_d(const PtContext &C, D3 p, D3 gn, D3 dir, double err) {
+  const double offset = std::max(err, ray_eps_d(C, p));
+  return p + gn * (dot(dir, gn) >= 0.0 ? offset : -offset);
+}
 
 double power_heuristic_d(double pf, double pg) {
   const double s = std::max(pf, pg);
@@ -1393,10 +1439,12 @@ double power_heuristic_d(double pf, double pg) {
   return f * f / (f * f + g * g);
 }
 
-struct PtLight { D3 pos, wi; double dist, pdf; };
+struct PtLight { D3 pos, wi, emission; double dist, pdf; uint32_t face; };
 
 PtLight sample_light_d(const PtContext &C, D3 p, ZSampler &seed) {
   PtLight ls{};
+  ls.face = 0xffffffffu;
+  ls.emission = d3(C.in->light.emission);
   const vt_quad_light &l = C.in->light;
   double u, v;
   seed.f2(u, v);
@@ -1417,20 +1465,205 @@ double light_pdf_d(const PtContext &C, D3 p, D3 hit) {
   return cos_l <= 0.0 ? 0.0 : dist * dist / (C.larea * cos_l);
 }
 
-bool visible_d(const PtContext &C, D3 p, D3 gn, const PtLight &ls) {
+// ---- emitter triangles (imported scenes): power sampling and the light tree -------------------
+// imported_geometry (main.swift:2721-2725).
+double imported_geometry_d(D3 p, D3 position, const PtTri &t) {
+  const D3 d = position - p;
+  const double d2 = dot(d, d);
+  const D3 n = cross(t.b - t.a, t.c - t.a);
+  return d2 > 1e-12 && dot(n, n) > 1e-20 ? std::max(0.0, dot(normalize(n), d * (-1.0 / std::sqrt(d2)))) / d2 : 0.0;
+}
+double triangle_area_d(const PtTri &t) { const D3 n = cross(t.b - t.a, t.c - t.a); return 0.5 * std::sqrt(dot(n, n)); }
+
+struct PtLtNode { D3 lo, hi, w; double phi, cosO, cosE; uint32_t child, parent, count; };
+
+// light_tree_axis / light_tree_node (main.swift:2751-2778), decoded in double.
+D3 lt_axis_d(uint32_t q) {
+  const double fx = double(q & 0xffffu) / 65535.0 * 2.0 - 1.0, fy = double(q >> 16) / 65535.0 * 2.0 - 1.0;
+  D3 v{fx, fy, 1.0 - std::fabs(fx) - std::fabs(fy)};
+  if (v.z < 0.0) {
+    const double vx = (1.0 - std::fabs(v.y)) * (v.x >= 0.0 ? 1.0 : -1.0), vy = (1.0 - std::fabs(v.x)) * (v.y >= 0.0 ? 1.0 : -1.0);
+    v.x = vx;
+    v.y = vy;
+  }
+  return normalize(v);
+}
+PtLtNode lt_node_d(const PtContext &C, uint32_t i) {
+  const uint32_t *a = C.ltNodes + 8 * (size_t)i, *b = a + 4;
+  PtLtNode n;
+  n.w = lt_axis_d(a[0]);
+  n.phi = fword(a[1]);
+  n.cosO = double(a[2] & 0xffffu) / 65535.0 * 2.0 - 1.0;
+  n.cosE = double(a[2] >> 16) / 65535.0 * 2.0 - 1.0;
+  n.lo = {C.ltLo[0] + double(a[3] & 0xffffu) * C.ltScale[0], C.ltLo[1] + double(a[3] >> 16) * C.ltScale[1],
+          C.ltLo[2] + double(b[0] & 0xffffu) * C.ltScale[2]};
+  n.hi = {C.ltLo[0] + double(b[0] >> 16) * C.ltScale[0], C.ltLo[1] + double(b[1] & 0xffffu) * C.ltScale[1],
+          C.ltLo[2] + double(b[1] >> 16) * C.ltScale[2]};
+  n.child = b[2];
+  n.parent = b[3] & 0x7ffffffu;
+  n.count = b[3] >> 27;
+  return n;
+}
+uint32_t lt_leaf_word_d(const PtContext &C, uint32_t position, uint32_t k) { return C.ltLeaves[3 * (size_t)position + k]; }
+double lt_leaf_sum_d(const PtContext &C, const PtLtNode &n) {
+  double sum = 0.0;
+  for (uint32_t i = 0; i < n.count; ++i) sum += fword(lt_leaf_word_d(C, n.child + i, 1u));
+  return sum;
+}
+double cos_sub_clamped_d(double sinA, double cosA, double sinB, double cosB) { return cosA > cosB ? 1.0 : cosA * cosB + sinA * sinB; }
+double sin_sub_clamped_d(double sinA, double cosA, double sinB, double cosB) { return cosA > cosB ? 0.0 : sinA * cosB - cosA * sinB; }
+
+// light_tree_importance (main.swift:2788-2805).
+double lt_importance_d(const PtLtNode &n, D3 p) {
+  if (!(n.phi > 0.0)) return 0.0;
+  const D3 pc = (n.lo + n.hi) * 0.5, dp = p - pc, ext = n.hi - n.lo;
+  const double dist2 = dot(dp, dp);
+  const double d2 = std::max(dist2, std::max(0.5 * std::sqrt(dot(ext, ext)), 1e-20));
+  if (p.x >= n.lo.x && p.y >= n.lo.y && p.z >= n.lo.z && p.x <= n.hi.x && p.y <= n.hi.y && p.z <= n.hi.z) return n.phi / d2;
+  const D3 wi = dp * (1.0 / std::sqrt(dist2));
+  const double cosW = dot(n.w, wi), sinW = std::sqrt(std::max(0.0, 1.0 - cosW * cosW));
+  const D3 dh = pc - n.hi;
+  const double s2 = dot(dh, dh) / dist2;
+  const double cosB = s2 >= 1.0 ? -1.0 : std::sqrt(std::max(0.0, 1.0 - s2)), sinB = std::sqrt(std::max(0.0, 1.0 - cosB * cosB));
+  const double sinO = std::sqrt(std::max(0.0, 1.0 - n.cosO * n.cosO));
+  const double cosX = cos_sub_clamped_d(sinW, cosW, sinO, n.cosO), sinX = sin_sub_clamped_d(sinW, cosW, sinO, n.cosO);
+  const double cosP = cos_sub_clamped_d(sinX, cosX, sinB, cosB);
+  return cosP <= n.cosE ? 0.0 : n.phi * cosP / d2;
+}
+
+// light_tree_sample (main.swift:2809-2833).
+uint32_t lt_sample_d(const PtContext &C, D3 p, double u, double &pmf) {
+  const double below1 = 1.0 - 1.0 / 16777216.0;
+  pmf = 1.0;
+  uint32_t index = 0;
+  for (uint32_t depth = 0; depth <= 64u; ++depth) {
+    const PtLtNode n = lt_node_d(C, index);
+    if (n.count != 0u) {
+      const double sum = lt_leaf_sum_d(C, n), target = u * sum;
+      double cumulative = 0.0, chosen = 0.0;
+      uint32_t position = 0xffffffffu;
+      for (uint32_t i = 0; i < n.count && sum > 0.0; ++i) {
+        const double power = fword(lt_leaf_word_d(C, n.child + i, 1u));
+        if (!(power > 0.0)) continue;
+        position = n.child + i;
+        chosen = power;
+        cumulative += power;
+        if (target < cumulative) break;
+      }
+      if (position == 0xffffffffu) break;
+      pmf *= chosen / sum;
+      return position;
+    }
+    const double l = lt_importance_d(lt_node_d(C, index + 1u), p), r = lt_importance_d(lt_node_d(C, n.child), p);
+    if (!(l + r > 0.0)) break;
+    const double pl = l / (l + r);
+    if (u < pl) { u = std::min(u / pl, below1); index = index + 1u; pmf *= pl; }
+    else { u = std::min((u - pl) / (1.0 - pl), below1); index = n.child; pmf *= r / (l + r); }
+  }
+  pmf = 0.0;
+  return 0xffffffffu;
+}
+
+// light_tree_pmf (main.swift:2835-2850).
+double lt_pmf_d(const PtContext &C, D3 p, uint32_t position) {
+  uint32_t index = lt_leaf_word_d(C, position, 2u);
+  PtLtNode node = lt_node_d(C, index);
+  const double sum = lt_leaf_sum_d(C, node);
+  double pmf = sum > 0.0 ? fword(lt_leaf_word_d(C, position, 1u)) / sum : 0.0;
+  for (uint32_t depth = 0; depth <= 64u && pmf > 0.0; ++depth) {
+    const uint32_t parent = node.parent;
+    if (parent == 0x7ffffffu) return pmf;
+    const PtLtNode up = lt_node_d(C, parent);
+    const double l = lt_importance_d(lt_node_d(C, parent + 1u), p), r = lt_importance_d(lt_node_d(C, up.child), p);
+    const double mine = index == parent + 1u ? l : r;
+    if (!(l + r > 0.0) || !(mine > 0.0)) return 0.0;
+    pmf *= mine / (l + r);
+    index = parent;
+    node = up;
+  }
+  return 0.0;
+}
+
+uint32_t emitter_position_d(const PtContext &C, uint32_t face) {
+  const uint32_t *ids = C.E + 1;
+  const uint32_t *it = std::lower_bound(ids, ids + C.ecount, face);
+  return it != ids + C.ecount && *it == face ? C.E[1 + C.ecount + (it - ids)] : 0xffffffffu;
+}
+
+// imported_emitter_area_pdf (main.swift:2859-2869).
+double emitter_area_pdf_d(const PtContext &C, uint32_t face, D3 p, const PtTri &t) {
+  if (C.ecount == 0) return 0.0;
+  if (C.treeNodes > 0) {
+    const uint32_t position = emitter_position_d(C, face);
+    const double area = triangle_area_d(t);
+    return position != 0xffffffffu && area > 0.0 ? lt_pmf_d(C, p, position) / area : 0.0;
+  }
+  return C.etotal > 0.0 && t.slot < C.emis.size() ? C.emis[t.slot][3] / C.etotal : 0.0;
+}
+
+// sample_direct_light's emitter branch (main.swift:2892-2920), emitter probability 1.
+PtLight sample_emitters_d(const PtContext &C, D3 p, ZSampler &seed) {
+  PtLight ls{};
+  ls.face = 0xffffffffu;
+  if (C.ecount == 0) return ls;
+  (void)seed.f1();
+  double qx, qy, qz;
+  seed.f3(qx, qy, qz);
+  const bool tree = C.treeNodes > 0;
+  double pmf = 0.0;
+  uint32_t face;
+  if (tree) {
+    const uint32_t position = lt_sample_d(C, p, qx, pmf);
+    if (position == 0xffffffffu) return ls;
+    face = lt_leaf_word_d(C, position, 0u);
+  } else {
+    uint32_t low = 0, high = C.ecount - 1;
+    while (low < high) {
+      const uint32_t middle = (low + high) / 2;
+      if (fword(C.E[1 + C.ecount + middle]) >= qx) high = middle; else low = middle + 1;
+    }
+    face = C.E[1 + low];
+  }
+  const PtTri t = pt_triangle(C, face);
+  const double root = std::sqrt(qy);
+  ls.pos = t.a * (1.0 - root) + t.b * (root * (1.0 - qz)) + t.c * (root * qz);
+  const D3 delta = ls.pos - p;
+  ls.dist = std::sqrt(dot(delta, delta));
+  ls.wi = delta * (1.0 / std::max(ls.dist, 1e-8));
+  const double geometry = imported_geometry_d(p, ls.pos, t);
+  ls.emission = t.slot < C.emis.size() ? D3{C.emis[t.slot][0], C.emis[t.slot][1], C.emis[t.slot][2]} : D3{0, 0, 0};
+  ls.face = face;
+  const double area = tree ? triangle_area_d(t) : 0.0;
+  const double areaPdf = !tree ? emitter_area_pdf_d(C, face, p, t) : (area > 0.0 ? pmf / area : 0.0);
+  ls.pdf = geometry > 1e-12 ? areaPdf / geometry : 0.0;
+  return ls;
+}
+
+// eval_light_pdf for imported emitters (main.swift:3066-3071).
+double emitter_pdf_d(const PtContext &C, D3 p, D3 hitPos, uint32_t face) {
+  if (C.ecount == 0) return 0.0;
+  const PtTri t = pt_triangle(C, face);
+  const double g = imported_geometry_d(p, hitPos, t);
+  return g > 1e-12 ? emitter_area_pdf_d(C, face, p, t) / g : 0.0;
+}
+
+// light_visible (main.swift:3254-3264) with endpoint_tolerance (main.swift:1358-1361).
+bool visible_d(const PtContext &C, D3 p, D3 gn, double err, const PtLight &ls) {
   if (!(ls.pdf > 0.0)) return false;
-  const D3 o = ray_origin_d(p, gn, ls.wi);
+  const D3 o = ray_origin_d(C, p, gn, ls.wi, err);
   D3 delta = ls.pos - o;
-  const double d = std::sqrt(dot(delta, delta)), tol = 2.0 * kEpsPt;
+  const double d = std::sqrt(dot(delta, delta));
+  const double legacy = 2.0 * ray_eps_d(C, ls.pos);
+  const double tol = C.imported ? std::max(legacy, 1.907349e-6 * (max_abs_d(o) + max_abs_d(ls.pos) + d)) : legacy;
   if (d <= tol) return false;
   return !pt_occluded(C, o, delta * (1.0 / d), d - tol);
 }
 
-D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 wo, const Spec4 &T, const Spec4 &albedo,
+D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, double err, D3 wo, const Spec4 &T, const Spec4 &albedo,
             bool useMIS, ZSampler &seed, bool requirePdf) {
-  const PtLight ls = sample_light_d(C, p, seed);
+  const PtLight ls = C.imported ? sample_emitters_d(C, p, seed) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
-  if (!visible_d(C, p, n, ls)) return {0, 0, 0};
+  if (!visible_d(C, p, n, err, ls)) return {0, 0, 0};
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
   double f = 0.0, bpdf = 0.0;
   if (no > 0.0) {
@@ -1438,7 +1671,8 @@ D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 wo, const Spec4
     if (ni > 0.0 && cosine >= 1e-7) f = 1.0 / kPi;
   }
   const double w = useMIS ? power_heuristic_d(ls.pdf, bpdf) : 1.0;
-  return to_rgb(C, L, scale(mul(mul(T, albedo), emission(C, L, C.in->light.emission)), f * cosine * w / ls.pdf));
+  const float le[3] = {(float)ls.emission.x, (float)ls.emission.y, (float)ls.emission.z};
+  return to_rgb(C, L, scale(mul(mul(T, albedo), emission(C, L, le)), f * cosine * w / ls.pdf));
 }
 
 void make_basis_d(D3 n, D3 &u, D3 &v) {
@@ -1462,14 +1696,18 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
   if (!hit0) return {0, 0, 0};
   vt_material m = pt_material(C, h.slot);
-  if (m.type == VT_MAT_EMISSIVE) return {m.emission[0], m.emission[1], m.emission[2]};
+  if (m.type == VT_MAT_EMISSIVE) {
+    // emitter_rgb (main.swift:7467-7468): the four-wavelength estimate in spectral transport.
+    if (C.imported && !h.front) return {0, 0, 0};
+    return to_rgb(C, L, emission(C, L, m.emission));
+  }
   const int limit = std::max(0, (int)C.p->max_depth - 1);
   const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode == 1u;
   Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
   D3 R{0, 0, 0};
   if (nee) {
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.gn, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
+    R = direct_d(C, L, h.pos, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
   }
   int scattering = 0;
   bool emissionOnly = false;
@@ -1494,19 +1732,19 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
     for (double t : T.v) finite = finite && std::isfinite(t);
     if (!finite || smax(C, T) <= 0.0) break;
     const D3 prev = h.pos;
-    const D3 o = ray_origin_d(h.pos, h.gn, nd);
+    const D3 o = ray_origin_d(C, h.pos, h.gn, nd, h.err);
     if (!pt_closest(C, o, nd, h)) break;
     m = pt_material(C, h.slot);
     if (m.type == VT_MAT_EMISSIVE) {
-      const double lpdf = light_pdf_d(C, prev, h.pos);
+      const double lpdf = C.imported ? emitter_pdf_d(C, prev, h.pos, h.face) : light_pdf_d(C, prev, h.pos);
       const double w = !nee || lpdf <= 0.0 ? 1.0 : (mis ? power_heuristic_d(bpdf, lpdf) : 0.0);
-      R = R + to_rgb(C, L, scale(mul(T, emission(C, L, m.emission)), w));
+      if (!C.imported || h.front) R = R + to_rgb(C, L, scale(mul(T, emission(C, L, m.emission)), w));
       break;
     }
     if (emissionOnly) break;
     if (nee) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.gn, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
+      R = R + direct_d(C, L, h.pos, h.gn, h.err, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
     }
     if (bounce > 3) {
       const double survival = std::min(std::max(smax(C, T), 0.05), 0.95);
@@ -1536,6 +1774,34 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
   C.aspect = double(p->width) / p->height;
   C.fovScale = std::tan(p->fov_deg * 0.5 * kPi / 180.0);
   C.larea = std::sqrt(dot(cross(d3(in->light.su), d3(in->light.sv)), cross(d3(in->light.su), d3(in->light.sv))));
+  C.imported = in->imported != 0;
+  if (C.imported) {
+    // Per slot (rgb, selection weight max(1e-8, luminance) in float, main.swift:9303-9306).
+    C.emis.assign(in->nmat, {0, 0, 0, 0});
+    for (uint32_t i = 0; i < in->nmat; ++i) {
+      const vt_material &mm = in->materials[i];
+      if (mm.type != VT_MAT_EMISSIVE) continue;
+      const float *e = mm.emission;
+      const bool lit = double(e[0]) * e[0] + double(e[1]) * e[1] + double(e[2]) * e[2] > 0;
+      const float lum = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2];
+      C.emis[i] = {e[0], e[1], e[2], lit ? double(std::max(1e-8f, lum)) : 0.0};
+    }
+    C.E = in->emitters;
+    C.ecount = in->nemitter_words ? in->emitters[0] : 0;
+    if (C.ecount) {
+      const uint32_t c = C.ecount;
+      C.etotal = fword(C.E[2 * c + 1]);
+      C.treeNodes = C.E[2 * c + 2];
+      if (C.treeNodes) {
+        C.ltNodes = C.E + C.E[2 * c + 3];
+        C.ltLeaves = C.E + C.E[2 * c + 4];
+        for (int k = 0; k < 3; ++k) {
+          C.ltLo[k] = fword(C.E[2 * c + 5 + k]);
+          C.ltScale[k] = (fword(C.E[2 * c + 8 + k]) - C.ltLo[k]) / 65535.0;
+        }
+      }
+    }
+  }
   std::vector<float> jx(spp), jy(spp);
   for (uint32_t k = 0; k < spp; ++k) {
     const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;

@@ -90,6 +90,11 @@ typedef struct vto_pt_inputs {
   const float *icdf;      /* segments + 1 */
   uint32_t nbins, segments;
   float lambda_min;
+  /* Imported scenes (emitter triangles instead of the quad light): the packed emitter list
+   * (vt_emitter_list_pack layout, ids = face indices); imported = 0 selects the quad light. */
+  const uint32_t *emitters;
+  uint32_t nemitter_words;
+  uint32_t imported;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

@@ -231,15 +231,20 @@ class PtInputs(C.Structure):
     _fields_ = [("faces", C.c_void_p), ("nfaces", C.c_uint32), ("verts", C.c_void_p), ("nverts", C.c_uint32),
                 ("materials", C.c_void_p), ("nmat", C.c_uint32), ("light", QuadLight),
                 ("cmf_rgb", C.c_void_p), ("illum", C.c_void_p), ("icdf", C.c_void_p),
-                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float)]
+                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float),
+                ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
 
 
 def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
-           spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1):
-    """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames."""
+           spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1, light_tree=True,
+           emitter_words=None):
+    """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames.
+
+    light=None renders an imported scene lit by its emissive faces; its emitter list is the
+    pure-Python restatement's (oracle/light_tree.py) unless `emitter_words` is given."""
     lib = load()
     if not hasattr(lib.vto_render, "_typed"):
         lib.vto_render.restype, lib.vto_render.argtypes = _SIGS["vto_render"]
@@ -251,11 +256,19 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         mats[i].albedo[:] = [float(x) for x in m["albedo"]]
         mats[i].emission[:] = [float(x) for x in m["emission"]]
     q = QuadLight()
-    for k in ("corner", "su", "sv", "normal", "emission"):
-        getattr(q, k)[:] = [float(x) for x in light[k]]
+    if light is not None:
+        for k in ("corner", "su", "sv", "normal", "emission"):
+            getattr(q, k)[:] = [float(x) for x in light[k]]
     inp = PtInputs(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0], C.cast(mats, C.c_void_p), len(materials), q,
-                   None, None, None, 0, 0, 0.0)
+                   None, None, None, 0, 0, 0.0, None, 0, 0)
     keep = []
+    if light is None:
+        if emitter_words is None:
+            from . import light_tree as LT
+            emitter_words = LT.emitter_list(*LT.scene_emitters(faces, verts, materials), light_tree=light_tree)
+        words = np.ascontiguousarray(emitter_words, np.uint32)
+        keep.append(words)
+        inp.emitters, inp.nemitter_words, inp.imported = words.ctypes.data, len(words), 1
     if spectral is not None:
         cmf = np.ascontiguousarray(spectral["cmf_rgb"], np.float32)
         ill = np.ascontiguousarray(spectral["illum"], np.float32)

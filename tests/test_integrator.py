@@ -69,8 +69,29 @@ def test_spectral_grey_scene_converges_to_rgb(oracle):
     np.testing.assert_allclose(spec, rgb, rtol=0.01)
 
 
-def test_camera_sees_the_emitter_exactly(oracle):
+def test_camera_sees_the_emitter(oracle):
+    """RGB transport returns the emitter's radiance; spectral transport its four-wavelength estimate
+    (emitter_rgb, main.swift:7467-7468), whose mean over the emitter's pixels is the radiance (D65
+    is the sRGB white)."""
     faces, verts, mats, light, cam = scenes.cornell_box()
-    img = oracle.render(faces, verts, mats, light, cam, 256, 256, 4, spectral=spectral())
-    assert img.max() == pytest.approx(17.0)
-    assert np.isfinite(img).all() and img.min() >= 0.0
+    rgb = oracle.render(faces, verts, mats, light, cam, 256, 256, 64)
+    assert rgb.max() == pytest.approx(17.0)
+    lit = np.all(rgb == 17.0, axis=-1)   # every sample of these pixels sees the emitter
+    assert lit.sum() >= 20
+    img = oracle.render(faces, verts, mats, light, cam, 256, 256, 64, spectral=spectral())
+    np.testing.assert_allclose(img[lit].mean(0), 17.0, rtol=0.02)
+    assert np.isfinite(img).all()
+
+
+def test_imported_scene_tree_and_power_agree(oracle):
+    """Light-tree and power selection estimate the same image of the emitter-lit Cornell box, and,
+    without the wall lamps, the same image as the quad light (LightTree: unbiased selection)."""
+    faces, verts, mats, cam = scenes.cornell_emitters()
+    a = oracle.render(faces, verts, mats, None, cam, 48, 32, 256, light_tree=True)
+    b = oracle.render(faces, verts, mats, None, cam, 48, 32, 256, light_tree=False)
+    assert abs(a.mean() / b.mean() - 1) < 0.02
+    faces, verts, mats, cam = scenes.cornell_emitters(lamps=False)
+    c = oracle.render(faces, verts, mats, None, cam, 48, 32, 256)
+    qf, qv, qm, light, _ = scenes.cornell_box()
+    d = oracle.render(qf, qv, qm, light, cam, 48, 32, 256)
+    assert abs(c.mean() / d.mean() - 1) < 0.02
