@@ -364,13 +364,15 @@ def main():
             peak_src = "measured"
         except Exception:
             pass
+    # DRAM bytes per launch of the dominant kernel, from the committed ncu summary (one capture on a
+    # smaller launch, scaled by the ray count).
     traffic = None
-    tpath = ROOT / "profiles" / "traffic.json"
+    tpath = ROOT / "profiles" / "dram_traffic.txt"
     if tpath.exists():
-        try:
-            traffic = json.loads(tpath.read_text()).get(names[dom])
-        except Exception:
-            traffic = None
+        for line in tpath.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#") and parts[0] == names[dom]:
+                traffic = float(parts[1])
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
         "traffic": traffic, "kernel": names[dom], "peak_source": peak_src,
