@@ -190,8 +190,9 @@ typedef struct vt_frame_params {
   float camera_target[3];
   uint32_t max_depth;       /* path depth, 1 = direct light only (Uniforms.cameraTarget.w) */
   float camera_up[3];
-  uint32_t sampling_mode;   /* 1 = NEE + BSDF with power-heuristic MIS, 2 = light sampling (NEE),
-                               3 = BSDF sampling (Uniforms.samplingMode 1-3) */
+  uint32_t sampling_mode;   /* 0 = ReSTIR DI at the primary vertex, MIS elsewhere; 1 = NEE + BSDF
+                               with power-heuristic MIS; 2 = light sampling (NEE); 3 = BSDF sampling
+                               (Uniforms.samplingMode 0-3) */
   uint32_t width, height;
   uint32_t first_sample;    /* sample index of the first frame (>= 1, Uniforms.sampleIndex) */
   uint32_t spectral;        /* 1 = four hero wavelengths, 0 = RGB transport */
@@ -199,7 +200,8 @@ typedef struct vt_frame_params {
   uint32_t z_temporal;      /* Z++ temporal model 0-3 (bits 7-8; the reference's default is 3) */
   uint32_t first_frame;     /* accumulation frame of the first sample (Uniforms.frameIndex, >= 1);
                                0 = continue the scene's accumulation */
-  uint32_t pad;
+  uint32_t di_candidates;   /* ReSTIR DI initial candidates per pixel (sampling_mode 0); 0 = the
+                               reference's 4 (restir_di_initial, main.swift:4646) */
 } vt_frame_params;
 
 /* A renderable scene: the mesh, its material slots, the area light and (optionally) the spectral
@@ -219,6 +221,12 @@ vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene);
 /* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3)
  * and the number of samples accumulated. Synchronises. */
 vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t n, uint32_t *samples);
+
+/* The ReSTIR DI reservoirs of the last frame rendered in sampling mode 0, for checking reuse: per
+ * pixel (weight sum, M, W, wavelength number), 4 floats into the HOST array out (n = width *
+ * height * 4). M counts the frame's candidates plus the confidence merged from the previous frame
+ * (capped at 20, restir_di_merge, main.swift:4686-4699). vt_accum_reset clears the history. */
+vt_status vt_scene_di_weights(vt_ctx *ctx, const vt_scene *scene, float *out, uint32_t n);
 
 /* Per pixel the first draws of one sampling event (vertex, stream) of the pixel's sampler: rand_f,
  * rand_f2 and rand_f3, 6 floats per pixel into the HOST array `out` (width * height * 6). The

@@ -90,6 +90,7 @@ SIGNATURES = {
     "vt_scene_create_imported": (_I32, [_P, _P, _P, _U32, _P, _U32, C.POINTER(_P)]),
     "vt_scene_emitter_words": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_light_estimate": (_I32, [_P, _P, _P, _U32, _U32, _U32, _P]),
+    "vt_scene_di_weights": (_I32, [_P, _P, _P, _U32]),
 }
 NOALLOC_MAX_FACES = 32768
 

@@ -70,6 +70,15 @@ struct RenderArgs {
   const uint4 *ltNodes;
   const uint32_t *ltLeaves;
   float3 ltLo, ltScale;
+  // ReSTIR DI (sampling mode 0): the primary-surface cache and reservoirs of this frame (written by
+  // pass 1, read by pass 2) and of the previous frame (temporal reuse), and the previous camera.
+  uint32_t diCandidates, diBits, history;
+  float4 *gPos, *gNrm;           // (position, distance or -1), (normal, material type)
+  uint4 *gInfo;                  // (face, slot | front << 31, error bits, 0)
+  float4 *rPos, *rEmit, *rW;     // (position, light id bits), (emission, pdf), (weight sum, M, W, u)
+  const float4 *hPos, *hNrm, *hrPos, *hrEmit, *hrW;
+  float3 pcam, pfwd, pright, pup;
+  float paspect, pfovScale;
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -609,42 +618,135 @@ __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes 
   return to_rgb(A, L, s);
 }
 
-__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
-                              int *stack) {
-  Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
+// ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
+// Light ids of stored samples (LightSample.isDirectional): 0 the quad light, face + 2 an emitter.
+struct DISample {
+  float3 pos, emission;
+  float pdf, u;
+  uint32_t id;
+};
+struct DIReservoir {
+  DISample s;
+  float wsum, M;
+};
+
+// light_geometry (main.swift:3165-3183): cos at the light over d^2 seen from p.
+__device__ __forceinline__ float light_geometry(const RenderArgs &A, float3 p, const DISample &c) {
+  if (A.imported && c.id >= 2u) return imported_geometry(p, c.pos, scene_triangle(A, c.id - 2u));
+  const float3 delta = sub(c.pos, p);
+  const float d2 = dot3(delta, delta);
+  if (d2 < 1e-10f) return 0.0f;
+  return fmaxf(0.0f, dot3(A.ln, mul(delta, -rsqrtf(d2)))) / d2;
+}
+
+// Lambert f (eval_bsdf for DIFFUSE, main.swift:2665-2686) as direct_light evaluates it.
+__device__ __forceinline__ float lambert_f(float3 n, float3 wo, float3 wi) {
+  const float ni = dot3(n, wi), no = dot3(n, wo);
+  return no > 0.0f && ni > 0.0f && fabsf(ni) >= 1e-7f ? kInvPi : 0.0f;
+}
+
+// The sample's contribution at the shading point before its weight: bsdf * Le * cos * G, in the
+// sample's own wavelengths (u), as linear sRGB.
+__device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 view,
+                                                  const vt_material &m, const DISample &c) {
+  const float3 dir = normalize3(sub(c.pos, p));
+  const float cos_th = fmaxf(0.0f, dot3(n, dir));
+  if (cos_th <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
   Lanes L;
-  if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
-  // Camera ray (restir_temporal_kernel, main.swift:4874-4893).
+  if (A.spectral) L = make_lanes(A, c.u);
+  const float f = lambert_f(n, mul(view, -1.0f), dir);
+  const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
+  const float4 s = scale4(mul4(reflectance(A, m), emission(A, L, e)), f * cos_th);
+  return mul(to_rgb(A, L, s), light_geometry(A, p, c));
+}
+
+// eval_restir_target_pdf (main.swift:3187-3197): the length of that contribution.
+__device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 view, const vt_material &m,
+                                           const DISample &c) {
+  if (c.pdf <= 0.0f) return 0.0f;
+  const float3 v = di_contribution(A, p, n, view, m, c);
+  return sqrtf(dot3(v, v));
+}
+
+__device__ __forceinline__ LightSample di_light_sample(const DISample &c, float3 p) {
+  LightSample ls;
+  ls.pos = c.pos;
+  const float3 d = sub(c.pos, p);
+  ls.dist = sqrtf(dot3(d, d));
+  ls.wi = normalize3(d);
+  ls.emission = c.emission;
+  ls.pdf = c.pdf;
+  ls.face = c.id >= 2u ? c.id - 2u : 0xffffffffu;
+  return ls;
+}
+
+__device__ __forceinline__ DISample load_di(const float4 *pos, const float4 *emit, const float4 *w, uint32_t i) {
+  const float4 a = pos[i], b = emit[i], c = w[i];
+  DISample s;
+  s.pos = f3(a.x, a.y, a.z);
+  s.id = __float_as_uint(a.w);
+  s.emission = f3(b.x, b.y, b.z);
+  s.pdf = b.w;
+  s.u = c.w;
+  return s;
+}
+
+// restir_same_surface (main.swift:4816-4820) and restir2020_compatible (main.swift:5030-5033).
+__device__ __forceinline__ bool same_surface(float4 pos, float4 nrm, float4 oldPos, float4 oldNrm) {
+  const float3 d = f3(oldPos.x - pos.x, oldPos.y - pos.y, oldPos.z - pos.z);
+  return oldPos.w > 0.0f && oldNrm.w == nrm.w && oldNrm.x * nrm.x + oldNrm.y * nrm.y + oldNrm.z * nrm.z > 0.95f &&
+         sqrtf(dot3(d, d)) < fmaxf(0.01f, pos.w * 0.01f);
+}
+__device__ __forceinline__ bool compatible(float4 pos, float4 nrm, float4 nPos, float4 nNrm) {
+  return nPos.w > 0.0f && nNrm.w == nrm.w && nrm.x * nNrm.x + nrm.y * nNrm.y + nrm.z * nNrm.z > 0.95f &&
+         fabsf(pos.w - nPos.w) < 0.05f * pos.w;
+}
+
+// restir_backproject (main.swift:4828-4836): the pixel of the previous frame's camera that sees p.
+__device__ __forceinline__ bool backproject(const RenderArgs &A, float3 p, int &px, int &py) {
+  if (!A.history) return false;
+  const float3 d = sub(p, A.pcam);
+  const float z = dot3(d, A.pfwd);
+  if (!(z > 0.0f)) return false;
+  const float nx = dot3(d, A.pright) / (z * A.paspect * A.pfovScale), ny = dot3(d, A.pup) / (z * A.pfovScale);
+  const float ux = nx * 0.5f + 0.5f, uy = -ny * 0.5f + 0.5f;
+  if (!(ux >= 0.0f && uy >= 0.0f && ux < 1.0f && uy < 1.0f)) return false;
+  px = (int)(ux * float(A.W));
+  py = (int)(uy * float(A.H));
+  return px >= 0 && px < (int)A.W && py >= 0 && py < (int)A.H;
+}
+
+// Camera ray (restir_temporal_kernel, main.swift:4874-4893).
+__device__ __forceinline__ float3 camera_dir(const RenderArgs &A, uint32_t x, uint32_t y, float2 jit) {
   const float jx = jit.x + 0.5f, jy = jit.y + 0.5f;
   float u = ((float(x) + jx) / float(A.W)) * 2.0f - 1.0f;
   float v = ((float(y) + jy) / float(A.H)) * 2.0f - 1.0f;
   v = -v;
   u *= A.aspect * A.fovScale;
   v *= A.fovScale;
-  const float3 dir0 = normalize3(add(A.fwd, add(mul(A.right, u), mul(A.up, v))));
-  Hit h;
-  const bool hit0 = rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack);
-  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
-  if (!hit0) return f3(0.0f, 0.0f, 0.0f);
-  Surface S = surface_at(A, h, A.cam, dir0);
-  vt_material m = material(A, S.slot);
-  if (m.type == VT_MAT_EMISSIVE) {
-    // The camera sees the emitter's radiance, in spectral transport its four-wavelength estimate
-    // (emitter_rgb, main.swift:7467-7468); imported emitters emit from their front face only
-    // (trace_scene, main.swift:2031).
-    if (A.imported && !S.front) return f3(0.0f, 0.0f, 0.0f);
-    return to_rgb(A, L, emission(A, L, m.emission));
-  }
+  return normalize3(add(A.fwd, add(mul(A.right, u), mul(A.up, v))));
+}
+
+// What the camera sees on an emitter: its radiance, in spectral transport its four-wavelength
+// estimate (emitter_rgb, main.swift:7467-7468); imported emitters emit from their front face only
+// (trace_scene, main.swift:2031).
+__device__ __forceinline__ float3 primary_emission(const RenderArgs &A, const Lanes &L, const Surface &S,
+                                                   const vt_material &m) {
+  if (A.imported && !S.front) return f3(0.0f, 0.0f, 0.0f);
+  return to_rgb(A, L, emission(A, L, m.emission));
+}
+
+// The path after its primary vertex S (the bounce loop of shading_kernel, main.swift:7709-7833):
+// BSDF continuations, NEE with MIS at later vertices, emitter hits weighed by emission_weight and
+// Russian roulette. With diPrimary (sampling mode 0) the primary vertex's direct light came from its
+// ReSTIR DI reservoir, so a BSDF hit on an emitter from it gets no weight (previousMIS false,
+// main.swift:7717-7718).
+__device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
+                                Sampler &seed, int *stack, bool diPrimary) {
   const int limit = max(0, (int)A.maxDepth - 1);
-  const bool nee = A.mode != 3u, mis = A.mode == 1u;
+  const bool nee = A.mode != 3u, mis = A.mode <= 1u;
   float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
   float3 R = f3(0.0f, 0.0f, 0.0f);
-  if (nee) {
-    sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), mis && limit > 0, seed, stack,
-                     true);
-  }
-  float3 dir = dir0;
   int scattering = 0;
   bool emissionOnly = false;
   for (int bounce = 1;; ++bounce) {
@@ -654,6 +756,7 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
       emissionOnly = true;
     }
     ++scattering;
+    const bool previousMIS = mis && !(diPrimary && bounce == 1);
     // sample_bsdf, Lambert: one 3D draw (three PCG draws), the direction from the last two.
     sampler_event(seed, (uint32_t)bounce, kZBsdf);
     const float3 r = rand_f3(seed);
@@ -665,14 +768,15 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     const float3 prev = S.pos;
     const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
+    Hit h;
     if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       // emission_weight (main.swift:3462-3466): 1 without NEE or without a light pdf, else the
-      // power heuristic (MIS) or 0 (light sampling).
+      // power heuristic (MIS) or 0 (light sampling, or a ReSTIR DI vertex).
       const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
-      const float w = !nee || lpdf <= 0.0f ? 1.0f : (mis ? power_heuristic(bpdf, lpdf) : 0.0f);
+      const float w = !nee || lpdf <= 0.0f ? 1.0f : (previousMIS ? power_heuristic(bpdf, lpdf) : 0.0f);
       if (!A.imported || S.front) R = add(R, to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w)));
       break;
     }
@@ -689,8 +793,163 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
       T = scale4(T, 1.0f / survival);
     }
   }
+  return R;
+}
+
+// One path of sampling modes 1-3: camera ray, primary hit, NEE there, then the continuation.
+__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
+                              int *stack) {
+  Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
+  const float3 dir0 = camera_dir(A, x, y, jit);
+  Hit h;
+  const bool hit0 = rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack);
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
+  if (!hit0) return f3(0.0f, 0.0f, 0.0f);
+  const Surface S = surface_at(A, h, A.cam, dir0);
+  const vt_material m = material(A, S.slot);
+  if (m.type == VT_MAT_EMISSIVE) return primary_emission(A, L, S, m);
+  float3 R = f3(0.0f, 0.0f, 0.0f);
+  if (A.mode != 3u) {
+    const int limit = max(0, (int)A.maxDepth - 1);
+    const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    sampler_event(seed, 1u, kZNee);
+    R = direct_light(A, L, S.pos, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), A.mode == 1u && limit > 0, seed,
+                     stack, true);
+  }
+  R = add(R, continue_path(A, L, S, m, dir0, seed, stack, false));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
+}
+
+// ReSTIR DI pass 1 for frame k (restir_temporal_kernel, main.swift:4842-4960): the primary hit into
+// the primary-surface cache, then at a diffuse hit the initial reservoir (RIS over the frame's
+// candidates, restir_di_initial, main.swift:4638-4668), merged with the previous frame's reservoir
+// of the backprojected pixel when it saw the same surface (restir_di_merge, main.swift:4686-4699,
+// confidence capped at 20), stored with W = wsum / (M p_hat) (restir_di_encode).
+__global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint32_t k) {
+  int stack[kRenderStack];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.W * A.H) return;
+  const uint32_t x = i % A.W, y = i / A.W;
+  Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
+  const float u = A.spectral ? wavelength_numbers(seed).x : 0.0f;
+  const float3 dir0 = camera_dir(A, x, y, A.jitter[k]);
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  Hit h;
+  if (!rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack)) {
+    A.gPos[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    A.gNrm[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+    A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
+    return;
+  }
+  const Surface S = surface_at(A, h, A.cam, dir0);
+  const vt_material m = material(A, S.slot);
+  const float4 gp = make_float4(S.pos.x, S.pos.y, S.pos.z, h.t), gn = make_float4(S.gn.x, S.gn.y, S.gn.z, float(m.type));
+  A.gPos[i] = gp;
+  A.gNrm[i] = gn;
+  A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
+  if (m.type != VT_MAT_DIFFUSE) {
+    A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
+    return;
+  }
+  DIReservoir r;
+  r.s.pos = f3(0.0f, 0.0f, 0.0f); r.s.emission = f3(0.0f, 0.0f, 0.0f);
+  r.s.pdf = 0.0f; r.s.u = u; r.s.id = 0u;
+  r.wsum = 0.0f;
+  r.M = 0.0f;
+  for (uint32_t c = 0; c < A.diCandidates; ++c) {
+    sampler_candidate(seed, 1u, kZDi, c, A.diBits);
+    const LightSample ls = sample_direct(A, S.pos, seed);
+    r.M += 1.0f;  // zero-weight candidates still count
+    if (!(ls.pdf > 0.0f)) continue;
+    DISample cand;
+    cand.pos = ls.pos; cand.emission = ls.emission; cand.pdf = ls.pdf; cand.u = u;
+    cand.id = ls.face == 0xffffffffu ? 0u : ls.face + 2u;
+    const float pHat = di_target(A, S.pos, S.gn, dir0, m, cand);
+    const float proposal = cand.pdf * light_geometry(A, S.pos, cand);
+    const float w = proposal > 0.0f ? pHat / proposal : 0.0f;
+    r.wsum += w;
+    if (rand_decision(seed) * r.wsum < w) r.s = cand;
+  }
+  int px, py;
+  if (backproject(A, S.pos, px, py)) {
+    const uint32_t j = (uint32_t)py * A.W + (uint32_t)px;
+    const float4 hw = A.hrW[j];
+    if (same_surface(gp, gn, A.hPos[j], A.hNrm[j]) && hw.y > 0.0f && hw.z > 0.0f) {
+      const DISample hs = load_di(A.hrPos, A.hrEmit, A.hrW, j);
+      const float cM = fminf(hw.y, 20.0f);
+      const float w = di_target(A, S.pos, S.gn, dir0, m, hs) * hw.z * cM;
+      r.M += cM;
+      r.wsum += w;
+      if (rand_decision(seed) * r.wsum < w) r.s = hs;
+    }
+  }
+  const float pHat = di_target(A, S.pos, S.gn, dir0, m, r.s);
+  const float W = r.M > 0.0f && pHat > 0.0f ? r.wsum / (r.M * pHat) : 0.0f;
+  A.rPos[i] = make_float4(r.s.pos.x, r.s.pos.y, r.s.pos.z, __uint_as_float(r.s.id));
+  A.rEmit[i] = make_float4(r.s.emission.x, r.s.emission.y, r.s.emission.z, r.s.pdf);
+  A.rW[i] = make_float4(r.wsum, r.M, W, r.s.u);
+}
+
+// ReSTIR DI pass 2 for frame k (shading_kernel, main.swift:7484-7561): spatial reuse of 4 uniform
+// taps in a 32-pixel box that pass RESTIR2020's compatibility test (uniform_neighbor, main.swift:
+// 5025-5027), the selected sample's contribution W * bsdf * Le * cos * G when visible, then the
+// path's continuation (MIS at later vertices). The sample is added to the FP64 accumulation.
+__global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_t k) {
+  int stack[kRenderStack];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.W * A.H) return;
+  const uint32_t x = i % A.W, y = i / A.W;
+  Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
+  const float3 dir0 = camera_dir(A, x, y, A.jitter[k]);
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
+  const float4 gp = A.gPos[i];
+  if (gp.w <= 0.0f) return;
+  const float4 gn = A.gNrm[i];
+  const uint4 gi = A.gInfo[i];
+  Surface S;
+  S.pos = f3(gp.x, gp.y, gp.z);
+  S.gn = f3(gn.x, gn.y, gn.z);
+  S.face = gi.x;
+  S.slot = gi.y & 0x7fffffffu;
+  S.front = (gi.y >> 31) != 0u;
+  S.err = __uint_as_float(gi.z);
+  const vt_material m = material(A, S.slot);
+  float3 R;
+  if (m.type == VT_MAT_EMISSIVE) {
+    R = primary_emission(A, L, S, m);
+  } else {
+    const float4 cw = A.rW[i];
+    DISample sel = load_di(A.rPos, A.rEmit, A.rW, i);
+    float wsum = di_target(A, S.pos, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
+    for (int t = 0; t < 4; ++t) {
+      const float ox = pcg_rand(seed.state), oy = pcg_rand(seed.state);
+      const int nx = (int)x + (int)((ox * 2.0f - 1.0f) * 16.0f), ny = (int)y + (int)((oy * 2.0f - 1.0f) * 16.0f);
+      if (nx < 0 || nx >= (int)A.W || ny < 0 || ny >= (int)A.H) continue;
+      const uint32_t j = (uint32_t)ny * A.W + (uint32_t)nx;
+      if (!compatible(gp, gn, A.gPos[j], A.gNrm[j])) continue;
+      const float4 nw = A.rW[j];
+      if (!(nw.y > 0.0f && nw.z > 0.0f)) continue;
+      const DISample ns = load_di(A.rPos, A.rEmit, A.rW, j);
+      const float w = di_target(A, S.pos, S.gn, dir0, m, ns) * nw.z * nw.y;
+      wsum += w;
+      M += nw.y;
+      if (rand_decision(seed) * wsum < w) sel = ns;
+    }
+    const float pHat = di_target(A, S.pos, S.gn, dir0, m, sel);
+    const float W = M > 0.0f && pHat > 0.0f ? wsum / (M * pHat) : 0.0f;
+    R = f3(0.0f, 0.0f, 0.0f);
+    if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
+      R = mul(di_contribution(A, S.pos, S.gn, dir0, m, sel), W);
+    R = add(R, continue_path(A, L, S, m, dir0, seed, stack, true));
+  }
+  if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) return;
+  double *acc = A.accum + 3 * (size_t)i;
+  acc[0] += R.x; acc[1] += R.y; acc[2] += R.z;
 }
 
 // Work item i = (sample group g, pixel p), pixel-major within a group so that a warp traces
@@ -846,6 +1105,7 @@ void scene_free(vt_scene *scene) {
   cudaFree(scene->d_emitters);
   cudaFree(scene->d_emissions);
   cudaFree(scene->d_face_pos);
+  cudaFree(scene->d_di);
   delete scene;
 }
 
@@ -1049,6 +1309,7 @@ vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene) {
   if (scene->d_accum)
     VT_CUDA(ctx, cudaMemset(scene->d_accum, 0, 3 * (size_t)scene->width * scene->height * sizeof(double)));
   scene->samples = 0;
+  scene->di_frames = 0;  // a cut clears the ReSTIR history; camera motion alone keeps it
   return VT_OK;
 }
 
@@ -1057,8 +1318,9 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
   if (p->width == 0 || p->height == 0 || (uint64_t)p->width * p->height > (1u << 28))
     return vt_fail(ctx, VT_ERR_INVALID, "bad image size");
-  if (p->sampling_mode < 1 || p->sampling_mode > 3)
-    return vt_fail(ctx, VT_ERR_INVALID, "sampling_mode must be 1 (MIS), 2 (light) or 3 (BSDF)");
+  if (p->sampling_mode > 3)
+    return vt_fail(ctx, VT_ERR_INVALID, "sampling_mode must be 0 (ReSTIR DI), 1 (MIS), 2 (light) or 3 (BSDF)");
+  if (p->di_candidates > 1024) return vt_fail(ctx, VT_ERR_INVALID, "di_candidates must be at most 1024");
   if (p->spectral && !scene->d_spec) return vt_fail(ctx, VT_ERR_INVALID, "spectral transport needs spectral tables");
   if (p->first_sample == 0) return vt_fail(ctx, VT_ERR_INVALID, "first_sample starts at 1");
   if (p->sampler > 1 || p->z_temporal > 3) return vt_fail(ctx, VT_ERR_INVALID, "sampler must be 0 (PCG) or 1 (Z++), z_temporal 0-3");
@@ -1142,8 +1404,52 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.jitter = scene->d_jitter;
   A.accum = scene->d_accum;
   emitter_args(scene, A);
-  // Enough (pixel, sample group) items to fill the GPU about four times over.
   const uint32_t npix = p->width * p->height;
+  if (p->sampling_mode == 0u) {
+    // ReSTIR DI: frames in order, two launches each (the primary pass, then reuse and shading).
+    if (!scene->d_di || scene->di_width != p->width || scene->di_height != p->height) {
+      cudaFree(scene->d_di);
+      scene->d_di = nullptr;
+      VT_CUDA(ctx, cudaMalloc(&scene->d_di, 11 * (size_t)npix * sizeof(float4)));
+      scene->di_width = p->width;
+      scene->di_height = p->height;
+      scene->di_frames = 0;
+    }
+    const uint32_t m = p->di_candidates ? p->di_candidates : 4u;
+    uint32_t bits = 0;
+    while ((1u << bits) < m) ++bits;
+    A.diCandidates = m;
+    A.diBits = bits;
+    float4 *base = scene->d_di;
+    A.gInfo = reinterpret_cast<uint4 *>(base + 10 * (size_t)npix);
+    const float cam[14] = {A.cam.x, A.cam.y, A.cam.z, A.fwd.x, A.fwd.y, A.fwd.z, A.right.x, A.right.y, A.right.z,
+                           A.up.x, A.up.y, A.up.z, A.aspect, A.fovScale};
+    const unsigned blocks = (npix + kRenderBlock - 1) / kRenderBlock;
+    for (uint32_t k = 0; k < spp; ++k) {
+      float4 *cur = base + 5 * (size_t)npix * scene->di_parity, *prev = base + 5 * (size_t)npix * (scene->di_parity ^ 1u);
+      A.gPos = cur; A.gNrm = cur + npix; A.rPos = cur + 2 * (size_t)npix; A.rEmit = cur + 3 * (size_t)npix;
+      A.rW = cur + 4 * (size_t)npix;
+      A.hPos = prev; A.hNrm = prev + npix; A.hrPos = prev + 2 * (size_t)npix; A.hrEmit = prev + 3 * (size_t)npix;
+      A.hrW = prev + 4 * (size_t)npix;
+      A.history = scene->di_frames > 0 ? 1u : 0u;
+      const float *pc = scene->di_cam;
+      A.pcam = make_float3(pc[0], pc[1], pc[2]);
+      A.pfwd = make_float3(pc[3], pc[4], pc[5]);
+      A.pright = make_float3(pc[6], pc[7], pc[8]);
+      A.pup = make_float3(pc[9], pc[10], pc[11]);
+      A.paspect = pc[12];
+      A.pfovScale = pc[13];
+      k_di_primary<<<blocks, kRenderBlock, 0, s>>>(A, k);
+      k_di_shade<<<blocks, kRenderBlock, 0, s>>>(A, k);
+      VT_CUDA(ctx, cudaGetLastError());
+      scene->di_parity ^= 1u;
+      ++scene->di_frames;
+      std::memcpy(scene->di_cam, cam, sizeof cam);
+    }
+    scene->samples += spp;
+    return VT_OK;
+  }
+  // Enough (pixel, sample group) items to fill the GPU about four times over.
   const uint64_t target = (uint64_t)ctx->sm_count * 2048u * 4u;
   uint32_t groups = (uint32_t)std::min<uint64_t>(spp, std::max<uint64_t>(1, (target + npix - 1) / npix));
   const uint32_t per = (spp + groups - 1) / groups;
@@ -1153,6 +1459,18 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   k_render<<<grid, kRenderBlock, 0, s>>>(A, groups, per);
   VT_CUDA(ctx, cudaGetLastError());
   scene->samples += spp;
+  return VT_OK;
+}
+
+vt_status vt_scene_di_weights(vt_ctx *ctx, const vt_scene *scene, float *out, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !out) return vt_fail(ctx, VT_ERR_INVALID, "scene or out is null");
+  if (!scene->d_di || scene->di_frames == 0) return vt_fail(ctx, VT_ERR_INVALID, "no ReSTIR DI frame rendered");
+  const size_t npix = (size_t)scene->di_width * scene->di_height;
+  if (n != 4 * npix) return vt_fail(ctx, VT_ERR_INVALID, "n must equal width * height * 4");
+  const float4 *last = scene->d_di + 5 * npix * (scene->di_parity ^ 1u) + 4 * npix;
+  VT_CUDA(ctx, cudaDeviceSynchronize());
+  VT_CUDA(ctx, cudaMemcpy(out, last, npix * sizeof(float4), cudaMemcpyDeviceToHost));
   return VT_OK;
 }
 

@@ -97,7 +97,7 @@ __device__ __forceinline__ uint32_t z_morton(uint32_t x, uint32_t y) {
 }
 
 // Sampling-event streams (main.swift:291-292): 32 dimensions each, 16 per path vertex.
-constexpr uint32_t kZBsdf = 0u, kZNee = 1u, kZRoulette = 2u, kZLens = 3u, kZWavelength = 12u;
+constexpr uint32_t kZBsdf = 0u, kZNee = 1u, kZRoulette = 2u, kZLens = 3u, kZDi = 4u, kZWavelength = 12u;
 
 struct Sampler {
   uint32_t state, key, dimension, sub, subBits;
@@ -186,6 +186,15 @@ __device__ __forceinline__ void sampler_event(Sampler &s, uint32_t vertex, uint3
   s.sub = 0u;
   s.subBits = 0u;
 }
+// sampler_candidate (main.swift:296-298): candidate `index` of an event draws from the event's
+// dimensions with `bits` extra frame bits, so a block of 2^bits candidates is stratified.
+__device__ __forceinline__ void sampler_candidate(Sampler &s, uint32_t vertex, uint32_t stream, uint32_t index,
+                                                  uint32_t bits) {
+  sampler_event(s, vertex, stream);
+  if (s.z) { s.sub = index; s.subBits = bits; }
+}
+// rand_decision (main.swift:117, 280): resampling decisions draw from the PCG state in either mode.
+__device__ __forceinline__ float rand_decision(Sampler &s) { return pcg_rand(s.state); }
 // wavelength_numbers (main.swift:2222-2231): from a copy, so the sampler's streams are unchanged.
 __device__ __forceinline__ float2 wavelength_numbers(Sampler s) {
   if (s.z) {

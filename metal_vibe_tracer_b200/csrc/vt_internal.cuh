@@ -85,6 +85,12 @@ struct vt_scene {
   uint32_t width = 0, height = 0, samples = 0;
   float2 *d_jitter = nullptr;
   uint32_t jitter_cap = 0;
+  // ReSTIR DI (sampling mode 0): per pixel the primary-surface cache (position, normal) and the
+  // reservoir (sample position, emission and pdf, weights) for this frame and the previous one,
+  // plus the primary hit's face/slot/error: 11 float4 per pixel in one allocation.
+  float4 *d_di = nullptr;
+  uint32_t di_width = 0, di_height = 0, di_frames = 0, di_parity = 0;
+  float di_cam[14] = {};  // previous frame's camera: position, forward, right, up, aspect, fov scale
 };
 
 // ---------------------------------------------------------------------------------------------

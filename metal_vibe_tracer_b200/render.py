@@ -35,7 +35,7 @@ class FrameParams(C.Structure):
                 ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
                 ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
-                ("first_frame", C.c_uint32), ("pad", C.c_uint32)]
+                ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32)]
 
 
 assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 80
@@ -58,20 +58,21 @@ def make_light(light) -> QuadLight:
 
 
 def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1, sampler=0, z_temporal=3,
-                first_frame=0) -> FrameParams:
+                first_frame=0, di_candidates=0) -> FrameParams:
     p = FrameParams()
     p.camera_pos[:] = [float(x) for x in camera["pos"]]
     p.camera_target[:] = [float(x) for x in camera["target"]]
     p.camera_up[:] = [float(x) for x in camera["up"]]
     p.fov_deg = float(camera["fov"])
     p.max_depth = int(max_depth)
-    p.sampling_mode = int(mode)  # 1 MIS, 2 light sampling, 3 BSDF sampling (Uniforms.samplingMode)
+    p.sampling_mode = int(mode)  # 0 ReSTIR DI, 1 MIS, 2 light sampling, 3 BSDF sampling (Uniforms.samplingMode)
     p.width, p.height = int(width), int(height)
     p.first_sample = int(first_sample)
     p.spectral = 1 if spectral else 0
     p.sampler = int(sampler)          # 0 PCG, 1 Z++
     p.z_temporal = int(z_temporal)    # Z++ temporal model (the reference's default: 3, reshuffled)
     p.first_frame = int(first_frame)  # 0: continue the scene's accumulation
+    p.di_candidates = int(di_candidates)  # ReSTIR DI candidates (0: the reference's 4)
     return p
 
 
@@ -120,6 +121,14 @@ class Scene:
         out = np.empty(n.value, np.uint32)
         _check(self.ctx.handle, lib.vt_scene_emitter_words(self.ctx.handle, self._p, out.ctypes.data, n.value,
                                                            C.byref(n)), "vt_scene_emitter_words")
+        return out
+
+    def di_weights(self) -> np.ndarray:
+        """(height, width, 4) float32 ReSTIR DI reservoir weights of the last mode-0 frame:
+        weight sum, M, W, wavelength number."""
+        out = np.empty((self.height, self.width, 4), np.float32)
+        _check(self.ctx.handle, _lib.load().vt_scene_di_weights(self.ctx.handle, self._p, out.ctypes.data, out.size),
+               "vt_scene_di_weights")
         return out
 
     def light_estimate(self, points, per_point: int, samples: int = 64) -> np.ndarray:

@@ -1225,6 +1225,12 @@ struct ZSampler {
     a = zfloat(x); b = zfloat(y); c = zfloat(w);
   }
   void event(uint32_t vertex, uint32_t stream) { dimension = (vertex * 16u + stream) * 32u; sub = 0u; subBits = 0u; }
+  // sampler_candidate (main.swift:296-298) and rand_decision (main.swift:117, 280).
+  void candidate(uint32_t vertex, uint32_t stream, uint32_t index, uint32_t bits) {
+    event(vertex, stream);
+    if (z) { sub = index; subBits = bits; }
+  }
+  double decision() { return pcg(); }
   // wavelength_numbers: from a copy.
   double wavelength_u() const {
     if (z) { ZSampler c = *this; c.event(0u, 12u); return c.f1(); }
@@ -1374,7 +1380,7 @@ inline double smax(const PtContext &C, const Spec4 &a) {
   return C.spectral ? std::max(m, a.v[3]) : m;
 }
 
-struct PtHit { D3 pos, gn; double err; uint32_t slot, face; bool front; };
+struct PtHit { D3 pos, gn; double err, t; uint32_t slot, face; bool front; };
 
 struct PtTri { D3 a, b, c; uint32_t slot; };
 PtTri pt_triangle(const PtContext &C, uint32_t face) {
@@ -1401,6 +1407,7 @@ bool pt_closest(const PtContext &C, D3 o, D3 d, PtHit &h) {
   h.gn = h.front ? ng : ng * -1.0;
   h.slot = tri.slot;
   h.face = (uint32_t)prim;
+  h.t = t;
   if (C.imported) {
     h.pos = tri.a * (1.0 - b1 - b2) + tri.b * b1 + tri.c * b2;
     h.err = mesh_hit_error_d(tri);
@@ -1681,34 +1688,28 @@ void make_basis_d(D3 n, D3 &u, D3 &v) {
   v = cross(n, u);
 }
 
-D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx_f, float jy_f) {
-  ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
-  PtLanes L{};
-  if (C.spectral) L = make_lanes(C, seed.wavelength_u());
+D3 camera_dir_d(const PtContext &C, uint32_t x, uint32_t y, float jx_f, float jy_f) {
   const double jx = double(jx_f) + 0.5, jy = double(jy_f) + 0.5;
   double u = ((x + jx) / C.p->width) * 2.0 - 1.0, v = ((y + jy) / C.p->height) * 2.0 - 1.0;
   v = -v;
   u *= C.aspect * C.fovScale;
   v *= C.fovScale;
-  const D3 dir0 = normalize(C.fwd + C.right * u + C.up * v);
-  PtHit h;
-  const bool hit0 = pt_closest(C, C.cam, dir0, h);
-  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
-  if (!hit0) return {0, 0, 0};
-  vt_material m = pt_material(C, h.slot);
-  if (m.type == VT_MAT_EMISSIVE) {
-    // emitter_rgb (main.swift:7467-7468): the four-wavelength estimate in spectral transport.
-    if (C.imported && !h.front) return {0, 0, 0};
-    return to_rgb(C, L, emission(C, L, m.emission));
-  }
+  return normalize(C.fwd + C.right * u + C.up * v);
+}
+
+// emitter_rgb at the primary hit (main.swift:7467-7468); imported emitters emit from the front.
+D3 primary_emission_d(const PtContext &C, const PtLanes &L, const PtHit &h, const vt_material &m) {
+  if (C.imported && !h.front) return {0, 0, 0};
+  return to_rgb(C, L, emission(C, L, m.emission));
+}
+
+// The path after its primary vertex (shading_kernel's bounce loop, main.swift:7709-7833). With
+// diPrimary (sampling mode 0) a BSDF hit on an emitter from the primary vertex gets no weight.
+D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m, ZSampler &seed, bool diPrimary) {
   const int limit = std::max(0, (int)C.p->max_depth - 1);
-  const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode == 1u;
+  const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode <= 1u;
   Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
   D3 R{0, 0, 0};
-  if (nee) {
-    seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), mis && limit > 0, seed, true);
-  }
   int scattering = 0;
   bool emissionOnly = false;
   for (int bounce = 1;; ++bounce) {
@@ -1717,6 +1718,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
       emissionOnly = true;
     }
     ++scattering;
+    const bool previousMIS = mis && !(diPrimary && bounce == 1);
     seed.event((uint32_t)bounce, 0u);
     double r0, r1, r2;
     seed.f3(r0, r1, r2);
@@ -1737,7 +1739,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
     m = pt_material(C, h.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       const double lpdf = C.imported ? emitter_pdf_d(C, prev, h.pos, h.face) : light_pdf_d(C, prev, h.pos);
-      const double w = !nee || lpdf <= 0.0 ? 1.0 : (mis ? power_heuristic_d(bpdf, lpdf) : 0.0);
+      const double w = !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
       if (!C.imported || h.front) R = R + to_rgb(C, L, scale(mul(T, emission(C, L, m.emission)), w));
       break;
     }
@@ -1753,6 +1755,188 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
       T = scale(T, 1.0 / survival);
     }
   }
+  return R;
+}
+
+// ---- ReSTIR DI (sampling mode 0), FP64 ---------------------------------------------------------
+// restir_temporal_kernel (main.swift:4842-4960) and the spatial reuse of shading_kernel
+// (main.swift:7484-7561): per frame, pass 1 over every pixel, then pass 2 over every pixel.
+struct DiS { D3 pos{0, 0, 0}, emission{0, 0, 0}; double pdf = 0, u = 0; uint32_t id = 0; };
+struct DiPix {
+  double pos[4] = {0, 0, 0, -1}, nrm[4] = {0, 0, 0, -1};
+  PtHit hit{};
+  DiS s;
+  double wsum = 0, M = 0, W = 0;
+};
+
+// light_geometry (main.swift:3165-3183).
+double light_geometry_d(const PtContext &C, D3 p, const DiS &c) {
+  if (C.imported && c.id >= 2u) return imported_geometry_d(p, c.pos, pt_triangle(C, c.id - 2u));
+  const D3 delta = c.pos - p;
+  const double d2 = dot(delta, delta);
+  if (d2 < 1e-10) return 0.0;
+  return std::max(0.0, dot(d3(C.in->light.normal), delta * (-1.0 / std::sqrt(d2)))) / d2;
+}
+
+D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 view, const vt_material &m, const DiS &c) {
+  const D3 dir = normalize(c.pos - p);
+  const double cos_th = std::max(0.0, dot(n, dir));
+  if (cos_th <= 0.0) return {0, 0, 0};
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, c.u);
+  const double ni = dot(n, dir), no = -dot(n, view);
+  const double f = no > 0.0 && ni > 0.0 && std::fabs(ni) >= 1e-7 ? 1.0 / kPi : 0.0;
+  const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
+  return to_rgb(C, L, scale(mul(reflectance(C, m), emission(C, L, e)), f * cos_th)) * light_geometry_d(C, p, c);
+}
+
+// eval_restir_target_pdf (main.swift:3187-3197).
+double di_target_d(const PtContext &C, D3 p, D3 n, D3 view, const vt_material &m, const DiS &c) {
+  if (c.pdf <= 0.0) return 0.0;
+  const D3 v = di_contribution_d(C, p, n, view, m, c);
+  return std::sqrt(dot(v, v));
+}
+
+bool same_surface_d(const double *pos, const double *nrm, const double *op, const double *on) {
+  const double dx = op[0] - pos[0], dy = op[1] - pos[1], dz = op[2] - pos[2];
+  return op[3] > 0.0 && on[3] == nrm[3] && on[0] * nrm[0] + on[1] * nrm[1] + on[2] * nrm[2] > 0.95 &&
+         std::sqrt(dx * dx + dy * dy + dz * dz) < std::max(0.01, pos[3] * 0.01);
+}
+bool compatible_d(const double *pos, const double *nrm, const double *np, const double *nn) {
+  return np[3] > 0.0 && nn[3] == nrm[3] && nrm[0] * nn[0] + nrm[1] * nn[1] + nrm[2] * nn[2] > 0.95 &&
+         std::fabs(pos[3] - np[3]) < 0.05 * pos[3];
+}
+
+// restir_backproject (main.swift:4828-4836) with an unmoved camera between frames.
+bool backproject_d(const PtContext &C, D3 p, int &px, int &py) {
+  const D3 d = p - C.cam;
+  const double z = dot(d, C.fwd);
+  if (!(z > 0.0)) return false;
+  const double nx = dot(d, C.right) / (z * C.aspect * C.fovScale), ny = dot(d, C.up) / (z * C.fovScale);
+  const double ux = nx * 0.5 + 0.5, uy = -ny * 0.5 + 0.5;
+  if (!(ux >= 0.0 && uy >= 0.0 && ux < 1.0 && uy < 1.0)) return false;
+  px = (int)(ux * C.p->width);
+  py = (int)(uy * C.p->height);
+  return px >= 0 && px < (int)C.p->width && py >= 0 && py < (int)C.p->height;
+}
+
+DiS di_from_light(const PtLight &ls, double u) {
+  DiS c;
+  c.pos = ls.pos; c.emission = ls.emission; c.pdf = ls.pdf; c.u = u;
+  c.id = ls.face == 0xffffffffu ? 0u : ls.face + 2u;
+  return c;
+}
+
+PtLight light_from_di(const DiS &c, D3 p) {
+  PtLight ls{};
+  ls.pos = c.pos;
+  const D3 d = c.pos - p;
+  ls.dist = std::sqrt(dot(d, d));
+  ls.wi = normalize(d);
+  ls.emission = c.emission;
+  ls.pdf = c.pdf;
+  ls.face = c.id >= 2u ? c.id - 2u : 0xffffffffu;
+  return ls;
+}
+
+void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx, float jy,
+                  uint32_t M, uint32_t bits, bool history, const std::vector<DiPix> &prev, DiPix &out) {
+  out = DiPix{};
+  ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
+  const double u = C.spectral ? seed.wavelength_u() : 0.0;
+  const D3 dir0 = camera_dir_d(C, x, y, jx, jy);
+  PtHit h;
+  if (!pt_closest(C, C.cam, dir0, h)) return;
+  const vt_material m = pt_material(C, h.slot);
+  out.hit = h;
+  const double pos[4] = {h.pos.x, h.pos.y, h.pos.z, h.t}, nrm[4] = {h.gn.x, h.gn.y, h.gn.z, double(m.type)};
+  std::memcpy(out.pos, pos, sizeof pos);
+  std::memcpy(out.nrm, nrm, sizeof nrm);
+  if (m.type != VT_MAT_DIFFUSE) return;
+  out.s.u = u;
+  for (uint32_t c = 0; c < M; ++c) {
+    seed.candidate(1u, 4u, c, bits);
+    const PtLight ls = C.imported ? sample_emitters_d(C, h.pos, seed) : sample_light_d(C, h.pos, seed);
+    out.M += 1.0;
+    if (!(ls.pdf > 0.0)) continue;
+    const DiS cand = di_from_light(ls, u);
+    const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, cand);
+    const double proposal = cand.pdf * light_geometry_d(C, h.pos, cand);
+    const double w = proposal > 0.0 ? pHat / proposal : 0.0;
+    out.wsum += w;
+    if (seed.decision() * out.wsum < w) out.s = cand;
+  }
+  int px, py;
+  if (history && backproject_d(C, h.pos, px, py)) {
+    const DiPix &o = prev[(size_t)py * C.p->width + px];
+    if (same_surface_d(pos, nrm, o.pos, o.nrm) && o.M > 0.0 && o.W > 0.0) {
+      const double cM = std::min(o.M, 20.0);
+      const double w = di_target_d(C, h.pos, h.gn, dir0, m, o.s) * o.W * cM;
+      out.M += cM;
+      out.wsum += w;
+      if (seed.decision() * out.wsum < w) out.s = o.s;
+    }
+  }
+  const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, out.s);
+  out.W = out.M > 0.0 && pHat > 0.0 ? out.wsum / (out.M * pHat) : 0.0;
+}
+
+D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx, float jy,
+              const std::vector<DiPix> &cur) {
+  ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, seed.wavelength_u());
+  const D3 dir0 = camera_dir_d(C, x, y, jx, jy);
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
+  const DiPix &me = cur[(size_t)y * C.p->width + x];
+  if (me.pos[3] <= 0.0) return {0, 0, 0};
+  const PtHit &h = me.hit;
+  const vt_material m = pt_material(C, h.slot);
+  if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
+  DiS sel = me.s;
+  double wsum = di_target_d(C, h.pos, h.gn, dir0, m, sel) * me.W * me.M, M = me.M;
+  for (int t = 0; t < 4; ++t) {
+    const double ox = seed.pcg(), oy = seed.pcg();
+    const int nx = (int)x + (int)((ox * 2.0 - 1.0) * 16.0), ny = (int)y + (int)((oy * 2.0 - 1.0) * 16.0);
+    if (nx < 0 || nx >= (int)C.p->width || ny < 0 || ny >= (int)C.p->height) continue;
+    const DiPix &n = cur[(size_t)ny * C.p->width + nx];
+    if (!compatible_d(me.pos, me.nrm, n.pos, n.nrm)) continue;
+    if (!(n.M > 0.0 && n.W > 0.0)) continue;
+    const double w = di_target_d(C, h.pos, h.gn, dir0, m, n.s) * n.W * n.M;
+    wsum += w;
+    M += n.M;
+    if (seed.decision() * wsum < w) sel = n.s;
+  }
+  const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, sel);
+  const double W = M > 0.0 && pHat > 0.0 ? wsum / (M * pHat) : 0.0;
+  D3 R{0, 0, 0};
+  if (W > 0.0 && visible_d(C, h.pos, h.gn, h.err, light_from_di(sel, h.pos)))
+    R = di_contribution_d(C, h.pos, h.gn, dir0, m, sel) * W;
+  R = R + continue_path_d(C, L, h, m, seed, true);
+  if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
+  return R;
+}
+
+D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx_f, float jy_f) {
+  ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, seed.wavelength_u());
+  const D3 dir0 = camera_dir_d(C, x, y, jx_f, jy_f);
+  PtHit h;
+  const bool hit0 = pt_closest(C, C.cam, dir0, h);
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
+  if (!hit0) return {0, 0, 0};
+  const vt_material m = pt_material(C, h.slot);
+  if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
+  const int limit = std::max(0, (int)C.p->max_depth - 1);
+  D3 R{0, 0, 0};
+  if (C.p->sampling_mode != 3u) {
+    const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
+    seed.event(1u, 1u);
+    R = direct_d(C, L, h.pos, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), C.p->sampling_mode == 1u && limit > 0,
+                 seed, true);
+  }
+  R = R + continue_path_d(C, L, h, m, seed, false);
   if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
   return R;
 }
@@ -1809,6 +1993,28 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
     jy[k] = halton_f(n, 3) - 0.5f;
   }
   const uint32_t npix = p->width * p->height;
+  if (p->sampling_mode == 0u) {
+    // ReSTIR DI: frames in order, each a primary pass over every pixel, then reuse and shading.
+    const uint32_t M = p->di_candidates ? p->di_candidates : 4u;
+    uint32_t bits = 0;
+    while ((1u << bits) < M) ++bits;
+    std::vector<DiPix> buf[2] = {std::vector<DiPix>(npix), std::vector<DiPix>(npix)};
+    std::vector<double> sum(3 * (size_t)npix, 0.0);
+    for (uint32_t k = 0; k < spp; ++k) {
+      std::vector<DiPix> &cur = buf[k & 1u], &prev = buf[(k & 1u) ^ 1u];
+      const uint32_t si = p->first_sample + k, frame = std::max(1u, p->first_frame) + k;
+      parallel_for(npix, threads, [&](uint32_t i) {
+        di_primary_d(C, i % p->width, i / p->width, si, frame, jx[k], jy[k], M, bits, k > 0, prev, cur[i]);
+      });
+      parallel_for(npix, threads, [&](uint32_t i) {
+        const D3 c = di_shade_d(C, i % p->width, i / p->width, si, frame, jx[k], jy[k], cur);
+        sum[3 * (size_t)i] += c.x; sum[3 * (size_t)i + 1] += c.y; sum[3 * (size_t)i + 2] += c.z;
+      });
+    }
+    for (size_t i = 0; i < sum.size(); ++i) out_rgb[i] = spp ? sum[i] / spp : 0.0;
+    vto_bvh_free(C.bvh);
+    return;
+  }
   parallel_for(npix, threads, [&](uint32_t i) {
     const uint32_t x = i % p->width, y = i / p->width;
     double s[3] = {0, 0, 0};

@@ -4,7 +4,7 @@
   reference generator's XYZ -> sRGB matrix, normalised D65 and wavelength inverse CDF
   (golden fixture tests/golden/spectral_360_830.json, written by make_spectral_golden.py).
 * Integrator energy (tests/Fix_integrator.swift:188-215): on the Cornell box, light sampling agrees
-  with MIS within 3 %, BSDF sampling within 12 %, and each depth adds light.
+  with MIS within 3 %, BSDF sampling within 12 %, ReSTIR DI within 6 %, and each depth adds light.
 * Spectral transport of a grey scene under D65 converges to the RGB render (D65 is the sRGB white).
 """
 import json
@@ -57,7 +57,9 @@ def test_integrator_energy_reference_protocol(oracle):
         mis = oracle.render(faces, verts, mats, light, cam, 48, 32, 256, max_depth=depth, mode=1).mean()
         nee = oracle.render(faces, verts, mats, light, cam, 48, 32, 256, max_depth=depth, mode=2).mean()
         bsdf = oracle.render(faces, verts, mats, light, cam, 48, 32, 256, max_depth=depth, mode=3).mean()
+        restir = oracle.render(faces, verts, mats, light, cam, 48, 32, 256, max_depth=depth, mode=0).mean()
         assert abs(nee / mis - 1) < 0.03 and abs(bsdf / mis - 1) < 0.12, (depth, mis, nee, bsdf)
+        assert abs(restir / mis - 1) < 0.06, (depth, mis, restir)
         assert mis > prev
         prev = mis
 
