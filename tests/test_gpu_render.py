@@ -93,7 +93,7 @@ def test_render_rejects_unsupported_input(ctx, cornell):
         vt.Scene(ctx, mesh, coloured, light, spectral_tables.load())
     scene = vt.Scene(ctx, mesh, coloured, light)   # RGB transport takes colours
     with pytest.raises(vt.MaterialLibraryError, match="sampling_mode"):
-        scene.render(vt.make_params(cam, 8, 8, 8, 1, False, mode=0), 1)
+        scene.render(vt.make_params(cam, 8, 8, 8, 1, False, mode=4), 1)
     with pytest.raises(vt.MaterialLibraryError, match="spectral tables"):
         scene.render(vt.make_params(cam, 8, 8, 8, 1, True), 1)
     scene.close()
