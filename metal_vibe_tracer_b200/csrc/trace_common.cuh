@@ -8,7 +8,7 @@
 
 namespace vtd {
 
-constexpr int kStack = 96;  // 1 + 3 (depth - 1) entries for depth <= 32
+constexpr int kStack = 100;  // 1 + 3 depth entries for depth <= 33 (leaf children are stack entries)
 
 struct Node4 {
   float4 lox, loy, loz, hix, hiy, hiz;

@@ -21,6 +21,18 @@
 namespace {
 using namespace vtd;
 
+// Single-ray traversals in the persistent kernels' order (leaf children pushed as stack entries,
+// near entries popped first), counting node visits and triangle tests when kCount.
+// A leaf child is the stack entry ~(node << 2 | slot) (node indices are below 2^29); popping it reads
+// the slot's first triangle and count from the node, in L1 since the node's visit.
+__device__ __forceinline__ int leaf_entry_of(int node, int slot) { return ~((node << 2) | slot); }
+__device__ __forceinline__ void leaf_range(const float4 *__restrict__ nodes, int entry, int &first, int &cnt) {
+  const int code = ~entry;
+  const int *nd = reinterpret_cast<const int *>(nodes + 8 * (size_t)(code >> 2));
+  first = -__ldg(nd + 24 + (code & 3)) - 1;
+  cnt = __ldg(nd + 28 + (code & 3));
+}
+
 template <bool kCount>
 __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
                                               const float4 *__restrict__ tris, float rootMax,
@@ -35,16 +47,10 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
   int top = 0;
   stack[top++] = 0;
   while (top > 0) {
-    Node4 nd;
-    load_node(nodes, stack[--top], nd);
-    if (kCount) ++nv;
-    float nearT[4];
-    const int mask = node_hits(nd, sr, tMin, closest, nearT);
-    const Sorted4 o = sort_children(nd, mask, nearT);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (j >= o.m || o.child[j] > 0 || beyond(o.key[j], closest)) continue;
-      const int first = -o.child[j] - 1, cnt = o.count[j];
+    const int entry = stack[--top];
+    if (entry < 0) {
+      int first, cnt;
+      leaf_range(nodes, entry, first, cnt);
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
@@ -53,10 +59,19 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
         if (!intersect_tri(wr, a, b, cc, tMin, closest, t, b1, b2)) continue;
         closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w); found = true;
       }
+      continue;
     }
+    Node4 nd;
+    load_node(nodes, entry, nd);
+    if (kCount) ++nv;
+    float nearT[4];
+    const int mask = node_hits(nd, sr, tMin, closest, nearT);
+    const Sorted4 o = sort_children(nd, mask, nearT);
 #pragma unroll
-    for (int j = 3; j >= 0; --j)
-      if (j < o.m && o.child[j] > 0 && !beyond(o.key[j], closest) && top < kStack) stack[top++] = o.child[j];
+    for (int j = 3; j >= 0; --j) {
+      if (j >= o.m || beyond(o.key[j], closest) || top >= kStack) continue;
+      stack[top++] = o.child[j] > 0 ? o.child[j] : leaf_entry_of(entry, (int)(o.key[j] & 3u));
+    }
   }
   best = closest;
   return found;
@@ -73,17 +88,10 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
   int top = 0;
   stack[top++] = 0;
   while (top > 0) {
-    Node4 nd;
-    load_node(nodes, stack[--top], nd);
-    if (kCount) ++nv;
-    float nearT[4];
-    const int mask = node_hits(nd, sr, tMin, tMax, nearT);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (!(mask >> k & 1)) continue;
-      const int c = i4(nd.child, k);
-      if (c > 0) { if (top < kStack) stack[top++] = c; continue; }
-      const int first = -c - 1, cnt = i4(nd.count, k);
+    const int entry = stack[--top];
+    if (entry < 0) {
+      int first, cnt;
+      leaf_range(nodes, entry, first, cnt);
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
@@ -91,6 +99,18 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
         if (kCount) ++nt;
         if (intersect_tri(wr, a, b, cc, tMin, tMax, t, b1, b2)) return true;
       }
+      continue;
+    }
+    Node4 nd;
+    load_node(nodes, entry, nd);
+    if (kCount) ++nv;
+    float nearT[4];
+    const int mask = node_hits(nd, sr, tMin, tMax, nearT);
+#pragma unroll
+    for (int k = 3; k >= 0; --k) {
+      if (!(mask >> k & 1) || top >= kStack) continue;
+      const int c = i4(nd.child, k);
+      stack[top++] = c > 0 ? c : leaf_entry_of(entry, k);
     }
   }
   return false;
@@ -98,12 +118,12 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
 
 // ---- persistent traversal -----------------------------------------------------------------------
 // Rays vary a lot in length (65 node visits on average for the incoherent set, with a long tail), so
-// a thread-per-ray grid leaves most lanes of a warp idle while its longest ray finishes. Here each
-// warp stays resident and refills idle lanes from a global ray counter: one warp-aggregated
-// atomicAdd hands out as many rays as there are idle lanes, whenever at least kRefill lanes are
-// idle. Each loop iteration visits one node per active lane with the reference's per-ray algorithm
-// (leaves tested at the node visit in near-to-far order, inner children pushed far to near), so
-// the hits are those of the thread-per-ray form bit for bit. Rays are read and hits written with
+// a thread-per-ray grid leaves most lanes of a warp idle while its longest ray finishes.
+// Persistent traversal (k_closest, k_any): each warp stays resident and refills idle lanes from a
+// global ray counter: one warp-aggregated atomicAdd hands out as many rays as there are idle lanes,
+// whenever at least kRefill lanes are idle. Each loop iteration handles one stack entry per active
+// lane (a node visit or a leaf's triangles) with the per-ray order of trace_closest / trace_any, so
+// the hits equal those of the single-ray form bit for bit. Rays are read and hits written with
 // streaming cache hints so that the ray stream does not evict the BVH from L2.
 #ifndef VT_TRACE_REFILL
 #define VT_TRACE_REFILL 8
@@ -147,6 +167,12 @@ __device__ __forceinline__ uint32_t refill(unsigned idle, uint32_t *counter, uin
 // word d * kBlock + t, so every lane of a warp hits its own bank whatever its stack depth.
 __device__ __forceinline__ int *stack_slot(int *sstack, int d) { return sstack + d * kBlock + threadIdx.x; }
 
+// Stack entries: an inner node is its index (>= 0); a leaf child is ~(node << 2 | slot).
+
+// Per lane, one iteration handles the top stack entry: a node visit (its hit children, leaves
+// included, pushed far to near, so they pop near first) or one leaf's triangle tests. The warp runs
+// only the kind more of its lanes need this iteration; the others wait one iteration. A ray's own
+// order (LIFO over its stack) does not depend on the warp.
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__restrict__ nodes,
                                                         const float4 *__restrict__ tris, float rootMax,
                                                         const float4 *__restrict__ rays, uint32_t n,
@@ -174,16 +200,15 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
       }
     }
     if (exhausted && !__any_sync(kFull, top > 0)) break;
-    if (top == 0) continue;
-    Node4 nd;
-    load_node(nodes, *stack_slot(sstack, --top), nd);
-    float nearT[4];
-    const int mask = node_hits(nd, s.sr, s.tMin, closest, nearT);
-    const Sorted4 o = sort_children(nd, mask, nearT);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (j >= o.m || o.child[j] > 0 || beyond(o.key[j], closest)) continue;
-      const int first = -o.child[j] - 1, cnt = o.count[j];
+    const int entry = top > 0 ? *stack_slot(sstack, top - 1) : 0;
+    const bool leaf = top > 0 && entry < 0;
+    const unsigned leaves = __ballot_sync(kFull, leaf), inner = __ballot_sync(kFull, top > 0 && !leaf);
+    const bool leafPhase = __popc(leaves) >= __popc(inner);
+    if (top == 0 || leaf != leafPhase) continue;
+    --top;
+    if (leaf) {
+      int first, cnt;
+      leaf_range(nodes, entry, first, cnt);
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
@@ -191,12 +216,19 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
         if (!intersect_tri(s.wr, a, b, cc, s.tMin, closest, t, b1, b2)) continue;
         closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w);
       }
-    }
+    } else {
+      Node4 nd;
+      load_node(nodes, entry, nd);
+      float nearT[4];
+      const int mask = node_hits(nd, s.sr, s.tMin, closest, nearT);
+      const Sorted4 o = sort_children(nd, mask, nearT);
 #pragma unroll
-    for (int j = 3; j >= 0; --j) {
-      if (j >= o.m || o.child[j] <= 0 || beyond(o.key[j], closest)) continue;
-      if (top < stackSize) *stack_slot(sstack, top++) = o.child[j];
-      else atomicOr(status, (uint32_t)VT_DEV_STACK);
+      for (int j = 3; j >= 0; --j) {
+        if (j >= o.m || beyond(o.key[j], closest)) continue;
+        const int e = o.child[j] > 0 ? o.child[j] : leaf_entry_of(entry, (int)(o.key[j] & 3u));
+        if (top < stackSize) *stack_slot(sstack, top++) = e;
+        else atomicOr(status, (uint32_t)VT_DEV_STACK);
+      }
     }
     if (top == 0) {
       const int4 out = prim >= 0 ? make_int4(__float_as_int(closest), __float_as_int(hb1), __float_as_int(hb2), prim)
@@ -229,27 +261,34 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_any(const float4 *__rest
       }
     }
     if (exhausted && !__any_sync(kFull, top > 0)) break;
-    if (top == 0) continue;
-    Node4 nd;
-    load_node(nodes, *stack_slot(sstack, --top), nd);
-    float nearT[4];
-    const int mask = node_hits(nd, s.sr, s.tMin, s.tMax, nearT);
+    const int entry = top > 0 ? *stack_slot(sstack, top - 1) : 0;
+    const bool leaf = top > 0 && entry < 0;
+    const unsigned leaves = __ballot_sync(kFull, leaf), inner = __ballot_sync(kFull, top > 0 && !leaf);
+    const bool leafPhase = __popc(leaves) >= __popc(inner);
+    if (top == 0 || leaf != leafPhase) continue;
+    --top;
     bool hit = false;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (hit || !(mask >> k & 1)) continue;
-      const int c = i4(nd.child, k);
-      if (c > 0) {
-        if (top < stackSize) *stack_slot(sstack, top++) = c;
-        else atomicOr(status, (uint32_t)VT_DEV_STACK);
-        continue;
-      }
-      const int first = -c - 1, cnt = i4(nd.count, k);
+    if (leaf) {
+      int first, cnt;
+      leaf_range(nodes, entry, first, cnt);
       for (int q = 0; q < cnt; ++q) {
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
         float t, b1, b2;
         if (intersect_tri(s.wr, a, b, cc, s.tMin, s.tMax, t, b1, b2)) { hit = true; break; }
+      }
+    } else {
+      Node4 nd;
+      load_node(nodes, entry, nd);
+      float nearT[4];
+      const int mask = node_hits(nd, s.sr, s.tMin, s.tMax, nearT);
+#pragma unroll
+      for (int k = 3; k >= 0; --k) {
+        if (!(mask >> k & 1)) continue;
+        const int c = i4(nd.child, k);
+        const int e = c > 0 ? c : leaf_entry_of(entry, k);
+        if (top < stackSize) *stack_slot(sstack, top++) = e;
+        else atomicOr(status, (uint32_t)VT_DEV_STACK);
       }
     }
     if (hit) top = 0;
@@ -353,7 +392,7 @@ __global__ void k_ray_keys(const float4 *__restrict__ rays, uint32_t n, float3 l
 namespace {
 // Stack entries a traversal of a tree of `depth` levels needs: the root, then at most 3 net pushes
 // per level below it (a visit pops one node and pushes up to four).
-inline int stack_entries(uint32_t depth) { return depth <= 1 ? 1 : 3 * (int)(depth - 1) + 1; }
+inline int stack_entries(uint32_t depth) { return 3 * (int)depth + 1; }
 
 // Resident blocks per SM for a persistent kernel with `smem` bytes of dynamic shared memory.
 template <typename K> int resident_blocks(K kernel, size_t smem) {

@@ -78,6 +78,8 @@ vt_status check_trace_args(vt_ctx *ctx, const vt_mesh *mesh, const void *rays, c
   if (!mesh) return vt_fail(ctx, VT_ERR_INVALID, "mesh is null");
   if (n > 0 && (!rays || !out)) return vt_fail(ctx, VT_ERR_INVALID, "rays or output is null");
   if (n > 0 && mesh->nfaces > 0 && !mesh->d_nodes) return vt_fail(ctx, VT_ERR_INVALID, "mesh has no nodes");
+  // Leaf stack entries hold (node << 2 | slot) in 31 bits.
+  if (mesh->nnodes >= (1u << 29)) return vt_fail(ctx, VT_ERR_LIMIT, "traversal supports up to 2^29 - 1 wide nodes");
   return VT_OK;
 }
 

@@ -919,9 +919,43 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
   SlabRay<T> s = make_slab(r, T(h.root_max));
   T closest = r.tmax;
   bool found = false;
-  int stack[128];
+  int stack[160];
   int top = 0;
   stack[top++] = 0;
+  if (std::is_same<T, float>::value) {
+    // The CUDA kernels' order: leaf children are stack entries ~(node << 2 | slot), pushed with the
+    // inner children far to near, so a ray pops its entries near first.
+    while (top > 0) {
+      const int entry = stack[--top];
+      if (entry < 0) {
+        const int code = ~entry;
+        const vt_wide_node &ln = h.nodes[code >> 2];
+        const int first = -ln.child[code & 3] - 1, cnt = ln.count[code & 3];
+        for (int q = 0; q < cnt; ++q) {
+          const float *tf = &h.tris[9 * (size_t)(first + q)];
+          T a[3] = {T(tf[0]), T(tf[1]), T(tf[2])}, b[3] = {T(tf[3]), T(tf[4]), T(tf[5])},
+            c[3] = {T(tf[6]), T(tf[7]), T(tf[8])};
+          T t, b1, b2;
+          if (tests) ++*tests;
+          if (!intersect_tri<T>(w, a, b, c, r.tmin, closest, t, b1, b2)) continue;
+          closest = t; prim = h.order[first + q]; hb1 = b1; hb2 = b2; found = true;
+        }
+        continue;
+      }
+      const vt_wide_node &nd = h.nodes[entry];
+      if (nodes) ++*nodes;
+      T nearT[4];
+      const int mask = node_hits(nd, s, r.tmin, closest, nearT);
+      const ChildOrder<T> co(mask, nearT);
+      for (int j = co.m - 1; j >= 0; --j) {
+        const int k = co.order[j];
+        if (co.beyond(j, closest) || top >= 160) continue;
+        stack[top++] = nd.child[k] > 0 ? nd.child[k] : ~((entry << 2) | k);
+      }
+    }
+    best = closest;
+    return found;
+  }
   while (top > 0) {
     const vt_wide_node &nd = h.nodes[stack[--top]];
     if (nodes) ++*nodes;
@@ -945,7 +979,7 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
     }
     for (int j = m - 1; j >= 0; --j) {
       int k = co.order[j];
-      if (nd.child[k] > 0 && !co.beyond(j, closest) && top < 128) stack[top++] = nd.child[k];
+      if (nd.child[k] > 0 && !co.beyond(j, closest) && top < 160) stack[top++] = nd.child[k];
     }
   }
   best = closest;
@@ -958,9 +992,39 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
   if (h.nodes.empty()) return false;
   WRay<T> w = make_wray(r.o, r.d);
   SlabRay<T> s = make_slab(r, T(h.root_max));
-  int stack[128];
+  int stack[160];
   int top = 0;
   stack[top++] = 0;
+  if (std::is_same<T, float>::value && !slack) {
+    // The CUDA kernels' order: leaf children are stack entries, pushed with the inner children from
+    // slot 3 down to slot 0.
+    while (top > 0) {
+      const int entry = stack[--top];
+      if (entry < 0) {
+        const int code = ~entry;
+        const vt_wide_node &ln = h.nodes[code >> 2];
+        const int first = -ln.child[code & 3] - 1, cnt = ln.count[code & 3];
+        for (int q = 0; q < cnt; ++q) {
+          const float *tf = &h.tris[9 * (size_t)(first + q)];
+          T a[3] = {T(tf[0]), T(tf[1]), T(tf[2])}, b[3] = {T(tf[3]), T(tf[4]), T(tf[5])},
+            c[3] = {T(tf[6]), T(tf[7]), T(tf[8])};
+          T t, b1, b2;
+          if (tests) ++*tests;
+          if (intersect_tri<T>(w, a, b, c, r.tmin, r.tmax, t, b1, b2)) return true;
+        }
+        continue;
+      }
+      const vt_wide_node &nd = h.nodes[entry];
+      if (nodes) ++*nodes;
+      T nearT[4];
+      const int mask = node_hits(nd, s, r.tmin, r.tmax, nearT);
+      for (int k = 3; k >= 0; --k) {
+        if (!(mask >> k & 1) || top >= 160) continue;
+        stack[top++] = nd.child[k] > 0 ? nd.child[k] : ~((entry << 2) | k);
+      }
+    }
+    return false;
+  }
   while (top > 0) {
     const vt_wide_node &nd = h.nodes[stack[--top]];
     if (nodes) ++*nodes;
@@ -968,7 +1032,7 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
     int mask = node_hits(nd, s, r.tmin, r.tmax, nearT);
     for (int k = 0; k < 4; ++k) {
       if (!(mask >> k & 1)) continue;
-      if (nd.child[k] > 0) { if (top < 128) stack[top++] = nd.child[k]; continue; }
+      if (nd.child[k] > 0) { if (top < 160) stack[top++] = nd.child[k]; continue; }
       int first = -nd.child[k] - 1;
       for (int q = 0; q < nd.count[k]; ++q) {
         const float *tf = &h.tris[9 * (size_t)(first + q)];
