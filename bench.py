@@ -355,13 +355,13 @@ def main():
     for name, (rays, closest) in zip(names, sets):
         counts[name] = mesh.count(rays, closest=closest)
 
-    # Roofline for the dominant launch: algorithmic bytes = node fetches x 128 B + triangle tests
+    # Roofline for the dominant launch: algorithmic bytes = node fetches x 64 B (quantised nodes) + triangle tests
     # x 48 B + ray record 32 B + result (16 B hit / 1 B flag), per launch, over its event duration.
     dom = int(np.argmax(kernel_ms))
     nv, nt = counts[names[dom]]
     n_rays = sets[dom][0].shape[0]
     out_b = 16 if sets[dom][1] else 1
-    alg_bytes = nv * 128 + nt * 48 + n_rays * (32 + out_b)
+    alg_bytes = nv * 64 + nt * 48 + n_rays * (32 + out_b)
     achieved = alg_bytes / (kernel_ms[dom] / 1e3) / 1e9
     peaks_path = ROOT / "MEASURED_PEAKS.json"
     peak, peak_src = 6650.0, "fallback"

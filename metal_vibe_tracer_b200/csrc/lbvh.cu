@@ -612,6 +612,10 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
   }
   if (primBase != n) return vt_fail(ctx, VT_ERR_DEVICE, "collapse emitted " + std::to_string(primBase) + " of " + std::to_string(n) + " triangles");
 
+  {
+    const vt_status qs = vt_quantize_nodes(ctx, mesh, s);
+    if (qs != VT_OK) return qs;
+  }
   // Keep the refined binary tree for parity checks.
   if (n >= 2) {
     VT_CUDA(ctx, cudaMalloc(&mesh->d_bin_child, 2 * (size_t)(n - 1) * sizeof(int32_t)));

@@ -202,4 +202,118 @@ __device__ __forceinline__ bool beyond(uint32_t key, float closest) {
   return (key & ~3u) > ord32(__fadd_rn(closest, 0.0f));
 }
 
+// ---- quantised nodes (qnode.cu): conservative decoding ---------------------------------------
+// A child's near distance on an axis is a lower bound, and its far distance an upper bound, of the
+// exact distances to the decoded planes p + q 2^e, which enclose the child's box: every product
+// and sum is rounded toward the safe side (FFMA.RM / FFMA.RP), so the test never culls a child the
+// reference's slab test (on the exact box, origin shifted by e) keeps. Per ray: the inverse
+// direction, and per axis the slab origins of the near and far planes times the inverse, rounded
+// up and down respectively.
+struct QRay {
+  float invx, invy, invz;
+  float nx, ny, nz;  // round-up (near-plane origin) * inv
+  float fx, fy, fz;  // round-down (far-plane origin) * inv
+  uint32_t neg;      // bit a: the ray runs toward decreasing coordinates on axis a
+};
+
+__device__ __forceinline__ QRay make_qray(float ox, float oy, float oz, float dx, float dy, float dz, float rootMax) {
+  const SlabRay sr = make_slab(ox, oy, oz, dx, dy, dz, rootMax);
+  QRay q;
+  q.invx = sr.invx; q.invy = sr.invy; q.invz = sr.invz;
+  const bool nx = sr.invx < 0.0f, ny = sr.invy < 0.0f, nz = sr.invz < 0.0f;
+  q.neg = (nx ? 1u : 0u) | (ny ? 2u : 0u) | (nz ? 4u : 0u);
+  // The lo plane pairs with the origin shifted by +e (low), the hi plane with -e (high).
+  q.nx = __fmul_ru(nx ? sr.highx : sr.lowx, sr.invx);
+  q.ny = __fmul_ru(ny ? sr.highy : sr.lowy, sr.invy);
+  q.nz = __fmul_ru(nz ? sr.highz : sr.lowz, sr.invz);
+  q.fx = __fmul_rd(nx ? sr.lowx : sr.highx, sr.invx);
+  q.fy = __fmul_rd(ny ? sr.lowy : sr.highy, sr.invy);
+  q.fz = __fmul_rd(nz ? sr.lowz : sr.highz, sr.invz);
+  return q;
+}
+
+struct QNode {
+  float px, py, pz;
+  uint32_t e;
+  uint32_t qlo[3], qhi[3];
+  int4 child;
+  uint32_t counts;
+};
+
+__device__ __forceinline__ void load_qnode(const float4 *__restrict__ qnodes, int i, QNode &n) {
+  const float4 *p = qnodes + 4 * (size_t)i;
+  float4 a, b, c, d;
+  ld256(p, a, b);
+  ld256(p + 2, c, d);
+  n.px = a.x; n.py = a.y; n.pz = a.z; n.e = __float_as_uint(a.w);
+  n.qlo[0] = __float_as_uint(b.x); n.qlo[1] = __float_as_uint(b.y); n.qlo[2] = __float_as_uint(b.z);
+  n.qhi[0] = __float_as_uint(b.w); n.qhi[1] = __float_as_uint(c.x); n.qhi[2] = __float_as_uint(c.y);
+  n.child = make_int4(__float_as_int(c.z), __float_as_int(c.w), __float_as_int(d.x), __float_as_int(d.y));
+  n.counts = __float_as_uint(d.z);
+}
+
+// Byte k of w as the float 1 + byte 2^-15 (the byte in mantissa bits 8-15), exact.
+__device__ __forceinline__ float qbyte(uint32_t w, int k) {
+  return __uint_as_float(__byte_perm(w, 0x3F800000u, 0x7604u | ((uint32_t)k << 4)));
+}
+
+struct QAxis {
+  float d, cn, cf;   // 2^15 step * inv; near and far offsets minus that (the byte's bias)
+  uint32_t nw, fw;   // near-plane and far-plane bytes
+};
+
+// A plane at p + q 2^e lies at (1 + q 2^-15) d + (p * inv - origin * inv - d) with d = 2^(e+15) inv;
+// the bias removal rounds to the safe side too, so the bound loosens by at most 2^-9 of a step.
+__device__ __forceinline__ QAxis q_axis(float p, uint32_t eb, uint32_t qlo, uint32_t qhi, float inv, float nO, float fO,
+                                        bool neg) {
+  QAxis a;
+  a.d = __uint_as_float((eb + 15u) << 23) * inv;  // 2^(e+15) * inv, exact
+  a.cn = __fadd_rd(__fmaf_rd(p, inv, -nO), -a.d);
+  a.cf = __fadd_ru(__fmaf_ru(p, inv, -fO), -a.d);
+  a.nw = neg ? qhi : qlo;
+  a.fw = neg ? qlo : qhi;
+  return a;
+}
+
+// Child hit mask and entry distances of a quantised node.
+__device__ __forceinline__ int qnode_hits(const QNode &n, const QRay &r, float tMin, float tMax, float nearT[4]) {
+  const QAxis x = q_axis(n.px, n.e & 0xffu, n.qlo[0], n.qhi[0], r.invx, r.nx, r.fx, (r.neg & 1u) != 0u);
+  const QAxis y = q_axis(n.py, (n.e >> 8) & 0xffu, n.qlo[1], n.qhi[1], r.invy, r.ny, r.fy, (r.neg & 2u) != 0u);
+  const QAxis z = q_axis(n.pz, (n.e >> 16) & 0xffu, n.qlo[2], n.qhi[2], r.invz, r.nz, r.fz, (r.neg & 4u) != 0u);
+  int mask = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float nxk = __fmaf_rd(qbyte(x.nw, k), x.d, x.cn), fxk = __fmaf_ru(qbyte(x.fw, k), x.d, x.cf);
+    const float nyk = __fmaf_rd(qbyte(y.nw, k), y.d, y.cn), fyk = __fmaf_ru(qbyte(y.fw, k), y.d, y.cf);
+    const float nzk = __fmaf_rd(qbyte(z.nw, k), z.d, z.cn), fzk = __fmaf_ru(qbyte(z.fw, k), z.d, z.cf);
+    const float nt = fmaxf(fmaxf(nxk, nyk), fmaxf(nzk, tMin));
+    const float ft = fminf(fminf(fxk, fyk), fminf(fzk, tMax));
+    nearT[k] = nt;
+    mask |= (nt <= ft && i4(n.child, k) != 0) ? (1 << k) : 0;
+  }
+  return mask;
+}
+
+// Hit children of a quantised node near to far (the packed-key network of sort_children).
+__device__ __forceinline__ Sorted4 sort_qchildren(const QNode &nd, int mask, const float nearT[4]) {
+  uint32_t k[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    k[c] = (mask >> c & 1) ? ((ord32(__fadd_rn(nearT[c], 0.0f)) & ~3u) | (uint32_t)c) : 0xffffffffu;
+  ucswap(k[0], k[1]);
+  ucswap(k[2], k[3]);
+  ucswap(k[0], k[2]);
+  ucswap(k[1], k[3]);
+  ucswap(k[1], k[2]);
+  Sorted4 o;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    o.key[j] = k[j];
+    o.child[j] = pick4(nd.child, k[j] & 3u);
+    o.count[j] = (int)((nd.counts >> (4u * (k[j] & 3u))) & 15u);
+  }
+  o.m = __popc(mask);
+  return o;
+}
+
 }  // namespace vtd

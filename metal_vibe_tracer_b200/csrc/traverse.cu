@@ -27,10 +27,10 @@ using namespace vtd;
 // the slot's first triangle and count from the node, in L1 since the node's visit.
 __device__ __forceinline__ int leaf_entry_of(int node, int slot) { return ~((node << 2) | slot); }
 __device__ __forceinline__ void leaf_range(const float4 *__restrict__ nodes, int entry, int &first, int &cnt) {
-  const int code = ~entry;
-  const int *nd = reinterpret_cast<const int *>(nodes + 8 * (size_t)(code >> 2));
-  first = -__ldg(nd + 24 + (code & 3)) - 1;
-  cnt = __ldg(nd + 28 + (code & 3));
+  const int code = ~entry, slot = code & 3;
+  const int *nd = reinterpret_cast<const int *>(nodes + 4 * (size_t)(code >> 2));
+  first = -__ldg(nd + 10 + slot) - 1;
+  cnt = (__ldg(nd + 14) >> (4 * slot)) & 15;
 }
 
 template <bool kCount>
@@ -39,7 +39,7 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
                                               float4 r0, float4 r1, float &best, float &hb1,
                                               float &hb2, int &prim, uint32_t &nv, uint32_t &nt) {
   const WRay wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-  const SlabRay sr = make_slab(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
+  const QRay qr = make_qray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
   const float tMin = r0.w;
   float closest = r1.w;
   bool found = false;
@@ -61,12 +61,12 @@ __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
       }
       continue;
     }
-    Node4 nd;
-    load_node(nodes, entry, nd);
+    QNode nd;
+    load_qnode(nodes, entry, nd);
     if (kCount) ++nv;
     float nearT[4];
-    const int mask = node_hits(nd, sr, tMin, closest, nearT);
-    const Sorted4 o = sort_children(nd, mask, nearT);
+    const int mask = qnode_hits(nd, qr, tMin, closest, nearT);
+    const Sorted4 o = sort_qchildren(nd, mask, nearT);
 #pragma unroll
     for (int j = 3; j >= 0; --j) {
       if (j >= o.m || beyond(o.key[j], closest) || top >= kStack) continue;
@@ -82,7 +82,7 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
                                           const float4 *__restrict__ tris, float rootMax, float4 r0,
                                           float4 r1, uint32_t &nv, uint32_t &nt) {
   const WRay wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-  const SlabRay sr = make_slab(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
+  const QRay qr = make_qray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
   const float tMin = r0.w, tMax = r1.w;
   int stack[kStack];
   int top = 0;
@@ -101,11 +101,11 @@ __device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
       }
       continue;
     }
-    Node4 nd;
-    load_node(nodes, entry, nd);
+    QNode nd;
+    load_qnode(nodes, entry, nd);
     if (kCount) ++nv;
     float nearT[4];
-    const int mask = node_hits(nd, sr, tMin, tMax, nearT);
+    const int mask = qnode_hits(nd, qr, tMin, tMax, nearT);
 #pragma unroll
     for (int k = 3; k >= 0; --k) {
       if (!(mask >> k & 1) || top >= kStack) continue;
@@ -138,7 +138,7 @@ constexpr int kMinBlocks = VT_TRACE_MIN_BLOCKS;  // register budget: 65536 / (kB
 
 struct RayState {
   WRay wr;
-  SlabRay sr;
+  QRay qr;
   float tMin, tMax;
 };
 
@@ -146,7 +146,7 @@ __device__ __forceinline__ void load_ray(const float4 *__restrict__ rays, uint32
                                          float rootMax) {
   const float4 r0 = __ldcs(rays + 2 * (size_t)r), r1 = __ldcs(rays + 2 * (size_t)r + 1);
   s.wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-  s.sr = make_slab(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
+  s.qr = make_qray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
   s.tMin = r0.w;
   s.tMax = r1.w;
 }
@@ -217,11 +217,11 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
         closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w);
       }
     } else {
-      Node4 nd;
-      load_node(nodes, entry, nd);
+      QNode nd;
+      load_qnode(nodes, entry, nd);
       float nearT[4];
-      const int mask = node_hits(nd, s.sr, s.tMin, closest, nearT);
-      const Sorted4 o = sort_children(nd, mask, nearT);
+      const int mask = qnode_hits(nd, s.qr, s.tMin, closest, nearT);
+      const Sorted4 o = sort_qchildren(nd, mask, nearT);
 #pragma unroll
       for (int j = 3; j >= 0; --j) {
         if (j >= o.m || beyond(o.key[j], closest)) continue;
@@ -278,10 +278,10 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_any(const float4 *__rest
         if (intersect_tri(s.wr, a, b, cc, s.tMin, s.tMax, t, b1, b2)) { hit = true; break; }
       }
     } else {
-      Node4 nd;
-      load_node(nodes, entry, nd);
+      QNode nd;
+      load_qnode(nodes, entry, nd);
       float nearT[4];
-      const int mask = node_hits(nd, s.sr, s.tMin, s.tMax, nearT);
+      const int mask = qnode_hits(nd, s.qr, s.tMin, s.tMax, nearT);
 #pragma unroll
       for (int k = 3; k >= 0; --k) {
         if (!(mask >> k & 1)) continue;
@@ -415,7 +415,7 @@ void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_h
   const uint32_t want = (n + kBlock - 1) / kBlock;
   const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_closest, smem) * sm_count));
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-  k_closest<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
+  k_closest<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris,
                                        mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
                                        reinterpret_cast<int4 *>(hits), counter, perm, S, status);
 }
@@ -429,7 +429,7 @@ void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t 
   const uint32_t want = (n + kBlock - 1) / kBlock;
   const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_any, smem) * sm_count));
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-  k_any<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
+  k_any<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris,
                                    mesh->root_max, reinterpret_cast<const float4 *>(rays), n, occ, counter, perm,
                                    S, status);
 }
@@ -437,7 +437,7 @@ void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t 
 void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int closest,
                      unsigned long long *acc, cudaStream_t s) {
   if (n == 0) return;
-  k_count<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const float4 *>(mesh->d_nodes), mesh->d_tris,
+  k_count<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris,
                                          mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
                                          closest, acc);
 }

@@ -28,6 +28,7 @@ void free_mesh(vt_mesh *m) {
   cudaFree(m->d_sorted);
   cudaFree(m->d_bin_child);
   cudaFree(m->d_bin_box);
+  cudaFree(m->d_qnodes);
   delete m;
 }
 

@@ -33,6 +33,11 @@ struct vt_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
+// Traversal copy of a 4-wide node with 8-bit child boxes (qnode.cu): 64 bytes, two 32-byte loads.
+struct __align__(64) vt_qnode {
+  uint32_t w[16];
+};
+
 struct vt_mesh {
   uint32_t nfaces = 0;
   uint32_t nnodes = 0;       // 4-wide nodes
@@ -48,6 +53,7 @@ struct vt_mesh {
   int32_t *d_sorted = nullptr;       // sorted position -> input face
   int32_t *d_bin_child = nullptr;    // 2 per binary internal node (refined)
   float *d_bin_box = nullptr;        // 8 per binary internal node (lo xyz, -, hi xyz, -)
+  vt_qnode *d_qnodes = nullptr;      // nnodes, quantised copy read by the traversal kernels
 };
 
 // Light BVH (host words, LightTree.Built).
@@ -143,6 +149,7 @@ size_t vt_radix_temp_words(uint32_t n);
 void vt_radix_sort_pairs(uint32_t *keys, uint32_t *vals, uint32_t *keys_alt, uint32_t *vals_alt,
                          uint32_t n, int bits, uint32_t *temp, cudaStream_t s);
 
+vt_status vt_quantize_nodes(vt_ctx *ctx, vt_mesh *mesh, cudaStream_t s);
 vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
                         uint32_t nverts, const vt_build_options &opt, vt_mesh *mesh);
 

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -123,7 +124,13 @@ struct vto_bvh {
   std::vector<int32_t> sorted;      // face index per sorted position
   std::vector<BinNode> binary;      // refined binary tree (n - 1 internal nodes)
   double sah = 0.0;
+  // The CUDA traversal's copy of the nodes with 8-bit child boxes (16 words each).
+  std::vector<std::array<uint32_t, 16>> qnodes;
 };
+
+namespace {
+void quantize_nodes(vto_bvh &h);
+}  // namespace
 
 namespace {
 
@@ -539,6 +546,7 @@ vto_bvh *vto_lbvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *
   h->binary = t.nodes;
   lbvh_collapse(t, h->sorted, leaf_size, h);
   finish_bvh(h, faces, verts);
+  quantize_nodes(*h);
   return h;
 }
 
@@ -772,6 +780,7 @@ vto_bvh *vto_widebvh_build(const vt_face *faces, uint32_t nfaces, const vt_verte
   if (depth > max_depth) depth = wide_build(bounds.data(), n, leaf_size, true, threads, h->order, h->nodes);
   h->depth = (uint32_t)depth;
   finish_bvh(h, faces, verts);
+  quantize_nodes(*h);
   return h;
 }
 
@@ -911,6 +920,132 @@ int node_hits(const vt_wide_node &n, const SlabRay<T> &w, T tMin, T tMax, T near
   return mask;
 }
 
+// ---- quantised nodes: the CUDA traversal's node copy and its conservative box test ------------------
+// Spec (restated from the CUDA build): per node, p = the children's union lower corner; per axis the
+// smallest e in [-126, 127] with 255 2^e >= (hi - p); per child qlo = floor((lo - p) / 2^e) and
+// qhi = ceil((hi - p) / 2^e), clamped to [0, 255], all in double, e in [-126, 112]. Words: p.xyz,
+// biased exponents, qlo.xyz, qhi.xyz (byte k = child k), child[4], 4-bit leaf counts, 0.
+int quant_exponent(double extent) {
+  if (!(extent > 0.0)) return -126;
+  int e;
+  std::frexp(extent, &e);
+  e = std::min(112, std::max(-126, e - 8));
+  while (e < 112 && std::ldexp(255.0, e) < extent) ++e;
+  while (e > -126 && std::ldexp(255.0, e - 1) >= extent) --e;
+  return e;
+}
+
+uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+float bitsf(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+
+void quantize_nodes(vto_bvh &h) {
+  h.qnodes.assign(h.nodes.size(), {});
+  for (size_t i = 0; i < h.nodes.size(); ++i) {
+    const vt_wide_node &nd = h.nodes[i];
+    std::array<uint32_t, 16> &q = h.qnodes[i];
+    const float *clo[3] = {nd.lox, nd.loy, nd.loz}, *chi[3] = {nd.hix, nd.hiy, nd.hiz};
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    bool any = false;
+    for (int k = 0; k < 4; ++k) {
+      if (nd.child[k] == 0) continue;
+      any = true;
+      for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], clo[a][k]); hi[a] = std::max(hi[a], chi[a][k]); }
+    }
+    if (any) {
+      for (int a = 0; a < 3; ++a) {
+        const float p = lo[a];
+        const int e = quant_exponent(double(hi[a]) - double(p));
+        q[a] = fbits(p);
+        q[3] |= uint32_t(e + 127) << (8 * a);
+        for (int k = 0; k < 4; ++k) {
+          if (nd.child[k] == 0) continue;
+          const double l = std::floor(std::ldexp(double(clo[a][k]) - double(p), -e));
+          const double u = std::ceil(std::ldexp(double(chi[a][k]) - double(p), -e));
+          q[4 + a] |= uint32_t(std::min(std::max(l, 0.0), 255.0)) << (8 * k);
+          q[7 + a] |= uint32_t(std::min(std::max(u, 0.0), 255.0)) << (8 * k);
+        }
+      }
+    }
+    for (int k = 0; k < 4; ++k) {
+      q[10 + k] = uint32_t(nd.child[k]);
+      q[14] |= (uint32_t(nd.count[k]) & 15u) << (4 * k);
+    }
+  }
+}
+
+// Directed rounding of a float FMA / product, from the round-to-nearest result and an exact
+// double-double of the real value (no floating-point environment changes).
+inline void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+// An overflowed result rounds to the largest finite value on the side it is rounded toward.
+inline float overflowed(float s, bool up) {
+  if (s == INFINITY && !up) return FLT_MAX;
+  if (s == -INFINITY && up) return -FLT_MAX;
+  return s;
+}
+inline float fma_dir(float a, float b, float c, bool up) {
+  const float s = std::fmaf(a, b, c);
+  if (!std::isfinite(s)) return std::isfinite(a) && std::isfinite(b) && std::isfinite(c) ? overflowed(s, up) : s;
+  double hi, lo;
+  two_sum(double(a) * double(b), double(c), hi, lo);
+  const double d = double(s) - hi;  // exact: s and hi agree to within a float ulp
+  if (up) return d < lo ? std::nextafter(s, INFINITY) : s;
+  return d > lo ? std::nextafter(s, -INFINITY) : s;
+}
+inline float mul_dir(float a, float b, bool up) {
+  const float s = a * b;
+  if (!std::isfinite(s)) return std::isfinite(a) && std::isfinite(b) ? overflowed(s, up) : s;
+  const double v = double(a) * double(b);
+  if (up) return double(s) < v ? std::nextafter(s, INFINITY) : s;
+  return double(s) > v ? std::nextafter(s, -INFINITY) : s;
+}
+
+struct QRayO {
+  float inv[3], n[3], f[3];
+  bool neg[3];
+};
+QRayO make_qray_o(const SlabRay<float> &s) {
+  QRayO q;
+  for (int a = 0; a < 3; ++a) {
+    q.inv[a] = s.inv[a];
+    q.neg[a] = s.inv[a] < 0.0f;
+    q.n[a] = mul_dir(q.neg[a] ? s.high[a] : s.low[a], s.inv[a], true);
+    q.f[a] = mul_dir(q.neg[a] ? s.low[a] : s.high[a], s.inv[a], false);
+  }
+  return q;
+}
+
+// The CUDA kernels' quantised child test (qnode_hits): lower bounds of near and upper bounds of
+// far plane distances.
+int qnode_hits_o(const std::array<uint32_t, 16> &q, const QRayO &r, float tMin, float tMax, float nearT[4]) {
+  float d[3], cn[3], cf[3];
+  uint32_t nw[3], fw[3];
+  for (int a = 0; a < 3; ++a) {
+    const float p = bitsf(q[a]);
+    d[a] = bitsf((((q[3] >> (8 * a)) & 0xffu) + 15u) << 23) * r.inv[a];
+    cn[a] = fma_dir(1.0f, fma_dir(p, r.inv[a], -r.n[a], false), -d[a], false);
+    cf[a] = fma_dir(1.0f, fma_dir(p, r.inv[a], -r.f[a], true), -d[a], true);
+    nw[a] = r.neg[a] ? q[7 + a] : q[4 + a];
+    fw[a] = r.neg[a] ? q[4 + a] : q[7 + a];
+  }
+  int mask = 0;
+  for (int k = 0; k < 4; ++k) {
+    float nt[3], ft[3];
+    for (int a = 0; a < 3; ++a) {
+      nt[a] = fma_dir(bitsf(0x3F800000u | (((nw[a] >> (8 * k)) & 0xffu) << 8)), d[a], cn[a], false);
+      ft[a] = fma_dir(bitsf(0x3F800000u | (((fw[a] >> (8 * k)) & 0xffu) << 8)), d[a], cf[a], true);
+    }
+    const float n0 = std::fmax(std::fmax(nt[0], nt[1]), std::fmax(nt[2], tMin));
+    const float f0 = std::fmin(std::fmin(ft[0], ft[1]), std::fmin(ft[2], tMax));
+    nearT[k] = n0;
+    if (n0 <= f0 && q[10 + k] != 0u) mask |= 1 << k;
+  }
+  return mask;
+}
+
 template <typename T>
 bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &hb1, T &hb2,
                  uint64_t *nodes = nullptr, uint64_t *tests = nullptr) {
@@ -922,9 +1057,11 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
   int stack[160];
   int top = 0;
   stack[top++] = 0;
-  if (std::is_same<T, float>::value) {
-    // The CUDA kernels' order: leaf children are stack entries ~(node << 2 | slot), pushed with the
-    // inner children far to near, so a ray pops its entries near first.
+  if constexpr (std::is_same<T, float>::value) {
+    // The CUDA kernels' order and node test: quantised nodes; leaf children are stack entries
+    // ~(node << 2 | slot), pushed with the inner children far to near, so a ray pops its entries
+    // near first.
+    const QRayO qr = make_qray_o(s);
     while (top > 0) {
       const int entry = stack[--top];
       if (entry < 0) {
@@ -945,7 +1082,7 @@ bool closest_hit(const vto_bvh &h, const TraceRay<T> &r, T &best, int &prim, T &
       const vt_wide_node &nd = h.nodes[entry];
       if (nodes) ++*nodes;
       T nearT[4];
-      const int mask = node_hits(nd, s, r.tmin, closest, nearT);
+      const int mask = qnode_hits_o(h.qnodes[entry], qr, r.tmin, closest, nearT);
       const ChildOrder<T> co(mask, nearT);
       for (int j = co.m - 1; j >= 0; --j) {
         const int k = co.order[j];
@@ -995,9 +1132,11 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
   int stack[160];
   int top = 0;
   stack[top++] = 0;
-  if (std::is_same<T, float>::value && !slack) {
-    // The CUDA kernels' order: leaf children are stack entries, pushed with the inner children from
-    // slot 3 down to slot 0.
+  if constexpr (std::is_same<T, float>::value) {
+   if (!slack) {
+    // The CUDA kernels' order and node test: quantised nodes; leaf children are stack entries,
+    // pushed with the inner children from slot 3 down to slot 0.
+    const QRayO qr = make_qray_o(s);
     while (top > 0) {
       const int entry = stack[--top];
       if (entry < 0) {
@@ -1017,13 +1156,14 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
       const vt_wide_node &nd = h.nodes[entry];
       if (nodes) ++*nodes;
       T nearT[4];
-      const int mask = node_hits(nd, s, r.tmin, r.tmax, nearT);
+      const int mask = qnode_hits_o(h.qnodes[entry], qr, r.tmin, r.tmax, nearT);
       for (int k = 3; k >= 0; --k) {
         if (!(mask >> k & 1) || top >= 160) continue;
         stack[top++] = nd.child[k] > 0 ? nd.child[k] : ~((entry << 2) | k);
       }
     }
     return false;
+   }
   }
   while (top > 0) {
     const vt_wide_node &nd = h.nodes[stack[--top]];
