@@ -202,6 +202,9 @@ typedef struct vt_frame_params {
                                0 = continue the scene's accumulation */
   uint32_t di_candidates;   /* ReSTIR DI initial candidates per pixel (sampling_mode 0); 0 = the
                                reference's 4 (restir_di_initial, main.swift:4646) */
+  float aperture;           /* thin-lens radius, 0 = pinhole (Uniforms.lens.x, lens_ray,
+                               main.swift:2210-2216) */
+  float focus_distance;     /* distance to the plane in focus along the view axis (Uniforms.lens.y) */
 } vt_frame_params;
 
 /* A renderable scene: the mesh, its material slots, the area light and (optionally) the spectral

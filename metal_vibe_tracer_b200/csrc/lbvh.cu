@@ -390,7 +390,7 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
                                 uint32_t nextBase, uint32_t primBase, vt_wide_node *nodes,
                                 int32_t *nextLevel, const uint32_t *sorted, const vt_face *faces,
                                 const vt_vertex *verts, int32_t *order, float4 *tris,
-                                uint32_t *status) {
+                                uint32_t *status, float4 *nrm = nullptr) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= L) return;
   int4 c4 = chIn[w];
@@ -427,6 +427,11 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
           tris[3 * prim] = make_float4(va.px, va.py, va.pz, __int_as_float((int)f));
           tris[3 * prim + 1] = make_float4(vb.px, vb.py, vb.pz, __uint_as_float(fc.tag));
           tris[3 * prim + 2] = make_float4(vc.px, vc.py, vc.pz, 0.0f);
+          if (nrm) {  // vertex normals for smooth shading (mesh_hit_attributes)
+            nrm[3 * prim] = make_float4(va.nx, va.ny, va.nz, 0.0f);
+            nrm[3 * prim + 1] = make_float4(vb.nx, vb.ny, vb.nz, 0.0f);
+            nrm[3 * prim + 2] = make_float4(vc.nx, vc.ny, vc.nz, 0.0f);
+          }
           ++prim;
           continue;
         }
@@ -532,6 +537,7 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
   VT_CUDA(ctx, cudaMalloc(&mesh->d_sorted, n * sizeof(int32_t)));
   VT_CUDA(ctx, cudaMalloc(&mesh->d_order, n * sizeof(int32_t)));
   VT_CUDA(ctx, cudaMalloc(&mesh->d_tris, 3 * (size_t)n * sizeof(float4)));
+  VT_CUDA(ctx, cudaMalloc(&mesh->d_nrm, 3 * (size_t)n * sizeof(float4)));
   codes = mesh->d_codes;
   vals = reinterpret_cast<uint32_t *>(mesh->d_sorted);
 
@@ -589,7 +595,8 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
     const uint32_t nextBase = base + L;
     k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, chBuf, nInner, nPrims, base,
                                                    nextBase, primBase, nodes, levelB, vals, faces,
-                                                   verts, mesh->d_order, mesh->d_tris, ctx->d_status);
+                                                   verts, mesh->d_order, mesh->d_tris, ctx->d_status,
+                                                   mesh->d_nrm);
     uint32_t st_level = 0;
     VT_CUDA(ctx, cudaMemcpyAsync(host_tot, totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     VT_CUDA(ctx, cudaMemcpyAsync(&st_level, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

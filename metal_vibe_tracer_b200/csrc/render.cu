@@ -43,6 +43,7 @@ constexpr int kRenderBlock = 128;
 
 struct RenderArgs {
   const float4 *nodes, *tris;
+  const float4 *nrm;  // vertex normals per BVH position (3 per triangle)
   float rootMax;
   const vt_material *mats;
   uint32_t nmat;
@@ -72,9 +73,11 @@ struct RenderArgs {
   float3 ltLo, ltScale;
   // ReSTIR DI (sampling mode 0): the primary-surface cache and reservoirs of this frame (written by
   // pass 1, read by pass 2) and of the previous frame (temporal reuse), and the previous camera.
+  float aperture, focus;  // thin lens (aperture 0: pinhole)
   uint32_t diCandidates, diBits, history;
   float4 *gPos, *gNrm;           // (position, distance or -1), (normal, material type)
   uint4 *gInfo;                  // (face, slot | front << 31, error bits, 0)
+  float4 *gGeo;                  // geometric normal (the shading normal is in gNrm)
   float4 *rPos, *rEmit, *rW;     // (position, light id bits), (emission, pdf), (weight sum, M, W, u)
   const float4 *hPos, *hNrm, *hrPos, *hrEmit, *hrW;
   float3 pcam, pfwd, pright, pup;
@@ -175,7 +178,8 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
 
 // ---- surfaces, lights, spectra -----------------------------------------------------------------
 struct Surface {
-  float3 pos, gn;  // position, geometric normal facing the incoming ray (the shading normal)
+  float3 pos, gn;  // position, geometric normal facing the incoming ray
+  float3 n;        // shading normal: the interpolated vertex normals on gn's side, else gn
   float err;       // HitRecord.error: the position's rounding bound
   uint32_t slot, face;
   bool front;      // the ray meets the side cross(b - a, c - a) points to
@@ -203,13 +207,25 @@ __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h,
   s.gn = s.front ? ng : mul(ng, -1.0f);
   s.slot = __float_as_uint(b.w);
   s.face = __float_as_uint(a.w);
+  const float b0 = 1.0f - h.b1 - h.b2;
   if (A.imported) {
-    const float b0 = 1.0f - h.b1 - h.b2;
     s.pos = add(add(mul(f3(a.x, a.y, a.z), b0), mul(f3(b.x, b.y, b.z), h.b1)), mul(f3(c.x, c.y, c.z), h.b2));
     s.err = mesh_hit_error(a, b, c);
   } else {
     s.pos = add(o, mul(d, h.t));
     s.err = kEps;
+  }
+  // mesh_hit_attributes (main.swift:1590-1593): smooth normal when the vertex normals give one.
+  s.n = s.gn;
+  if (A.nrm) {
+    const float4 na = __ldg(A.nrm + 3 * (size_t)h.pos), nb = __ldg(A.nrm + 3 * (size_t)h.pos + 1),
+                 nc = __ldg(A.nrm + 3 * (size_t)h.pos + 2);
+    const float3 sm = add(add(mul(f3(na.x, na.y, na.z), b0), mul(f3(nb.x, nb.y, nb.z), h.b1)),
+                          mul(f3(nc.x, nc.y, nc.z), h.b2));
+    if (dot3(sm, sm) > 1e-12f) {
+      s.n = normalize3(sm);
+      if (dot3(s.n, s.gn) < 0.0f) s.n = mul(s.n, -1.0f);
+    }
   }
   return s;
 }
@@ -597,19 +613,21 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
 }
 
 // NEE at a Lambert vertex: the contribution's rgb (quad: 2 draws; emitters: 4).
-__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float err,
-                                               float3 wo, float4 T, float4 albedo, bool useMIS, Sampler &seed,
-                                               int *stack, bool requirePdf) {
+// n is the shading normal, gn the geometric one (both facing the incoming ray).
+__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
+                                               float err, float3 wo, float4 T, float4 albedo, bool useMIS,
+                                               Sampler &seed, int *stack, bool requirePdf) {
   const LightSample ls = sample_direct(A, p, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
-  if (!light_visible(A, p, n, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
+  if (!light_visible(A, p, gn, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
   const float cosine = fabsf(dot3(n, ls.wi));
-  // eval_bsdf / eval_bsdf_pdf for DIFFUSE (main.swift:2665-2686), shading normal = geometric.
+  // eval_bsdf / eval_bsdf_pdf for DIFFUSE (main.swift:2659-2676): no light below the geometric
+  // surface; cosine, f and pdf from the shading normal.
   float f = 0.0f, bpdf = 0.0f;
   const float ni = dot3(n, ls.wi), no = dot3(n, wo);
   if (no > 0.0f) {
     bpdf = fmaxf(0.0f, ni) * kInvPi;
-    if (ni > 0.0f && cosine >= 1e-7f) f = kInvPi;
+    if (ni > 0.0f && cosine >= 1e-7f && dot3(ls.wi, gn) > 0.0f) f = kInvPi;
   }
   const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
   const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
@@ -640,31 +658,31 @@ __device__ __forceinline__ float light_geometry(const RenderArgs &A, float3 p, c
 }
 
 // Lambert f (eval_bsdf for DIFFUSE, main.swift:2665-2686) as direct_light evaluates it.
-__device__ __forceinline__ float lambert_f(float3 n, float3 wo, float3 wi) {
+__device__ __forceinline__ float lambert_f(float3 n, float3 gn, float3 wo, float3 wi) {
   const float ni = dot3(n, wi), no = dot3(n, wo);
-  return no > 0.0f && ni > 0.0f && fabsf(ni) >= 1e-7f ? kInvPi : 0.0f;
+  return no > 0.0f && ni > 0.0f && fabsf(ni) >= 1e-7f && dot3(wi, gn) > 0.0f ? kInvPi : 0.0f;
 }
 
 // The sample's contribution at the shading point before its weight: bsdf * Le * cos * G, in the
 // sample's own wavelengths (u), as linear sRGB.
-__device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 view,
+__device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
                                                   const vt_material &m, const DISample &c) {
   const float3 dir = normalize3(sub(c.pos, p));
   const float cos_th = fmaxf(0.0f, dot3(n, dir));
   if (cos_th <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
   Lanes L;
   if (A.spectral) L = make_lanes(A, c.u);
-  const float f = lambert_f(n, mul(view, -1.0f), dir);
+  const float f = lambert_f(n, gn, mul(view, -1.0f), dir);
   const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
   const float4 s = scale4(mul4(reflectance(A, m), emission(A, L, e)), f * cos_th);
   return mul(to_rgb(A, L, s), light_geometry(A, p, c));
 }
 
 // eval_restir_target_pdf (main.swift:3187-3197): the length of that contribution.
-__device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 view, const vt_material &m,
-                                           const DISample &c) {
+__device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
+                                           const vt_material &m, const DISample &c) {
   if (c.pdf <= 0.0f) return 0.0f;
-  const float3 v = di_contribution(A, p, n, view, m, c);
+  const float3 v = di_contribution(A, p, n, gn, view, m, c);
   return sqrtf(dot3(v, v));
 }
 
@@ -727,6 +745,20 @@ __device__ __forceinline__ float3 camera_dir(const RenderArgs &A, uint32_t x, ui
   return normalize3(add(A.fwd, add(mul(A.right, u), mul(A.up, v))));
 }
 
+// lens_ray (main.swift:2210-2216): a thin lens moves the origin on the aperture disk (one 2D draw of
+// the vertex-0 lens event) and aims through the point in focus.
+__device__ __forceinline__ void lens_ray(const RenderArgs &A, float3 &o, float3 &d, Sampler &seed) {
+  if (A.aperture <= 0.0f) return;
+  sampler_event(seed, 0u, kZLens);
+  const float2 r = rand_f2(seed);
+  const float radius = sqrtf(r.x) * A.aperture, angle = kTwoPi * r.y;
+  const float3 focus = add(o, mul(d, A.focus / fmaxf(1e-5f, dot3(d, A.fwd))));
+  float sn, cs;
+  sincosf(angle, &sn, &cs);
+  o = add(o, add(mul(A.right, radius * cs), mul(A.up, radius * sn)));
+  d = normalize3(sub(focus, o));
+}
+
 // What the camera sees on an emitter: its radiance, in spectral transport its four-wavelength
 // estimate (emitter_rgb, main.swift:7467-7468); imported emitters emit from their front face only
 // (trace_scene, main.swift:2031).
@@ -760,8 +792,8 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     // sample_bsdf, Lambert: one 3D draw (three PCG draws), the direction from the last two.
     sampler_event(seed, (uint32_t)bounce, kZBsdf);
     const float3 r = rand_f3(seed);
-    const float3 nd = cosine_hemisphere(S.gn, r.y, r.z);
-    const float bpdf = fmaxf(0.0f, dot3(S.gn, nd)) * kInvPi;
+    const float3 nd = cosine_hemisphere(S.n, r.y, r.z);
+    const float bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
     if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
     T = mul4(T, reflectance(A, m));
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
@@ -783,7 +815,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     if (emissionOnly) break;
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light(A, L, S.pos, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit,
+      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -802,12 +834,13 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
   Lanes L;
   if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
-  const float3 dir0 = camera_dir(A, x, y, jit);
+  float3 dir0 = camera_dir(A, x, y, jit), o0 = A.cam;
+  lens_ray(A, o0, dir0, seed);
   Hit h;
-  const bool hit0 = rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack);
+  const bool hit0 = rt_closest(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   if (!hit0) return f3(0.0f, 0.0f, 0.0f);
-  const Surface S = surface_at(A, h, A.cam, dir0);
+  const Surface S = surface_at(A, h, o0, dir0);
   const vt_material m = material(A, S.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission(A, L, S, m);
   float3 R = f3(0.0f, 0.0f, 0.0f);
@@ -815,7 +848,7 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), A.mode == 1u && limit > 0, seed,
+    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
   R = add(R, continue_path(A, L, S, m, dir0, seed, stack, false));
@@ -835,20 +868,22 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
   const uint32_t x = i % A.W, y = i / A.W;
   Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
   const float u = A.spectral ? wavelength_numbers(seed).x : 0.0f;
-  const float3 dir0 = camera_dir(A, x, y, A.jitter[k]);
+  float3 dir0 = camera_dir(A, x, y, A.jitter[k]), o0 = A.cam;
+  lens_ray(A, o0, dir0, seed);
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   Hit h;
-  if (!rt_closest(A, A.cam, dir0, ray_tmin(A, A.cam), __int_as_float(0x7f800000), h, stack)) {
+  if (!rt_closest(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack)) {
     A.gPos[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     A.gNrm[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
     return;
   }
-  const Surface S = surface_at(A, h, A.cam, dir0);
+  const Surface S = surface_at(A, h, o0, dir0);
   const vt_material m = material(A, S.slot);
-  const float4 gp = make_float4(S.pos.x, S.pos.y, S.pos.z, h.t), gn = make_float4(S.gn.x, S.gn.y, S.gn.z, float(m.type));
+  const float4 gp = make_float4(S.pos.x, S.pos.y, S.pos.z, h.t), gn = make_float4(S.n.x, S.n.y, S.n.z, float(m.type));
   A.gPos[i] = gp;
   A.gNrm[i] = gn;
+  A.gGeo[i] = make_float4(S.gn.x, S.gn.y, S.gn.z, 0.0f);
   A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
   if (m.type != VT_MAT_DIFFUSE) {
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
@@ -867,7 +902,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
     DISample cand;
     cand.pos = ls.pos; cand.emission = ls.emission; cand.pdf = ls.pdf; cand.u = u;
     cand.id = ls.face == 0xffffffffu ? 0u : ls.face + 2u;
-    const float pHat = di_target(A, S.pos, S.gn, dir0, m, cand);
+    const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, cand);
     const float proposal = cand.pdf * light_geometry(A, S.pos, cand);
     const float w = proposal > 0.0f ? pHat / proposal : 0.0f;
     r.wsum += w;
@@ -880,13 +915,13 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
     if (same_surface(gp, gn, A.hPos[j], A.hNrm[j]) && hw.y > 0.0f && hw.z > 0.0f) {
       const DISample hs = load_di(A.hrPos, A.hrEmit, A.hrW, j);
       const float cM = fminf(hw.y, 20.0f);
-      const float w = di_target(A, S.pos, S.gn, dir0, m, hs) * hw.z * cM;
+      const float w = di_target(A, S.pos, S.n, S.gn, dir0, m, hs) * hw.z * cM;
       r.M += cM;
       r.wsum += w;
       if (rand_decision(seed) * r.wsum < w) r.s = hs;
     }
   }
-  const float pHat = di_target(A, S.pos, S.gn, dir0, m, r.s);
+  const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, r.s);
   const float W = r.M > 0.0f && pHat > 0.0f ? r.wsum / (r.M * pHat) : 0.0f;
   A.rPos[i] = make_float4(r.s.pos.x, r.s.pos.y, r.s.pos.z, __uint_as_float(r.s.id));
   A.rEmit[i] = make_float4(r.s.emission.x, r.s.emission.y, r.s.emission.z, r.s.pdf);
@@ -905,7 +940,8 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
   Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
   Lanes L;
   if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
-  const float3 dir0 = camera_dir(A, x, y, A.jitter[k]);
+  float3 dir0 = camera_dir(A, x, y, A.jitter[k]), o0 = A.cam;
+  lens_ray(A, o0, dir0, seed);  // the same draws as pass 1
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   const float4 gp = A.gPos[i];
   if (gp.w <= 0.0f) return;
@@ -913,7 +949,9 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
   const uint4 gi = A.gInfo[i];
   Surface S;
   S.pos = f3(gp.x, gp.y, gp.z);
-  S.gn = f3(gn.x, gn.y, gn.z);
+  S.n = f3(gn.x, gn.y, gn.z);
+  const float4 gg = A.gGeo[i];
+  S.gn = f3(gg.x, gg.y, gg.z);
   S.face = gi.x;
   S.slot = gi.y & 0x7fffffffu;
   S.front = (gi.y >> 31) != 0u;
@@ -925,7 +963,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
   } else {
     const float4 cw = A.rW[i];
     DISample sel = load_di(A.rPos, A.rEmit, A.rW, i);
-    float wsum = di_target(A, S.pos, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
+    float wsum = di_target(A, S.pos, S.n, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
     for (int t = 0; t < 4; ++t) {
       const float ox = pcg_rand(seed.state), oy = pcg_rand(seed.state);
       const int nx = (int)x + (int)((ox * 2.0f - 1.0f) * 16.0f), ny = (int)y + (int)((oy * 2.0f - 1.0f) * 16.0f);
@@ -935,16 +973,16 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
       const float4 nw = A.rW[j];
       if (!(nw.y > 0.0f && nw.z > 0.0f)) continue;
       const DISample ns = load_di(A.rPos, A.rEmit, A.rW, j);
-      const float w = di_target(A, S.pos, S.gn, dir0, m, ns) * nw.z * nw.y;
+      const float w = di_target(A, S.pos, S.n, S.gn, dir0, m, ns) * nw.z * nw.y;
       wsum += w;
       M += nw.y;
       if (rand_decision(seed) * wsum < w) sel = ns;
     }
-    const float pHat = di_target(A, S.pos, S.gn, dir0, m, sel);
+    const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, sel);
     const float W = M > 0.0f && pHat > 0.0f ? wsum / (M * pHat) : 0.0f;
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
-      R = mul(di_contribution(A, S.pos, S.gn, dir0, m, sel), W);
+      R = mul(di_contribution(A, S.pos, S.n, S.gn, dir0, m, sel), W);
     R = add(R, continue_path(A, L, S, m, dir0, seed, stack, true));
   }
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) return;
@@ -1274,6 +1312,7 @@ vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *poi
   std::memset(&A, 0, sizeof A);
   A.nodes = reinterpret_cast<const float4 *>(mesh->d_nodes);
   A.tris = mesh->d_tris;
+  A.nrm = mesh->d_nrm;
   A.rootMax = mesh->root_max;
   A.mats = scene->d_mats;
   A.nmat = scene->nmat;
@@ -1357,6 +1396,7 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   std::memset(&A, 0, sizeof A);
   A.nodes = reinterpret_cast<const float4 *>(mesh->d_nodes);
   A.tris = mesh->d_tris;
+  A.nrm = mesh->d_nrm;
   A.rootMax = mesh->root_max;
   A.mats = scene->d_mats;
   A.nmat = scene->nmat;
@@ -1392,6 +1432,8 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.up = make_float3(up[0], up[1], up[2]);
   A.aspect = float(p->width) / float(p->height);
   A.fovScale = std::tan((p->fov_deg * 0.5f) * 3.14159265358979323846f / 180.0f);
+  A.aperture = p->aperture;
+  A.focus = p->focus_distance;
   A.W = p->width;
   A.H = p->height;
   A.maxDepth = p->max_depth;
@@ -1410,7 +1452,7 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
     if (!scene->d_di || scene->di_width != p->width || scene->di_height != p->height) {
       cudaFree(scene->d_di);
       scene->d_di = nullptr;
-      VT_CUDA(ctx, cudaMalloc(&scene->d_di, 11 * (size_t)npix * sizeof(float4)));
+      VT_CUDA(ctx, cudaMalloc(&scene->d_di, 12 * (size_t)npix * sizeof(float4)));
       scene->di_width = p->width;
       scene->di_height = p->height;
       scene->di_frames = 0;
@@ -1422,6 +1464,7 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
     A.diBits = bits;
     float4 *base = scene->d_di;
     A.gInfo = reinterpret_cast<uint4 *>(base + 10 * (size_t)npix);
+    A.gGeo = base + 11 * (size_t)npix;
     const float cam[14] = {A.cam.x, A.cam.y, A.cam.z, A.fwd.x, A.fwd.y, A.fwd.z, A.right.x, A.right.y, A.right.z,
                            A.up.x, A.up.y, A.up.z, A.aspect, A.fovScale};
     const unsigned blocks = (npix + kRenderBlock - 1) / kRenderBlock;

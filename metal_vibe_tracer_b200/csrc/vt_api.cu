@@ -29,6 +29,7 @@ void free_mesh(vt_mesh *m) {
   cudaFree(m->d_bin_child);
   cudaFree(m->d_bin_box);
   cudaFree(m->d_qnodes);
+  cudaFree(m->d_nrm);
   delete m;
 }
 

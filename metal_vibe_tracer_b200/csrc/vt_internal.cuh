@@ -54,6 +54,7 @@ struct vt_mesh {
   int32_t *d_bin_child = nullptr;    // 2 per binary internal node (refined)
   float *d_bin_box = nullptr;        // 8 per binary internal node (lo xyz, -, hi xyz, -)
   vt_qnode *d_qnodes = nullptr;      // nnodes, quantised copy read by the traversal kernels
+  float4 *d_nrm = nullptr;           // 3 per BVH position: the vertex normals (smooth shading)
 };
 
 // Light BVH (host words, LightTree.Built).
@@ -93,7 +94,8 @@ struct vt_scene {
   uint32_t jitter_cap = 0;
   // ReSTIR DI (sampling mode 0): per pixel the primary-surface cache (position, normal) and the
   // reservoir (sample position, emission and pdf, weights) for this frame and the previous one,
-  // plus the primary hit's face/slot/error: 11 float4 per pixel in one allocation.
+  // plus the primary hit's face/slot/error and geometric normal: 12 float4 per pixel in one
+  // allocation.
   float4 *d_di = nullptr;
   uint32_t di_width = 0, di_height = 0, di_frames = 0, di_parity = 0;
   float di_cam[14] = {};  // previous frame's camera: position, forward, right, up, aspect, fov scale

@@ -35,10 +35,11 @@ class FrameParams(C.Structure):
                 ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
                 ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
-                ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32)]
+                ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32),
+                ("aperture", C.c_float), ("focus_distance", C.c_float)]
 
 
-assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 80
+assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 88
 
 
 def make_materials(materials) -> C.Array:
@@ -58,7 +59,7 @@ def make_light(light) -> QuadLight:
 
 
 def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1, sampler=0, z_temporal=3,
-                first_frame=0, di_candidates=0) -> FrameParams:
+                first_frame=0, di_candidates=0, aperture=0.0, focus_distance=1.0) -> FrameParams:
     p = FrameParams()
     p.camera_pos[:] = [float(x) for x in camera["pos"]]
     p.camera_target[:] = [float(x) for x in camera["target"]]
@@ -73,6 +74,7 @@ def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=Tru
     p.z_temporal = int(z_temporal)    # Z++ temporal model (the reference's default: 3, reshuffled)
     p.first_frame = int(first_frame)  # 0: continue the scene's accumulation
     p.di_candidates = int(di_candidates)  # ReSTIR DI candidates (0: the reference's 4)
+    p.aperture, p.focus_distance = float(aperture), float(focus_distance)  # thin lens (0: pinhole)
     return p
 
 

@@ -285,3 +285,71 @@ def cornell_emitters(grid: int = 4, seed: int = 0, lamps: bool = True):
         {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (6.0,) * 3},
         {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (40.0,) * 3}]
     return faces, verts, materials, camera
+
+
+def icosphere(subdivisions: int = 3, center=(0.0, 0.0, 0.0), radius: float = 1.0, displace: float = 0.0,
+              seed: int = 0):
+    """A unit icosahedron subdivided `subdivisions` times (each triangle into 4, midpoints pushed to
+    the sphere), scaled and moved. With `displace` > 0 each vertex moves along its normal by
+    displace * (2 n - 1), n a smooth value noise of the direction (a PCG hash of a 16^3 lattice,
+    trilinear). Returns (positions (V, 3), normals (V, 3), triangles (F, 3)); the normals are
+    the normalised averages of the incident face normals (smooth shading)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    pts = [np.array(p, float) / np.linalg.norm(p) for p in v]
+    for _ in range(subdivisions):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = pts[a] + pts[b]
+                pts.append(m / np.linalg.norm(m))
+                mid[key] = len(pts) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    p = np.array(pts)
+    if displace > 0.0:
+        lattice = np.array([_pcg_hash((seed * 4099 + i) & 0xFFFFFFFF) for i in range(17 ** 3)], np.float64) / 2.0 ** 32
+        g = (p * 0.5 + 0.5) * 16.0
+        i0 = np.clip(np.floor(g).astype(int), 0, 15)
+        fr = g - i0
+        noise = np.zeros(len(p))
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    w = (fr[:, 0] if dx else 1 - fr[:, 0]) * (fr[:, 1] if dy else 1 - fr[:, 1]) * (fr[:, 2] if dz else 1 - fr[:, 2])
+                    noise += w * lattice[((i0[:, 0] + dx) * 17 + (i0[:, 1] + dy)) * 17 + (i0[:, 2] + dz)]
+        p = p * (1.0 + displace * (2.0 * noise - 1.0))[:, None]
+    tri = np.array(f, np.int64)
+    fn = np.cross(p[tri[:, 1]] - p[tri[:, 0]], p[tri[:, 2]] - p[tri[:, 0]])
+    vn = np.zeros_like(p)
+    for k in range(3):
+        np.add.at(vn, tri[:, k], fn)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+    return p * radius + np.asarray(center, float), vn, tri
+
+
+def cornell_sphere(subdivisions: int = 3, seed: int = 0):
+    """The Cornell box (quad light) with a smooth-shaded icosphere (radius 0.3 at (-0.45, -0.7, -0.35),
+    the short box's albedo, vertex normals for shading) in front of the boxes. Returns faces,
+    vertices, materials, the quad light and the camera."""
+    faces, verts, materials, light, camera = cornell_box(seed=seed)
+    p, n, tri = icosphere(subdivisions, (-0.45, -0.7, -0.35), 0.3)
+    base = len(verts)
+    sv = np.zeros(len(p), VERTEX_DTYPE)
+    sv["p"] = p.astype(np.float32)
+    sv["n"] = n.astype(np.float32)
+    sf = np.zeros(len(tri), FACE_DTYPE)
+    sf["a"], sf["b"], sf["c"] = tri[:, 0] + base, tri[:, 1] + base, tri[:, 2] + base
+    sf["tag"] = 6
+    return np.concatenate([faces, sf]), np.concatenate([verts, sv]), materials, light, camera

@@ -1584,7 +1584,7 @@ inline double smax(const PtContext &C, const Spec4 &a) {
   return C.spectral ? std::max(m, a.v[3]) : m;
 }
 
-struct PtHit { D3 pos, gn; double err, t; uint32_t slot, face; bool front; };
+struct PtHit { D3 pos, gn, n; double err, t; uint32_t slot, face; bool front; };
 
 struct PtTri { D3 a, b, c; uint32_t slot; };
 PtTri pt_triangle(const PtContext &C, uint32_t face) {
@@ -1612,6 +1612,15 @@ bool pt_closest(const PtContext &C, D3 o, D3 d, PtHit &h) {
   h.slot = tri.slot;
   h.face = (uint32_t)prim;
   h.t = t;
+  // mesh_hit_attributes (main.swift:1590-1593): the interpolated vertex normals on gn's side.
+  const vt_face &fc = C.in->faces[prim];
+  const vt_vertex &va = C.in->verts[fc.a], &vb = C.in->verts[fc.b], &vc = C.in->verts[fc.c];
+  const D3 sm = D3{va.nx, va.ny, va.nz} * (1.0 - b1 - b2) + D3{vb.nx, vb.ny, vb.nz} * b1 + D3{vc.nx, vc.ny, vc.nz} * b2;
+  h.n = h.gn;
+  if (dot(sm, sm) > 1e-12) {
+    h.n = normalize(sm);
+    if (dot(h.n, h.gn) < 0.0) h.n = h.n * -1.0;
+  }
   if (C.imported) {
     h.pos = tri.a * (1.0 - b1 - b2) + tri.b * b1 + tri.c * b2;
     h.err = mesh_hit_error_d(tri);
@@ -1870,16 +1879,17 @@ bool visible_d(const PtContext &C, D3 p, D3 gn, double err, const PtLight &ls) {
   return !pt_occluded(C, o, delta * (1.0 / d), d - tol);
 }
 
-D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, double err, D3 wo, const Spec4 &T, const Spec4 &albedo,
-            bool useMIS, ZSampler &seed, bool requirePdf) {
+// n: shading normal; gn: geometric normal (eval_bsdf for DIFFUSE, main.swift:2659-2676).
+D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
+            const Spec4 &albedo, bool useMIS, ZSampler &seed, bool requirePdf) {
   const PtLight ls = C.imported ? sample_emitters_d(C, p, seed) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
-  if (!visible_d(C, p, n, err, ls)) return {0, 0, 0};
+  if (!visible_d(C, p, gn, err, ls)) return {0, 0, 0};
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
   double f = 0.0, bpdf = 0.0;
   if (no > 0.0) {
     bpdf = std::max(0.0, ni) / kPi;
-    if (ni > 0.0 && cosine >= 1e-7) f = 1.0 / kPi;
+    if (ni > 0.0 && cosine >= 1e-7 && dot(ls.wi, gn) > 0.0) f = 1.0 / kPi;
   }
   const double w = useMIS ? power_heuristic_d(ls.pdf, bpdf) : 1.0;
   const float le[3] = {(float)ls.emission.x, (float)ls.emission.y, (float)ls.emission.z};
@@ -1899,6 +1909,18 @@ D3 camera_dir_d(const PtContext &C, uint32_t x, uint32_t y, float jx_f, float jy
   u *= C.aspect * C.fovScale;
   v *= C.fovScale;
   return normalize(C.fwd + C.right * u + C.up * v);
+}
+
+// lens_ray (main.swift:2210-2216).
+void lens_d(const PtContext &C, D3 &o, D3 &d, ZSampler &seed) {
+  if (!(C.p->aperture > 0.0f)) return;
+  seed.event(0u, 3u);
+  double r0, r1;
+  seed.f2(r0, r1);
+  const double radius = std::sqrt(r0) * C.p->aperture, angle = 2.0 * kPi * r1;
+  const D3 focus = o + d * (double(C.p->focus_distance) / std::max(1e-5, dot(d, C.fwd)));
+  o = o + C.right * (radius * std::cos(angle)) + C.up * (radius * std::sin(angle));
+  d = normalize(focus - o);
 }
 
 // emitter_rgb at the primary hit (main.swift:7467-7468); imported emitters emit from the front.
@@ -1929,9 +1951,9 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
     const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
     D3 bu, bv;
-    make_basis_d(h.gn, bu, bv);
-    const D3 nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.gn * cos_th);
-    const double bpdf = std::max(0.0, dot(h.gn, nd)) / kPi;
+    make_basis_d(h.n, bu, bv);
+    const D3 nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.n * cos_th);
+    const double bpdf = std::max(0.0, dot(h.n, nd)) / kPi;
     if (!(bpdf > 0.0) || !(dot(nd, h.gn) > 0.0)) break;
     T = mul(T, reflectance(C, m));
     bool finite = true;
@@ -1950,7 +1972,8 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     if (emissionOnly) break;
     if (nee) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.gn, h.err, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed, false);
+      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed,
+                       false);
     }
     if (bounce > 3) {
       const double survival = std::min(std::max(smax(C, T), 0.05), 0.95);
@@ -1982,22 +2005,22 @@ double light_geometry_d(const PtContext &C, D3 p, const DiS &c) {
   return std::max(0.0, dot(d3(C.in->light.normal), delta * (-1.0 / std::sqrt(d2)))) / d2;
 }
 
-D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 view, const vt_material &m, const DiS &c) {
+D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_material &m, const DiS &c) {
   const D3 dir = normalize(c.pos - p);
   const double cos_th = std::max(0.0, dot(n, dir));
   if (cos_th <= 0.0) return {0, 0, 0};
   PtLanes L{};
   if (C.spectral) L = make_lanes(C, c.u);
   const double ni = dot(n, dir), no = -dot(n, view);
-  const double f = no > 0.0 && ni > 0.0 && std::fabs(ni) >= 1e-7 ? 1.0 / kPi : 0.0;
+  const double f = no > 0.0 && ni > 0.0 && std::fabs(ni) >= 1e-7 && dot(dir, gn) > 0.0 ? 1.0 / kPi : 0.0;
   const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
   return to_rgb(C, L, scale(mul(reflectance(C, m), emission(C, L, e)), f * cos_th)) * light_geometry_d(C, p, c);
 }
 
 // eval_restir_target_pdf (main.swift:3187-3197).
-double di_target_d(const PtContext &C, D3 p, D3 n, D3 view, const vt_material &m, const DiS &c) {
+double di_target_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_material &m, const DiS &c) {
   if (c.pdf <= 0.0) return 0.0;
-  const D3 v = di_contribution_d(C, p, n, view, m, c);
+  const D3 v = di_contribution_d(C, p, n, gn, view, m, c);
   return std::sqrt(dot(v, v));
 }
 
@@ -2048,12 +2071,13 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   out = DiPix{};
   ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
   const double u = C.spectral ? seed.wavelength_u() : 0.0;
-  const D3 dir0 = camera_dir_d(C, x, y, jx, jy);
+  D3 dir0 = camera_dir_d(C, x, y, jx, jy), o0 = C.cam;
+  lens_d(C, o0, dir0, seed);
   PtHit h;
-  if (!pt_closest(C, C.cam, dir0, h)) return;
+  if (!pt_closest(C, o0, dir0, h)) return;
   const vt_material m = pt_material(C, h.slot);
   out.hit = h;
-  const double pos[4] = {h.pos.x, h.pos.y, h.pos.z, h.t}, nrm[4] = {h.gn.x, h.gn.y, h.gn.z, double(m.type)};
+  const double pos[4] = {h.pos.x, h.pos.y, h.pos.z, h.t}, nrm[4] = {h.n.x, h.n.y, h.n.z, double(m.type)};
   std::memcpy(out.pos, pos, sizeof pos);
   std::memcpy(out.nrm, nrm, sizeof nrm);
   if (m.type != VT_MAT_DIFFUSE) return;
@@ -2064,7 +2088,7 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
     out.M += 1.0;
     if (!(ls.pdf > 0.0)) continue;
     const DiS cand = di_from_light(ls, u);
-    const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, cand);
+    const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, cand);
     const double proposal = cand.pdf * light_geometry_d(C, h.pos, cand);
     const double w = proposal > 0.0 ? pHat / proposal : 0.0;
     out.wsum += w;
@@ -2075,13 +2099,13 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
     const DiPix &o = prev[(size_t)py * C.p->width + px];
     if (same_surface_d(pos, nrm, o.pos, o.nrm) && o.M > 0.0 && o.W > 0.0) {
       const double cM = std::min(o.M, 20.0);
-      const double w = di_target_d(C, h.pos, h.gn, dir0, m, o.s) * o.W * cM;
+      const double w = di_target_d(C, h.pos, h.n, h.gn, dir0, m, o.s) * o.W * cM;
       out.M += cM;
       out.wsum += w;
       if (seed.decision() * out.wsum < w) out.s = o.s;
     }
   }
-  const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, out.s);
+  const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, out.s);
   out.W = out.M > 0.0 && pHat > 0.0 ? out.wsum / (out.M * pHat) : 0.0;
 }
 
@@ -2090,7 +2114,8 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
   PtLanes L{};
   if (C.spectral) L = make_lanes(C, seed.wavelength_u());
-  const D3 dir0 = camera_dir_d(C, x, y, jx, jy);
+  D3 dir0 = camera_dir_d(C, x, y, jx, jy), o0 = C.cam;
+  lens_d(C, o0, dir0, seed);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
   const DiPix &me = cur[(size_t)y * C.p->width + x];
   if (me.pos[3] <= 0.0) return {0, 0, 0};
@@ -2098,7 +2123,7 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   const vt_material m = pt_material(C, h.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
   DiS sel = me.s;
-  double wsum = di_target_d(C, h.pos, h.gn, dir0, m, sel) * me.W * me.M, M = me.M;
+  double wsum = di_target_d(C, h.pos, h.n, h.gn, dir0, m, sel) * me.W * me.M, M = me.M;
   for (int t = 0; t < 4; ++t) {
     const double ox = seed.pcg(), oy = seed.pcg();
     const int nx = (int)x + (int)((ox * 2.0 - 1.0) * 16.0), ny = (int)y + (int)((oy * 2.0 - 1.0) * 16.0);
@@ -2106,16 +2131,16 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
     const DiPix &n = cur[(size_t)ny * C.p->width + nx];
     if (!compatible_d(me.pos, me.nrm, n.pos, n.nrm)) continue;
     if (!(n.M > 0.0 && n.W > 0.0)) continue;
-    const double w = di_target_d(C, h.pos, h.gn, dir0, m, n.s) * n.W * n.M;
+    const double w = di_target_d(C, h.pos, h.n, h.gn, dir0, m, n.s) * n.W * n.M;
     wsum += w;
     M += n.M;
     if (seed.decision() * wsum < w) sel = n.s;
   }
-  const double pHat = di_target_d(C, h.pos, h.gn, dir0, m, sel);
+  const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, sel);
   const double W = M > 0.0 && pHat > 0.0 ? wsum / (M * pHat) : 0.0;
   D3 R{0, 0, 0};
   if (W > 0.0 && visible_d(C, h.pos, h.gn, h.err, light_from_di(sel, h.pos)))
-    R = di_contribution_d(C, h.pos, h.gn, dir0, m, sel) * W;
+    R = di_contribution_d(C, h.pos, h.n, h.gn, dir0, m, sel) * W;
   R = R + continue_path_d(C, L, h, m, seed, true);
   if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
   return R;
@@ -2125,9 +2150,10 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   ZSampler seed = ZSampler::pixel(x, y, C.p->width, si, C.p->sampler != 0u, C.p->z_temporal, frame);
   PtLanes L{};
   if (C.spectral) L = make_lanes(C, seed.wavelength_u());
-  const D3 dir0 = camera_dir_d(C, x, y, jx_f, jy_f);
+  D3 dir0 = camera_dir_d(C, x, y, jx_f, jy_f), o0 = C.cam;
+  lens_d(C, o0, dir0, seed);
   PtHit h;
-  const bool hit0 = pt_closest(C, C.cam, dir0, h);
+  const bool hit0 = pt_closest(C, o0, dir0, h);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
   if (!hit0) return {0, 0, 0};
   const vt_material m = pt_material(C, h.slot);
@@ -2137,7 +2163,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (C.p->sampling_mode != 3u) {
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), C.p->sampling_mode == 1u && limit > 0,
+    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), C.p->sampling_mode == 1u && limit > 0,
                  seed, true);
   }
   R = R + continue_path_d(C, L, h, m, seed, false);

@@ -224,7 +224,8 @@ class FrameParams(C.Structure):
                 ("max_depth", C.c_uint32), ("camera_up", C.c_float * 3), ("sampling_mode", C.c_uint32),
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
                 ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
-                ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32)]
+                ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32),
+                ("aperture", C.c_float), ("focus_distance", C.c_float)]
 
 
 class PtInputs(C.Structure):
@@ -240,7 +241,7 @@ _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32,
 
 def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
            spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1, light_tree=True,
-           emitter_words=None, di_candidates=0):
+           emitter_words=None, di_candidates=0, aperture=0.0, focus_distance=1.0):
     """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames.
 
     light=None renders an imported scene lit by its emissive faces; its emitter list is the
@@ -285,6 +286,7 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
     p.first_sample, p.spectral = first_sample, 1 if spectral is not None else 0
     p.sampler, p.z_temporal, p.first_frame = sampler, z_temporal, first_frame
     p.di_candidates = di_candidates
+    p.aperture, p.focus_distance = aperture, focus_distance
     out = np.empty(3 * width * height, np.float64)
     lib.vto_render(C.byref(inp), C.byref(p), spp, out.ctypes.data, nthreads or threads())
     return out.reshape(height, width, 3)

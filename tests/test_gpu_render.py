@@ -114,3 +114,45 @@ def test_cornell_z_sampler_matches_oracle(ctx, oracle, cornell, model):
     # Z++ and PCG estimate the same image.
     pcg = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, spectral=tables)
     assert abs(gpu.mean() / pcg.mean() - 1) < 0.02
+
+
+def _parity(gpu, ref, other, same_frac=0.9):
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < MEAN_REL), (gm, rm)
+    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    same = np.all(np.abs(gpu - ref) <= 1e-4 * np.maximum(np.abs(ref), 1e-3), axis=-1)
+    assert same.mean() > same_frac, same.mean()
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_thin_lens_matches_oracle(ctx, oracle, cornell, spectral):
+    """lens_ray (main.swift:2210-2216): aperture 0.05, focus on the tall box."""
+    faces, verts, mats, light, cam, mesh = cornell
+    tables = spectral_tables.load() if spectral else None
+    scene = vt.Scene(ctx, mesh, mats, light, tables)
+    scene.render(vt.make_params(cam, 128, 128, 8, 1, spectral, aperture=0.05, focus_distance=3.0), 16)
+    gpu, _ = scene.readback()
+    scene.close()
+    kw = dict(spectral=tables, aperture=0.05, focus_distance=3.0)
+    ref = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, **kw)
+    other = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, first_sample=1001, **kw)
+    _parity(gpu, ref, other)
+    pinhole = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, spectral=tables)
+    assert relmse(ref, pinhole) > 0.1 * relmse(other, ref)   # the lens changes the image
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_smooth_normals_match_oracle(ctx, oracle, mode):
+    """mesh_hit_attributes (main.swift:1587-1602): shading with interpolated vertex normals."""
+    faces, verts, mats, light, cam = scenes.cornell_sphere()
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, light)
+    scene.render(vt.make_params(cam, 128, 128, 8, 1, False, mode), 16)
+    gpu, _ = scene.readback()
+    scene.close()
+    mesh.close()
+    ref = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, mode=mode)
+    other = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, first_sample=1001, mode=mode)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < (MEAN_REL if mode else 5e-3)), (gm, rm)
+    assert relmse(gpu, ref) < (0.25 if mode else 1.0) * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))

@@ -97,3 +97,15 @@ def test_imported_scene_tree_and_power_agree(oracle):
     qf, qv, qm, light, _ = scenes.cornell_box()
     d = oracle.render(qf, qv, qm, light, cam, 48, 32, 256)
     assert abs(c.mean() / d.mean() - 1) < 0.02
+
+
+def test_smooth_normals_shade_the_sphere(oracle):
+    """Vertex normals change the sphere's shading (mesh_hit_attributes) but not the energy balance."""
+    faces, verts, mats, light, cam = scenes.cornell_sphere()
+    smooth = oracle.render(faces, verts, mats, light, cam, 64, 64, 64)
+    flat_verts = verts.copy()
+    flat_verts["n"] = 0.0
+    flat = oracle.render(faces, flat_verts, mats, light, cam, 64, 64, 64)
+    # Same sample streams: only the sphere's pixels (and what they light) differ.
+    assert np.count_nonzero(np.abs(smooth - flat).max(-1) > 1e-6) > 100
+    assert abs(smooth.mean() / flat.mean() - 1) < 0.05
