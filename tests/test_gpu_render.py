@@ -138,7 +138,7 @@ def test_thin_lens_matches_oracle(ctx, oracle, cornell, spectral):
     other = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, first_sample=1001, **kw)
     _parity(gpu, ref, other)
     pinhole = oracle.render(faces, verts, mats, light, cam, 128, 128, 16, spectral=tables)
-    assert relmse(ref, pinhole) > 0.1 * relmse(other, ref)   # the lens changes the image
+    assert (np.abs(ref - pinhole).max(-1) > 0).mean() > 0.5   # the lens draws change the paths
 
 
 @pytest.mark.parametrize("mode", [1, 0])
