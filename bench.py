@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--profile", action="store_true", help="small run for ncu: no e2e, no CPU leg")
     p.add_argument("--no-cornell", action="store_true", help="skip the integrator measurement")
     p.add_argument("--reference-spp", type=int, default=65536, help="spp of the FP64 reference image")
+    p.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-launch measurement (0: skip)")
+    p.add_argument("--batch-passes", type=int, default=2, help="timed batched passes after the tuning passes")
     return p.parse_args()
 
 
@@ -264,6 +266,50 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     return out
 
 
+def bench_batch(a, ctx) -> dict:
+    """Batched scenes: `batch_scenes` grid scenes (triangles log-uniform in 10k-2M, resolutions from
+    {256, 512, 1024} squared, 4-64 spp) rendered by one persistent launch per pass. The first six
+    passes try launch shapes (block size x work-grab size); the timed passes replay the captured CUDA
+    graph of the fastest. Reports aggregate paths/s and the per-scene completion latency."""
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes
+    from metal_vibe_tracer_b200.render import Batch
+
+    work = scenes.batch_workload(a.batch_scenes, seed=0)
+    t0 = time.perf_counter()
+    meshes, members, params, spp = [], [], [], []
+    for i, (tris, res, n) in enumerate(work):
+        f, v, m, cam = scenes.sphere_grid(tris, seed=i)
+        mesh = vt.Mesh(ctx, f, v)
+        meshes.append(mesh)
+        members.append(vt.Scene(ctx, mesh, m, None))
+        params.append(vt.make_params(cam, res, res, 8, 1, False, 1))
+        spp.append(n)
+    setup_s = time.perf_counter() - t0
+    batch = Batch(ctx, members, params, spp)
+    tune = []
+    while batch.stats()[0].tuned == 0:
+        tune.append(batch.render())
+    timed = [batch.render() for _ in range(a.batch_passes)]
+    st, scene_ms = batch.stats()
+    paths = sum(p.width * p.height * n for p, n in zip(params, spp))
+    ms = sum(timed) / len(timed)
+    out = {"workload": "%d grid scenes (displaced icospheres, %.1fM triangles in all, imported emissive-triangle "
+                       "lighting under light trees), resolutions 256/512/1024 squared, 4-64 spp, MIS, depth 8, RGB"
+                       % (len(work), sum(w[0] for w in work) / 1e6),
+           "paths_per_pass": paths, "ms_per_pass": ms, "paths_per_s": paths / (ms / 1e3),
+           "tuning_ms": tune, "chosen": {"block": st.block, "chunk": st.chunk},
+           "scene_latency_ms": {"median": float(np.median(scene_ms)), "max": float(scene_ms.max()),
+                                "min": float(scene_ms.min())},
+           "gpu_launches_per_pass": 2, "setup_s": setup_s}
+    batch.close()
+    for sc in members:
+        sc.close()
+    for m in meshes:
+        m.close()
+    return out
+
+
 # ---- our arm ----------------------------------------------------------------------------------
 def main():
     a = parse()
@@ -449,6 +495,9 @@ def main():
     cornell = None
     if world == 1 and not a.no_cornell:
         cornell = bench_cornell(a, ctx, dev, stream, cpu_leg=(rank == 0 and not a.no_cpu_baseline))
+    batched = None
+    if world == 1 and not a.no_cornell and a.batch_scenes > 0:
+        batched = bench_batch(a, ctx)
 
     if rank == 0:
         line = {
@@ -464,6 +513,7 @@ def main():
                                          for k, (n, c) in enumerate(counts.items())},
             "build": {"ms": info.build_ms, "sah_cost": info.sah_cost, "wide_nodes": info.wide_nodes, "depth": info.depth},
             "cornell_pt": cornell,
+            "batched_scenes": batched,
         }
         print(json.dumps(line))
     if world > 1:

@@ -239,6 +239,33 @@ vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_
                            uint32_t sample_index, uint32_t frame_index, uint32_t vertex, uint32_t stream,
                            float *out);
 
+/* ---- batched scenes ---------------------------------------------------------------------- */
+
+/* Many scenes of uneven size rendered by one persistent launch per pass (config C4; no counterpart
+ * in the reference, which renders one scene per encodeSample). Each pass renders spp[i] frames of
+ * scene i (sampling modes 1-3) into its accumulation, items being (scene, pixel) pairs handed out
+ * to warps by an atomic work counter. The first passes try six launch shapes (64/128/256 threads,
+ * 1 or 4 items per lane per fetch), one per pass, and keep the fastest, which later passes replay
+ * as one captured CUDA graph. Sample and frame indices advance on the device. A scene belongs to
+ * at most one live batch, and must not be rendered otherwise while its batch lives. */
+typedef struct vt_batch vt_batch;
+typedef struct vt_batch_info {
+  uint32_t scenes, passes;
+  unsigned long long items;   /* pixels per pass */
+  float last_ms;              /* the last pass, device time */
+  uint32_t tuned;             /* 1 once the launch shape is chosen and captured */
+  uint32_t block, chunk;      /* the launch shape of the last pass */
+  uint32_t pad;
+} vt_batch_info;
+vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_params *params, const uint32_t *spp,
+                          uint32_t n, vt_batch **out);
+/* One pass; synchronises (it times the pass). */
+vt_status vt_batch_render(vt_ctx *ctx, vt_batch *batch, void *stream);
+/* Statistics of the last pass; scene_ms (n = scene count, may be NULL) receives each scene's
+ * completion time from the pass's start, in ms. */
+vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *batch, vt_batch_info *out, double *scene_ms, uint32_t n);
+vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *batch);
+
 /* ---- emitter lights: light tree and emitter list ----------------------------------------- */
 
 /* One emitter triangle (LightTree.Emitter, Sources/LightTree.swift:11-16): world corners, power

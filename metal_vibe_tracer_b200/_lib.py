@@ -46,6 +46,11 @@ class LightTreeInfo(C.Structure):
                 ("grid_lo", C.c_float * 3), ("grid_hi", C.c_float * 3)]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("scenes", C.c_uint32), ("passes", C.c_uint32), ("items", C.c_ulonglong), ("last_ms", C.c_float),
+                ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
+
+
 VT_OK = 0
 STATUS_NAMES = {0: "VT_OK", 1: "VT_ERR_INVALID", 2: "VT_ERR_CUDA", 3: "VT_ERR_MEMORY",
                 4: "VT_ERR_LIMIT", 5: "VT_ERR_DEVICE"}
@@ -91,6 +96,10 @@ SIGNATURES = {
     "vt_scene_emitter_words": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_light_estimate": (_I32, [_P, _P, _P, _U32, _U32, _U32, _P]),
     "vt_scene_di_weights": (_I32, [_P, _P, _P, _U32]),
+    "vt_batch_create": (_I32, [_P, _P, _P, _P, _U32, C.POINTER(_P)]),
+    "vt_batch_render": (_I32, [_P, _P, _P]),
+    "vt_batch_stats": (_I32, [_P, _P, C.POINTER(BatchStats), _P, _U32]),
+    "vt_batch_destroy": (_I32, [_P, _P]),
 }
 NOALLOC_MAX_FACES = 32768
 

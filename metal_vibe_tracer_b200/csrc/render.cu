@@ -1017,6 +1017,80 @@ __global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t 
   }
 }
 
+// ---- batched scenes: one persistent launch over many scenes (config C4) ---------------------------
+// frameJitter on the device, with the host's float operations (no contraction).
+__device__ __forceinline__ float halton_d(uint32_t index, uint32_t base) {
+  uint32_t n = index;
+  float fraction = 1.0f, result = 0.0f;
+  while (n > 0) {
+    fraction = __fdiv_rn(fraction, float(base));
+    result = __fadd_rn(result, __fmul_rn(fraction, float(n % base)));
+    n /= base;
+  }
+  return result;
+}
+__device__ __forceinline__ float2 frame_jitter(uint32_t sampleIndex) {
+  const uint32_t n = (max(1u, sampleIndex) - 1u) % 1024u + 1u;
+  return make_float2(__fsub_rn(halton_d(n, 2u), 0.5f), __fsub_rn(halton_d(n, 3u), 0.5f));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Items are (scene, pixel), each running all of the pass's samples of its pixel. Warps take 32 x chunk
+// consecutive items with one atomic; a scene's last finished item stamps its completion time.
+__global__ void __launch_bounds__(256) k_render_batch(const RenderArgs *__restrict__ scenes,
+                                                      const unsigned long long *__restrict__ begin, uint32_t nscenes,
+                                                      unsigned long long total, uint32_t chunk,
+                                                      const uint32_t *__restrict__ firstSample,
+                                                      const uint32_t *__restrict__ firstFrame,
+                                                      unsigned long long *counter, unsigned long long *start,
+                                                      uint32_t *done, unsigned long long *doneNs) {
+  int stack[kRenderStack];
+  if (threadIdx.x == 0) atomicMin(start, global_ns());
+  const uint32_t lane = threadIdx.x & 31u;
+  while (true) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ull * chunk);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= total) break;
+    for (uint32_t j = 0; j < chunk; ++j) {
+      const unsigned long long item = base + lane + 32ull * j;
+      if (item >= total) break;
+      uint32_t lo = 0, hi = nscenes - 1u;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) / 2u;
+        if (begin[mid] <= item) lo = mid; else hi = mid - 1u;
+      }
+      const RenderArgs &A = scenes[lo];
+      const uint32_t p = (uint32_t)(item - begin[lo]);
+      const uint32_t x = p % A.W, y = p / A.W, f0 = firstSample[lo], fr0 = firstFrame[lo];
+      double sr = 0.0, sg = 0.0, sb = 0.0;
+      for (uint32_t k = 0; k < A.spp; ++k) {
+        const float3 c = path_sample(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
+        sr += c.x; sg += c.y; sb += c.z;
+      }
+      double *acc = A.accum + 3 * (size_t)p;
+      acc[0] += sr; acc[1] += sg; acc[2] += sb;
+      const uint32_t items = (uint32_t)(begin[lo + 1] - begin[lo]);
+      if (atomicAdd(done + lo, 1u) == items - 1u) doneNs[lo] = global_ns();
+    }
+  }
+}
+
+// After a pass: each scene's sample and frame indices move on by its spp; counters reset.
+__global__ void k_batch_advance(const RenderArgs *__restrict__ scenes, uint32_t nscenes, uint32_t *firstSample,
+                                uint32_t *firstFrame, uint32_t *done) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nscenes) return;
+  firstSample[s] += scenes[s].spp;
+  firstFrame[s] += scenes[s].spp;
+  done[s] = 0u;
+}
+
 // ---- imported scenes: emitter collection and the light-selection check --------------------------
 __global__ void k_face_positions(const int32_t *__restrict__ order, uint32_t n, int32_t *__restrict__ facePos) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1352,9 +1426,12 @@ vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene) {
   return VT_OK;
 }
 
-vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
-  if (!ctx) return VT_ERR_INVALID;
-  if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+}  // extern "C"
+
+namespace {
+
+// Checks one scene's frame parameters (vt_render's contract).
+vt_status check_params(vt_ctx *ctx, const vt_scene *scene, const vt_frame_params *p) {
   if (p->width == 0 || p->height == 0 || (uint64_t)p->width * p->height > (1u << 28))
     return vt_fail(ctx, VT_ERR_INVALID, "bad image size");
   if (p->sampling_mode > 3)
@@ -1365,34 +1442,26 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   if (p->sampler > 1 || p->z_temporal > 3) return vt_fail(ctx, VT_ERR_INVALID, "sampler must be 0 (PCG) or 1 (Z++), z_temporal 0-3");
   const vt_mesh *mesh = scene->mesh;
   if (mesh->nfaces > 0 && mesh->depth > 32) return vt_fail(ctx, VT_ERR_LIMIT, "BVH deeper than the render stack");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  VT_CUDA(ctx, cudaSetDevice(ctx->device));
-  if (p->width != scene->width || p->height != scene->height || !scene->d_accum) {
-    cudaFree(scene->d_accum);
-    scene->d_accum = nullptr;
-    const size_t bytes = 3 * (size_t)p->width * p->height * sizeof(double);
-    VT_CUDA(ctx, cudaMalloc(&scene->d_accum, bytes));
-    VT_CUDA(ctx, cudaMemset(scene->d_accum, 0, bytes));
-    scene->width = p->width;
-    scene->height = p->height;
-    scene->samples = 0;
-  }
-  if (spp == 0) return VT_OK;
-  if (spp > scene->jitter_cap) {
-    cudaFree(scene->d_jitter);
-    scene->d_jitter = nullptr;
-    VT_CUDA(ctx, cudaMalloc(&scene->d_jitter, spp * sizeof(float2)));
-    scene->jitter_cap = spp;
-  }
-  std::vector<float2> jit(spp);
-  for (uint32_t k = 0; k < spp; ++k) {
-    const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
-    jit[k] = make_float2(halton(n, 2) - 0.5f, halton(n, 3) - 0.5f);
-  }
-  VT_CUDA(ctx, cudaMemcpyAsync(scene->d_jitter, jit.data(), spp * sizeof(float2), cudaMemcpyHostToDevice, s));
-  if (mesh->nfaces == 0) { scene->samples += spp; return VT_OK; }
+  return VT_OK;
+}
 
-  RenderArgs A;
+// Sizes the scene's accumulation to the frame (a new size starts a new accumulation).
+vt_status ensure_accum(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p) {
+  if (p->width == scene->width && p->height == scene->height && scene->d_accum) return VT_OK;
+  cudaFree(scene->d_accum);
+  scene->d_accum = nullptr;
+  const size_t bytes = 3 * (size_t)p->width * p->height * sizeof(double);
+  VT_CUDA(ctx, cudaMalloc(&scene->d_accum, bytes));
+  VT_CUDA(ctx, cudaMemset(scene->d_accum, 0, bytes));
+  scene->width = p->width;
+  scene->height = p->height;
+  scene->samples = 0;
+  return VT_OK;
+}
+
+// The kernel arguments of one scene and frame (everything but the jitter and ReSTIR buffers).
+void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, RenderArgs &A) {
+  const vt_mesh *mesh = scene->mesh;
   std::memset(&A, 0, sizeof A);
   A.nodes = reinterpret_cast<const float4 *>(mesh->d_nodes);
   A.tris = mesh->d_tris;
@@ -1443,9 +1512,46 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   A.zSampler = p->sampler;
   A.zModel = p->z_temporal;
   A.firstFrame = p->first_frame ? p->first_frame : scene->samples + 1u;
-  A.jitter = scene->d_jitter;
   A.accum = scene->d_accum;
   emitter_args(scene, A);
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+  {
+    const vt_status st = check_params(ctx, scene, p);
+    if (st != VT_OK) return st;
+  }
+  const vt_mesh *mesh = scene->mesh;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  {
+    const vt_status st = ensure_accum(ctx, scene, p);
+    if (st != VT_OK) return st;
+  }
+  if (spp == 0) return VT_OK;
+  if (spp > scene->jitter_cap) {
+    cudaFree(scene->d_jitter);
+    scene->d_jitter = nullptr;
+    VT_CUDA(ctx, cudaMalloc(&scene->d_jitter, spp * sizeof(float2)));
+    scene->jitter_cap = spp;
+  }
+  std::vector<float2> jit(spp);
+  for (uint32_t k = 0; k < spp; ++k) {
+    const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
+    jit[k] = make_float2(halton(n, 2) - 0.5f, halton(n, 3) - 0.5f);
+  }
+  VT_CUDA(ctx, cudaMemcpyAsync(scene->d_jitter, jit.data(), spp * sizeof(float2), cudaMemcpyHostToDevice, s));
+  if (mesh->nfaces == 0) { scene->samples += spp; return VT_OK; }
+
+  RenderArgs A;
+  fill_args(scene, p, spp, A);
+  A.jitter = scene->d_jitter;
   const uint32_t npix = p->width * p->height;
   if (p->sampling_mode == 0u) {
     // ReSTIR DI: frames in order, two launches each (the primary pass, then reuse and shading).
@@ -1502,6 +1608,199 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   k_render<<<grid, kRenderBlock, 0, s>>>(A, groups, per);
   VT_CUDA(ctx, cudaGetLastError());
   scene->samples += spp;
+  return VT_OK;
+}
+
+}  // extern "C"
+
+// A batch of scenes rendered by one persistent launch per pass (vt_batch_*).
+struct vt_batch {
+  struct Config {
+    int block;
+    uint32_t chunk;
+    float ms;
+  };
+  std::vector<vt_scene *> scenes;
+  std::vector<uint32_t> spp;
+  unsigned long long total = 0;
+  RenderArgs *d_args = nullptr;
+  unsigned long long *d_begin = nullptr, *d_counter = nullptr, *d_start = nullptr, *d_doneNs = nullptr;
+  uint32_t *d_first = nullptr, *d_frame = nullptr, *d_done = nullptr;
+  std::vector<Config> configs;
+  size_t tried = 0;
+  int best = -1;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float last_ms = 0.0f;
+  uint32_t passes = 0;
+};
+
+namespace {
+
+void batch_free(vt_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->e0) cudaEventDestroy(b->e0);
+  if (b->e1) cudaEventDestroy(b->e1);
+  cudaFree(b->d_args);
+  cudaFree(b->d_begin);
+  cudaFree(b->d_counter);
+  cudaFree(b->d_start);
+  cudaFree(b->d_doneNs);
+  cudaFree(b->d_first);
+  cudaFree(b->d_frame);
+  cudaFree(b->d_done);
+  delete b;
+}
+
+// One pass: reset the work counter and start stamp, run every scene's items, advance the indices.
+cudaError_t batch_enqueue(vt_ctx *ctx, vt_batch *b, const vt_batch::Config &c, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_start, 0xff, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  int perSm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_render_batch, c.block, 0) != cudaSuccess || perSm < 1)
+    perSm = 1;
+  const unsigned long long warps = (b->total + 32ull * c.chunk - 1) / (32ull * c.chunk);
+  const unsigned long long want = (warps * 32ull + c.block - 1) / c.block;
+  const unsigned grid = (unsigned)std::min<unsigned long long>(want, (unsigned long long)perSm * ctx->sm_count);
+  const uint32_t n = (uint32_t)b->scenes.size();
+  k_render_batch<<<grid, c.block, 0, s>>>(b->d_args, b->d_begin, n, b->total, c.chunk, b->d_first, b->d_frame,
+                                           b->d_counter, b->d_start, b->d_done, b->d_doneNs);
+  k_batch_advance<<<(n + 127) / 128, 128, 0, s>>>(b->d_args, n, b->d_first, b->d_frame, b->d_done);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_params *params, const uint32_t *spp,
+                          uint32_t n, vt_batch **out) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scenes || !params || !spp || !out || n == 0) return vt_fail(ctx, VT_ERR_INVALID, "null argument or empty batch");
+  *out = nullptr;
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!scenes[i]) return vt_fail(ctx, VT_ERR_INVALID, "scene " + std::to_string(i) + " is null");
+    for (uint32_t j = 0; j < i; ++j)
+      if (scenes[j] == scenes[i]) return vt_fail(ctx, VT_ERR_INVALID, "a scene appears twice in the batch");
+    const vt_status st = check_params(ctx, scenes[i], params + i);
+    if (st != VT_OK) return st;
+    if (params[i].sampling_mode == 0)
+      return vt_fail(ctx, VT_ERR_INVALID, "batched scenes use sampling modes 1-3 (ReSTIR DI frames run in order per scene)");
+    if (spp[i] == 0 || spp[i] > 65536) return vt_fail(ctx, VT_ERR_INVALID, "spp must be 1 .. 65536 per scene");
+    if (scenes[i]->mesh->nfaces == 0) return vt_fail(ctx, VT_ERR_INVALID, "scene " + std::to_string(i) + " has no faces");
+  }
+  vt_batch *b = new vt_batch();
+  std::vector<RenderArgs> args(n);
+  std::vector<unsigned long long> begin(n + 1, 0);
+  std::vector<uint32_t> first(n), frame(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    vt_status st = ensure_accum(ctx, scenes[i], params + i);
+    if (st != VT_OK) { batch_free(b); return st; }
+    fill_args(scenes[i], params + i, spp[i], args[i]);
+    args[i].jitter = nullptr;
+    first[i] = args[i].first;
+    frame[i] = args[i].firstFrame;
+    begin[i + 1] = begin[i] + (unsigned long long)params[i].width * params[i].height;
+    b->scenes.push_back(scenes[i]);
+    b->spp.push_back(spp[i]);
+  }
+  b->total = begin[n];
+  auto fail = [&](cudaError_t e, const char *what) { batch_free(b); return vt_cuda_fail(ctx, e, what); };
+  cudaError_t e;
+  if ((e = cudaMalloc(&b->d_args, n * sizeof(RenderArgs))) != cudaSuccess) return fail(e, "cudaMalloc(batch args)");
+  if ((e = cudaMalloc(&b->d_begin, (n + 1) * sizeof(unsigned long long))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_counter, sizeof(unsigned long long))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_start, sizeof(unsigned long long))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_doneNs, n * sizeof(unsigned long long))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_first, n * sizeof(uint32_t))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_frame, n * sizeof(uint32_t))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMalloc(&b->d_done, n * sizeof(uint32_t))) != cudaSuccess) return fail(e, "cudaMalloc(batch)");
+  if ((e = cudaMemcpy(b->d_args, args.data(), n * sizeof(RenderArgs), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->d_begin, begin.data(), (n + 1) * sizeof(unsigned long long), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->d_first, first.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemcpy(b->d_frame, frame.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = cudaMemset(b->d_done, 0, n * sizeof(uint32_t))) != cudaSuccess ||
+      (e = cudaMemset(b->d_doneNs, 0, n * sizeof(unsigned long long))) != cudaSuccess)
+    return fail(e, "uploading the batch");
+  if ((e = cudaEventCreate(&b->e0)) != cudaSuccess || (e = cudaEventCreate(&b->e1)) != cudaSuccess)
+    return fail(e, "cudaEventCreate");
+  // Launch shapes the first passes try, one each; the fastest is then captured in a graph.
+  for (int block : {64, 128, 256})
+    for (uint32_t chunk : {1u, 4u}) b->configs.push_back({block, chunk, 0.0f});
+  *out = b;
+  return VT_OK;
+}
+
+vt_status vt_batch_render(vt_ctx *ctx, vt_batch *b, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!b) return vt_fail(ctx, VT_ERR_INVALID, "batch is null");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VT_CUDA(ctx, cudaEventRecord(b->e0, s));
+  if (b->best < 0) {
+    const cudaError_t be = batch_enqueue(ctx, b, b->configs[b->tried], s);
+    if (be != cudaSuccess) return vt_cuda_fail(ctx, be, "batched render");
+  } else {
+    VT_CUDA(ctx, cudaGraphLaunch(b->exec, s));
+  }
+  VT_CUDA(ctx, cudaEventRecord(b->e1, s));
+  VT_CUDA(ctx, cudaEventSynchronize(b->e1));
+  VT_CUDA(ctx, cudaEventElapsedTime(&b->last_ms, b->e0, b->e1));
+  for (size_t i = 0; i < b->scenes.size(); ++i) b->scenes[i]->samples += b->spp[i];
+  ++b->passes;
+  if (b->best < 0) {
+    b->configs[b->tried].ms = b->last_ms;
+    if (++b->tried == b->configs.size()) {
+      b->best = 0;
+      for (size_t c = 1; c < b->configs.size(); ++c)
+        if (b->configs[c].ms < b->configs[b->best].ms) b->best = (int)c;
+      // Capture the fastest shape: later passes replay one graph.
+      VT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const cudaError_t ce = batch_enqueue(ctx, b, b->configs[b->best], ctx->stream);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &g);
+      if (ce != cudaSuccess) { if (g) cudaGraphDestroy(g); return vt_cuda_fail(ctx, ce, "capturing the batch"); }
+      VT_CUDA(ctx, ee);
+      b->graph = g;
+      VT_CUDA(ctx, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+  }
+  return VT_OK;
+}
+
+vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *b, vt_batch_info *out, double *scene_ms, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!b || !out) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
+  if (scene_ms && n != b->scenes.size()) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the batch's scene count");
+  std::memset(out, 0, sizeof *out);
+  out->scenes = (uint32_t)b->scenes.size();
+  out->passes = b->passes;
+  out->items = b->total;
+  out->last_ms = b->last_ms;
+  out->tuned = b->best >= 0 ? 1u : 0u;
+  const vt_batch::Config &c = b->configs[b->best >= 0 ? (size_t)b->best : (b->tried ? b->tried - 1 : 0)];
+  out->block = (uint32_t)c.block;
+  out->chunk = c.chunk;
+  if (scene_ms && b->passes) {
+    std::vector<unsigned long long> done(b->scenes.size());
+    unsigned long long start = 0;
+    VT_CUDA(ctx, cudaDeviceSynchronize());
+    VT_CUDA(ctx, cudaMemcpy(done.data(), b->d_doneNs, done.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    VT_CUDA(ctx, cudaMemcpy(&start, b->d_start, sizeof start, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < done.size(); ++i) scene_ms[i] = done[i] >= start ? double(done[i] - start) * 1e-6 : 0.0;
+  }
+  return VT_OK;
+}
+
+vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *b) {
+  if (!b) return VT_OK;
+  if (ctx) cudaSetDevice(ctx->device);
+  cudaDeviceSynchronize();
+  batch_free(b);
   return VT_OK;
 }
 

@@ -182,3 +182,47 @@ def sampler_frame(ctx: Context, width: int, height: int, z: bool, model: int, sa
     _check(ctx.handle, _lib.load().vt_sampler_frame(ctx.handle, width, height, 1 if z else 0, model, sample_index,
                                                     frame_index, vertex, stream, out.ctypes.data), "vt_sampler_frame")
     return out
+
+
+class Batch:
+    """Scenes rendered by one persistent launch per pass (vt_batch): each pass adds spp[i] frames to
+    scene i. The first six passes try launch shapes; later passes replay a captured CUDA graph."""
+
+    def __init__(self, ctx: Context, scenes, params, spp):
+        lib = _lib.load()
+        self.ctx, self.scenes = ctx, list(scenes)
+        n = len(self.scenes)
+        self._ptrs = (C.c_void_p * n)(*[sc._p.value for sc in self.scenes])
+        self._params = (FrameParams * n)(*params)
+        self._spp = (C.c_uint32 * n)(*[int(x) for x in spp])
+        p = C.c_void_p()
+        _check(ctx.handle, lib.vt_batch_create(ctx.handle, self._ptrs, self._params, self._spp, n, C.byref(p)),
+               "vt_batch_create")
+        self._p = p
+        for sc, prm in zip(self.scenes, params):
+            sc.width, sc.height = prm.width, prm.height
+
+    def render(self, stream=None) -> float:
+        """One pass; returns its device time in ms."""
+        _check(self.ctx.handle, _lib.load().vt_batch_render(self.ctx.handle, self._p, stream), "vt_batch_render")
+        return self.stats()[0].last_ms
+
+    def stats(self):
+        """(vt_batch_stats, per-scene completion ms of the last pass)."""
+        st = _lib.BatchStats()
+        ms = np.zeros(len(self.scenes), np.float64)
+        _check(self.ctx.handle, _lib.load().vt_batch_stats(self.ctx.handle, self._p, C.byref(st), ms.ctypes.data,
+                                                           len(self.scenes)), "vt_batch_stats")
+        return st, ms
+
+    def close(self) -> None:
+        if getattr(self, "_p", None) is not None and self.ctx._p is not None:
+            _lib.load().vt_batch_destroy(self.ctx.handle, self._p)
+        self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -353,3 +353,97 @@ def cornell_sphere(subdivisions: int = 3, seed: int = 0):
     sf["a"], sf["b"], sf["c"] = tri[:, 0] + base, tri[:, 1] + base, tri[:, 2] + base
     sf["tag"] = 6
     return np.concatenate([faces, sf]), np.concatenate([verts, sv]), materials, light, camera
+
+
+_UNIT_SPHERES: dict = {}
+
+
+def _unit_icosphere(subdivisions: int):
+    """Cached undisplaced unit icosphere: (positions (V, 3), triangles (F, 3))."""
+    if subdivisions not in _UNIT_SPHERES:
+        p, _, t = icosphere(subdivisions)
+        _UNIT_SPHERES[subdivisions] = (p, t)
+    return _UNIT_SPHERES[subdivisions]
+
+
+def _lattice_noise(dirs, seeds):
+    """icosphere's displacement noise for many spheres at once: dirs (V, 3) unit directions, seeds (S,)
+    -> (S, V) trilinear value noise of a 17^3 lattice of PCG hashes of (seed * 4099 + node)."""
+    idx = np.arange(17 ** 3, dtype=np.uint64)
+    h = ((np.asarray(seeds, np.uint64)[:, None] * np.uint64(4099) + idx[None, :]) & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+    state = h * np.uint32(747796405) + np.uint32(2891336453)
+    word = ((state >> ((state >> np.uint32(28)) + np.uint32(4))) ^ state) * np.uint32(277803737)
+    lattice = ((word >> np.uint32(22)) ^ word).astype(np.float64) / 2.0 ** 32
+    g = (dirs * 0.5 + 0.5) * 16.0
+    i0 = np.clip(np.floor(g).astype(int), 0, 15)
+    fr = g - i0
+    noise = np.zeros((len(seeds), len(dirs)))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = (fr[:, 0] if dx else 1 - fr[:, 0]) * (fr[:, 1] if dy else 1 - fr[:, 1]) * (fr[:, 2] if dz else 1 - fr[:, 2])
+                noise += w[None, :] * lattice[:, ((i0[:, 0] + dx) * 17 + (i0[:, 1] + dy)) * 17 + (i0[:, 2] + dz)]
+    return noise
+
+
+def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displace: float = 0.05):
+    """The grid scene's generator (configs C3/C4): a k x k grid of displaced icospheres on a ground quad,
+    with k and the subdivision level chosen so that the mesh has about `triangles` triangles (the
+    largest subdivision <= 5 whose 20 * 4^s triangles fit four spheres, then k = round(sqrt(T / per))).
+    Spheres have radius 0.4 on a unit lattice; each vertex moves along its direction by
+    displace * (2 n - 1), n a trilinear value noise of the direction over a 17^3 lattice of PCG hashes
+    seeded per sphere; normals are the normalised sums of incident face normals (smooth shading).
+    Albedos are grey Lambert 0.2 + 0.6 u from 8 slots; every `emissive_every`-th sphere is an emitter
+    (radiance 4, 8 or 12, grey), so the scene is an imported scene lit by its emissive triangles.
+    Returns faces, vertices, materials and a camera looking down on the grid."""
+    per = 20
+    sub = 0
+    while sub < 5 and per * 4 * 4 <= max(triangles, 1) / 4:
+        per *= 4
+        sub += 1
+    k = max(1, int(round((triangles / per) ** 0.5)))
+    rng = np.random.default_rng(seed)
+    unit, tri = _unit_icosphere(sub)
+    S, V, F = k * k, len(unit), len(tri)
+    sid = np.arange(S)
+    centers = np.stack([sid // k - (k - 1) / 2.0, np.full(S, 0.4), sid % k - (k - 1) / 2.0], 1)
+    scale = 1.0 + displace * (2.0 * _lattice_noise(unit, seed * 7919 + sid) - 1.0)        # (S, V)
+    local = unit[None, :, :] * scale[:, :, None]                                           # (S, V, 3)
+    fn = np.cross(local[:, tri[:, 1]] - local[:, tri[:, 0]], local[:, tri[:, 2]] - local[:, tri[:, 0]])
+    vn = np.zeros_like(local)
+    for c in range(3):
+        for ax in range(3):
+            vn[:, :, ax] += np.stack([np.bincount(tri[:, c], weights=fn[s, :, ax], minlength=V) for s in range(S)])
+    vn /= np.linalg.norm(vn, axis=2, keepdims=True)
+    pos = local * 0.4 + centers[:, None, :]
+    emissive = (emissive_every > 0) & (sid % max(emissive_every, 1) == emissive_every // 2)
+    sphere_tag = np.where(emissive, 8 + sid % 3, sid % 8).astype(np.uint32)
+    half = k / 2.0 + 1.0
+    ground = np.array([(-half, 0.0, -half), (half, 0.0, -half), (half, 0.0, half), (-half, 0.0, half)])
+    p = np.concatenate([pos.reshape(-1, 3), ground])
+    n = np.concatenate([vn.reshape(-1, 3), np.tile([0.0, 1.0, 0.0], (4, 1))])
+    t = np.concatenate([(tri[None, :, :] + (sid * V)[:, None, None]).reshape(-1, 3),
+                        np.array([[0, 2, 1], [0, 3, 2]]) + S * V])
+    tg = np.concatenate([np.repeat(sphere_tag, F), np.zeros(2, np.uint32)])
+    verts = np.zeros(len(p), VERTEX_DTYPE)
+    verts["p"] = p.astype(np.float32)
+    verts["n"] = n.astype(np.float32)
+    faces = np.zeros(len(t), FACE_DTYPE)
+    faces["a"], faces["b"], faces["c"] = t[:, 0], t[:, 1], t[:, 2]
+    faces["tag"] = tg
+    mats = [{"type": 0, "albedo": (float(a),) * 3, "emission": (0.0, 0.0, 0.0)}
+            for a in 0.2 + 0.6 * rng.random(8)]
+    mats += [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (float(e),) * 3} for e in (4.0, 8.0, 12.0)]
+    d = max(2.0, 0.9 * k)
+    camera = {"pos": (0.0, 0.8 * d, -1.2 * d), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 45.0}
+    return faces, verts, mats, camera
+
+
+def batch_workload(count: int = 64, seed: int = 0, lo: int = 10_000, hi: int = 2_000_000):
+    """Config C4's scene list: per scene (triangles log-uniform in [lo, hi], resolution from
+    {256, 512, 1024} squared, spp uniform in 4..64), seeded."""
+    rng = np.random.default_rng(seed)
+    tri = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).astype(int)
+    res = rng.choice([256, 512, 1024], count)
+    spp = rng.integers(4, 65, count)
+    return [(int(a), int(b), int(c)) for a, b, c in zip(tri, res, spp)]
