@@ -21,9 +21,12 @@ struct Node4 {
 // A node is fetched through the read-only path as four 32-byte vector loads (sm_100 ld.global.v8;
 // nodes are 128-byte records in a 256-byte aligned buffer): half the load instructions, and so half
 // the L1 wavefronts, of eight 16-byte loads when the lanes of a warp fetch different nodes.
+// The asm is volatile so that the compiler cannot speculate the load above the branch that guards
+// it: a traversal pops leaf entries (negative) and node indices from one stack, and a load hoisted
+// above the entry's sign test would read before the start of the node array.
 __device__ __forceinline__ void ld256(const float4 *p, float4 &a, float4 &b) {
 #if VT_NODE_LD256
-  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
                : "l"(p));
 #else
@@ -250,6 +253,17 @@ __device__ __forceinline__ void load_qnode(const float4 *__restrict__ qnodes, in
   n.qhi[0] = __float_as_uint(b.w); n.qhi[1] = __float_as_uint(c.x); n.qhi[2] = __float_as_uint(c.y);
   n.child = make_int4(__float_as_int(c.z), __float_as_int(c.w), __float_as_int(d.x), __float_as_int(d.y));
   n.counts = __float_as_uint(d.z);
+}
+
+// A leaf child goes on a traversal stack as the entry ~(node << 2 | slot) (node indices are below
+// 2^29); popping it reads the slot's first triangle and count from the node, in L1 since the node's
+// visit.
+__device__ __forceinline__ int leaf_entry_of(int node, int slot) { return ~((node << 2) | slot); }
+__device__ __forceinline__ void leaf_range(const float4 *__restrict__ qnodes, int entry, int &first, int &cnt) {
+  const int code = ~entry, slot = code & 3;
+  const int *nd = reinterpret_cast<const int *>(qnodes + 4 * (size_t)(code >> 2));
+  first = -__ldg(nd + 10 + slot) - 1;
+  cnt = (__ldg(nd + 14) >> (4 * slot)) & 15;
 }
 
 // Byte k of w as the float 1 + byte 2^-15 (the byte in mantissa bits 8-15), exact.

@@ -23,15 +23,6 @@ using namespace vtd;
 
 // Single-ray traversals in the persistent kernels' order (leaf children pushed as stack entries,
 // near entries popped first), counting node visits and triangle tests when kCount.
-// A leaf child is the stack entry ~(node << 2 | slot) (node indices are below 2^29); popping it reads
-// the slot's first triangle and count from the node, in L1 since the node's visit.
-__device__ __forceinline__ int leaf_entry_of(int node, int slot) { return ~((node << 2) | slot); }
-__device__ __forceinline__ void leaf_range(const float4 *__restrict__ nodes, int entry, int &first, int &cnt) {
-  const int code = ~entry, slot = code & 3;
-  const int *nd = reinterpret_cast<const int *>(nodes + 4 * (size_t)(code >> 2));
-  first = -__ldg(nd + 10 + slot) - 1;
-  cnt = (__ldg(nd + 14) >> (4 * slot)) & 15;
-}
 
 template <bool kCount>
 __device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
