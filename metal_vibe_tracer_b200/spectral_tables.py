@@ -16,6 +16,20 @@ reads that file at run time. Every table is a 1 nm table over [lambda_min, lambd
 The renderer's default range is 380-780 nm (the traversal-path configs ask for four hero
 wavelengths over 380-780 nm); the reference tabulates 360-830 nm, which `generate(360, 830)`
 reproduces for the golden-vector check.
+
+RGB -> spectrum uplift (scripts/generate_spectral_tables.py `Data` :142-181; main.swift:842-907): a
+bounded colour's reflectance is the bounded MESE of three trigonometric moments on Peters' even XYZ
+phase warp (Peters et al. 2019). The file also holds what the device needs to solve the moment grid
+and to evaluate reflectances:
+
+* uplift_w[i]   per nm over 360-830 (always that range, the colour model's): linear-sRGB CMFs times
+                D65 normalised to Y = 1, float64 (reflectance -> linear sRGB is sum_i uplift_w[i] g_i);
+* uplift_cos[i] cos(phi(lambda_i)) over 360-830, float64, phi the warp (XYZWarp.h
+                applyXYZWarpEven: piecewise linear in 5 nm steps over 95 nodes);
+* cos_phase[i]  cos(phi) at the render range's 1 nm bins, float32.
+
+The warp's 95 nodes come from the reference's vendored copy of Peters' BSD code
+(Vendor/Spectral/Peters2019/XYZWarp.h), read at build time like the CIE data.
 """
 from __future__ import annotations
 
@@ -29,10 +43,12 @@ import numpy as np
 PKG = Path(__file__).resolve().parent
 DATA_DIR = PKG / "data"
 REFERENCE_CIE = Path("/root/reference/Vendor/Spectral/CIE")
+REFERENCE_WARP = Path("/root/reference/Vendor/Spectral/Peters2019/XYZWarp.h")
+UPLIFT_MIN, UPLIFT_MAX = 360, 830
 SRGB_PRIMARIES = ((0.64, 0.33), (0.30, 0.60), (0.15, 0.06))
 ICDF_SEGMENTS = 1024
 DEFENSIVE = 0.1
-MAGIC = b"VTSPEC01"
+MAGIC = b"VTSPEC02"
 
 
 def _read(path: Path):
@@ -94,6 +110,35 @@ def compute(lambda_min: int, lambda_max: int, cie_dir: Path = REFERENCE_CIE) -> 
             "illum": d65, "icdf": icdf, "xyz_to_rgb": xyz_to_rgb, "density": density}
 
 
+def read_warp(path: Path = REFERENCE_WARP) -> list:
+    """The 95 nodes of Peters' even XYZ phase warp (-pi at 360 nm ... 0 at 830 nm, 5 nm apart)."""
+    text = path.read_text()
+    key = "pXYZWarpEven[] = {"
+    start = text.index(key) + len(key)
+    values = [float(v.strip().rstrip("f")) for v in text[start:text.index("}", start)].split(",")]
+    if len(values) != 95:
+        raise RuntimeError(f"{path}: expected 95 warp nodes, found {len(values)}")
+    return values
+
+
+def warp_phase(warp, lam: float) -> float:
+    """phi(lambda): linear between the 5 nm nodes (XYZWarp.h applyXYZWarpEven)."""
+    t = (lam - 360.0) * 0.2
+    i = min(max(int(math.floor(t)), 0), 93)
+    f = t - i
+    return warp[i] * (1.0 - f) + warp[i + 1] * f
+
+
+def uplift_model(cie_dir: Path = REFERENCE_CIE, warp_path: Path = REFERENCE_WARP) -> dict:
+    """The uplift's colour model over 360-830 nm in float64: per nm weights (rgb CMF x D65, Y = 1)
+    and cos of the warped phase."""
+    t = compute(UPLIFT_MIN, UPLIFT_MAX, cie_dir)
+    w = [[c[k] * s for k in range(3)] for c, s in zip(t["cmf_rgb"], t["illum"])]
+    warp = read_warp(warp_path)
+    cos_phi = [math.cos(warp_phase(warp, lam)) for lam in range(UPLIFT_MIN, UPLIFT_MAX + 1)]
+    return {"weights": w, "cos": cos_phi, "warp": warp}
+
+
 def inverse_cdf(density, lambda_min, lambda_max, segments=ICDF_SEGMENTS):
     """Wavelengths at u = i / segments of the CDF of a piecewise-linear 1 nm density (exact)."""
     cdf = [0.0]
@@ -124,9 +169,11 @@ def path(lambda_min: int = 380, lambda_max: int = 780) -> Path:
     return DATA_DIR / f"spectral_{lambda_min}_{lambda_max}.bin"
 
 
-def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path = REFERENCE_CIE) -> Path:
-    """Write the float32 table file (build time; needs the CIE CSVs)."""
+def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path = REFERENCE_CIE,
+             warp_path: Path = REFERENCE_WARP) -> Path:
+    """Write the table file (build time; needs the CIE CSVs and the warp)."""
     t = compute(lambda_min, lambda_max, cie_dir)
+    u = uplift_model(cie_dir, warp_path)
     n = lambda_max - lambda_min + 1
     DATA_DIR.mkdir(parents=True, exist_ok=True)
     out = path(lambda_min, lambda_max)
@@ -135,6 +182,10 @@ def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path = REFER
     blob += np.asarray(t["illum"], np.float32).tobytes()
     blob += np.asarray(t["icdf"], np.float32).tobytes()
     blob += np.asarray(t["xyz_to_rgb"], np.float64).tobytes()
+    blob += np.asarray(u["weights"], np.float64).tobytes()
+    blob += np.asarray(u["cos"], np.float64).tobytes()
+    cos_bins = [math.cos(warp_phase(u["warp"], float(lam))) for lam in range(lambda_min, lambda_max + 1)]
+    blob += np.asarray(cos_bins, np.float32).tobytes()
     tmp = out.with_suffix(".tmp")
     tmp.write_bytes(blob)
     tmp.replace(out)
@@ -155,6 +206,11 @@ def load(lambda_min: int = 380, lambda_max: int = 780) -> dict:
     cmf_rgb = np.frombuffer(b, np.float32, 3 * n, off).reshape(n, 3); off += 12 * n
     illum = np.frombuffer(b, np.float32, n, off); off += 4 * n
     icdf = np.frombuffer(b, np.float32, seg + 1, off); off += 4 * (seg + 1)
-    m = np.frombuffer(b, np.float64, 9, off).reshape(3, 3)
+    m = np.frombuffer(b, np.float64, 9, off).reshape(3, 3); off += 72
+    nu = UPLIFT_MAX - UPLIFT_MIN + 1
+    uw = np.frombuffer(b, np.float64, 3 * nu, off).reshape(nu, 3); off += 24 * nu
+    uc = np.frombuffer(b, np.float64, nu, off); off += 8 * nu
+    cos_phase = np.frombuffer(b, np.float32, n, off)
     return {"lambda_min": lo, "lambda_max": hi, "n": n, "segments": seg, "cmf_rgb": cmf_rgb.copy(),
-            "illum": illum.copy(), "icdf": icdf.copy(), "xyz_to_rgb": m.copy()}
+            "illum": illum.copy(), "icdf": icdf.copy(), "xyz_to_rgb": m.copy(),
+            "uplift_w": np.ascontiguousarray(uw), "uplift_cos": uc.copy(), "cos_phase": cos_phase.copy()}

@@ -322,3 +322,93 @@ def sampler_frame(width, height, z, model, sample_index, frame_index, vertex, st
     _fn("vto_sampler_frame")(width, height, 1 if z else 0, model, sample_index, frame_index, vertex, stream,
                              out.ctypes.data)
     return out
+
+
+# ---- RGB -> spectrum uplift (spectral_uplift.cpp) ---------------------------------------------
+_SIGS["vto_uplift_create"] = (_P, [_P, _P, _U32])
+_SIGS["vto_uplift_destroy"] = (None, [_P])
+_SIGS["vto_fourier_lagrange"] = (None, [_P, _P])
+_SIGS["vto_uplift_solve_code"] = (C.c_double, [_P, _P, _P, _P])
+_SIGS["vto_uplift_rgb_of_lagrange"] = (None, [_P, _P, _P])
+_SIGS["vto_uplift_moments_of_lagrange"] = (None, [_P, _P])
+_SIGS["vto_uplift_node"] = (None, [_P, _U32, _U32, _U32, _P])
+_SIGS["vto_uplift_code_error"] = (C.c_double, [_P, _P])
+_SIGS["vto_uplift_cell_refined"] = (_I32, [_P, _P])
+_SIGS["vto_spectral_lagrange"] = (None, [_P, _P, _U32, _P])
+
+
+def fourier_lagrange(c) -> np.ndarray:
+    """Bounded-MESE Lagrange multipliers of three moments (with the biasing of invalid ones)."""
+    c = np.ascontiguousarray(c, np.float64)
+    out = np.empty(3, np.float64)
+    _fn("vto_fourier_lagrange")(c.ctypes.data, out.ctypes.data)
+    return out
+
+
+def moments_of_lagrange(L) -> np.ndarray:
+    L = np.ascontiguousarray(L, np.float64)
+    out = np.empty(3, np.float64)
+    _fn("vto_uplift_moments_of_lagrange")(L.ctypes.data, out.ctypes.data)
+    return out
+
+
+class Uplift:
+    """The uplift's colour model (spectral_tables.load()['uplift_w'], ['uplift_cos']) with the
+    lazily solved moment grid."""
+
+    def __init__(self, weights, cos_phi):
+        self._w = np.ascontiguousarray(weights, np.float64)
+        self._c = np.ascontiguousarray(cos_phi, np.float64)
+        self._p = _fn("vto_uplift_create")(self._w.ctypes.data, self._c.ctypes.data, self._c.shape[0])
+
+    def solve_code(self, code):
+        code = np.ascontiguousarray(code, np.uint32)
+        m, L = np.empty(3, np.float64), np.empty(3, np.float64)
+        err = _fn("vto_uplift_solve_code")(self._p, code.ctypes.data, m.ctypes.data, L.ctypes.data)
+        return m, L, err
+
+    def rgb_of_lagrange(self, L):
+        L = np.ascontiguousarray(L, np.float64)
+        out = np.empty(3, np.float64)
+        _fn("vto_uplift_rgb_of_lagrange")(self._p, L.ctypes.data, out.ctypes.data)
+        return out
+
+    def node(self, i, j, k):
+        out = np.empty(3, np.float64)
+        _fn("vto_uplift_node")(self._p, i, j, k, out.ctypes.data)
+        return out
+
+    def code_error(self, code):
+        code = np.ascontiguousarray(code, np.uint32)
+        return _fn("vto_uplift_code_error")(self._p, code.ctypes.data)
+
+    def cell_refined(self, cell):
+        cell = np.ascontiguousarray(cell, np.uint32)
+        return bool(_fn("vto_uplift_cell_refined")(self._p, cell.ctypes.data))
+
+    def lagrange(self, rgb):
+        """spectral_lagrange of linear colours (n, 3) -> (n, 4): L0, L1, L2, flag (2 = flat L0)."""
+        rgb = np.ascontiguousarray(np.atleast_2d(rgb), np.float64)
+        out = np.empty((rgb.shape[0], 4), np.float64)
+        _fn("vto_spectral_lagrange")(self._p, rgb.ctypes.data, rgb.shape[0], out.ctypes.data)
+        return out
+
+    def close(self):
+        if getattr(self, "_p", None):
+            _fn("vto_uplift_destroy")(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def reflectance(L4, cos_phi):
+    """Eq. 11 at cos(phi) values; a flat quadruple (flag 2) gives its value."""
+    L4 = np.asarray(L4, np.float64)
+    x = np.asarray(cos_phi, np.float64)
+    if L4[3] == 2.0:
+        return np.full(x.shape, L4[0])
+    return np.arctan(L4[0] + 2.0 * L4[1] * x + 2.0 * L4[2] * (2.0 * x * x - 1.0)) / np.pi + 0.5
