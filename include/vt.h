@@ -173,7 +173,12 @@ typedef struct vt_quad_light {
 
 /* Spectral transport tables (1 nm bins from lambda_min): linear-sRGB colour-matching functions,
  * the emitters' illuminant (luminance 1) and the wavelength inverse CDF (segments + 1 nodes); the
- * roles of the spectral sampling buffer written by spectral_icdf_kernel (main.swift:8117-8185). */
+ * roles of the spectral sampling buffer written by spectral_icdf_kernel (main.swift:8117-8185).
+ * The uplift part is the colour model of the RGB -> spectrum conversion (bounded MESE of three
+ * trigonometric moments, main.swift:842-944): per nm over the model's range (360-830 nm, uplift_n
+ * = 471) the linear-sRGB CMFs times D65 (Y = 1) and the cosine of Peters' warped phase, in double,
+ * plus the cosine at each of the render bins. The moment grid is solved from it on the device
+ * (vt_spectral_grid_build) and reflectances and emitters use it at the path's wavelengths. */
 typedef struct vt_spectral_tables {
   const float *cmf_rgb;     /* nbins x 3 */
   const float *illuminant;  /* nbins */
@@ -181,6 +186,10 @@ typedef struct vt_spectral_tables {
   uint32_t nbins, segments;
   float lambda_min;
   uint32_t pad;
+  const float *cos_phase;        /* nbins: cos(phi(lambda)) at the render bins */
+  const double *uplift_weights;  /* uplift_n x 3 */
+  const double *uplift_cos;      /* uplift_n */
+  uint32_t uplift_n, pad2;
 } vt_spectral_tables;
 
 /* Per-frame parameters: the subset of Uniforms (main.swift:393-420) the integrator reads. */
@@ -265,6 +274,34 @@ vt_status vt_batch_render(vt_ctx *ctx, vt_batch *batch, void *stream);
  * completion time from the pass's start, in ms. */
 vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *batch, vt_batch_info *out, double *scene_ms, uint32_t n);
 vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *batch);
+
+/* ---- RGB -> spectrum uplift (spectral.cu) ------------------------------------------------------ */
+/* Solves the uplift's moment grid on the device for the tables' colour model, once per context
+ * (a second call with the same model returns at once; another model is an error). The reference
+ * ships the 86^3 grid solved offline (scripts/generate_spectral_tables.py: solve_lagrange,
+ * moments_of_lagrange; FourierSRGB86.bin) and refines it on the GPU (refineSpectralGrid,
+ * main.swift:10658-10705): here both steps run as kernels. Scene creation with spectral tables
+ * calls this itself. */
+vt_status vt_spectral_grid_build(vt_ctx *ctx, const vt_spectral_tables *tables);
+
+typedef struct vt_spectral_grid_info {
+  uint32_t built;          /* 1 once the grid is solved */
+  uint32_t refined_cells;  /* cells given exact 4x4x4 blocks (at most 8192) */
+  uint32_t flagged_cells;  /* cells whose interpolation missed a code by more than 0.35 steps */
+  uint32_t pad;
+  double max_residual;     /* largest linear-sRGB residual of the coarse solves */
+} vt_spectral_grid_info;
+vt_status vt_spectral_grid_get_info(vt_ctx *ctx, vt_spectral_grid_info *out);
+/* The grid as float4 (c0, c1, c2, refined slot + 1 or 0): 86^3 nodes then 64 per refined cell;
+ * n = 4 * (86^3 + 64 * refined_cells) floats. */
+vt_status vt_spectral_grid_read(vt_ctx *ctx, float *out, uint32_t n);
+/* spectral_lagrange (main.swift:889-897) of n linear colours (rgb n x 3) on the device: per colour
+ * (L0, L1, L2, 1), or (value, 0, 0, 2) for a grey. */
+vt_status vt_spectral_lagrange(vt_ctx *ctx, const float *rgb, uint32_t n, float *out);
+/* Every 8-bit sRGB code through the runtime conversion (grid, multipliers, reflectance at 1 nm,
+ * back to sRGB under D65), on the device: the largest error in 8-bit steps and how many codes
+ * miss by more than half a step (the reference's round-trip check, tests/Fix_spectral.swift). */
+vt_status vt_spectral_round_trip(vt_ctx *ctx, float *worst, uint32_t *over_half);
 
 /* ---- emitter lights: light tree and emitter list ----------------------------------------- */
 

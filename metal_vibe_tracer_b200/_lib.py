@@ -46,6 +46,11 @@ class LightTreeInfo(C.Structure):
                 ("grid_lo", C.c_float * 3), ("grid_hi", C.c_float * 3)]
 
 
+class SpectralGridInfo(C.Structure):
+    _fields_ = [("built", C.c_uint32), ("refined_cells", C.c_uint32), ("flagged_cells", C.c_uint32),
+                ("pad", C.c_uint32), ("max_residual", C.c_double)]
+
+
 class BatchStats(C.Structure):
     _fields_ = [("scenes", C.c_uint32), ("passes", C.c_uint32), ("items", C.c_ulonglong), ("last_ms", C.c_float),
                 ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
@@ -100,6 +105,11 @@ SIGNATURES = {
     "vt_batch_render": (_I32, [_P, _P, _P]),
     "vt_batch_stats": (_I32, [_P, _P, C.POINTER(BatchStats), _P, _U32]),
     "vt_batch_destroy": (_I32, [_P, _P]),
+    "vt_spectral_grid_build": (_I32, [_P, _P]),
+    "vt_spectral_grid_get_info": (_I32, [_P, C.POINTER(SpectralGridInfo)]),
+    "vt_spectral_grid_read": (_I32, [_P, _P, _U32]),
+    "vt_spectral_lagrange": (_I32, [_P, _P, _U32, _P]),
+    "vt_spectral_round_trip": (_I32, [_P, C.POINTER(C.c_float), C.POINTER(_U32)]),
 }
 NOALLOC_MAX_FACES = 32768
 

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "sampler.cuh"
+#include "spectral.cuh"
 #include "trace_common.cuh"
 #include "vt_internal.cuh"
 
@@ -51,6 +52,9 @@ struct RenderArgs {
   float larea;
   const float4 *spec;
   const float *icdf;
+  const float4 *slotL;     // per slot: the albedo's uplift multipliers (L0, L1, L2, flag)
+  const float *cosPhase;   // per bin: cos of the warped phase
+  const float4 *ebasis;    // per bin: the emission basis (R, G, B, 0), (C, M, Y, 0)
   uint32_t nbins, segments;
   float lambdaMin;
   int spectral;
@@ -236,6 +240,7 @@ __device__ __forceinline__ vt_material material(const RenderArgs &A, uint32_t sl
   m.type = VT_MAT_DIFFUSE;
   m.albedo[0] = m.albedo[1] = m.albedo[2] = 0.0f;
   m.emission[0] = m.emission[1] = m.emission[2] = 0.0f;
+  m.pad = __uint_as_float(0xffffffffu);  // no slot: black in spectral transport too
   return m;
 }
 
@@ -273,10 +278,21 @@ __device__ __forceinline__ float3 lanes_rgb(const RenderArgs &A, const Lanes &L,
   return rgb;
 }
 
-// Grey emission e under the illuminant, per lane.
-__device__ __forceinline__ float4 lanes_emission(const RenderArgs &A, const Lanes &L, float e) {
-  return make_float4(e * __ldg(A.spec + L.bin[0]).w, e * __ldg(A.spec + L.bin[1]).w, e * __ldg(A.spec + L.bin[2]).w,
-                     e * __ldg(A.spec + L.bin[3]).w);
+// An RGB emission e under the illuminant S, per lane (spectral_emission, main.swift:933-944): the
+// emission basis at the lane's bin times S there; white is S exactly.
+__device__ __forceinline__ float4 lanes_emission(const RenderArgs &A, const Lanes &L, float3 e) {
+  if (!(fmaxf(e.x, fmaxf(e.y, e.z)) > 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const EmissionWeights w = emission_weights(e);
+  float v[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) v[k] = emission_basis(w, A.ebasis, (uint32_t)L.bin[k]) * __ldg(A.spec + L.bin[k]).w;
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+// A slot's albedo as a reflectance at the lanes' bins (spectral_reflectance, main.swift:905-907).
+__device__ __forceinline__ float4 lanes_reflectance(const RenderArgs &A, const Lanes &L, uint32_t slot) {
+  const float4 q = __ldg(A.slotL + slot);
+  return make_float4(fourier_reflectance(q, __ldg(A.cosPhase + L.bin[0])), fourier_reflectance(q, __ldg(A.cosPhase + L.bin[1])),
+                     fourier_reflectance(q, __ldg(A.cosPhase + L.bin[2])), fourier_reflectance(q, __ldg(A.cosPhase + L.bin[3])));
 }
 
 struct LightSample {
@@ -592,15 +608,17 @@ __device__ __forceinline__ float3 cosine_hemisphere(float3 n, float r0, float r1
   return normalize3(add(add(mul(u, c * sin_th), mul(v, s * sin_th)), mul(n, cos_th)));
 }
 
-__device__ __forceinline__ float grey(const float c[3]) { return (c[0] + c[1] + c[2]) * (1.0f / 3.0f); }
-
-// Reflectance / emission as a 4-lane spectrum (spectral) or rgb in xyz (RGB transport).
-__device__ __forceinline__ float4 reflectance(const RenderArgs &A, const vt_material &m) {
-  if (A.spectral) { const float g = grey(m.albedo); return make_float4(g, g, g, g); }
+// Reflectance / emission as a 4-lane spectrum (spectral) or rgb in xyz (RGB transport). A slot's
+// material carries its index in `pad`; a slot out of range (material()'s black default) has none.
+__device__ __forceinline__ float4 reflectance(const RenderArgs &A, const Lanes &L, const vt_material &m) {
+  if (A.spectral) {
+    const uint32_t slot = __float_as_uint(m.pad);
+    return slot < A.nmat ? lanes_reflectance(A, L, slot) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
   return make_float4(m.albedo[0], m.albedo[1], m.albedo[2], 0.0f);
 }
 __device__ __forceinline__ float4 emission(const RenderArgs &A, const Lanes &L, const float e[3]) {
-  if (A.spectral) return lanes_emission(A, L, e[0]);
+  if (A.spectral) return lanes_emission(A, L, make_float3(e[0], e[1], e[2]));
   return make_float4(e[0], e[1], e[2], 0.0f);
 }
 __device__ __forceinline__ float3 to_rgb(const RenderArgs &A, const Lanes &L, float4 s) {
@@ -674,7 +692,7 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
   if (A.spectral) L = make_lanes(A, c.u);
   const float f = lambert_f(n, gn, mul(view, -1.0f), dir);
   const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
-  const float4 s = scale4(mul4(reflectance(A, m), emission(A, L, e)), f * cos_th);
+  const float4 s = scale4(mul4(reflectance(A, L, m), emission(A, L, e)), f * cos_th);
   return mul(to_rgb(A, L, s), light_geometry(A, p, c));
 }
 
@@ -795,7 +813,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     const float3 nd = cosine_hemisphere(S.n, r.y, r.z);
     const float bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
     if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
-    T = mul4(T, reflectance(A, m));
+    T = mul4(T, reflectance(A, L, m));
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
     const float3 prev = S.pos;
     const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
@@ -815,7 +833,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     if (emissionOnly) break;
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, m), mis && scattering < limit,
+      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, L, m), mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -848,7 +866,7 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, m), A.mode == 1u && limit > 0, seed,
+    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, L, m), A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
   R = add(R, continue_path(A, L, S, m, dir0, seed, stack, false));
@@ -1172,26 +1190,22 @@ namespace {
 // Shared by both scene kinds: validation, material slots, spectral tables.
 vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
                        const float *lightEmission, const vt_spectral_tables *tables, vt_scene *sc) {
+  (void)lightEmission;
   if (tables) {
     if (!tables->cmf_rgb || !tables->illuminant || !tables->icdf || tables->nbins < 2 || tables->segments < 1)
       return vt_fail(ctx, VT_ERR_INVALID, "incomplete spectral tables");
-    // Spectral transport here supports grey reflectances and grey emitters (flat spectra).
-    for (uint32_t i = 0; i < nmat; ++i) {
-      const float *c = materials[i].type == VT_MAT_EMISSIVE ? materials[i].emission : materials[i].albedo;
-      if (std::fabs(c[0] - c[1]) > 1e-4f || std::fabs(c[1] - c[2]) > 1e-4f)
-        return vt_fail(ctx, VT_ERR_INVALID, "spectral transport supports grey materials only (slot " + std::to_string(i) + ")");
-    }
-    if (lightEmission) {
-      const float *e = lightEmission;
-      if (std::fabs(e[0] - e[1]) > 1e-4f || std::fabs(e[1] - e[2]) > 1e-4f)
-        return vt_fail(ctx, VT_ERR_INVALID, "spectral transport supports a grey light emission only");
-    }
+    if (!tables->cos_phase) return vt_fail(ctx, VT_ERR_INVALID, "spectral tables need cos_phase (the render bins' phase)");
+    const vt_status st = vt_uplift_ensure(ctx, tables);
+    if (st != VT_OK) return st;
   }
   sc->mesh = mesh;
   sc->nmat = nmat;
   if (nmat) {
+    // The device copy carries each slot's index in `pad` (the key of its uplifted reflectance).
+    std::vector<vt_material> mats(materials, materials + nmat);
+    for (uint32_t i = 0; i < nmat; ++i) std::memcpy(&mats[i].pad, &i, sizeof i);
     VT_CUDA(ctx, cudaMalloc(&sc->d_mats, nmat * sizeof(vt_material)));
-    VT_CUDA(ctx, cudaMemcpy(sc->d_mats, materials, nmat * sizeof(vt_material), cudaMemcpyHostToDevice));
+    VT_CUDA(ctx, cudaMemcpy(sc->d_mats, mats.data(), nmat * sizeof(vt_material), cudaMemcpyHostToDevice));
   }
   if (tables) {
     std::vector<float4> spec(tables->nbins);
@@ -1204,11 +1218,28 @@ vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *mate
     VT_CUDA(ctx, cudaMemcpy(sc->d_spec, spec.data(), spec.size() * sizeof(float4), cudaMemcpyHostToDevice));
     VT_CUDA(ctx, cudaMalloc(&sc->d_icdf, (tables->segments + 1) * sizeof(float)));
     VT_CUDA(ctx, cudaMemcpy(sc->d_icdf, tables->icdf, (tables->segments + 1) * sizeof(float), cudaMemcpyHostToDevice));
+    // Uplift: the bins' phase, the emission basis there, and each slot's albedo multipliers.
+    VT_CUDA(ctx, cudaMalloc(&sc->d_cosphase, tables->nbins * sizeof(float)));
+    VT_CUDA(ctx, cudaMemcpy(sc->d_cosphase, tables->cos_phase, tables->nbins * sizeof(float), cudaMemcpyHostToDevice));
+    VT_CUDA(ctx, cudaMalloc(&sc->d_ebasis, 2 * (size_t)tables->nbins * sizeof(float4)));
+    vt_status st = vt_uplift_basis(ctx, sc->d_cosphase, tables->nbins, sc->d_ebasis);
+    if (st != VT_OK) return st;
+    if (nmat) {
+      std::vector<float> albedo(3 * (size_t)nmat);
+      for (uint32_t i = 0; i < nmat; ++i)
+        for (int k = 0; k < 3; ++k) albedo[3 * i + k] = materials[i].albedo[k];
+      VT_CUDA(ctx, cudaMalloc(&sc->d_slotL, nmat * sizeof(float4)));
+      st = vt_uplift_colours(ctx, albedo.data(), nmat, sc->d_slotL);
+      if (st != VT_OK) return st;
+    }
   }
   return VT_OK;
 }
 
 void scene_free(vt_scene *scene) {
+  cudaFree(scene->d_slotL);
+  cudaFree(scene->d_cosphase);
+  cudaFree(scene->d_ebasis);
   cudaFree(scene->d_mats);
   cudaFree(scene->d_spec);
   cudaFree(scene->d_icdf);
@@ -1482,6 +1513,9 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   }
   A.spec = scene->d_spec;
   A.icdf = scene->d_icdf;
+  A.slotL = scene->d_slotL;
+  A.cosPhase = scene->d_cosphase;
+  A.ebasis = scene->d_ebasis;
   A.nbins = scene->nbins;
   A.segments = scene->segments;
   A.lambdaMin = scene->lambda_min;

@@ -31,6 +31,14 @@ struct vt_ctx {
   uint32_t *d_order[3] = {nullptr, nullptr, nullptr};
   size_t order_words[3] = {0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // RGB -> spectrum uplift (spectral.cu), built once per context: the moment grid (86^3 float4
+  // nodes, then refined 64-entry blocks) and the 86 node values; the colour model it was solved for.
+  float4 *d_fgrid = nullptr;
+  float *d_gnodes = nullptr;
+  uint32_t fgrid_cells = 0;        // refined cells
+  uint32_t fgrid_flagged = 0;      // cells flagged (before the capacity cap)
+  double fgrid_residual = 0.0;     // largest linear-sRGB residual of the coarse solves
+  std::vector<double> fgrid_model; // weights and cos phase it was solved with
 };
 
 // Traversal copy of a 4-wide node with 8-bit child boxes (qnode.cu): 64 bytes, two 32-byte loads.
@@ -96,6 +104,10 @@ struct vt_scene {
   // reservoir (sample position, emission and pdf, weights) for this frame and the previous one,
   // plus the primary hit's face/slot/error and geometric normal: 12 float4 per pixel in one
   // allocation.
+  // Spectral uplift: per slot the albedo's multipliers, per bin the phase and the emission basis.
+  float4 *d_slotL = nullptr;
+  float *d_cosphase = nullptr;
+  float4 *d_ebasis = nullptr;
   float4 *d_di = nullptr;
   uint32_t di_width = 0, di_height = 0, di_frames = 0, di_parity = 0;
   float di_cam[14] = {};  // previous frame's camera: position, forward, right, up, aspect, fov scale
@@ -105,6 +117,12 @@ struct vt_scene {
 // Error plumbing.
 
 vt_status vt_fail(vt_ctx *ctx, vt_status code, const std::string &msg);
+// RGB -> spectrum uplift (spectral.cu): build the context's moment grid for the tables' colour model
+// (once), uplift host colours into device (L0, L1, L2, flag) quadruples, and tabulate the emission
+// basis at device bins of the given phase.
+vt_status vt_uplift_ensure(vt_ctx *ctx, const vt_spectral_tables *tables);
+vt_status vt_uplift_colours(vt_ctx *ctx, const float *rgb, uint32_t n, float4 *out_dev);
+vt_status vt_uplift_basis(vt_ctx *ctx, const float *cosPhase_dev, uint32_t nbins, float4 *basis_dev);
 vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what);
 
 #define VT_CUDA(ctx, call)                                   \

@@ -27,7 +27,23 @@ class QuadLight(C.Structure):
 
 class SpectralTables(C.Structure):
     _fields_ = [("cmf_rgb", C.c_void_p), ("illuminant", C.c_void_p), ("icdf", C.c_void_p),
-                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float), ("pad", C.c_uint32)]
+                ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float), ("pad", C.c_uint32),
+                ("cos_phase", C.c_void_p), ("uplift_weights", C.c_void_p), ("uplift_cos", C.c_void_p),
+                ("uplift_n", C.c_uint32), ("pad2", C.c_uint32)]
+
+
+def spectral_struct(spectral: dict):
+    """vt_spectral_tables for a spectral_tables.load() dict, with the arrays it points to (keep
+    them alive as long as the struct is used)."""
+    arrays = [np.ascontiguousarray(spectral["cmf_rgb"], np.float32), np.ascontiguousarray(spectral["illum"], np.float32),
+              np.ascontiguousarray(spectral["icdf"], np.float32), np.ascontiguousarray(spectral["cos_phase"], np.float32),
+              np.ascontiguousarray(spectral["uplift_w"], np.float64), np.ascontiguousarray(spectral["uplift_cos"], np.float64)]
+    cmf, ill, icdf, cosp, uw, uc = arrays
+    if uw.shape != (uc.shape[0], 3) or cosp.shape[0] != cmf.shape[0] or ill.shape[0] != cmf.shape[0]:
+        raise ValueError("spectral tables: uplift_w must be (len(uplift_cos), 3) and cos_phase / illum one per bin")
+    s = SpectralTables(cmf.ctypes.data, ill.ctypes.data, icdf.ctypes.data, cmf.shape[0], icdf.shape[0] - 1,
+                       float(spectral["lambda_min"]), 0, cosp.ctypes.data, uw.ctypes.data, uc.ctypes.data, uc.shape[0], 0)
+    return s, arrays
 
 
 class FrameParams(C.Structure):
@@ -96,11 +112,7 @@ class Scene:
         self._light = None if light is None else make_light(light)
         tables = None
         if spectral is not None:
-            self._cmf = np.ascontiguousarray(spectral["cmf_rgb"], np.float32)
-            self._illum = np.ascontiguousarray(spectral["illum"], np.float32)
-            self._icdf = np.ascontiguousarray(spectral["icdf"], np.float32)
-            tables = SpectralTables(self._cmf.ctypes.data, self._illum.ctypes.data, self._icdf.ctypes.data,
-                                    self._cmf.shape[0], self._icdf.shape[0] - 1, float(spectral["lambda_min"]), 0)
+            tables, self._spectral_arrays = spectral_struct(spectral)
         p = C.c_void_p()
         tp = C.byref(tables) if tables is not None else None
         if self.imported:
@@ -226,3 +238,43 @@ class Batch:
         except Exception:
             pass
 
+
+
+# ---- RGB -> spectrum uplift (spectral.cu) -----------------------------------------------------
+def spectral_grid_build(ctx: Context, spectral: dict) -> None:
+    """Solve the context's uplift moment grid for the tables' colour model (once per context)."""
+    s, keep = spectral_struct(spectral)
+    _check(ctx.handle, _lib.load().vt_spectral_grid_build(ctx.handle, C.byref(s)), "vt_spectral_grid_build")
+    del keep
+
+
+def spectral_grid_info(ctx: Context) -> dict:
+    info = _lib.SpectralGridInfo()
+    _check(ctx.handle, _lib.load().vt_spectral_grid_get_info(ctx.handle, C.byref(info)), "vt_spectral_grid_get_info")
+    return {"built": bool(info.built), "refined_cells": int(info.refined_cells), "flagged_cells": int(info.flagged_cells),
+            "max_residual": float(info.max_residual)}
+
+
+def spectral_grid(ctx: Context) -> np.ndarray:
+    """The grid as (86^3 + 64 * refined cells, 4) float32: c0, c1, c2, refined slot + 1."""
+    n = 86 ** 3 + 64 * spectral_grid_info(ctx)["refined_cells"]
+    out = np.empty((n, 4), np.float32)
+    _check(ctx.handle, _lib.load().vt_spectral_grid_read(ctx.handle, out.ctypes.data, out.size), "vt_spectral_grid_read")
+    return out
+
+
+def spectral_lagrange(ctx: Context, rgb) -> np.ndarray:
+    """Device spectral_lagrange of linear colours (n, 3) -> (n, 4)."""
+    rgb = np.ascontiguousarray(np.atleast_2d(rgb), np.float32)
+    out = np.empty((rgb.shape[0], 4), np.float32)
+    _check(ctx.handle, _lib.load().vt_spectral_lagrange(ctx.handle, rgb.ctypes.data, rgb.shape[0], out.ctypes.data),
+           "vt_spectral_lagrange")
+    return out
+
+
+def spectral_round_trip(ctx: Context) -> tuple[float, int]:
+    """(largest 8-bit error over every code, codes off by more than half a step)."""
+    worst, over = C.c_float(), C.c_uint32()
+    _check(ctx.handle, _lib.load().vt_spectral_round_trip(ctx.handle, C.byref(worst), C.byref(over)),
+           "vt_spectral_round_trip")
+    return float(worst.value), int(over.value)

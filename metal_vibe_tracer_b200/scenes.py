@@ -213,6 +213,24 @@ def cornell_box(light_radiance: float = 17.0, seed: int = 0):
     return faces, verts, materials, light, camera
 
 
+def cornell_coloured(seed: int = 0):
+    """The Cornell box with the classic coloured walls and the reference's scene-1 light colour
+    (procedural_light_emission, main.swift:711-715: (18, 15, 10)): floor, ceiling and back white
+    (0.73), left red (0.63, 0.065, 0.05), right green (0.14, 0.45, 0.091), tall box yellow
+    (0.8, 0.6, 0.1), short box blue (0.1, 0.2, 0.7). Saturated colours exercise the spectral uplift
+    (refined grid cells) and a coloured emitter the emission basis. Same geometry and camera as
+    cornell_box."""
+    faces, verts, materials, light, camera = cornell_box(seed=seed)
+    palette = [(0.73, 0.73, 0.73), (0.73, 0.73, 0.73), (0.73, 0.73, 0.73), (0.63, 0.065, 0.05), (0.14, 0.45, 0.091),
+               (0.8, 0.6, 0.1), (0.1, 0.2, 0.7)]
+    for s, c in enumerate(palette):
+        materials[s] = {"type": 0, "albedo": c, "emission": (0.0, 0.0, 0.0)}
+    e = (18.0, 15.0, 10.0)
+    materials[7] = {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": e}
+    light = dict(light, emission=e)
+    return faces, verts, materials, light, camera
+
+
 def _mesh_from_triangles(tris, tags):
     n = len(tris)
     verts = np.zeros(3 * n, VERTEX_DTYPE)

@@ -5,6 +5,7 @@
 // rounds on its own, exactly as the CUDA kernels' __fmul_rn/__fadd_rn sequence does.
 // See vt_oracle.h for the list of reference functions restated here.
 #include "vt_oracle.h"
+#include "spectral_uplift.h"
 
 #include <algorithm>
 #include <array>
@@ -1529,6 +1530,11 @@ struct PtContext {
   double etotal = 0;
   const uint32_t *ltNodes = nullptr, *ltLeaves = nullptr;
   double ltLo[3] = {0, 0, 0}, ltScale[3] = {0, 0, 0};
+  // Spectral uplift: materials carrying their slot in `pad`, per slot the albedo's multipliers,
+  // per bin the emission basis (R, G, B, C, M, Y).
+  std::vector<vt_material> mats;
+  std::vector<std::array<double, 4>> slotL;
+  std::vector<std::array<double, 6>> basis;
 };
 
 inline double fword(uint32_t w) { float f; std::memcpy(&f, &w, 4); return f; }
@@ -1565,14 +1571,29 @@ D3 to_rgb(const PtContext &C, const PtLanes &L, const Spec4 &s) {
   return rgb;
 }
 
-Spec4 reflectance(const PtContext &C, const vt_material &m) {
-  if (C.spectral) { const double g = (double(m.albedo[0]) + m.albedo[1] + m.albedo[2]) / 3.0; return {{g, g, g, g}}; }
+// spectral_reflectance (main.swift:905-907) of the slot's albedo at the lanes' bins.
+Spec4 reflectance(const PtContext &C, const PtLanes &L, const vt_material &m) {
+  if (C.spectral) {
+    uint32_t slot;
+    std::memcpy(&slot, &m.pad, sizeof slot);
+    if (slot >= C.slotL.size()) return {{0, 0, 0, 0}};
+    Spec4 s;
+    for (int k = 0; k < 4; ++k) s.v[k] = vto_uplift_impl::spectral_value(C.slotL[slot].data(), C.in->cos_phase[L.bin[k]]);
+    return s;
+  }
   return {{m.albedo[0], m.albedo[1], m.albedo[2], 0.0}};
 }
+// spectral_emission (main.swift:913-944): Smits' decomposition on the corners' spectra, times S.
 Spec4 emission(const PtContext &C, const PtLanes &L, const float e[3]) {
   if (C.spectral) {
-    Spec4 s;
-    for (int k = 0; k < 4; ++k) s.v[k] = double(e[0]) * C.in->illum[L.bin[k]];
+    Spec4 s{{0, 0, 0, 0}};
+    if (!(std::max(e[0], std::max(e[1], e[2])) > 0.0f)) return s;
+    const double ed[3] = {e[0], e[1], e[2]};
+    const vto_uplift_impl::EmissionWeights w = vto_uplift_impl::emission_weights(ed);
+    for (int k = 0; k < 4; ++k) {
+      const std::array<double, 6> &b = C.basis[L.bin[k]];
+      s.v[k] = (w.lo + w.secondary * b[3 + w.secondary_index] + w.primary * b[w.primary_index]) * C.in->illum[L.bin[k]];
+    }
     return s;
   }
   return {{e[0], e[1], e[2], 0.0}};
@@ -1640,9 +1661,11 @@ bool pt_occluded(const PtContext &C, D3 o, D3 d, double tmax) {
 }
 
 vt_material pt_material(const PtContext &C, uint32_t slot) {
-  if (slot < C.in->nmat) return C.in->materials[slot];
+  if (slot < C.in->nmat) return C.mats[slot];
   vt_material m;
   std::memset(&m, 0, sizeof m);
+  const uint32_t none = 0xffffffffu;
+  std::memcpy(&m.pad, &none, sizeof none);
   return m;
 }
 
@@ -1955,7 +1978,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     const D3 nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.n * cos_th);
     const double bpdf = std::max(0.0, dot(h.n, nd)) / kPi;
     if (!(bpdf > 0.0) || !(dot(nd, h.gn) > 0.0)) break;
-    T = mul(T, reflectance(C, m));
+    T = mul(T, reflectance(C, L, m));
     bool finite = true;
     for (double t : T.v) finite = finite && std::isfinite(t);
     if (!finite || smax(C, T) <= 0.0) break;
@@ -1972,7 +1995,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     if (emissionOnly) break;
     if (nee) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, reflectance(C, m), mis && scattering < limit, seed,
+      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, reflectance(C, L, m), mis && scattering < limit, seed,
                        false);
     }
     if (bounce > 3) {
@@ -2014,7 +2037,7 @@ D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_ma
   const double ni = dot(n, dir), no = -dot(n, view);
   const double f = no > 0.0 && ni > 0.0 && std::fabs(ni) >= 1e-7 && dot(dir, gn) > 0.0 ? 1.0 / kPi : 0.0;
   const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
-  return to_rgb(C, L, scale(mul(reflectance(C, m), emission(C, L, e)), f * cos_th)) * light_geometry_d(C, p, c);
+  return to_rgb(C, L, scale(mul(reflectance(C, L, m), emission(C, L, e)), f * cos_th)) * light_geometry_d(C, p, c);
 }
 
 // eval_restir_target_pdf (main.swift:3187-3197).
@@ -2163,7 +2186,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (C.p->sampling_mode != 3u) {
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, reflectance(C, m), C.p->sampling_mode == 1u && limit > 0,
+    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, reflectance(C, L, m), C.p->sampling_mode == 1u && limit > 0,
                  seed, true);
   }
   R = R + continue_path_d(C, L, h, m, seed, false);
@@ -2180,6 +2203,22 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
   C.p = p;
   C.bvh = vto_lbvh_build(in->faces, in->nfaces, in->verts, in->nverts, 2, 7, 2);
   C.spectral = p->spectral != 0 && in->cmf_rgb != nullptr;
+  C.mats.assign(in->materials, in->materials + in->nmat);
+  for (uint32_t i = 0; i < in->nmat; ++i) std::memcpy(&C.mats[i].pad, &i, sizeof i);
+  if (C.spectral) {
+    // The uplift: each slot's albedo and the six saturated corners (main.swift:10730-10733).
+    C.slotL.resize(in->nmat);
+    for (uint32_t i = 0; i < in->nmat; ++i) {
+      const double rgb[3] = {in->materials[i].albedo[0], in->materials[i].albedo[1], in->materials[i].albedo[2]};
+      vto_spectral_lagrange(in->uplift, rgb, 1, C.slotL[i].data());
+    }
+    const double corners[18] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 1, 1, 1, 0, 1, 1, 1, 0};
+    double cl[24];
+    vto_spectral_lagrange(in->uplift, corners, 6, cl);
+    C.basis.resize(in->nbins);
+    for (uint32_t b = 0; b < in->nbins; ++b)
+      for (int k = 0; k < 6; ++k) C.basis[b][k] = vto_uplift_impl::spectral_value(cl + 4 * k, in->cos_phase[b]);
+  }
   const D3 pos = d3(p->camera_pos), target = d3(p->camera_target), upv = d3(p->camera_up);
   C.cam = pos;
   C.fwd = normalize(target - pos);

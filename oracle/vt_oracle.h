@@ -95,6 +95,10 @@ typedef struct vto_pt_inputs {
   const uint32_t *emitters;
   uint32_t nemitter_words;
   uint32_t imported;
+  /* Spectral uplift (spectral_uplift.h): the colour model with its lazily solved grid, and cos of
+   * the warped phase at each of the nbins bins. Needed when spectral. */
+  const struct vto_uplift *uplift;
+  const float *cos_phase;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

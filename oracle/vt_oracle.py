@@ -233,7 +233,8 @@ class PtInputs(C.Structure):
                 ("materials", C.c_void_p), ("nmat", C.c_uint32), ("light", QuadLight),
                 ("cmf_rgb", C.c_void_p), ("illum", C.c_void_p), ("icdf", C.c_void_p),
                 ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float),
-                ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32)]
+                ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32),
+                ("uplift", C.c_void_p), ("cos_phase", C.c_void_p)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -261,7 +262,7 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         for k in ("corner", "su", "sv", "normal", "emission"):
             getattr(q, k)[:] = [float(x) for x in light[k]]
     inp = PtInputs(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0], C.cast(mats, C.c_void_p), len(materials), q,
-                   None, None, None, 0, 0, 0.0, None, 0, 0)
+                   None, None, None, 0, 0, 0.0, None, 0, 0, None, None)
     keep = []
     if light is None:
         if emitter_words is None:
@@ -277,6 +278,10 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         keep += [cmf, ill, icdf]
         inp.cmf_rgb, inp.illum, inp.icdf = cmf.ctypes.data, ill.ctypes.data, icdf.ctypes.data
         inp.nbins, inp.segments, inp.lambda_min = cmf.shape[0], icdf.shape[0] - 1, float(spectral["lambda_min"])
+        cosp = np.ascontiguousarray(spectral["cos_phase"], np.float32)
+        up = uplift_for(spectral)
+        keep += [cosp, up]
+        inp.uplift, inp.cos_phase = up._p, cosp.ctypes.data
     p = FrameParams()
     p.camera_pos[:] = [float(x) for x in camera["pos"]]
     p.camera_target[:] = [float(x) for x in camera["target"]]
@@ -412,3 +417,15 @@ def reflectance(L4, cos_phi):
     if L4[3] == 2.0:
         return np.full(x.shape, L4[0])
     return np.arctan(L4[0] + 2.0 * L4[1] * x + 2.0 * L4[2] * (2.0 * x * x - 1.0)) / np.pi + 0.5
+
+
+_UPLIFTS = {}
+
+
+def uplift_for(spectral) -> "Uplift":
+    """One oracle uplift per colour model (its solved grid nodes are kept between renders)."""
+    key = (np.asarray(spectral["uplift_w"], np.float64).tobytes(), np.asarray(spectral["uplift_cos"], np.float64).tobytes())
+    key = hash(key)
+    if key not in _UPLIFTS:
+        _UPLIFTS[key] = Uplift(spectral["uplift_w"], spectral["uplift_cos"])
+    return _UPLIFTS[key]

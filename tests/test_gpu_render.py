@@ -89,9 +89,10 @@ def test_render_rejects_unsupported_input(ctx, cornell):
     faces, verts, mats, light, cam, mesh = cornell
     coloured = [dict(m) for m in mats]
     coloured[3] = {"type": 0, "albedo": (0.65, 0.05, 0.05), "emission": (0, 0, 0)}
-    with pytest.raises(vt.MaterialLibraryError, match="grey materials"):
-        vt.Scene(ctx, mesh, coloured, light, spectral_tables.load())
-    scene = vt.Scene(ctx, mesh, coloured, light)   # RGB transport takes colours
+    tables = spectral_tables.load()
+    with pytest.raises(vt.MaterialLibraryError, match="colour model"):
+        vt.Scene(ctx, mesh, coloured, light, dict(tables, uplift_w=np.zeros((1, 3)), uplift_cos=np.zeros(1)))
+    scene = vt.Scene(ctx, mesh, coloured, light)   # RGB transport needs no tables
     with pytest.raises(vt.MaterialLibraryError, match="sampling_mode"):
         scene.render(vt.make_params(cam, 8, 8, 8, 1, False, mode=4), 1)
     with pytest.raises(vt.MaterialLibraryError, match="spectral tables"):
