@@ -431,6 +431,9 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
             nrm[3 * prim] = make_float4(va.nx, va.ny, va.nz, 0.0f);
             nrm[3 * prim + 1] = make_float4(vb.nx, vb.ny, vb.nz, 0.0f);
             nrm[3 * prim + 2] = make_float4(vc.nx, vc.ny, vc.nz, 0.0f);
+            const bool some = va.nx != 0.0f || va.ny != 0.0f || va.nz != 0.0f || vb.nx != 0.0f || vb.ny != 0.0f ||
+                              vb.nz != 0.0f || vc.nx != 0.0f || vc.ny != 0.0f || vc.nz != 0.0f;
+            if (some) atomicOr(status, (uint32_t)VT_DEV_NORMALS);
           }
           ++prim;
           continue;
@@ -616,6 +619,11 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
     VT_CUDA(ctx, cudaMemcpy(&st0, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     if (st0 & VT_DEV_BAD_INDEX) return vt_fail(ctx, VT_ERR_INVALID, "a face indexes past the vertex array");
     if (st0 & VT_DEV_NONFINITE) return vt_fail(ctx, VT_ERR_INVALID, "a vertex position is not finite");
+    // A mesh without vertex normals shades with geometric normals: no normal buffer to read.
+    if (!(st0 & VT_DEV_NORMALS)) {
+      VT_CUDA(ctx, cudaFree(mesh->d_nrm));
+      mesh->d_nrm = nullptr;
+    }
   }
   if (primBase != n) return vt_fail(ctx, VT_ERR_DEVICE, "collapse emitted " + std::to_string(primBase) + " of " + std::to_string(n) + " triangles");
 

@@ -282,6 +282,9 @@ __device__ __forceinline__ float3 lanes_rgb(const RenderArgs &A, const Lanes &L,
 // emission basis at the lane's bin times S there; white is S exactly.
 __device__ __forceinline__ float4 lanes_emission(const RenderArgs &A, const Lanes &L, float3 e) {
   if (!(fmaxf(e.x, fmaxf(e.y, e.z)) > 0.0f)) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (e.x == e.y && e.y == e.z)  // white: e S exactly (the basis terms have zero weight)
+    return make_float4(e.x * __ldg(A.spec + L.bin[0]).w, e.x * __ldg(A.spec + L.bin[1]).w, e.x * __ldg(A.spec + L.bin[2]).w,
+                       e.x * __ldg(A.spec + L.bin[3]).w);
   const EmissionWeights w = emission_weights(e);
   float v[4];
 #pragma unroll
@@ -291,6 +294,7 @@ __device__ __forceinline__ float4 lanes_emission(const RenderArgs &A, const Lane
 // A slot's albedo as a reflectance at the lanes' bins (spectral_reflectance, main.swift:905-907).
 __device__ __forceinline__ float4 lanes_reflectance(const RenderArgs &A, const Lanes &L, uint32_t slot) {
   const float4 q = __ldg(A.slotL + slot);
+  if (q.w == 2.0f) return make_float4(q.x, q.x, q.x, q.x);  // a grey: flat
   return make_float4(fourier_reflectance(q, __ldg(A.cosPhase + L.bin[0])), fourier_reflectance(q, __ldg(A.cosPhase + L.bin[1])),
                      fourier_reflectance(q, __ldg(A.cosPhase + L.bin[2])), fourier_reflectance(q, __ldg(A.cosPhase + L.bin[3])));
 }

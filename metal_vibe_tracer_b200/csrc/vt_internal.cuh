@@ -151,7 +151,8 @@ enum : uint32_t {
   VT_DEV_BAD_INDEX = 1u,       // a face indexes past the vertex array
   VT_DEV_NONFINITE = 2u,       // a vertex position is NaN or infinite
   VT_DEV_STACK = 4u,           // traversal stack overflow
-  VT_DEV_TREELET = 8u          // treelet restructuring hit an internal inconsistency
+  VT_DEV_TREELET = 8u,         // treelet restructuring hit an internal inconsistency
+  VT_DEV_NORMALS = 16u         // information, not an error: some vertex normal is nonzero
 };
 
 // ---------------------------------------------------------------------------------------------

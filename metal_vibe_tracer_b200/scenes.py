@@ -404,15 +404,17 @@ def _lattice_noise(dirs, seeds):
     return noise
 
 
-def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displace: float = 0.05):
+def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displace: float = 0.05, nmat: int = 8,
+                coloured: bool = False):
     """The grid scene's generator (configs C3/C4): a k x k grid of displaced icospheres on a ground quad,
     with k and the subdivision level chosen so that the mesh has about `triangles` triangles (the
     largest subdivision <= 5 whose 20 * 4^s triangles fit four spheres, then k = round(sqrt(T / per))).
     Spheres have radius 0.4 on a unit lattice; each vertex moves along its direction by
     displace * (2 n - 1), n a trilinear value noise of the direction over a 17^3 lattice of PCG hashes
     seeded per sphere; normals are the normalised sums of incident face normals (smooth shading).
-    Albedos are grey Lambert 0.2 + 0.6 u from 8 slots; every `emissive_every`-th sphere is an emitter
-    (radiance 4, 8 or 12, grey), so the scene is an imported scene lit by its emissive triangles.
+    Albedos are grey Lambert 0.2 + 0.6 u from `nmat` slots (with `coloured`, base colours uniform in
+    [0, 1]^3 instead); every `emissive_every`-th sphere is an emitter (radiance 4, 8 or 12, grey, in
+    slots nmat .. nmat + 2), so the scene is an imported scene lit by its emissive triangles.
     Returns faces, vertices, materials and a camera looking down on the grid."""
     per = 20
     sub = 0
@@ -435,7 +437,7 @@ def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displac
     vn /= np.linalg.norm(vn, axis=2, keepdims=True)
     pos = local * 0.4 + centers[:, None, :]
     emissive = (emissive_every > 0) & (sid % max(emissive_every, 1) == emissive_every // 2)
-    sphere_tag = np.where(emissive, 8 + sid % 3, sid % 8).astype(np.uint32)
+    sphere_tag = np.where(emissive, nmat + sid % 3, sid % nmat).astype(np.uint32)
     half = k / 2.0 + 1.0
     ground = np.array([(-half, 0.0, -half), (half, 0.0, -half), (half, 0.0, half), (-half, 0.0, half)])
     p = np.concatenate([pos.reshape(-1, 3), ground])
@@ -449,12 +451,24 @@ def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displac
     faces = np.zeros(len(t), FACE_DTYPE)
     faces["a"], faces["b"], faces["c"] = t[:, 0], t[:, 1], t[:, 2]
     faces["tag"] = tg
-    mats = [{"type": 0, "albedo": (float(a),) * 3, "emission": (0.0, 0.0, 0.0)}
-            for a in 0.2 + 0.6 * rng.random(8)]
+    if coloured:
+        mats = [{"type": 0, "albedo": tuple(float(x) for x in c), "emission": (0.0, 0.0, 0.0)} for c in rng.random((nmat, 3))]
+    else:
+        mats = [{"type": 0, "albedo": (float(a),) * 3, "emission": (0.0, 0.0, 0.0)} for a in 0.2 + 0.6 * rng.random(nmat)]
     mats += [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (float(e),) * 3} for e in (4.0, 8.0, 12.0)]
     d = max(2.0, 0.9 * k)
     camera = {"pos": (0.0, 0.8 * d, -1.2 * d), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 45.0}
     return faces, verts, mats, camera
+
+
+def production_scene(seed: int = 0, triangles: int = 10_000_000, emitters: int = 100_000, nmat: int = 287):
+    """The production-scale grid scene: ~`triangles` triangles of displaced subdivision-5 icospheres
+    (20,480 triangles each), ~`emitters` emissive triangles (whole emissive spheres), `nmat` material
+    slots with base colours uniform in [0, 1]^3 (Lambert: the OpenPBR lobes are not built) and a
+    camera over the grid. Returns faces, vertices, materials, camera."""
+    spheres = max(1, round(triangles / 20480))
+    every = max(1, round(spheres / max(1, round(emitters / 20480))))
+    return sphere_grid(triangles, seed=seed, emissive_every=every, nmat=nmat, coloured=True)
 
 
 def batch_workload(count: int = 64, seed: int = 0, lo: int = 10_000, hi: int = 2_000_000):
