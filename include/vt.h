@@ -151,12 +151,12 @@ vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_de
 typedef struct vt_scene vt_scene;
 
 /* Material types: the reference's MaterialType values (main.swift:316-322). */
-enum { VT_MAT_DIFFUSE = 0, VT_MAT_EMISSIVE = 3 };
+enum { VT_MAT_DIFFUSE = 0, VT_MAT_EMISSIVE = 3, VT_MAT_OPENPBR = 4 };
 
 /* A constant material slot (the role of SurfaceSettings / MaterialResources, main.swift:2253-2263,
  * 628-654, for constant Lambert and emissive surfaces). A face's tag selects its slot. 32 bytes. */
 typedef struct vt_material {
-  int32_t type;        /* VT_MAT_DIFFUSE or VT_MAT_EMISSIVE */
+  int32_t type;        /* VT_MAT_DIFFUSE, VT_MAT_EMISSIVE or VT_MAT_OPENPBR (base colour = albedo) */
   float albedo[3];     /* linear sRGB reflectance (Lambert) */
   float emission[3];   /* linear sRGB radiance (emissive) */
   float pad;
@@ -302,6 +302,46 @@ vt_status vt_spectral_lagrange(vt_ctx *ctx, const float *rgb, uint32_t n, float 
  * back to sRGB under D65), on the device: the largest error in 8-bit steps and how many codes
  * miss by more than half a step (the reference's round-trip check, tests/Fix_spectral.swift). */
 vt_status vt_spectral_round_trip(vt_ctx *ctx, float *worst, uint32_t *over_half);
+
+/* ---- OpenPBR materials (openpbr.cu) ------------------------------------------------------------ */
+/* The layered BSDF of the reference's OPENPBR material type (prepare_openpbr, main.swift:2485-2512,
+ * around the vendored Adobe openpbr-bsdf) for opaque materials: specular_weight, base colour,
+ * metalness, specular roughness and IOR, diffuse roughness; coat, fuzz, transmission, thin film and
+ * anisotropy are not supported. Its energy-compensation data: the dense metal table is solved on the
+ * device (the reference's Shaders/MetalEnergy.metal); the opaque-dielectric energy complement tables
+ * (32^3 and 32^2 unorm16, the upstream library's data) come from the caller, once per context. */
+typedef struct vt_openpbr_tables {
+  const uint16_t *opaque_energy;   /* 32 x 32 x 32: IOR, sqrt(alpha), cos */
+  const uint16_t *opaque_average;  /* 32 x 32: IOR, sqrt(alpha) */
+} vt_openpbr_tables;
+vt_status vt_openpbr_tables_set(vt_ctx *ctx, const vt_openpbr_tables *tables);
+/* The dense isotropic GGX energy complement (129 x 129: roughness i/128, sqrt(cos) j/128) and its
+ * per-roughness average (129), as solved on the device. */
+vt_status vt_openpbr_energy_table(vt_ctx *ctx, float *table, float *average);
+
+/* One BSDF query: an OPENPBR material's parameters as the adapter reads them (roughness and IOR are
+ * clamped to >= 0.03 and >= 1.01 inside), a unit shading normal, the view (outward) and light
+ * directions, and three random numbers for a sample. 80 bytes. */
+typedef struct vt_openpbr_case {
+  float base_color[3], metalness, roughness, ior, specular_weight, diffuse_roughness;
+  float normal[3], view[3], light[3], rand[3];
+} vt_openpbr_case;
+/* f |cos| at the light direction and its pdf; the sample: direction, weight f |cos| / pdf, its pdf,
+ * and 1 when a sample was produced. 48 bytes. */
+typedef struct vt_openpbr_result {
+  float f_cos[3], pdf;
+  float dir[3], weight[3], sample_pdf, ok;
+} vt_openpbr_result;
+/* openpbr_prepare + openpbr_eval / openpbr_pdf / openpbr_sample for n queries on the device. */
+vt_status vt_openpbr_evaluate(vt_ctx *ctx, const vt_openpbr_case *cases, uint32_t n, vt_openpbr_result *out);
+
+/* A scene's OPENPBR slot parameters (SurfaceSettings surface/detail, main.swift:2253-2263, as
+ * resolve_material sets them; base colour is the slot's albedo): one per material slot, read for the
+ * slots whose type is VT_MAT_OPENPBR. Needs vt_openpbr_tables_set on the context first. */
+typedef struct vt_openpbr_params {
+  float roughness, metalness, ior, diffuse_roughness;
+} vt_openpbr_params;
+vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n);
 
 /* ---- emitter lights: light tree and emitter list ----------------------------------------- */
 

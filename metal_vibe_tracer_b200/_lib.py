@@ -51,6 +51,28 @@ class SpectralGridInfo(C.Structure):
                 ("pad", C.c_uint32), ("max_residual", C.c_double)]
 
 
+class OpenPBRTables(C.Structure):
+    _fields_ = [("opaque_energy", C.c_void_p), ("opaque_average", C.c_void_p)]
+
+
+class OpenPBRCase(C.Structure):
+    _fields_ = [("base_color", C.c_float * 3), ("metalness", C.c_float), ("roughness", C.c_float), ("ior", C.c_float),
+                ("specular_weight", C.c_float), ("diffuse_roughness", C.c_float), ("normal", C.c_float * 3),
+                ("view", C.c_float * 3), ("light", C.c_float * 3), ("rand", C.c_float * 3)]
+
+
+class OpenPBRResult(C.Structure):
+    _fields_ = [("f_cos", C.c_float * 3), ("pdf", C.c_float), ("dir", C.c_float * 3), ("weight", C.c_float * 3),
+                ("sample_pdf", C.c_float), ("ok", C.c_float)]
+
+
+class OpenPBRParams(C.Structure):
+    _fields_ = [("roughness", C.c_float), ("metalness", C.c_float), ("ior", C.c_float), ("diffuse_roughness", C.c_float)]
+
+
+assert C.sizeof(OpenPBRCase) == 80 and C.sizeof(OpenPBRResult) == 48
+
+
 class BatchStats(C.Structure):
     _fields_ = [("scenes", C.c_uint32), ("passes", C.c_uint32), ("items", C.c_ulonglong), ("last_ms", C.c_float),
                 ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
@@ -110,6 +132,10 @@ SIGNATURES = {
     "vt_spectral_grid_read": (_I32, [_P, _P, _U32]),
     "vt_spectral_lagrange": (_I32, [_P, _P, _U32, _P]),
     "vt_spectral_round_trip": (_I32, [_P, C.POINTER(C.c_float), C.POINTER(_U32)]),
+    "vt_openpbr_tables_set": (_I32, [_P, C.POINTER(OpenPBRTables)]),
+    "vt_openpbr_energy_table": (_I32, [_P, _P, _P]),
+    "vt_openpbr_evaluate": (_I32, [_P, _P, _U32, _P]),
+    "vt_scene_set_openpbr": (_I32, [_P, _P, _P, _U32]),
 }
 NOALLOC_MAX_FACES = 32768
 

@@ -1,0 +1,467 @@
+// openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials: a GGX (VNDF-sampled)
+// specular lobe with dielectric Fresnel on the dielectric part and F82-tinted Schlick on the metal
+// part, the metal's microfacet multiple-scattering lobe, and the energy-conserving (EON) diffuse
+// base, combined as one aggregate with lobe selection by estimated contribution.
+//
+// Reference: the reference's adapter prepare_openpbr / prepared_eval / prepared_pdf /
+// prepared_sample (main.swift:2485-2512, 2594-2644) around the vendored Adobe openpbr-bsdf
+// (c91aad1d, Vendor/OpenPBR): openpbr_prepare_lobes (impl/openpbr_bsdf.h:289-912), the aggregate
+// lobe (impl/openpbr_aggregate_lobe.h), the comprehensive microfacet lobe
+// (impl/openpbr_comprehensive_microfacet_lobe.h) with its coefficients
+// (impl/openpbr_reflection_transmission_coefficient.h), the multiple-scattering lobes
+// (impl/openpbr_microfacet_multiple_scattering_lobes.h), the EON diffuse lobe
+// (impl/openpbr_diffuse_lobe.h), and the spherical-cap VNDF sampler and Smith G1
+// (impl/openpbr_lobe_utils.h:85-128; Dupuy and Benyoub 2023, Heitz 2018). The metal lookups use
+// the dense 129 x 129 table of Shaders/MetalEnergy.metal, solved on the device (openpbr.cu), as the
+// reference substitutes it (scripts/prepare_shaders.py:28-39).
+//
+// What the restatement covers: specular_weight, base_color, base_metalness, specular_roughness,
+// specular_ior, base_diffuse_roughness, with coat, fuzz, transmission, subsurface, thin film,
+// anisotropy and dispersion at zero. In that case the upstream coat and fuzz layers pass the base
+// through (presence 0), the dielectric multiple-scattering lobe and both thin-wall lobes have zero
+// weight and value, and specular transmission has zero probability; the code below keeps only what
+// is left, in the upstream operation order. The coat and fuzz layers' recomputation of the sample
+// weight (w pdf / pdf, twice) is kept for the same rounding.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vtd {
+
+constexpr float kPbrPi = 3.14159265f;
+constexpr float kPbrTwoPi = 6.28318531f;
+constexpr float kPbrRcpPi = 0.318309886f;
+constexpr float kPbrRcpTwoPi = 0.159154943f;
+constexpr float kPbrBelowOne = 0.999999940f;
+constexpr float kPbrFloatMin = 1.175494351e-38f;
+constexpr float kPbrMinAlphaEnergyLoss = 0.04f * 0.04f;
+constexpr int kPbrTable = 32;           // the opaque-dielectric energy tables' size per axis
+constexpr float kPbrIorMax = 2.5f;
+constexpr uint32_t kMetalEnergyN = 129;  // the dense metal table: 129 roughness x 129 sqrt-cosine nodes
+
+// Per slot: base colour (clamped), metalness, roughness (>= 0.03), IOR (>= 1.01), specular weight,
+// diffuse roughness.
+struct PbrParams {
+  float3 base;
+  float metal, rough, ior, sw, diffRough;
+};
+
+struct PbrTables {
+  const float *metalE;     // 129 x 129
+  const float *metalAvg;   // 129
+  const float *opaqueE;    // 32 x 32 x 32 (ior, alpha, cos)
+  const float *opaqueAvg;  // 32 x 32 (ior, alpha)
+};
+
+__device__ __forceinline__ float3 pf3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 padd(float3 a, float3 b) { return pf3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 psub(float3 a, float3 b) { return pf3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 pmul(float3 a, float3 b) { return pf3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float3 pscale(float3 a, float s) { return pf3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float pdot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 pnormalize(float3 a) {
+  const float l = sqrtf(pdot(a, a));
+  return pf3(a.x / l, a.y / l, a.z / l);
+}
+__device__ __forceinline__ float pmax3(float3 v) { return fmaxf(fmaxf(v.x, v.y), v.z); }
+__device__ __forceinline__ float psq(float x) { return x * x; }
+__device__ __forceinline__ float pmix(float a, float b, float t) { return a + (b - a) * t; }
+__device__ __forceinline__ float psat(float x) { return x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x); }
+__device__ __forceinline__ float psafe_div(float n, float d, float fallback) { return d != 0.0f ? n / d : fallback; }
+__device__ __forceinline__ float pclamp_rand(float r) { return fminf(r, kPbrBelowOne); }
+
+// An orthonormal frame (openpbr_make_basis from a normal; Duff et al. 2017).
+struct PbrBasis {
+  float3 t, b, n;
+};
+__device__ __forceinline__ PbrBasis pbr_basis(float3 n) {
+  PbrBasis B;
+  B.n = n;
+  const float s = n.z < 0.0f ? -1.0f : 1.0f;
+  const float a = -1.0f / (s + n.z);
+  const float b = n.x * n.y * a;
+  B.t = pf3(b, s + n.y * n.y * a, -n.y);
+  B.b = pf3(1.0f + s * n.x * n.x * a, s * b, -s * n.x);
+  return B;
+}
+__device__ __forceinline__ float3 pbr_to_local(const PbrBasis &B, float3 d) { return pf3(pdot(d, B.t), pdot(d, B.b), pdot(d, B.n)); }
+__device__ __forceinline__ float3 pbr_to_world(const PbrBasis &B, float3 d) {
+  return padd(padd(pscale(B.t, d.x), pscale(B.b, d.y)), pscale(B.n, d.z));
+}
+
+// GGX with Smith masking (isotropic alpha on both axes), local frame.
+__device__ __forceinline__ float ggx_d(float3 h, float ax) {
+  return 1.0f / (kPbrPi * ax * ax * psq(psq(h.x / ax) + psq(h.y / ax) + psq(h.z)));
+}
+__device__ __forceinline__ float smith_g1(float3 v, float ax) {
+  const float vz2 = psq(v.z);
+  if (vz2 == 0.0f) return 0.0f;
+  return 2.0f / (1.0f + sqrtf(1.0f + (psq(ax * v.x) + psq(ax * v.y)) / vz2));
+}
+// Spherical-cap VNDF sampling (Dupuy and Benyoub 2023), local frame.
+__device__ __forceinline__ float3 ggx_sample_vndf(float ax, float3 wi, float2 r) {
+  const float3 ih = pnormalize(pf3(ax * wi.x, ax * wi.y, wi.z));
+  const float c = fminf(ih.z, 1.0f);
+  const float angle = kPbrTwoPi * r.x;
+  const float onePlusCos = 1.0f + c;
+  const float hz = (1.0f - r.y) * onePlusCos;
+  const float oneMinusZ = r.y * onePlusCos;
+  const float onePlusZ = hz + (1.0f - c);
+  const float tangent = sqrtf(onePlusZ * oneMinusZ);
+  const float3 m = pf3(tangent * cosf(angle) + ih.x, tangent * sinf(angle) + ih.y, hz);
+  return pnormalize(pf3(ax * m.x, ax * m.y, m.z));
+}
+
+// Real unpolarised Fresnel reflectance (openpbr_fresnel).
+__device__ __forceinline__ float pbr_fresnel(float eta, float ci) {
+  if (eta == 1.0f) return 0.0f;
+  const float s2i = 1.0f - psq(ci);
+  const float s2t = s2i / psq(eta);
+  if (s2t >= 1.0f) return 1.0f;
+  const float ct = sqrtf(1.0f - s2t);
+  const float eci = eta * ci, ect = eta * ct;
+  const float rs = psq((ci - ect) / (ci + ect));
+  const float rp = psq((ct - eci) / (ct + eci));
+  return 0.5f * (rs + rp);
+}
+// F82-tinted Schlick for the metal (white tint: b = r (1 - cos_max)^5 ... with t = 1 gives b = 0).
+__device__ __forceinline__ float3 pbr_f82_b(float3 f0, float3 tint) {
+  const float cm = 1.0f / 7.0f, omc = 1.0f - cm;
+  const float omc2 = omc * omc;
+  const float p5 = omc2 * omc2 * omc, p6 = omc2 * omc2 * omc2;
+  const float rden = 1.0f / (cm * p6);
+  return pf3((f0.x + (1.0f - f0.x) * p5) * (1.0f - tint.x) * rden, (f0.y + (1.0f - f0.y) * p5) * (1.0f - tint.y) * rden,
+             (f0.z + (1.0f - f0.z) * p5) * (1.0f - tint.z) * rden);
+}
+__device__ __forceinline__ float3 pbr_metal_fresnel(float3 f0, float cosT) {
+  const float3 b = pbr_f82_b(f0, pf3(1.0f, 1.0f, 1.0f));
+  const float omc = 1.0f - cosT, omc2 = omc * omc, p5 = omc2 * omc2 * omc;
+  return pf3(psat(f0.x + ((1.0f - f0.x) - b.x * cosT * omc) * p5), psat(f0.y + ((1.0f - f0.y) - b.y * cosT * omc) * p5),
+             psat(f0.z + ((1.0f - f0.z) - b.z * cosT * omc) * p5));
+}
+__device__ __forceinline__ float3 pbr_metal_average_fresnel(float3 f0) {
+  const float3 b = pbr_f82_b(f0, pf3(1.0f, 1.0f, 1.0f));
+  return pf3(psat(f0.x + (1.0f - f0.x) * (1.0f / 21.0f) - b.x * (1.0f / 126.0f)),
+             psat(f0.y + (1.0f - f0.y) * (1.0f / 21.0f) - b.y * (1.0f / 126.0f)),
+             psat(f0.z + (1.0f - f0.z) * (1.0f / 21.0f) - b.z * (1.0f / 126.0f)));
+}
+// specular_weight applied to a relative IOR (openpbr_apply_specular_weight_to_ior).
+__device__ __forceinline__ float pbr_weighted_ior(float eta, float sw) {
+  const float f0 = psq((eta - 1.0f) / (eta + 1.0f));
+  const float sf0 = fminf(f0 * sw, 0.9999f);
+  const float s = sqrtf(sf0);
+  const float ext = (1.0f + s) / (1.0f - s);
+  return eta < 1.0f ? 1.0f / ext : ext;
+}
+
+// ---- energy tables ---------------------------------------------------------------------------
+// The dense metal table (vibe_metal_energy / vibe_metal_average_energy, Shaders/MetalEnergy.metal:
+// 2108-2119): bilinear in (sqrt(alpha), sqrt(cos)) over 129 x 129 nodes.
+__device__ __forceinline__ float pbr_metal_energy(const PbrTables &T, float alpha, float c) {
+  const float x = fminf(fmaxf(sqrtf(alpha) * 128.0f, 0.0f), 128.0f);
+  const float y = sqrtf(psat(c)) * 128.0f;
+  const uint32_t ix = min((uint32_t)x, 127u), iy = min((uint32_t)y, 127u);
+  const float *t = T.metalE;
+  return pmix(pmix(__ldg(t + ix * kMetalEnergyN + iy), __ldg(t + ix * kMetalEnergyN + iy + 1), y - float(iy)),
+              pmix(__ldg(t + (ix + 1) * kMetalEnergyN + iy), __ldg(t + (ix + 1) * kMetalEnergyN + iy + 1), y - float(iy)), x - float(ix));
+}
+__device__ __forceinline__ float pbr_metal_average(const PbrTables &T, float alpha) {
+  const float x = fminf(fmaxf(sqrtf(alpha) * 128.0f, 0.0f), 128.0f);
+  const uint32_t ix = min((uint32_t)x, 127u);
+  return pmix(__ldg(T.metalAvg + ix), __ldg(T.metalAvg + ix + 1), x - float(ix));
+}
+// The 32^3 / 32^2 opaque-dielectric tables (impl/openpbr_microfacet_multiple_scattering_data.h).
+__device__ __forceinline__ float pbr_ior_index(float ior) {
+  const float inv = 1.0f / (kPbrIorMax - 1.0f);
+  if (ior < 1.0f) return float(kPbrTable / 2 - 1) - ((1.0f / ior) - 1.0f) * inv * float(kPbrTable / 2 - 1);
+  return float(kPbrTable / 2) + (ior - 1.0f) * inv * float(kPbrTable / 2 - 1);
+}
+__device__ __forceinline__ float pbr_clamp_index(float x) { return fminf(fmaxf(x, 0.0f), float(kPbrTable - 1)); }
+__device__ __forceinline__ float pbr_beyond_ior_max(float v, float ior) {
+  if (ior > kPbrIorMax || ior < 1.0f / kPbrIorMax) {
+    const float f0max = psq((kPbrIorMax - 1.0f) / (kPbrIorMax + 1.0f));
+    const float f0 = psq((ior - 1.0f) / (ior + 1.0f));
+    return (1.0f - (f0 - f0max) * (1.0f / (1.0f - f0max))) * v;
+  }
+  return v;
+}
+__device__ __forceinline__ float pbr_opaque_energy(const PbrTables &T, float ior, float alpha, float c) {
+  const float fx = pbr_clamp_index(pbr_ior_index(ior)), fy = pbr_clamp_index(sqrtf(alpha) * float(kPbrTable - 1)),
+              fz = pbr_clamp_index(c * float(kPbrTable - 1));
+  const int x0 = (int)floorf(fx), y0 = (int)floorf(fy), z0 = (int)floorf(fz);
+  const int x1 = min(x0 + 1, kPbrTable - 1), y1 = min(y0 + 1, kPbrTable - 1), z1 = min(z0 + 1, kPbrTable - 1);
+  const float tx = fx - float(x0), ty = fy - float(y0), tz = fz - float(z0);
+  const float *t = T.opaqueE;
+  auto at = [&](int x, int y, int z) { return __ldg(t + (x * kPbrTable + y) * kPbrTable + z); };
+  const float v00 = pmix(at(x0, y0, z0), at(x1, y0, z0), tx), v01 = pmix(at(x0, y0, z1), at(x1, y0, z1), tx);
+  const float v10 = pmix(at(x0, y1, z0), at(x1, y1, z0), tx), v11 = pmix(at(x0, y1, z1), at(x1, y1, z1), tx);
+  return pbr_beyond_ior_max(pmix(pmix(v00, v10, ty), pmix(v01, v11, ty), tz), ior);
+}
+__device__ __forceinline__ float pbr_opaque_average(const PbrTables &T, float ior, float alpha) {
+  const float fx = pbr_clamp_index(pbr_ior_index(ior)), fy = pbr_clamp_index(sqrtf(alpha) * float(kPbrTable - 1));
+  const int x0 = (int)floorf(fx), y0 = (int)floorf(fy);
+  const int x1 = min(x0 + 1, kPbrTable - 1), y1 = min(y0 + 1, kPbrTable - 1);
+  const float tx = fx - float(x0), ty = fy - float(y0);
+  const float *t = T.opaqueAvg;
+  const float v0 = pmix(__ldg(t + x0 * kPbrTable + y0), __ldg(t + x1 * kPbrTable + y0), tx);
+  const float v1 = pmix(__ldg(t + x0 * kPbrTable + y1), __ldg(t + x1 * kPbrTable + y1), tx);
+  return pbr_beyond_ior_max(pmix(v0, v1, ty), ior);
+}
+
+// ---- the prepared BSDF -----------------------------------------------------------------------
+struct PbrPrepared {
+  PbrBasis B;          // face-forwarded shading frame (normal_ff = B.n)
+  float3 wo;           // view direction (outward)
+  float alpha, ax;     // specular alpha, and the microfacet alpha (clamped at 1e-6)
+  float etaOpaque;     // relative IOR of the opaque reflection
+  float scaleOpaque;   // opaque dielectric share (specular colour 1)
+  float metalAmount;   // darkened metal
+  float3 f0;           // weighted base colour: the metal's normal-incidence reflectance
+  float3 metalScale;   // metal multiple-scattering scale
+  float metalEc;       // metal energy complement at the view
+  float3 diffAlbedo;
+  float diffRough, diffComp;
+  float wSpec, wMetal, wDiff, total;
+};
+
+// openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit).
+__device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const PbrTables &T, float3 n, float3 wo) {
+  PbrPrepared p;
+  p.wo = wo;
+  p.B = pbr_basis(n);
+  const bool back = pdot(wo, n) < 0.0f;
+  if (back) {
+    p.B.t = pscale(p.B.t, -1.0f);
+    p.B.b = pscale(p.B.b, -1.0f);
+    p.B.n = pscale(p.B.n, -1.0f);
+  }
+  const float wior = 1.0f * pbr_weighted_ior(P.ior / 1.0f, P.sw);
+  p.etaOpaque = back ? wior / 1.0f : wior / 1.0f;
+  p.alpha = psq(P.rough);
+  p.ax = fmaxf(p.alpha, 1e-6f);
+  const float dielectric = 1.0f - P.metal;
+  p.scaleOpaque = 1.0f * 1.0f * dielectric;
+  p.metalAmount = P.metal * P.sw;
+  p.f0 = pscale(P.base, 1.0f);  // base_weight 1
+  const float3 maf = pbr_metal_average_fresnel(p.f0);
+  p.metalScale = pscale(pmul(maf, maf), p.metalAmount);
+  const float idotn = pdot(wo, p.B.n);
+  p.metalEc = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pbr_metal_energy(T, p.alpha, idotn);
+  p.diffAlbedo = pscale(p.f0, p.scaleOpaque);
+  p.diffRough = P.diffRough;
+  {
+    const float num = pbr_opaque_energy(T, p.etaOpaque, p.alpha, idotn);
+    const float den = pbr_opaque_average(T, p.etaOpaque, p.alpha);
+    p.diffComp = num / fmaxf(den, 1e-12f);
+  }
+  // Lobe weights (estimated contributions with a white throughput).
+  {
+    const float F = pbr_fresnel(p.etaOpaque, idotn);
+    const float3 fm = pbr_metal_fresnel(p.f0, idotn);
+    const float3 refl = padd(pf3(p.scaleOpaque * F, p.scaleOpaque * F, p.scaleOpaque * F), pscale(fm, p.metalAmount));
+    p.wSpec = pmax3(refl);
+  }
+  p.wMetal = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pmax3(p.metalScale) * p.metalEc;
+  p.wDiff = pmax3(pscale(p.diffAlbedo, p.diffComp));
+  p.total = ((((p.wSpec + 0.0f) + p.wMetal) + p.wDiff) + 0.0f) + 0.0f;
+  return p;
+}
+
+// Reflection coefficient of the specular lobe at |cos| to the half vector.
+__device__ __forceinline__ float3 pbr_spec_coeff(const PbrPrepared &p, float c) {
+  const float F = pbr_fresnel(p.etaOpaque, c);
+  const float3 fm = pbr_metal_fresnel(p.f0, c);
+  return padd(pf3(p.scaleOpaque * F, p.scaleOpaque * F, p.scaleOpaque * F), pscale(fm, p.metalAmount));
+}
+
+__device__ __forceinline__ float3 pbr_spec_value(const PbrPrepared &p, float3 wi) {
+  const float idotn = pdot(p.B.n, p.wo), odotn = pdot(p.B.n, wi);
+  if (!(idotn * odotn > 0.0f)) return pf3(0.0f, 0.0f, 0.0f);
+  const float3 h = pnormalize(padd(p.wo, wi));
+  const float idoth = pdot(p.wo, h);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  const float other = 1.0f / (4.0f * idotn);
+  const float3 F = pbr_spec_coeff(p, fabsf(idoth));
+  const float3 DoF = pscale(F, D * other);
+  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.ax) * smith_g1(pbr_to_local(p.B, wi), p.ax);
+  return pscale(DoF, G);
+}
+// The specular lobe's pdf: transmission has zero probability, reflection probability 1 unless the
+// reflection coefficient is zero.
+__device__ __forceinline__ float pbr_spec_pdf(const PbrPrepared &p, float3 wi) {
+  const float idotn = pdot(p.B.n, p.wo), odotn = pdot(p.B.n, wi);
+  if (!(idotn * odotn > 0.0f)) return 0.0f;
+  const float3 h = pnormalize(padd(p.wo, wi));
+  const float idoth = pdot(p.wo, h), odoth = pdot(wi, h);
+  if (idoth * odoth < 0.0f) return 0.0f;
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  const float other = idoth / (4.0f * odoth * idotn);
+  const float rmax = pmax3(pbr_spec_coeff(p, fabsf(idoth)));
+  const float Fprob = psafe_div(rmax, rmax + 0.0f, 0.0f);
+  return smith_g1(pbr_to_local(p.B, p.wo), p.ax) * (Fprob * D * other);
+}
+__device__ __forceinline__ bool pbr_spec_sample(const PbrPrepared &p, float3 r, float3 &wi, float3 &w, float &pdf) {
+  const float idotn = pdot(p.wo, p.B.n);
+  const float3 hl = ggx_sample_vndf(p.ax, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y));
+  const float3 h = pbr_to_world(p.B, hl);
+  const float idoth = pdot(p.wo, h);
+  if (idoth < 0.0f) return false;
+  const float3 Fr = pbr_spec_coeff(p, idoth);
+  const float rmax = pmax3(Fr);
+  const float Prefl = psafe_div(rmax, rmax + 0.0f, 0.0f);
+  if (Prefl + 0.0f == 0.0f) return false;
+  wi = pnormalize(padd(pscale(p.wo, -1.0f), pscale(h, 2.0f * idoth)));
+  const float odotn = pdot(p.B.n, wi);
+  if (idotn * odotn <= 0.0f) return false;
+  const float odoth = pdot(wi, h);
+  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.ax);
+  w = pscale(pscale(Fr, 1.0f / Prefl), Gs);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  if (D <= 0.0f) return false;
+  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.ax);
+  pdf = Prefl * D * Gm * idoth / (4.0f * odoth * idotn);
+  return true;
+}
+
+// Metal multiple scattering: a cosine-weighted lobe restoring the energy single scattering loses.
+__device__ __forceinline__ float pbr_metal_factor(const PbrPrepared &p, const PbrTables &T, float odotn) {
+  const float f = p.metalEc * pbr_metal_energy(T, p.alpha, odotn) / fmaxf(pbr_metal_average(T, p.alpha), 1e-12f);
+  return fminf(f, psafe_div(1.0f, odotn, 0.0f));
+}
+__device__ __forceinline__ float3 pbr_metal_value(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  if (p.alpha < kPbrMinAlphaEnergyLoss) return pf3(0.0f, 0.0f, 0.0f);
+  const float odotn = pdot(wi, p.B.n);
+  if (!(odotn > 0.0f)) return pf3(0.0f, 0.0f, 0.0f);
+  return pscale(p.metalScale, pbr_metal_factor(p, T, odotn) * kPbrRcpPi * odotn);
+}
+__device__ __forceinline__ float pbr_metal_pdf(const PbrPrepared &p, float3 wi) {
+  if (p.alpha < kPbrMinAlphaEnergyLoss) return 0.0f;
+  return pdot(wi, p.B.n) > 0.0f ? kPbrRcpTwoPi : 0.0f;
+}
+__device__ __forceinline__ bool pbr_metal_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w,
+                                                 float &pdf) {
+  if (p.alpha < kPbrMinAlphaEnergyLoss) return false;
+  const float z = r.x, horizontal = sqrtf(1.0f - psq(z)), az = kPbrTwoPi * r.y;
+  wi = pbr_to_world(pbr_basis(p.B.n), pf3(cosf(az) * horizontal, sinf(az) * horizontal, z));
+  const float odotn = pdot(wi, p.B.n);
+  w = pscale(p.metalScale, 2.0f * odotn * pbr_metal_factor(p, T, odotn));
+  pdf = kPbrRcpTwoPi;
+  return true;
+}
+
+// EON diffuse (Fujii-Oren-Nayar with the approximate albedo), scaled by the opaque specular's
+// energy complement at the light (openpbr_diffuse_lobe.h).
+__device__ __forceinline__ float pbr_e_fon(float mu, float r) {
+  const float mc = 1.0f - mu;
+  const float g = mc * (0.0571085289f + mc * (0.491881867f + mc * (-0.332181442f + mc * 0.0714429953f)));
+  return (1.0f + r * g) / (1.0f + (0.5f - 2.0f / (3.0f * kPbrPi)) * r);
+}
+__device__ __forceinline__ float3 pbr_diffuse_local(const PbrPrepared &p, const PbrTables &T, float3 vi, float3 vo) {
+  const float A = 0.5f - 2.0f / (3.0f * kPbrPi), Bc = 2.0f / 3.0f - 28.0f / (15.0f * kPbrPi);
+  const float r = p.diffRough, mui = vi.z, muo = vo.z;
+  const float s = pdot(vi, vo) - mui * muo;
+  const float sot = s > 0.0f ? s / fmaxf(mui, muo) : s;
+  const float AF = 1.0f / (1.0f + A * r);
+  const float3 rho = p.diffAlbedo;
+  const float ks = 1.0f + r * sot;
+  const float3 fss = pf3(rho.x * kPbrRcpPi * AF * ks, rho.y * kPbrRcpPi * AF * ks, rho.z * kPbrRcpPi * AF * ks);
+  const float EFo = pbr_e_fon(muo, r), EFi = pbr_e_fon(mui, r);
+  const float avg = AF * (1.0f + Bc * r);
+  const float mo = fmaxf(1e-7f, 1.0f - EFo), mi = fmaxf(1e-7f, 1.0f - EFi), ma = fmaxf(1e-7f, 1.0f - avg);
+  const float3 rms = pf3(rho.x * rho.x * avg / (1.0f - rho.x * (1.0f - avg)), rho.y * rho.y * avg / (1.0f - rho.y * (1.0f - avg)),
+                         rho.z * rho.z * avg / (1.0f - rho.z * (1.0f - avg)));
+  const float3 fms = pf3(rms.x * kPbrRcpPi * mo * mi / ma, rms.y * kPbrRcpPi * mo * mi / ma, rms.z * kPbrRcpPi * mo * mi / ma);
+  const float comp = p.diffComp * pbr_opaque_energy(T, p.etaOpaque, p.alpha, muo);
+  return pscale(padd(fss, fms), comp);
+}
+__device__ __forceinline__ float3 pbr_diffuse_value(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  const float co = pdot(wi, p.B.n);
+  if (co <= 0.0f) return pf3(0.0f, 0.0f, 0.0f);
+  const PbrBasis b = pbr_basis(p.B.n);
+  return pscale(pbr_diffuse_local(p, T, pbr_to_local(b, p.wo), pbr_to_local(b, wi)), co);
+}
+__device__ __forceinline__ float pbr_diffuse_pdf(const PbrPrepared &p, float3 wi) { return fmaxf(pdot(wi, p.B.n), 0.0f) * kPbrRcpPi; }
+__device__ __forceinline__ bool pbr_diffuse_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w,
+                                                   float &pdf) {
+  const float phi = kPbrTwoPi * r.x, z = sqrtf(r.y), rr = sqrtf(1.0f - r.y);
+  const float3 lo = pf3(cosf(phi) * rr, sinf(phi) * rr, z);
+  if (lo.z == 0.0f) return false;
+  const PbrBasis b = pbr_basis(p.B.n);
+  wi = pbr_to_world(b, lo);
+  w = pscale(pbr_diffuse_local(p, T, pbr_to_local(b, p.wo), lo), kPbrPi);
+  pdf = lo.z * kPbrRcpPi;
+  return true;
+}
+
+// The aggregate: f |cos| and the lobe-weighted pdf.
+__device__ __forceinline__ float3 pbr_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  float3 v = pbr_spec_value(p, wi);
+  v = padd(v, pbr_metal_value(p, T, wi));
+  v = padd(v, pbr_diffuse_value(p, T, wi));
+  return v;
+}
+__device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, float3 wi) {
+  float sum = p.wSpec * pbr_spec_pdf(p, wi);
+  sum += p.wMetal * pbr_metal_pdf(p, wi);
+  sum += p.wDiff * pbr_diffuse_pdf(p, wi);
+  return p.total > 0.0f ? sum / p.total : 0.0f;
+}
+// One sample from three numbers: direction, weight f |cos| / pdf and pdf; false when none.
+__device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w, float &pdf) {
+  if (p.total <= kPbrFloatMin) return false;
+  float rx = r.x * p.total;
+  int lobe;
+  float sel;
+  if (rx < p.wSpec) {
+    lobe = 0; sel = p.wSpec; rx = rx / sel;
+  } else if (rx < p.wSpec + 0.0f + p.wMetal) {
+    lobe = 2; sel = p.wMetal; rx = (rx - (p.wSpec + 0.0f)) / sel;
+  } else {
+    lobe = 3; sel = p.wDiff; rx = (rx - ((p.wSpec + 0.0f) + p.wMetal)) / sel;
+  }
+  rx = pclamp_rand(rx);
+  const float3 rr = pf3(rx, r.y, r.z);
+  float3 lw;
+  float lp;
+  bool ok;
+  if (lobe == 0) ok = pbr_spec_sample(p, rr, wi, lw, lp);
+  else if (lobe == 2) ok = pbr_metal_sample(p, T, rr, wi, lw, lp);
+  else ok = pbr_diffuse_sample(p, T, rr, wi, lw, lp);
+  if (!ok) return false;
+  float3 fc = pscale(lw, lp);
+  float q = lp * sel;
+  if (lobe != 0) {
+    fc = padd(fc, pbr_spec_value(p, wi));
+    q += p.wSpec * pbr_spec_pdf(p, wi);
+  }
+  if (lobe != 2) {
+    fc = padd(fc, pbr_metal_value(p, T, wi));
+    q += p.wMetal * pbr_metal_pdf(p, wi);
+  }
+  if (lobe != 3) {
+    fc = padd(fc, pbr_diffuse_value(p, T, wi));
+    q += p.wDiff * pbr_diffuse_pdf(p, wi);
+  }
+  q /= p.total;
+  w = pscale(fc, 1.0f / q);
+  // The coat and fuzz layers (presence 0) recompute the weight from f |cos| and the pdf.
+  w = pscale(pscale(w, q), 1.0f / q);
+  w = pscale(pscale(w, q), 1.0f / q);
+  pdf = q;
+  return true;
+}
+
+}  // namespace vtd
+
+namespace vtd {
+// The tables inside one allocation: metal table, metal averages, opaque table, opaque averages.
+inline PbrTables pbr_tables_at(const float *base) {
+  PbrTables T;
+  T.metalE = base;
+  T.metalAvg = base + kMetalEnergyN * kMetalEnergyN;
+  T.opaqueE = T.metalAvg + kMetalEnergyN;
+  T.opaqueAvg = T.opaqueE + kPbrTable * kPbrTable * kPbrTable;
+  return T;
+}
+}  // namespace vtd

@@ -30,6 +30,7 @@
 
 #include "sampler.cuh"
 #include "spectral.cuh"
+#include "openpbr.cuh"
 #include "trace_common.cuh"
 #include "vt_internal.cuh"
 
@@ -55,6 +56,8 @@ struct RenderArgs {
   const float4 *slotL;     // per slot: the albedo's uplift multipliers (L0, L1, L2, flag)
   const float *cosPhase;   // per bin: cos of the warped phase
   const float4 *ebasis;    // per bin: the emission basis (R, G, B, 0), (C, M, Y, 0)
+  const float4 *pbr;       // per slot: OPENPBR roughness, metalness, IOR, diffuse roughness
+  PbrTables pbrT;          // OpenPBR energy tables
   uint32_t nbins, segments;
   float lambdaMin;
   int spectral;
@@ -634,15 +637,79 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
   return A.spectral ? fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)) : fmaxf(fmaxf(a.x, a.y), a.z);
 }
 
+// ---- OpenPBR vertices (openpbr.cuh) --------------------------------------------------------------
+// prepare_bsdf (main.swift:2547-2568): RGB transport evaluates the base colour's three channels; in
+// spectral transport `a` takes the reflectance at lanes 0-2 and `b` lane 3, skipped for a flat
+// (grey) base where lane 3 equals lane 0. Sampling, lobe choice and pdfs are those of `a`.
+__device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_material &m, float3 base) {
+  const float4 q = __ldg(A.pbr + __float_as_uint(m.pad));
+  PbrParams P;
+  P.base = make_float3(psat(base.x), psat(base.y), psat(base.z));
+  P.rough = fmaxf(0.03f, q.x);
+  P.metal = q.y;
+  P.ior = fmaxf(1.01f, q.z);
+  P.sw = 1.0f;
+  P.diffRough = q.w;
+  return P;
+}
+__device__ __forceinline__ bool is_pbr(const RenderArgs &A, const vt_material &m) {
+  return m.type == VT_MAT_OPENPBR && A.pbr && __float_as_uint(m.pad) < A.nmat;
+}
+// eval_bsdf_with_pdf (main.swift:2695-2706) at an OPENPBR vertex: f (without the cosine) per lane
+// and the pdf of `a`.
+__device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 wo,
+                                 float3 wi, float &pdf) {
+  pdf = 0.0f;
+  const float cosine = fabsf(dot3(n, wi));
+  if (cosine < 1e-7f || dot3(n, wo) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float4 rho = reflectance(A, L, m);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z)), A.pbrT, n, wo);
+  pdf = pbr_pdf(a, wi);
+  if (dot3(wi, gn) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float3 fa = pbr_eval(a, A.pbrT, wi);
+  float f3w = fa.x;
+  if (A.spectral && rho.w != rho.x) {
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w)), A.pbrT, n, wo);
+    f3w = pbr_eval(b, A.pbrT, wi).x;
+  }
+  return make_float4(fa.x / cosine, fa.y / cosine, fa.z / cosine, A.spectral ? f3w / cosine : 0.0f);
+}
+// sample_bsdf (main.swift:3359-3366) at an OPENPBR vertex: direction, weight f |cos| / pdf per lane.
+__device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 wo,
+                                 float3 r, float3 &dir, float4 &weight, float &pdf) {
+  const float4 rho = reflectance(A, L, m);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z)), A.pbrT, n, wo);
+  float3 w;
+  if (!pbr_sample(a, A.pbrT, r, dir, w, pdf) || !(pdf > 0.0f)) return false;
+  if (dot3(dir, gn) <= 0.0f) return false;
+  float w3 = w.x;
+  if (A.spectral && rho.w != rho.x) {
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w)), A.pbrT, n, wo);
+    w3 = pbr_eval(b, A.pbrT, dir).x / pdf;
+  }
+  weight = make_float4(w.x, w.y, w.z, A.spectral ? w3 : 0.0f);
+  return isfinite(weight.x) && isfinite(weight.y) && isfinite(weight.z) && isfinite(weight.w) && weight.x >= 0.0f &&
+         weight.y >= 0.0f && weight.z >= 0.0f && weight.w >= 0.0f;
+}
+
 // NEE at a Lambert vertex: the contribution's rgb (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
-                                               float err, float3 wo, float4 T, float4 albedo, bool useMIS,
+                                               float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                Sampler &seed, int *stack, bool requirePdf) {
   const LightSample ls = sample_direct(A, p, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
   if (!light_visible(A, p, gn, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
   const float cosine = fabsf(dot3(n, ls.wi));
+  if (is_pbr(A, m)) {
+    float bpdf;
+    const float4 f = pbr_eval_lanes(A, L, m, n, gn, wo, ls.wi, bpdf);
+    const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
+    const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
+    const float4 s = scale4(mul4(mul4(T, f), emission(A, L, le)), cosine * weight / ls.pdf);
+    return to_rgb(A, L, s);
+  }
+  const float4 albedo = reflectance(A, L, m);
   // eval_bsdf / eval_bsdf_pdf for DIFFUSE (main.swift:2659-2676): no light below the geometric
   // surface; cosine, f and pdf from the shading normal.
   float f = 0.0f, bpdf = 0.0f;
@@ -694,8 +761,13 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
   if (cos_th <= 0.0f) return f3(0.0f, 0.0f, 0.0f);
   Lanes L;
   if (A.spectral) L = make_lanes(A, c.u);
-  const float f = lambert_f(n, gn, mul(view, -1.0f), dir);
   const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
+  if (is_pbr(A, m)) {
+    float pdf;
+    const float4 f = pbr_eval_lanes(A, L, m, n, gn, mul(view, -1.0f), dir, pdf);
+    return mul(to_rgb(A, L, scale4(mul4(f, emission(A, L, e)), cos_th)), light_geometry(A, p, c));
+  }
+  const float f = lambert_f(n, gn, mul(view, -1.0f), dir);
   const float4 s = scale4(mul4(reflectance(A, L, m), emission(A, L, e)), f * cos_th);
   return mul(to_rgb(A, L, s), light_geometry(A, p, c));
 }
@@ -814,10 +886,18 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     // sample_bsdf, Lambert: one 3D draw (three PCG draws), the direction from the last two.
     sampler_event(seed, (uint32_t)bounce, kZBsdf);
     const float3 r = rand_f3(seed);
-    const float3 nd = cosine_hemisphere(S.n, r.y, r.z);
-    const float bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
-    if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
-    T = mul4(T, reflectance(A, L, m));
+    float3 nd;
+    float bpdf;
+    if (is_pbr(A, m)) {  // the prepared OpenPBR sample, from all three numbers
+      float4 w;
+      if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+      T = mul4(T, w);
+    } else {
+      nd = cosine_hemisphere(S.n, r.y, r.z);
+      bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+      if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
+      T = mul4(T, reflectance(A, L, m));
+    }
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
     const float3 prev = S.pos;
     const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
@@ -837,7 +917,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     if (emissionOnly) break;
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, reflectance(A, L, m), mis && scattering < limit,
+      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -870,7 +950,7 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, reflectance(A, L, m), A.mode == 1u && limit > 0, seed,
+    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
   R = add(R, continue_path(A, L, S, m, dir0, seed, stack, false));
@@ -907,7 +987,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
   A.gNrm[i] = gn;
   A.gGeo[i] = make_float4(S.gn.x, S.gn.y, S.gn.z, 0.0f);
   A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
-  if (m.type != VT_MAT_DIFFUSE) {
+  if (m.type != VT_MAT_DIFFUSE && !is_pbr(A, m)) {
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
     return;
   }
@@ -1241,6 +1321,7 @@ vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *mate
 }
 
 void scene_free(vt_scene *scene) {
+  cudaFree(scene->d_pbr);
   cudaFree(scene->d_slotL);
   cudaFree(scene->d_cosphase);
   cudaFree(scene->d_ebasis);
@@ -1518,6 +1599,8 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.spec = scene->d_spec;
   A.icdf = scene->d_icdf;
   A.slotL = scene->d_slotL;
+  A.pbr = scene->d_pbr;
+  if (scene->pbr_tables) A.pbrT = pbr_tables_at(scene->pbr_tables);
   A.cosPhase = scene->d_cosphase;
   A.ebasis = scene->d_ebasis;
   A.nbins = scene->nbins;
@@ -1839,6 +1922,27 @@ vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *b) {
   if (ctx) cudaSetDevice(ctx->device);
   cudaDeviceSynchronize();
   batch_free(b);
+  return VT_OK;
+}
+
+vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || (!params && n)) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+  if (n != scene->nmat) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the scene's material slot count");
+  if (!ctx->pbr_opaque) return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables are not set (vt_openpbr_tables_set)");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  std::vector<float4> q(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const vt_openpbr_params &p = params[i];
+    if (!(p.roughness >= 0.0f && p.roughness <= 1.0f) || !(p.metalness >= 0.0f && p.metalness <= 1.0f) || !(p.ior > 0.0f) ||
+        !(p.diffuse_roughness >= 0.0f && p.diffuse_roughness <= 1.0f))
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": roughness, metalness and diffuse roughness "
+                                          "must lie in [0, 1] and the IOR be positive");
+    q[i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
+  }
+  if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, n * sizeof(float4)));
+  if (n) VT_CUDA(ctx, cudaMemcpy(scene->d_pbr, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+  scene->pbr_tables = ctx->d_pbr;
   return VT_OK;
 }
 

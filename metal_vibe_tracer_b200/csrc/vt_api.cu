@@ -141,6 +141,7 @@ vt_status vt_ctx_destroy(vt_ctx *ctx) {
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_fgrid);
+  cudaFree(ctx->d_pbr);
   cudaFree(ctx->d_gnodes);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);

@@ -39,6 +39,10 @@ struct vt_ctx {
   uint32_t fgrid_flagged = 0;      // cells flagged (before the capacity cap)
   double fgrid_residual = 0.0;     // largest linear-sRGB residual of the coarse solves
   std::vector<double> fgrid_model; // weights and cos phase it was solved with
+  // OpenPBR energy tables (openpbr.cu): the dense metal table (129 x 129) and its averages (129),
+  // then the opaque-dielectric energy complement (32^3) and its average (32^2), as floats.
+  float *d_pbr = nullptr;
+  bool pbr_opaque = false;         // the opaque-dielectric tables are set
 };
 
 // Traversal copy of a 4-wide node with 8-bit child boxes (qnode.cu): 64 bytes, two 32-byte loads.
@@ -104,6 +108,10 @@ struct vt_scene {
   // reservoir (sample position, emission and pdf, weights) for this frame and the previous one,
   // plus the primary hit's face/slot/error and geometric normal: 12 float4 per pixel in one
   // allocation.
+  // OpenPBR slots (vt_scene_set_openpbr): per slot (roughness, metalness, IOR, diffuse roughness),
+  // and the context's energy tables.
+  float4 *d_pbr = nullptr;
+  const float *pbr_tables = nullptr;
   // Spectral uplift: per slot the albedo's multipliers, per bin the phase and the emission basis.
   float4 *d_slotL = nullptr;
   float *d_cosphase = nullptr;
@@ -123,6 +131,9 @@ vt_status vt_fail(vt_ctx *ctx, vt_status code, const std::string &msg);
 vt_status vt_uplift_ensure(vt_ctx *ctx, const vt_spectral_tables *tables);
 vt_status vt_uplift_colours(vt_ctx *ctx, const float *rgb, uint32_t n, float4 *out_dev);
 vt_status vt_uplift_basis(vt_ctx *ctx, const float *cosPhase_dev, uint32_t nbins, float4 *basis_dev);
+// OpenPBR (openpbr.cu): solve the metal energy table once per context and, with `tables`, set the
+// opaque-dielectric tables.
+vt_status vt_openpbr_ensure(vt_ctx *ctx, const vt_openpbr_tables *tables);
 vt_status vt_cuda_fail(vt_ctx *ctx, cudaError_t err, const char *what);
 
 #define VT_CUDA(ctx, call)                                   \

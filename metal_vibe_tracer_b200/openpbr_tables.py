@@ -1,0 +1,52 @@
+"""OpenPBR energy-compensation data: the opaque-dielectric energy complement tables of the Adobe
+openpbr-bsdf library the reference vendors (Vendor/OpenPBR/impl/data, Apache-2.0), which the
+diffuse base lobe uses (impl/openpbr_diffuse_lobe.h).
+
+They are library data, not part of this repository: `generate()` reads them at build time from the
+reference's vendored headers (32^3 and 32^2 unorm16 values) and writes
+`data/openpbr_energy.bin` (git-ignored, shipped with the built library); `load()` reads that file
+at run time and `set_tables(ctx)` hands them to the device. The dense metal table the reference
+substitutes for the library's (Shaders/MetalEnergy.metal) is solved on the device instead
+(vt_openpbr_energy_table).
+"""
+from __future__ import annotations
+
+import re
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+DATA = PKG / "data" / "openpbr_energy.bin"
+REFERENCE_DATA = Path("/root/reference/Vendor/OpenPBR/impl/data")
+MAGIC = b"VTPBR001"
+N = 32
+
+
+def _read_values(path: Path) -> np.ndarray:
+    text = "\n".join(line for line in path.read_text().splitlines() if not line.lstrip().startswith("//"))
+    return np.array([int(v) for v in re.findall(r"\d+", text)], np.uint16)
+
+
+def generate(data_dir: Path = REFERENCE_DATA) -> Path:
+    energy = _read_values(data_dir / "openpbr_opaque_dielectric_energy_complement_data.h")
+    average = _read_values(data_dir / "openpbr_opaque_dielectric_avg_energy_complement_data.h")
+    if energy.size != N ** 3 or average.size != N ** 2:
+        raise RuntimeError(f"unexpected OpenPBR table sizes {energy.size}, {average.size}")
+    DATA.parent.mkdir(parents=True, exist_ok=True)
+    tmp = DATA.with_suffix(".tmp")
+    tmp.write_bytes(MAGIC + energy.tobytes() + average.tobytes())
+    tmp.replace(DATA)
+    return DATA
+
+
+def load() -> dict:
+    if not DATA.exists():
+        raise RuntimeError(f"{DATA} is missing: it is generated at build time from the reference's vendored "
+                           "OpenPBR data (metal_vibe_tracer_b200.openpbr_tables.generate)")
+    b = DATA.read_bytes()
+    if b[:8] != MAGIC:
+        raise RuntimeError(f"{DATA}: bad header")
+    energy = np.frombuffer(b, np.uint16, N ** 3, 8).copy()
+    average = np.frombuffer(b, np.uint16, N ** 2, 8 + 2 * N ** 3).copy()
+    return {"opaque_energy": energy, "opaque_average": average}

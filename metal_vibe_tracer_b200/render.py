@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from .accel import Context, MaterialLibraryError, Mesh, _check
 
-VT_MAT_DIFFUSE, VT_MAT_EMISSIVE = 0, 3
+VT_MAT_DIFFUSE, VT_MAT_EMISSIVE, VT_MAT_OPENPBR = 0, 3, 4
 
 
 class Material(C.Structure):
@@ -125,6 +125,17 @@ class Scene:
             _check(ctx.handle, st, "vt_scene_create")
         self._p = p
         self.width = self.height = 0
+        if any(int(m["type"]) == VT_MAT_OPENPBR for m in materials):
+            # OPENPBR slots: roughness, metalness, IOR and diffuse roughness per slot (the reference's
+            # SurfaceSettings surface.x/y and detail.y; base colour is the albedo).
+            openpbr_tables_set(ctx)
+            params = (_lib.OpenPBRParams * len(materials))()
+            for i, m in enumerate(materials):
+                params[i].roughness = float(m.get("roughness", 0.5))
+                params[i].metalness = float(m.get("metalness", 0.0))
+                params[i].ior = float(m.get("ior", 1.5))
+                params[i].diffuse_roughness = float(m.get("diffuse_roughness", 0.0))
+            _check(ctx.handle, lib.vt_scene_set_openpbr(ctx.handle, self._p, params, len(materials)), "vt_scene_set_openpbr")
 
     def emitter_words(self) -> np.ndarray:
         """The packed emitter list of an imported scene (uint32 words)."""
@@ -278,3 +289,36 @@ def spectral_round_trip(ctx: Context) -> tuple[float, int]:
     _check(ctx.handle, _lib.load().vt_spectral_round_trip(ctx.handle, C.byref(worst), C.byref(over)),
            "vt_spectral_round_trip")
     return float(worst.value), int(over.value)
+
+
+# ---- OpenPBR (openpbr.cu) ---------------------------------------------------------------------
+def openpbr_tables_set(ctx: Context) -> None:
+    """Hand the context the OpenPBR energy tables (once; data/openpbr_energy.bin)."""
+    if getattr(ctx, "_pbr_tables_set", False):
+        return
+    from . import openpbr_tables
+    t = openpbr_tables.load()
+    e, a = t["opaque_energy"], t["opaque_average"]
+    s = _lib.OpenPBRTables(e.ctypes.data, a.ctypes.data)
+    _check(ctx.handle, _lib.load().vt_openpbr_tables_set(ctx.handle, C.byref(s)), "vt_openpbr_tables_set")
+    ctx._pbr_tables_set = True
+
+
+def openpbr_energy_table(ctx: Context) -> tuple[np.ndarray, np.ndarray]:
+    """The dense GGX energy complement solved on the device: (129, 129) and (129,)."""
+    table = np.empty((129, 129), np.float32)
+    avg = np.empty(129, np.float32)
+    _check(ctx.handle, _lib.load().vt_openpbr_energy_table(ctx.handle, table.ctypes.data, avg.ctypes.data),
+           "vt_openpbr_energy_table")
+    return table, avg
+
+
+def openpbr_evaluate(ctx: Context, cases) -> np.ndarray:
+    """BSDF queries on the device: `cases` is a structured array of _lib.OpenPBRCase fields or an
+    (n, 20) float32 array in that order; returns (n, 12) float32 results (f_cos, pdf, dir, weight,
+    sample_pdf, ok)."""
+    arr = np.ascontiguousarray(cases, np.float32).reshape(-1, 20)
+    out = np.empty((arr.shape[0], 12), np.float32)
+    _check(ctx.handle, _lib.load().vt_openpbr_evaluate(ctx.handle, arr.ctypes.data, arr.shape[0], out.ctypes.data),
+           "vt_openpbr_evaluate")
+    return out

@@ -231,6 +231,21 @@ def cornell_coloured(seed: int = 0):
     return faces, verts, materials, light, camera
 
 
+def cornell_openpbr(seed: int = 0):
+    """The coloured Cornell box with OPENPBR slots (material type 4): glossy dielectric walls
+    (roughness 0.35, IOR 1.5), a rough gold-coloured metal tall box (roughness 0.3, metalness 1) and a
+    half-metallic short box (roughness 0.6, metalness 0.5); floor and ceiling stay Lambert."""
+    faces, verts, materials, light, camera = cornell_coloured(seed=seed)
+    def pbr(c, rough, metal, ior=1.5):
+        return {"type": 4, "albedo": c, "emission": (0.0, 0.0, 0.0), "roughness": rough, "metalness": metal, "ior": ior}
+    materials[2] = pbr((0.73, 0.73, 0.73), 0.35, 0.0)
+    materials[3] = pbr((0.63, 0.065, 0.05), 0.35, 0.0)
+    materials[4] = pbr((0.14, 0.45, 0.091), 0.35, 0.0, 1.4)
+    materials[5] = pbr((0.95, 0.75, 0.3), 0.3, 1.0)
+    materials[6] = pbr((0.1, 0.2, 0.7), 0.6, 0.5, 1.6)
+    return faces, verts, materials, light, camera
+
+
 def _mesh_from_triangles(tris, tags):
     n = len(tris)
     verts = np.zeros(3 * n, VERTEX_DTYPE)

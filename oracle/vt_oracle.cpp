@@ -1903,12 +1903,90 @@ bool visible_d(const PtContext &C, D3 p, D3 gn, double err, const PtLight &ls) {
 }
 
 // n: shading normal; gn: geometric normal (eval_bsdf for DIFFUSE, main.swift:2659-2676).
+// ---- OPENPBR vertices: the reference BSDF (float) through vto_pt_inputs ---------------------------
+bool pbr_slot(const PtContext &C, const vt_material &m) {
+  uint32_t slot;
+  std::memcpy(&slot, &m.pad, sizeof slot);
+  return m.type == 4 && C.in->pbr_params && C.in->pbr_eval && slot < C.in->nmat;
+}
+vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double b0, double b1, double b2) {
+  uint32_t slot;
+  std::memcpy(&slot, &m.pad, sizeof slot);
+  vto_pbr_material q;
+  std::memset(&q, 0, sizeof q);
+  q.type = 4;
+  q.albedo[0] = (float)b0;
+  q.albedo[1] = (float)b1;
+  q.albedo[2] = (float)b2;
+  const float *pp = C.in->pbr_params + 4 * (size_t)slot;
+  q.roughness = pp[0];
+  q.metalness = pp[1];
+  q.ior = pp[2];
+  return q;
+}
+// eval_bsdf_with_pdf (main.swift:2695-2706): f (no cosine) per lane, pdf of lanes 0-2.
+Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, D3 wi, double &pdf) {
+  pdf = 0.0;
+  const double cosine = std::fabs(dot(n, wi));
+  if (cosine < 1e-7 || dot(n, wo) <= 0.0) return {{0, 0, 0, 0}};
+  const Spec4 rho = reflectance(C, L, m);
+  const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
+              fi[3] = {(float)wi.x, (float)wi.y, (float)wi.z};
+  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  float f[3], q;
+  C.in->pbr_eval(&a, fn, fo, fi, nullptr, f, &q);
+  pdf = q;
+  if (dot(wi, gn) <= 0.0) return {{0, 0, 0, 0}};
+  double f3 = f[0];
+  if (C.spectral && rho.v[3] != rho.v[0]) {
+    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
+    float g[3], qb;
+    C.in->pbr_eval(&b, fn, fo, fi, nullptr, g, &qb);
+    f3 = g[0];
+  }
+  return {{f[0] / cosine, f[1] / cosine, f[2] / cosine, C.spectral ? f3 / cosine : 0.0}};
+}
+// sample_bsdf (main.swift:3359-3366): direction, f |cos| / pdf per lane, pdf.
+bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, const double r[3],
+                        D3 &dir, Spec4 &w, double &pdf) {
+  const Spec4 rho = reflectance(C, L, m);
+  const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
+              fr[3] = {(float)r[0], (float)r[1], (float)r[2]};
+  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  float d[3], ww[3], q;
+  int32_t lobe;
+  C.in->pbr_sample(&a, fn, fo, fr, nullptr, d, ww, &q, &lobe);
+  if (!(q > 0.0f)) return false;
+  dir = D3{d[0], d[1], d[2]};
+  if (dot(dir, gn) <= 0.0) return false;
+  pdf = q;
+  double w3 = ww[0];
+  if (C.spectral && rho.v[3] != rho.v[0]) {
+    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
+    float g[3], qb;
+    C.in->pbr_eval(&b, fn, fo, d, nullptr, g, &qb);
+    w3 = g[0] / q;
+  }
+  w = {{ww[0], ww[1], ww[2], C.spectral ? w3 : 0.0}};
+  for (double x : w.v)
+    if (!std::isfinite(x) || x < 0.0) return false;
+  return true;
+}
+
 D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
-            const Spec4 &albedo, bool useMIS, ZSampler &seed, bool requirePdf) {
+            const vt_material &m, bool useMIS, ZSampler &seed, bool requirePdf) {
   const PtLight ls = C.imported ? sample_emitters_d(C, p, seed) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
   if (!visible_d(C, p, gn, err, ls)) return {0, 0, 0};
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
+  if (pbr_slot(C, m)) {
+    double bpdf;
+    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, wo, ls.wi, bpdf);
+    const double w = useMIS ? power_heuristic_d(ls.pdf, bpdf) : 1.0;
+    const float le[3] = {(float)ls.emission.x, (float)ls.emission.y, (float)ls.emission.z};
+    return to_rgb(C, L, scale(mul(mul(T, f), emission(C, L, le)), cosine * w / ls.pdf));
+  }
+  const Spec4 albedo = reflectance(C, L, m);
   double f = 0.0, bpdf = 0.0;
   if (no > 0.0) {
     bpdf = std::max(0.0, ni) / kPi;
@@ -1954,7 +2032,7 @@ D3 primary_emission_d(const PtContext &C, const PtLanes &L, const PtHit &h, cons
 
 // The path after its primary vertex (shading_kernel's bounce loop, main.swift:7709-7833). With
 // diPrimary (sampling mode 0) a BSDF hit on an emitter from the primary vertex gets no weight.
-D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m, ZSampler &seed, bool diPrimary) {
+D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m, D3 dir, ZSampler &seed, bool diPrimary) {
   const int limit = std::max(0, (int)C.p->max_depth - 1);
   const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode <= 1u;
   Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
@@ -1971,14 +2049,24 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     seed.event((uint32_t)bounce, 0u);
     double r0, r1, r2;
     seed.f3(r0, r1, r2);
-    const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
-    const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
-    D3 bu, bv;
-    make_basis_d(h.n, bu, bv);
-    const D3 nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.n * cos_th);
-    const double bpdf = std::max(0.0, dot(h.n, nd)) / kPi;
-    if (!(bpdf > 0.0) || !(dot(nd, h.gn) > 0.0)) break;
-    T = mul(T, reflectance(C, L, m));
+    D3 nd;
+    double bpdf;
+    if (pbr_slot(C, m)) {
+      const double r[3] = {r0, r1, r2};
+      Spec4 w;
+      if (!pbr_sample_lanes_d(C, L, m, h.n, h.gn, dir * -1.0, r, nd, w, bpdf)) break;
+      T = mul(T, w);
+    } else {
+      const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
+      const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
+      D3 bu, bv;
+      make_basis_d(h.n, bu, bv);
+      nd = normalize(bu * (std::cos(phi) * sin_th) + bv * (std::sin(phi) * sin_th) + h.n * cos_th);
+      bpdf = std::max(0.0, dot(h.n, nd)) / kPi;
+      if (!(bpdf > 0.0) || !(dot(nd, h.gn) > 0.0)) break;
+      T = mul(T, reflectance(C, L, m));
+    }
+    dir = nd;
     bool finite = true;
     for (double t : T.v) finite = finite && std::isfinite(t);
     if (!finite || smax(C, T) <= 0.0) break;
@@ -1995,7 +2083,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     if (emissionOnly) break;
     if (nee) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, reflectance(C, L, m), mis && scattering < limit, seed,
+      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, seed,
                        false);
     }
     if (bounce > 3) {
@@ -2034,9 +2122,14 @@ D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_ma
   if (cos_th <= 0.0) return {0, 0, 0};
   PtLanes L{};
   if (C.spectral) L = make_lanes(C, c.u);
+  const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
+  if (pbr_slot(C, m)) {
+    double pdf;
+    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, view * -1.0, dir, pdf);
+    return to_rgb(C, L, scale(mul(f, emission(C, L, e)), cos_th)) * light_geometry_d(C, p, c);
+  }
   const double ni = dot(n, dir), no = -dot(n, view);
   const double f = no > 0.0 && ni > 0.0 && std::fabs(ni) >= 1e-7 && dot(dir, gn) > 0.0 ? 1.0 / kPi : 0.0;
-  const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
   return to_rgb(C, L, scale(mul(reflectance(C, L, m), emission(C, L, e)), f * cos_th)) * light_geometry_d(C, p, c);
 }
 
@@ -2103,7 +2196,7 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   const double pos[4] = {h.pos.x, h.pos.y, h.pos.z, h.t}, nrm[4] = {h.n.x, h.n.y, h.n.z, double(m.type)};
   std::memcpy(out.pos, pos, sizeof pos);
   std::memcpy(out.nrm, nrm, sizeof nrm);
-  if (m.type != VT_MAT_DIFFUSE) return;
+  if (m.type != VT_MAT_DIFFUSE && !pbr_slot(C, m)) return;
   out.s.u = u;
   for (uint32_t c = 0; c < M; ++c) {
     seed.candidate(1u, 4u, c, bits);
@@ -2164,7 +2257,7 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   D3 R{0, 0, 0};
   if (W > 0.0 && visible_d(C, h.pos, h.gn, h.err, light_from_di(sel, h.pos)))
     R = di_contribution_d(C, h.pos, h.n, h.gn, dir0, m, sel) * W;
-  R = R + continue_path_d(C, L, h, m, seed, true);
+  R = R + continue_path_d(C, L, h, m, dir0, seed, true);
   if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
   return R;
 }
@@ -2186,10 +2279,10 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (C.p->sampling_mode != 3u) {
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, reflectance(C, L, m), C.p->sampling_mode == 1u && limit > 0,
+    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0,
                  seed, true);
   }
-  R = R + continue_path_d(C, L, h, m, seed, false);
+  R = R + continue_path_d(C, L, h, m, dir0, seed, false);
   if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
   return R;
 }

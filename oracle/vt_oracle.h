@@ -77,6 +77,22 @@ void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t c
  * faces' tags select material slots, the procedural quad light (main.swift:2957-2978, 3046-3050)
  * and, when `spectral`, four hero wavelengths from the tables (main.swift:755-848, 945-959). All
  * arithmetic in double; random numbers are the reference's exact 24-bit PCG draws. */
+/* OpenPBR materials: the reference BSDF (oracle/openpbr_ref, compiled from the reference's vendored
+ * headers) called through these entry points; the material record mirrors its adapter's fields. */
+typedef struct vto_pbr_material {
+  int32_t type;
+  float albedo[3];
+  float roughness, metalness, ior, coat, anisotropy, fuzz, transmission;
+  float thin_film_weight, thin_film_thickness, thin_film_ior;
+  int32_t inside;
+  float tangent[3];
+  float pad;
+} vto_pbr_material;
+typedef void (*vto_pbr_eval_fn)(const vto_pbr_material *m, const float *n, const float *wo, const float *wi,
+                                const float *lambda, float *f_cos, float *pdf);
+typedef void (*vto_pbr_sample_fn)(const vto_pbr_material *m, const float *n, const float *wo, const float *rand,
+                                  const float *lambda, float *dir, float *weight, float *pdf, int32_t *lobe);
+
 typedef struct vto_pt_inputs {
   const vt_face *faces;
   uint32_t nfaces;
@@ -99,6 +115,10 @@ typedef struct vto_pt_inputs {
    * the warped phase at each of the nbins bins. Needed when spectral. */
   const struct vto_uplift *uplift;
   const float *cos_phase;
+  /* OPENPBR slots (type 4): per slot roughness, metalness, IOR, diffuse roughness, and the BSDF. */
+  const float *pbr_params;
+  vto_pbr_eval_fn pbr_eval;
+  vto_pbr_sample_fn pbr_sample;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

@@ -234,7 +234,8 @@ class PtInputs(C.Structure):
                 ("cmf_rgb", C.c_void_p), ("illum", C.c_void_p), ("icdf", C.c_void_p),
                 ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float),
                 ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32),
-                ("uplift", C.c_void_p), ("cos_phase", C.c_void_p)]
+                ("uplift", C.c_void_p), ("cos_phase", C.c_void_p),
+                ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -262,8 +263,18 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         for k in ("corner", "su", "sv", "normal", "emission"):
             getattr(q, k)[:] = [float(x) for x in light[k]]
     inp = PtInputs(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0], C.cast(mats, C.c_void_p), len(materials), q,
-                   None, None, None, 0, 0, 0.0, None, 0, 0, None, None)
+                   None, None, None, 0, 0, 0.0, None, 0, 0, None, None, None, None, None)
     keep = []
+    if any(int(m["type"]) == 4 for m in materials):
+        # OPENPBR slots: the reference's own BSDF (oracle/openpbr_ref).
+        from . import openpbr_ref
+        ref = openpbr_ref.load()
+        params = np.array([[float(m.get("roughness", 0.5)), float(m.get("metalness", 0.0)), float(m.get("ior", 1.5)),
+                            float(m.get("diffuse_roughness", 0.0))] for m in materials], np.float32)
+        keep.append(params)
+        inp.pbr_params = params.ctypes.data
+        inp.pbr_eval = C.cast(ref.ref_openpbr_eval, C.c_void_p).value
+        inp.pbr_sample = C.cast(ref.ref_openpbr_sample, C.c_void_p).value
     if light is None:
         if emitter_words is None:
             from . import light_tree as LT

@@ -1,0 +1,56 @@
+"""Writes tests/golden/openpbr_cases.json and tests/golden/metal_energy.json from the reference's
+own OpenPBR BSDF (oracle/_ref/libopenpbr_ref.so, compiled from the reference's vendored Adobe
+openpbr-bsdf headers and Shaders/MetalEnergy.metal by oracle/openpbr_ref/Makefile).
+
+Cases: seeded opaque OPENPBR materials (base colour uniform, metalness 0, 1 or uniform, roughness
+uniform in [0, 1] (the adapter clamps at 0.03), IOR uniform in [1.3, 1.8], specular weight 1),
+random unit shading normals, views mostly on the normal's side (some behind it), light directions
+uniform on the sphere and three uniform random numbers: each with the reference's f |cos| and pdf
+at the light direction and its sample (direction, weight, pdf). The metal table: every 8th node of
+the 129 x 129 table and all 129 averages.
+"""
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle import openpbr_ref as R  # noqa: E402
+
+
+def unit(v):
+    return v / np.linalg.norm(v)
+
+
+rng = np.random.default_rng(20261203)
+cases = []
+for i in range(600):
+    base = rng.random(3)
+    metal = [0.0, 1.0, float(rng.random())][i % 3]
+    rough = float(rng.random())
+    ior = float(1.3 + 0.5 * rng.random())
+    n = unit(rng.normal(size=3))
+    wo = unit(rng.normal(size=3))
+    if (np.dot(wo, n) < 0) != (i % 10 == 9):
+        wo = -wo
+    wi = unit(rng.normal(size=3))
+    if i % 4 != 3 and np.dot(wi, n) < 0:
+        wi = -wi
+    r = rng.random(3).astype(np.float32)
+    f32 = lambda x: [float(v) for v in np.asarray(x, np.float32)]
+    m = R.material(base, metal, rough, ior)
+    f, pdf = R.evaluate(m, f32(n), f32(wo), f32(wi))
+    d, w, spdf, lobe = R.sample(m, f32(n), f32(wo), f32(r))
+    cases.append({"base": f32(base), "metalness": metal, "roughness": rough, "ior": ior, "normal": f32(n), "view": f32(wo),
+                  "light": f32(wi), "rand": f32(r), "f_cos": f32(f), "pdf": float(pdf), "dir": f32(d), "weight": f32(w),
+                  "sample_pdf": float(spdf), "lobe": lobe})
+here = Path(__file__).resolve().parent
+(here / "openpbr_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF)",
+                                                     "cases": cases}) + "\n")
+t, a = R.metal_energy_table()
+(here / "metal_energy.json").write_text(json.dumps({"source": "Shaders/MetalEnergy.metal via oracle/_ref",
+                                                    "step": 8, "table": t[::8, ::8].astype(float).tolist(),
+                                                    "average": a.astype(float).tolist()}) + "\n")
+print("wrote", len(cases), "cases")
