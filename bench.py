@@ -313,9 +313,9 @@ def bench_batch(a, ctx) -> dict:
 
 def bench_production(a, ctx, stream) -> dict:
     """The production-scale scene: ~10M triangles of displaced icospheres, ~100k emissive triangles
-    under a light tree, 287 coloured material slots (Lambert; the OpenPBR lobes are not built), at
-    1920x1080, spectral (4 wavelengths), depth 12: ReSTIR DI with 32 candidates (temporal + spatial
-    reuse) and plain MIS path tracing. Device time per frame."""
+    under a light tree, 287 OPENPBR material slots (thin film left out), at 1920x1080, spectral
+    (4 wavelengths), depth 12: ReSTIR DI with 32 candidates (temporal + spatial reuse) and plain MIS
+    path tracing. Device time per frame."""
     import torch
 
     import metal_vibe_tracer_b200 as vt
@@ -334,8 +334,8 @@ def bench_production(a, ctx, stream) -> dict:
     cs = stream.cuda_stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"workload": "production grid scene: %d triangles (displaced subdivision-5 icospheres), %d emissive under a "
-                       "light tree, %d material slots (Lambert, coloured, spectral uplift), 1920x1080, 4 wavelengths, "
-                       "depth 12" % (len(faces), int((faces["tag"] >= 287).sum()), len(mats)),
+                       "light tree, %d material slots (OPENPBR: base colour, roughness, metalness, IOR; spectral uplift), "
+                       "1920x1080, 4 wavelengths, depth 12" % (len(faces), int((faces["tag"] >= 287).sum()), len(mats)),
            "triangles": int(len(faces)), "build_ms": info.build_ms, "scene_create_s": scene_s, "generate_s": gen_s}
     for name, mode, cand in (("restir_di_32", 0, 32), ("mis", 1, 0)):
         scene.reset()

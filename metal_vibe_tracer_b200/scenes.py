@@ -478,12 +478,18 @@ def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displac
 
 def production_scene(seed: int = 0, triangles: int = 10_000_000, emitters: int = 100_000, nmat: int = 287):
     """The production-scale grid scene: ~`triangles` triangles of displaced subdivision-5 icospheres
-    (20,480 triangles each), ~`emitters` emissive triangles (whole emissive spheres), `nmat` material
-    slots with base colours uniform in [0, 1]^3 (Lambert: the OpenPBR lobes are not built) and a
+    (20,480 triangles each), ~`emitters` emissive triangles (whole emissive spheres), `nmat` OPENPBR
+    slots (base colour uniform in [0, 1]^3, roughness uniform in [0, 1], metalness 1 with
+    probability 0.3 else 0, IOR uniform in [1.3, 1.8]; thin film is not supported and left out) and a
     camera over the grid. Returns faces, vertices, materials, camera."""
     spheres = max(1, round(triangles / 20480))
     every = max(1, round(spheres / max(1, round(emitters / 20480))))
-    return sphere_grid(triangles, seed=seed, emissive_every=every, nmat=nmat, coloured=True)
+    faces, verts, mats, camera = sphere_grid(triangles, seed=seed, emissive_every=every, nmat=nmat, coloured=True)
+    rng = np.random.default_rng(seed + 1)
+    for i in range(nmat):
+        mats[i] = dict(mats[i], type=4, roughness=float(rng.random()), metalness=1.0 if rng.random() < 0.3 else 0.0,
+                       ior=float(1.3 + 0.5 * rng.random()))
+    return faces, verts, mats, camera
 
 
 def batch_workload(count: int = 64, seed: int = 0, lo: int = 10_000, hi: int = 2_000_000):
