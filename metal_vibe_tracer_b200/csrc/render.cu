@@ -652,8 +652,11 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
   P.diffRough = q.w;
   return P;
 }
+// kPbr: the kernel variant for scenes with OPENPBR slots; scenes without them run a variant
+// compiled without the OpenPBR code, which keeps its register count (and occupancy) down.
+template <bool kPbr>
 __device__ __forceinline__ bool is_pbr(const RenderArgs &A, const vt_material &m) {
-  return m.type == VT_MAT_OPENPBR && A.pbr && __float_as_uint(m.pad) < A.nmat;
+  return kPbr && m.type == VT_MAT_OPENPBR && A.pbr && __float_as_uint(m.pad) < A.nmat;
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706) at an OPENPBR vertex: f (without the cosine) per lane
 // and the pdf of `a`.
@@ -694,6 +697,7 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 
 // NEE at a Lambert vertex: the contribution's rgb (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
+template <bool kPbr>
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                Sampler &seed, int *stack, bool requirePdf) {
@@ -701,7 +705,7 @@ __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes 
   if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
   if (!light_visible(A, p, gn, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
   const float cosine = fabsf(dot3(n, ls.wi));
-  if (is_pbr(A, m)) {
+  if (is_pbr<kPbr>(A, m)) {
     float bpdf;
     const float4 f = pbr_eval_lanes(A, L, m, n, gn, wo, ls.wi, bpdf);
     const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
@@ -754,6 +758,7 @@ __device__ __forceinline__ float lambert_f(float3 n, float3 gn, float3 wo, float
 
 // The sample's contribution at the shading point before its weight: bsdf * Le * cos * G, in the
 // sample's own wavelengths (u), as linear sRGB.
+template <bool kPbr>
 __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
                                                   const vt_material &m, const DISample &c) {
   const float3 dir = normalize3(sub(c.pos, p));
@@ -762,7 +767,7 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
   Lanes L;
   if (A.spectral) L = make_lanes(A, c.u);
   const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
-  if (is_pbr(A, m)) {
+  if (is_pbr<kPbr>(A, m)) {
     float pdf;
     const float4 f = pbr_eval_lanes(A, L, m, n, gn, mul(view, -1.0f), dir, pdf);
     return mul(to_rgb(A, L, scale4(mul4(f, emission(A, L, e)), cos_th)), light_geometry(A, p, c));
@@ -773,10 +778,11 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
 }
 
 // eval_restir_target_pdf (main.swift:3187-3197): the length of that contribution.
+template <bool kPbr>
 __device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
                                            const vt_material &m, const DISample &c) {
   if (c.pdf <= 0.0f) return 0.0f;
-  const float3 v = di_contribution(A, p, n, gn, view, m, c);
+  const float3 v = di_contribution<kPbr>(A, p, n, gn, view, m, c);
   return sqrtf(dot3(v, v));
 }
 
@@ -867,6 +873,7 @@ __device__ __forceinline__ float3 primary_emission(const RenderArgs &A, const La
 // Russian roulette. With diPrimary (sampling mode 0) the primary vertex's direct light came from its
 // ReSTIR DI reservoir, so a BSDF hit on an emitter from it gets no weight (previousMIS false,
 // main.swift:7717-7718).
+template <bool kPbr>
 __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
                                 Sampler &seed, int *stack, bool diPrimary) {
   const int limit = max(0, (int)A.maxDepth - 1);
@@ -888,7 +895,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     const float3 r = rand_f3(seed);
     float3 nd;
     float bpdf;
-    if (is_pbr(A, m)) {  // the prepared OpenPBR sample, from all three numbers
+    if (is_pbr<kPbr>(A, m)) {  // the prepared OpenPBR sample, from all three numbers
       float4 w;
       if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
       T = mul4(T, w);
@@ -917,7 +924,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     if (emissionOnly) break;
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
+      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -931,6 +938,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
 }
 
 // One path of sampling modes 1-3: camera ray, primary hit, NEE there, then the continuation.
+template <bool kPbr>
 __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
                               int *stack) {
   Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
@@ -950,10 +958,10 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
-  R = add(R, continue_path(A, L, S, m, dir0, seed, stack, false));
+  R = add(R, continue_path<kPbr>(A, L, S, m, dir0, seed, stack, false));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
 }
@@ -963,7 +971,8 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
 // candidates, restir_di_initial, main.swift:4638-4668), merged with the previous frame's reservoir
 // of the backprojected pixel when it saw the same surface (restir_di_merge, main.swift:4686-4699,
 // confidence capped at 20), stored with W = wsum / (M p_hat) (restir_di_encode).
-__global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint32_t k) {
+template <bool kPbr>
+__global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(RenderArgs A, uint32_t k) {
   int stack[kRenderStack];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.W * A.H) return;
@@ -987,7 +996,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
   A.gNrm[i] = gn;
   A.gGeo[i] = make_float4(S.gn.x, S.gn.y, S.gn.z, 0.0f);
   A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
-  if (m.type != VT_MAT_DIFFUSE && !is_pbr(A, m)) {
+  if (m.type != VT_MAT_DIFFUSE && !is_pbr<kPbr>(A, m)) {
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
     return;
   }
@@ -1004,7 +1013,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
     DISample cand;
     cand.pos = ls.pos; cand.emission = ls.emission; cand.pdf = ls.pdf; cand.u = u;
     cand.id = ls.face == 0xffffffffu ? 0u : ls.face + 2u;
-    const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, cand);
+    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, cand);
     const float proposal = cand.pdf * light_geometry(A, S.pos, cand);
     const float w = proposal > 0.0f ? pHat / proposal : 0.0f;
     r.wsum += w;
@@ -1017,13 +1026,13 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
     if (same_surface(gp, gn, A.hPos[j], A.hNrm[j]) && hw.y > 0.0f && hw.z > 0.0f) {
       const DISample hs = load_di(A.hrPos, A.hrEmit, A.hrW, j);
       const float cM = fminf(hw.y, 20.0f);
-      const float w = di_target(A, S.pos, S.n, S.gn, dir0, m, hs) * hw.z * cM;
+      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, hs) * hw.z * cM;
       r.M += cM;
       r.wsum += w;
       if (rand_decision(seed) * r.wsum < w) r.s = hs;
     }
   }
-  const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, r.s);
+  const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, r.s);
   const float W = r.M > 0.0f && pHat > 0.0f ? r.wsum / (r.M * pHat) : 0.0f;
   A.rPos[i] = make_float4(r.s.pos.x, r.s.pos.y, r.s.pos.z, __uint_as_float(r.s.id));
   A.rEmit[i] = make_float4(r.s.emission.x, r.s.emission.y, r.s.emission.z, r.s.pdf);
@@ -1034,7 +1043,8 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_primary(RenderArgs A, uint3
 // taps in a 32-pixel box that pass RESTIR2020's compatibility test (uniform_neighbor, main.swift:
 // 5025-5027), the selected sample's contribution W * bsdf * Le * cos * G when visible, then the
 // path's continuation (MIS at later vertices). The sample is added to the FP64 accumulation.
-__global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_t k) {
+template <bool kPbr>
+__global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderArgs A, uint32_t k) {
   int stack[kRenderStack];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.W * A.H) return;
@@ -1065,7 +1075,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
   } else {
     const float4 cw = A.rW[i];
     DISample sel = load_di(A.rPos, A.rEmit, A.rW, i);
-    float wsum = di_target(A, S.pos, S.n, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
+    float wsum = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
     for (int t = 0; t < 4; ++t) {
       const float ox = pcg_rand(seed.state), oy = pcg_rand(seed.state);
       const int nx = (int)x + (int)((ox * 2.0f - 1.0f) * 16.0f), ny = (int)y + (int)((oy * 2.0f - 1.0f) * 16.0f);
@@ -1075,17 +1085,17 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
       const float4 nw = A.rW[j];
       if (!(nw.y > 0.0f && nw.z > 0.0f)) continue;
       const DISample ns = load_di(A.rPos, A.rEmit, A.rW, j);
-      const float w = di_target(A, S.pos, S.n, S.gn, dir0, m, ns) * nw.z * nw.y;
+      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, ns) * nw.z * nw.y;
       wsum += w;
       M += nw.y;
       if (rand_decision(seed) * wsum < w) sel = ns;
     }
-    const float pHat = di_target(A, S.pos, S.n, S.gn, dir0, m, sel);
+    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel);
     const float W = M > 0.0f && pHat > 0.0f ? wsum / (M * pHat) : 0.0f;
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
-      R = mul(di_contribution(A, S.pos, S.n, S.gn, dir0, m, sel), W);
-    R = add(R, continue_path(A, L, S, m, dir0, seed, stack, true));
+      R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel), W);
+    R = add(R, continue_path<kPbr>(A, L, S, m, dir0, seed, stack, true));
   }
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) return;
   double *acc = A.accum + 3 * (size_t)i;
@@ -1095,7 +1105,8 @@ __global__ void __launch_bounds__(kRenderBlock) k_di_shade(RenderArgs A, uint32_
 // Work item i = (sample group g, pixel p), pixel-major within a group so that a warp traces
 // neighbouring pixels; a group covers `per` consecutive samples of the call. Each item adds its
 // FP64 sum to the pixel with one atomic per channel (groups > 1) or a plain add (groups = 1).
-__global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t groups, uint32_t per) {
+template <bool kPbr>
+__global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArgs A, uint32_t groups, uint32_t per) {
   int stack[kRenderStack];
   const uint32_t npix = A.W * A.H;
   const uint64_t items = (uint64_t)npix * groups;
@@ -1105,7 +1116,7 @@ __global__ void __launch_bounds__(kRenderBlock) k_render(RenderArgs A, uint32_t 
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
-      const float3 c = path_sample(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack);
+      const float3 c = path_sample<kPbr>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack);
       sr += c.x;
       sg += c.y;
       sb += c.z;
@@ -1144,6 +1155,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Items are (scene, pixel), each running all of the pass's samples of its pixel. Warps take 32 x chunk
 // consecutive items with one atomic; a scene's last finished item stamps its completion time.
+template <bool kPbr>
 __global__ void __launch_bounds__(256) k_render_batch(const RenderArgs *__restrict__ scenes,
                                                       const unsigned long long *__restrict__ begin, uint32_t nscenes,
                                                       unsigned long long total, uint32_t chunk,
@@ -1172,7 +1184,7 @@ __global__ void __launch_bounds__(256) k_render_batch(const RenderArgs *__restri
       const uint32_t x = p % A.W, y = p / A.W, f0 = firstSample[lo], fr0 = firstFrame[lo];
       double sr = 0.0, sg = 0.0, sb = 0.0;
       for (uint32_t k = 0; k < A.spp; ++k) {
-        const float3 c = path_sample(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
+        const float3 c = path_sample<kPbr>(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
         sr += c.x; sg += c.y; sb += c.z;
       }
       double *acc = A.accum + 3 * (size_t)p;
@@ -1709,8 +1721,13 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
       A.pup = make_float3(pc[9], pc[10], pc[11]);
       A.paspect = pc[12];
       A.pfovScale = pc[13];
-      k_di_primary<<<blocks, kRenderBlock, 0, s>>>(A, k);
-      k_di_shade<<<blocks, kRenderBlock, 0, s>>>(A, k);
+      if (A.pbr) {
+        k_di_primary<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        k_di_shade<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+      } else {
+        k_di_primary<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        k_di_shade<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
+      }
       VT_CUDA(ctx, cudaGetLastError());
       scene->di_parity ^= 1u;
       ++scene->di_frames;
@@ -1726,7 +1743,8 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   groups = (spp + per - 1) / per;
   const uint64_t items = (uint64_t)npix * groups;
   const uint32_t grid = (uint32_t)std::min<uint64_t>((items + kRenderBlock - 1) / kRenderBlock, (uint64_t)ctx->sm_count * 32u);
-  k_render<<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+  if (A.pbr) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+  else k_render<false><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
   VT_CUDA(ctx, cudaGetLastError());
   scene->samples += spp;
   return VT_OK;
@@ -1755,6 +1773,7 @@ struct vt_batch {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   float last_ms = 0.0f;
   uint32_t passes = 0;
+  bool pbr = false;  // some scene has OPENPBR slots: the kernel variant with the OpenPBR code
 };
 
 namespace {
@@ -1781,13 +1800,14 @@ cudaError_t batch_enqueue(vt_ctx *ctx, vt_batch *b, const vt_batch::Config &c, c
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_start, 0xff, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   int perSm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_render_batch, c.block, 0) != cudaSuccess || perSm < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, b->pbr ? k_render_batch<true> : k_render_batch<false>, c.block, 0) !=
+          cudaSuccess || perSm < 1)
     perSm = 1;
   const unsigned long long warps = (b->total + 32ull * c.chunk - 1) / (32ull * c.chunk);
   const unsigned long long want = (warps * 32ull + c.block - 1) / c.block;
   const unsigned grid = (unsigned)std::min<unsigned long long>(want, (unsigned long long)perSm * ctx->sm_count);
   const uint32_t n = (uint32_t)b->scenes.size();
-  k_render_batch<<<grid, c.block, 0, s>>>(b->d_args, b->d_begin, n, b->total, c.chunk, b->d_first, b->d_frame,
+  (b->pbr ? k_render_batch<true> : k_render_batch<false>)<<<grid, c.block, 0, s>>>(b->d_args, b->d_begin, n, b->total, c.chunk, b->d_first, b->d_frame,
                                            b->d_counter, b->d_start, b->d_done, b->d_doneNs);
   k_batch_advance<<<(n + 127) / 128, 128, 0, s>>>(b->d_args, n, b->d_first, b->d_frame, b->d_done);
   return cudaGetLastError();
@@ -1824,6 +1844,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     fill_args(scenes[i], params + i, spp[i], args[i]);
     args[i].jitter = nullptr;
     first[i] = args[i].first;
+    if (args[i].pbr) b->pbr = true;
     frame[i] = args[i].firstFrame;
     begin[i + 1] = begin[i] + (unsigned long long)params[i].width * params[i].height;
     b->scenes.push_back(scenes[i]);
