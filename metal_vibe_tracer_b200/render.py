@@ -185,6 +185,14 @@ class Scene:
                                                               C.byref(samples)), "vt_accum_readback")
         return out.reshape(self.height, self.width, 3), int(samples.value)
 
+    def save_exr(self, path) -> int:
+        """Write the accumulation's mean radiance as a FLOAT RGB OpenEXR (the reference's HDR export);
+        returns the sample count."""
+        from .exr import write_exr
+        img, n = self.readback()
+        write_exr(path, img)
+        return n
+
     def close(self) -> None:
         if getattr(self, "_p", None) is not None and self.ctx._p is not None:
             _lib.load().vt_scene_destroy(self.ctx.handle, self._p)
