@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-launch measurement (0: skip)")
     p.add_argument("--batch-passes", type=int, default=2, help="timed batched passes after the tuning passes")
     p.add_argument("--production-frames", type=int, default=8, help="timed frames of the production scene (0: skip)")
+    p.add_argument("--nrc-pretrain", type=int, default=64, help="training-only frames of the radiance cache, timed")
+    p.add_argument("--nrc-max-spp", type=int, default=4096, help="spp cap of the radiance cache's relMSE runs")
     return p.parse_args()
 
 
@@ -247,12 +249,57 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
 
     pt_s, pt_spp, pt_err = time_to_relmse(1)
     di_s, di_spp, di_err = time_to_relmse(0)
+
+    # The radiance cache's arms: the cache is trained from scratch inside the timed region (training
+    # frames first, then every rendered frame trains once more and renders 16 spp whose paths end at
+    # their first bounce's hit with the cache's prediction), until the same relMSE bar or the spp cap.
+    def time_to_relmse_nrc(mode):
+        from metal_vibe_tracer_b200.nrc import RadianceCache
+        info = mesh.info()
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7)
+        scene.reset()
+        e0.record(stream)
+        for f in range(a.nrc_pretrain):
+            cache.render(scene, vt.make_params(cam, W, H, depth, 1 + f, True, mode), 0, render=False, stream=cs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms, done, err, frames = e0.elapsed_time(e1), 0, None, 0
+        while done < a.nrc_max_spp:
+            e0.record(stream)
+            cache.render(scene, vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp, stream=cs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            done += spp
+            frames += 1
+            img, _ = scene.readback()
+            err = rel_mse(img, ref)
+            if err <= 1e-3:
+                break
+        # Device time of one cached 16-spp frame with its training step, after the loop.
+        e0.record(stream)
+        cache.render(scene, vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp, stream=cs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        frame_ms = e0.elapsed_time(e1)
+        ci = cache.info()
+        cache.close()
+        return (total_ms / 1e3 if err is not None and err <= 1e-3 else None), done, err, frame_ms, ci
+
+    nrc = {}
+    for name, mode in (("nrc_restir", 0), ("nrc_mis", 1)):
+        s_, spp_, err_, fms, ci = time_to_relmse_nrc(mode)
+        nrc.update({f"{name}_s": s_, f"{name}_spp": spp_, f"{name}_relmse": err_, f"{name}_frame_ms": fms,
+                    f"{name}_loss": ci["last_loss"]})
+    nrc["nrc_pretrain_frames"] = a.nrc_pretrain
+    nrc["nrc_restir_speedup_vs_plain"] = (pt_s / nrc["nrc_restir_s"]) if (pt_s and nrc["nrc_restir_s"]) else None
     out["time_to_relmse_1e-3"] = {
         "plain_pt_s": pt_s, "spp": pt_spp, "relmse": pt_err,
         "restir_di_s": di_s, "restir_di_spp": di_spp, "restir_di_relmse": di_err,
+        **nrc,
         "reference_spp": nref, "reference_wall_s": ref_s,
-        "definition": "relMSE of luminance vs the FP64-accumulated reference (scripts/compare_mitsuba.py:353-354)",
-        "nrc": "not built (neural radiance cache is later work): the NRC arm of the metric is unmeasured"}
+        "definition": "relMSE of luminance vs the FP64-accumulated reference (scripts/compare_mitsuba.py:353-354); "
+                      "device time of the frames (and, for the cache, its training from scratch), readbacks untimed"}
     if cpu_leg:
         from oracle import vt_oracle as O
         cpu_spp = 256

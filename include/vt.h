@@ -410,6 +410,73 @@ vt_status vt_scene_emitter_words(vt_ctx *ctx, const vt_scene *scene, uint32_t *w
 vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *points, uint32_t npoints,
                             uint32_t per_point, uint32_t samples, float *out);
 
+/* ---- neural radiance cache (nrc.cu) -------------------------------------------------------------
+ * No counterpart in the reference (it has no radiance cache). A radiance cache after Mueller et al.
+ * 2021: a multiresolution hash grid of the position (Mueller et al. 2022) plus one-blob encodings of
+ * the outgoing direction, the shading normal and the roughness, and the reflectances, into an MLP
+ * of 5 hidden layers 64 wide (fp16 operands, fp32 accumulation, ReLU) with 3 linear outputs: the
+ * radiance leaving the vertex toward the previous one, without the vertex's own emission, in linear
+ * sRGB. Trained online by Adam under the relative L2 loss on the suffix radiance of training paths
+ * that the integrator traces to full depth. */
+typedef struct vt_nrc vt_nrc;
+typedef struct vt_nrc_config {
+  uint32_t levels;           /* hash-grid levels, 1-16 (16) */
+  uint32_t log2_table;       /* log2 of the entries per level, 12-24 (19) */
+  uint32_t base_resolution;  /* cells per axis of the coarsest level, >= 2 (16) */
+  uint32_t max_resolution;   /* cells per axis of the finest level (2048) */
+  uint32_t train_records;    /* training records per optimiser step (65536) */
+  uint32_t train_paths;      /* training paths per frame; 0: train_records / 4 */
+  uint32_t query_vertex;     /* rendered paths query the cache at this vertex, 1 = the first
+                                bounce's hit (1); vertices before it are traced as usual */
+  uint32_t seed;             /* parameter initialisation and training-path pixels */
+  float learning_rate;       /* Adam step size (0.01) */
+  float beta1, beta2, epsilon;  /* Adam (0.9, 0.99, 1e-15) */
+} vt_nrc_config;
+/* A cache query (48 bytes). Directions are (theta / pi, phi / (2 pi) + 1/2), theta from +z and phi
+ * = atan2(y, x). */
+typedef struct vt_nrc_input {
+  float position[3];
+  float roughness;       /* 1 for Lambert slots */
+  float direction[2];    /* outgoing direction (toward the previous vertex) */
+  float normal[2];       /* shading normal */
+  float diffuse[3];      /* diffuse reflectance: albedo x (1 - metalness) */
+  float specular;        /* specular reflectance: metalness */
+} vt_nrc_input;
+typedef struct vt_nrc_info {
+  unsigned long long mlp_params, grid_params;  /* 21,504; levels x 2^log2_table x 2 */
+  uint32_t steps;          /* optimiser steps taken */
+  uint32_t last_records;   /* records of the last step */
+  float last_loss;         /* mean relative L2 loss of the last step's records */
+  uint32_t pad;
+} vt_nrc_info;
+enum { VT_NRC_TRAIN = 1, VT_NRC_RENDER = 2 };
+
+vt_status vt_nrc_config_default(vt_nrc_config *cfg);
+/* A cache over the box [lo, hi] (the scene's bounds), parameters initialised from cfg->seed. */
+vt_status vt_nrc_create(vt_ctx *ctx, const vt_nrc_config *cfg, const float lo[3], const float hi[3], vt_nrc **out);
+vt_status vt_nrc_destroy(vt_ctx *ctx, vt_nrc *nrc);
+/* Synchronises the context's stream and the cache's last step. */
+vt_status vt_nrc_get_info(vt_ctx *ctx, vt_nrc *nrc, vt_nrc_info *out);
+/* Parameters as fp32: mlp = 21,504 floats (5 hidden 64 x 64 matrices [out][in], then the output
+ * layer 16 x 64 with rows 3-15 zero), grid = levels x 2^log2_table x 2 floats (may be NULL).
+ * Setting them also clears Adam's moments and step count. */
+vt_status vt_nrc_get_params(vt_ctx *ctx, const vt_nrc *nrc, float *mlp, float *grid);
+vt_status vt_nrc_set_params(vt_ctx *ctx, vt_nrc *nrc, const float *mlp, const float *grid);
+/* Predictions for n host queries: rgb = n x 3 floats. */
+vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_t n, float *rgb);
+/* The loss and its gradient sums over n host records (targets n x 3), without an update: mlp_grad
+ * 21,504 floats, grid_grad as vt_nrc_get_params' grid (may be NULL), loss the loss sum. */
+vt_status vt_nrc_gradients(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, const float *target, uint32_t n,
+                           float *mlp_grad, float *grid_grad, double *loss);
+/* One Adam step on n host records; loss (may be NULL) receives their mean loss before the step. */
+vt_status vt_nrc_train(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, const float *target, uint32_t n, float *loss);
+/* One frame of spp samples with the cache, stream-ordered like vt_render. flags VT_NRC_TRAIN:
+ * trace the frame's training paths (MIS, full depth) and take one optimiser step on their records
+ * first; VT_NRC_RENDER: render spp samples per pixel whose paths end at the query vertex with the
+ * cache's prediction (sampling modes 0 and 1), added to the scene's accumulation. */
+vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_frame_params *p, uint32_t spp,
+                        uint32_t flags, void *stream);
+
 /* ---- allocation-free build --------------------------------------------------------------- */
 
 /* No counterpart in the reference. The same GPU build as vt_mesh_build_device, for callers that

@@ -78,6 +78,23 @@ class BatchStats(C.Structure):
                 ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
 
 
+class NRCConfig(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
+                ("max_resolution", C.c_uint32), ("train_records", C.c_uint32), ("train_paths", C.c_uint32),
+                ("query_vertex", C.c_uint32), ("seed", C.c_uint32), ("learning_rate", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float)]
+
+
+class NRCInput(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("roughness", C.c_float), ("direction", C.c_float * 2),
+                ("normal", C.c_float * 2), ("diffuse", C.c_float * 3), ("specular", C.c_float)]
+
+
+class NRCInfo(C.Structure):
+    _fields_ = [("mlp_params", C.c_ulonglong), ("grid_params", C.c_ulonglong), ("steps", C.c_uint32),
+                ("last_records", C.c_uint32), ("last_loss", C.c_float), ("pad", C.c_uint32)]
+
+
 VT_OK = 0
 STATUS_NAMES = {0: "VT_OK", 1: "VT_ERR_INVALID", 2: "VT_ERR_CUDA", 3: "VT_ERR_MEMORY",
                 4: "VT_ERR_LIMIT", 5: "VT_ERR_DEVICE"}
@@ -136,6 +153,16 @@ SIGNATURES = {
     "vt_openpbr_energy_table": (_I32, [_P, _P, _P]),
     "vt_openpbr_evaluate": (_I32, [_P, _P, _U32, _P]),
     "vt_scene_set_openpbr": (_I32, [_P, _P, _P, _U32]),
+    "vt_nrc_config_default": (_I32, [C.POINTER(NRCConfig)]),
+    "vt_nrc_create": (_I32, [_P, C.POINTER(NRCConfig), _P, _P, C.POINTER(_P)]),
+    "vt_nrc_destroy": (_I32, [_P, _P]),
+    "vt_nrc_get_info": (_I32, [_P, _P, C.POINTER(NRCInfo)]),
+    "vt_nrc_get_params": (_I32, [_P, _P, _P, _P]),
+    "vt_nrc_set_params": (_I32, [_P, _P, _P, _P]),
+    "vt_nrc_infer": (_I32, [_P, _P, _P, _U32, _P]),
+    "vt_nrc_gradients": (_I32, [_P, _P, _P, _P, _U32, _P, _P, C.POINTER(C.c_double)]),
+    "vt_nrc_train": (_I32, [_P, _P, _P, _P, _U32, C.POINTER(C.c_float)]),
+    "vt_render_nrc": (_I32, [_P, _P, _P, _P, _U32, _U32, _P]),
 }
 NOALLOC_MAX_FACES = 32768
 

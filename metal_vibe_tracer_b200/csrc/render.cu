@@ -31,6 +31,7 @@
 #include "sampler.cuh"
 #include "spectral.cuh"
 #include "openpbr.cuh"
+#include "nrc.cuh"
 #include "trace_common.cuh"
 #include "vt_internal.cuh"
 
@@ -89,6 +90,15 @@ struct RenderArgs {
   const float4 *hPos, *hNrm, *hrPos, *hrEmit, *hrW;
   float3 pcam, pfwd, pright, pup;
   float paspect, pfovScale;
+  // Radiance cache (vt_render_nrc): per (sample, pixel) slot the query at vertex nrcVertex, the
+  // path's per-lane throughput there (times the lane's share) and its lanes' bins.
+  NrcInput *nrcIn;
+  float4 *nrcT;
+  uint2 *nrcBins;
+  uint32_t nrcVertex;
+  // Index checks: BVH nodes and triangles; a failed check sets a bit of *status and skips the read.
+  uint32_t nodeCount, faceCount;
+  uint32_t *status;
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -100,6 +110,12 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
   return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 __device__ __forceinline__ float3 normalize3(float3 a) { return mul(a, rsqrtf(dot3(a, a))); }
+
+// Status bits of the integrator's index checks (the context's status word 2).
+constexpr uint32_t kBadNode = 1u, kBadTriangle = 2u, kBadHit = 4u, kBadRecord = 8u;
+__device__ __forceinline__ void render_fault(const RenderArgs &A, uint32_t bit) {
+  if (A.status) atomicOr(A.status, bit);
+}
 
 // ---- traversal (the 4-wide watertight traversal with a local stack) ---------------------------
 struct Hit {
@@ -116,7 +132,12 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
   stack[top++] = 0;
   while (top > 0) {
     Node4 nd;
-    load_node(A.nodes, stack[--top], nd);
+    const int ni = stack[--top];
+    if ((uint32_t)ni >= A.nodeCount) {
+      render_fault(A, kBadNode);
+      break;
+    }
+    load_node(A.nodes, ni, nd);
     float nearT[4];
     const int mask = node_hits(nd, sr, tMin, closest, nearT);
     const Sorted4 s = sort_children(nd, mask, nearT);
@@ -125,6 +146,10 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
       if (j >= s.m || s.child[j] > 0 || beyond(s.key[j], closest)) continue;
       const int first = -s.child[j] - 1;
       for (int q = 0; q < s.count[j]; ++q) {
+        if ((uint32_t)(first + q) >= A.faceCount) {
+          render_fault(A, kBadTriangle);
+          break;
+        }
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         float t, b1, b2;
         if (!intersect_tri(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
@@ -163,7 +188,12 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
   stack[top++] = 0;
   while (top > 0) {
     Node4 nd;
-    load_node(A.nodes, stack[--top], nd);
+    const int ni = stack[--top];
+    if ((uint32_t)ni >= A.nodeCount) {
+      render_fault(A, kBadNode);
+      break;
+    }
+    load_node(A.nodes, ni, nd);
     float nearT[4];
     const int mask = node_hits(nd, sr, tMin, tMax, nearT);
 #pragma unroll
@@ -173,6 +203,10 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
       if (c > 0) { if (top < kRenderStack) stack[top++] = c; continue; }
       const int first = -c - 1, cnt = i4(nd.count, k);
       for (int q = 0; q < cnt; ++q) {
+        if ((uint32_t)(first + q) >= A.faceCount) {
+          render_fault(A, kBadTriangle);
+          break;
+        }
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
         float t, b1, b2;
@@ -206,8 +240,12 @@ __device__ __forceinline__ float ray_tmin(const RenderArgs &A, float3 o) {
 // scenes rebuild the point from barycentrics and take the triangle's rounding bound as its error.
 __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h, float3 o, float3 d) {
   Surface s;
-  const float4 a = __ldg(A.tris + 3 * (size_t)h.pos), b = __ldg(A.tris + 3 * (size_t)h.pos + 1),
-               c = __ldg(A.tris + 3 * (size_t)h.pos + 2);
+  size_t hp = (size_t)h.pos;
+  if ((uint32_t)h.pos >= A.faceCount) {
+    render_fault(A, kBadHit);
+    hp = 0;
+  }
+  const float4 a = __ldg(A.tris + 3 * hp), b = __ldg(A.tris + 3 * hp + 1), c = __ldg(A.tris + 3 * hp + 2);
   const float3 e1 = f3(b.x - a.x, b.y - a.y, b.z - a.z), e2 = f3(c.x - a.x, c.y - a.y, c.z - a.z);
   const float3 ng = normalize3(cross3(e1, e2));
   s.front = dot3(ng, d) < 0.0f;
@@ -225,8 +263,7 @@ __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h,
   // mesh_hit_attributes (main.swift:1590-1593): smooth normal when the vertex normals give one.
   s.n = s.gn;
   if (A.nrm) {
-    const float4 na = __ldg(A.nrm + 3 * (size_t)h.pos), nb = __ldg(A.nrm + 3 * (size_t)h.pos + 1),
-                 nc = __ldg(A.nrm + 3 * (size_t)h.pos + 2);
+    const float4 na = __ldg(A.nrm + 3 * hp), nb = __ldg(A.nrm + 3 * hp + 1), nc = __ldg(A.nrm + 3 * hp + 2);
     const float3 sm = add(add(mul(f3(na.x, na.y, na.z), b0), mul(f3(nb.x, nb.y, nb.z), h.b1)),
                           mul(f3(nc.x, nc.y, nc.z), h.b2));
     if (dot3(sm, sm) > 1e-12f) {
@@ -633,6 +670,7 @@ __device__ __forceinline__ float3 to_rgb(const RenderArgs &A, const Lanes &L, fl
 }
 __device__ __forceinline__ float4 scale4(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
 __device__ __forceinline__ float4 mul4(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+__device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
 __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
   return A.spectral ? fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)) : fmaxf(fmaxf(a.x, a.y), a.z);
 }
@@ -695,23 +733,23 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
          weight.y >= 0.0f && weight.z >= 0.0f && weight.w >= 0.0f;
 }
 
-// NEE at a Lambert vertex: the contribution's rgb (quad: 2 draws; emitters: 4).
+// NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
 template <bool kPbr>
-__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
-                                               float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
-                                               Sampler &seed, int *stack, bool requirePdf) {
+__device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
+                                                     float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
+                                                     Sampler &seed, int *stack, bool requirePdf) {
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const LightSample ls = sample_direct(A, p, seed);
-  if (requirePdf && !(ls.pdf > 0.0f)) return f3(0.0f, 0.0f, 0.0f);
-  if (!light_visible(A, p, gn, err, ls, stack)) return f3(0.0f, 0.0f, 0.0f);
+  if (requirePdf && !(ls.pdf > 0.0f)) return zero;
+  if (!light_visible(A, p, gn, err, ls, stack)) return zero;
   const float cosine = fabsf(dot3(n, ls.wi));
   if (is_pbr<kPbr>(A, m)) {
     float bpdf;
     const float4 f = pbr_eval_lanes(A, L, m, n, gn, wo, ls.wi, bpdf);
     const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
     const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
-    const float4 s = scale4(mul4(mul4(T, f), emission(A, L, le)), cosine * weight / ls.pdf);
-    return to_rgb(A, L, s);
+    return scale4(mul4(mul4(T, f), emission(A, L, le)), cosine * weight / ls.pdf);
   }
   const float4 albedo = reflectance(A, L, m);
   // eval_bsdf / eval_bsdf_pdf for DIFFUSE (main.swift:2659-2676): no light below the geometric
@@ -725,8 +763,14 @@ __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes 
   const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
   const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
   const float4 Le = emission(A, L, le);
-  const float4 s = scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
-  return to_rgb(A, L, s);
+  return scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
+}
+// The same as rgb.
+template <bool kPbr>
+__device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
+                                               float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
+                                               Sampler &seed, int *stack, bool requirePdf) {
+  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
 }
 
 // ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
@@ -873,9 +917,43 @@ __device__ __forceinline__ float3 primary_emission(const RenderArgs &A, const La
 // Russian roulette. With diPrimary (sampling mode 0) the primary vertex's direct light came from its
 // ReSTIR DI reservoir, so a BSDF hit on an emitter from it gets no weight (previousMIS false,
 // main.swift:7717-7718).
+// The cache's query record of a vertex (nrc.cuh's input layout): OpenPBR slots give their
+// roughness and split the base colour by metalness; Lambert slots are rough and diffuse.
 template <bool kPbr>
+__device__ __forceinline__ NrcInput nrc_query(const RenderArgs &A, const Surface &S, const vt_material &m, float3 dir) {
+  NrcInput q;
+  float rough = 1.0f, metal = 0.0f;
+  if (is_pbr<kPbr>(A, m)) {
+    const float4 pq = __ldg(A.pbr + __float_as_uint(m.pad));
+    rough = pq.x;
+    metal = nrc_sat(pq.y);
+  }
+  const float2 w = nrc_sphere(mul(dir, -1.0f)), n = nrc_sphere(S.n);
+  q.a = make_float4(S.pos.x, S.pos.y, S.pos.z, rough);
+  q.b = make_float4(w.x, w.y, n.x, n.y);
+  q.c = make_float4(m.albedo[0] * (1.0f - metal), m.albedo[1] * (1.0f - metal), m.albedo[2] * (1.0f - metal), metal);
+  return q;
+}
+// Stores the query of slot `slot`, with the throughput T (times the lanes' shares) and the bins.
+__device__ __forceinline__ void nrc_store(const RenderArgs &A, size_t slot, const NrcInput &q, const Lanes &L, float4 T) {
+  A.nrcIn[slot] = q;
+  if (A.spectral) {
+    A.nrcT[slot] = make_float4(T.x * L.w[0], T.y * L.w[1], T.z * L.w[2], T.w * L.w[3]);
+    A.nrcBins[slot] = make_uint2((uint32_t)L.bin[0] | ((uint32_t)L.bin[1] << 16), (uint32_t)L.bin[2] | ((uint32_t)L.bin[3] << 16));
+  } else {
+    A.nrcT[slot] = make_float4(T.x, T.y, T.z, 0.0f);
+    A.nrcBins[slot] = make_uint2(0u, 0u);
+  }
+}
+__device__ __forceinline__ void nrc_store_none(const RenderArgs &A, size_t slot) {
+  A.nrcT[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// kNrc (vt_render_nrc): the path ends at vertex A.nrcVertex, after that vertex's emission, with
+// its cache query stored in `slot`; `queried` tells whether it got there.
+template <bool kPbr, bool kNrc = false>
 __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
-                                Sampler &seed, int *stack, bool diPrimary) {
+                                Sampler &seed, int *stack, bool diPrimary, size_t slot = 0, bool *queried = nullptr) {
   const int limit = max(0, (int)A.maxDepth - 1);
   const bool nee = A.mode != 3u, mis = A.mode <= 1u;
   float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -922,6 +1000,11 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       break;
     }
     if (emissionOnly) break;
+    if (kNrc && (uint32_t)bounce >= A.nrcVertex) {
+      nrc_store(A, slot, nrc_query<kPbr>(A, S, m, dir), L, T);
+      *queried = true;
+      break;
+    }
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
       R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
@@ -938,9 +1021,9 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
 }
 
 // One path of sampling modes 1-3: camera ray, primary hit, NEE there, then the continuation.
-template <bool kPbr>
-__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
-                              int *stack) {
+template <bool kPbr, bool kNrc>
+__device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame,
+                                                   float2 jit, int *stack, size_t slot, bool &queried) {
   Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
   Lanes L;
   if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
@@ -961,9 +1044,17 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
     R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
-  R = add(R, continue_path<kPbr>(A, L, S, m, dir0, seed, stack, false));
+  R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
+}
+template <bool kPbr, bool kNrc = false>
+__device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
+                              int *stack, size_t slot = 0) {
+  bool queried = false;
+  const float3 c = path_sample_body<kPbr, kNrc>(A, x, y, si, frame, jit, stack, slot, queried);
+  if (kNrc && !queried) nrc_store_none(A, slot);
+  return c;
 }
 
 // ReSTIR DI pass 1 for frame k (restir_temporal_kernel, main.swift:4842-4960): the primary hit into
@@ -1043,11 +1134,13 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
 // taps in a 32-pixel box that pass RESTIR2020's compatibility test (uniform_neighbor, main.swift:
 // 5025-5027), the selected sample's contribution W * bsdf * Le * cos * G when visible, then the
 // path's continuation (MIS at later vertices). The sample is added to the FP64 accumulation.
-template <bool kPbr>
+template <bool kPbr, bool kNrc = false>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderArgs A, uint32_t k) {
   int stack[kRenderStack];
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.W * A.H) return;
+  const size_t slot = (size_t)k * A.W * A.H + i;
+  bool queried = false;
   const uint32_t x = i % A.W, y = i / A.W;
   Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
   Lanes L;
@@ -1056,7 +1149,10 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
   lens_ray(A, o0, dir0, seed);  // the same draws as pass 1
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   const float4 gp = A.gPos[i];
-  if (gp.w <= 0.0f) return;
+  if (gp.w <= 0.0f) {
+    if (kNrc) nrc_store_none(A, slot);
+    return;
+  }
   const float4 gn = A.gNrm[i];
   const uint4 gi = A.gInfo[i];
   Surface S;
@@ -1095,8 +1191,9 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
       R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel), W);
-    R = add(R, continue_path<kPbr>(A, L, S, m, dir0, seed, stack, true));
+    R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, true, slot, &queried));
   }
+  if (kNrc && !queried) nrc_store_none(A, slot);
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) return;
   double *acc = A.accum + 3 * (size_t)i;
   acc[0] += R.x; acc[1] += R.y; acc[2] += R.z;
@@ -1105,7 +1202,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
 // Work item i = (sample group g, pixel p), pixel-major within a group so that a warp traces
 // neighbouring pixels; a group covers `per` consecutive samples of the call. Each item adds its
 // FP64 sum to the pixel with one atomic per channel (groups > 1) or a plain add (groups = 1).
-template <bool kPbr>
+template <bool kPbr, bool kNrc = false>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArgs A, uint32_t groups, uint32_t per) {
   int stack[kRenderStack];
   const uint32_t npix = A.W * A.H;
@@ -1116,7 +1213,8 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
-      const float3 c = path_sample<kPbr>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack);
+      const float3 c = path_sample<kPbr, kNrc>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack,
+                                               (size_t)k * npix + p);
       sr += c.x;
       sg += c.y;
       sb += c.z;
@@ -1128,6 +1226,156 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
       atomicAdd(acc, sr); atomicAdd(acc + 1, sg); atomicAdd(acc + 2, sb);
     }
   }
+}
+
+// ---- radiance cache: training paths and the resolve (vt_render_nrc) -----------------------------
+constexpr int kNrcRecords = 8;  // records per training path: its first 8 vertices
+
+// Training path j of a frame (sampling mode 1 semantics: NEE with MIS at every vertex, Russian
+// roulette after bounce 3, full depth): pixel (offset + j stride) mod npix, its own PCG stream
+// (sample index si), a random sub-pixel position. Each non-emissive vertex i of the path gives a
+// record: its cache query and, as target, the radiance the rest of the path brought to it, rgb of
+// the lanes' (R_end - R_i) / T_i, R_i the path's radiance when it reached vertex i (after that
+// vertex's emission) and T_i its throughput there. Records go to consecutive slots claimed with
+// one atomic per path; those past `cap` are dropped.
+template <bool kPbr>
+__global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
+    k_nrc_paths(RenderArgs A, uint32_t npaths, uint32_t offset, uint32_t stride, uint32_t si0, uint32_t cap,
+                float4 *__restrict__ scratch, size_t scratchCap, NrcInput *__restrict__ outIn,
+                float4 *__restrict__ outTarget, uint32_t outCap, uint32_t *__restrict__ count) {
+  int stack[kRenderStack];
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j == 0) count[1] = cap;
+  if (j >= npaths) return;
+  const uint32_t npix = A.W * A.H;
+  const uint64_t lin = (uint64_t)offset + (uint64_t)j * stride;
+  const uint32_t p = (uint32_t)(lin % npix), wrap = (uint32_t)(lin / npix);
+  const uint32_t x = p % A.W, y = p / A.W;
+  Sampler seed = pixel_sampler(x, y, A.W, si0 + wrap, false, 0u, 0u);
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, wavelength_numbers(seed).x);
+  const float2 jit = make_float2(rand_f(seed) - 0.5f, rand_f(seed) - 0.5f);
+  float3 dir = camera_dir(A, x, y, jit), o = A.cam;
+  lens_ray(A, o, dir, seed);
+  Hit h;
+  if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return;
+  seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
+  Surface S = surface_at(A, h, o, dir);
+  vt_material m = material(A, S.slot);
+  if (m.type == VT_MAT_EMISSIVE) return;
+  const int limit = max(0, (int)A.maxDepth - 1);
+  float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+  float4 R = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // The path's records as they are met: query, T_i, R_i (5 float4 each) in its scratch slots.
+  if ((size_t)(j + 1) * kNrcRecords * 5 > scratchCap) {
+    render_fault(A, kBadRecord);
+    return;
+  }
+  float4 *rec = scratch + (size_t)j * kNrcRecords * 5;
+  int nrec = 0;
+  {
+    const NrcInput q = nrc_query<kPbr>(A, S, m, dir);
+    rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
+    nrec = 1;
+  }
+  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
+  int scattering = 0;
+  for (int bounce = 1; scattering < limit; ++bounce) {
+    ++scattering;
+    const float3 r = rand_f3(seed);
+    float3 nd;
+    float bpdf;
+    if (is_pbr<kPbr>(A, m)) {
+      float4 w;
+      if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+      T = mul4(T, w);
+    } else {
+      nd = cosine_hemisphere(S.n, r.y, r.z);
+      bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+      if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
+      T = mul4(T, reflectance(A, L, m));
+    }
+    if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
+    const float3 prev = S.pos;
+    o = ray_origin(A, S.pos, S.gn, nd, S.err);
+    dir = nd;
+    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
+    S = surface_at(A, h, o, dir);
+    m = material(A, S.slot);
+    if (m.type == VT_MAT_EMISSIVE) {
+      const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
+      const float w = lpdf <= 0.0f ? 1.0f : power_heuristic(bpdf, lpdf);
+      if (!A.imported || S.front) R = add4(R, scale4(mul4(T, emission(A, L, m.emission)), w));
+      break;
+    }
+    if (nrec < kNrcRecords) {
+      const NrcInput q = nrc_query<kPbr>(A, S, m, dir);
+      float4 *r = rec + 5 * nrec;
+      r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
+      ++nrec;
+    }
+    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
+                                         stack, false));
+    if (bounce > 3) {
+      const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+      if (rand_f(seed) >= survival) break;
+      T = scale4(T, 1.0f / survival);
+    }
+  }
+  const uint32_t first = atomicAdd(count, (uint32_t)nrec);
+  for (int i = 0; i < nrec; ++i) {
+    if (first + (uint32_t)i >= cap) break;
+    if (first + (uint32_t)i >= outCap) {
+      render_fault(A, kBadRecord);
+      break;
+    }
+    const float4 *r = rec + 5 * i;
+    const float4 t = r[3], r0 = r[4];
+    const float4 d = make_float4(t.x > 1e-20f ? (R.x - r0.x) / t.x : 0.0f, t.y > 1e-20f ? (R.y - r0.y) / t.y : 0.0f,
+                                 t.z > 1e-20f ? (R.z - r0.z) / t.z : 0.0f, t.w > 1e-20f ? (R.w - r0.w) / t.w : 0.0f);
+    float3 c = to_rgb(A, L, d);
+    if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) c = f3(0.0f, 0.0f, 0.0f);
+    NrcInput q;
+    q.a = r[0]; q.b = r[1]; q.c = r[2];
+    outIn[first + i] = q;
+    outTarget[first + i] = make_float4(c.x, c.y, c.z, 0.0f);
+  }
+}
+
+// Adds each pixel's cache contributions: per sample slot with a query, the throughput times the
+// prediction (clamped at zero), in spectral transport the prediction's emission uplift at the
+// slot's lanes, to rgb.
+__global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uint32_t spp) {
+  const uint32_t npix = A.W * A.H;
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  double sr = 0.0, sg = 0.0, sb = 0.0;
+  for (uint32_t k = 0; k < spp; ++k) {
+    const size_t slot = (size_t)k * npix + p;
+    const float4 t = A.nrcT[slot];
+    if (t.x == 0.0f && t.y == 0.0f && t.z == 0.0f && t.w == 0.0f) continue;
+    const float4 c = pred[slot];
+    const float3 e = f3(fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f));
+    float3 v;
+    if (A.spectral) {
+      const uint2 b = A.nrcBins[slot];
+      Lanes L;
+      L.bin[0] = (int)(b.x & 0xffffu); L.bin[1] = (int)(b.x >> 16);
+      L.bin[2] = (int)(b.y & 0xffffu); L.bin[3] = (int)(b.y >> 16);
+      L.w[0] = L.w[1] = L.w[2] = L.w[3] = 1.0f;
+      v = lanes_rgb(A, L, mul4(t, lanes_emission(A, L, e)));
+    } else {
+      v = f3(t.x * e.x, t.y * e.y, t.z * e.z);
+    }
+    if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) continue;
+    sr += v.x;
+    sg += v.y;
+    sb += v.z;
+  }
+  double *acc = A.accum + 3 * (size_t)p;
+  acc[0] += sr;
+  acc[1] += sg;
+  acc[2] += sb;
 }
 
 // ---- batched scenes: one persistent launch over many scenes (config C4) ---------------------------
@@ -1518,6 +1766,9 @@ vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *poi
   A.rootMax = mesh->root_max;
   A.mats = scene->d_mats;
   A.nmat = scene->nmat;
+  A.nodeCount = mesh->nnodes;
+  A.faceCount = mesh->nfaces;
+  A.status = ctx->d_status + 2;
   emitter_args(scene, A);
   float4 *d_points = nullptr;
   float *d_out = nullptr;
@@ -1646,16 +1897,32 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.zModel = p->z_temporal;
   A.firstFrame = p->first_frame ? p->first_frame : scene->samples + 1u;
   A.accum = scene->d_accum;
+  A.nodeCount = mesh->nnodes;
+  A.faceCount = mesh->nfaces;
   emitter_args(scene, A);
 }
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
-  if (!ctx) return VT_ERR_INVALID;
-  if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+// The cache's part of a frame rendered with queries: predictions for every slot, then the resolve.
+vt_status nrc_finish(vt_ctx *ctx, vt_nrc *nrc, const RenderArgs &A, uint32_t spp, cudaStream_t s) {
+  const size_t n = (size_t)A.W * A.H * spp;
+  if (n > 0xffffffffull) return vt_fail(ctx, VT_ERR_LIMIT, "too many cache queries in one frame");
+  {
+    const vt_status st = vt_nrc_predict(ctx, nrc, nrc->d_q, (uint32_t)n, nrc->d_qout, s);
+    if (st != VT_OK) return st;
+  }
+  k_nrc_resolve<<<(A.W * A.H + 255) / 256, 256, 0, s>>>(A, nrc->d_qout, spp);
+  VT_CUDA(ctx, cudaGetLastError());
+  return VT_OK;
+}
+
+// vt_render, and with a cache (nrc not null) vt_render_nrc's rendering: the same frames, paths
+// ending at the cache's query vertex, then the predictions and the resolve.
+vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream,
+                      vt_nrc *nrc) {
   {
     const vt_status st = check_params(ctx, scene, p);
     if (st != VT_OK) return st;
@@ -1685,7 +1952,16 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   RenderArgs A;
   fill_args(scene, p, spp, A);
   A.jitter = scene->d_jitter;
+  A.status = ctx->d_status + 2;
   const uint32_t npix = p->width * p->height;
+  if (nrc) {
+    const vt_status st = vt_nrc_reserve_queries(ctx, nrc, (size_t)npix * spp);
+    if (st != VT_OK) return st;
+    A.nrcIn = nrc->d_q;
+    A.nrcT = nrc->d_qT;
+    A.nrcBins = nrc->d_qbins;
+    A.nrcVertex = nrc->cfg.query_vertex;
+  }
   if (p->sampling_mode == 0u) {
     // ReSTIR DI: frames in order, two launches each (the primary pass, then reuse and shading).
     if (!scene->d_di || scene->di_width != p->width || scene->di_height != p->height) {
@@ -1723,15 +1999,21 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
       A.pfovScale = pc[13];
       if (A.pbr) {
         k_di_primary<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
-        k_di_shade<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        if (nrc) k_di_shade<true, true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        else k_di_shade<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
       } else {
         k_di_primary<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
-        k_di_shade<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        if (nrc) k_di_shade<false, true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        else k_di_shade<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
       }
       VT_CUDA(ctx, cudaGetLastError());
       scene->di_parity ^= 1u;
       ++scene->di_frames;
       std::memcpy(scene->di_cam, cam, sizeof cam);
+    }
+    if (nrc) {
+      const vt_status st = nrc_finish(ctx, nrc, A, spp, s);
+      if (st != VT_OK) return st;
     }
     scene->samples += spp;
     return VT_OK;
@@ -1743,10 +2025,84 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   groups = (spp + per - 1) / per;
   const uint64_t items = (uint64_t)npix * groups;
   const uint32_t grid = (uint32_t)std::min<uint64_t>((items + kRenderBlock - 1) / kRenderBlock, (uint64_t)ctx->sm_count * 32u);
-  if (A.pbr) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
-  else k_render<false><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
-  VT_CUDA(ctx, cudaGetLastError());
+  if (nrc) {
+    if (A.pbr) k_render<true, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    else k_render<false, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    VT_CUDA(ctx, cudaGetLastError());
+    const vt_status st = nrc_finish(ctx, nrc, A, spp, s);
+    if (st != VT_OK) return st;
+  } else {
+    if (A.pbr) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    else k_render<false><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    VT_CUDA(ctx, cudaGetLastError());
+  }
   scene->samples += spp;
+  return VT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+  return render_impl(ctx, scene, p, spp, stream, nullptr);
+}
+
+vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_frame_params *p, uint32_t spp,
+                        uint32_t flags, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !p || !nrc) return vt_fail(ctx, VT_ERR_INVALID, "scene, nrc or params is null");
+  if (flags & ~(uint32_t)(VT_NRC_TRAIN | VT_NRC_RENDER)) return vt_fail(ctx, VT_ERR_INVALID, "unknown flags");
+  if ((flags & VT_NRC_RENDER) && p->sampling_mode > 1)
+    return vt_fail(ctx, VT_ERR_INVALID, "the cache renders sampling modes 0 (ReSTIR DI) and 1 (MIS)");
+  {
+    const vt_status st = check_params(ctx, scene, p);
+    if (st != VT_OK) return st;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  if ((flags & VT_NRC_TRAIN) && scene->mesh->nfaces > 0) {
+    const uint32_t cap = nrc->cfg.train_records;
+    const uint32_t npaths = nrc->cfg.train_paths ? nrc->cfg.train_paths : std::max(1u, cap / 4u);
+    {
+      const vt_status st = vt_nrc_reserve_records(ctx, nrc, cap);
+      if (st != VT_OK) return st;
+    }
+    RenderArgs A;
+    fill_args(scene, p, 1, A);
+    A.status = ctx->d_status + 2;
+    const uint32_t npix = p->width * p->height;
+    // A fresh pixel pattern each frame: an offset from the frame's index, pixels `stride` apart.
+    const uint32_t frame = nrc->frames++;
+    uint32_t h = nrc->cfg.seed ^ (frame * 0x9e3779b9u);
+    h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+    const uint32_t stride = std::max(1u, npix / npaths);
+    VT_CUDA(ctx, cudaMemsetAsync(nrc->d_count, 0, sizeof(uint32_t), s));
+    const uint32_t si0 = 0x40000000u + (frame << 8);
+    const size_t scratch = (size_t)npaths * kNrcRecords * 5;
+    if (scratch > nrc->scratch_cap) {
+      cudaFree(nrc->d_scratch);
+      nrc->d_scratch = nullptr;
+      nrc->scratch_cap = 0;
+      VT_CUDA(ctx, cudaMalloc(&nrc->d_scratch, scratch * sizeof(float4)));
+      nrc->scratch_cap = scratch;
+    }
+    const unsigned blocks = (npaths + kRenderBlock - 1) / kRenderBlock;
+    if (A.pbr)
+      k_nrc_paths<true><<<blocks, kRenderBlock, 0, s>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
+                                                        nrc->scratch_cap, nrc->d_tin, nrc->d_ttarget, nrc->tcap,
+                                                        nrc->d_count);
+    else
+      k_nrc_paths<false><<<blocks, kRenderBlock, 0, s>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
+                                                         nrc->scratch_cap, nrc->d_tin, nrc->d_ttarget, nrc->tcap,
+                                                         nrc->d_count);
+    VT_CUDA(ctx, cudaGetLastError());
+    const vt_status st = vt_nrc_step(ctx, nrc, cap, s);
+    if (st != VT_OK) return st;
+  }
+  if (flags & VT_NRC_RENDER) return render_impl(ctx, scene, p, spp, stream, nrc);
   return VT_OK;
 }
 
@@ -1842,6 +2198,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     vt_status st = ensure_accum(ctx, scenes[i], params + i);
     if (st != VT_OK) { batch_free(b); return st; }
     fill_args(scenes[i], params + i, spp[i], args[i]);
+    args[i].status = ctx->d_status + 2;
     args[i].jitter = nullptr;
     first[i] = args[i].first;
     if (args[i].pbr) b->pbr = true;
@@ -1985,6 +2342,15 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
   const size_t want = 3 * (size_t)scene->width * scene->height;
   if (n != want) return vt_fail(ctx, VT_ERR_INVALID, "n must equal width * height * 3");
   VT_CUDA(ctx, cudaDeviceSynchronize());
+  {
+    uint32_t bad = 0;
+    VT_CUDA(ctx, cudaMemcpy(&bad, ctx->d_status + 2, sizeof bad, cudaMemcpyDeviceToHost));
+    if (bad) {
+      VT_CUDA(ctx, cudaMemset(ctx->d_status + 2, 0, sizeof bad));
+      return vt_fail(ctx, VT_ERR_DEVICE, "the integrator met an out-of-range index (status " + std::to_string(bad) +
+                                             ": 1 BVH node, 2 triangle, 4 hit, 8 cache record); the accesses were skipped");
+    }
+  }
   if (want) VT_CUDA(ctx, cudaMemcpy(rgb, scene->d_accum, want * sizeof(double), cudaMemcpyDeviceToHost));
   const double inv = scene->samples ? 1.0 / scene->samples : 0.0;
   for (size_t i = 0; i < want; ++i) rgb[i] *= inv;
