@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--production-frames", type=int, default=8, help="timed frames of the production scene (0: skip)")
     p.add_argument("--nrc-pretrain", type=int, default=64, help="training-only frames of the radiance cache, timed")
     p.add_argument("--nrc-max-spp", type=int, default=4096, help="spp cap of the radiance cache's relMSE runs")
+    p.add_argument("--nrc-records", type=int, default=16384,
+                   help="cache training records per frame (a quarter of the 256x256 image's pixels)")
     return p.parse_args()
 
 
@@ -256,7 +258,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     def time_to_relmse_nrc(mode):
         from metal_vibe_tracer_b200.nrc import RadianceCache
         info = mesh.info()
-        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7)
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records)
         scene.reset()
         e0.record(stream)
         for f in range(a.nrc_pretrain):
@@ -292,6 +294,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
         nrc.update({f"{name}_s": s_, f"{name}_spp": spp_, f"{name}_relmse": err_, f"{name}_frame_ms": fms,
                     f"{name}_loss": ci["last_loss"]})
     nrc["nrc_pretrain_frames"] = a.nrc_pretrain
+    nrc["nrc_train_records"] = a.nrc_records
     nrc["nrc_restir_speedup_vs_plain"] = (pt_s / nrc["nrc_restir_s"]) if (pt_s and nrc["nrc_restir_s"]) else None
     out["time_to_relmse_1e-3"] = {
         "plain_pt_s": pt_s, "spp": pt_spp, "relmse": pt_err,

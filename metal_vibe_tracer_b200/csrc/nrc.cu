@@ -20,7 +20,8 @@ namespace {
 using namespace vtd;
 
 constexpr int kLd = kNrcLd;
-constexpr size_t kInferSmem = (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kNrcTile * kLd) * sizeof(__half);
+constexpr int kInferRows = 256;  // inference rows per CTA (8 warps share the weights; 2 CTAs per SM)
+constexpr size_t kInferSmem = (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kInferRows * kLd) * sizeof(__half);
 constexpr size_t kTrainSmem =
     (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kNrcTile * kLd * (kNrcHidden + 2)) * sizeof(__half);
 constexpr float kGradClip = 512.0f;  // per-output loss gradient bound (fp16 range of the backward pass)
@@ -143,15 +144,15 @@ __device__ __forceinline__ void output_layer(const uint32_t (&a)[2][4][4], const
   }
 }
 
-// Inference: out[row] = (r, g, b, 0) for rows < n. Persistent CTAs over 128-row tiles.
-__global__ void __launch_bounds__(kNrcTile) k_nrc_infer(NrcGrid G, const float *__restrict__ mlp,
+// Inference: out[row] = (r, g, b, 0) for rows < n. Persistent CTAs over 256-row tiles.
+__global__ void __launch_bounds__(kInferRows, 2) k_nrc_infer(NrcGrid G, const float *__restrict__ mlp,
                                                         const NrcInput *__restrict__ in, uint32_t n,
                                                         float4 *__restrict__ out) {
   extern __shared__ __align__(16) __half sm[];
   __half *W = sm, *Wo = W + kNrcHidden * 64 * kLd, *X = Wo + kNrcOutRows * kLd;
   load_weights(mlp, W, Wo);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, row0 = 32 * warp;
-  for (uint32_t base = blockIdx.x * kNrcTile; base < n; base += gridDim.x * kNrcTile) {
+  for (uint32_t base = blockIdx.x * kInferRows; base < n; base += gridDim.x * kInferRows) {
     const uint32_t row = base + threadIdx.x;
     NrcInput q;
     if (row < n) {
@@ -498,9 +499,9 @@ vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s) {
 
 vt_status vt_nrc_predict(vt_ctx *ctx, vt_nrc *nrc, const NrcInput *in, uint32_t n, float4 *out, cudaStream_t s) {
   if (n == 0) return VT_OK;
-  const uint32_t tiles = (n + kNrcTile - 1) / kNrcTile;
-  const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * 3u);
-  k_nrc_infer<<<grid, kNrcTile, kInferSmem, s>>>(nrc->grid, nrc->d_p, in, n, out);
+  const uint32_t tiles = (n + kInferRows - 1) / kInferRows;
+  const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * 2u);
+  k_nrc_infer<<<grid, kInferRows, kInferSmem, s>>>(nrc->grid, nrc->d_p, in, n, out);
   VT_CUDA(ctx, cudaGetLastError());
   return VT_OK;
 }
@@ -562,8 +563,12 @@ vt_status vt_nrc_create(vt_ctx *ctx, const vt_nrc_config *cfg, const float lo[3]
   const double growth = c.levels > 1 ? std::exp((std::log((double)c.max_resolution) - std::log((double)c.base_resolution)) /
                                                 (double)(c.levels - 1))
                                      : 1.0;
-  for (uint32_t l = 0; l < (uint32_t)kNrcMaxLevels; ++l)
+  G.dense = 0;
+  for (uint32_t l = 0; l < (uint32_t)kNrcMaxLevels; ++l) {
     G.res[l] = l < c.levels ? (uint32_t)std::floor((double)c.base_resolution * std::pow(growth, (double)l) + 1e-6) : 1u;
+    const uint64_t side = G.res[l] + 1ull;
+    if (side * side * side <= (1ull << c.log2_table)) G.dense |= 1u << l;
+  }
   n->nparams = (uint64_t)kNrcMlpParams + 2ull * c.levels * (1ull << c.log2_table);
   vt_status st = VT_OK;
   const size_t bytes = n->nparams * sizeof(float);

@@ -46,7 +46,8 @@ struct NrcGrid {
   uint32_t levels, logT;
   float lo[3], inv[3];          // position -> [0, 1]^3: (p - lo) * inv
   uint32_t res[kNrcMaxLevels];  // cells per axis per level
-  uint32_t *status;             // index checks: a failed one sets a bit and skips the access
+  uint32_t dense;               // bit l: level l indexes its (res + 1)^3 points directly
+  uint32_t *status;             // index checks: an entry out of range is clamped and sets a bit
 };
 
 // Status bits of the cache's index checks (the context's status word 3).
@@ -59,12 +60,11 @@ __device__ __forceinline__ float nrc_sat(float x) { return fminf(fmaxf(x, 0.0f),
 
 // Corner index of level `l` at integer grid point (x, y, z): dense while (res + 1)^3 fits the
 // table, else the spatial hash x ^ y * 2654435761 ^ z * 805459861 modulo the table size.
-__device__ __forceinline__ uint32_t nrc_index(const NrcGrid &G, uint32_t res, uint32_t x, uint32_t y, uint32_t z) {
+__device__ __forceinline__ uint32_t nrc_index(const NrcGrid &G, uint32_t l, uint32_t res, uint32_t x, uint32_t y,
+                                              uint32_t z) {
   const uint32_t side = res + 1u;
-  const uint64_t dense = (uint64_t)side * side * side;
-  const uint32_t mask = (1u << G.logT) - 1u;
-  if (dense <= (uint64_t)mask + 1u) return x + side * (y + side * z);
-  return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & mask;
+  if ((G.dense >> l) & 1u) return x + side * (y + side * z);
+  return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & ((1u << G.logT) - 1u);
 }
 
 // The 8 corners of level l around normalised position q: entry indices (within the level) and
@@ -78,7 +78,7 @@ __device__ __forceinline__ void nrc_corners(const NrcGrid &G, uint32_t l, float3
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const uint32_t dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-    idx[c] = nrc_index(G, res, cx + dx, cy + dy, cz + dz);
+    idx[c] = nrc_index(G, l, res, cx + dx, cy + dy, cz + dz);
     w[c] = (dx ? fx : 1.0f - fx) * (dy ? fy : 1.0f - fy) * (dz ? fz : 1.0f - fz);
   }
 }
@@ -98,31 +98,50 @@ __device__ __forceinline__ void nrc_blob4(float s, __half *out) {
   }
 }
 
-// The 64-half input row of one query.
+// The 64-half input row of one query. Levels go in groups of four whose 32 corner loads are all
+// issued before any is summed (the gathers are latency-bound L2 reads); an entry index out of range
+// (none by construction) is clamped and flagged.
 __device__ __forceinline__ void nrc_encode(const NrcGrid &G, const NrcInput &in, __half *row) {
   const float3 q = nrc_position(G, in);
-  for (uint32_t l = 0; l < kNrcMaxLevels; ++l) {
-    float f0 = 0.0f, f1 = 0.0f;
-    if (l < G.levels) {
-      uint32_t idx[8];
-      float w[8];
-      nrc_corners(G, l, q, idx, w);
-      const float2 *lev = G.table + ((size_t)l << G.logT);
-      const uint32_t mask = (1u << G.logT) - 1u;
+  const uint32_t mask = (1u << G.logT) - 1u;
+  bool bad = false;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        if (idx[c] > mask) {
-          nrc_fault(G, kNrcBadEntry);
-          continue;
+  for (int grp = 0; grp < kNrcMaxLevels / 4; ++grp) {
+    float2 v[4][8];
+    float w[4][8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t l = 4u * grp + j;
+      if (l < G.levels) {
+        uint32_t idx[8];
+        nrc_corners(G, l, q, idx, w[j]);
+        const float2 *lev = G.table + ((size_t)l << G.logT);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          bad |= idx[c] > mask;
+          v[j][c] = __ldg(lev + min(idx[c], mask));
         }
-        const float2 v = __ldg(lev + idx[c]);
-        f0 += w[c] * v.x;
-        f1 += w[c] * v.y;
+      } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          v[j][c] = make_float2(0.0f, 0.0f);
+          w[j][c] = 0.0f;
+        }
       }
     }
-    row[2 * l] = __float2half_rn(f0);
-    row[2 * l + 1] = __float2half_rn(f1);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float f0 = 0.0f, f1 = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        f0 += w[j][c] * v[j][c].x;
+        f1 += w[j][c] * v[j][c].y;
+      }
+      row[2 * (4 * grp + j)] = __float2half_rn(f0);
+      row[2 * (4 * grp + j) + 1] = __float2half_rn(f1);
+    }
   }
+  if (bad) nrc_fault(G, kNrcBadEntry);
   nrc_blob4(in.b.x, row + 32);
   nrc_blob4(in.b.y, row + 36);
   nrc_blob4(in.b.z, row + 40);

@@ -96,9 +96,11 @@ struct RenderArgs {
   float4 *nrcT;
   uint2 *nrcBins;
   uint32_t nrcVertex;
-  // Index checks: BVH nodes and triangles; a failed check sets a bit of *status and skips the read.
-  uint32_t nodeCount, faceCount;
+  // Index checks: a hit's triangle index is clamped into the triangle array, a training record's
+  // slot into its buffers; one out of range sets a bit of *status (read back with the accumulation).
+  uint32_t faceCount;
   uint32_t *status;
+  uint32_t kernelId;  // which kernel a failed check was in (render_fault)
 };
 
 __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -111,10 +113,18 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 }
 __device__ __forceinline__ float3 normalize3(float3 a) { return mul(a, rsqrtf(dot3(a, a))); }
 
-// Status bits of the integrator's index checks (the context's status word 2).
-constexpr uint32_t kBadNode = 1u, kBadTriangle = 2u, kBadHit = 4u, kBadRecord = 8u;
-__device__ __forceinline__ void render_fault(const RenderArgs &A, uint32_t bit) {
-  if (A.status) atomicOr(A.status, bit);
+// Status bits of the integrator's index checks (the context's status word 2): a hit's triangle
+// index, a training record's slot.
+constexpr uint32_t kBadHit = 4u, kBadRecord = 8u;
+// The first failure also records its value and the kernel it happened in: status words 8-10 of
+// the context (status[6..8] here).
+__device__ __forceinline__ void render_fault(const RenderArgs &A, uint32_t bit, uint32_t value = 0u) {
+  if (!A.status) return;
+  atomicOr(A.status, bit);
+  if (atomicCAS(A.status + 6, 0u, 1u) == 0u) {
+    A.status[7] = value;
+    A.status[8] = A.kernelId | (bit << 24);
+  }
 }
 
 // ---- traversal (the 4-wide watertight traversal with a local stack) ---------------------------
@@ -123,6 +133,7 @@ struct Hit {
   int pos;  // BVH position of the triangle
 };
 
+template <bool kSel = false>
 __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, Hit &h, int *stack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -132,12 +143,7 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
   stack[top++] = 0;
   while (top > 0) {
     Node4 nd;
-    const int ni = stack[--top];
-    if ((uint32_t)ni >= A.nodeCount) {
-      render_fault(A, kBadNode);
-      break;
-    }
-    load_node(A.nodes, ni, nd);
+    load_node(A.nodes, stack[--top], nd);
     float nearT[4];
     const int mask = node_hits(nd, sr, tMin, closest, nearT);
     const Sorted4 s = sort_children(nd, mask, nearT);
@@ -146,13 +152,9 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
       if (j >= s.m || s.child[j] > 0 || beyond(s.key[j], closest)) continue;
       const int first = -s.child[j] - 1;
       for (int q = 0; q < s.count[j]; ++q) {
-        if ((uint32_t)(first + q) >= A.faceCount) {
-          render_fault(A, kBadTriangle);
-          break;
-        }
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         float t, b1, b2;
-        if (!intersect_tri(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
+        if (!intersect_tri<kSel>(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
         closest = t;
         bb1 = b1;
         bb2 = b2;
@@ -181,6 +183,7 @@ __device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) {
 // Any hit in [tMin, tMax); with `slack` (imported scenes) each triangle's own rounding bound is
 // taken off tMax, so the endpoint surface does not occlude itself (scene_occluded, main.swift:
 // 2066-2069).
+template <bool kSel = false>
 __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, int *stack, bool slack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -188,12 +191,7 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
   stack[top++] = 0;
   while (top > 0) {
     Node4 nd;
-    const int ni = stack[--top];
-    if ((uint32_t)ni >= A.nodeCount) {
-      render_fault(A, kBadNode);
-      break;
-    }
-    load_node(A.nodes, ni, nd);
+    load_node(A.nodes, stack[--top], nd);
     float nearT[4];
     const int mask = node_hits(nd, sr, tMin, tMax, nearT);
 #pragma unroll
@@ -203,14 +201,10 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
       if (c > 0) { if (top < kRenderStack) stack[top++] = c; continue; }
       const int first = -c - 1, cnt = i4(nd.count, k);
       for (int q = 0; q < cnt; ++q) {
-        if ((uint32_t)(first + q) >= A.faceCount) {
-          render_fault(A, kBadTriangle);
-          break;
-        }
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
         float t, b1, b2;
-        if (intersect_tri(wr, ta, tb, tc, tMin, slack ? tMax - mesh_hit_error(ta, tb, tc) : tMax, t, b1, b2)) return true;
+        if (intersect_tri<kSel>(wr, ta, tb, tc, tMin, slack ? tMax - mesh_hit_error(ta, tb, tc) : tMax, t, b1, b2)) return true;
       }
     }
   }
@@ -240,11 +234,8 @@ __device__ __forceinline__ float ray_tmin(const RenderArgs &A, float3 o) {
 // scenes rebuild the point from barycentrics and take the triangle's rounding bound as its error.
 __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h, float3 o, float3 d) {
   Surface s;
-  size_t hp = (size_t)h.pos;
-  if ((uint32_t)h.pos >= A.faceCount) {
-    render_fault(A, kBadHit);
-    hp = 0;
-  }
+  const size_t hp = min((uint32_t)h.pos, A.faceCount - 1u);
+  if ((uint32_t)h.pos >= A.faceCount) render_fault(A, kBadHit, (uint32_t)h.pos);
   const float4 a = __ldg(A.tris + 3 * hp), b = __ldg(A.tris + 3 * hp + 1), c = __ldg(A.tris + 3 * hp + 2);
   const float3 e1 = f3(b.x - a.x, b.y - a.y, b.z - a.z), e2 = f3(c.x - a.x, c.y - a.y, c.z - a.z);
   const float3 ng = normalize3(cross3(e1, e2));
@@ -614,6 +605,7 @@ __device__ __forceinline__ float3 ray_origin(const RenderArgs &A, float3 p, floa
 
 // light_visible (main.swift:3254-3264): shadow ray from the offset origin to the sample, shortened
 // by the endpoint tolerance (endpoint_tolerance, main.swift:1358-1361).
+template <bool kSel = false>
 __device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
                                               const LightSample &ls, int *stack) {
   if (ls.pdf <= 0.0f) return false;
@@ -624,7 +616,7 @@ __device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, flo
   const float tol = A.imported ? fmaxf(legacy, 1.907349e-6f * (max_abs(o) + max_abs(ls.pos) + d)) : legacy;
   if (d <= tol) return false;
   delta = mul(delta, 1.0f / d);
-  return !rt_any(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
+  return !rt_any<kSel>(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
 }
 
 __device__ __forceinline__ float power_heuristic(float pf, float pg) {
@@ -735,14 +727,14 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 
 // NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
-template <bool kPbr>
+template <bool kPbr, bool kSel = false>
 __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                      float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                      Sampler &seed, int *stack, bool requirePdf) {
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const LightSample ls = sample_direct(A, p, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return zero;
-  if (!light_visible(A, p, gn, err, ls, stack)) return zero;
+  if (!light_visible<kSel>(A, p, gn, err, ls, stack)) return zero;
   const float cosine = fabsf(dot3(n, ls.wi));
   if (is_pbr<kPbr>(A, m)) {
     float bpdf;
@@ -1237,7 +1229,9 @@ constexpr int kNrcRecords = 8;  // records per training path: its first 8 vertic
 // record: its cache query and, as target, the radiance the rest of the path brought to it, rgb of
 // the lanes' (R_end - R_i) / T_i, R_i the path's radiance when it reached vertex i (after that
 // vertex's emission) and T_i its throughput there. Records go to consecutive slots claimed with
-// one atomic per path; those past `cap` are dropped.
+// one atomic per path; those past `cap` are dropped. Its traversals use the select form of the
+// triangle test (intersect_tri<true>): with the array form this kernel's traversal stack read back
+// a vertex coordinate.
 template <bool kPbr>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     k_nrc_paths(RenderArgs A, uint32_t npaths, uint32_t offset, uint32_t stride, uint32_t si0, uint32_t cap,
@@ -1258,7 +1252,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
   float3 dir = camera_dir(A, x, y, jit), o = A.cam;
   lens_ray(A, o, dir, seed);
   Hit h;
-  if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return;
+  if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return;
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   Surface S = surface_at(A, h, o, dir);
   vt_material m = material(A, S.slot);
@@ -1278,7 +1272,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
   }
-  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
+  R = add4(R, direct_light_lanes<kPbr, true>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
   int scattering = 0;
   for (int bounce = 1; scattering < limit; ++bounce) {
     ++scattering;
@@ -1299,7 +1293,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     const float3 prev = S.pos;
     o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
-    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
+    if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
@@ -1314,7 +1308,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
       ++nrec;
     }
-    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
+    R = add4(R, direct_light_lanes<kPbr, true>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
                                          stack, false));
     if (bounce > 3) {
       const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
@@ -1766,9 +1760,9 @@ vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *poi
   A.rootMax = mesh->root_max;
   A.mats = scene->d_mats;
   A.nmat = scene->nmat;
-  A.nodeCount = mesh->nnodes;
   A.faceCount = mesh->nfaces;
   A.status = ctx->d_status + 2;
+  A.kernelId = 8;
   emitter_args(scene, A);
   float4 *d_points = nullptr;
   float *d_out = nullptr;
@@ -1897,7 +1891,6 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.zModel = p->z_temporal;
   A.firstFrame = p->first_frame ? p->first_frame : scene->samples + 1u;
   A.accum = scene->d_accum;
-  A.nodeCount = mesh->nnodes;
   A.faceCount = mesh->nfaces;
   emitter_args(scene, A);
 }
@@ -1998,11 +1991,15 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
       A.paspect = pc[12];
       A.pfovScale = pc[13];
       if (A.pbr) {
+        A.kernelId = 3;
         k_di_primary<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        A.kernelId = nrc ? 5 : 4;
         if (nrc) k_di_shade<true, true><<<blocks, kRenderBlock, 0, s>>>(A, k);
         else k_di_shade<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
       } else {
+        A.kernelId = 3;
         k_di_primary<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
+        A.kernelId = nrc ? 5 : 4;
         if (nrc) k_di_shade<false, true><<<blocks, kRenderBlock, 0, s>>>(A, k);
         else k_di_shade<false><<<blocks, kRenderBlock, 0, s>>>(A, k);
       }
@@ -2026,12 +2023,14 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
   const uint64_t items = (uint64_t)npix * groups;
   const uint32_t grid = (uint32_t)std::min<uint64_t>((items + kRenderBlock - 1) / kRenderBlock, (uint64_t)ctx->sm_count * 32u);
   if (nrc) {
+    A.kernelId = 2;
     if (A.pbr) k_render<true, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     else k_render<false, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     VT_CUDA(ctx, cudaGetLastError());
     const vt_status st = nrc_finish(ctx, nrc, A, spp, s);
     if (st != VT_OK) return st;
   } else {
+    A.kernelId = 1;
     if (A.pbr) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     else k_render<false><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     VT_CUDA(ctx, cudaGetLastError());
@@ -2073,6 +2072,7 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
     RenderArgs A;
     fill_args(scene, p, 1, A);
     A.status = ctx->d_status + 2;
+    A.kernelId = 6;
     const uint32_t npix = p->width * p->height;
     // A fresh pixel pattern each frame: an offset from the frame's index, pixels `stride` apart.
     const uint32_t frame = nrc->frames++;
@@ -2199,6 +2199,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     if (st != VT_OK) { batch_free(b); return st; }
     fill_args(scenes[i], params + i, spp[i], args[i]);
     args[i].status = ctx->d_status + 2;
+    args[i].kernelId = 7;
     args[i].jitter = nullptr;
     first[i] = args[i].first;
     if (args[i].pbr) b->pbr = true;
@@ -2343,12 +2344,15 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
   if (n != want) return vt_fail(ctx, VT_ERR_INVALID, "n must equal width * height * 3");
   VT_CUDA(ctx, cudaDeviceSynchronize());
   {
-    uint32_t bad = 0;
-    VT_CUDA(ctx, cudaMemcpy(&bad, ctx->d_status + 2, sizeof bad, cudaMemcpyDeviceToHost));
-    if (bad) {
-      VT_CUDA(ctx, cudaMemset(ctx->d_status + 2, 0, sizeof bad));
-      return vt_fail(ctx, VT_ERR_DEVICE, "the integrator met an out-of-range index (status " + std::to_string(bad) +
-                                             ": 1 BVH node, 2 triangle, 4 hit, 8 cache record); the accesses were skipped");
+    uint32_t w[16];
+    VT_CUDA(ctx, cudaMemcpy(w, ctx->d_status, sizeof w, cudaMemcpyDeviceToHost));
+    if (w[2]) {
+      VT_CUDA(ctx, cudaMemset(ctx->d_status + 2, 0, sizeof(uint32_t)));
+      VT_CUDA(ctx, cudaMemset(ctx->d_status + 8, 0, 3 * sizeof(uint32_t)));
+      return vt_fail(ctx, VT_ERR_DEVICE,
+                     "the integrator met an out-of-range index (status " + std::to_string(w[2]) +
+                         ": 4 hit, 8 cache record; first: value " + std::to_string(w[9]) +
+                         ", kernel " + std::to_string(w[10] & 0xffu) + "); those accesses were clamped or skipped");
     }
   }
   if (want) VT_CUDA(ctx, cudaMemcpy(rgb, scene->d_accum, want * sizeof(double), cudaMemcpyDeviceToHost));

