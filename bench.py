@@ -50,12 +50,15 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--profile", action="store_true", help="small run for ncu: no e2e, no CPU leg")
     p.add_argument("--no-cornell", action="store_true", help="skip the integrator measurement")
+    p.add_argument("--profile-nrc", action="store_true", help="short radiance-cache sequence for ncu, then exit")
     p.add_argument("--reference-spp", type=int, default=65536, help="spp of the FP64 reference image")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-launch measurement (0: skip)")
     p.add_argument("--batch-passes", type=int, default=2, help="timed batched passes after the tuning passes")
     p.add_argument("--production-frames", type=int, default=8, help="timed frames of the production scene (0: skip)")
     p.add_argument("--nrc-pretrain", type=int, default=64, help="training-only frames of the radiance cache, timed")
     p.add_argument("--nrc-max-spp", type=int, default=4096, help="spp cap of the radiance cache's relMSE runs")
+    p.add_argument("--nrc-train-every", type=int, default=1,
+                   help="after the training frames, the cache trains on every n-th rendered frame")
     p.add_argument("--nrc-records", type=int, default=16384,
                    help="cache training records per frame (a quarter of the 256x256 image's pixels)")
     return p.parse_args()
@@ -268,7 +271,8 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
         total_ms, done, err, frames = e0.elapsed_time(e1), 0, None, 0
         while done < a.nrc_max_spp:
             e0.record(stream)
-            cache.render(scene, vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp, stream=cs)
+            cache.render(scene, vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp,
+                         train=frames % a.nrc_train_every == 0, stream=cs)
             e1.record(stream)
             torch.cuda.synchronize()
             total_ms += e0.elapsed_time(e1)
@@ -295,6 +299,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
                     f"{name}_loss": ci["last_loss"]})
     nrc["nrc_pretrain_frames"] = a.nrc_pretrain
     nrc["nrc_train_records"] = a.nrc_records
+    nrc["nrc_train_every"] = a.nrc_train_every
     nrc["nrc_restir_speedup_vs_plain"] = (pt_s / nrc["nrc_restir_s"]) if (pt_s and nrc["nrc_restir_s"]) else None
     out["time_to_relmse_1e-3"] = {
         "plain_pt_s": pt_s, "spp": pt_spp, "relmse": pt_err,
@@ -410,8 +415,33 @@ def bench_production(a, ctx, stream) -> dict:
 
 
 # ---- our arm ----------------------------------------------------------------------------------
+def profile_nrc(a) -> int:
+    """A short radiance-cache sequence for ncu: the spectral Cornell box at 256 x 256, a cache with
+    `--nrc-records` records per frame, 4 training frames, then 3 cached 16-spp frames (MIS primary
+    vertex) and one plain 16-spp frame."""
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes, spectral_tables
+    from metal_vibe_tracer_b200.nrc import RadianceCache
+    ctx = vt.Context(0)
+    faces, verts, mats, light, cam = scenes.cornell_box()
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, light, spectral_tables.load())
+    info = mesh.info()
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records)
+    for f in range(4):
+        cache.render(scene, vt.make_params(cam, 256, 256, 8, 1 + f, True, 1), 0, render=False)
+    for f in range(3):
+        cache.render(scene, vt.make_params(cam, 256, 256, 8, 1 + 16 * f, True, 1), 16)
+    scene.render(vt.make_params(cam, 256, 256, 8, 1000, True, 1), 16)
+    img, n = scene.readback()
+    print(json.dumps({"profile_nrc": "ok", "samples": n, "mean": float(img.mean())}))
+    return 0
+
+
 def main():
     a = parse()
+    if a.profile_nrc:
+        return profile_nrc(a)
     if a.profile:
         a.no_e2e = True
         a.no_cpu_baseline = True

@@ -416,7 +416,8 @@ vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *poi
  * the outgoing direction, the shading normal and the roughness, and the reflectances, into an MLP
  * of 5 hidden layers 64 wide (fp16 operands, fp32 accumulation, ReLU) with 3 linear outputs: the
  * radiance leaving the vertex toward the previous one, without the vertex's own emission, in linear
- * sRGB. Trained online by Adam under the relative L2 loss on the suffix radiance of training paths
+ * sRGB. Trained online by Adam (lazy for the hash grid: an entry without gradient in a step keeps
+ * its moments) under the relative L2 loss on the suffix radiance of training paths
  * that the integrator traces to full depth. */
 typedef struct vt_nrc vt_nrc;
 typedef struct vt_nrc_config {

@@ -391,15 +391,19 @@ __global__ void __launch_bounds__(kNrcTile, 1) k_nrc_train(NrcGrid G, const floa
 }
 
 // Adam on params p with moments m, v and gradient sums g (zeroed after use), the batch being
-// min(*count, cap) rows; lr already carries the bias corrections.
+// min(*count, cap) rows; lr already carries the bias corrections. Grid entries (from float4 `dense4`
+// on) whose four gradients are all zero are left as they are (lazy Adam, as for embedding tables:
+// a step touches a few percent of the hash grid, and the dense update would stream all of it).
 __global__ void k_nrc_adam(float4 *__restrict__ p, float4 *__restrict__ m, float4 *__restrict__ v,
-                           float4 *__restrict__ gsum, uint64_t n4, const uint32_t *__restrict__ count, uint32_t cap,
-                           float lr, float beta1, float beta2, float eps) {
+                           float4 *__restrict__ gsum, uint64_t n4, uint64_t dense4, const uint32_t *__restrict__ count,
+                           uint32_t cap, float lr, float beta1, float beta2, float eps) {
   const uint32_t rows = count ? min(*count, cap) : cap;
   if (rows == 0u) return;
   const float scale = 1.0f / float(rows);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
-    float4 gg = gsum[i], mm = m[i], vv = v[i], pp = p[i];
+    float4 gg = gsum[i];
+    if (i >= dense4 && gg.x == 0.0f && gg.y == 0.0f && gg.z == 0.0f && gg.w == 0.0f) continue;
+    float4 mm = m[i], vv = v[i], pp = p[i];
     float *gp = &gg.x, *mp = &mm.x, *vp = &vv.x, *pq = &pp.x;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -492,7 +496,8 @@ vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s) {
   const uint32_t blocks = (uint32_t)std::min<uint64_t>((n4 + 255) / 256, (uint64_t)ctx->sm_count * 8u);
   k_nrc_adam<<<blocks, 256, 0, s>>>(reinterpret_cast<float4 *>(nrc->d_p), reinterpret_cast<float4 *>(nrc->d_m),
                                     reinterpret_cast<float4 *>(nrc->d_v), reinterpret_cast<float4 *>(nrc->d_g), n4,
-                                    nrc->d_count, cap, (float)lr, nrc->cfg.beta1, nrc->cfg.beta2, nrc->cfg.epsilon);
+                                    kNrcMlpParams / 4, nrc->d_count, cap, (float)lr, nrc->cfg.beta1, nrc->cfg.beta2,
+                                    nrc->cfg.epsilon);
   VT_CUDA(ctx, cudaGetLastError());
   return VT_OK;
 }
