@@ -85,10 +85,10 @@ __device__ __forceinline__ void acc_to_a(const float (&acc)[2][8][4], uint32_t (
     for (int kk = 0; kk < 4; ++kk) {
       const float *c0 = acc[mt][2 * kk], *c1 = acc[mt][2 * kk + 1];
       if (relu) {
-        a[mt][kk][0] = nrc_pack(fmaxf(c0[0], 0.0f), fmaxf(c0[1], 0.0f));
-        a[mt][kk][1] = nrc_pack(fmaxf(c0[2], 0.0f), fmaxf(c0[3], 0.0f));
-        a[mt][kk][2] = nrc_pack(fmaxf(c1[0], 0.0f), fmaxf(c1[1], 0.0f));
-        a[mt][kk][3] = nrc_pack(fmaxf(c1[2], 0.0f), fmaxf(c1[3], 0.0f));
+        a[mt][kk][0] = nrc_pack_relu(c0[0], c0[1]);
+        a[mt][kk][1] = nrc_pack_relu(c0[2], c0[3]);
+        a[mt][kk][2] = nrc_pack_relu(c1[0], c1[1]);
+        a[mt][kk][3] = nrc_pack_relu(c1[2], c1[3]);
       } else {
         a[mt][kk][0] = nrc_pack(c0[0], c0[1]);
         a[mt][kk][1] = nrc_pack(c0[2], c0[3]);
@@ -586,6 +586,15 @@ vt_status vt_nrc_create(vt_ctx *ctx, const vt_nrc_config *cfg, const float lo[3]
   }
   G.table = reinterpret_cast<float2 *>(n->d_p + kNrcMlpParams);
   G.status = ctx->d_status + 3;
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&n->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&n->ev_start, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&n->ev_paths, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      vt_nrc_destroy(ctx, n);
+      return vt_cuda_fail(ctx, e, "creating the cache's side stream");
+    }
+  }
   cudaError_t e = cudaMemsetAsync(n->d_m, 0, bytes, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(n->d_v, 0, bytes, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(n->d_g, 0, bytes, ctx->stream);
@@ -615,6 +624,9 @@ vt_status vt_nrc_destroy(vt_ctx *ctx, vt_nrc *nrc) {
                   (void *)nrc->d_loss, (void *)nrc->d_tin, (void *)nrc->d_ttarget, (void *)nrc->d_q, (void *)nrc->d_qT,
                   (void *)nrc->d_qbins, (void *)nrc->d_qout, (void *)nrc->d_scratch})
     cudaFree(p);
+  if (nrc->ev_start) cudaEventDestroy(nrc->ev_start);
+  if (nrc->ev_paths) cudaEventDestroy(nrc->ev_paths);
+  if (nrc->side) cudaStreamDestroy(nrc->side);
   delete nrc;
   return VT_OK;
 }

@@ -58,29 +58,29 @@ __device__ __forceinline__ void nrc_fault(const NrcGrid &G, uint32_t bit) {
 
 __device__ __forceinline__ float nrc_sat(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }  // NaN -> 0
 
-// Corner index of level `l` at integer grid point (x, y, z): dense while (res + 1)^3 fits the
-// table, else the spatial hash x ^ y * 2654435761 ^ z * 805459861 modulo the table size.
-__device__ __forceinline__ uint32_t nrc_index(const NrcGrid &G, uint32_t l, uint32_t res, uint32_t x, uint32_t y,
-                                              uint32_t z) {
-  const uint32_t side = res + 1u;
-  if ((G.dense >> l) & 1u) return x + side * (y + side * z);
-  return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & ((1u << G.logT) - 1u);
-}
-
 // The 8 corners of level l around normalised position q: entry indices (within the level) and
-// trilinear weights.
+// trilinear weights. Corner c is (cx + (c & 1), cy + (c >> 1 & 1), cz + (c >> 2)); the hash terms of
+// y and z and the dense strides are formed once per level.
 __device__ __forceinline__ void nrc_corners(const NrcGrid &G, uint32_t l, float3 q, uint32_t (&idx)[8], float (&w)[8]) {
   const uint32_t res = G.res[l];
   const float fr = float(res);
   const float x = q.x * fr, y = q.y * fr, z = q.z * fr;
   const uint32_t cx = min((uint32_t)x, res - 1u), cy = min((uint32_t)y, res - 1u), cz = min((uint32_t)z, res - 1u);
   const float fx = x - float(cx), fy = y - float(cy), fz = z - float(cz);
+  const float wx[2] = {1.0f - fx, fx}, wy[2] = {1.0f - fy, fy}, wz[2] = {1.0f - fz, fz};
+  if ((G.dense >> l) & 1u) {
+    const uint32_t side = res + 1u, plane = side * side, base = cx + side * cy + plane * cz;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const uint32_t dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-    idx[c] = nrc_index(G, l, res, cx + dx, cy + dy, cz + dz);
-    w[c] = (dx ? fx : 1.0f - fx) * (dy ? fy : 1.0f - fy) * (dz ? fz : 1.0f - fz);
+    for (int c = 0; c < 8; ++c) idx[c] = base + (c & 1) + ((c >> 1) & 1) * side + (c >> 2) * plane;
+  } else {
+    const uint32_t mask = (1u << G.logT) - 1u;
+    const uint32_t hy[2] = {cy * 2654435761u, (cy + 1u) * 2654435761u};
+    const uint32_t hz[2] = {cz * 805459861u, (cz + 1u) * 805459861u};
+#pragma unroll
+    for (int c = 0; c < 8; ++c) idx[c] = ((cx + (c & 1)) ^ hy[(c >> 1) & 1] ^ hz[c >> 2]) & mask;
   }
+#pragma unroll
+  for (int c = 0; c < 8; ++c) w[c] = (wx[c & 1] * wy[(c >> 1) & 1]) * wz[c >> 2];
 }
 
 __device__ __forceinline__ float3 nrc_position(const NrcGrid &G, const NrcInput &in) {
@@ -182,6 +182,12 @@ __device__ __forceinline__ void nrc_ldsm4t(uint32_t (&r)[4], const __half *p) {
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                : "r"(s));
 }
+// max(0, x) of two floats as a half2 register (lo in the low 16 bits), one conversion instruction.
+__device__ __forceinline__ uint32_t nrc_pack_relu(float lo, float hi) {
+  uint32_t r;
+  asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+  return r;
+}
 // Two floats as a half2 register (lo in the low 16 bits), clamped to the finite fp16 range.
 __device__ __forceinline__ uint32_t nrc_pack(float lo, float hi) {
   lo = fminf(fmaxf(lo, -65504.0f), 65504.0f);
@@ -214,6 +220,9 @@ struct vt_nrc {
   uint2 *d_qbins = nullptr;
   float4 *d_qout = nullptr;
   size_t qcap = 0;
+  // A frame that trains and renders traces its training paths on `side`, beside the rendering.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_paths = nullptr;
 };
 
 // One optimiser step on the records in d_tin / d_ttarget (d_count[0] of them, at most cap).

@@ -2062,6 +2062,15 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  // Training and rendering: the training paths run on the cache's side stream beside the frame's
+  // rendering (which reads the parameters of the previous step); the step follows both.
+  const bool both = (flags & VT_NRC_TRAIN) && (flags & VT_NRC_RENDER) && scene->mesh->nfaces > 0;
+  cudaStream_t ps = s;
+  if (both) {
+    VT_CUDA(ctx, cudaEventRecord(nrc->ev_start, s));
+    VT_CUDA(ctx, cudaStreamWaitEvent(nrc->side, nrc->ev_start, 0));
+    ps = nrc->side;
+  }
   if ((flags & VT_NRC_TRAIN) && scene->mesh->nfaces > 0) {
     const uint32_t cap = nrc->cfg.train_records;
     const uint32_t npaths = nrc->cfg.train_paths ? nrc->cfg.train_paths : std::max(1u, cap / 4u);
@@ -2079,7 +2088,7 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
     uint32_t h = nrc->cfg.seed ^ (frame * 0x9e3779b9u);
     h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
     const uint32_t stride = std::max(1u, npix / npaths);
-    VT_CUDA(ctx, cudaMemsetAsync(nrc->d_count, 0, sizeof(uint32_t), s));
+    VT_CUDA(ctx, cudaMemsetAsync(nrc->d_count, 0, sizeof(uint32_t), ps));
     const uint32_t si0 = 0x40000000u + (frame << 8);
     const size_t scratch = (size_t)npaths * kNrcRecords * 5;
     if (scratch > nrc->scratch_cap) {
@@ -2091,18 +2100,29 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
     }
     const unsigned blocks = (npaths + kRenderBlock - 1) / kRenderBlock;
     if (A.pbr)
-      k_nrc_paths<true><<<blocks, kRenderBlock, 0, s>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
+      k_nrc_paths<true><<<blocks, kRenderBlock, 0, ps>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
                                                         nrc->scratch_cap, nrc->d_tin, nrc->d_ttarget, nrc->tcap,
                                                         nrc->d_count);
     else
-      k_nrc_paths<false><<<blocks, kRenderBlock, 0, s>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
+      k_nrc_paths<false><<<blocks, kRenderBlock, 0, ps>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
                                                          nrc->scratch_cap, nrc->d_tin, nrc->d_ttarget, nrc->tcap,
                                                          nrc->d_count);
     VT_CUDA(ctx, cudaGetLastError());
-    const vt_status st = vt_nrc_step(ctx, nrc, cap, s);
-    if (st != VT_OK) return st;
+    if (!both) {
+      const vt_status st = vt_nrc_step(ctx, nrc, cap, s);
+      if (st != VT_OK) return st;
+    }
   }
-  if (flags & VT_NRC_RENDER) return render_impl(ctx, scene, p, spp, stream, nrc);
+  if (flags & VT_NRC_RENDER) {
+    const vt_status st = render_impl(ctx, scene, p, spp, stream, nrc);
+    if (both) {
+      VT_CUDA(ctx, cudaEventRecord(nrc->ev_paths, nrc->side));
+      VT_CUDA(ctx, cudaStreamWaitEvent(s, nrc->ev_paths, 0));
+      if (st != VT_OK) return st;
+      return vt_nrc_step(ctx, nrc, nrc->cfg.train_records, s);
+    }
+    return st;
+  }
   return VT_OK;
 }
 
