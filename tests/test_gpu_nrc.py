@@ -137,3 +137,31 @@ def test_render_nrc_rejects_other_modes(ctx, cornell_scene):
     with pytest.raises(vt.MaterialLibraryError, match="query_vertex"):
         RadianceCache(ctx, list(info.lo), list(info.hi), query_vertex=0)
     cache.close()
+
+
+def test_cached_openpbr_cornell(ctx):
+    """The OpenPBR variants of the cache's kernels (training paths, cache-terminated paths with MIS and
+    ReSTIR DI primaries): a trained cache's image of the OpenPBR Cornell box within 4 % of the path
+    tracer's mean radiance."""
+    faces, verts, mats, light, cam = scenes.cornell_openpbr()
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, light, spectral_tables.load())
+    W = H = 64
+    scene.render(vt.make_params(cam, W, H, 8, 1, True, 1), 1024)
+    ref, _ = scene.readback()
+    info = mesh.info()
+    for mode in (1, 0):
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=5)
+        scene.reset()
+        for f in range(120):
+            cache.render(scene, vt.make_params(cam, W, H, 8, 1 + f, True, mode), 0, render=False)
+        scene.reset()
+        for f in range(16):
+            cache.render(scene, vt.make_params(cam, W, H, 8, 7001 + 16 * f, True, mode), 16)
+        img, n = scene.readback()
+        assert n == 256 and np.isfinite(img).all()
+        gm, rm = img.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+        assert np.all(np.abs(gm / rm - 1) < 0.04), (mode, gm, rm)
+        cache.close()
+    scene.close()
+    mesh.close()
