@@ -410,6 +410,28 @@ vt_status vt_scene_emitter_words(vt_ctx *ctx, const vt_scene *scene, uint32_t *w
 vt_status vt_light_estimate(vt_ctx *ctx, const vt_scene *scene, const float *points, uint32_t npoints,
                             uint32_t per_point, uint32_t samples, float *out);
 
+/* ---- environment of imported scenes ------------------------------------------------------------
+ * The reference's procedural sky and sun for sceneIndex 6 (eval_procedural_sky, main.swift:541-597;
+ * eval_environment, :2127-2134): three presets of sky gradient with a sun lobe and a sun disc.
+ * Next-event estimation splits its samples between the emitter triangles (half of them when both
+ * exist, imported_light_probability, :2716-2719) and the environment (the sun cone with probability
+ * 0.6 while the sun is above the horizon, else a cosine lobe about the receiver's normal,
+ * :2922-2955); rays that escape pick up the environment with the power-heuristic weight against that
+ * density (:7751-7756) and camera rays that miss see it directly (:7453-7455). Spectral transport
+ * upsamples it as a D65-relative colour. Not built: image maps (environment.z), their rotation, the
+ * compensated sampling tables, imported DistantLight suns and other sun illuminants. */
+typedef struct vt_environment {
+  float intensity;      /* Uniforms.environment.x: the sky's scale; 0 = no environment */
+  float sun_dir[3];     /* Uniforms.sunParams.xyz, toward the sun (normalised by the library) */
+  float sun_intensity;  /* Uniforms.sunParams.w: the disc's brightness; 0 = no sun disc or sun sampling */
+  uint32_t sky_mode;    /* Uniforms.skyMode: 0 golden hour, 1 high noon, 2 twilight */
+  uint32_t pad[2];
+} vt_environment;
+/* Sets (or with NULL / intensity 0 clears) an imported scene's environment; restarts its
+ * accumulation. Sampling modes 1-3 only: ReSTIR DI (mode 0) and vt_render_nrc reject a scene with an
+ * environment. */
+vt_status vt_scene_set_environment(vt_ctx *ctx, vt_scene *scene, const vt_environment *env);
+
 /* ---- neural radiance cache (nrc.cu) -------------------------------------------------------------
  * No counterpart in the reference (it has no radiance cache). A radiance cache after Mueller et al.
  * 2021: a multiresolution hash grid of the position (Mueller et al. 2022) plus one-blob encodings of

@@ -78,6 +78,11 @@ class BatchStats(C.Structure):
                 ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
 
 
+class Environment(C.Structure):
+    _fields_ = [("intensity", C.c_float), ("sun_dir", C.c_float * 3), ("sun_intensity", C.c_float),
+                ("sky_mode", C.c_uint32), ("pad", C.c_uint32 * 2)]
+
+
 class NRCConfig(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
                 ("max_resolution", C.c_uint32), ("train_records", C.c_uint32), ("train_paths", C.c_uint32),
@@ -153,6 +158,7 @@ SIGNATURES = {
     "vt_openpbr_energy_table": (_I32, [_P, _P, _P]),
     "vt_openpbr_evaluate": (_I32, [_P, _P, _U32, _P]),
     "vt_scene_set_openpbr": (_I32, [_P, _P, _P, _U32]),
+    "vt_scene_set_environment": (_I32, [_P, _P, C.POINTER(Environment)]),
     "vt_nrc_config_default": (_I32, [C.POINTER(NRCConfig)]),
     "vt_nrc_create": (_I32, [_P, C.POINTER(NRCConfig), _P, _P, C.POINTER(_P)]),
     "vt_nrc_destroy": (_I32, [_P, _P]),

@@ -75,6 +75,12 @@ struct RenderArgs {
   const float4 *emissions;   // per slot: emission rgb, selection weight
   const int32_t *facePos;    // input face -> BVH position
   uint32_t ecount, treeNodes;
+  // Procedural sky and sun of imported scenes (Uniforms.environment.x, sunParams, skyMode); env = 1
+  // when the sky's intensity is positive.
+  int env;
+  float envIntensity, sunIntensity;
+  float3 sunDir;
+  uint32_t skyMode;
   float etotal;
   const uint4 *ltNodes;
   const uint32_t *ltLeaves;
@@ -115,7 +121,7 @@ __device__ __forceinline__ float3 normalize3(float3 a) { return mul(a, rsqrtf(do
 
 // Status bits of the integrator's index checks (the context's status word 2): a hit's triangle
 // index, a training record's slot.
-constexpr uint32_t kBadHit = 4u, kBadRecord = 8u;
+constexpr uint32_t kBadHit = 4u, kBadRecord = 8u, kBadEmitter = 16u;
 // The first failure also records its value and the kernel it happened in: status words 8-10 of
 // the context (status[6..8] here).
 __device__ __forceinline__ void render_fault(const RenderArgs &A, uint32_t bit, uint32_t value = 0u) {
@@ -133,7 +139,7 @@ struct Hit {
   int pos;  // BVH position of the triangle
 };
 
-template <bool kSel = false>
+template <bool kSel = true>
 __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, Hit &h, int *stack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -183,7 +189,7 @@ __device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) {
 // Any hit in [tMin, tMax); with `slack` (imported scenes) each triangle's own rounding bound is
 // taken off tMax, so the endpoint surface does not occlude itself (scene_occluded, main.swift:
 // 2066-2069).
-template <bool kSel = false>
+template <bool kSel = true>
 __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, int *stack, bool slack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -373,7 +379,16 @@ struct Tri {
 };
 
 __device__ __forceinline__ Tri scene_triangle(const RenderArgs &A, uint32_t face) {
-  const float4 *t = A.tris + 3 * (size_t)__ldg(A.facePos + face);
+  if (face >= A.faceCount) {
+    render_fault(A, kBadEmitter, face);
+    face = 0;
+  }
+  uint32_t pos = __ldg(A.facePos + face);
+  if (pos >= A.faceCount) {
+    render_fault(A, kBadEmitter, pos);
+    pos = 0;
+  }
+  const float4 *t = A.tris + 3 * (size_t)pos;
   const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
   return Tri{f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), __float_as_uint(b.w)};
 }
@@ -546,13 +561,128 @@ __device__ __forceinline__ float emitter_area_pdf(const RenderArgs &A, uint32_t 
 
 // sample_direct_light's emitter branch (main.swift:2892-2920), with the emitter probability 1 (no
 // environment): the choice draw, then one 3D draw (emitter, point on it).
-__device__ LightSample sample_emitters(const RenderArgs &A, float3 p, Sampler &seed) {
+__device__ __forceinline__ void make_basis(float3 n, float3 &u, float3 &v) {
+  const float3 up = fabsf(n.z) < 0.999f ? f3(0.0f, 0.0f, 1.0f) : f3(1.0f, 0.0f, 0.0f);
+  u = normalize3(cross3(up, n));
+  v = cross3(n, u);
+}
+
+// sample_cosine_hemisphere (main.swift:2462-2472).
+__device__ __forceinline__ float3 cosine_hemisphere(float3 n, float r0, float r1) {
+  const float phi = kTwoPi * r0;
+  const float cos_th = sqrtf(r1 + (0.5f / 16777216.0f));
+  const float sin_th = sqrtf(fmaxf(0.0f, 1.0f - cos_th * cos_th));
+  float3 u, v;
+  make_basis(n, u, v);
+  float s, c;
+  sincosf(phi, &s, &c);
+  return normalize3(add(add(mul(u, c * sin_th), mul(v, s * sin_th)), mul(n, cos_th)));
+}
+
+// ---- procedural sky and sun (imported scenes) ----------------------------------------------------
+constexpr uint32_t kEnvFace = 0xfffffffeu;  // LightSample.face of an environment sample
+constexpr float kPiF = 3.14159265358979323846f;
+
+// in_sun_cone (main.swift:522-525): sin^2 through a cross product, for sub-degree cones.
+__device__ __forceinline__ bool in_sun_cone(float3 d, float3 sunDir, float oneMinusCos) {
+  const float3 c = cross3(d, sunDir);
+  return dot3(d, sunDir) > 0.0f && dot3(c, c) <= oneMinusCos * (2.0f - oneMinusCos);
+}
+// procedural_sun_one_minus_cos (main.swift:527-529).
+__device__ __forceinline__ float sun_one_minus_cos(uint32_t skyMode) {
+  return skyMode == 0u ? 8e-4f : (skyMode == 1u ? 7e-4f : 9e-4f);
+}
+__device__ __forceinline__ float3 mix3(float3 a, float3 b, float t) { return add(a, mul(sub(b, a), t)); }
+
+// eval_procedural_sky (main.swift:541-597): three presets of horizon-to-zenith gradients with a Mie
+// lobe and a sun disc of brightness sunIntensity above the horizon, a darkened ground below.
+__device__ float3 procedural_sky(const RenderArgs &A, float3 d) {
+  const float sunCos = dot3(d, A.sunDir), y = d.y;
+  float3 zenith, horizon, ground, lobe, disc;
+  float gradient, lobePower, lobeGain, discGain, groundPower, groundScale, gain;
+  if (A.skyMode == 0u) {
+    zenith = f3(0.08f, 0.18f, 0.46f); horizon = f3(0.96f, 0.52f, 0.22f); ground = f3(0.12f, 0.10f, 0.08f);
+    lobe = f3(1.0f, 0.70f, 0.30f); disc = f3(1.0f, 0.78f, 0.45f);
+    gradient = 0.40f; lobePower = 6.0f; lobeGain = 3.0f; discGain = 0.45f; groundPower = 5.0f; groundScale = 0.35f;
+    gain = 1.5f;
+  } else if (A.skyMode == 1u) {
+    zenith = f3(0.16f, 0.42f, 0.92f); horizon = f3(0.74f, 0.85f, 0.96f); ground = f3(0.14f, 0.15f, 0.12f);
+    lobe = f3(1.0f, 0.98f, 0.92f); disc = f3(1.0f, 0.98f, 0.94f);
+    gradient = 0.48f; lobePower = 12.0f; lobeGain = 2.2f; discGain = 0.40f; groundPower = 4.0f; groundScale = 0.40f;
+    gain = 1.8f;
+  } else {
+    zenith = f3(0.04f, 0.06f, 0.14f); horizon = f3(0.46f, 0.26f, 0.42f); ground = f3(0.04f, 0.04f, 0.05f);
+    lobe = f3(0.95f, 0.65f, 0.75f); disc = f3(1.0f, 0.85f, 0.78f);
+    gradient = 0.55f; lobePower = 10.0f; lobeGain = 1.8f; discGain = 0.35f; groundPower = 3.0f; groundScale = 0.25f;
+    gain = 1.6f;
+  }
+  float3 col;
+  if (y >= 0.0f) {
+    col = mix3(horizon, zenith, powf(y, gradient));
+    col = add(col, mul(lobe, powf(fmaxf(0.0f, sunCos), lobePower) * lobeGain));
+    if (in_sun_cone(d, A.sunDir, sun_one_minus_cos(A.skyMode))) col = add(col, mul(disc, A.sunIntensity * discGain));
+  } else {
+    col = mix3(ground, mul(horizon, groundScale), powf(1.0f + y, groundPower));
+  }
+  return mul(col, gain);
+}
+// eval_environment (main.swift:2127-2134) without an image map or an imported sun.
+__device__ __forceinline__ float3 environment(const RenderArgs &A, float3 d) {
+  return mul(procedural_sky(A, d), A.envIntensity);
+}
+// imported_light_probability (main.swift:2716-2719): emitters and the environment share NEE.
+__device__ __forceinline__ float imported_probability(const RenderArgs &A) {
+  if (A.ecount == 0u) return 0.0f;
+  return A.env ? 0.5f : 1.0f;
+}
+// environment_sun_probability (main.swift:2700-2706) for the procedural sun: 0.6 while the disc is above
+// the horizon.
+__device__ __forceinline__ float sun_probability(const RenderArgs &A) {
+  if (!(A.sunIntensity > 0.0f) || !A.env) return 0.0f;
+  const float w = sun_one_minus_cos(A.skyMode);
+  return A.sunDir.y >= -sqrtf(w * (2.0f - w)) ? 0.60f : 0.0f;
+}
+// eval_environment_pdf (main.swift:2880-2883, environment_mixture_pdf :2707-2712): the sun cone and a
+// cosine lobe about the receiver's normal n, times the environment's share of NEE.
+__device__ __forceinline__ float environment_pdf(const RenderArgs &A, float3 wi, float3 n) {
+  const float sp = sun_probability(A), w = sun_one_minus_cos(A.skyMode);
+  const float sunPdf = in_sun_cone(wi, A.sunDir, w) ? 1.0f / (kTwoPi * w) : 0.0f;
+  const float rest = fmaxf(0.0f, dot3(n, wi)) * kInvPi;
+  return (1.0f - imported_probability(A)) * (sp * sunPdf + (1.0f - sp) * rest);
+}
+
+// sample_direct_light's imported branch (main.swift:2889-2955): an emitter triangle with probability
+// imported_probability, else the environment (the sun cone with probability sun_probability, else a
+// cosine lobe about n).
+__device__ LightSample sample_emitters(const RenderArgs &A, float3 p, float3 n, Sampler &seed) {
   LightSample ls;
   ls.pdf = 0.0f;
   ls.face = 0xffffffffu;
   ls.emission = f3(0.0f, 0.0f, 0.0f);
-  if (A.ecount == 0u) return ls;
-  (void)rand_f(seed);  // rand_f(seed) < importedProbability (= 1)
+  const float ip = imported_probability(A);
+  if (!(ip > 0.0f) && !A.env) return ls;
+  if (!(ip > 0.0f && rand_f(seed) < ip)) {
+    const float sp = sun_probability(A);
+    const float3 q = sp > 0.0f ? rand_f3(seed) : f3(1.0f, 1.0f, 1.0f);
+    if (sp > 0.0f && q.x < sp) {
+      const float oneMinusCos = q.y * sun_one_minus_cos(A.skyMode);
+      const float cosTh = 1.0f - oneMinusCos, sinTh = sqrtf(fmaxf(0.0f, oneMinusCos * (2.0f - oneMinusCos)));
+      float3 su, sv;
+      make_basis(A.sunDir, su, sv);
+      float sn, cs;
+      sincosf(kTwoPi * q.z, &sn, &cs);
+      ls.wi = normalize3(add(add(mul(su, cs * sinTh), mul(sv, sn * sinTh)), mul(A.sunDir, cosTh)));
+    } else {
+      const float2 r = sp > 0.0f ? make_float2(q.y, q.z) : rand_f2(seed);
+      ls.wi = cosine_hemisphere(n, r.x, r.y);
+    }
+    ls.pos = add(p, mul(ls.wi, 1e6f));
+    ls.dist = 1e6f;
+    ls.face = kEnvFace;
+    ls.pdf = environment_pdf(A, ls.wi, n);
+    ls.emission = environment(A, ls.wi);
+    return ls;
+  }
   const float3 q = rand_f3(seed);
   const bool tree = A.treeNodes > 0u;
   float pmf = 0.0f;
@@ -581,7 +711,7 @@ __device__ LightSample sample_emitters(const RenderArgs &A, float3 p, Sampler &s
   ls.face = face;
   const float area = tree ? triangle_area(t) : 0.0f;
   const float areaPdf = !tree ? emitter_area_pdf(A, face, p, t) : (area > 0.0f ? pmf / area : 0.0f);
-  ls.pdf = geometry > 1e-12f ? areaPdf / geometry : 0.0f;
+  ls.pdf = geometry > 1e-12f ? ip * areaPdf / geometry : 0.0f;
   return ls;
 }
 
@@ -590,11 +720,11 @@ __device__ __forceinline__ float emitter_pdf(const RenderArgs &A, float3 p, floa
   if (A.ecount == 0u) return 0.0f;
   const Tri t = scene_triangle(A, face);
   const float g = imported_geometry(p, hitPos, t);
-  return g > 1e-12f ? emitter_area_pdf(A, face, p, t) / g : 0.0f;
+  return g > 1e-12f ? imported_probability(A) * emitter_area_pdf(A, face, p, t) / g : 0.0f;
 }
 
-__device__ __forceinline__ LightSample sample_direct(const RenderArgs &A, float3 p, Sampler &seed) {
-  return A.imported ? sample_emitters(A, p, seed) : sample_light(A, p, seed);
+__device__ __forceinline__ LightSample sample_direct(const RenderArgs &A, float3 p, float3 n, Sampler &seed) {
+  return A.imported ? sample_emitters(A, p, n, seed) : sample_light(A, p, seed);
 }
 
 // ray_origin (main.swift:1366-1369): offset along the geometric normal by max(error, epsilon).
@@ -605,7 +735,7 @@ __device__ __forceinline__ float3 ray_origin(const RenderArgs &A, float3 p, floa
 
 // light_visible (main.swift:3254-3264): shadow ray from the offset origin to the sample, shortened
 // by the endpoint tolerance (endpoint_tolerance, main.swift:1358-1361).
-template <bool kSel = false>
+template <bool kSel = true>
 __device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
                                               const LightSample &ls, int *stack) {
   if (ls.pdf <= 0.0f) return false;
@@ -626,24 +756,6 @@ __device__ __forceinline__ float power_heuristic(float pf, float pg) {
   return f * f / (f * f + g * g);
 }
 
-__device__ __forceinline__ void make_basis(float3 n, float3 &u, float3 &v) {
-  const float3 up = fabsf(n.z) < 0.999f ? f3(0.0f, 0.0f, 1.0f) : f3(1.0f, 0.0f, 0.0f);
-  u = normalize3(cross3(up, n));
-  v = cross3(n, u);
-}
-
-// sample_cosine_hemisphere (main.swift:2462-2472).
-__device__ __forceinline__ float3 cosine_hemisphere(float3 n, float r0, float r1) {
-  const float phi = kTwoPi * r0;
-  const float cos_th = sqrtf(r1 + (0.5f / 16777216.0f));
-  const float sin_th = sqrtf(fmaxf(0.0f, 1.0f - cos_th * cos_th));
-  float3 u, v;
-  make_basis(n, u, v);
-  float s, c;
-  sincosf(phi, &s, &c);
-  return normalize3(add(add(mul(u, c * sin_th), mul(v, s * sin_th)), mul(n, cos_th)));
-}
-
 // Reflectance / emission as a 4-lane spectrum (spectral) or rgb in xyz (RGB transport). A slot's
 // material carries its index in `pad`; a slot out of range (material()'s black default) has none.
 __device__ __forceinline__ float4 reflectance(const RenderArgs &A, const Lanes &L, const vt_material &m) {
@@ -656,6 +768,10 @@ __device__ __forceinline__ float4 reflectance(const RenderArgs &A, const Lanes &
 __device__ __forceinline__ float4 emission(const RenderArgs &A, const Lanes &L, const float e[3]) {
   if (A.spectral) return lanes_emission(A, L, make_float3(e[0], e[1], e[2]));
   return make_float4(e[0], e[1], e[2], 0.0f);
+}
+__device__ __forceinline__ float4 emission3(const RenderArgs &A, const Lanes &L, float3 e) {
+  if (A.spectral) return lanes_emission(A, L, e);
+  return make_float4(e.x, e.y, e.z, 0.0f);
 }
 __device__ __forceinline__ float3 to_rgb(const RenderArgs &A, const Lanes &L, float4 s) {
   return A.spectral ? lanes_rgb(A, L, s) : f3(s.x, s.y, s.z);
@@ -727,12 +843,12 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 
 // NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
-template <bool kPbr, bool kSel = false>
+template <bool kPbr, bool kSel = true>
 __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                      float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                      Sampler &seed, int *stack, bool requirePdf) {
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const LightSample ls = sample_direct(A, p, seed);
+  const LightSample ls = sample_direct(A, p, n, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return zero;
   if (!light_visible<kSel>(A, p, gn, err, ls, stack)) return zero;
   const float cosine = fabsf(dot3(n, ls.wi));
@@ -758,11 +874,11 @@ __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const 
   return scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
 }
 // The same as rgb.
-template <bool kPbr>
+template <bool kPbr, bool kSel = true>
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                Sampler &seed, int *stack, bool requirePdf) {
-  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
+  return to_rgb(A, L, direct_light_lanes<kPbr, kSel>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
 }
 
 // ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
@@ -943,7 +1059,7 @@ __device__ __forceinline__ void nrc_store_none(const RenderArgs &A, size_t slot)
 
 // kNrc (vt_render_nrc): the path ends at vertex A.nrcVertex, after that vertex's emission, with
 // its cache query stored in `slot`; `queried` tells whether it got there.
-template <bool kPbr, bool kNrc = false>
+template <bool kPbr, bool kNrc = false, bool kSel = true>
 __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
                                 Sampler &seed, int *stack, bool diPrimary, size_t slot = 0, bool *queried = nullptr) {
   const int limit = max(0, (int)A.maxDepth - 1);
@@ -980,7 +1096,16 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
     Hit h;
-    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
+    if (!rt_closest<kSel>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
+      // An escape sees the environment, weighed like an emitter hit against its NEE density at the
+      // previous vertex (main.swift:7751-7756).
+      if (A.env) {
+        const float lpdf = nee ? environment_pdf(A, dir, S.n) : 0.0f;
+        const float w = !nee || lpdf <= 0.0f ? 1.0f : (previousMIS ? power_heuristic(bpdf, lpdf) : 0.0f);
+        R = add(R, to_rgb(A, L, scale4(mul4(T, emission3(A, L, environment(A, dir))), w)));
+      }
+      break;
+    }
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
@@ -999,7 +1124,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     }
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
+      R = add(R, direct_light<kPbr, kSel>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -1013,7 +1138,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
 }
 
 // One path of sampling modes 1-3: camera ray, primary hit, NEE there, then the continuation.
-template <bool kPbr, bool kNrc>
+template <bool kPbr, bool kNrc, bool kSel>
 __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame,
                                                    float2 jit, int *stack, size_t slot, bool &queried) {
   Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
@@ -1022,9 +1147,9 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
   float3 dir0 = camera_dir(A, x, y, jit), o0 = A.cam;
   lens_ray(A, o0, dir0, seed);
   Hit h;
-  const bool hit0 = rt_closest(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack);
+  const bool hit0 = rt_closest<kSel>(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
-  if (!hit0) return f3(0.0f, 0.0f, 0.0f);
+  if (!hit0) return A.env ? environment(A, dir0) : f3(0.0f, 0.0f, 0.0f);  // environment_rgb (main.swift:7453-7455)
   const Surface S = surface_at(A, h, o0, dir0);
   const vt_material m = material(A, S.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission(A, L, S, m);
@@ -1033,18 +1158,18 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
+    R = direct_light<kPbr, kSel>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
-  R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
+  R = add(R, continue_path<kPbr, kNrc, kSel>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
 }
-template <bool kPbr, bool kNrc = false>
+template <bool kPbr, bool kNrc = false, bool kSel = true>
 __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
                               int *stack, size_t slot = 0) {
   bool queried = false;
-  const float3 c = path_sample_body<kPbr, kNrc>(A, x, y, si, frame, jit, stack, slot, queried);
+  const float3 c = path_sample_body<kPbr, kNrc, kSel>(A, x, y, si, frame, jit, stack, slot, queried);
   if (kNrc && !queried) nrc_store_none(A, slot);
   return c;
 }
@@ -1090,7 +1215,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
   r.M = 0.0f;
   for (uint32_t c = 0; c < A.diCandidates; ++c) {
     sampler_candidate(seed, 1u, kZDi, c, A.diBits);
-    const LightSample ls = sample_direct(A, S.pos, seed);
+    const LightSample ls = sample_direct(A, S.pos, S.n, seed);
     r.M += 1.0f;  // zero-weight candidates still count
     if (!(ls.pdf > 0.0f)) continue;
     DISample cand;
@@ -1205,7 +1330,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
-      const float3 c = path_sample<kPbr, kNrc>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack,
+      const float3 c = path_sample<kPbr, kNrc, false>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack,
                                                (size_t)k * npix + p);
       sr += c.x;
       sg += c.y;
@@ -1426,7 +1551,7 @@ __global__ void __launch_bounds__(256) k_render_batch(const RenderArgs *__restri
       const uint32_t x = p % A.W, y = p / A.W, f0 = firstSample[lo], fr0 = firstFrame[lo];
       double sr = 0.0, sg = 0.0, sb = 0.0;
       for (uint32_t k = 0; k < A.spp; ++k) {
-        const float3 c = path_sample<kPbr>(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
+        const float3 c = path_sample<kPbr, false, false>(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
         sr += c.x; sg += c.y; sb += c.z;
       }
       double *acc = A.accum + 3 * (size_t)p;
@@ -1483,7 +1608,7 @@ __global__ void k_light_estimate(RenderArgs A, const float4 *__restrict__ points
   seed.key = seed.dimension = seed.sub = seed.subBits = 0u;
   float sum = 0.0f, squares = 0.0f, hits = 0.0f, zero = 0.0f, error = 0.0f, backFacing = 0.0f;
   for (uint32_t i = 0; i < samples; ++i) {
-    const LightSample ls = sample_emitters(A, p, seed);
+    const LightSample ls = sample_emitters(A, p, f3(0.0f, 0.0f, 1.0f), seed);
     if (ls.face == 0xffffffffu) continue;
     const Tri t = scene_triangle(A, ls.face);
     if (dot3(cross3(sub(t.b, t.a), sub(t.c, t.a)), sub(p, ls.pos)) <= 0.0f) backFacing += 1.0f;
@@ -1813,6 +1938,8 @@ vt_status check_params(vt_ctx *ctx, const vt_scene *scene, const vt_frame_params
   if (p->spectral && !scene->d_spec) return vt_fail(ctx, VT_ERR_INVALID, "spectral transport needs spectral tables");
   if (p->first_sample == 0) return vt_fail(ctx, VT_ERR_INVALID, "first_sample starts at 1");
   if (p->sampler > 1 || p->z_temporal > 3) return vt_fail(ctx, VT_ERR_INVALID, "sampler must be 0 (PCG) or 1 (Z++), z_temporal 0-3");
+  if (p->sampling_mode == 0 && scene->environment.intensity > 0.0f)
+    return vt_fail(ctx, VT_ERR_INVALID, "ReSTIR DI (sampling mode 0) does not sample the environment; use modes 1-3");
   const vt_mesh *mesh = scene->mesh;
   if (mesh->nfaces > 0 && mesh->depth > 32) return vt_fail(ctx, VT_ERR_LIMIT, "BVH deeper than the render stack");
   return VT_OK;
@@ -1893,6 +2020,14 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.accum = scene->d_accum;
   A.faceCount = mesh->nfaces;
   emitter_args(scene, A);
+  const vt_environment &env = scene->environment;
+  if (scene->imported && env.intensity > 0.0f) {
+    A.env = 1;
+    A.envIntensity = env.intensity;
+    A.sunIntensity = env.sun_intensity;
+    A.sunDir = make_float3(env.sun_dir[0], env.sun_dir[1], env.sun_dir[2]);
+    A.skyMode = env.sky_mode;
+  }
 }
 
 }  // namespace
@@ -2056,6 +2191,8 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
   if (flags & ~(uint32_t)(VT_NRC_TRAIN | VT_NRC_RENDER)) return vt_fail(ctx, VT_ERR_INVALID, "unknown flags");
   if ((flags & VT_NRC_RENDER) && p->sampling_mode > 1)
     return vt_fail(ctx, VT_ERR_INVALID, "the cache renders sampling modes 0 (ReSTIR DI) and 1 (MIS)");
+  if (scene->environment.intensity > 0.0f)
+    return vt_fail(ctx, VT_ERR_INVALID, "the cache does not handle scenes with an environment");
   {
     const vt_status st = check_params(ctx, scene, p);
     if (st != VT_OK) return st;
@@ -2324,6 +2461,25 @@ vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *b) {
   return VT_OK;
 }
 
+vt_status vt_scene_set_environment(vt_ctx *ctx, vt_scene *scene, const vt_environment *env) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene) return vt_fail(ctx, VT_ERR_INVALID, "scene is null");
+  vt_environment e{};
+  if (env && env->intensity > 0.0f) {
+    if (!scene->imported) return vt_fail(ctx, VT_ERR_INVALID, "an environment needs an imported scene");
+    e = *env;
+    if (!std::isfinite(e.intensity) || !std::isfinite(e.sun_intensity) || e.sun_intensity < 0.0f)
+      return vt_fail(ctx, VT_ERR_INVALID, "intensities must be finite, the sun's non-negative");
+    if (e.sky_mode > 2) return vt_fail(ctx, VT_ERR_INVALID, "sky_mode must be 0, 1 or 2");
+    const double l = std::sqrt((double)e.sun_dir[0] * e.sun_dir[0] + (double)e.sun_dir[1] * e.sun_dir[1] +
+                               (double)e.sun_dir[2] * e.sun_dir[2]);
+    if (!(l > 0.0) || !std::isfinite(l)) return vt_fail(ctx, VT_ERR_INVALID, "sun_dir must be a non-zero vector");
+    for (int k = 0; k < 3; ++k) e.sun_dir[k] = (float)(e.sun_dir[k] / l);
+  }
+  scene->environment = e;
+  return vt_accum_reset(ctx, scene);
+}
+
 vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n) {
   if (!ctx) return VT_ERR_INVALID;
   if (!scene || (!params && n)) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
@@ -2371,7 +2527,7 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
       VT_CUDA(ctx, cudaMemset(ctx->d_status + 8, 0, 3 * sizeof(uint32_t)));
       return vt_fail(ctx, VT_ERR_DEVICE,
                      "the integrator met an out-of-range index (status " + std::to_string(w[2]) +
-                         ": 4 hit, 8 cache record; first: value " + std::to_string(w[9]) +
+                         ": 4 hit, 8 cache record, 16 emitter face; first: value " + std::to_string(w[9]) +
                          ", kernel " + std::to_string(w[10] & 0xffu) + "); those accesses were clamped or skipped");
     }
   }

@@ -88,8 +88,10 @@ __device__ __forceinline__ float edge_fn(float px, float py, float qx, float qy)
 // Two-sided hit in [tMin, tMax) (main.swift:1564-1579). kSelect picks the permuted coordinates with
 // selects (comp3); otherwise they are indexed from three-element arrays, which the compiler keeps in
 // local memory. The arrays cost fewer registers (the integrator's megakernels run 25 % faster with
-// them), but in one integrator kernel their local slots overlapped the traversal stack: a stack entry
-// popped right after its push read back a vertex coordinate. Kernels that showed that use kSelect.
+// them), but in two integrator kernels their local slots overlapped the traversal stack: a stack entry
+// popped right after its push read back a vertex coordinate. The integrator selects everywhere except
+// in its two throughput megakernels (render.cu: k_render, k_render_batch), which run every test clean
+// with the arrays.
 template <bool kSelect = true>
 __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b, float4 c, float tMin,
                                               float tMax, float &t, float &b1, float &b2) {

@@ -87,6 +87,7 @@ struct vt_scene {
   // Imported scenes (emissive triangles, no quad light): the packed emitter list, per slot
   // (emission rgb, selection weight), and face -> BVH position.
   bool imported = false;
+  vt_environment environment{};  // procedural sky and sun of an imported scene (intensity 0: none)
   uint32_t *d_emitters = nullptr;
   std::vector<uint32_t> emitter_words;
   float4 *d_emissions = nullptr;

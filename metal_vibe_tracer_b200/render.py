@@ -137,6 +137,19 @@ class Scene:
                 params[i].diffuse_roughness = float(m.get("diffuse_roughness", 0.0))
             _check(ctx.handle, lib.vt_scene_set_openpbr(ctx.handle, self._p, params, len(materials)), "vt_scene_set_openpbr")
 
+    def set_environment(self, intensity: float = 0.0, sun_dir=(0.0, 1.0, 0.0), sun_intensity: float = 0.0,
+                        sky_mode: int = 0) -> None:
+        """The procedural sky and sun of an imported scene (vt_scene_set_environment; the reference's
+        Uniforms.environment.x, sunParams and skyMode); intensity 0 removes it. Restarts the
+        accumulation."""
+        e = _lib.Environment()
+        e.intensity = float(intensity)
+        e.sun_dir[:] = [float(x) for x in sun_dir]
+        e.sun_intensity = float(sun_intensity)
+        e.sky_mode = int(sky_mode)
+        _check(self.ctx.handle, _lib.load().vt_scene_set_environment(self.ctx.handle, self._p, C.byref(e)),
+               "vt_scene_set_environment")
+
     def emitter_words(self) -> np.ndarray:
         """The packed emitter list of an imported scene (uint32 words)."""
         lib = _lib.load()

@@ -419,6 +419,42 @@ def _lattice_noise(dirs, seeds):
     return noise
 
 
+def sky_scene(emitter: bool = True, subdivisions: int = 2):
+    """An open scene for the procedural sky and sun (imported-scene lighting): a 10 x 10 ground
+    quad, a smooth-shaded icosphere of radius 1 resting on it, a 1 x 1 x 1 box and, with `emitter`,
+    a small emissive triangle above them. Returns (faces, vertices, materials, camera)."""
+    tris, tags = [], []
+    g = 5.0
+    tris += [((-g, 0, -g), (g, 0, g), (g, 0, -g)), ((-g, 0, -g), (-g, 0, g), (g, 0, g))]
+    tags += [0, 0]
+    lo, hi = np.array([1.2, 0.0, -0.3]), np.array([2.2, 1.0, 0.7])
+    c = [np.array([hi[0] if i & 1 else lo[0], hi[1] if i & 2 else lo[1], hi[2] if i & 4 else lo[2]]) for i in range(8)]
+    for a, b, cc, d in ((0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)):
+        tris += [(c[a], c[b], c[cc]), (c[a], c[cc], c[d])]
+        tags += [2, 2]
+    if emitter:
+        tris.append(((-1.5, 2.5, 0.5), (-1.0, 2.5, -0.5), (-0.5, 2.5, 0.5)))  # faces down
+        tags.append(3)
+    faces, verts = _mesh_from_triangles(tris, tags)
+    pos, nrm, ftri = icosphere(subdivisions, center=(-0.3, 1.0, 0.4), radius=1.0)
+    base = len(verts)
+    sv = np.zeros(len(pos), VERTEX_DTYPE)
+    sv["p"] = pos.astype(np.float32)
+    sv["n"] = nrm.astype(np.float32)
+    sf = np.zeros(len(ftri), FACE_DTYPE)
+    sf["a"], sf["b"], sf["c"] = (ftri[:, 0] + base).astype(np.uint32), (ftri[:, 1] + base).astype(np.uint32), \
+        (ftri[:, 2] + base).astype(np.uint32)
+    sf["tag"] = 1
+    faces = np.concatenate([faces, sf])
+    verts = np.concatenate([verts, sv])
+    materials = [{"type": 0, "albedo": (0.5, 0.5, 0.5), "emission": (0.0, 0.0, 0.0)},
+                 {"type": 0, "albedo": (0.7, 0.35, 0.2), "emission": (0.0, 0.0, 0.0)},
+                 {"type": 0, "albedo": (0.25, 0.45, 0.7), "emission": (0.0, 0.0, 0.0)},
+                 {"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (6.0, 5.0, 4.0)}]
+    camera = {"pos": (0.0, 1.6, -5.5), "target": (0.0, 0.8, 0.0), "up": (0.0, 1.0, 0.0), "fov": 50.0}
+    return faces, verts, materials, camera
+
+
 def sphere_grid(triangles: int, seed: int = 0, emissive_every: int = 16, displace: float = 0.05, nmat: int = 8,
                 coloured: bool = False):
     """The grid scene's generator (configs C3/C4): a k x k grid of displaced icospheres on a ground quad,

@@ -1535,6 +1535,12 @@ struct PtContext {
   std::vector<vt_material> mats;
   std::vector<std::array<double, 4>> slotL;
   std::vector<std::array<double, 6>> basis;
+  // Imported scenes: the procedural sky and sun (vt_environment; the sun direction normalised as the
+  // library does, in double and then stored as float).
+  bool env = false;
+  double envIntensity = 0, sunIntensity = 0;
+  D3 sunDir{0, 1, 0};
+  uint32_t skyMode = 0;
 };
 
 inline double fword(uint32_t w) { float f; std::memcpy(&f, &w, 4); return f; }
@@ -1844,12 +1850,95 @@ double emitter_area_pdf_d(const PtContext &C, uint32_t face, D3 p, const PtTri &
   return C.etotal > 0.0 && t.slot < C.emis.size() ? C.emis[t.slot][3] / C.etotal : 0.0;
 }
 
-// sample_direct_light's emitter branch (main.swift:2892-2920), emitter probability 1.
-PtLight sample_emitters_d(const PtContext &C, D3 p, ZSampler &seed) {
+void make_basis_d(D3 n, D3 &u, D3 &v);
+
+// ---- procedural sky and sun (imported scenes; main.swift:522-597, 2127-2134, 2700-2719) ----------
+constexpr uint32_t kEnvFaceD = 0xfffffffeu;
+bool in_sun_cone_d(D3 d, D3 s, double omc) {
+  const D3 c = cross(d, s);
+  return dot(d, s) > 0.0 && dot(c, c) <= omc * (2.0 - omc);
+}
+double sun_omc_d(uint32_t mode) { return mode == 0u ? (double)8e-4f : (mode == 1u ? (double)7e-4f : (double)9e-4f); }
+D3 mix_d(D3 a, D3 b, double t) { return a + (b - a) * t; }
+D3 f3d(float x, float y, float z) { return D3{x, y, z}; }
+D3 procedural_sky_d(const PtContext &C, D3 d) {
+  const double sunCos = dot(d, C.sunDir), y = d.y;
+  D3 zenith, horizon, ground, lobe, disc;
+  double gradient, lobePower, lobeGain, discGain, groundPower, groundScale, gain;
+  if (C.skyMode == 0u) {
+    zenith = f3d(0.08f, 0.18f, 0.46f); horizon = f3d(0.96f, 0.52f, 0.22f); ground = f3d(0.12f, 0.10f, 0.08f);
+    lobe = f3d(1.0f, 0.70f, 0.30f); disc = f3d(1.0f, 0.78f, 0.45f);
+    gradient = 0.40f; lobePower = 6.0; lobeGain = 3.0; discGain = 0.45f; groundPower = 5.0; groundScale = 0.35f; gain = 1.5;
+  } else if (C.skyMode == 1u) {
+    zenith = f3d(0.16f, 0.42f, 0.92f); horizon = f3d(0.74f, 0.85f, 0.96f); ground = f3d(0.14f, 0.15f, 0.12f);
+    lobe = f3d(1.0f, 0.98f, 0.92f); disc = f3d(1.0f, 0.98f, 0.94f);
+    gradient = 0.48f; lobePower = 12.0; lobeGain = 2.2f; discGain = 0.40f; groundPower = 4.0; groundScale = 0.40f; gain = 1.8f;
+  } else {
+    zenith = f3d(0.04f, 0.06f, 0.14f); horizon = f3d(0.46f, 0.26f, 0.42f); ground = f3d(0.04f, 0.04f, 0.05f);
+    lobe = f3d(0.95f, 0.65f, 0.75f); disc = f3d(1.0f, 0.85f, 0.78f);
+    gradient = 0.55f; lobePower = 10.0; lobeGain = 1.8f; discGain = 0.35f; groundPower = 3.0; groundScale = 0.25f; gain = 1.6f;
+  }
+  D3 col;
+  if (y >= 0.0) {
+    col = mix_d(horizon, zenith, std::pow(y, gradient));
+    col = col + lobe * (std::pow(std::max(0.0, sunCos), lobePower) * lobeGain);
+    if (in_sun_cone_d(d, C.sunDir, sun_omc_d(C.skyMode))) col = col + disc * (C.sunIntensity * discGain);
+  } else {
+    col = mix_d(ground, horizon * groundScale, std::pow(1.0 + y, groundPower));
+  }
+  return col * gain;
+}
+D3 environment_d(const PtContext &C, D3 d) { return procedural_sky_d(C, d) * C.envIntensity; }
+double imported_probability_d(const PtContext &C) { return C.ecount == 0 ? 0.0 : (C.env ? 0.5 : 1.0); }
+double sun_probability_d(const PtContext &C) {
+  if (!(C.sunIntensity > 0.0) || !C.env) return 0.0;
+  const double w = sun_omc_d(C.skyMode);
+  return C.sunDir.y >= -std::sqrt(w * (2.0 - w)) ? 0.60 : 0.0;
+}
+double environment_pdf_d(const PtContext &C, D3 wi, D3 n) {
+  const double sp = sun_probability_d(C), w = sun_omc_d(C.skyMode);
+  const double sunPdf = in_sun_cone_d(wi, C.sunDir, w) ? 1.0 / (2.0 * kPi * w) : 0.0;
+  const double rest = std::max(0.0, dot(n, wi)) / kPi;
+  return (1.0 - imported_probability_d(C)) * (sp * sunPdf + (1.0 - sp) * rest);
+}
+D3 cosine_hemisphere_d(D3 n, double r0, double r1) {
+  const double phi = 2.0 * kPi * r0, cos_th = std::sqrt(r1 + 0.5 / 16777216.0);
+  const double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
+  D3 u, v;
+  make_basis_d(n, u, v);
+  return normalize(u * (std::cos(phi) * sin_th) + v * (std::sin(phi) * sin_th) + n * cos_th);
+}
+
+// sample_direct_light's imported branch (main.swift:2889-2955): an emitter triangle with probability
+// imported_probability_d, else the environment (sun cone or cosine lobe about n).
+PtLight sample_emitters_d(const PtContext &C, D3 p, D3 n, ZSampler &seed) {
   PtLight ls{};
   ls.face = 0xffffffffu;
-  if (C.ecount == 0) return ls;
-  (void)seed.f1();
+  const double ip = imported_probability_d(C);
+  if (!(ip > 0.0) && !C.env) return ls;
+  if (!(ip > 0.0 && seed.f1() < ip)) {
+    const double sp = sun_probability_d(C);
+    double qx = 1.0, qy = 1.0, qz = 1.0;
+    if (sp > 0.0) seed.f3(qx, qy, qz);
+    if (sp > 0.0 && qx < sp) {
+      const double omc = qy * sun_omc_d(C.skyMode);
+      const double cos_th = 1.0 - omc, sin_th = std::sqrt(std::max(0.0, omc * (2.0 - omc)));
+      D3 su, sv;
+      make_basis_d(C.sunDir, su, sv);
+      const double phi = 2.0 * kPi * qz;
+      ls.wi = normalize(su * (std::cos(phi) * sin_th) + sv * (std::sin(phi) * sin_th) + C.sunDir * cos_th);
+    } else {
+      double r0 = qy, r1 = qz;
+      if (!(sp > 0.0)) seed.f2(r0, r1);
+      ls.wi = cosine_hemisphere_d(n, r0, r1);
+    }
+    ls.pos = p + ls.wi * 1e6;
+    ls.dist = 1e6;
+    ls.face = kEnvFaceD;
+    ls.pdf = environment_pdf_d(C, ls.wi, n);
+    ls.emission = environment_d(C, ls.wi);
+    return ls;
+  }
   double qx, qy, qz;
   seed.f3(qx, qy, qz);
   const bool tree = C.treeNodes > 0;
@@ -1878,7 +1967,7 @@ PtLight sample_emitters_d(const PtContext &C, D3 p, ZSampler &seed) {
   ls.face = face;
   const double area = tree ? triangle_area_d(t) : 0.0;
   const double areaPdf = !tree ? emitter_area_pdf_d(C, face, p, t) : (area > 0.0 ? pmf / area : 0.0);
-  ls.pdf = geometry > 1e-12 ? areaPdf / geometry : 0.0;
+  ls.pdf = geometry > 1e-12 ? ip * areaPdf / geometry : 0.0;
   return ls;
 }
 
@@ -1887,7 +1976,7 @@ double emitter_pdf_d(const PtContext &C, D3 p, D3 hitPos, uint32_t face) {
   if (C.ecount == 0) return 0.0;
   const PtTri t = pt_triangle(C, face);
   const double g = imported_geometry_d(p, hitPos, t);
-  return g > 1e-12 ? emitter_area_pdf_d(C, face, p, t) / g : 0.0;
+  return g > 1e-12 ? imported_probability_d(C) * emitter_area_pdf_d(C, face, p, t) / g : 0.0;
 }
 
 // light_visible (main.swift:3254-3264) with endpoint_tolerance (main.swift:1358-1361).
@@ -1975,7 +2064,7 @@ bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material 
 
 D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
             const vt_material &m, bool useMIS, ZSampler &seed, bool requirePdf) {
-  const PtLight ls = C.imported ? sample_emitters_d(C, p, seed) : sample_light_d(C, p, seed);
+  const PtLight ls = C.imported ? sample_emitters_d(C, p, n, seed) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
   if (!visible_d(C, p, gn, err, ls)) return {0, 0, 0};
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
@@ -2070,9 +2159,19 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     bool finite = true;
     for (double t : T.v) finite = finite && std::isfinite(t);
     if (!finite || smax(C, T) <= 0.0) break;
-    const D3 prev = h.pos;
+    const D3 prev = h.pos, prevN = h.n;
     const D3 o = ray_origin_d(C, h.pos, h.gn, nd, h.err);
-    if (!pt_closest(C, o, nd, h)) break;
+    if (!pt_closest(C, o, nd, h)) {
+      // An escape sees the environment, weighed against its NEE density (main.swift:7751-7756).
+      if (C.env) {
+        const double lpdf = nee ? environment_pdf_d(C, nd, prevN) : 0.0;
+        const double w = !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
+        const D3 e = environment_d(C, nd);
+        const float ef[3] = {(float)e.x, (float)e.y, (float)e.z};
+        R = R + to_rgb(C, L, scale(mul(T, emission(C, L, ef)), w));
+      }
+      break;
+    }
     m = pt_material(C, h.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       const double lpdf = C.imported ? emitter_pdf_d(C, prev, h.pos, h.face) : light_pdf_d(C, prev, h.pos);
@@ -2200,7 +2299,7 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   out.s.u = u;
   for (uint32_t c = 0; c < M; ++c) {
     seed.candidate(1u, 4u, c, bits);
-    const PtLight ls = C.imported ? sample_emitters_d(C, h.pos, seed) : sample_light_d(C, h.pos, seed);
+    const PtLight ls = C.imported ? sample_emitters_d(C, h.pos, h.n, seed) : sample_light_d(C, h.pos, seed);
     out.M += 1.0;
     if (!(ls.pdf > 0.0)) continue;
     const DiS cand = di_from_light(ls, u);
@@ -2271,7 +2370,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   PtHit h;
   const bool hit0 = pt_closest(C, o0, dir0, h);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);
-  if (!hit0) return {0, 0, 0};
+  if (!hit0) return C.env ? environment_d(C, dir0) : D3{0, 0, 0};
   const vt_material m = pt_material(C, h.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
   const int limit = std::max(0, (int)C.p->max_depth - 1);
@@ -2321,6 +2420,16 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
   C.fovScale = std::tan(p->fov_deg * 0.5 * kPi / 180.0);
   C.larea = std::sqrt(dot(cross(d3(in->light.su), d3(in->light.sv)), cross(d3(in->light.su), d3(in->light.sv))));
   C.imported = in->imported != 0;
+  if (C.imported && in->environment.intensity > 0.0f) {
+    const vt_environment &e = in->environment;
+    const double l = std::sqrt((double)e.sun_dir[0] * e.sun_dir[0] + (double)e.sun_dir[1] * e.sun_dir[1] +
+                               (double)e.sun_dir[2] * e.sun_dir[2]);
+    C.env = true;
+    C.envIntensity = e.intensity;
+    C.sunIntensity = e.sun_intensity;
+    C.sunDir = D3{(float)(e.sun_dir[0] / l), (float)(e.sun_dir[1] / l), (float)(e.sun_dir[2] / l)};
+    C.skyMode = e.sky_mode;
+  }
   if (C.imported) {
     // Per slot (rgb, selection weight max(1e-8, luminance) in float, main.swift:9303-9306).
     C.emis.assign(in->nmat, {0, 0, 0, 0});

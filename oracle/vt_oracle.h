@@ -119,6 +119,8 @@ typedef struct vto_pt_inputs {
   const float *pbr_params;
   vto_pbr_eval_fn pbr_eval;
   vto_pbr_sample_fn pbr_sample;
+  /* Imported scenes: the procedural sky and sun (intensity 0: none). */
+  vt_environment environment;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

@@ -228,6 +228,11 @@ class FrameParams(C.Structure):
                 ("aperture", C.c_float), ("focus_distance", C.c_float)]
 
 
+class Environment(C.Structure):
+    _fields_ = [("intensity", C.c_float), ("sun_dir", C.c_float * 3), ("sun_intensity", C.c_float),
+                ("sky_mode", C.c_uint32), ("pad", C.c_uint32 * 2)]
+
+
 class PtInputs(C.Structure):
     _fields_ = [("faces", C.c_void_p), ("nfaces", C.c_uint32), ("verts", C.c_void_p), ("nverts", C.c_uint32),
                 ("materials", C.c_void_p), ("nmat", C.c_uint32), ("light", QuadLight),
@@ -235,7 +240,8 @@ class PtInputs(C.Structure):
                 ("nbins", C.c_uint32), ("segments", C.c_uint32), ("lambda_min", C.c_float),
                 ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32),
                 ("uplift", C.c_void_p), ("cos_phase", C.c_void_p),
-                ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p)]
+                ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p),
+                ("environment", Environment)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -243,11 +249,12 @@ _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32,
 
 def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
            spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1, light_tree=True,
-           emitter_words=None, di_candidates=0, aperture=0.0, focus_distance=1.0):
+           emitter_words=None, di_candidates=0, aperture=0.0, focus_distance=1.0, environment=None):
     """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames.
 
     light=None renders an imported scene lit by its emissive faces; its emitter list is the
-    pure-Python restatement's (oracle/light_tree.py) unless `emitter_words` is given."""
+    pure-Python restatement's (oracle/light_tree.py) unless `emitter_words` is given. An imported
+    scene may also have an `environment` (dict: intensity, sun_dir, sun_intensity, sky_mode)."""
     lib = load()
     if not hasattr(lib.vto_render, "_typed"):
         lib.vto_render.restype, lib.vto_render.argtypes = _SIGS["vto_render"]
@@ -275,6 +282,12 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         inp.pbr_params = params.ctypes.data
         inp.pbr_eval = C.cast(ref.ref_openpbr_eval, C.c_void_p).value
         inp.pbr_sample = C.cast(ref.ref_openpbr_sample, C.c_void_p).value
+    if light is None and environment is not None and float(environment.get("intensity", 0.0)) > 0.0:
+        env = inp.environment
+        env.intensity = float(environment["intensity"])
+        env.sun_dir[:] = [float(x) for x in environment.get("sun_dir", (0.0, 1.0, 0.0))]
+        env.sun_intensity = float(environment.get("sun_intensity", 0.0))
+        env.sky_mode = int(environment.get("sky_mode", 0))
     if light is None:
         if emitter_words is None:
             from . import light_tree as LT
