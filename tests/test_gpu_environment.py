@@ -87,3 +87,40 @@ def test_environment_rejections(ctx):
     quad.close()
     cmesh.close()
     mesh.close()
+
+
+def test_batched_sky_scene_equals_single_render(ctx):
+    """A scene with an environment in a batch (one persistent launch, then the captured graph) adds
+    exactly the samples vt_render adds, beside a scene without one."""
+    from metal_vibe_tracer_b200.render import Batch
+    faces, verts, mats, cam = scenes.sky_scene(emitter=True)
+    mesh = vt.Mesh(ctx, faces, verts)
+    tables = spectral_tables.load()
+    cf, cv, cm, light, ccam = scenes.cornell_box()
+    cmesh = vt.Mesh(ctx, cf, cv)
+
+    def make_sky():
+        s = vt.Scene(ctx, mesh, mats, None, tables)
+        s.set_environment(**dict(SUN, sky_mode=2))
+        return s
+
+    specs = [(make_sky, vt.make_params(cam, 48, 40, 8, 1, True, 1), 2),
+             (lambda: vt.Scene(ctx, cmesh, cm, light), vt.make_params(ccam, 32, 32, 6, 1, False, 2), 3)]
+    members = [make() for make, _, _ in specs]
+    batch = Batch(ctx, members, [p for _, p, _ in specs], [s for _, _, s in specs])
+    passes = 7
+    for _ in range(passes):
+        batch.render()
+    for scene, (make, params, spp) in zip(members, specs):
+        img, n = scene.readback()
+        ref_scene = make()
+        ref_scene.render(params, passes * spp)
+        ref, m = ref_scene.readback()
+        ref_scene.close()
+        assert n == m == passes * spp and np.isfinite(img).all() and img.max() > 0
+        np.testing.assert_allclose(img, ref, rtol=1e-12, atol=1e-12)
+    batch.close()
+    for s in members:
+        s.close()
+    cmesh.close()
+    mesh.close()
