@@ -428,8 +428,8 @@ typedef struct vt_environment {
   uint32_t pad[2];
 } vt_environment;
 /* Sets (or with NULL / intensity 0 clears) an imported scene's environment; restarts its
- * accumulation. Sampling modes 1-3 only: ReSTIR DI (mode 0) and vt_render_nrc reject a scene with an
- * environment. */
+ * accumulation. Sampling modes 1-3 only: ReSTIR DI (mode 0) rejects a scene with an environment, so
+ * vt_render_nrc renders one with MIS primaries (mode 1); its training paths see the environment. */
 vt_status vt_scene_set_environment(vt_ctx *ctx, vt_scene *scene, const vt_environment *env);
 
 /* ---- neural radiance cache (nrc.cu) -------------------------------------------------------------

@@ -1418,7 +1418,15 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     const float3 prev = S.pos;
     o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
-    if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) break;
+    if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
+      // An escape sees the environment, weighed against its NEE density at the last vertex.
+      if (A.env) {
+        const float lpdf = environment_pdf(A, dir, S.n);
+        const float w = lpdf <= 0.0f ? 1.0f : power_heuristic(bpdf, lpdf);
+        R = add4(R, scale4(mul4(T, emission3(A, L, environment(A, dir))), w));
+      }
+      break;
+    }
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
@@ -2191,8 +2199,6 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
   if (flags & ~(uint32_t)(VT_NRC_TRAIN | VT_NRC_RENDER)) return vt_fail(ctx, VT_ERR_INVALID, "unknown flags");
   if ((flags & VT_NRC_RENDER) && p->sampling_mode > 1)
     return vt_fail(ctx, VT_ERR_INVALID, "the cache renders sampling modes 0 (ReSTIR DI) and 1 (MIS)");
-  if (scene->environment.intensity > 0.0f)
-    return vt_fail(ctx, VT_ERR_INVALID, "the cache does not handle scenes with an environment");
   {
     const vt_status st = check_params(ctx, scene, p);
     if (st != VT_OK) return st;

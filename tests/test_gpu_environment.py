@@ -124,3 +124,36 @@ def test_batched_sky_scene_equals_single_render(ctx):
         s.close()
     cmesh.close()
     mesh.close()
+
+
+def test_cached_sky_scene_matches_path_tracer(ctx):
+    """The radiance cache on an open scene: training paths and cache-terminated paths that escape
+    pick up the sky (MIS primaries, spectral). A trained cache's image within 4 % of the path
+    tracer's mean radiance, the cache's own bias being what the bound covers."""
+    from metal_vibe_tracer_b200.nrc import RadianceCache
+    faces, verts, mats, cam = scenes.sky_scene(emitter=True)
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, None, spectral_tables.load())
+    scene.set_environment(**dict(SUN, sky_mode=0))
+    W = H = 64
+    scene.render(vt.make_params(cam, W, H, 8, 1, True, 1), 1024)
+    ref, _ = scene.readback()
+    info = mesh.info()
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=13)
+    scene.reset()
+    for f in range(120):
+        cache.render(scene, vt.make_params(cam, W, H, 8, 1 + f, True, 1), 0, render=False)
+    ci = cache.info()
+    assert ci["last_records"] > 1000 and np.isfinite(ci["last_loss"])
+    scene.reset()
+    for f in range(16):
+        cache.render(scene, vt.make_params(cam, W, H, 8, 9001 + 16 * f, True, 1), 16)
+    img, n = scene.readback()
+    assert n == 256 and np.isfinite(img).all()
+    gm, rm = img.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 0.04), (gm, rm)
+    with pytest.raises(vt.MaterialLibraryError, match="sampling mode 0"):
+        cache.render(scene, vt.make_params(cam, W, H, 8, 1, True, 0), 1)
+    cache.close()
+    scene.close()
+    mesh.close()
