@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--profile", action="store_true", help="small run for ncu: no e2e, no CPU leg")
     p.add_argument("--no-cornell", action="store_true", help="skip the integrator measurement")
     p.add_argument("--profile-nrc", action="store_true", help="short radiance-cache sequence for ncu, then exit")
+    p.add_argument("--profile-production", action="store_true",
+                   help="the production scene's frames only (for an ncu launch list), then exit")
     p.add_argument("--reference-spp", type=int, default=65536, help="spp of the FP64 reference image")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-launch measurement (0: skip)")
     p.add_argument("--batch-passes", type=int, default=2, help="timed batched passes after the tuning passes")
@@ -447,10 +449,26 @@ def profile_nrc(a) -> int:
     return 0
 
 
+def profile_production(a) -> int:
+    """The production scene's frames for an ncu launch list: 2 warm-up and `--production-frames`
+    timed frames each of ReSTIR DI (32 candidates) and MIS, as the bench times them, then exit."""
+    import torch
+
+    import metal_vibe_tracer_b200 as vt
+    ctx = vt.Context(0)
+    stream = torch.cuda.Stream()
+    out = bench_production(a, ctx, stream)
+    print(json.dumps({"profile_production": "ok", "restir_di_32_ms": out["restir_di_32"]["ms_per_frame"],
+                      "mis_ms": out["mis"]["ms_per_frame"]}))
+    return 0
+
+
 def main():
     a = parse()
     if a.profile_nrc:
         return profile_nrc(a)
+    if a.profile_production:
+        return profile_production(a)
     if a.profile:
         a.no_e2e = True
         a.no_cpu_baseline = True
