@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--nrc-max-spp", type=int, default=4096, help="spp cap of the radiance cache's relMSE runs")
     p.add_argument("--nrc-train-every", type=int, default=2,
                    help="after the training frames, the cache trains on every n-th rendered frame")
+    p.add_argument("--nrc-levels", type=int, default=8,
+                   help="hash-grid levels of the radiance cache (8 reach the same spp at relMSE 1e-3 on the Cornell box as 16, in cheaper frames)")
     p.add_argument("--nrc-records", type=int, default=16384,
                    help="cache training records per frame (a quarter of the 256x256 image's pixels)")
     return p.parse_args()
@@ -263,7 +265,8 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     def time_to_relmse_nrc(mode):
         from metal_vibe_tracer_b200.nrc import RadianceCache
         info = mesh.info()
-        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records)
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records,
+                              levels=a.nrc_levels)
         scene.reset()
         e0.record(stream)
         for f in range(a.nrc_pretrain):
@@ -309,6 +312,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
         nrc.update({f"{name}_s": s_, f"{name}_spp": spp_, f"{name}_relmse": err_, f"{name}_frame_ms": fms,
                     f"{name}_loss": ci["last_loss"]})
     nrc["nrc_pretrain_frames"] = a.nrc_pretrain
+    nrc["nrc_levels"] = a.nrc_levels
     nrc["nrc_train_records"] = a.nrc_records
     nrc["nrc_train_every"] = a.nrc_train_every
     nrc["nrc_restir_speedup_vs_plain"] = (pt_s / nrc["nrc_restir_s"]) if (pt_s and nrc["nrc_restir_s"]) else None
