@@ -248,6 +248,16 @@ vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_
                            uint32_t sample_index, uint32_t frame_index, uint32_t vertex, uint32_t stream,
                            float *out);
 
+/* The reference's device known answers (regression_checks, tests/GPUChecks.swift:14-37), evaluated
+ * by the integrator's own device functions on the reference's inputs, VT_KNOWN_ANSWERS floats into
+ * the HOST array `out`: [0] power_heuristic(1e-10, 1e-10); [1..3] emission_weight(false, true,
+ * false, 0.2, 1), (true, true, true, 0, 1), (false, false, false, 0.2, 1); [4] the second PCG draw
+ * from seed 890625759; [5] the cosine of the grazing cosine-hemisphere sample drawn from that seed
+ * against its normal; [6..7] min and max of 100,000 rand_f draws from seed 17; [8..10]
+ * scattering_limit of depths 0, 1, 8. */
+#define VT_KNOWN_ANSWERS 11u
+vt_status vt_known_answers(vt_ctx *ctx, float *out, uint32_t n);
+
 /* ---- batched scenes ---------------------------------------------------------------------- */
 
 /* Many scenes of uneven size rendered by one persistent launch per pass (config C4; no counterpart
@@ -512,8 +522,10 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
  *   tris:  12 floats per face (three float4 per BVH position: a with the input face index's bits
  *          in .w, b with the face's tag bits in .w, c; 16-byte aligned).
  *   order: nfaces int32 (BVH position -> input face).
- *   info:  host output (build_ms is host wall time).  stream: NULL = the CUDA default stream;
- *          the call returns when the build on that stream is complete.
+ *   info:  host output (build_ms is host wall time).  stream: NULL = the CUDA default stream.
+ *          The call blocks the host: it synchronises that stream once per collapse level (the
+ *          level's node count sizes the next launch) and at the end, so it returns when the build
+ *          is complete; a call that fails after queueing work also waits for that work first.
  *   error: optional host buffer of error_capacity bytes for the failure message.
  * Meshes over VT_NOALLOC_MAX_FACES faces are rejected with VT_ERR_LIMIT. The first call on each
  * device looks up the static array's address (with that device current), so make that first call

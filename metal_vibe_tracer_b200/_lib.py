@@ -135,6 +135,7 @@ SIGNATURES = {
     "vt_accum_reset": (_I32, [_P, _P]),
     "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_sampler_frame": (_I32, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _P]),
+    "vt_known_answers": (_I32, [_P, _P, _U32]),
     "vt_light_tree_build": (_I32, [_P, _P, _U32, _U32, C.c_double, C.POINTER(_P)]),
     "vt_light_tree_destroy": (_I32, [_P, _P]),
     "vt_light_tree_get_info": (_I32, [_P, _P, C.POINTER(LightTreeInfo)]),
@@ -171,6 +172,7 @@ SIGNATURES = {
     "vt_render_nrc": (_I32, [_P, _P, _P, _P, _U32, _U32, _P]),
 }
 NOALLOC_MAX_FACES = 32768
+KNOWN_ANSWERS = 11
 
 _lib: C.CDLL | None = None
 

@@ -389,7 +389,7 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
                                 const uint32_t *offInner, const uint32_t *offPrims, uint32_t base,
                                 uint32_t nextBase, uint32_t primBase, vt_wide_node *nodes,
                                 int32_t *nextLevel, const uint32_t *sorted, const vt_face *faces,
-                                const vt_vertex *verts, int32_t *order, float4 *tris,
+                                const vt_vertex *verts, uint32_t nverts, int32_t *order, float4 *tris,
                                 uint32_t *status, float4 *nrm = nullptr) {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= L) return;
@@ -423,6 +423,18 @@ __global__ void k_collapse_emit(TreeView t, uint32_t L, int leafSize, const int4
           uint32_t f = sorted[-c - 1];
           order[prim] = (int32_t)f;
           vt_face fc = faces[f];
+          if (fc.a >= nverts || fc.b >= nverts || fc.c >= nverts) {
+            // k_face_boxes flagged this face already; its vertices are not read (the build then
+            // returns VT_ERR_INVALID), the slot gets a degenerate triangle at the origin.
+            atomicOr(status, (uint32_t)VT_DEV_BAD_INDEX);
+            const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            tris[3 * prim] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float((int)f));
+            tris[3 * prim + 1] = z;
+            tris[3 * prim + 2] = z;
+            if (nrm) nrm[3 * prim] = nrm[3 * prim + 1] = nrm[3 * prim + 2] = z;
+            ++prim;
+            continue;
+          }
           const vt_vertex &va = verts[fc.a], &vb = verts[fc.b], &vc = verts[fc.c];
           tris[3 * prim] = make_float4(va.px, va.py, va.pz, __int_as_float((int)f));
           tris[3 * prim + 1] = make_float4(vb.px, vb.py, vb.pz, __uint_as_float(fc.tag));
@@ -598,7 +610,7 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
     const uint32_t nextBase = base + L;
     k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, chBuf, nInner, nPrims, base,
                                                    nextBase, primBase, nodes, levelB, vals, faces,
-                                                   verts, mesh->d_order, mesh->d_tris, ctx->d_status,
+                                                   verts, nverts, mesh->d_order, mesh->d_tris, ctx->d_status,
                                                    mesh->d_nrm);
     uint32_t st_level = 0;
     VT_CUDA(ctx, cudaMemcpyAsync(host_tot, totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
@@ -677,6 +689,9 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
 // library holds until the process exits. It fits VT_NOALLOC_MAX_FACES faces; larger meshes are
 // rejected. The first call on a device looks the array's address up (cudaGetSymbolAddress, with
 // that device current) and caches it, so that first call should come before any stream capture.
+// Every call blocks the host until its build has finished: it synchronises its stream once per
+// collapse level (the level's node count sizes the next launch) and at the end, and on an error
+// after its first launch it still waits for the work it queued before returning.
 // All calls share the one array and find the previous call's contents in it: every region the
 // build needs zeroed is cleared on the call's stream, and two calls overlapping on the GPU (other
 // streams or other host threads) race on it.
@@ -763,7 +778,14 @@ extern "C" vt_status vt_mesh_build_noalloc(const vt_face *faces, uint32_t nfaces
                                            char *error, uint32_t error_capacity) {
   auto t_start = std::chrono::steady_clock::now();
   if (error && error_capacity) error[0] = '\0';
-  auto fail = [&](vt_status code, const std::string &msg) { return noalloc_fail(error, error_capacity, code, msg); };
+  // Once work is queued on the stream, a failing call first waits for it (ignoring the result), so
+  // that no kernel of this call still writes the shared scratch array after the call returns.
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  bool queued = false;
+  auto fail = [&](vt_status code, const std::string &msg) {
+    if (queued) (void)cudaStreamSynchronize(s);
+    return noalloc_fail(error, error_capacity, code, msg);
+  };
   if (nfaces > VT_NOALLOC_MAX_FACES)
     return fail(VT_ERR_LIMIT, "vt_mesh_build_noalloc: " + std::to_string(nfaces) + " faces exceed the limit of " +
                                   std::to_string(VT_NOALLOC_MAX_FACES) + " (the library's static build scratch)");
@@ -809,13 +831,13 @@ extern "C" vt_status vt_mesh_build_noalloc(const vt_face *faces, uint32_t nfaces
   NoAllocBuffers b;
   carve_noalloc(scratch, nfaces, b);
 
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const uint32_t n = nfaces, ni = n > 1 ? n - 1 : 1;
 #define VT_NA(call)                                                                  \
   do {                                                                               \
     cudaError_t _e = (call);                                                         \
     if (_e != cudaSuccess) return fail(VT_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
   } while (0)
+  queued = true;
   VT_NA(cudaMemsetAsync(b.status, 0, 4 * sizeof(uint32_t), s));
   k_init_bounds<<<1, 32, 0, s>>>(b.bounds);
   k_face_boxes<<<blocks(n, 256), 256, 0, s>>>(faces, n, verts, nverts, b.boxes, b.bounds, b.status);
@@ -847,7 +869,7 @@ extern "C" vt_status vt_mesh_build_noalloc(const vt_face *faces, uint32_t nfaces
     vt_scan_exclusive(b.nPrims, b.nPrims, L, b.scanTemp, b.totals + 1, s);
     const uint32_t nextBase = base + L;
     k_collapse_emit<<<blocks(L, 128), 128, 0, s>>>(t, L, leafSize, b.chBuf, b.nInner, b.nPrims, base, nextBase,
-                                                   primBase, nodes, levelB, b.vals, faces, verts, order,
+                                                   primBase, nodes, levelB, b.vals, faces, verts, nverts, order,
                                                    reinterpret_cast<float4 *>(tris), b.status);
     uint32_t tot[2] = {0, 0}, st = 0;
     VT_NA(cudaMemcpyAsync(tot, b.totals, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));

@@ -1,3 +1,7 @@
+// SPDX-License-Identifier: Apache-2.0
+// Derivative work of the Adobe OpenPBR BSDF (https://github.com/adobe/openpbr-bsdf, c91aad1d),
+// Copyright 2026 Adobe, licensed under the Apache License, Version 2.0 (LICENSES/Apache-2.0.txt,
+// http://www.apache.org/licenses/LICENSE-2.0); modified as described below and in NOTICE.
 // openpbr.cu — the OpenPBR energy tables on the device, and the BSDF's diagnostic entry point.
 //
 // The dense isotropic GGX energy complement (the reference's Shaders/MetalEnergy.metal, generated

@@ -1,3 +1,7 @@
+// SPDX-License-Identifier: Apache-2.0
+// Derivative work of the Adobe OpenPBR BSDF (https://github.com/adobe/openpbr-bsdf, c91aad1d),
+// Copyright 2026 Adobe, licensed under the Apache License, Version 2.0 (LICENSES/Apache-2.0.txt,
+// http://www.apache.org/licenses/LICENSE-2.0); modified as described below and in NOTICE.
 // openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials: a GGX (VNDF-sampled)
 // specular lobe with dielectric Fresnel on the dielectric part and F82-tinted Schlick on the metal
 // part, the metal's microfacet multiple-scattering lobe, and the energy-conserving (EON) diffuse

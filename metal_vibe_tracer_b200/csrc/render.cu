@@ -139,7 +139,6 @@ struct Hit {
   int pos;  // BVH position of the triangle
 };
 
-template <bool kSel = true>
 __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, Hit &h, int *stack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -160,7 +159,7 @@ __device__ bool rt_closest(const RenderArgs &A, float3 o, float3 d, float tMin, 
       for (int q = 0; q < s.count[j]; ++q) {
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         float t, b1, b2;
-        if (!intersect_tri<kSel>(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
+        if (!intersect_tri(wr, __ldg(tp), __ldg(tp + 1), __ldg(tp + 2), tMin, closest, t, b1, b2)) continue;
         closest = t;
         bb1 = b1;
         bb2 = b2;
@@ -189,7 +188,6 @@ __device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) {
 // Any hit in [tMin, tMax); with `slack` (imported scenes) each triangle's own rounding bound is
 // taken off tMax, so the endpoint surface does not occlude itself (scene_occluded, main.swift:
 // 2066-2069).
-template <bool kSel = true>
 __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, float tMax, int *stack, bool slack) {
   const WRay wr = make_wray(o.x, o.y, o.z, d.x, d.y, d.z);
   const SlabRay sr = make_slab(o.x, o.y, o.z, d.x, d.y, d.z, A.rootMax);
@@ -210,7 +208,7 @@ __device__ bool rt_any(const RenderArgs &A, float3 o, float3 d, float tMin, floa
         const float4 *tp = A.tris + 3 * (size_t)(first + q);
         const float4 ta = __ldg(tp), tb = __ldg(tp + 1), tc = __ldg(tp + 2);
         float t, b1, b2;
-        if (intersect_tri<kSel>(wr, ta, tb, tc, tMin, slack ? tMax - mesh_hit_error(ta, tb, tc) : tMax, t, b1, b2)) return true;
+        if (intersect_tri(wr, ta, tb, tc, tMin, slack ? tMax - mesh_hit_error(ta, tb, tc) : tMax, t, b1, b2)) return true;
       }
     }
   }
@@ -735,7 +733,6 @@ __device__ __forceinline__ float3 ray_origin(const RenderArgs &A, float3 p, floa
 
 // light_visible (main.swift:3254-3264): shadow ray from the offset origin to the sample, shortened
 // by the endpoint tolerance (endpoint_tolerance, main.swift:1358-1361).
-template <bool kSel = true>
 __device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
                                               const LightSample &ls, int *stack) {
   if (ls.pdf <= 0.0f) return false;
@@ -746,14 +743,21 @@ __device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, flo
   const float tol = A.imported ? fmaxf(legacy, 1.907349e-6f * (max_abs(o) + max_abs(ls.pos) + d)) : legacy;
   if (d <= tol) return false;
   delta = mul(delta, 1.0f / d);
-  return !rt_any<kSel>(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
+  return !rt_any(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
 }
 
+// power_heuristic (main.swift:2454-2460): beta = 2, scaled by the larger density.
 __device__ __forceinline__ float power_heuristic(float pf, float pg) {
   const float scale = fmaxf(pf, pg);
   if (scale <= 0.0f) return 0.0f;
   const float f = pf / scale, g = pg / scale;
   return f * f / (f * f + g * g);
+}
+// emission_weight (main.swift:3462-3466): the weight of an emitter reached by a BSDF continuation.
+__device__ __forceinline__ float emission_weight(bool previousDelta, bool previousNEE, bool previousMIS, float bsdfPdf,
+                                                 float lightPdf) {
+  if (previousDelta || !previousNEE || lightPdf <= 0.0f) return 1.0f;
+  return previousMIS ? power_heuristic(bsdfPdf, lightPdf) : 0.0f;
 }
 
 // Reflectance / emission as a 4-lane spectrum (spectral) or rgb in xyz (RGB transport). A slot's
@@ -843,14 +847,14 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 
 // NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
-template <bool kPbr, bool kSel = true>
+template <bool kPbr>
 __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                      float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                      Sampler &seed, int *stack, bool requirePdf) {
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const LightSample ls = sample_direct(A, p, n, seed);
   if (requirePdf && !(ls.pdf > 0.0f)) return zero;
-  if (!light_visible<kSel>(A, p, gn, err, ls, stack)) return zero;
+  if (!light_visible(A, p, gn, err, ls, stack)) return zero;
   const float cosine = fabsf(dot3(n, ls.wi));
   if (is_pbr<kPbr>(A, m)) {
     float bpdf;
@@ -874,11 +878,11 @@ __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const 
   return scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
 }
 // The same as rgb.
-template <bool kPbr, bool kSel = true>
+template <bool kPbr>
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                Sampler &seed, int *stack, bool requirePdf) {
-  return to_rgb(A, L, direct_light_lanes<kPbr, kSel>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
+  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
 }
 
 // ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
@@ -1059,7 +1063,7 @@ __device__ __forceinline__ void nrc_store_none(const RenderArgs &A, size_t slot)
 
 // kNrc (vt_render_nrc): the path ends at vertex A.nrcVertex, after that vertex's emission, with
 // its cache query stored in `slot`; `queried` tells whether it got there.
-template <bool kPbr, bool kNrc = false, bool kSel = true>
+template <bool kPbr, bool kNrc = false>
 __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
                                 Sampler &seed, int *stack, bool diPrimary, size_t slot = 0, bool *queried = nullptr) {
   const int limit = max(0, (int)A.maxDepth - 1);
@@ -1096,12 +1100,12 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     const float3 o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
     Hit h;
-    if (!rt_closest<kSel>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
+    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
       // An escape sees the environment, weighed like an emitter hit against its NEE density at the
       // previous vertex (main.swift:7751-7756).
       if (A.env) {
         const float lpdf = nee ? environment_pdf(A, dir, S.n) : 0.0f;
-        const float w = !nee || lpdf <= 0.0f ? 1.0f : (previousMIS ? power_heuristic(bpdf, lpdf) : 0.0f);
+        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
         R = add(R, to_rgb(A, L, scale4(mul4(T, emission3(A, L, environment(A, dir))), w)));
       }
       break;
@@ -1112,7 +1116,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       // emission_weight (main.swift:3462-3466): 1 without NEE or without a light pdf, else the
       // power heuristic (MIS) or 0 (light sampling, or a ReSTIR DI vertex).
       const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
-      const float w = !nee || lpdf <= 0.0f ? 1.0f : (previousMIS ? power_heuristic(bpdf, lpdf) : 0.0f);
+      const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
       if (!A.imported || S.front) R = add(R, to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w)));
       break;
     }
@@ -1124,7 +1128,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     }
     if (nee) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light<kPbr, kSel>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
+      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -1138,7 +1142,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
 }
 
 // One path of sampling modes 1-3: camera ray, primary hit, NEE there, then the continuation.
-template <bool kPbr, bool kNrc, bool kSel>
+template <bool kPbr, bool kNrc>
 __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame,
                                                    float2 jit, int *stack, size_t slot, bool &queried) {
   Sampler seed = pixel_sampler(x, y, A.W, si, A.zSampler != 0u, A.zModel, frame);
@@ -1147,7 +1151,7 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
   float3 dir0 = camera_dir(A, x, y, jit), o0 = A.cam;
   lens_ray(A, o0, dir0, seed);
   Hit h;
-  const bool hit0 = rt_closest<kSel>(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack);
+  const bool hit0 = rt_closest(A, o0, dir0, ray_tmin(A, o0), __int_as_float(0x7f800000), h, stack);
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   if (!hit0) return A.env ? environment(A, dir0) : f3(0.0f, 0.0f, 0.0f);  // environment_rgb (main.swift:7453-7455)
   const Surface S = surface_at(A, h, o0, dir0);
@@ -1158,18 +1162,18 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr, kSel>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
-  R = add(R, continue_path<kPbr, kNrc, kSel>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
+  R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
 }
-template <bool kPbr, bool kNrc = false, bool kSel = true>
+template <bool kPbr, bool kNrc = false>
 __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float2 jit,
                               int *stack, size_t slot = 0) {
   bool queried = false;
-  const float3 c = path_sample_body<kPbr, kNrc, kSel>(A, x, y, si, frame, jit, stack, slot, queried);
+  const float3 c = path_sample_body<kPbr, kNrc>(A, x, y, si, frame, jit, stack, slot, queried);
   if (kNrc && !queried) nrc_store_none(A, slot);
   return c;
 }
@@ -1330,7 +1334,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
-      const float3 c = path_sample<kPbr, kNrc, false>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack,
+      const float3 c = path_sample<kPbr, kNrc>(A, x, y, A.first + k, A.firstFrame + k, A.jitter[k], stack,
                                                (size_t)k * npix + p);
       sr += c.x;
       sg += c.y;
@@ -1354,9 +1358,7 @@ constexpr int kNrcRecords = 8;  // records per training path: its first 8 vertic
 // record: its cache query and, as target, the radiance the rest of the path brought to it, rgb of
 // the lanes' (R_end - R_i) / T_i, R_i the path's radiance when it reached vertex i (after that
 // vertex's emission) and T_i its throughput there. Records go to consecutive slots claimed with
-// one atomic per path; those past `cap` are dropped. Its traversals use the select form of the
-// triangle test (intersect_tri<true>): with the array form this kernel's traversal stack read back
-// a vertex coordinate.
+// one atomic per path; those past `cap` are dropped.
 template <bool kPbr>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     k_nrc_paths(RenderArgs A, uint32_t npaths, uint32_t offset, uint32_t stride, uint32_t si0, uint32_t cap,
@@ -1377,7 +1379,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
   float3 dir = camera_dir(A, x, y, jit), o = A.cam;
   lens_ray(A, o, dir, seed);
   Hit h;
-  if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return;
+  if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return;
   seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
   Surface S = surface_at(A, h, o, dir);
   vt_material m = material(A, S.slot);
@@ -1397,7 +1399,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
   }
-  R = add4(R, direct_light_lanes<kPbr, true>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
+  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
   int scattering = 0;
   for (int bounce = 1; scattering < limit; ++bounce) {
     ++scattering;
@@ -1418,11 +1420,11 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     const float3 prev = S.pos;
     o = ray_origin(A, S.pos, S.gn, nd, S.err);
     dir = nd;
-    if (!rt_closest<true>(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
+    if (!rt_closest(A, o, dir, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) {
       // An escape sees the environment, weighed against its NEE density at the last vertex.
       if (A.env) {
         const float lpdf = environment_pdf(A, dir, S.n);
-        const float w = lpdf <= 0.0f ? 1.0f : power_heuristic(bpdf, lpdf);
+        const float w = emission_weight(false, true, true, bpdf, lpdf);
         R = add4(R, scale4(mul4(T, emission3(A, L, environment(A, dir))), w));
       }
       break;
@@ -1431,7 +1433,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
-      const float w = lpdf <= 0.0f ? 1.0f : power_heuristic(bpdf, lpdf);
+      const float w = emission_weight(false, true, true, bpdf, lpdf);
       if (!A.imported || S.front) R = add4(R, scale4(mul4(T, emission(A, L, m.emission)), w));
       break;
     }
@@ -1441,7 +1443,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
       ++nrec;
     }
-    R = add4(R, direct_light_lanes<kPbr, true>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
+    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
                                          stack, false));
     if (bounce > 3) {
       const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
@@ -1559,7 +1561,7 @@ __global__ void __launch_bounds__(256) k_render_batch(const RenderArgs *__restri
       const uint32_t x = p % A.W, y = p / A.W, f0 = firstSample[lo], fr0 = firstFrame[lo];
       double sr = 0.0, sg = 0.0, sb = 0.0;
       for (uint32_t k = 0; k < A.spp; ++k) {
-        const float3 c = path_sample<kPbr, false, false>(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
+        const float3 c = path_sample<kPbr, false>(A, x, y, f0 + k, fr0 + k, frame_jitter(f0 + k), stack);
         sr += c.x; sg += c.y; sb += c.z;
       }
       double *acc = A.accum + 3 * (size_t)p;
@@ -2580,5 +2582,59 @@ extern "C" vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t heig
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   cudaFree(d);
   if (e != cudaSuccess) return vt_cuda_fail(ctx, e, "vt_sampler_frame");
+  return VT_OK;
+}
+
+// ---- the reference's device known answers (regression_checks, tests/GPUChecks.swift:14-37) ------
+// One thread evaluates the device functions on the reference's own inputs; the host compares.
+//   out[0]     power_heuristic(1e-10, 1e-10) (expected 0.5)
+//   out[1..3]  emission_weight(false, true, false, 0.2, 1), (true, true, true, 0, 1),
+//              (false, false, false, 0.2, 1) (expected 0, 1, 1)
+//   out[4]     the second PCG draw from seed 890625759 (expected exactly 0)
+//   out[5]     dot(n, sample_cosine_hemisphere(n, seed 890625759)) for the grazing normal
+//              normalize(0.31456656, 0, -0.9492354) (expected > 1e-4: above the tangent plane)
+//   out[6..7]  min and max of rand_f over 100,000 draws from seed 17 (expected in [0, 1))
+//   out[8..10] scattering_limit of depths 0, 1 and 8 (main.swift:3471-3473; expected 0, 0, 7)
+namespace {
+__global__ void k_known_answers(float *out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  out[0] = power_heuristic(1e-10f, 1e-10f);
+  out[1] = emission_weight(false, true, false, 0.2f, 1.0f);
+  out[2] = emission_weight(true, true, true, 0.0f, 1.0f);
+  out[3] = emission_weight(false, false, false, 0.2f, 1.0f);
+  uint32_t g = 890625759u;
+  const float r0 = pcg_rand(g), r1 = pcg_rand(g);
+  out[4] = r1;
+  const float3 n = normalize3(f3(0.31456656f, 0.0f, -0.9492354f));
+  out[5] = dot3(n, cosine_hemisphere(n, r0, r1));
+  uint32_t s = 17u;
+  float lo = 1.0f, hi = 0.0f;
+  for (int i = 0; i < 100000; ++i) {
+    const float v = pcg_rand(s);
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+  out[6] = lo;
+  out[7] = hi;
+  const uint32_t depths[3] = {0u, 1u, 8u};
+  for (int k = 0; k < 3; ++k) out[8 + k] = float(max(0, (int)depths[k] - 1));
+}
+}  // namespace
+
+extern "C" vt_status vt_known_answers(vt_ctx *ctx, float *out, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!out || n < VT_KNOWN_ANSWERS) return vt_fail(ctx, VT_ERR_INVALID, "out must hold VT_KNOWN_ANSWERS floats");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  float *d = nullptr;
+  VT_CUDA(ctx, cudaMalloc(&d, VT_KNOWN_ANSWERS * sizeof(float)));
+  cudaError_t e = cudaMemsetAsync(d, 0xff, VT_KNOWN_ANSWERS * sizeof(float), ctx->stream);
+  if (e == cudaSuccess) {
+    k_known_answers<<<1, 32, 0, ctx->stream>>>(d);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, VT_KNOWN_ANSWERS * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return vt_cuda_fail(ctx, e, "vt_known_answers");
   return VT_OK;
 }

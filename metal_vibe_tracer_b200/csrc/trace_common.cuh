@@ -85,34 +85,24 @@ __device__ __forceinline__ float edge_fn(float px, float py, float qx, float qy)
   return e;
 }
 
-// Two-sided hit in [tMin, tMax) (main.swift:1564-1579). kSelect picks the permuted coordinates with
-// selects (comp3); otherwise they are indexed from three-element arrays, which the compiler keeps in
-// local memory. The arrays cost fewer registers (the integrator's megakernels run 25 % faster with
-// them), but in two integrator kernels their local slots overlapped the traversal stack: a stack entry
-// popped right after its push read back a vertex coordinate. The integrator selects everywhere except
-// in its two throughput megakernels (render.cu: k_render, k_render_batch), which run every test clean
-// with the arrays.
-template <bool kSelect = true>
+// Two-sided hit in [tMin, tMax) (main.swift:1564-1579). The ray's permuted coordinates are picked
+// with selects (comp3), so the test keeps every value in registers. The shear of each vertex,
+// A[kx] - Sx A[kz], is one fused multiply-add (a single rounding), and so is each step of the
+// numerator T; the edge functions keep the reference's separately rounded products with the exact
+// fallback on ties (main.swift:1557-1562). The CPU oracle uses the same operations (std::fma), so
+// hits compare bit for bit. Each vertex is transformed on its own, from the vertex and the ray only,
+// so an edge shared by two triangles gets the same edge-function value in both: the test stays
+// watertight.
 __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b, float4 c, float tMin,
                                               float tMax, float &t, float &b1, float &b2) {
-  float ax, ay, bx, by, cx, cy, Akz, Bkz, Ckz;
-  if constexpr (kSelect) {
-    const float A0 = __fsub_rn(a.x, r.ox), A1 = __fsub_rn(a.y, r.oy), A2 = __fsub_rn(a.z, r.oz);
-    const float B0 = __fsub_rn(b.x, r.ox), B1 = __fsub_rn(b.y, r.oy), B2 = __fsub_rn(b.z, r.oz);
-    const float C0 = __fsub_rn(c.x, r.ox), C1 = __fsub_rn(c.y, r.oy), C2 = __fsub_rn(c.z, r.oz);
-    Akz = comp3(A0, A1, A2, r.kz); Bkz = comp3(B0, B1, B2, r.kz); Ckz = comp3(C0, C1, C2, r.kz);
-    ax = __fsub_rn(comp3(A0, A1, A2, r.kx), __fmul_rn(r.Sx, Akz)); ay = __fsub_rn(comp3(A0, A1, A2, r.ky), __fmul_rn(r.Sy, Akz));
-    bx = __fsub_rn(comp3(B0, B1, B2, r.kx), __fmul_rn(r.Sx, Bkz)); by = __fsub_rn(comp3(B0, B1, B2, r.ky), __fmul_rn(r.Sy, Bkz));
-    cx = __fsub_rn(comp3(C0, C1, C2, r.kx), __fmul_rn(r.Sx, Ckz)); cy = __fsub_rn(comp3(C0, C1, C2, r.ky), __fmul_rn(r.Sy, Ckz));
-  } else {
-    float A[3] = {__fsub_rn(a.x, r.ox), __fsub_rn(a.y, r.oy), __fsub_rn(a.z, r.oz)};
-    float B[3] = {__fsub_rn(b.x, r.ox), __fsub_rn(b.y, r.oy), __fsub_rn(b.z, r.oz)};
-    float C[3] = {__fsub_rn(c.x, r.ox), __fsub_rn(c.y, r.oy), __fsub_rn(c.z, r.oz)};
-    Akz = A[r.kz]; Bkz = B[r.kz]; Ckz = C[r.kz];
-    ax = __fsub_rn(A[r.kx], __fmul_rn(r.Sx, Akz)); ay = __fsub_rn(A[r.ky], __fmul_rn(r.Sy, Akz));
-    bx = __fsub_rn(B[r.kx], __fmul_rn(r.Sx, Bkz)); by = __fsub_rn(B[r.ky], __fmul_rn(r.Sy, Bkz));
-    cx = __fsub_rn(C[r.kx], __fmul_rn(r.Sx, Ckz)); cy = __fsub_rn(C[r.ky], __fmul_rn(r.Sy, Ckz));
-  }
+  const float A0 = __fsub_rn(a.x, r.ox), A1 = __fsub_rn(a.y, r.oy), A2 = __fsub_rn(a.z, r.oz);
+  const float B0 = __fsub_rn(b.x, r.ox), B1 = __fsub_rn(b.y, r.oy), B2 = __fsub_rn(b.z, r.oz);
+  const float C0 = __fsub_rn(c.x, r.ox), C1 = __fsub_rn(c.y, r.oy), C2 = __fsub_rn(c.z, r.oz);
+  const float Akz = comp3(A0, A1, A2, r.kz), Bkz = comp3(B0, B1, B2, r.kz), Ckz = comp3(C0, C1, C2, r.kz);
+  const float nSx = -r.Sx, nSy = -r.Sy;
+  const float ax = __fmaf_rn(nSx, Akz, comp3(A0, A1, A2, r.kx)), ay = __fmaf_rn(nSy, Akz, comp3(A0, A1, A2, r.ky));
+  const float bx = __fmaf_rn(nSx, Bkz, comp3(B0, B1, B2, r.kx)), by = __fmaf_rn(nSy, Bkz, comp3(B0, B1, B2, r.ky));
+  const float cx = __fmaf_rn(nSx, Ckz, comp3(C0, C1, C2, r.kx)), cy = __fmaf_rn(nSy, Ckz, comp3(C0, C1, C2, r.ky));
   const float U = edge_fn(cx, cy, bx, by), V = edge_fn(ax, ay, cx, cy);
   if ((U < 0.0f && V > 0.0f) || (U > 0.0f && V < 0.0f)) return false;
   const float W = edge_fn(bx, by, ax, ay);
@@ -120,7 +110,7 @@ __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b,
   const float det = __fadd_rn(__fadd_rn(U, V), W);
   if (det == 0.0f) return false;
   const float az = __fmul_rn(r.Sz, Akz), bz = __fmul_rn(r.Sz, Bkz), cz = __fmul_rn(r.Sz, Ckz);
-  const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, az), __fmul_rn(V, bz)), __fmul_rn(W, cz));
+  const float T = __fmaf_rn(W, cz, __fmaf_rn(V, bz, __fmul_rn(U, az)));
   const float inv = __fdiv_rn(1.0f, det);
   t = __fmul_rn(T, inv);
   b1 = __fmul_rn(V, inv);

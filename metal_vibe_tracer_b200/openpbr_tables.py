@@ -18,7 +18,14 @@ import numpy as np
 
 PKG = Path(__file__).resolve().parent
 DATA = PKG / "data" / "openpbr_energy.bin"
-REFERENCE_DATA = Path("/root/reference/Vendor/OpenPBR/impl/data")
+
+
+def reference_data() -> Path | None:
+    """The vendored OpenPBR data directory of the reference checkout named by VT_REFERENCE_ROOT (see
+    spectral_tables.reference_root); None when unset."""
+    from .spectral_tables import reference_root
+    r = reference_root()
+    return r / "Vendor" / "OpenPBR" / "impl" / "data" if r else None
 MAGIC = b"VTPBR001"
 N = 32
 
@@ -28,7 +35,10 @@ def _read_values(path: Path) -> np.ndarray:
     return np.array([int(v) for v in re.findall(r"\d+", text)], np.uint16)
 
 
-def generate(data_dir: Path = REFERENCE_DATA) -> Path:
+def generate(data_dir: Path | None = None) -> Path:
+    data_dir = data_dir or reference_data()
+    if data_dir is None:
+        raise RuntimeError("OpenPBR data: set VT_REFERENCE_ROOT to the reference checkout")
     energy = _read_values(data_dir / "openpbr_opaque_dielectric_energy_complement_data.h")
     average = _read_values(data_dir / "openpbr_opaque_dielectric_avg_energy_complement_data.h")
     if energy.size != N ** 3 or average.size != N ** 2:

@@ -228,6 +228,15 @@ def sampler_frame(ctx: Context, width: int, height: int, z: bool, model: int, sa
     return out
 
 
+def known_answers(ctx: Context) -> np.ndarray:
+    """The reference's device known answers (regression_checks, tests/GPUChecks.swift:14-37) as the
+    integrator's device functions compute them: power heuristic, emission weights, the grazing
+    cosine sample, rand_f's range and the scattering budget (layout in include/vt.h)."""
+    out = np.empty(_lib.KNOWN_ANSWERS, np.float32)
+    _check(ctx.handle, _lib.load().vt_known_answers(ctx.handle, out.ctypes.data, out.size), "vt_known_answers")
+    return out
+
+
 class Batch:
     """Scenes rendered by one persistent launch per pass (vt_batch): each pass adds spp[i] frames to
     scene i. The first six passes try launch shapes; later passes replay a captured CUDA graph."""

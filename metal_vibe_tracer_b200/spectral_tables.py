@@ -35,6 +35,7 @@ from __future__ import annotations
 
 import csv
 import math
+import os
 import struct
 from pathlib import Path
 
@@ -42,8 +43,37 @@ import numpy as np
 
 PKG = Path(__file__).resolve().parent
 DATA_DIR = PKG / "data"
-REFERENCE_CIE = Path("/root/reference/Vendor/Spectral/CIE")
-REFERENCE_WARP = Path("/root/reference/Vendor/Spectral/Peters2019/XYZWarp.h")
+REFERENCE_ENV = "VT_REFERENCE_ROOT"
+
+
+def reference_root() -> Path | None:
+    """The checkout of the reference (gabinfor/metal-vibe-tracer) whose vendored data the build-time
+    generators read, from the VT_REFERENCE_ROOT environment variable; None when it is unset. The
+    build recipe (__graft_entry__.build) and the test set-up give it their default checkout path when
+    unset. Run-time code never reads the reference: it loads the generated files under data/."""
+    v = os.environ.get(REFERENCE_ENV)
+    return Path(v) if v else None
+
+
+def reference_cie() -> Path | None:
+    r = reference_root()
+    return r / "Vendor" / "Spectral" / "CIE" if r else None
+
+
+def reference_warp() -> Path | None:
+    r = reference_root()
+    return r / "Vendor" / "Spectral" / "Peters2019" / "XYZWarp.h" if r else None
+
+
+def have_reference_data() -> bool:
+    c = reference_cie()
+    return c is not None and (c / "CIE_xyz_1931_2deg.csv").exists()
+
+
+def _need(path: Path | None, what: str) -> Path:
+    if path is None:
+        raise RuntimeError(f"{what}: set {REFERENCE_ENV} to the reference checkout (its vendored data is read at build time)")
+    return path
 UPLIFT_MIN, UPLIFT_MAX = 360, 830
 SRGB_PRIMARIES = ((0.64, 0.33), (0.30, 0.60), (0.15, 0.06))
 ICDF_SEGMENTS = 1024
@@ -82,7 +112,8 @@ def _apply(m, v):
     return [m[r][0] * v[0] + m[r][1] * v[1] + m[r][2] * v[2] for r in range(3)]
 
 
-def compute(lambda_min: int, lambda_max: int, cie_dir: Path = REFERENCE_CIE) -> dict:
+def compute(lambda_min: int, lambda_max: int, cie_dir: Path | None = None) -> dict:
+    cie_dir = _need(cie_dir or reference_cie(), "CIE datasets")
     """All tables in float64 (lists), from the CIE CSVs."""
     wl = list(range(lambda_min, lambda_max + 1))
     cmf_rows = _read(cie_dir / "CIE_xyz_1931_2deg.csv")
@@ -110,7 +141,8 @@ def compute(lambda_min: int, lambda_max: int, cie_dir: Path = REFERENCE_CIE) -> 
             "illum": d65, "icdf": icdf, "xyz_to_rgb": xyz_to_rgb, "density": density}
 
 
-def read_warp(path: Path = REFERENCE_WARP) -> list:
+def read_warp(path: Path | None = None) -> list:
+    path = _need(path or reference_warp(), "XYZ warp")
     """The 95 nodes of Peters' even XYZ phase warp (-pi at 360 nm ... 0 at 830 nm, 5 nm apart)."""
     text = path.read_text()
     key = "pXYZWarpEven[] = {"
@@ -129,7 +161,9 @@ def warp_phase(warp, lam: float) -> float:
     return warp[i] * (1.0 - f) + warp[i + 1] * f
 
 
-def uplift_model(cie_dir: Path = REFERENCE_CIE, warp_path: Path = REFERENCE_WARP) -> dict:
+def uplift_model(cie_dir: Path | None = None, warp_path: Path | None = None) -> dict:
+    cie_dir = _need(cie_dir or reference_cie(), "CIE datasets")
+    warp_path = _need(warp_path or reference_warp(), "XYZ warp")
     """The uplift's colour model over 360-830 nm in float64: per nm weights (rgb CMF x D65, Y = 1)
     and cos of the warped phase."""
     t = compute(UPLIFT_MIN, UPLIFT_MAX, cie_dir)
@@ -169,8 +203,10 @@ def path(lambda_min: int = 380, lambda_max: int = 780) -> Path:
     return DATA_DIR / f"spectral_{lambda_min}_{lambda_max}.bin"
 
 
-def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path = REFERENCE_CIE,
-             warp_path: Path = REFERENCE_WARP) -> Path:
+def generate(lambda_min: int = 380, lambda_max: int = 780, cie_dir: Path | None = None,
+             warp_path: Path | None = None) -> Path:
+    cie_dir = _need(cie_dir or reference_cie(), "CIE datasets")
+    warp_path = _need(warp_path or reference_warp(), "XYZ warp")
     """Write the table file (build time; needs the CIE CSVs and the warp)."""
     t = compute(lambda_min, lambda_max, cie_dir)
     u = uplift_model(cie_dir, warp_path)

@@ -57,9 +57,10 @@ inline Box face_box(const vt_face &f, const vt_vertex *v) {
 
 // ------------------------------------------------------------------------------------------
 // Watertight ray/triangle test (main.swift:1536-1582). The ray is translated to the origin and
-// sheared/scaled onto +z once; each vertex maps to (A[kx] - Sx A[kz], A[ky] - Sy A[kz], Sz A[kz]);
-// edge functions are fl(fl(p.x q.y) - fl(p.y q.x)) with the exact FMA tie fallback; a hit needs
-// all edge signs to agree (0 counts for both), det != 0 and t in [tMin, tMax).
+// sheared/scaled onto +z once; each vertex maps to (fma(-Sx, A[kz], A[kx]), fma(-Sy, A[kz], A[ky]),
+// Sz A[kz]); edge functions are fl(fl(p.x q.y) - fl(p.y q.x)) with the exact FMA tie fallback
+// (main.swift:1557-1562); a hit needs all edge signs to agree (0 counts for both), det != 0 and t in
+// [tMin, tMax); the numerator is fma(W, cz, fma(V, bz, U az)).
 template <typename T> struct WRay {
   T o[3];
   int kx, ky, kz;
@@ -89,9 +90,10 @@ bool intersect_tri(const WRay<T> &r, const T a[3], const T b[3], const T c[3], T
                    T &b1, T &b2) {
   T A[3], B[3], C[3];
   for (int k = 0; k < 3; ++k) { A[k] = a[k] - r.o[k]; B[k] = b[k] - r.o[k]; C[k] = c[k] - r.o[k]; }
-  T ax = A[r.kx] - r.Sx * A[r.kz], ay = A[r.ky] - r.Sy * A[r.kz];
-  T bx = B[r.kx] - r.Sx * B[r.kz], by = B[r.ky] - r.Sy * B[r.kz];
-  T cx = C[r.kx] - r.Sx * C[r.kz], cy = C[r.ky] - r.Sy * C[r.kz];
+  // The shear is one fused multiply-add per coordinate, as the CUDA test computes it.
+  T ax = std::fma(-r.Sx, A[r.kz], A[r.kx]), ay = std::fma(-r.Sy, A[r.kz], A[r.ky]);
+  T bx = std::fma(-r.Sx, B[r.kz], B[r.kx]), by = std::fma(-r.Sy, B[r.kz], B[r.ky]);
+  T cx = std::fma(-r.Sx, C[r.kz], C[r.kx]), cy = std::fma(-r.Sy, C[r.kz], C[r.ky]);
   T U = edge_fn(cx, cy, bx, by), V = edge_fn(ax, ay, cx, cy);
   if ((U < 0 && V > 0) || (U > 0 && V < 0)) return false;
   T W = edge_fn(bx, by, ax, ay);
@@ -99,7 +101,7 @@ bool intersect_tri(const WRay<T> &r, const T a[3], const T b[3], const T c[3], T
   T det = (U + V) + W;
   if (det == T(0)) return false;
   T az = r.Sz * A[r.kz], bz = r.Sz * B[r.kz], cz = r.Sz * C[r.kz];
-  T Tn = (U * az + V * bz) + W * cz;
+  T Tn = std::fma(W, cz, std::fma(V, bz, U * az));
   T inv = T(1) / det;
   t = Tn * inv;
   b1 = V * inv;

@@ -67,6 +67,11 @@ def test_build_rejects_bad_input(ctx):
     bad["b"][17] = len(verts)
     with pytest.raises(vt.MaterialLibraryError, match="indexes past"):
         vt.Mesh(ctx, bad, verts)
+    # An index far past the vertex array: no kernel of the build reads its vertex.
+    far = faces.copy()
+    far["c"][3] = 0xFFFFFFFF
+    with pytest.raises(vt.MaterialLibraryError, match="indexes past"):
+        vt.Mesh(ctx, far, verts)
     v = verts.copy()
     v["p"][5, 1] = np.nan
     with pytest.raises(vt.MaterialLibraryError, match="not finite"):

@@ -16,7 +16,7 @@ import pytest
 from metal_vibe_tracer_b200 import scenes, spectral_tables
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "spectral_360_830.json"
-HAVE_CIE = (spectral_tables.REFERENCE_CIE / "CIE_xyz_1931_2deg.csv").exists()
+HAVE_CIE = spectral_tables.have_reference_data()
 
 
 @pytest.mark.skipif(not HAVE_CIE, reason="CIE datasets are read from the reference checkout")
