@@ -63,6 +63,13 @@ def parse():
                    help="after the training frames, the cache trains on every n-th rendered frame")
     p.add_argument("--nrc-levels", type=int, default=8,
                    help="hash-grid levels of the radiance cache (8 reach the same spp at relMSE 1e-3 on the Cornell box as 16, in cheaper frames)")
+    p.add_argument("--c5", type=int, default=1, help="1: measure config C5 (the cache on the production scene)")
+    p.add_argument("--c5-stride", type=int, default=8, help="pixel stride of C5's FP64 reference and relMSE")
+    p.add_argument("--c5-ref-spp", type=int, default=65536, help="spp of C5's FP64 reference")
+    p.add_argument("--c5-ref-file", default="", help="resume/save C5's reference accumulation (.npz)")
+    p.add_argument("--c5-max-s", type=float, default=60.0, help="device-time cap per C5 arm, seconds")
+    p.add_argument("--c5-check", type=int, default=16, help="spp between C5's relMSE checks")
+    p.add_argument("--c5-pretrain", type=int, default=32, help="training-only frames of C5's cache, timed")
     p.add_argument("--nrc-records", type=int, default=16384,
                    help="cache training records per frame (a quarter of the 256x256 image's pixels)")
     return p.parse_args()
@@ -266,7 +273,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
         from metal_vibe_tracer_b200.nrc import RadianceCache
         info = mesh.info()
         cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records,
-                              levels=a.nrc_levels)
+                              levels=a.nrc_levels, spectral=1)
         scene.reset()
         e0.record(stream)
         for f in range(a.nrc_pretrain):
@@ -301,7 +308,7 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     # one small untimed frame loads them before the timed arms.
     from metal_vibe_tracer_b200.nrc import RadianceCache
     info0 = mesh.info()
-    warm = RadianceCache(ctx, list(info0.lo), list(info0.hi), seed=1, train_records=4096)
+    warm = RadianceCache(ctx, list(info0.lo), list(info0.hi), seed=1, train_records=4096, spectral=1)
     for mode in (0, 1):
         warm.render(scene, vt.make_params(cam, 64, 64, depth, 1, True, mode), 2, stream=cs)
     torch.cuda.synchronize()
@@ -429,6 +436,125 @@ def bench_production(a, ctx, stream) -> dict:
     return out
 
 
+def bench_nrc_c5(a, ctx, stream) -> dict:
+    """Config C5: the radiance cache on the production scene (9.9M triangles, 102k emitters under a
+    light tree, 287 OPENPBR slots) at 1920x1080, spectral, depth 12, against plain MIS path tracing
+    and ReSTIR DI (32 candidates): device time to relMSE 1e-3 against a 65,536-spp FP64-accumulated
+    MIS reference. The reference and the relMSE cover every `c5_stride`-th pixel in x and y (the
+    frame's own camera rays and sample streams at those pixels, vt_frame_params.pixel_stride): a
+    uniform sample of the image's pixels, which makes the 64k-spp reference affordable. The cache:
+    16 levels x 2^19 x 2 features, 65,536 training records per frame, the spread-angle heuristic
+    (c = 0.01), trained from scratch inside the timed region. An arm that does not reach the bar in
+    `c5_max_s` device seconds reports the relMSE it reached; for the unbiased arms the time is then
+    extrapolated with relMSE proportional to 1 / spp (marked as such)."""
+    import torch
+
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes, spectral_tables
+    from metal_vibe_tracer_b200.nrc import RadianceCache
+
+    faces, verts, mats, cam = scenes.production_scene(seed=0)
+    mesh = vt.Mesh(ctx, faces, verts)
+    info = mesh.info()
+    tables = spectral_tables.load()
+    W, H, depth, S = 1920, 1080, 12, max(1, a.c5_stride)
+    cs = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # The FP64 reference: MIS, strided, resumable.
+    ref_scene = vt.Scene(ctx, mesh, mats, None, tables)
+    done = 0
+    if a.c5_ref_file and Path(a.c5_ref_file).exists():
+        done = ref_scene.restore_accumulation(a.c5_ref_file)
+    t_ref = time.perf_counter()
+    chunk = 1024
+    while done < a.c5_ref_spp:
+        n = min(chunk, a.c5_ref_spp - done)
+        params = vt.make_params(cam, W, H, depth, done + 1, True, 1, pixel_stride=S)
+        ref_scene.render(params, n, cs)
+        done += n
+        if a.c5_ref_file and (done % 8192 == 0 or done >= a.c5_ref_spp):
+            torch.cuda.synchronize()
+            ref_scene.save_accumulation(a.c5_ref_file, params)
+    torch.cuda.synchronize()
+    ref_wall = time.perf_counter() - t_ref
+    ref, nref = ref_scene.readback()
+    ref_scene.close()
+
+    def rel(img):
+        return rel_mse(img[::S, ::S], ref)
+
+    scene = vt.Scene(ctx, mesh, mats, None, tables)
+
+    def arm(mode, cand, cache=None, per=1):
+        """Frames of `per` spp until relMSE <= 1e-3 or the time cap: (device s, spp, relMSE)."""
+        scene.reset()
+        total, spp_done, err = 0.0, 0, None
+        if cache is not None:
+            e0.record(stream)
+            for f in range(a.c5_pretrain):
+                cache.render(scene, vt.make_params(cam, W, H, depth, 1 + f, True, mode, di_candidates=cand), 0,
+                             render=False, stream=cs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total = e0.elapsed_time(e1) / 1e3
+        next_check = a.c5_check
+        while total < a.c5_max_s:
+            e0.record(stream)
+            while spp_done < next_check:
+                params = vt.make_params(cam, W, H, depth, 1 + spp_done, True, mode, di_candidates=cand)
+                if cache is not None:
+                    cache.render(scene, params, per, stream=cs)
+                else:
+                    scene.render(params, per, cs)
+                spp_done += per
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1) / 1e3
+            img, _ = scene.readback()
+            err = rel(img)
+            if err <= 1e-3:
+                break
+            next_check = spp_done + max(a.c5_check, spp_done // 4)
+        return total, spp_done, err
+
+    out = {"workload": "config C5: production grid scene (%d triangles, 287 OPENPBR slots, light tree), 1920x1080, "
+                       "spectral, depth 12; relMSE of luminance on every %d-th pixel in x and y" % (len(faces), S),
+           "reference_spp": nref, "reference_wall_s": ref_wall, "pixel_stride": S,
+           "cache": {"levels": 16, "log2_table": 19, "train_records": 65536, "query": "spread-angle heuristic, c = 0.01",
+                     "pretrain_frames": a.c5_pretrain},
+           "definition": "device time of the frames (the cache's training from scratch included) until the relMSE of "
+                         "luminance (scripts/compare_mitsuba.py:353-354) on the strided pixels is <= 1e-3; readbacks "
+                         "untimed"}
+    # One untimed frame of each kernel family first (module loads).
+    scene.render(vt.make_params(cam, 64, 64, depth, 1, True, 1), 1, cs)
+    scene.render(vt.make_params(cam, 64, 64, depth, 1, True, 0, di_candidates=32), 1, cs)
+    torch.cuda.synchronize()
+    for name, mode, cand in (("plain_pt", 1, 0), ("restir_di", 0, 32)):
+        t, n, err = arm(mode, cand)
+        r = {"s": t, "spp": n, "relmse": err, "ms_per_spp": 1e3 * t / max(n, 1), "reached": err is not None and err <= 1e-3}
+        if not r["reached"] and err:
+            r["extrapolated_s"] = t * err / 1e-3
+        out[name] = r
+    for name, mode, cand in (("nrc_restir", 0, 32), ("nrc_mis", 1, 0)):
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=65536, levels=16,
+                              log2_table=19, spectral=1)
+        t, n, err = arm(mode, cand, cache)
+        ci = cache.info()
+        cache.close()
+        out[name] = {"s": t, "spp": n, "relmse": err, "reached": err is not None and err <= 1e-3,
+                     "loss": ci["last_loss"], "steps": ci["steps"]}
+    base = out["plain_pt"]["s"] if out["plain_pt"]["reached"] else out["plain_pt"].get("extrapolated_s")
+    for name in ("nrc_restir", "nrc_mis", "restir_di"):
+        r = out[name]
+        t = r["s"] if r["reached"] else r.get("extrapolated_s")
+        r["speedup_vs_plain_pt"] = (base / t) if (base and t) else None
+    out["target"] = "NRC+ReSTIR >= 3x less time than plain path tracing to relMSE 1e-3"
+    scene.close()
+    mesh.close()
+    return out
+
+
 # ---- our arm ----------------------------------------------------------------------------------
 def profile_nrc(a) -> int:
     """A short radiance-cache sequence for ncu: the spectral Cornell box at 256 x 256, a cache with
@@ -442,7 +568,7 @@ def profile_nrc(a) -> int:
     mesh = vt.Mesh(ctx, faces, verts)
     scene = vt.Scene(ctx, mesh, mats, light, spectral_tables.load())
     info = mesh.info()
-    cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records)
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), seed=7, train_records=a.nrc_records, spectral=1)
     for f in range(4):
         cache.render(scene, vt.make_params(cam, 256, 256, 8, 1 + f, True, 1), 0, render=False)
     for f in range(3):
@@ -661,6 +787,9 @@ def main():
     batched = None
     if world == 1 and not a.no_cornell and a.batch_scenes > 0:
         batched = bench_batch(a, ctx)
+    c5 = None
+    if world == 1 and not a.no_cornell and a.c5:
+        c5 = bench_nrc_c5(a, ctx, stream)
 
     if rank == 0:
         line = {
@@ -678,6 +807,7 @@ def main():
             "cornell_pt": cornell,
             "production_scene": production,
             "batched_scenes": batched,
+            "nrc_c5": c5,
         }
         print(json.dumps(line))
     if world > 1:

@@ -214,6 +214,11 @@ typedef struct vt_frame_params {
   float aperture;           /* thin-lens radius, 0 = pinhole (Uniforms.lens.x, lens_ray,
                                main.swift:2210-2216) */
   float focus_distance;     /* distance to the plane in focus along the view axis (Uniforms.lens.y) */
+  uint32_t pixel_stride;    /* 0 or 1: every pixel; s > 1: only pixels (s i, s j) of the width x
+                               height frame, with the full frame's camera rays and sample streams,
+                               into a ceil(width / s) x ceil(height / s) accumulation (sampling
+                               modes 1-3; a subsampled render of the same image, for long reference
+                               renders and sampled error measurements) */
 } vt_frame_params;
 
 /* A renderable scene: the mesh, its material slots, the area light and (optionally) the spectral
@@ -230,9 +235,18 @@ vt_status vt_scene_destroy(vt_ctx *ctx, vt_scene *scene);
  * Stream-ordered; NULL = the CUDA default stream. */
 vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *params, uint32_t spp, void *stream);
 vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene);
-/* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3)
- * and the number of samples accumulated. Synchronises. */
+/* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3
+ * of the accumulation, ceil(width / s) * ceil(height / s) * 3 for a pixel stride s) and the number
+ * of samples accumulated. Synchronises. */
 vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t n, uint32_t *samples);
+/* Resumes an accumulation saved from vt_accum_readback: sets the scene's FP64 accumulation to
+ * rgb x samples (the FP64 sums) and its sample count to `samples`, for a width x height frame at
+ * pixel stride s (n as vt_accum_readback's). The next vt_render continues it (first_sample =
+ * samples + 1 continues the same sample streams). A long render (the 64k-spp FP64 reference) is
+ * taken in pieces this way. No counterpart in the reference, whose accumulation restarts on any
+ * change (main.swift:10993-11009). */
+vt_status vt_accum_restore(vt_ctx *ctx, vt_scene *scene, uint32_t width, uint32_t height, uint32_t pixel_stride,
+                           const double *rgb, uint32_t n, uint32_t samples);
 
 /* The ReSTIR DI reservoirs of the last frame rendered in sampling mode 0, for checking reuse: per
  * pixel (weight sum, M, W, wavelength number), 4 floats into the HOST array out (n = width *
@@ -459,13 +473,21 @@ typedef struct vt_nrc_config {
   uint32_t max_resolution;   /* cells per axis of the finest level (2048) */
   uint32_t train_records;    /* training records per optimiser step (65536) */
   uint32_t train_paths;      /* training paths per frame; 0: train_records / 4 */
-  uint32_t query_vertex;     /* rendered paths query the cache at this vertex, 1 = the first
-                                bounce's hit (1); vertices before it are traced as usual */
+  uint32_t query_vertex;     /* 0: rendered paths query the cache where their spread exceeds
+                                `spread` times the primary spread (the spread-angle heuristic of
+                                Mueller et al. 2021) (0); k >= 1: at vertex k, 1 = the first
+                                bounce's hit; vertices before it are traced as usual */
   uint32_t seed;             /* parameter initialisation and training-path pixels */
   float learning_rate;       /* Adam step size (0.01) */
   float beta1, beta2, epsilon;  /* Adam (0.9, 0.99, 1e-15) */
+  float spread;              /* the heuristic's constant c: a path stops at vertex n once
+                                (sum_i sqrt(|x_i-1 - x_i|^2 / (p(w_i) |cos theta_i|)))^2 > c a0,
+                                a0 = |x0 - x1|^2 / (4 pi cos theta_1) (0.01) */
+  uint32_t spectral;         /* 1: the outputs are, per hero wavelength of a path, its radiance
+                                times the lane's share 1 / (4 p(lambda)), and scenes render with
+                                spectral transport; 0: rgb (0) */
 } vt_nrc_config;
-/* A cache query (48 bytes). Directions are (theta / pi, phi / (2 pi) + 1/2), theta from +z and phi
+/* A cache query (64 bytes). Directions are (theta / pi, phi / (2 pi) + 1/2), theta from +z and phi
  * = atan2(y, x). */
 typedef struct vt_nrc_input {
   float position[3];
@@ -474,6 +496,9 @@ typedef struct vt_nrc_input {
   float normal[2];       /* shading normal */
   float diffuse[3];      /* diffuse reflectance: albedo x (1 - metalness) */
   float specular;        /* specular reflectance: metalness */
+  float wavelength;      /* the path's wavelength number u in [0, 1): its hero wavelengths are
+                            F^-1((u + k) / 4), k = 0..3 (spectral caches; 0 for rgb) */
+  float pad[3];
 } vt_nrc_input;
 typedef struct vt_nrc_info {
   unsigned long long mlp_params, grid_params;  /* 21,504; levels x 2^log2_table x 2 */
@@ -491,22 +516,27 @@ vt_status vt_nrc_destroy(vt_ctx *ctx, vt_nrc *nrc);
 /* Synchronises the context's stream and the cache's last step. */
 vt_status vt_nrc_get_info(vt_ctx *ctx, vt_nrc *nrc, vt_nrc_info *out);
 /* Parameters as fp32: mlp = 21,504 floats (5 hidden 64 x 64 matrices [out][in], then the output
- * layer 16 x 64 with rows 3-15 zero), grid = levels x 2^log2_table x 2 floats (may be NULL).
+ * layer 16 x 64 with rows 4-15 zero), grid = levels x 2^log2_table x 2 floats (may be NULL).
  * Setting them also clears Adam's moments and step count. */
 vt_status vt_nrc_get_params(vt_ctx *ctx, const vt_nrc *nrc, float *mlp, float *grid);
 vt_status vt_nrc_set_params(vt_ctx *ctx, vt_nrc *nrc, const float *mlp, const float *grid);
-/* Predictions for n host queries: rgb = n x 3 floats. */
-vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_t n, float *rgb);
-/* The loss and its gradient sums over n host records (targets n x 3), without an update: mlp_grad
- * 21,504 floats, grid_grad as vt_nrc_get_params' grid (may be NULL), loss the loss sum. */
+/* Predictions for n host queries: out = n x 4 floats (the four lanes' terms, or rgb and 0). The
+ * network runs on the tcgen05 tensor cores (M = 128 tiles, fp16 operands, fp32 accumulators in
+ * tensor memory). */
+vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_t n, float *out);
+/* The loss and its gradient sums over n host records (targets n x 4, as vt_nrc_infer's outputs),
+ * without an update: mlp_grad 21,504 floats, grid_grad as vt_nrc_get_params' grid (may be NULL),
+ * loss the loss sum. The backward pass runs with the loss scaled by 64 in fp16; the sums returned
+ * are the loss's own. */
 vt_status vt_nrc_gradients(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, const float *target, uint32_t n,
                            float *mlp_grad, float *grid_grad, double *loss);
 /* One Adam step on n host records; loss (may be NULL) receives their mean loss before the step. */
 vt_status vt_nrc_train(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, const float *target, uint32_t n, float *loss);
 /* One frame of spp samples with the cache, stream-ordered like vt_render. flags VT_NRC_TRAIN:
  * trace the frame's training paths (MIS, full depth) and take one optimiser step on their records
- * first; VT_NRC_RENDER: render spp samples per pixel whose paths end at the query vertex with the
- * cache's prediction (sampling modes 0 and 1), added to the scene's accumulation. */
+ * first; VT_NRC_RENDER: render spp samples per pixel whose paths end where the cache's query rule
+ * (query_vertex, spread) stops them, with the cache's prediction (sampling modes 0 and 1), added to
+ * the scene's accumulation. The frame's transport must match the cache's `spectral` setting. */
 vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_frame_params *p, uint32_t spp,
                         uint32_t flags, void *stream);
 

@@ -87,12 +87,14 @@ class NRCConfig(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
                 ("max_resolution", C.c_uint32), ("train_records", C.c_uint32), ("train_paths", C.c_uint32),
                 ("query_vertex", C.c_uint32), ("seed", C.c_uint32), ("learning_rate", C.c_float),
-                ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float)]
+                ("beta1", C.c_float), ("beta2", C.c_float), ("epsilon", C.c_float), ("spread", C.c_float),
+                ("spectral", C.c_uint32)]
 
 
 class NRCInput(C.Structure):
     _fields_ = [("position", C.c_float * 3), ("roughness", C.c_float), ("direction", C.c_float * 2),
-                ("normal", C.c_float * 2), ("diffuse", C.c_float * 3), ("specular", C.c_float)]
+                ("normal", C.c_float * 2), ("diffuse", C.c_float * 3), ("specular", C.c_float),
+                ("wavelength", C.c_float), ("pad", C.c_float * 3)]
 
 
 class NRCInfo(C.Structure):
@@ -134,6 +136,7 @@ SIGNATURES = {
     "vt_render": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_accum_reset": (_I32, [_P, _P]),
     "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
+    "vt_accum_restore": (_I32, [_P, _P, _U32, _U32, _U32, _P, _U32, _U32]),
     "vt_sampler_frame": (_I32, [_P, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _U32, _P]),
     "vt_known_answers": (_I32, [_P, _P, _U32]),
     "vt_light_tree_build": (_I32, [_P, _P, _U32, _U32, C.c_double, C.POINTER(_P)]),

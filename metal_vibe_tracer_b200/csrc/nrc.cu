@@ -10,6 +10,7 @@
 // dH = dZ W reads W the same way. Rows are padded to 72 halves (144 B), which keeps the fragment
 // loads and stores free of bank conflicts.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -24,7 +25,7 @@ constexpr int kInferRows = 256;  // inference rows per CTA (8 warps share the we
 constexpr size_t kInferSmem = (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kInferRows * kLd) * sizeof(__half);
 constexpr size_t kTrainSmem =
     (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kNrcTile * kLd * (kNrcHidden + 2)) * sizeof(__half);
-constexpr float kGradClip = 512.0f;  // per-output loss gradient bound (fp16 range of the backward pass)
+constexpr float kGradClip = 512.0f;  // per-output loss gradient bound before the loss scale (x 64 stays in fp16 range)
 
 __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
   x ^= x >> 16; x *= 0x7feb352du;
@@ -37,7 +38,7 @@ __device__ __forceinline__ float hash_uniform(uint32_t seed, uint64_t i) {
   return (float)(h >> 8) * (1.0f / 16777216.0f);
 }
 
-// Xavier-uniform hidden and output weights (output rows 3-15 zero); grid features U(-1e-4, 1e-4).
+// Xavier-uniform hidden and output weights (output rows 4-15 zero); grid features U(-1e-4, 1e-4).
 __global__ void k_nrc_init(float *__restrict__ p, uint64_t n, uint32_t seed) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const float u = hash_uniform(seed, i) * 2.0f - 1.0f;
@@ -46,7 +47,7 @@ __global__ void k_nrc_init(float *__restrict__ p, uint64_t n, uint32_t seed) {
       v = u * 0.21650635f;  // sqrt(6 / (64 + 64))
     } else if (i < (uint64_t)kNrcMlpParams) {
       const uint32_t r = (uint32_t)(i - (uint64_t)kNrcHidden * 4096u) >> 6;
-      v = r < 3u ? u * 0.29260868f : 0.0f;  // sqrt(6 / (64 + 6)); unused rows zero
+      v = r < (uint32_t)kNrcOut ? u * 0.29704426f : 0.0f;  // sqrt(6 / (64 + 4)); unused rows zero
     } else {
       v = u * 1e-4f;
     }
@@ -144,7 +145,8 @@ __device__ __forceinline__ void output_layer(const uint32_t (&a)[2][4][4], const
   }
 }
 
-// Inference: out[row] = (r, g, b, 0) for rows < n. Persistent CTAs over 256-row tiles.
+// Inference on the legacy tensor path (mma.sync): out[row] = the four outputs for rows < n.
+// Persistent CTAs over 256-row tiles.
 __global__ void __launch_bounds__(kInferRows, 2) k_nrc_infer(NrcGrid G, const float *__restrict__ mlp,
                                                         const NrcInput *__restrict__ in, uint32_t n,
                                                         float4 *__restrict__ out) {
@@ -173,8 +175,8 @@ __global__ void __launch_bounds__(kInferRows, 2) k_nrc_infer(NrcGrid G, const fl
       for (int mt = 0; mt < 2; ++mt) {
         const uint32_t r0 = base + row0 + 16 * mt + g, r1 = r0 + 8;
         float *o0 = reinterpret_cast<float *>(out + r0) + 2 * t, *o1 = reinterpret_cast<float *>(out + r1) + 2 * t;
-        if (r0 < n) *reinterpret_cast<float2 *>(o0) = make_float2(o[mt][0], t == 0 ? o[mt][1] : 0.0f);
-        if (r1 < n) *reinterpret_cast<float2 *>(o1) = make_float2(o[mt][2], t == 0 ? o[mt][3] : 0.0f);
+        if (r0 < n) *reinterpret_cast<float2 *>(o0) = make_float2(o[mt][0], o[mt][1]);
+        if (r1 < n) *reinterpret_cast<float2 *>(o1) = make_float2(o[mt][2], o[mt][3]);
       }
     }
     __syncthreads();  // X is rewritten by the next tile
@@ -239,15 +241,16 @@ __device__ __forceinline__ void relu_mask(float (&acc)[2][8][4], const __half *H
 }
 
 // Gradient sums of one batch (rows < min(*count, cap), or cap when count is null) under the relative
-// L2 loss sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01), lum with the prediction held constant (Mueller
-// et al. 2021): the weights' into gmlp, the grid features' into gtable (float2 atomics), the loss sum
-// into *loss. One CTA per 128-row tile.
+// L2 loss sum_c (p_c - y_c)^2 / (lum(p)^2 + 0.01) over the four outputs, lum = lumW . p held constant
+// (Mueller et al. 2021; lumW the luminance weights of rgb, or the lanes' mean for a spectral cache):
+// the weights' into gmlp, the grid features' into gtable (float2 atomics), both times kNrcLossScale,
+// and the loss sum into *loss. One CTA per 128-row tile.
 __global__ void __launch_bounds__(kNrcTile, 1) k_nrc_train(NrcGrid G, const float *__restrict__ mlp,
                                                            const NrcInput *__restrict__ in,
                                                            const float4 *__restrict__ target,
                                                            const uint32_t *__restrict__ count, uint32_t cap,
                                                            float *__restrict__ gmlp, float2 *__restrict__ gtable,
-                                                           float *__restrict__ loss) {
+                                                           float *__restrict__ loss, float4 lumW) {
   extern __shared__ __align__(16) __half sm[];
   __half *W = sm, *Wo = W + kNrcHidden * 64 * kLd, *X = Wo + kNrcOutRows * kLd, *H = X + kNrcTile * kLd,
          *DZ = H + kNrcHidden * kNrcTile * kLd;
@@ -277,37 +280,41 @@ __global__ void __launch_bounds__(kNrcTile, 1) k_nrc_train(NrcGrid G, const floa
   }
   float o[2][4];
   output_layer(a, Wo, g, t, o);
-  // Loss gradient per row, laid out as the A fragment of k-tile 0 (outputs 0-2 of 16).
+  // Loss gradient per row (clipped, then times the loss scale), laid out as the A fragment of
+  // k-tile 0 (outputs 0-3 of 16).
   uint32_t da[2][4][4];
   float lsum = 0.0f;
 #pragma unroll
   for (int mt = 0; mt < 2; ++mt) {
     const int q0 = lane & ~3, q1 = q0 | 1;
-    float p[2][3];
+    float p[2][4];
     p[0][0] = __shfl_sync(0xffffffffu, o[mt][0], q0);
     p[0][1] = __shfl_sync(0xffffffffu, o[mt][1], q0);
     p[0][2] = __shfl_sync(0xffffffffu, o[mt][0], q1);
+    p[0][3] = __shfl_sync(0xffffffffu, o[mt][1], q1);
     p[1][0] = __shfl_sync(0xffffffffu, o[mt][2], q0);
     p[1][1] = __shfl_sync(0xffffffffu, o[mt][3], q0);
     p[1][2] = __shfl_sync(0xffffffffu, o[mt][2], q1);
-    float d[2][3];
+    p[1][3] = __shfl_sync(0xffffffffu, o[mt][3], q1);
+    float d[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const uint32_t row = base + row0 + 16 * mt + g + 8 * h;
-      d[h][0] = d[h][1] = d[h][2] = 0.0f;
+      d[h][0] = d[h][1] = d[h][2] = d[h][3] = 0.0f;
       if (row < n) {
         const float4 y = __ldg(target + row);
-        const float lum = 0.2126f * p[h][0] + 0.7152f * p[h][1] + 0.0722f * p[h][2];
+        const float lum = lumW.x * p[h][0] + lumW.y * p[h][1] + lumW.z * p[h][2] + lumW.w * p[h][3];
         const float inv = 1.0f / (lum * lum + 0.01f);
-        const float e0 = p[h][0] - y.x, e1 = p[h][1] - y.y, e2 = p[h][2] - y.z;
-        if (t == 0) lsum += (e0 * e0 + e1 * e1 + e2 * e2) * inv;
-        d[h][0] = fminf(fmaxf(2.0f * e0 * inv, -kGradClip), kGradClip);
-        d[h][1] = fminf(fmaxf(2.0f * e1 * inv, -kGradClip), kGradClip);
-        d[h][2] = fminf(fmaxf(2.0f * e2 * inv, -kGradClip), kGradClip);
+        const float e0 = p[h][0] - y.x, e1 = p[h][1] - y.y, e2 = p[h][2] - y.z, e3 = p[h][3] - y.w;
+        if (t == 0) lsum += (e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3) * inv;
+        d[h][0] = fminf(fmaxf(2.0f * e0 * inv, -kGradClip), kGradClip) * kNrcLossScale;
+        d[h][1] = fminf(fmaxf(2.0f * e1 * inv, -kGradClip), kGradClip) * kNrcLossScale;
+        d[h][2] = fminf(fmaxf(2.0f * e2 * inv, -kGradClip), kGradClip) * kNrcLossScale;
+        d[h][3] = fminf(fmaxf(2.0f * e3 * inv, -kGradClip), kGradClip) * kNrcLossScale;
       }
     }
-    da[mt][0][0] = t == 0 ? nrc_pack(d[0][0], d[0][1]) : (t == 1 ? nrc_pack(d[0][2], 0.0f) : 0u);
-    da[mt][0][1] = t == 0 ? nrc_pack(d[1][0], d[1][1]) : (t == 1 ? nrc_pack(d[1][2], 0.0f) : 0u);
+    da[mt][0][0] = t == 0 ? nrc_pack(d[0][0], d[0][1]) : (t == 1 ? nrc_pack(d[0][2], d[0][3]) : 0u);
+    da[mt][0][1] = t == 0 ? nrc_pack(d[1][0], d[1][1]) : (t == 1 ? nrc_pack(d[1][2], d[1][3]) : 0u);
     da[mt][0][2] = da[mt][0][3] = 0u;
 #pragma unroll
     for (int kk = 1; kk < 4; ++kk) da[mt][kk][0] = da[mt][kk][1] = da[mt][kk][2] = da[mt][kk][3] = 0u;
@@ -321,7 +328,7 @@ __global__ void __launch_bounds__(kNrcTile, 1) k_nrc_train(NrcGrid G, const floa
   {
     float acc[2][4];
     weight_grad<1>(DZ, H + (kNrcHidden - 1) * kNrcTile * kLd, 0, 16 * warp, lane, acc);
-    if (g < 3) {
+    if (g < kNrcOut) {
       float *dst = gmlp + kNrcHidden * 4096 + g * 64 + 16 * warp + 2 * t;
 #pragma unroll
       for (int nt = 0; nt < 2; ++nt) {
@@ -399,7 +406,7 @@ __global__ void k_nrc_adam(float4 *__restrict__ p, float4 *__restrict__ m, float
                            uint32_t cap, float lr, float beta1, float beta2, float eps) {
   const uint32_t rows = count ? min(*count, cap) : cap;
   if (rows == 0u) return;
-  const float scale = 1.0f / float(rows);
+  const float scale = 1.0f / (float(rows) * kNrcLossScale);
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
     float4 gg = gsum[i];
     if (i >= dense4 && gg.x == 0.0f && gg.y == 0.0f && gg.z == 0.0f && gg.w == 0.0f) continue;
@@ -431,6 +438,11 @@ vt_status nrc_alloc(vt_ctx *ctx, void **p, size_t bytes) {
   return VT_OK;
 }
 
+// The loss normaliser's weights on the four outputs: rgb luminance, or the lanes' mean.
+float4 nrc_lum_weights(const vt_nrc *nrc) {
+  return nrc->cfg.spectral ? make_float4(0.25f, 0.25f, 0.25f, 0.25f) : make_float4(0.2126f, 0.7152f, 0.0722f, 0.0f);
+}
+
 vt_status nrc_check_config(vt_ctx *ctx, const vt_nrc_config &c) {
   if (c.levels < 1 || c.levels > (uint32_t)kNrcMaxLevels) return vt_fail(ctx, VT_ERR_INVALID, "levels must be 1-16");
   if (c.log2_table < 12 || c.log2_table > 24) return vt_fail(ctx, VT_ERR_INVALID, "log2_table must be 12-24");
@@ -438,7 +450,8 @@ vt_status nrc_check_config(vt_ctx *ctx, const vt_nrc_config &c) {
     return vt_fail(ctx, VT_ERR_INVALID, "resolutions must satisfy 2 <= base <= max <= 2^20");
   if (c.train_records == 0 || c.train_records > (1u << 24))
     return vt_fail(ctx, VT_ERR_INVALID, "train_records must be 1 - 2^24");
-  if (c.query_vertex < 1) return vt_fail(ctx, VT_ERR_INVALID, "query_vertex must be at least 1");
+  if (c.query_vertex == 0 && !(c.spread > 0.0f)) return vt_fail(ctx, VT_ERR_INVALID, "spread must be positive");
+  if (c.spectral > 1) return vt_fail(ctx, VT_ERR_INVALID, "spectral must be 0 or 1");
   if (!(c.learning_rate > 0.0f) || !(c.beta1 >= 0.0f && c.beta1 < 1.0f) || !(c.beta2 >= 0.0f && c.beta2 < 1.0f) ||
       !(c.epsilon >= 0.0f))
     return vt_fail(ctx, VT_ERR_INVALID, "bad Adam parameters");
@@ -487,7 +500,7 @@ vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s) {
   VT_CUDA(ctx, cudaMemsetAsync(nrc->d_loss, 0, sizeof(float), s));
   const uint32_t tiles = (cap + kNrcTile - 1) / kNrcTile;
   k_nrc_train<<<tiles, kNrcTile, kTrainSmem, s>>>(nrc->grid, mlp, nrc->d_tin, nrc->d_ttarget, nrc->d_count, cap,
-                                                  nrc->d_g, gtable, nrc->d_loss);
+                                                  nrc->d_g, gtable, nrc->d_loss, nrc_lum_weights(nrc));
   VT_CUDA(ctx, cudaGetLastError());
   ++nrc->steps;
   const double b1 = nrc->cfg.beta1, b2 = nrc->cfg.beta2;
@@ -504,6 +517,7 @@ vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s) {
 
 vt_status vt_nrc_predict(vt_ctx *ctx, vt_nrc *nrc, const NrcInput *in, uint32_t n, float4 *out, cudaStream_t s) {
   if (n == 0) return VT_OK;
+  if (!getenv("VT_NRC_MMA_SYNC")) return vt_nrc_infer_tc(ctx, nrc, in, n, out, s);
   const uint32_t tiles = (n + kInferRows - 1) / kInferRows;
   const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * 2u);
   k_nrc_infer<<<grid, kInferRows, kInferSmem, s>>>(nrc->grid, nrc->d_p, in, n, out);
@@ -522,7 +536,9 @@ vt_status vt_nrc_config_default(vt_nrc_config *cfg) {
   cfg->max_resolution = 2048;
   cfg->train_records = 65536;
   cfg->train_paths = 0;
-  cfg->query_vertex = 1;
+  cfg->query_vertex = 0;
+  cfg->spread = 0.01f;
+  cfg->spectral = 0;
   cfg->seed = 1337;
   cfg->learning_rate = 0.01f;
   cfg->beta1 = 0.9f;
@@ -645,8 +661,9 @@ vt_status vt_nrc_get_info(vt_ctx *ctx, vt_nrc *nrc, vt_nrc_info *out) {
     VT_CUDA(ctx, cudaMemcpy(&bad, ctx->d_status + 3, sizeof bad, cudaMemcpyDeviceToHost));
     if (bad) {
       VT_CUDA(ctx, cudaMemset(ctx->d_status + 3, 0, sizeof bad));
-      return vt_fail(ctx, VT_ERR_DEVICE, "the cache met an out-of-range grid index (status " + std::to_string(bad) +
-                                             "); the accesses were skipped");
+      return vt_fail(ctx, VT_ERR_DEVICE, "the cache's kernels reported status " + std::to_string(bad) +
+                                             " (1, 2: an out-of-range grid index, the access skipped; 4: a tensor-core "
+                                             "wait timed out, the inference stopped)");
     }
   }
   std::memset(out, 0, sizeof *out);
@@ -688,9 +705,9 @@ vt_status vt_nrc_set_params(vt_ctx *ctx, vt_nrc *nrc, const float *mlp, const fl
   return VT_OK;
 }
 
-vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_t n, float *rgb) {
+vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_t n, float *out) {
   if (!ctx) return VT_ERR_INVALID;
-  if (!nrc || ((!in || !rgb) && n)) return vt_fail(ctx, VT_ERR_INVALID, "nrc, in or rgb is null");
+  if (!nrc || ((!in || !out) && n)) return vt_fail(ctx, VT_ERR_INVALID, "nrc, in or out is null");
   if (n == 0) return VT_OK;
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
   {
@@ -702,14 +719,8 @@ vt_status vt_nrc_infer(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, uint32_
     const vt_status st = vt_nrc_predict(ctx, nrc, nrc->d_q, n, nrc->d_qout, ctx->stream);
     if (st != VT_OK) return st;
   }
-  std::vector<float4> o(n);
-  VT_CUDA(ctx, cudaMemcpyAsync(o.data(), nrc->d_qout, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+  VT_CUDA(ctx, cudaMemcpyAsync(out, nrc->d_qout, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
   VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (uint32_t i = 0; i < n; ++i) {
-    rgb[3 * i] = o[i].x;
-    rgb[3 * i + 1] = o[i].y;
-    rgb[3 * i + 2] = o[i].z;
-  }
   return VT_OK;
 }
 
@@ -723,11 +734,9 @@ vt_status nrc_upload_records(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, c
     const vt_status st = vt_nrc_reserve_records(ctx, nrc, n);
     if (st != VT_OK) return st;
   }
-  std::vector<float4> t(n);
-  for (uint32_t i = 0; i < n; ++i) t[i] = make_float4(target[3 * i], target[3 * i + 1], target[3 * i + 2], 0.0f);
   const uint32_t cnt[4] = {n, n, 0, 0};
   VT_CUDA(ctx, cudaMemcpyAsync(nrc->d_tin, in, (size_t)n * sizeof(NrcInput), cudaMemcpyHostToDevice, ctx->stream));
-  VT_CUDA(ctx, cudaMemcpyAsync(nrc->d_ttarget, t.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+  VT_CUDA(ctx, cudaMemcpyAsync(nrc->d_ttarget, target, (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
   VT_CUDA(ctx, cudaMemcpyAsync(nrc->d_count, cnt, sizeof cnt, cudaMemcpyHostToDevice, ctx->stream));
   VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return VT_OK;
@@ -753,14 +762,18 @@ vt_status vt_nrc_gradients(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, con
   if (n) {
     k_nrc_train<<<(n + kNrcTile - 1) / kNrcTile, kNrcTile, kTrainSmem, ctx->stream>>>(
         nrc->grid, nrc->d_p, nrc->d_tin, nrc->d_ttarget, nrc->d_count, n, nrc->d_g,
-        reinterpret_cast<float2 *>(nrc->d_g + kNrcMlpParams), nrc->d_loss);
+        reinterpret_cast<float2 *>(nrc->d_g + kNrcMlpParams), nrc->d_loss, nrc_lum_weights(nrc));
     VT_CUDA(ctx, cudaGetLastError());
   }
   VT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // The device sums carry the loss scale; the caller gets the loss's own gradient sums.
   VT_CUDA(ctx, cudaMemcpy(mlp_grad, nrc->d_g, kNrcMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
-  if (grid_grad)
-    VT_CUDA(ctx, cudaMemcpy(grid_grad, nrc->d_g + kNrcMlpParams, (nrc->nparams - kNrcMlpParams) * sizeof(float),
-                            cudaMemcpyDeviceToHost));
+  for (int i = 0; i < kNrcMlpParams; ++i) mlp_grad[i] /= kNrcLossScale;
+  if (grid_grad) {
+    const size_t ng = nrc->nparams - kNrcMlpParams;
+    VT_CUDA(ctx, cudaMemcpy(grid_grad, nrc->d_g + kNrcMlpParams, ng * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < ng; ++i) grid_grad[i] /= kNrcLossScale;
+  }
   if (loss) {
     float l = 0.0f;
     VT_CUDA(ctx, cudaMemcpy(&l, nrc->d_loss, sizeof l, cudaMemcpyDeviceToHost));

@@ -10,10 +10,14 @@
 // Input vector (64 halves): [0, 32) the grid's 16 levels x 2 features; [32, 36) one-blob(4) of the
 // outgoing direction's theta / pi, [36, 40) of its phi / 2 pi + 1/2; [40, 48) the same for the
 // shading normal; [48, 52) one-blob(4) of 1 - exp(-roughness); [52, 55) diffuse reflectance;
-// [55] specular reflectance; [56, 63) zero; [63] one (the first layer's bias).
-// Network: 64 -> 64 (ReLU) x 5 hidden layers -> 3 (linear), fp16 operands, fp32 accumulation,
-// no biases besides input 63. Weights are stored [out][in], fp32 masters, the output layer padded
-// to 16 rows (rows 3-15 stay zero).
+// [55] specular reflectance; [56, 60) one-blob(4) of the path's wavelength number u (spectral
+// transport: the four hero wavelengths are F^-1((u + k) / 4); 0 in RGB transport); [60, 63) the
+// frequency encoding sin(2 pi q) of the normalised position q (a collision-free coarse term beside
+// the hash grid); [63] one (the first layer's bias).
+// Network: 64 -> 64 (ReLU) x 5 hidden layers -> 4 (linear), fp16 operands, fp32 accumulation,
+// no biases besides input 63. Outputs: per hero wavelength of the path its radiance times the
+// lane's share 1 / (4 p(lambda)) (spectral caches), or rgb and 0 (RGB caches). Weights are stored
+// [out][in], fp32 masters, the output layer padded to 16 rows (rows 4-15 stay zero).
 #pragma once
 
 #include <cuda_fp16.h>
@@ -26,19 +30,25 @@ namespace vtd {
 constexpr int kNrcIn = 64;
 constexpr int kNrcWidth = 64;
 constexpr int kNrcHidden = 5;                 // hidden layers (64 x 64 matrices)
-constexpr int kNrcOutRows = 16;               // output layer rows (3 used)
+constexpr int kNrcOutRows = 16;               // output layer rows (kNrcOut used)
 constexpr int kNrcMlpParams = kNrcHidden * kNrcWidth * kNrcIn + kNrcOutRows * kNrcWidth;  // 21,504
 constexpr int kNrcMaxLevels = 16;
 constexpr int kNrcLd = 72;                    // padded smem row stride in halves (144 B)
 constexpr int kNrcTile = 128;                 // rows per CTA tile (4 warps x 32 rows)
+constexpr int kNrcOut = 4;                    // outputs used (rows of the output layer)
+// The backward pass multiplies the loss gradient by this before it meets fp16 (so that small
+// per-record gradients keep their precision instead of flushing to fp16 subnormals or zero); the
+// fp32 gradient sums are divided by it in the optimiser step.
+constexpr float kNrcLossScale = 64.0f;
 
-// A cache query at a path vertex (vt_nrc_input, 48 B).
+// A cache query at a path vertex (vt_nrc_input, 64 B).
 struct NrcInput {
   float4 a;  // position xyz, roughness
   float4 b;  // outgoing direction (theta / pi, phi / 2 pi + 1/2), shading normal (same)
   float4 c;  // diffuse reflectance rgb, specular reflectance
+  float4 d;  // wavelength number u, 0, 0, 0
 };
-static_assert(sizeof(NrcInput) == 48, "NrcInput layout");
+static_assert(sizeof(NrcInput) == 64, "NrcInput layout");
 
 // The hash grid: levels x 2^logT entries x 2 fp32 features; positions normalised by the scene box.
 struct NrcGrid {
@@ -151,8 +161,10 @@ __device__ __forceinline__ void nrc_encode(const NrcGrid &G, const NrcInput &in,
   row[53] = __float2half_rn(nrc_sat(in.c.y));
   row[54] = __float2half_rn(nrc_sat(in.c.z));
   row[55] = __float2half_rn(nrc_sat(in.c.w));
-#pragma unroll
-  for (int i = 56; i < 63; ++i) row[i] = __float2half_rn(0.0f);
+  nrc_blob4(in.d.x, row + 56);
+  row[60] = __float2half_rn(sinpif(2.0f * q.x));
+  row[61] = __float2half_rn(sinpif(2.0f * q.y));
+  row[62] = __float2half_rn(sinpif(2.0f * q.z));
   row[63] = __float2half_rn(1.0f);
 }
 
@@ -229,5 +241,7 @@ struct vt_nrc {
 vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s);
 // Predictions for n device queries into out (n float4).
 vt_status vt_nrc_predict(vt_ctx *ctx, vt_nrc *nrc, const vtd::NrcInput *in, uint32_t n, float4 *out, cudaStream_t s);
+// The inference kernel on the tcgen05 tensor cores (nrc_tc.cu), which vt_nrc_predict launches.
+vt_status vt_nrc_infer_tc(vt_ctx *ctx, vt_nrc *nrc, const vtd::NrcInput *in, uint32_t n, float4 *out, cudaStream_t s);
 vt_status vt_nrc_reserve_queries(vt_ctx *ctx, vt_nrc *nrc, size_t n);
 vt_status vt_nrc_reserve_records(vt_ctx *ctx, vt_nrc *nrc, uint32_t n);

@@ -25,6 +25,7 @@
 // samples are split into several groups to fill the GPU). Traversal is the 4-wide watertight
 // traversal of traverse.cu with a per-thread local stack.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -65,6 +66,7 @@ struct RenderArgs {
   float3 cam, fwd, right, up;
   float aspect, fovScale;
   uint32_t W, H, maxDepth, first, spp;
+  uint32_t stride, OW, OH;  // pixel stride; the accumulation's width and height (ceil(W / stride), ...)
   uint32_t mode;  // Uniforms.samplingMode: 1 MIS, 2 light sampling, 3 BSDF sampling
   uint32_t zSampler, zModel, firstFrame;  // Z++ sampler on/off, its temporal model, frame of `first`
   const float2 *jitter;
@@ -101,7 +103,8 @@ struct RenderArgs {
   NrcInput *nrcIn;
   float4 *nrcT;
   uint2 *nrcBins;
-  uint32_t nrcVertex;
+  uint32_t nrcVertex;  // 0: the spread-angle heuristic with constant nrcSpread
+  float nrcSpread;
   // Index checks: a hit's triangle index is clamped into the triangle array, a training record's
   // slot into its buffers; one out of range sets a bit of *status (read back with the accumulation).
   uint32_t faceCount;
@@ -283,10 +286,12 @@ __device__ __forceinline__ vt_material material(const RenderArgs &A, uint32_t sl
 struct Lanes {
   int bin[4];
   float w[4];
+  float u;  // the wavelength number the lanes come from
 };
 
 __device__ __forceinline__ Lanes make_lanes(const RenderArgs &A, float u) {
   Lanes L;
+  L.u = u;
   const float seg = float(A.segments);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
@@ -1032,7 +1037,8 @@ __device__ __forceinline__ float3 primary_emission(const RenderArgs &A, const La
 // The cache's query record of a vertex (nrc.cuh's input layout): OpenPBR slots give their
 // roughness and split the base colour by metalness; Lambert slots are rough and diffuse.
 template <bool kPbr>
-__device__ __forceinline__ NrcInput nrc_query(const RenderArgs &A, const Surface &S, const vt_material &m, float3 dir) {
+__device__ __forceinline__ NrcInput nrc_query(const RenderArgs &A, const Lanes &L, const Surface &S, const vt_material &m,
+                                              float3 dir) {
   NrcInput q;
   float rough = 1.0f, metal = 0.0f;
   if (is_pbr<kPbr>(A, m)) {
@@ -1044,13 +1050,23 @@ __device__ __forceinline__ NrcInput nrc_query(const RenderArgs &A, const Surface
   q.a = make_float4(S.pos.x, S.pos.y, S.pos.z, rough);
   q.b = make_float4(w.x, w.y, n.x, n.y);
   q.c = make_float4(m.albedo[0] * (1.0f - metal), m.albedo[1] * (1.0f - metal), m.albedo[2] * (1.0f - metal), metal);
+  q.d = make_float4(A.spectral ? L.u : 0.0f, 0.0f, 0.0f, 0.0f);
   return q;
 }
-// Stores the query of slot `slot`, with the throughput T (times the lanes' shares) and the bins.
+// The primary spread a0 = |x0 - x1|^2 / (4 pi cos theta_1) of a path's first hit at distance t, times
+// the cache's constant c: the spread-angle heuristic (Mueller et al. 2021) stops the path at the
+// first vertex n whose spread (sum_i sqrt(|x_i-1 - x_i|^2 / (p(w_i) |cos theta_i|)))^2 exceeds it.
+__device__ __forceinline__ float nrc_spread_limit(const RenderArgs &A, float t, float3 gn, float3 dir) {
+  const float c = fmaxf(fabsf(dot3(gn, dir)), 1e-6f);
+  return A.nrcSpread * t * t / (4.0f * 3.14159265f * c);
+}
+// Stores the query of slot `slot`, with the throughput T and the lanes' bins. (A spectral cache
+// predicts each lane's radiance times the lane's share 1 / (4 p(lambda)), the lane's term of the
+// spectral estimator, so T is stored without the shares.)
 __device__ __forceinline__ void nrc_store(const RenderArgs &A, size_t slot, const NrcInput &q, const Lanes &L, float4 T) {
   A.nrcIn[slot] = q;
   if (A.spectral) {
-    A.nrcT[slot] = make_float4(T.x * L.w[0], T.y * L.w[1], T.z * L.w[2], T.w * L.w[3]);
+    A.nrcT[slot] = T;
     A.nrcBins[slot] = make_uint2((uint32_t)L.bin[0] | ((uint32_t)L.bin[1] << 16), (uint32_t)L.bin[2] | ((uint32_t)L.bin[3] << 16));
   } else {
     A.nrcT[slot] = make_float4(T.x, T.y, T.z, 0.0f);
@@ -1061,17 +1077,20 @@ __device__ __forceinline__ void nrc_store_none(const RenderArgs &A, size_t slot)
   A.nrcT[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// kNrc (vt_render_nrc): the path ends at vertex A.nrcVertex, after that vertex's emission, with
+// kNrc (vt_render_nrc): the path ends, after the vertex's emission, at vertex A.nrcVertex, or with
+// A.nrcVertex 0 at the first vertex where its spread exceeds spreadLimit (nrc_spread_limit), with
 // its cache query stored in `slot`; `queried` tells whether it got there.
 template <bool kPbr, bool kNrc = false>
 __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, vt_material m, float3 dir,
-                                Sampler &seed, int *stack, bool diPrimary, size_t slot = 0, bool *queried = nullptr) {
+                                Sampler &seed, int *stack, bool diPrimary, float spreadLimit = 0.0f, size_t slot = 0,
+                                bool *queried = nullptr) {
   const int limit = max(0, (int)A.maxDepth - 1);
   const bool nee = A.mode != 3u, mis = A.mode <= 1u;
   float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
   float3 R = f3(0.0f, 0.0f, 0.0f);
   int scattering = 0;
   bool emissionOnly = false;
+  float spread = 0.0f;  // sum of the vertices' sqrt(d^2 / (p |cos|)) (kNrc)
   for (int bounce = 1;; ++bounce) {
     if (scattering >= limit) {
       // BSDF-only paths take one final continuation that may only reach emission.
@@ -1112,6 +1131,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     }
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
+    if (kNrc) spread += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
     if (m.type == VT_MAT_EMISSIVE) {
       // emission_weight (main.swift:3462-3466): 1 without NEE or without a light pdf, else the
       // power heuristic (MIS) or 0 (light sampling, or a ReSTIR DI vertex).
@@ -1121,8 +1141,8 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       break;
     }
     if (emissionOnly) break;
-    if (kNrc && (uint32_t)bounce >= A.nrcVertex) {
-      nrc_store(A, slot, nrc_query<kPbr>(A, S, m, dir), L, T);
+    if (kNrc && (A.nrcVertex ? (uint32_t)bounce >= A.nrcVertex : spread * spread > spreadLimit)) {
+      nrc_store(A, slot, nrc_query<kPbr>(A, L, S, m, dir), L, T);
       *queried = true;
       break;
     }
@@ -1165,7 +1185,8 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
     R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
                      stack, true);
   }
-  R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, slot, &queried));
+  const float spreadLimit = kNrc ? nrc_spread_limit(A, h.t, S.gn, dir0) : 0.0f;
+  R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, spreadLimit, slot, &queried));
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) R = f3(0.0f, 0.0f, 0.0f);
   return R;
 }
@@ -1312,7 +1333,8 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
       R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel), W);
-    R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, true, slot, &queried));
+    const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
+    R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, true, spreadLimit, slot, &queried));
   }
   if (kNrc && !queried) nrc_store_none(A, slot);
   if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) return;
@@ -1326,11 +1348,11 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
 template <bool kPbr, bool kNrc = false>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArgs A, uint32_t groups, uint32_t per) {
   int stack[kRenderStack];
-  const uint32_t npix = A.W * A.H;
+  const uint32_t npix = A.OW * A.OH;  // accumulation pixels: the frame's pixels (s i, s j)
   const uint64_t items = (uint64_t)npix * groups;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < items; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t p = (uint32_t)(i % npix), g = (uint32_t)(i / npix);
-    const uint32_t x = p % A.W, y = p / A.W;
+    const uint32_t x = (p % A.OW) * A.stride, y = (p / A.OW) * A.stride;
     const uint32_t k0 = g * per, k1 = min(A.spp, k0 + per);
     double sr = 0.0, sg = 0.0, sb = 0.0;
     for (uint32_t k = k0; k < k1; ++k) {
@@ -1395,7 +1417,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
   float4 *rec = scratch + (size_t)j * kNrcRecords * 5;
   int nrec = 0;
   {
-    const NrcInput q = nrc_query<kPbr>(A, S, m, dir);
+    const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
   }
@@ -1438,7 +1460,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       break;
     }
     if (nrec < kNrcRecords) {
-      const NrcInput q = nrc_query<kPbr>(A, S, m, dir);
+      const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
       float4 *r = rec + 5 * nrec;
       r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
       ++nrec;
@@ -1460,20 +1482,24 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     }
     const float4 *r = rec + 5 * i;
     const float4 t = r[3], r0 = r[4];
-    const float4 d = make_float4(t.x > 1e-20f ? (R.x - r0.x) / t.x : 0.0f, t.y > 1e-20f ? (R.y - r0.y) / t.y : 0.0f,
-                                 t.z > 1e-20f ? (R.z - r0.z) / t.z : 0.0f, t.w > 1e-20f ? (R.w - r0.w) / t.w : 0.0f);
-    float3 c = to_rgb(A, L, d);
-    if (!isfinite(c.x) || !isfinite(c.y) || !isfinite(c.z)) c = f3(0.0f, 0.0f, 0.0f);
+    float4 d = make_float4(t.x > 1e-20f ? (R.x - r0.x) / t.x : 0.0f, t.y > 1e-20f ? (R.y - r0.y) / t.y : 0.0f,
+                           t.z > 1e-20f ? (R.z - r0.z) / t.z : 0.0f, t.w > 1e-20f ? (R.w - r0.w) / t.w : 0.0f);
+    // Spectral targets: each lane's radiance times its share (values of the size of rgb radiance;
+    // the bare lane radiance of a D65-relative emitter is ~1/100 of it, where the relative loss's
+    // epsilon would swamp it).
+    if (A.spectral) d = make_float4(d.x * L.w[0], d.y * L.w[1], d.z * L.w[2], d.w * L.w[3]);
+    if (!isfinite(d.x) || !isfinite(d.y) || !isfinite(d.z) || !isfinite(d.w)) d = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     NrcInput q;
     q.a = r[0]; q.b = r[1]; q.c = r[2];
+    q.d = make_float4(A.spectral ? L.u : 0.0f, 0.0f, 0.0f, 0.0f);
     outIn[first + i] = q;
-    outTarget[first + i] = make_float4(c.x, c.y, c.z, 0.0f);
+    outTarget[first + i] = d;
   }
 }
 
 // Adds each pixel's cache contributions: per sample slot with a query, the throughput times the
-// prediction (clamped at zero), in spectral transport the prediction's emission uplift at the
-// slot's lanes, to rgb.
+// prediction (clamped at zero) lane by lane, to rgb (spectral transport: the lanes' colour-matching
+// functions at the slot's bins; the prediction carries each lane's share).
 __global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uint32_t spp) {
   const uint32_t npix = A.W * A.H;
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1484,7 +1510,7 @@ __global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uin
     const float4 t = A.nrcT[slot];
     if (t.x == 0.0f && t.y == 0.0f && t.z == 0.0f && t.w == 0.0f) continue;
     const float4 c = pred[slot];
-    const float3 e = f3(fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f));
+    const float4 e = make_float4(fmaxf(c.x, 0.0f), fmaxf(c.y, 0.0f), fmaxf(c.z, 0.0f), fmaxf(c.w, 0.0f));
     float3 v;
     if (A.spectral) {
       const uint2 b = A.nrcBins[slot];
@@ -1492,7 +1518,8 @@ __global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uin
       L.bin[0] = (int)(b.x & 0xffffu); L.bin[1] = (int)(b.x >> 16);
       L.bin[2] = (int)(b.y & 0xffffu); L.bin[3] = (int)(b.y >> 16);
       L.w[0] = L.w[1] = L.w[2] = L.w[3] = 1.0f;
-      v = lanes_rgb(A, L, mul4(t, lanes_emission(A, L, e)));
+      L.u = 0.0f;
+      v = lanes_rgb(A, L, mul4(t, e));
     } else {
       v = f3(t.x * e.x, t.y * e.y, t.z * e.z);
     }
@@ -1950,21 +1977,34 @@ vt_status check_params(vt_ctx *ctx, const vt_scene *scene, const vt_frame_params
   if (p->sampler > 1 || p->z_temporal > 3) return vt_fail(ctx, VT_ERR_INVALID, "sampler must be 0 (PCG) or 1 (Z++), z_temporal 0-3");
   if (p->sampling_mode == 0 && scene->environment.intensity > 0.0f)
     return vt_fail(ctx, VT_ERR_INVALID, "ReSTIR DI (sampling mode 0) does not sample the environment; use modes 1-3");
+  if (p->pixel_stride > 64) return vt_fail(ctx, VT_ERR_INVALID, "pixel_stride must be at most 64");
+  if (p->pixel_stride > 1 && p->sampling_mode == 0)
+    return vt_fail(ctx, VT_ERR_INVALID, "a pixel stride needs sampling modes 1-3 (ReSTIR DI reuses neighbouring pixels)");
   const vt_mesh *mesh = scene->mesh;
   if (mesh->nfaces > 0 && mesh->depth > 32) return vt_fail(ctx, VT_ERR_LIMIT, "BVH deeper than the render stack");
   return VT_OK;
 }
 
 // Sizes the scene's accumulation to the frame (a new size starts a new accumulation).
+// The accumulation's size for a frame: width x height, or ceil(width / s) x ceil(height / s) at a
+// pixel stride s.
+void accum_dims(const vt_frame_params *p, uint32_t &w, uint32_t &h) {
+  const uint32_t st = p->pixel_stride > 1 ? p->pixel_stride : 1u;
+  w = (p->width + st - 1) / st;
+  h = (p->height + st - 1) / st;
+}
+
 vt_status ensure_accum(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p) {
-  if (p->width == scene->width && p->height == scene->height && scene->d_accum) return VT_OK;
+  uint32_t w, h;
+  accum_dims(p, w, h);
+  if (w == scene->width && h == scene->height && scene->d_accum) return VT_OK;
   cudaFree(scene->d_accum);
   scene->d_accum = nullptr;
-  const size_t bytes = 3 * (size_t)p->width * p->height * sizeof(double);
+  const size_t bytes = 3 * (size_t)w * h * sizeof(double);
   VT_CUDA(ctx, cudaMalloc(&scene->d_accum, bytes));
   VT_CUDA(ctx, cudaMemset(scene->d_accum, 0, bytes));
-  scene->width = p->width;
-  scene->height = p->height;
+  scene->width = w;
+  scene->height = h;
   scene->samples = 0;
   return VT_OK;
 }
@@ -2019,6 +2059,9 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.aperture = p->aperture;
   A.focus = p->focus_distance;
   A.W = p->width;
+  A.stride = p->pixel_stride > 1 ? p->pixel_stride : 1u;
+  A.OW = (p->width + A.stride - 1) / A.stride;
+  A.OH = (p->height + A.stride - 1) / A.stride;
   A.H = p->height;
   A.maxDepth = p->max_depth;
   A.first = p->first_sample;
@@ -2091,7 +2134,7 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
   fill_args(scene, p, spp, A);
   A.jitter = scene->d_jitter;
   A.status = ctx->d_status + 2;
-  const uint32_t npix = p->width * p->height;
+  const uint32_t npix = A.OW * A.OH;  // the frame's pixels, or its strided subset
   if (nrc) {
     const vt_status st = vt_nrc_reserve_queries(ctx, nrc, (size_t)npix * spp);
     if (st != VT_OK) return st;
@@ -2099,6 +2142,7 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
     A.nrcT = nrc->d_qT;
     A.nrcBins = nrc->d_qbins;
     A.nrcVertex = nrc->cfg.query_vertex;
+    A.nrcSpread = nrc->cfg.spread;
   }
   if (p->sampling_mode == 0u) {
     // ReSTIR DI: frames in order, two launches each (the primary pass, then reuse and shading).
@@ -2201,6 +2245,9 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
   if (flags & ~(uint32_t)(VT_NRC_TRAIN | VT_NRC_RENDER)) return vt_fail(ctx, VT_ERR_INVALID, "unknown flags");
   if ((flags & VT_NRC_RENDER) && p->sampling_mode > 1)
     return vt_fail(ctx, VT_ERR_INVALID, "the cache renders sampling modes 0 (ReSTIR DI) and 1 (MIS)");
+  if ((p->spectral != 0) != (nrc->cfg.spectral != 0))
+    return vt_fail(ctx, VT_ERR_INVALID, "the frame's transport (spectral or rgb) differs from the cache's `spectral` setting");
+  if (p->pixel_stride > 1) return vt_fail(ctx, VT_ERR_INVALID, "the cache renders whole frames (pixel_stride 0 or 1)");
   {
     const vt_status st = check_params(ctx, scene, p);
     if (st != VT_OK) return st;
@@ -2352,6 +2399,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     if (st != VT_OK) return st;
     if (params[i].sampling_mode == 0)
       return vt_fail(ctx, VT_ERR_INVALID, "batched scenes use sampling modes 1-3 (ReSTIR DI frames run in order per scene)");
+    if (params[i].pixel_stride > 1) return vt_fail(ctx, VT_ERR_INVALID, "batched scenes render whole frames (pixel_stride 0 or 1)");
     if (spp[i] == 0 || spp[i] > 65536) return vt_fail(ctx, VT_ERR_INVALID, "spp must be 1 .. 65536 per scene");
     if (scenes[i]->mesh->nfaces == 0) return vt_fail(ctx, VT_ERR_INVALID, "scene " + std::to_string(i) + " has no faces");
   }
@@ -2543,6 +2591,36 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
   const double inv = scene->samples ? 1.0 / scene->samples : 0.0;
   for (size_t i = 0; i < want; ++i) rgb[i] *= inv;
   if (samples) *samples = scene->samples;
+  return VT_OK;
+}
+
+vt_status vt_accum_restore(vt_ctx *ctx, vt_scene *scene, uint32_t width, uint32_t height, uint32_t pixel_stride,
+                           const double *rgb, uint32_t n, uint32_t samples) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !rgb) return vt_fail(ctx, VT_ERR_INVALID, "scene or rgb is null");
+  if (width == 0 || height == 0 || (uint64_t)width * height > (1u << 28) || pixel_stride > 64)
+    return vt_fail(ctx, VT_ERR_INVALID, "bad image size or pixel stride");
+  vt_frame_params p;
+  std::memset(&p, 0, sizeof p);
+  p.width = width;
+  p.height = height;
+  p.pixel_stride = pixel_stride;
+  uint32_t w, h;
+  accum_dims(&p, w, h);
+  const size_t want = 3 * (size_t)w * h;
+  if (n != want) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the accumulation's pixels * 3");
+  for (size_t i = 0; i < want; ++i)
+    if (!std::isfinite(rgb[i])) return vt_fail(ctx, VT_ERR_INVALID, "the saved accumulation holds a non-finite value");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  VT_CUDA(ctx, cudaDeviceSynchronize());
+  {
+    const vt_status st = ensure_accum(ctx, scene, &p);
+    if (st != VT_OK) return st;
+  }
+  std::vector<double> sums(rgb, rgb + want);
+  for (double &v : sums) v *= (double)samples;
+  VT_CUDA(ctx, cudaMemcpy(scene->d_accum, sums.data(), want * sizeof(double), cudaMemcpyHostToDevice));
+  scene->samples = samples;
   return VT_OK;
 }
 

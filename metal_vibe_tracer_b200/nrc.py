@@ -1,10 +1,13 @@
-"""The neural radiance cache (vt_nrc_*, nrc.cu): a hash-grid encoded MLP trained online on the
-suffix radiance of training paths, queried by rendered paths at their first bounce's hit.
+"""The neural radiance cache (vt_nrc_*, nrc.cu, nrc_tc.cu): a hash-grid encoded MLP trained online on
+the suffix radiance of training paths, queried by rendered paths where the spread-angle heuristic
+stops them (or at a fixed vertex).
 
 The reference has no radiance cache; the design follows Mueller et al. 2021 ("Real-time Neural
 Radiance Caching for Path Tracing") with the multiresolution hash encoding of Mueller et al. 2022.
-Queries are (n, 12) float32 rows in vt_nrc_input's order: position xyz, roughness, outgoing
-direction (theta / pi, phi / 2 pi + 1/2), shading normal (same), diffuse rgb, specular.
+Queries are (n, 13) float32 rows in vt_nrc_input's order: position xyz, roughness, outgoing
+direction (theta / pi, phi / 2 pi + 1/2), shading normal (same), diffuse rgb, specular, the path's
+wavelength number u (spectral caches; 0 for rgb). Predictions and training targets are (n, 4): per
+hero wavelength its radiance times the lane's share (spectral caches), or rgb and 0.
 """
 from __future__ import annotations
 
@@ -17,7 +20,8 @@ from .accel import Context, _check
 
 NRC_TRAIN, NRC_RENDER = 1, 2
 MLP_PARAMS = 21504
-INPUT_FLOATS = 12
+INPUT_FLOATS = 13
+OUTPUTS = 4
 
 
 def default_config() -> dict:
@@ -78,14 +82,16 @@ class RadianceCache:
 
     @staticmethod
     def _rows(inputs) -> np.ndarray:
-        x = np.ascontiguousarray(inputs, np.float32)
+        x = np.asarray(inputs, np.float32)
         if x.ndim != 2 or x.shape[1] != INPUT_FLOATS:
-            raise ValueError("inputs must be (n, 12) float32")
-        return x
+            raise ValueError("inputs must be (n, 13) float32")
+        rows = np.zeros((len(x), 16), np.float32)  # vt_nrc_input: 64 bytes, 3 floats of padding
+        rows[:, :INPUT_FLOATS] = x
+        return rows
 
     def infer(self, inputs) -> np.ndarray:
         x = self._rows(inputs)
-        out = np.empty((len(x), 3), np.float32)
+        out = np.empty((len(x), OUTPUTS), np.float32)
         _check(self.ctx.handle, _lib.load().vt_nrc_infer(self.ctx.handle, self._p, x.ctypes.data, len(x), out.ctypes.data),
                "vt_nrc_infer")
         return out
@@ -93,7 +99,7 @@ class RadianceCache:
     def gradients(self, inputs, targets, grid: bool = True):
         """(mlp gradient sums, grid gradient sums or None, loss sum) over the records, no update."""
         x = self._rows(inputs)
-        y = np.ascontiguousarray(targets, np.float32).reshape(len(x), 3)
+        y = np.ascontiguousarray(targets, np.float32).reshape(len(x), OUTPUTS)
         gm = np.empty(MLP_PARAMS, np.float32)
         gg = np.empty(self.grid_params, np.float32) if grid else None
         loss = C.c_double()
@@ -105,7 +111,7 @@ class RadianceCache:
     def train(self, inputs, targets) -> float:
         """One Adam step; the records' mean loss before it."""
         x = self._rows(inputs)
-        y = np.ascontiguousarray(targets, np.float32).reshape(len(x), 3)
+        y = np.ascontiguousarray(targets, np.float32).reshape(len(x), OUTPUTS)
         loss = C.c_float()
         _check(self.ctx.handle, _lib.load().vt_nrc_train(self.ctx.handle, self._p, x.ctypes.data, y.ctypes.data, len(x),
                                                          C.byref(loss)), "vt_nrc_train")

@@ -52,10 +52,10 @@ class FrameParams(C.Structure):
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
                 ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
                 ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32),
-                ("aperture", C.c_float), ("focus_distance", C.c_float)]
+                ("aperture", C.c_float), ("focus_distance", C.c_float), ("pixel_stride", C.c_uint32)]
 
 
-assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 88
+assert C.sizeof(Material) == 32 and C.sizeof(QuadLight) == 64 and C.sizeof(FrameParams) == 92
 
 
 def make_materials(materials) -> C.Array:
@@ -75,7 +75,7 @@ def make_light(light) -> QuadLight:
 
 
 def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=True, mode=1, sampler=0, z_temporal=3,
-                first_frame=0, di_candidates=0, aperture=0.0, focus_distance=1.0) -> FrameParams:
+                first_frame=0, di_candidates=0, aperture=0.0, focus_distance=1.0, pixel_stride=1) -> FrameParams:
     p = FrameParams()
     p.camera_pos[:] = [float(x) for x in camera["pos"]]
     p.camera_target[:] = [float(x) for x in camera["target"]]
@@ -91,7 +91,15 @@ def make_params(camera, width, height, max_depth=8, first_sample=1, spectral=Tru
     p.first_frame = int(first_frame)  # 0: continue the scene's accumulation
     p.di_candidates = int(di_candidates)  # ReSTIR DI candidates (0: the reference's 4)
     p.aperture, p.focus_distance = float(aperture), float(focus_distance)  # thin lens (0: pinhole)
+    p.pixel_stride = int(pixel_stride)  # s > 1: pixels (s i, s j) only (sampling modes 1-3)
     return p
+
+
+def accum_shape(params: FrameParams) -> tuple[int, int]:
+    """(height, width) of the accumulation a frame renders into: the frame's, or ceil(h / s) x
+    ceil(w / s) at a pixel stride s."""
+    s = max(1, int(params.pixel_stride))
+    return (params.height + s - 1) // s, (params.width + s - 1) // s
 
 
 class Scene:
@@ -182,7 +190,7 @@ class Scene:
 
     def render(self, params: FrameParams, spp: int, stream=None) -> None:
         """Adds `spp` frames (one sample per pixel each) to the accumulation; stream-ordered."""
-        self.width, self.height = params.width, params.height
+        self.height, self.width = accum_shape(params)
         _check(self.ctx.handle, _lib.load().vt_render(self.ctx.handle, self._p, C.byref(params), int(spp), stream),
                "vt_render")
 
@@ -197,6 +205,26 @@ class Scene:
         _check(self.ctx.handle, _lib.load().vt_accum_readback(self.ctx.handle, self._p, out.ctypes.data, n,
                                                               C.byref(samples)), "vt_accum_readback")
         return out.reshape(self.height, self.width, 3), int(samples.value)
+
+    def save_accumulation(self, path, params: FrameParams) -> int:
+        """Save the accumulation (mean radiance in FP64 and its sample count, with the frame's size and
+        pixel stride) to an .npz file, to resume a long render later (restore_accumulation); returns
+        the sample count."""
+        img, n = self.readback()
+        np.savez(path, rgb=img, samples=n, width=params.width, height=params.height,
+                 pixel_stride=max(1, int(params.pixel_stride)))
+        return n
+
+    def restore_accumulation(self, path) -> int:
+        """Resume an accumulation saved by save_accumulation (vt_accum_restore); the next render
+        continues it with first_sample = the returned sample count + 1."""
+        d = np.load(path)
+        rgb = np.ascontiguousarray(d["rgb"], np.float64)
+        w, h, s, n = int(d["width"]), int(d["height"]), int(d["pixel_stride"]), int(d["samples"])
+        _check(self.ctx.handle, _lib.load().vt_accum_restore(self.ctx.handle, self._p, w, h, s, rgb.ctypes.data,
+                                                             rgb.size, n), "vt_accum_restore")
+        self.height, self.width = rgb.shape[0], rgb.shape[1]
+        return n
 
     def save_exr(self, path) -> int:
         """Write the accumulation's mean radiance as a FLOAT RGB OpenEXR (the reference's HDR export);

@@ -7,9 +7,14 @@ kernels follow (Mueller et al. 2021, neural radiance caching: relative L2 loss w
 held constant in the denominator; Mueller et al. 2022, multiresolution hash encoding: the spatial
 hash x ^ 2654435761 y ^ 805459861 z and trilinear corner weights; Mueller et al. 2019, one-blob
 encoding), with the same fp16 roundings of the device: encoded inputs, weights, every layer's
-output, the loss gradient and every layer's pre-activation gradient are rounded to fp16 (clamped to
-+-65504); sums are exact (float64) where the device accumulates in fp32. `exact=True` drops the
-roundings, for finite-difference checks of the gradients.
+output, the loss gradient (times the loss scale, as the device's backward pass carries it) and every
+layer's pre-activation gradient are rounded to fp16 (clamped to +-65504); sums are exact (float64)
+where the device accumulates in fp32. `exact=True` drops the roundings, for finite-difference checks
+of the gradients.
+
+Records are (n, 13) rows in vt_nrc_input's order (position, roughness, direction, normal, diffuse,
+specular, wavelength number u); the network has four outputs, and the loss normaliser weighs them
+by rgb luminance (rgb caches) or equally (spectral caches: the four hero wavelengths' terms).
 """
 from __future__ import annotations
 
@@ -19,8 +24,10 @@ import numpy as np
 
 HIDDEN = 5
 OUT_ROWS = 16
+OUTPUTS = 4
 MLP_PARAMS = HIDDEN * 64 * 64 + OUT_ROWS * 64
 GRAD_CLIP = 512.0
+LOSS_SCALE = 64.0
 PRIMES = (1, 2654435761, 805459861)
 
 
@@ -43,9 +50,13 @@ class Grid:
     def entries(self) -> int:
         return 1 << self.log_t
 
+    def position(self, pos: np.ndarray) -> np.ndarray:
+        """Normalised positions in [0, 1]^3 (float32 as the device)."""
+        return np.clip(np.nan_to_num((pos.astype(np.float32) - self.lo) * self.inv, nan=0.0), 0.0, 1.0).astype(np.float32)
+
     def corners(self, pos: np.ndarray, level: int):
         """(n, 8) entry indices within the level and (n, 8) trilinear weights (float32 as the device)."""
-        q = np.clip(np.nan_to_num((pos.astype(np.float32) - self.lo) * self.inv, nan=0.0), 0.0, 1.0).astype(np.float32)
+        q = self.position(pos)
         res = self.res[level]
         x = (q * np.float32(res)).astype(np.float32)
         c = np.minimum(x.astype(np.int64), res - 1)
@@ -96,6 +107,8 @@ def encode(inputs: np.ndarray, table: np.ndarray, grid: Grid, exact: bool = Fals
     out[:, 44:48] = blob4(x[:, 7])
     out[:, 48:52] = blob4(1.0 - np.exp(-np.maximum(x[:, 3], 0.0)))
     out[:, 52:56] = np.clip(np.nan_to_num(x[:, 8:12], nan=0.0), 0.0, 1.0)
+    out[:, 56:60] = blob4(x[:, 12])
+    out[:, 60:63] = np.sin(2.0 * np.pi * grid.position(x[:, 0:3]).astype(np.float64))
     out[:, 63] = 1.0
     return _h(out, exact)
 
@@ -108,7 +121,7 @@ def split(mlp: np.ndarray):
 
 
 def forward(x: np.ndarray, mlp: np.ndarray, exact: bool = False):
-    """Layer outputs (fp16 values unless exact) and the (n, 3) prediction."""
+    """Layer outputs (fp16 values unless exact) and the (n, 4) prediction."""
     ws, wo = split(mlp)
     ws = [_h(w, exact) for w in ws]
     wo = _h(wo, exact)
@@ -117,31 +130,38 @@ def forward(x: np.ndarray, mlp: np.ndarray, exact: bool = False):
     for w in ws:
         h = _h(np.maximum(h @ w.T, 0.0), exact)
         hs.append(h)
-    return hs, (h @ wo.T)[:, :3]
+    return hs, (h @ wo.T)[:, :OUTPUTS]
 
 
 def predict(inputs, mlp, table, grid: Grid, exact: bool = False) -> np.ndarray:
     return forward(encode(inputs, table, grid, exact), mlp, exact)[1]
 
 
-def gradients(inputs, targets, mlp, table, grid: Grid, exact: bool = False):
+def lum_weights(spectral: bool) -> np.ndarray:
+    return np.full(4, 0.25) if spectral else np.array([0.2126, 0.7152, 0.0722, 0.0])
+
+
+def gradients(inputs, targets, mlp, table, grid: Grid, exact: bool = False, spectral: bool = False,
+              loss_scale: float = LOSS_SCALE):
     """Gradient sums of the relative L2 loss over the records: (mlp grad (21,504), table grad
-    (levels, entries, 2), loss sum)."""
+    (levels, entries, 2), loss sum). The fp16 roundings see the loss gradient times `loss_scale`, as
+    on the device; the sums returned are the loss's own."""
     x = encode(inputs, table, grid, exact)
     ws, wo = split(mlp)
     wsh = [_h(w, exact) for w in ws]
     woh = _h(wo, exact)
     hs, p = forward(x, mlp, exact)
-    y = np.asarray(targets, np.float64).reshape(-1, 3)
-    lum = p @ np.array([0.2126, 0.7152, 0.0722])
+    y = np.asarray(targets, np.float64).reshape(-1, OUTPUTS)
+    lum = p @ lum_weights(spectral)
     inv = 1.0 / (lum * lum + 0.01)
     e = p - y
     loss = float(np.sum(np.sum(e * e, 1) * inv))
     d = 2.0 * e * inv[:, None]
+    scale = 1.0 if exact else loss_scale
     if not exact:
         d = np.clip(d, -GRAD_CLIP, GRAD_CLIP)
     dout = np.zeros((len(x), OUT_ROWS))
-    dout[:, :3] = _h(d, exact)
+    dout[:, :OUTPUTS] = _h(d * scale, exact)
     g_mlp = np.zeros(MLP_PARAMS)
     g_mlp[HIDDEN * 4096:] = (dout.T @ hs[-1]).ravel()
     dh = dout @ woh
@@ -157,24 +177,24 @@ def gradients(inputs, targets, mlp, table, grid: Grid, exact: bool = False):
         idx, w = grid.corners(pos, l)
         for k in range(8):
             np.add.at(g_table[l], idx[:, k], w[:, k, None].astype(np.float64) * dfeat[:, 2 * l:2 * l + 2])
-    return g_mlp, g_table, loss
+    return g_mlp / scale, g_table / scale, loss
 
 
-def loss_sum(inputs, targets, mlp, table, grid: Grid, den=None) -> float:
+def loss_sum(inputs, targets, mlp, table, grid: Grid, den=None, spectral: bool = False) -> float:
     """The exact loss (no roundings), for finite differences. `den` holds the per-record
     denominators lum(p)^2 + 0.01 fixed (the stop-gradient the gradient assumes); None computes
     them from this prediction."""
     p = predict(inputs, mlp, table, grid, exact=True)
-    y = np.asarray(targets, np.float64).reshape(-1, 3)
+    y = np.asarray(targets, np.float64).reshape(-1, OUTPUTS)
     if den is None:
-        lum = p @ np.array([0.2126, 0.7152, 0.0722])
+        lum = p @ lum_weights(spectral)
         den = lum * lum + 0.01
     return float(np.sum(np.sum((p - y) ** 2, 1) / den))
 
 
-def denominators(inputs, mlp, table, grid: Grid) -> np.ndarray:
+def denominators(inputs, mlp, table, grid: Grid, spectral: bool = False) -> np.ndarray:
     p = predict(inputs, mlp, table, grid, exact=True)
-    lum = p @ np.array([0.2126, 0.7152, 0.0722])
+    lum = p @ lum_weights(spectral)
     return lum * lum + 0.01
 
 

@@ -225,7 +225,7 @@ class FrameParams(C.Structure):
                 ("width", C.c_uint32), ("height", C.c_uint32), ("first_sample", C.c_uint32),
                 ("spectral", C.c_uint32), ("sampler", C.c_uint32), ("z_temporal", C.c_uint32),
                 ("first_frame", C.c_uint32), ("di_candidates", C.c_uint32),
-                ("aperture", C.c_float), ("focus_distance", C.c_float)]
+                ("aperture", C.c_float), ("focus_distance", C.c_float), ("pixel_stride", C.c_uint32)]
 
 
 class Environment(C.Structure):

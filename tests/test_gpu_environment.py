@@ -139,7 +139,7 @@ def test_cached_sky_scene_matches_path_tracer(ctx):
     scene.render(vt.make_params(cam, W, H, 8, 1, True, 1), 1024)
     ref, _ = scene.readback()
     info = mesh.info()
-    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=13)
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=13, spectral=1)
     scene.reset()
     for f in range(120):
         cache.render(scene, vt.make_params(cam, W, H, 8, 1 + f, True, 1), 0, render=False)

@@ -21,22 +21,23 @@ pytestmark = pytest.mark.gpu
 
 def random_inputs(n, seed):
     rng = np.random.default_rng(seed)
-    x = np.zeros((n, 12), np.float32)
+    x = np.zeros((n, 13), np.float32)
     x[:, 0:3] = rng.uniform(-0.95, 0.95, (n, 3))
     x[:, 3] = rng.uniform(0, 2, n)
     x[:, 4:8] = rng.uniform(0, 1, (n, 4))
     x[:, 8:11] = rng.uniform(0, 1, (n, 3))
     x[:, 11] = rng.uniform(0, 1, n)
+    x[:, 12] = rng.uniform(0, 1, n)
     return x
 
 
-def cache_with_params(ctx, seed, levels=8, log_t=14):
+def cache_with_params(ctx, seed, levels=8, log_t=14, spectral=False):
     cache = RadianceCache(ctx, [-1, -1, -1], [1, 1, 1], levels=levels, log2_table=log_t, base_resolution=8,
-                          max_resolution=256, seed=seed)
+                          max_resolution=256, seed=seed, spectral=int(spectral))
     rng = np.random.default_rng(seed)
     mlp = np.zeros(R.MLP_PARAMS, np.float32)
     mlp[:R.HIDDEN * 4096] = rng.uniform(-0.25, 0.25, R.HIDDEN * 4096)
-    mlp[R.HIDDEN * 4096:R.HIDDEN * 4096 + 3 * 64] = rng.uniform(-0.25, 0.25, 3 * 64)
+    mlp[R.HIDDEN * 4096:R.HIDDEN * 4096 + 4 * 64] = rng.uniform(-0.25, 0.25, 4 * 64)
     table = rng.uniform(-1, 1, cache.grid_params).astype(np.float32)
     cache.set_params(mlp, table)
     grid = R.Grid(levels, log_t, 8, 256, [-1, -1, -1], [1, 1, 1])
@@ -56,21 +57,22 @@ def test_infer_matches_oracle(ctx):
     cache.close()
 
 
-def test_gradients_match_oracle(ctx):
-    cache, grid, mlp, table = cache_with_params(ctx, 7)
+@pytest.mark.parametrize("spectral", [False, True])
+def test_gradients_match_oracle(ctx, spectral):
+    cache, grid, mlp, table = cache_with_params(ctx, 7, spectral=spectral)
     x = random_inputs(2000, 8)
     # Records whose ReLUs are all clear of zero (a flipped ReLU changes a record's gradient).
     x = x[R.relu_margins(x, mlp, table, grid) > 5e-4][:1000]  # not a multiple of the 128-row tile
     assert len(x) == 1000
-    y = np.random.default_rng(9).uniform(0, 2, (1000, 3)).astype(np.float32)
+    y = np.random.default_rng(9).uniform(0, 2, (1000, 4)).astype(np.float32)
     gm, gg, loss = cache.gradients(x, y)
-    rm, rg, rloss = R.gradients(x, y, mlp, table, grid)
+    rm, rg, rloss = R.gradients(x, y, mlp, table, grid, spectral=spectral)
     assert loss == pytest.approx(rloss, rel=2e-3)
     for l in range(R.HIDDEN + 1):
         a = gm[l * 4096:(l + 1) * 4096] if l < R.HIDDEN else gm[R.HIDDEN * 4096:]
         b = rm[l * 4096:(l + 1) * 4096] if l < R.HIDDEN else rm[R.HIDDEN * 4096:]
         assert np.abs(a - b).max() <= 1e-2 * np.abs(b).max(), (l, np.abs(a - b).max(), np.abs(b).max())
-    assert np.all(gm[R.HIDDEN * 4096 + 3 * 64:] == 0.0)  # unused output rows
+    assert np.all(gm[R.HIDDEN * 4096 + 4 * 64:] == 0.0)  # unused output rows
     rg = rg.ravel()
     assert np.abs(gg - rg).max() <= 1e-2 * np.abs(rg).max(), np.abs(gg - rg).max()
     assert np.count_nonzero(gg) > 0
@@ -81,7 +83,8 @@ def test_training_fits_a_smooth_target(ctx):
     cache = RadianceCache(ctx, [-1, -1, -1], [1, 1, 1], log2_table=16, seed=11, learning_rate=5e-3)
     x = random_inputs(8192, 12)
     p = x[:, 0:3]
-    y = np.stack([0.6 + 0.4 * np.sin(3 * p[:, 0]), 0.5 + 0.3 * np.cos(2 * p[:, 1]), 0.4 + 0.2 * p[:, 2] * x[:, 8]], 1)
+    y = np.stack([0.6 + 0.4 * np.sin(3 * p[:, 0]), 0.5 + 0.3 * np.cos(2 * p[:, 1]), 0.4 + 0.2 * p[:, 2] * x[:, 8],
+                  np.zeros(len(x))], 1)
     first = cache.train(x, y)
     last = first
     for _ in range(300):
@@ -112,7 +115,7 @@ def test_cached_cornell_matches_path_tracer(ctx, cornell_scene, mode):
     scene.render(vt.make_params(cam, W, H, 8, 1, True, 1), 1024)
     ref, _ = scene.readback()
     info = mesh.info()
-    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=21)
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=21, spectral=1)
     scene.reset()
     for f in range(120):  # training frames only
         cache.render(scene, vt.make_params(cam, W, H, 8, 1 + f, True, mode), 0, render=False)
@@ -131,11 +134,15 @@ def test_cached_cornell_matches_path_tracer(ctx, cornell_scene, mode):
 def test_render_nrc_rejects_other_modes(ctx, cornell_scene):
     mesh, scene, cam = cornell_scene
     info = mesh.info()
-    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=1024)
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=1024, spectral=1)
     with pytest.raises(vt.MaterialLibraryError, match="sampling modes 0"):
         cache.render(scene, vt.make_params(cam, 16, 16, 8, 1, True, 2), 1)
-    with pytest.raises(vt.MaterialLibraryError, match="query_vertex"):
-        RadianceCache(ctx, list(info.lo), list(info.hi), query_vertex=0)
+    with pytest.raises(vt.MaterialLibraryError, match="transport"):
+        cache.render(scene, vt.make_params(cam, 16, 16, 8, 1, False, 1), 1)
+    with pytest.raises(vt.MaterialLibraryError, match="whole frames"):
+        cache.render(scene, vt.make_params(cam, 16, 16, 8, 1, True, 1, pixel_stride=2), 1)
+    with pytest.raises(vt.MaterialLibraryError, match="spread"):
+        RadianceCache(ctx, list(info.lo), list(info.hi), query_vertex=0, spread=0.0)
     cache.close()
 
 
@@ -151,7 +158,7 @@ def test_cached_openpbr_cornell(ctx):
     ref, _ = scene.readback()
     info = mesh.info()
     for mode in (1, 0):
-        cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=5)
+        cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=16384, seed=5, spectral=1)
         scene.reset()
         for f in range(120):
             cache.render(scene, vt.make_params(cam, W, H, 8, 1 + f, True, mode), 0, render=False)

@@ -157,3 +157,40 @@ def test_smooth_normals_match_oracle(ctx, oracle, mode):
     gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
     assert np.all(np.abs(gm / rm - 1) < (MEAN_REL if mode else 5e-3)), (gm, rm)
     assert relmse(gpu, ref) < (0.25 if mode else 1.0) * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+
+
+@pytest.mark.parametrize("stride", [3, 8])
+def test_pixel_stride_renders_the_frames_own_pixels(ctx, cornell, stride):
+    """A strided render (vt_frame_params.pixel_stride) is the full frame's pixels (s i, s j): the same
+    camera rays and sample streams, so the same FP64 sums up to summation order."""
+    faces, verts, mats, light, cam, mesh = cornell
+    tables = spectral_tables.load()
+    full = gpu_render(ctx, cornell, 64, 48, 8, True)
+    scene = vt.Scene(ctx, mesh, mats, light, tables)
+    scene.render(vt.make_params(cam, 64, 48, 8, 1, True, 1, pixel_stride=stride), 8)
+    img, n = scene.readback()
+    assert n == 8 and img.shape == (-(-48 // stride), -(-64 // stride), 3)
+    np.testing.assert_allclose(img, full[::stride, ::stride], rtol=1e-12, atol=1e-15)
+    with pytest.raises(vt.MaterialLibraryError, match="pixel stride"):
+        scene.render(vt.make_params(cam, 64, 48, 8, 1, True, 0, pixel_stride=stride), 1)
+    scene.close()
+
+
+def test_accumulation_save_and_restore_continue_a_render(ctx, cornell, tmp_path):
+    """A render taken in two pieces through save_accumulation / restore_accumulation (vt_accum_restore)
+    equals the same render in one piece: the FP64 sums and the sample count carry over."""
+    faces, verts, mats, light, cam, mesh = cornell
+    tables = spectral_tables.load()
+    whole = gpu_render(ctx, cornell, 48, 48, 16, True)
+    a = vt.Scene(ctx, mesh, mats, light, tables)
+    p = vt.make_params(cam, 48, 48, 8, 1, True, 1, pixel_stride=2)
+    a.render(p, 8)
+    assert a.save_accumulation(tmp_path / "acc.npz", p) == 8
+    a.close()
+    b = vt.Scene(ctx, mesh, mats, light, tables)
+    assert b.restore_accumulation(tmp_path / "acc.npz") == 8
+    b.render(vt.make_params(cam, 48, 48, 8, 9, True, 1, pixel_stride=2), 8)
+    img, n = b.readback()
+    b.close()
+    assert n == 16
+    np.testing.assert_allclose(img, whole[::2, ::2], rtol=1e-12, atol=1e-15)

@@ -12,28 +12,30 @@ from oracle import nrc_ref as R
 def random_case(n=12, levels=4, log_t=12, seed=0):
     rng = np.random.default_rng(seed)
     grid = R.Grid(levels, log_t, 4, 64, [-1, -1, -1], [1, 1, 1])
-    x = np.zeros((n, 12), np.float32)
+    x = np.zeros((n, 13), np.float32)
     x[:, 0:3] = rng.uniform(-0.9, 0.9, (n, 3))
     x[:, 3] = rng.uniform(0, 1, n)
     x[:, 4:8] = rng.uniform(0, 1, (n, 4))
     x[:, 8:11] = rng.uniform(0, 1, (n, 3))
     x[:, 11] = rng.uniform(0, 1, n)
+    x[:, 12] = rng.uniform(0, 1, n)
     mlp = np.zeros(R.MLP_PARAMS)
     mlp[:R.HIDDEN * 4096] = rng.uniform(-0.3, 0.3, R.HIDDEN * 4096)
-    mlp[R.HIDDEN * 4096:R.HIDDEN * 4096 + 3 * 64] = rng.uniform(-0.3, 0.3, 3 * 64)
+    mlp[R.HIDDEN * 4096:R.HIDDEN * 4096 + 4 * 64] = rng.uniform(-0.3, 0.3, 4 * 64)
     table = rng.uniform(-1, 1, (levels, grid.entries, 2))
-    y = rng.uniform(0, 2, (n, 3))
+    y = rng.uniform(0, 2, (n, 4))
     return grid, x, mlp, table, y
 
 
-def test_gradients_match_finite_differences():
+@pytest.mark.parametrize("spectral", [False, True])
+def test_gradients_match_finite_differences(spectral):
     grid, x, mlp, table, y = random_case()
-    gm, gt, loss = R.gradients(x, y, mlp, table, grid, exact=True)
-    den = R.denominators(x, mlp, table, grid)
+    gm, gt, loss = R.gradients(x, y, mlp, table, grid, exact=True, spectral=spectral)
+    den = R.denominators(x, mlp, table, grid, spectral=spectral)
     assert loss == pytest.approx(R.loss_sum(x, y, mlp, table, grid, den), rel=1e-12)
     rng = np.random.default_rng(1)
     h = 1e-6
-    picks = list(rng.choice(R.HIDDEN * 4096, 12, replace=False)) + list(R.HIDDEN * 4096 + rng.choice(3 * 64, 4, replace=False))
+    picks = list(rng.choice(R.HIDDEN * 4096, 12, replace=False)) + list(R.HIDDEN * 4096 + rng.choice(4 * 64, 4, replace=False))
     for i in picks:
         mp, mm = mlp.copy(), mlp.copy()
         mp[i] += h
@@ -70,8 +72,29 @@ def test_corners_dense_and_hashed():
 def test_encoding_fixed_entries():
     grid, x, mlp, table, y = random_case(n=5)
     e = R.encode(x, table, grid)
-    assert np.all(e[:, 63] == 1.0) and np.all(e[:, 56:63] == 0.0)
-    # One-blob: the kernel of the bin holding s is the largest.
+    assert np.all(e[:, 63] == 1.0)
+    # One-blob: the kernel of the bin holding s is the largest (direction, wavelength number).
     assert np.all(np.argmax(e[:, 32:36], 1) == np.minimum((x[:, 4] * 4).astype(int), 3))
+    assert np.all(np.argmax(e[:, 56:60], 1) == np.minimum((x[:, 12] * 4).astype(int), 3))
+    # The frequency encoding of the normalised position.
+    q = grid.position(x[:, 0:3]).astype(np.float64)
+    assert np.abs(e[:, 60:63] - np.sin(2 * np.pi * q)).max() < 1e-3
     # fp16 values.
     assert np.all(e.astype(np.float16).astype(np.float64) == e)
+
+
+def test_loss_scale_keeps_small_gradients():
+    """The backward pass's fp16 values carry the loss gradient times LOSS_SCALE. With targets within
+    1e-6 of the (fp16) prediction, the per-record gradients fall into fp16's subnormal range: without
+    the scale they lose most of their precision, with it they stay close to a run whose scale leaves
+    every value normal."""
+    grid, x, mlp, table, _ = random_case(n=64, seed=3)
+    p = R.predict(x, mlp, table, grid)
+    y = p + 1e-6 * np.random.default_rng(4).standard_normal(p.shape)
+    ref, _, _ = R.gradients(x, y, mlp, table, grid, loss_scale=4096.0)
+    scaled, _, _ = R.gradients(x, y, mlp, table, grid)
+    unscaled, _, _ = R.gradients(x, y, mlp, table, grid, loss_scale=1.0)
+    n = R.HIDDEN * 4096
+    e_scaled = np.abs(scaled[:n] - ref[:n]).max()
+    e_unscaled = np.abs(unscaled[:n] - ref[:n]).max()
+    assert e_scaled < 0.02 * np.abs(ref[:n]).max() and e_scaled < 0.1 * e_unscaled, (e_scaled, e_unscaled)
