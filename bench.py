@@ -414,23 +414,27 @@ def bench_production(a, ctx, stream) -> dict:
                        "light tree, %d material slots (OPENPBR: base colour, roughness, metalness, IOR; spectral uplift), "
                        "1920x1080, 4 wavelengths, depth 12" % (len(faces), int((faces["tag"] >= 287).sum()), len(mats)),
            "triangles": int(len(faces)), "build_ms": info.build_ms, "scene_create_s": scene_s, "generate_s": gen_s}
-    for name, mode, cand in (("restir_di_32", 0, 32), ("mis", 1, 0)):
+    for name, mode, cand, wavefront in (("restir_di_32", 0, 32, False), ("mis", 1, 0, False),
+                                        ("mis_wavefront", 1, 0, True)):
         scene.reset()
         frame = 0
+        render = scene.render_wavefront if wavefront else scene.render
         for _ in range(2):
             frame += 1
-            scene.render(vt.make_params(cam, W, H, depth, frame, True, mode, di_candidates=cand), 1, cs)
+            render(vt.make_params(cam, W, H, depth, frame, True, mode, di_candidates=cand), 1, cs)
         torch.cuda.synchronize()
         n = max(1, a.production_frames)
         e0.record(stream)
         for _ in range(n):
             frame += 1
-            scene.render(vt.make_params(cam, W, H, depth, frame, True, mode, di_candidates=cand), 1, cs)
+            render(vt.make_params(cam, W, H, depth, frame, True, mode, di_candidates=cand), 1, cs)
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / n
-        out[name] = {"ms_per_frame": ms, "paths_per_s": W * H / (ms / 1e3), "frames": n,
-                     "gpu_launches_per_frame": 2 if mode == 0 else 1}
+        # Launches per frame: the megakernel's 1 (2 for ReSTIR DI); the wavefront's camera rays,
+        # (depth + 1) x (extend, shade, shadow) and the accumulation.
+        launches = 2 if mode == 0 else (2 + 3 * (depth + 1) if wavefront else 1)
+        out[name] = {"ms_per_frame": ms, "paths_per_s": W * H / (ms / 1e3), "frames": n, "gpu_launches_per_frame": launches}
     scene.close()
     mesh.close()
     return out

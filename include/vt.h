@@ -234,6 +234,15 @@ vt_status vt_scene_destroy(vt_ctx *ctx, vt_scene *scene);
  * (shading_kernel, main.swift:7370-7914). Resizing (a new width/height) resets the accumulation.
  * Stream-ordered; NULL = the CUDA default stream. */
 vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *params, uint32_t spp, void *stream);
+/* The same frames and samples (sampling modes 1-3) through the wavefront integrator: the paths'
+ * state lives in device memory between stage kernels over queues of live paths (camera rays;
+ * per bounce the closest-hit traversal of the queue, shading with NEE and the BSDF continuation,
+ * the shadow rays' any-hit traversal; then the accumulation), with the megakernel's sampler draws
+ * and arithmetic per path, so the image equals vt_render's up to the order of the FP64 sums. The
+ * reference has no wavefront path; its design note proposes the split (docs/KERNEL_SPLIT_DESIGN.md:
+ * 72-74). Paths per pass are capped at 4M (whole samples of the frame); the state takes ~250 bytes
+ * per path, allocated with the scene on first use. */
+vt_status vt_render_wavefront(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *params, uint32_t spp, void *stream);
 vt_status vt_accum_reset(vt_ctx *ctx, vt_scene *scene);
 /* Mean radiance per pixel (linear sRGB, row-major, 3 doubles per pixel; n = width * height * 3
  * of the accumulation, ceil(width / s) * ceil(height / s) * 3 for a pixel stride s) and the number
@@ -484,7 +493,7 @@ typedef struct vt_nrc_config {
                                 (sum_i sqrt(|x_i-1 - x_i|^2 / (p(w_i) |cos theta_i|)))^2 > c a0,
                                 a0 = |x0 - x1|^2 / (4 pi cos theta_1) (0.01) */
   uint32_t spectral;         /* 1: the outputs are, per hero wavelength of a path, its radiance
-                                times the lane's share 1 / (4 p(lambda)), and scenes render with
+                                over the illuminant at that wavelength, and scenes render with
                                 spectral transport; 0: rgb (0) */
 } vt_nrc_config;
 /* A cache query (64 bytes). Directions are (theta / pi, phi / (2 pi) + 1/2), theta from +z and phi

@@ -134,6 +134,7 @@ SIGNATURES = {
     "vt_scene_create": (_I32, [_P, _P, _P, _U32, _P, _P, C.POINTER(_P)]),
     "vt_scene_destroy": (_I32, [_P, _P]),
     "vt_render": (_I32, [_P, _P, _P, _U32, _P]),
+    "vt_render_wavefront": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_accum_reset": (_I32, [_P, _P]),
     "vt_accum_readback": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_accum_restore": (_I32, [_P, _P, _U32, _U32, _U32, _P, _U32, _U32]),

@@ -15,8 +15,8 @@
 // frequency encoding sin(2 pi q) of the normalised position q (a collision-free coarse term beside
 // the hash grid); [63] one (the first layer's bias).
 // Network: 64 -> 64 (ReLU) x 5 hidden layers -> 4 (linear), fp16 operands, fp32 accumulation,
-// no biases besides input 63. Outputs: per hero wavelength of the path its radiance times the
-// lane's share 1 / (4 p(lambda)) (spectral caches), or rgb and 0 (RGB caches). Weights are stored
+// no biases besides input 63. Outputs: per hero wavelength of the path its radiance over the
+// illuminant at that wavelength (spectral caches), or rgb and 0 (RGB caches). Weights are stored
 // [out][in], fp32 masters, the output layer padded to 16 rows (rows 4-15 stay zero).
 #pragma once
 

@@ -184,9 +184,7 @@ __device__ __forceinline__ float max_abs3(float x, float y, float z) { return fm
 __device__ __forceinline__ float max_abs(float3 p) { return max_abs3(p.x, p.y, p.z); }
 
 // mesh_hit_error (main.swift:1353-1355) of an imported triangle: its vertices' rounding bound.
-__device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) {
-  return fmaxf(1e-7f, 1.907349e-6f * fmaxf(max_abs3(a.x, a.y, a.z), fmaxf(max_abs3(b.x, b.y, b.z), max_abs3(c.x, c.y, c.z))));
-}
+__device__ __forceinline__ float mesh_hit_error(float4 a, float4 b, float4 c) { return tri_error_bound(a, b, c); }
 
 // Any hit in [tMin, tMax); with `slack` (imported scenes) each triangle's own rounding bound is
 // taken off tMax, so the endpoint surface does not occlude itself (scene_occluded, main.swift:
@@ -738,17 +736,27 @@ __device__ __forceinline__ float3 ray_origin(const RenderArgs &A, float3 p, floa
 
 // light_visible (main.swift:3254-3264): shadow ray from the offset origin to the sample, shortened
 // by the endpoint tolerance (endpoint_tolerance, main.swift:1358-1361).
-__device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
-                                              const LightSample &ls, int *stack) {
+// Its shadow ray: origin, unit direction and end; false when there is none to trace (no sample, or
+// the sample within the endpoint tolerance).
+__device__ __forceinline__ bool shadow_ray(const RenderArgs &A, float3 p, float3 gn, float err, const LightSample &ls,
+                                           float3 &o, float3 &dir, float &tmax) {
   if (ls.pdf <= 0.0f) return false;
-  const float3 o = ray_origin(A, p, gn, ls.wi, err);
+  o = ray_origin(A, p, gn, ls.wi, err);
   float3 delta = sub(ls.pos, o);
   const float d = sqrtf(dot3(delta, delta));
   const float legacy = 2.0f * ray_eps(A, ls.pos);
   const float tol = A.imported ? fmaxf(legacy, 1.907349e-6f * (max_abs(o) + max_abs(ls.pos) + d)) : legacy;
   if (d <= tol) return false;
-  delta = mul(delta, 1.0f / d);
-  return !rt_any(A, o, delta, ray_tmin(A, o), d - tol, stack, A.imported != 0u);
+  dir = mul(delta, 1.0f / d);
+  tmax = d - tol;
+  return true;
+}
+__device__ __forceinline__ bool light_visible(const RenderArgs &A, float3 p, float3 gn, float err,
+                                              const LightSample &ls, int *stack) {
+  float3 o, dir;
+  float tmax;
+  if (!shadow_ray(A, p, gn, err, ls, o, dir, tmax)) return false;
+  return !rt_any(A, o, dir, ray_tmin(A, o), tmax, stack, A.imported != 0u);
 }
 
 // power_heuristic (main.swift:2454-2460): beta = 2, scaled by the larger density.
@@ -852,14 +860,11 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 
 // NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
 // n is the shading normal, gn the geometric one (both facing the incoming ray).
+// The contribution of a visible light sample ls per lane (throughput T, BSDF, emission, cosine,
+// MIS weight against the BSDF pdf when useMIS, over the light pdf).
 template <bool kPbr>
-__device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
-                                                     float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
-                                                     Sampler &seed, int *stack, bool requirePdf) {
-  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const LightSample ls = sample_direct(A, p, n, seed);
-  if (requirePdf && !(ls.pdf > 0.0f)) return zero;
-  if (!light_visible(A, p, gn, err, ls, stack)) return zero;
+__device__ __forceinline__ float4 nee_lanes(const RenderArgs &A, const Lanes &L, float3 n, float3 gn, float3 wo, float4 T,
+                                            const vt_material &m, bool useMIS, const LightSample &ls) {
   const float cosine = fabsf(dot3(n, ls.wi));
   if (is_pbr<kPbr>(A, m)) {
     float bpdf;
@@ -881,6 +886,16 @@ __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const 
   const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
   const float4 Le = emission(A, L, le);
   return scale4(mul4(mul4(T, albedo), Le), f * cosine * weight / ls.pdf);
+}
+template <bool kPbr>
+__device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
+                                                     float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
+                                                     Sampler &seed, int *stack, bool requirePdf) {
+  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const LightSample ls = sample_direct(A, p, n, seed);
+  if (requirePdf && !(ls.pdf > 0.0f)) return zero;
+  if (!light_visible(A, p, gn, err, ls, stack)) return zero;
+  return nee_lanes<kPbr>(A, L, n, gn, wo, T, m, useMIS, ls);
 }
 // The same as rgb.
 template <bool kPbr>
@@ -1060,13 +1075,18 @@ __device__ __forceinline__ float nrc_spread_limit(const RenderArgs &A, float t, 
   const float c = fmaxf(fabsf(dot3(gn, dir)), 1e-6f);
   return A.nrcSpread * t * t / (4.0f * 3.14159265f * c);
 }
-// Stores the query of slot `slot`, with the throughput T and the lanes' bins. (A spectral cache
-// predicts each lane's radiance times the lane's share 1 / (4 p(lambda)), the lane's term of the
-// spectral estimator, so T is stored without the shares.)
+// The illuminant at a lane's bin: a spectral cache learns each lane's radiance over it.
+__device__ __forceinline__ float lane_illuminant(const RenderArgs &A, const Lanes &L, int k) {
+  return __ldg(A.spec + L.bin[k]).w;
+}
+// Stores the query of slot `slot`, with the lanes' bins and the throughput T times, per lane, its
+// share and the illuminant there (a spectral cache predicts each lane's radiance over the
+// illuminant, so the resolve multiplies both back).
 __device__ __forceinline__ void nrc_store(const RenderArgs &A, size_t slot, const NrcInput &q, const Lanes &L, float4 T) {
   A.nrcIn[slot] = q;
   if (A.spectral) {
-    A.nrcT[slot] = T;
+    A.nrcT[slot] = make_float4(T.x * L.w[0] * lane_illuminant(A, L, 0), T.y * L.w[1] * lane_illuminant(A, L, 1),
+                               T.z * L.w[2] * lane_illuminant(A, L, 2), T.w * L.w[3] * lane_illuminant(A, L, 3));
     A.nrcBins[slot] = make_uint2((uint32_t)L.bin[0] | ((uint32_t)L.bin[1] << 16), (uint32_t)L.bin[2] | ((uint32_t)L.bin[3] << 16));
   } else {
     A.nrcT[slot] = make_float4(T.x, T.y, T.z, 0.0f);
@@ -1371,6 +1391,300 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
   }
 }
 
+// ---- wavefront integrator (vt_render_wavefront; sampling modes 1-3) ------------------------------
+// The paths of k_render / path_sample taken apart into stage kernels over queues of path indices,
+// with the path's state in HBM between them (WfArgs, structure of arrays). Per bounce b:
+//   extend  the persistent closest-hit traversal of traverse.cu (quantised nodes, shared-memory
+//           stacks) over the queue of live paths, hits reporting BVH positions;
+//   shade   k_wf_shade: first the previous vertex's shadow result, then one vertex of the path in
+//           continue_path's order (emission with its MIS weight, NEE, Russian roulette, the BSDF
+//           continuation), drawing the same numbers from the same sampler; the NEE sample's shadow
+//           ray and contribution go to the shadow queue, a continuing path to the next live queue;
+//   shadow  the persistent any-hit traversal over the shadow queue (with imported scenes' endpoint
+//           slack).
+// Queues are compacted per block: a warp ballot gives each surviving lane its rank, one shared-
+// memory atomic per warp and one global atomic per block reserve the slots, and the block's
+// entries land contiguously. k_wf_finish adds each path's radiance (primary NEE + continuation,
+// summed in k_render's order) to its pixel's FP64 accumulation.
+constexpr int kWfBlock = 256;
+constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u;
+
+struct WfArgs {
+  float4 *T;      // throughput per lane
+  float4 *Rc;     // radiance of the continuation (rgb)
+  float4 *Rp;     // radiance at the primary vertex: its NEE, or its emission / the sky it sees (rgb)
+  float4 *prev;   // previous vertex: position, BSDF pdf of the continuation from it
+  float4 *prevN;  // previous vertex's shading normal, the path's wavelength number
+  uint4 *seedA;   // sampler: state, key, dimension, sub
+  uint2 *seedB;   // sampler: subBits, z
+  uint4 *meta;    // pixel, bounce, scattering, flags
+  float4 *ray;    // the path's next ray (vt_ray: origin, tmin; direction, tmax)
+  const int4 *hit;  // its closest hit (t, b1, b2 bits; BVH position or -1)
+  float4 *sray;   // the NEE sample's shadow ray (vt_ray)
+  float4 *scon;   // its contribution (rgb)
+  const uint8_t *occ;  // its occlusion
+  const uint32_t *inQ, *inCount;  // live paths of this bounce (null: paths 0 .. paths - 1)
+  uint32_t *outQ, *outCount;      // live paths of the next bounce
+  uint32_t *shQ, *shCount;        // shadow rays of this bounce
+  uint32_t npix, paths, k0;       // accumulation pixels; paths of the pass; its first sample (of the call)
+};
+
+__device__ __forceinline__ void wf_store_seed(const WfArgs &W, uint32_t i, const Sampler &s) {
+  W.seedA[i] = make_uint4(s.state, s.key, s.dimension, s.sub);
+  W.seedB[i] = make_uint2(s.subBits, s.z ? 1u : 0u);
+}
+__device__ __forceinline__ Sampler wf_load_seed(const WfArgs &W, uint32_t i) {
+  const uint4 a = W.seedA[i];
+  const uint2 b = W.seedB[i];
+  Sampler s;
+  s.state = a.x; s.key = a.y; s.dimension = a.z; s.sub = a.w; s.subBits = b.x; s.z = b.y != 0u;
+  return s;
+}
+__device__ __forceinline__ void wf_set_ray(float4 *r, uint32_t i, float3 o, float tmin, float3 d, float tmax) {
+  r[2 * (size_t)i] = make_float4(o.x, o.y, o.z, tmin);
+  r[2 * (size_t)i + 1] = make_float4(d.x, d.y, d.z, tmax);
+}
+
+// Appends v to queue q when `push`; every thread of the block calls it (uniform control flow).
+__device__ __forceinline__ void wf_push(bool push, uint32_t v, uint32_t *q, uint32_t *count, uint32_t &sTotal,
+                                        uint32_t &sBase) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned m = __ballot_sync(0xffffffffu, push);
+  if (threadIdx.x == 0) sTotal = 0;
+  __syncthreads();
+  uint32_t w = 0;
+  if (lane == 0 && m) w = atomicAdd(&sTotal, (uint32_t)__popc(m));
+  w = __shfl_sync(0xffffffffu, w, 0);
+  __syncthreads();
+  if (threadIdx.x == 0) sBase = sTotal ? atomicAdd(count, sTotal) : 0u;
+  __syncthreads();
+  if (push) q[sBase + w + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
+  __syncthreads();  // sTotal and sBase are reused by the next push
+}
+
+// The NEE of one vertex up to its visibility: the sample (the draws of direct_light_lanes), its
+// shadow ray into sray[i] and its contribution as rgb into scon[i]; false when there is nothing
+// to trace.
+template <bool kPbr>
+__device__ __forceinline__ bool wf_nee(const RenderArgs &A, const WfArgs &W, uint32_t i, const Lanes &L, const Surface &S,
+                                       float3 wo, float4 T, const vt_material &m, bool useMIS, Sampler &seed,
+                                       bool requirePdf) {
+  const LightSample ls = sample_direct(A, S.pos, S.n, seed);
+  if (requirePdf && !(ls.pdf > 0.0f)) return false;
+  float3 o, dir;
+  float tmax;
+  if (!shadow_ray(A, S.pos, S.gn, S.err, ls, o, dir, tmax)) return false;
+  const float3 c = to_rgb(A, L, nee_lanes<kPbr>(A, L, S.n, S.gn, wo, T, m, useMIS, ls));
+  W.scon[i] = make_float4(c.x, c.y, c.z, 0.0f);
+  wf_set_ray(W.sray, i, o, ray_tmin(A, o), dir, tmax);
+  return true;
+}
+
+// One vertex of path i at bounce b (0: the primary hit). Sets `next` when the path continues and
+// `shadow` when it queued a shadow ray.
+template <bool kPbr>
+__device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, uint32_t i, uint32_t b, bool &next,
+                                          bool &shadow) {
+  uint4 meta = W.meta[i];
+  uint32_t flags = meta.w;
+  float4 Rc = W.Rc[i], Rp = W.Rp[i];
+  if (flags & kWfShadow) {  // the previous vertex's NEE, traced since
+    if (!W.occ[i]) {
+      const float4 c = W.scon[i];
+      if (flags & kWfShadowPrimary) Rp = make_float4(Rp.x + c.x, Rp.y + c.y, Rp.z + c.z, 0.0f);
+      else Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
+    }
+    flags &= ~(kWfShadow | kWfShadowPrimary);
+  }
+  Sampler seed = wf_load_seed(W, i);
+  const float4 pn = W.prevN[i];
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, pn.w);
+  const float4 r0 = W.ray[2 * (size_t)i], r1 = W.ray[2 * (size_t)i + 1];
+  const float3 o = f3(r0.x, r0.y, r0.z), dir = f3(r1.x, r1.y, r1.z);
+  const int4 h4 = W.hit[i];
+  Hit h;
+  h.t = __int_as_float(h4.x); h.b1 = __int_as_float(h4.y); h.b2 = __int_as_float(h4.z); h.pos = h4.w;
+  const int limit = max(0, (int)A.maxDepth - 1);
+  const bool nee = A.mode != 3u, mis = A.mode <= 1u;
+  float4 T = W.T[i];
+  int scattering = (int)meta.z;
+  bool emissionOnly = (flags & kWfEmissionOnly) != 0u;
+  Surface S;
+  vt_material m;
+  bool alive = true;
+  if (b == 0u) {  // path_sample_body after the camera ray's trace
+    if (h.pos < 0) {
+      if (A.env) {
+        const float3 e = environment(A, dir);
+        Rp = make_float4(e.x, e.y, e.z, 0.0f);
+      }
+      alive = false;
+    } else {
+      S = surface_at(A, h, o, dir);
+      m = material(A, S.slot);
+      if (m.type == VT_MAT_EMISSIVE) {
+        const float3 e = primary_emission(A, L, S, m);
+        Rp = make_float4(e.x, e.y, e.z, 0.0f);
+        alive = false;
+      } else {
+        T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        if (A.mode != 3u) {
+          sampler_event(seed, 1u, kZNee);
+          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, A.mode == 1u && limit > 0, seed, true)) {
+            shadow = true;
+            flags |= kWfShadow | kWfShadowPrimary;
+          }
+        }
+        scattering = 0;
+        emissionOnly = false;
+      }
+    }
+  } else {  // continue_path after its trace at bounce b
+    const float4 pv = W.prev[i];
+    const float bpdf = pv.w;
+    const bool previousMIS = (flags & kWfPrevMIS) != 0u;
+    if (h.pos < 0) {
+      if (A.env) {
+        const float lpdf = nee ? environment_pdf(A, dir, f3(pn.x, pn.y, pn.z)) : 0.0f;
+        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+        const float3 c = to_rgb(A, L, scale4(mul4(T, emission3(A, L, environment(A, dir))), w));
+        Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
+      }
+      alive = false;
+    } else {
+      const float3 prevPos = f3(pv.x, pv.y, pv.z);
+      S = surface_at(A, h, o, dir);
+      m = material(A, S.slot);
+      if (m.type == VT_MAT_EMISSIVE) {
+        const float lpdf = A.imported ? emitter_pdf(A, prevPos, S.pos, S.face) : light_pdf(A, prevPos, S.pos);
+        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+        if (!A.imported || S.front) {
+          const float3 c = to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w));
+          Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
+        }
+        alive = false;
+      } else if (emissionOnly) {
+        alive = false;
+      } else {
+        if (nee) {
+          sampler_event(seed, b + 1u, kZNee);
+          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, mis && scattering < limit, seed, false)) {
+            shadow = true;
+            flags |= kWfShadow;
+          }
+        }
+        if (b > 3u) {
+          const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+          sampler_event(seed, b + 1u, kZRoulette);
+          if (rand_f(seed) >= survival) alive = false;
+          else T = scale4(T, 1.0f / survival);
+        }
+      }
+    }
+  }
+  if (alive) {  // continue_path's loop head at bounce b + 1: the BSDF continuation
+    const uint32_t nb = b + 1u;
+    if (scattering >= limit) {
+      if (nee || emissionOnly) alive = false;
+      emissionOnly = true;
+    }
+    if (alive) {
+      ++scattering;
+      sampler_event(seed, nb, kZBsdf);
+      const float3 r = rand_f3(seed);
+      float3 nd;
+      float bpdf;
+      if (is_pbr<kPbr>(A, m)) {
+        float4 w;
+        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) alive = false;
+        else T = mul4(T, w);
+      } else {
+        nd = cosine_hemisphere(S.n, r.y, r.z);
+        bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+        if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) alive = false;
+        else T = mul4(T, reflectance(A, L, m));
+      }
+      if (alive && (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f))
+        alive = false;
+      if (alive) {
+        const float3 no = ray_origin(A, S.pos, S.gn, nd, S.err);
+        wf_set_ray(W.ray, i, no, ray_tmin(A, no), nd, __int_as_float(0x7f800000));
+        W.prev[i] = make_float4(S.pos.x, S.pos.y, S.pos.z, bpdf);
+        W.prevN[i] = make_float4(S.n.x, S.n.y, S.n.z, pn.w);
+        W.T[i] = T;
+        flags = mis ? (flags | kWfPrevMIS) : (flags & ~kWfPrevMIS);
+        next = true;
+      }
+    }
+  }
+  flags = emissionOnly ? (flags | kWfEmissionOnly) : (flags & ~kWfEmissionOnly);
+  W.meta[i] = make_uint4(meta.x, next ? b + 1u : b, (uint32_t)scattering, flags);
+  W.Rc[i] = Rc;
+  W.Rp[i] = Rp;
+  if (next) wf_store_seed(W, i, seed);
+}
+
+// The pass's paths: sampler, wavelengths and camera ray (path_sample_body's draws before the trace;
+// the shading seed's rehash needs no hit, so it happens here too); path i is sample k0 + i / npix
+// of accumulation pixel i % npix.
+__global__ void __launch_bounds__(kWfBlock) k_wf_generate(RenderArgs A, WfArgs W) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.paths; i += gridDim.x * blockDim.x) {
+    const uint32_t p = i % W.npix, k = W.k0 + i / W.npix;
+    const uint32_t x = (p % A.OW) * A.stride, y = (p / A.OW) * A.stride;
+    Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
+    const float u = A.spectral ? wavelength_numbers(seed).x : 0.0f;
+    float3 dir0 = camera_dir(A, x, y, A.jitter[k]), o0 = A.cam;
+    lens_ray(A, o0, dir0, seed);
+    seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
+    wf_set_ray(W.ray, i, o0, ray_tmin(A, o0), dir0, __int_as_float(0x7f800000));
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    W.T[i] = zero;
+    W.Rc[i] = zero;
+    W.Rp[i] = zero;
+    W.prevN[i] = make_float4(0.0f, 0.0f, 0.0f, u);
+    W.meta[i] = make_uint4(p, 0u, 0u, 0u);
+    wf_store_seed(W, i, seed);
+  }
+}
+
+template <bool kPbr>
+__global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, uint32_t bounce) {
+  __shared__ uint32_t sTotal, sBase;
+  const uint32_t n = W.inCount ? min(*W.inCount, W.paths) : W.paths;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t q = base + threadIdx.x;
+    bool next = false, shadow = false;
+    uint32_t i = 0;
+    if (q < n) {
+      i = W.inQ ? W.inQ[q] : q;
+      wf_vertex<kPbr>(A, W, i, bounce, next, shadow);
+    }
+    wf_push(next, i, W.outQ, W.outCount, sTotal, sBase);
+    wf_push(shadow, i, W.shQ, W.shCount, sTotal, sBase);
+  }
+}
+
+// Each path's radiance (its last shadow result first) into its pixel's FP64 sum: primary NEE plus
+// continuation, in k_render's order, non-finite sums dropped.
+__global__ void __launch_bounds__(kWfBlock) k_wf_finish(RenderArgs A, WfArgs W) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.paths; i += gridDim.x * blockDim.x) {
+    const uint4 meta = W.meta[i];
+    float4 Rc = W.Rc[i], Rp = W.Rp[i];
+    if ((meta.w & kWfShadow) && !W.occ[i]) {
+      const float4 c = W.scon[i];
+      if (meta.w & kWfShadowPrimary) Rp = make_float4(Rp.x + c.x, Rp.y + c.y, Rp.z + c.z, 0.0f);
+      else Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
+    }
+    const float3 R = add(f3(Rp.x, Rp.y, Rp.z), f3(Rc.x, Rc.y, Rc.z));
+    if (!isfinite(R.x) || !isfinite(R.y) || !isfinite(R.z)) continue;
+    double *acc = A.accum + 3 * (size_t)meta.x;
+    atomicAdd(acc, (double)R.x);
+    atomicAdd(acc + 1, (double)R.y);
+    atomicAdd(acc + 2, (double)R.z);
+  }
+}
+
 // ---- radiance cache: training paths and the resolve (vt_render_nrc) -----------------------------
 constexpr int kNrcRecords = 8;  // records per training path: its first 8 vertices
 
@@ -1484,10 +1798,12 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     const float4 t = r[3], r0 = r[4];
     float4 d = make_float4(t.x > 1e-20f ? (R.x - r0.x) / t.x : 0.0f, t.y > 1e-20f ? (R.y - r0.y) / t.y : 0.0f,
                            t.z > 1e-20f ? (R.z - r0.z) / t.z : 0.0f, t.w > 1e-20f ? (R.w - r0.w) / t.w : 0.0f);
-    // Spectral targets: each lane's radiance times its share (values of the size of rgb radiance;
-    // the bare lane radiance of a D65-relative emitter is ~1/100 of it, where the relative loss's
-    // epsilon would swamp it).
-    if (A.spectral) d = make_float4(d.x * L.w[0], d.y * L.w[1], d.z * L.w[2], d.w * L.w[3]);
+    // Spectral targets: each lane's radiance over the illuminant at its wavelength (a smooth quantity
+    // of the size of rgb radiance; the bare lane radiance of a D65-relative emitter is ~1/100 of it,
+    // where the relative loss's epsilon would swamp it).
+    if (A.spectral)
+      d = make_float4(d.x / lane_illuminant(A, L, 0), d.y / lane_illuminant(A, L, 1), d.z / lane_illuminant(A, L, 2),
+                      d.w / lane_illuminant(A, L, 3));
     if (!isfinite(d.x) || !isfinite(d.y) || !isfinite(d.z) || !isfinite(d.w)) d = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     NrcInput q;
     q.a = r[0]; q.b = r[1]; q.c = r[2];
@@ -1499,7 +1815,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
 
 // Adds each pixel's cache contributions: per sample slot with a query, the throughput times the
 // prediction (clamped at zero) lane by lane, to rgb (spectral transport: the lanes' colour-matching
-// functions at the slot's bins; the prediction carries each lane's share).
+// functions at the slot's bins; the stored throughput carries each lane's share and illuminant).
 __global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uint32_t spp) {
   const uint32_t npix = A.W * A.H;
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1750,6 +2066,7 @@ void scene_free(vt_scene *scene) {
   cudaFree(scene->d_emissions);
   cudaFree(scene->d_face_pos);
   cudaFree(scene->d_di);
+  cudaFree(scene->d_wf);
   delete scene;
 }
 
@@ -2228,6 +2545,134 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
   return VT_OK;
 }
 
+
+// ---- wavefront integrator: host side ------------------------------------------------------------
+// Paths per pass: as many whole samples of the frame as fit 4M paths (about 1 GB of state).
+constexpr uint32_t kWfMaxPaths = 1u << 22;
+
+// Bytes of wavefront state per path (each array 256-byte aligned in wf_carve).
+size_t wf_carve(unsigned char *base, uint32_t cap, WfArgs &W, uint32_t **q0, uint32_t **q1, uint32_t **counts,
+                uint8_t **occ, int4 **hit) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char *p = base ? base + off : nullptr;
+    off += (bytes + 255) & ~size_t(255);
+    return p;
+  };
+  const size_t n = cap;
+  W.T = reinterpret_cast<float4 *>(take(16 * n));
+  W.Rc = reinterpret_cast<float4 *>(take(16 * n));
+  W.Rp = reinterpret_cast<float4 *>(take(16 * n));
+  W.prev = reinterpret_cast<float4 *>(take(16 * n));
+  W.prevN = reinterpret_cast<float4 *>(take(16 * n));
+  W.seedA = reinterpret_cast<uint4 *>(take(16 * n));
+  W.seedB = reinterpret_cast<uint2 *>(take(8 * n));
+  W.meta = reinterpret_cast<uint4 *>(take(16 * n));
+  W.ray = reinterpret_cast<float4 *>(take(32 * n));
+  *hit = reinterpret_cast<int4 *>(take(16 * n));
+  W.sray = reinterpret_cast<float4 *>(take(32 * n));
+  W.scon = reinterpret_cast<float4 *>(take(16 * n));
+  *occ = reinterpret_cast<uint8_t *>(take(n));
+  *q0 = reinterpret_cast<uint32_t *>(take(4 * n));
+  *q1 = reinterpret_cast<uint32_t *>(take(4 * n));
+  W.shQ = reinterpret_cast<uint32_t *>(take(4 * n));
+  *counts = reinterpret_cast<uint32_t *>(take(64));
+  return off;
+}
+
+vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
+  if (p->sampling_mode == 0)
+    return vt_fail(ctx, VT_ERR_INVALID, "the wavefront integrator renders sampling modes 1-3 (ReSTIR DI frames use vt_render)");
+  {
+    const vt_status st = check_params(ctx, scene, p);
+    if (st != VT_OK) return st;
+  }
+  const vt_mesh *mesh = scene->mesh;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  {
+    const vt_status st = ensure_accum(ctx, scene, p);
+    if (st != VT_OK) return st;
+  }
+  if (spp == 0) return VT_OK;
+  if (spp > scene->jitter_cap) {
+    cudaFree(scene->d_jitter);
+    scene->d_jitter = nullptr;
+    VT_CUDA(ctx, cudaMalloc(&scene->d_jitter, spp * sizeof(float2)));
+    scene->jitter_cap = spp;
+  }
+  std::vector<float2> jit(spp);
+  for (uint32_t k = 0; k < spp; ++k) {
+    const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
+    jit[k] = make_float2(halton(n, 2) - 0.5f, halton(n, 3) - 0.5f);
+  }
+  VT_CUDA(ctx, cudaMemcpyAsync(scene->d_jitter, jit.data(), spp * sizeof(float2), cudaMemcpyHostToDevice, s));
+  if (mesh->nfaces == 0) { scene->samples += spp; return VT_OK; }
+
+  RenderArgs A;
+  fill_args(scene, p, spp, A);
+  A.jitter = scene->d_jitter;
+  A.status = ctx->d_status + 2;
+  A.kernelId = 7;
+  const uint32_t npix = A.OW * A.OH;
+  if (npix > kWfMaxPaths) return vt_fail(ctx, VT_ERR_LIMIT, "the wavefront integrator takes at most 4M pixels per frame");
+  const uint32_t chunk = std::max(1u, std::min(spp, kWfMaxPaths / npix));
+  const uint32_t cap = npix * chunk;
+  if (cap > scene->wf_cap) {
+    cudaFree(scene->d_wf);
+    scene->d_wf = nullptr;
+    scene->wf_cap = 0;
+    WfArgs probe;
+    uint32_t *a, *b, *c;
+    uint8_t *o;
+    int4 *h;
+    const size_t bytes = wf_carve(nullptr, cap, probe, &a, &b, &c, &o, &h);
+    VT_CUDA(ctx, cudaMalloc(&scene->d_wf, bytes));
+    scene->wf_cap = cap;
+  }
+  WfArgs W;
+  uint32_t *q[2], *counts;
+  uint8_t *occ;
+  int4 *hit;
+  wf_carve(scene->d_wf, scene->wf_cap, W, &q[0], &q[1], &counts, &occ, &hit);
+  W.hit = hit;
+  W.occ = occ;
+  W.npix = npix;
+  const bool pbr = A.pbr != nullptr;
+  const uint32_t gridMax = (uint32_t)ctx->sm_count * 8u;
+  uint32_t *slot = vt_queue_slot(ctx);
+  for (uint32_t k0 = 0; k0 < spp; k0 += chunk) {
+    const uint32_t P = npix * std::min(chunk, spp - k0);
+    W.paths = P;
+    W.k0 = k0;
+    const uint32_t grid = std::min<uint32_t>((P + kWfBlock - 1) / kWfBlock, gridMax);
+    k_wf_generate<<<grid, kWfBlock, 0, s>>>(A, W);
+    VT_CUDA(ctx, cudaGetLastError());
+    for (uint32_t b = 0; b <= A.maxDepth; ++b) {
+      // Live queue of bounce b (all paths at b = 0), the next bounce's queue and the shadow queue.
+      const uint32_t *inQ = b == 0 ? nullptr : q[b & 1u];
+      const uint32_t *inCount = b == 0 ? nullptr : counts + (b & 1u);
+      W.inQ = inQ;
+      W.inCount = inCount;
+      W.outQ = q[(b + 1) & 1u];
+      W.outCount = counts + ((b + 1) & 1u);
+      W.shCount = counts + 2;
+      VT_CUDA(ctx, cudaMemsetAsync(W.outCount, 0, sizeof(uint32_t), s));
+      VT_CUDA(ctx, cudaMemsetAsync(W.shCount, 0, sizeof(uint32_t), s));
+      vt_launch_closest(mesh, reinterpret_cast<const vt_ray *>(W.ray), P, reinterpret_cast<vt_hit *>(hit), ctx->sm_count,
+                        slot, inQ, ctx->d_status + 1, s, inCount, true);
+      if (pbr) k_wf_shade<true><<<grid, kWfBlock, 0, s>>>(A, W, b);
+      else k_wf_shade<false><<<grid, kWfBlock, 0, s>>>(A, W, b);
+      vt_launch_any(mesh, reinterpret_cast<const vt_ray *>(W.sray), P, occ, ctx->sm_count, slot, W.shQ, ctx->d_status + 1, s,
+                    W.shCount, A.imported != 0u);
+      VT_CUDA(ctx, cudaGetLastError());
+    }
+    k_wf_finish<<<grid, kWfBlock, 0, s>>>(A, W);
+    VT_CUDA(ctx, cudaGetLastError());
+  }
+  scene->samples += spp;
+  return VT_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -2236,6 +2681,12 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint
   if (!ctx) return VT_ERR_INVALID;
   if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
   return render_impl(ctx, scene, p, spp, stream, nullptr);
+}
+
+vt_status vt_render_wavefront(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !p) return vt_fail(ctx, VT_ERR_INVALID, "scene or params is null");
+  return wavefront_impl(ctx, scene, p, spp, stream);
 }
 
 vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_frame_params *p, uint32_t spp,
@@ -2578,6 +3029,10 @@ vt_status vt_accum_readback(vt_ctx *ctx, vt_scene *scene, double *rgb, uint32_t 
   {
     uint32_t w[16];
     VT_CUDA(ctx, cudaMemcpy(w, ctx->d_status, sizeof w, cudaMemcpyDeviceToHost));
+    if (w[1] & VT_DEV_STACK) {
+      VT_CUDA(ctx, cudaMemset(ctx->d_status + 1, 0, sizeof(uint32_t)));
+      return vt_fail(ctx, VT_ERR_DEVICE, "a traversal stack would have overflowed; the entries were dropped");
+    }
     if (w[2]) {
       VT_CUDA(ctx, cudaMemset(ctx->d_status + 2, 0, sizeof(uint32_t)));
       VT_CUDA(ctx, cudaMemset(ctx->d_status + 8, 0, 3 * sizeof(uint32_t)));

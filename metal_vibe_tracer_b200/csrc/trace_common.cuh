@@ -118,6 +118,16 @@ __device__ __forceinline__ bool intersect_tri(const WRay &r, float4 a, float4 b,
   return t >= tMin && t < tMax;
 }
 
+// mesh_hit_error (main.swift:1353-1355) of a triangle: its vertices' rounding bound. Shadow rays of
+// imported scenes end this far before each triangle's own endpoint (scene_occluded's slack,
+// main.swift:2066-2069), so the surface a light sample lies on does not occlude itself.
+__device__ __forceinline__ float tri_error_bound(float4 a, float4 b, float4 c) {
+  const float ma = fmaxf(fabsf(a.x), fmaxf(fabsf(a.y), fabsf(a.z)));
+  const float mb = fmaxf(fabsf(b.x), fmaxf(fabsf(b.y), fabsf(b.z)));
+  const float mc = fmaxf(fabsf(c.x), fmaxf(fabsf(c.y), fabsf(c.z)));
+  return fmaxf(1e-7f, 1.907349e-6f * fmaxf(ma, fmaxf(mb, mc)));
+}
+
 // Conservative slab ray (wide_ray, main.swift:1758-1763): origins shifted by the per-ray bound
 // e = 2^-23 (max|o| + rootMax) so traversal never culls a triangle the edge test would hit. An axis
 // the ray runs parallel to (|d| < 1e-8) gets the inverse +-1e30 instead of the reference's separate

@@ -164,13 +164,17 @@ __device__ __forceinline__ int *stack_slot(int *sstack, int d) { return sstack +
 // included, pushed far to near, so they pop near first) or one leaf's triangle tests. The warp runs
 // only the kind more of its lanes need this iteration; the others wait one iteration. A ray's own
 // order (LIFO over its stack) does not depend on the warp.
+// kPos: a hit reports the triangle's BVH position instead of its input face (the integrator's
+// hit record). count: when not null, the queue length on the device (at most n).
+template <bool kPos>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__restrict__ nodes,
                                                         const float4 *__restrict__ tris, float rootMax,
                                                         const float4 *__restrict__ rays, uint32_t n,
                                                         int4 *__restrict__ hits, uint32_t *counter,
                                                         const uint32_t *__restrict__ perm, int stackSize,
-                                                        uint32_t *status) {
+                                                        uint32_t *status, const uint32_t *__restrict__ count) {
   extern __shared__ int sstack[];
+  if (count) n = min(n, *count);
   int top = 0;  // 0: the lane holds no ray
   uint32_t rid = 0;
   RayState s;
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
         float t, b1, b2;
         if (!intersect_tri(s.wr, a, b, cc, s.tMin, closest, t, b1, b2)) continue;
-        closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w);
+        closest = t; hb1 = b1; hb2 = b2; prim = kPos ? first + q : __float_as_int(a.w);
       }
     } else {
       QNode nd;
@@ -229,13 +233,17 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_closest(const float4 *__
   }
 }
 
+// kSlack: each triangle's own rounding bound comes off tmax (the integrator's shadow rays in
+// imported scenes, scene_occluded main.swift:2066-2069). count: as k_closest's.
+template <bool kSlack>
 __global__ void __launch_bounds__(kBlock, kMinBlocks) k_any(const float4 *__restrict__ nodes,
                                                     const float4 *__restrict__ tris, float rootMax,
                                                     const float4 *__restrict__ rays, uint32_t n,
                                                     uint8_t *__restrict__ occ, uint32_t *counter,
                                                     const uint32_t *__restrict__ perm, int stackSize,
-                                                    uint32_t *status) {
+                                                    uint32_t *status, const uint32_t *__restrict__ count) {
   extern __shared__ int sstack[];
+  if (count) n = min(n, *count);
   int top = 0;
   uint32_t rid = 0;
   RayState s;
@@ -266,7 +274,8 @@ __global__ void __launch_bounds__(kBlock, kMinBlocks) k_any(const float4 *__rest
         const float4 *tp = tris + 3 * (size_t)(first + q);
         const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
         float t, b1, b2;
-        if (intersect_tri(s.wr, a, b, cc, s.tMin, s.tMax, t, b1, b2)) { hit = true; break; }
+        const float tMax = kSlack ? s.tMax - tri_error_bound(a, b, cc) : s.tMax;
+        if (intersect_tri(s.wr, a, b, cc, s.tMin, tMax, t, b1, b2)) { hit = true; break; }
       }
     } else {
       QNode nd;
@@ -398,31 +407,34 @@ template <typename K> void prepare(K kernel, size_t smem) {
 }  // namespace
 
 void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits, int sm_count,
-                       uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s) {
+                       uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s,
+                       const uint32_t *count, bool bvhPos) {
   if (n == 0) return;
   const int S = stack_entries(mesh->depth);
   const size_t smem = (size_t)S * kBlock * sizeof(int);
-  prepare(k_closest, smem);
+  auto kernel = bvhPos ? k_closest<true> : k_closest<false>;
+  prepare(kernel, smem);
   const uint32_t want = (n + kBlock - 1) / kBlock;
-  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_closest, smem) * sm_count));
+  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(kernel, smem) * sm_count));
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-  k_closest<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris,
-                                       mesh->root_max, reinterpret_cast<const float4 *>(rays), n,
-                                       reinterpret_cast<int4 *>(hits), counter, perm, S, status);
+  kernel<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris, mesh->root_max,
+                                    reinterpret_cast<const float4 *>(rays), n, reinterpret_cast<int4 *>(hits), counter,
+                                    perm, S, status, count);
 }
 
 void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t *occ, int sm_count,
-                   uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s) {
+                   uint32_t *counter, const uint32_t *perm, uint32_t *status, cudaStream_t s,
+                   const uint32_t *count, bool slack) {
   if (n == 0) return;
   const int S = stack_entries(mesh->depth);
   const size_t smem = (size_t)S * kBlock * sizeof(int);
-  prepare(k_any, smem);
+  auto kernel = slack ? k_any<true> : k_any<false>;
+  prepare(kernel, smem);
   const uint32_t want = (n + kBlock - 1) / kBlock;
-  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(k_any, smem) * sm_count));
+  const uint32_t grid = std::min<uint32_t>(want, (uint32_t)(resident_blocks(kernel, smem) * sm_count));
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-  k_any<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris,
-                                   mesh->root_max, reinterpret_cast<const float4 *>(rays), n, occ, counter, perm,
-                                   S, status);
+  kernel<<<grid, kBlock, smem, s>>>(reinterpret_cast<const float4 *>(mesh->d_qnodes), mesh->d_tris, mesh->root_max,
+                                    reinterpret_cast<const float4 *>(rays), n, occ, counter, perm, S, status, count);
 }
 
 void vt_launch_count(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, int closest,

@@ -119,6 +119,10 @@ struct vt_scene {
   float4 *d_ebasis = nullptr;
   float4 *d_di = nullptr;
   uint32_t di_width = 0, di_height = 0, di_frames = 0, di_parity = 0;
+  // Wavefront integrator (vt_render_wavefront): the paths' state, rays and queues, one allocation
+  // sized for wf_cap paths.
+  unsigned char *d_wf = nullptr;
+  uint32_t wf_cap = 0;
   float di_cam[14] = {};  // previous frame's camera: position, forward, right, up, aspect, fov scale
 };
 
@@ -191,12 +195,15 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
 // launch on stream s.
 // `status` receives VT_DEV_STACK if a traversal stack would overflow (it cannot for a tree within
 // the mesh's recorded depth; the check keeps a corrupted tree from writing out of bounds).
+// `count` (optional): the queue length on the device, at most n (the wavefront integrator's queues);
+// `bvhPos`: hits report BVH positions instead of input faces; `slack`: shadow rays end each
+// triangle's rounding bound early (imported scenes).
 void vt_launch_closest(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, vt_hit *hits,
                        int sm_count, uint32_t *counter, const uint32_t *perm, uint32_t *status,
-                       cudaStream_t s);
+                       cudaStream_t s, const uint32_t *count = nullptr, bool bvhPos = false);
 void vt_launch_any(const vt_mesh *mesh, const vt_ray *rays, uint32_t n, uint8_t *occ,
                    int sm_count, uint32_t *counter, const uint32_t *perm, uint32_t *status,
-                   cudaStream_t s);
+                   cudaStream_t s, const uint32_t *count = nullptr, bool slack = false);
 // Ray ordering for large batches: returns the device permutation (inside `scratch`, which must
 // hold vt_ray_order_words(n) words) or nullptr when the batch is traced in input order.
 size_t vt_ray_order_words(uint32_t n);

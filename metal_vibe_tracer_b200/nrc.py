@@ -7,7 +7,7 @@ Radiance Caching for Path Tracing") with the multiresolution hash encoding of Mu
 Queries are (n, 13) float32 rows in vt_nrc_input's order: position xyz, roughness, outgoing
 direction (theta / pi, phi / 2 pi + 1/2), shading normal (same), diffuse rgb, specular, the path's
 wavelength number u (spectral caches; 0 for rgb). Predictions and training targets are (n, 4): per
-hero wavelength its radiance times the lane's share (spectral caches), or rgb and 0.
+hero wavelength its radiance over the illuminant there (spectral caches), or rgb and 0.
 """
 from __future__ import annotations
 

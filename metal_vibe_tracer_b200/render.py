@@ -194,6 +194,12 @@ class Scene:
         _check(self.ctx.handle, _lib.load().vt_render(self.ctx.handle, self._p, C.byref(params), int(spp), stream),
                "vt_render")
 
+    def render_wavefront(self, params: FrameParams, spp: int, stream=None) -> None:
+        """The same frames through the wavefront integrator (vt_render_wavefront; sampling modes 1-3)."""
+        self.height, self.width = accum_shape(params)
+        _check(self.ctx.handle, _lib.load().vt_render_wavefront(self.ctx.handle, self._p, C.byref(params), int(spp),
+                                                                stream), "vt_render_wavefront")
+
     def reset(self) -> None:
         _check(self.ctx.handle, _lib.load().vt_accum_reset(self.ctx.handle, self._p), "vt_accum_reset")
 
