@@ -1,16 +1,15 @@
-// nrc.cu — the neural radiance cache's network: parameter initialisation, the fused inference
-// kernel, the fused training kernel (forward, relative-L2 loss, backward to the weights and to the
-// hash-grid entries) and Adam.
+// nrc.cu — the neural radiance cache's network: parameter initialisation, the fused training kernel
+// (forward, relative-L2 loss, backward to the weights and to the hash-grid entries), Adam and the
+// host API. Inference runs on the tcgen05 tensor cores (nrc_tc.cu).
 //
-// Both network kernels keep a 128-row tile per CTA (4 warps x 32 rows). Activations stay in
-// registers between layers: the fp32 accumulator fragment of m16n8k16 for two adjacent n-tiles is
-// the fp16 A fragment of the next layer's k-tile, so a layer is 64 mma.sync per warp and no shared
-// memory traffic. The training kernel also writes each layer's fp16 output to shared memory, where
-// the weight gradient dW = dZ^T H reads it (and dZ) through ldmatrix.trans; the data gradient
-// dH = dZ W reads W the same way. Rows are padded to 72 halves (144 B), which keeps the fragment
-// loads and stores free of bank conflicts.
+// The training kernel keeps a 128-row tile per CTA (4 warps x 32 rows) on the warp-level tensor path
+// (mma.sync m16n8k16; its backward pass reads every layer's activations and the weights transposed,
+// which the register fragments give directly). Activations stay in registers between layers: the
+// fp32 accumulator fragment for two adjacent n-tiles is the fp16 A fragment of the next layer's
+// k-tile. Each layer's fp16 output also goes to shared memory, where the weight gradient dW = dZ^T H
+// reads it (and dZ) through ldmatrix.trans; the data gradient dH = dZ W reads W the same way. Rows
+// are padded to 72 halves (144 B), which keeps the fragment loads and stores free of bank conflicts.
 #include <cmath>
-#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -21,8 +20,6 @@ namespace {
 using namespace vtd;
 
 constexpr int kLd = kNrcLd;
-constexpr int kInferRows = 256;  // inference rows per CTA (8 warps share the weights; 2 CTAs per SM)
-constexpr size_t kInferSmem = (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kInferRows * kLd) * sizeof(__half);
 constexpr size_t kTrainSmem =
     (size_t)(kNrcHidden * 64 * kLd + kNrcOutRows * kLd + kNrcTile * kLd * (kNrcHidden + 2)) * sizeof(__half);
 constexpr float kGradClip = 512.0f;  // per-output loss gradient bound before the loss scale (x 64 stays in fp16 range)
@@ -142,44 +139,6 @@ __device__ __forceinline__ void output_layer(const uint32_t (&a)[2][4][4], const
     const uint32_t b0 = *reinterpret_cast<const uint32_t *>(w), b1 = *reinterpret_cast<const uint32_t *>(w + 8);
     nrc_mma(o[0], a[0][kt], b0, b1);
     nrc_mma(o[1], a[1][kt], b0, b1);
-  }
-}
-
-// Inference on the legacy tensor path (mma.sync): out[row] = the four outputs for rows < n.
-// Persistent CTAs over 256-row tiles.
-__global__ void __launch_bounds__(kInferRows, 2) k_nrc_infer(NrcGrid G, const float *__restrict__ mlp,
-                                                        const NrcInput *__restrict__ in, uint32_t n,
-                                                        float4 *__restrict__ out) {
-  extern __shared__ __align__(16) __half sm[];
-  __half *W = sm, *Wo = W + kNrcHidden * 64 * kLd, *X = Wo + kNrcOutRows * kLd;
-  load_weights(mlp, W, Wo);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3, row0 = 32 * warp;
-  for (uint32_t base = blockIdx.x * kInferRows; base < n; base += gridDim.x * kInferRows) {
-    const uint32_t row = base + threadIdx.x;
-    NrcInput q;
-    if (row < n) {
-      q = in[row];
-    } else {
-      q.a = q.b = q.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    }
-    nrc_encode(G, q, X + threadIdx.x * kLd);
-    __syncthreads();
-    uint32_t a[2][4][4];
-    load_a(a, X, row0, lane);
-#pragma unroll 1
-    for (int l = 0; l < kNrcHidden; ++l) hidden_layer(a, W + l * 64 * kLd, g, t);
-    float o[2][4];
-    output_layer(a, Wo, g, t, o);
-    if (t < 2) {
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        const uint32_t r0 = base + row0 + 16 * mt + g, r1 = r0 + 8;
-        float *o0 = reinterpret_cast<float *>(out + r0) + 2 * t, *o1 = reinterpret_cast<float *>(out + r1) + 2 * t;
-        if (r0 < n) *reinterpret_cast<float2 *>(o0) = make_float2(o[mt][0], o[mt][1]);
-        if (r1 < n) *reinterpret_cast<float2 *>(o1) = make_float2(o[mt][2], o[mt][3]);
-      }
-    }
-    __syncthreads();  // X is rewritten by the next tile
   }
 }
 
@@ -516,13 +475,7 @@ vt_status vt_nrc_step(vt_ctx *ctx, vt_nrc *nrc, uint32_t cap, cudaStream_t s) {
 }
 
 vt_status vt_nrc_predict(vt_ctx *ctx, vt_nrc *nrc, const NrcInput *in, uint32_t n, float4 *out, cudaStream_t s) {
-  if (n == 0) return VT_OK;
-  if (!getenv("VT_NRC_MMA_SYNC")) return vt_nrc_infer_tc(ctx, nrc, in, n, out, s);
-  const uint32_t tiles = (n + kInferRows - 1) / kInferRows;
-  const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * 2u);
-  k_nrc_infer<<<grid, kInferRows, kInferSmem, s>>>(nrc->grid, nrc->d_p, in, n, out);
-  VT_CUDA(ctx, cudaGetLastError());
-  return VT_OK;
+  return vt_nrc_infer_tc(ctx, nrc, in, n, out, s);
 }
 
 extern "C" {
@@ -565,7 +518,6 @@ vt_status vt_nrc_create(vt_ctx *ctx, const vt_nrc_config *cfg, const float lo[3]
   static bool attrs = false;
   if (!attrs) {
     VT_CUDA(ctx, cudaFuncSetAttribute(k_nrc_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrainSmem));
-    VT_CUDA(ctx, cudaFuncSetAttribute(k_nrc_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem));
     attrs = true;
   }
   vt_nrc *n = new vt_nrc();
