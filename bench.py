@@ -233,9 +233,20 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
+    # The same images through the wavefront integrator.
+    for k in range(2):
+        scene.render_wavefront(params(1 + spp * k), spp, cs)
+    e0.record(stream)
+    for k in range(reps):
+        scene.render_wavefront(params(1 + spp * k), spp, cs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_wf = e0.elapsed_time(e1) / reps
     out = {"workload": "spectral Cornell box, 36 triangles, 256x256, 16 spp, depth 8, 4 hero wavelengths 380-780 nm, "
                        "MIS, FP64 accumulation", "ms_per_image": ms, "paths_per_s": W * H * spp / (ms / 1e3),
-           "gpu_launches_per_image": 1}
+           "gpu_launches_per_image": 1,
+           "wavefront": {"ms_per_image": ms_wf, "paths_per_s": W * H * spp / (ms_wf / 1e3),
+                         "gpu_launches_per_image": 2 + 3 * (depth + 1)}}
     # FP64 reference: reference_spp samples from independent sample indices.
     ref_scene = vt.Scene(ctx, mesh, mats, light, tables)
     chunk = 1024
@@ -465,7 +476,7 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
     cs = stream.cuda_stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    # The FP64 reference: MIS, strided, resumable.
+    # The FP64 reference: MIS through the wavefront integrator, strided, resumable.
     ref_scene = vt.Scene(ctx, mesh, mats, None, tables)
     done = 0
     if a.c5_ref_file and Path(a.c5_ref_file).exists():
@@ -475,7 +486,7 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
     while done < a.c5_ref_spp:
         n = min(chunk, a.c5_ref_spp - done)
         params = vt.make_params(cam, W, H, depth, done + 1, True, 1, pixel_stride=S)
-        ref_scene.render(params, n, cs)
+        ref_scene.render_wavefront(params, n, cs)
         done += n
         if a.c5_ref_file and (done % 8192 == 0 or done >= a.c5_ref_spp):
             torch.cuda.synchronize()
@@ -490,8 +501,9 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
 
     scene = vt.Scene(ctx, mesh, mats, None, tables)
 
-    def arm(mode, cand, cache=None, per=1):
-        """Frames of `per` spp until relMSE <= 1e-3 or the time cap: (device s, spp, relMSE)."""
+    def arm(mode, cand, cache=None, per=1, wavefront=False):
+        """Frames of `per` spp until relMSE <= 1e-3 or the time cap: (device s, spp, relMSE). Plain path
+        tracing runs the wavefront integrator (the cache's MIS arm renders through it as well)."""
         scene.reset()
         total, spp_done, err = 0.0, 0, None
         if cache is not None:
@@ -509,6 +521,8 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
                 params = vt.make_params(cam, W, H, depth, 1 + spp_done, True, mode, di_candidates=cand)
                 if cache is not None:
                     cache.render(scene, params, per, stream=cs)
+                elif wavefront:
+                    scene.render_wavefront(params, per, cs)
                 else:
                     scene.render(params, per, cs)
                 spp_done += per
@@ -532,10 +546,11 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
                          "untimed"}
     # One untimed frame of each kernel family first (module loads).
     scene.render(vt.make_params(cam, 64, 64, depth, 1, True, 1), 1, cs)
+    scene.render_wavefront(vt.make_params(cam, 64, 64, depth, 1, True, 1), 1, cs)
     scene.render(vt.make_params(cam, 64, 64, depth, 1, True, 0, di_candidates=32), 1, cs)
     torch.cuda.synchronize()
     for name, mode, cand in (("plain_pt", 1, 0), ("restir_di", 0, 32)):
-        t, n, err = arm(mode, cand)
+        t, n, err = arm(mode, cand, wavefront=mode == 1)
         r = {"s": t, "spp": n, "relmse": err, "ms_per_spp": 1e3 * t / max(n, 1), "reached": err is not None and err <= 1e-3}
         if not r["reached"] and err:
             r["extrapolated_s"] = t * err / 1e-3

@@ -545,7 +545,9 @@ vt_status vt_nrc_train(vt_ctx *ctx, vt_nrc *nrc, const vt_nrc_input *in, const f
  * trace the frame's training paths (MIS, full depth) and take one optimiser step on their records
  * first; VT_NRC_RENDER: render spp samples per pixel whose paths end where the cache's query rule
  * (query_vertex, spread) stops them, with the cache's prediction (sampling modes 0 and 1), added to
- * the scene's accumulation. The frame's transport must match the cache's `spectral` setting. */
+ * the scene's accumulation; sampling mode 1 renders through the wavefront integrator
+ * (vt_render_wavefront's stages), mode 0 through ReSTIR DI's two passes. The frame's transport must
+ * match the cache's `spectral` setting. */
 vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_frame_params *p, uint32_t spp,
                         uint32_t flags, void *stream);
 

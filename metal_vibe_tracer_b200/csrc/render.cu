@@ -1407,7 +1407,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
 // entries land contiguously. k_wf_finish adds each path's radiance (primary NEE + continuation,
 // summed in k_render's order) to its pixel's FP64 accumulation.
 constexpr int kWfBlock = 256;
-constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u;
+constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u, kWfQueried = 16u;
 
 struct WfArgs {
   float4 *T;      // throughput per lane
@@ -1418,6 +1418,7 @@ struct WfArgs {
   uint4 *seedA;   // sampler: state, key, dimension, sub
   uint2 *seedB;   // sampler: subBits, z
   uint4 *meta;    // pixel, bounce, scattering, flags
+  float2 *spread; // the cache's termination: the path's spread so far, its limit (nrc_spread_limit)
   float4 *ray;    // the path's next ray (vt_ray: origin, tmin; direction, tmax)
   const int4 *hit;  // its closest hit (t, b1, b2 bits; BVH position or -1)
   float4 *sray;   // the NEE sample's shadow ray (vt_ray)
@@ -1428,6 +1429,8 @@ struct WfArgs {
   uint32_t *shQ, *shCount;        // shadow rays of this bounce
   uint32_t npix, paths, k0;       // accumulation pixels; paths of the pass; its first sample (of the call)
 };
+// The cache's query slot of path i: sample k0 + i / npix of pixel i % npix (k_render's slots).
+__device__ __forceinline__ size_t wf_slot(const WfArgs &W, uint32_t i) { return (size_t)W.k0 * W.npix + i; }
 
 __device__ __forceinline__ void wf_store_seed(const WfArgs &W, uint32_t i, const Sampler &s) {
   W.seedA[i] = make_uint4(s.state, s.key, s.dimension, s.sub);
@@ -1481,8 +1484,9 @@ __device__ __forceinline__ bool wf_nee(const RenderArgs &A, const WfArgs &W, uin
 }
 
 // One vertex of path i at bounce b (0: the primary hit). Sets `next` when the path continues and
-// `shadow` when it queued a shadow ray.
-template <bool kPbr>
+// `shadow` when it queued a shadow ray. kNrc: the path ends with a cache query where continue_path's
+// query rule stops it (vt_render_nrc).
+template <bool kPbr, bool kNrc>
 __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, uint32_t i, uint32_t b, bool &next,
                                           bool &shadow) {
   uint4 meta = W.meta[i];
@@ -1529,6 +1533,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         alive = false;
       } else {
         T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        if (kNrc) W.spread[i] = make_float2(0.0f, nrc_spread_limit(A, h.t, S.gn, dir));
         if (A.mode != 3u) {
           sampler_event(seed, 1u, kZNee);
           if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, A.mode == 1u && limit > 0, seed, true)) {
@@ -1556,6 +1561,12 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
       const float3 prevPos = f3(pv.x, pv.y, pv.z);
       S = surface_at(A, h, o, dir);
       m = material(A, S.slot);
+      float2 sp = make_float2(0.0f, 0.0f);
+      if (kNrc) {
+        sp = W.spread[i];
+        sp.x += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
+        W.spread[i] = sp;
+      }
       if (m.type == VT_MAT_EMISSIVE) {
         const float lpdf = A.imported ? emitter_pdf(A, prevPos, S.pos, S.face) : light_pdf(A, prevPos, S.pos);
         const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
@@ -1565,6 +1576,10 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         }
         alive = false;
       } else if (emissionOnly) {
+        alive = false;
+      } else if (kNrc && (A.nrcVertex ? b >= A.nrcVertex : sp.x * sp.x > sp.y)) {
+        nrc_store(A, wf_slot(W, i), nrc_query<kPbr>(A, L, S, m, dir), L, T);
+        flags |= kWfQueried;
         alive = false;
       } else {
         if (nee) {
@@ -1648,7 +1663,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(RenderArgs A, WfArgs W
   }
 }
 
-template <bool kPbr>
+template <bool kPbr, bool kNrc>
 __global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, uint32_t bounce) {
   __shared__ uint32_t sTotal, sBase;
   const uint32_t n = W.inCount ? min(*W.inCount, W.paths) : W.paths;
@@ -1658,7 +1673,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, u
     uint32_t i = 0;
     if (q < n) {
       i = W.inQ ? W.inQ[q] : q;
-      wf_vertex<kPbr>(A, W, i, bounce, next, shadow);
+      wf_vertex<kPbr, kNrc>(A, W, i, bounce, next, shadow);
     }
     wf_push(next, i, W.outQ, W.outCount, sTotal, sBase);
     wf_push(shadow, i, W.shQ, W.shCount, sTotal, sBase);
@@ -1666,10 +1681,13 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, u
 }
 
 // Each path's radiance (its last shadow result first) into its pixel's FP64 sum: primary NEE plus
-// continuation, in k_render's order, non-finite sums dropped.
+// continuation, in k_render's order, non-finite sums dropped. kNrc: a path without a query clears its
+// slot's throughput (the resolve skips it).
+template <bool kNrc>
 __global__ void __launch_bounds__(kWfBlock) k_wf_finish(RenderArgs A, WfArgs W) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < W.paths; i += gridDim.x * blockDim.x) {
     const uint4 meta = W.meta[i];
+    if (kNrc && !(meta.w & kWfQueried)) nrc_store_none(A, wf_slot(W, i));
     float4 Rc = W.Rc[i], Rp = W.Rp[i];
     if ((meta.w & kWfShadow) && !W.occ[i]) {
       const float4 c = W.scon[i];
@@ -2568,6 +2586,7 @@ size_t wf_carve(unsigned char *base, uint32_t cap, WfArgs &W, uint32_t **q0, uin
   W.seedA = reinterpret_cast<uint4 *>(take(16 * n));
   W.seedB = reinterpret_cast<uint2 *>(take(8 * n));
   W.meta = reinterpret_cast<uint4 *>(take(16 * n));
+  W.spread = reinterpret_cast<float2 *>(take(8 * n));
   W.ray = reinterpret_cast<float4 *>(take(32 * n));
   *hit = reinterpret_cast<int4 *>(take(16 * n));
   W.sray = reinterpret_cast<float4 *>(take(32 * n));
@@ -2580,7 +2599,12 @@ size_t wf_carve(unsigned char *base, uint32_t cap, WfArgs &W, uint32_t **q0, uin
   return off;
 }
 
-vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream) {
+vt_status nrc_finish(vt_ctx *ctx, vt_nrc *nrc, const RenderArgs &A, uint32_t spp, cudaStream_t s);
+
+// vt_render_wavefront, and with a cache (nrc not null, sampling mode 1) vt_render_nrc's rendering:
+// paths ending where the cache's query rule stops them, then the predictions and the resolve.
+vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream,
+                         vt_nrc *nrc = nullptr) {
   if (p->sampling_mode == 0)
     return vt_fail(ctx, VT_ERR_INVALID, "the wavefront integrator renders sampling modes 1-3 (ReSTIR DI frames use vt_render)");
   {
@@ -2616,6 +2640,15 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
   A.kernelId = 7;
   const uint32_t npix = A.OW * A.OH;
   if (npix > kWfMaxPaths) return vt_fail(ctx, VT_ERR_LIMIT, "the wavefront integrator takes at most 4M pixels per frame");
+  if (nrc) {
+    const vt_status st = vt_nrc_reserve_queries(ctx, nrc, (size_t)npix * spp);
+    if (st != VT_OK) return st;
+    A.nrcIn = nrc->d_q;
+    A.nrcT = nrc->d_qT;
+    A.nrcBins = nrc->d_qbins;
+    A.nrcVertex = nrc->cfg.query_vertex;
+    A.nrcSpread = nrc->cfg.spread;
+  }
   const uint32_t chunk = std::max(1u, std::min(spp, kWfMaxPaths / npix));
   const uint32_t cap = npix * chunk;
   if (cap > scene->wf_cap) {
@@ -2661,14 +2694,24 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
       VT_CUDA(ctx, cudaMemsetAsync(W.shCount, 0, sizeof(uint32_t), s));
       vt_launch_closest(mesh, reinterpret_cast<const vt_ray *>(W.ray), P, reinterpret_cast<vt_hit *>(hit), ctx->sm_count,
                         slot, inQ, ctx->d_status + 1, s, inCount, true);
-      if (pbr) k_wf_shade<true><<<grid, kWfBlock, 0, s>>>(A, W, b);
-      else k_wf_shade<false><<<grid, kWfBlock, 0, s>>>(A, W, b);
+      if (nrc) {
+        if (pbr) k_wf_shade<true, true><<<grid, kWfBlock, 0, s>>>(A, W, b);
+        else k_wf_shade<false, true><<<grid, kWfBlock, 0, s>>>(A, W, b);
+      } else {
+        if (pbr) k_wf_shade<true, false><<<grid, kWfBlock, 0, s>>>(A, W, b);
+        else k_wf_shade<false, false><<<grid, kWfBlock, 0, s>>>(A, W, b);
+      }
       vt_launch_any(mesh, reinterpret_cast<const vt_ray *>(W.sray), P, occ, ctx->sm_count, slot, W.shQ, ctx->d_status + 1, s,
                     W.shCount, A.imported != 0u);
       VT_CUDA(ctx, cudaGetLastError());
     }
-    k_wf_finish<<<grid, kWfBlock, 0, s>>>(A, W);
+    if (nrc) k_wf_finish<true><<<grid, kWfBlock, 0, s>>>(A, W);
+    else k_wf_finish<false><<<grid, kWfBlock, 0, s>>>(A, W);
     VT_CUDA(ctx, cudaGetLastError());
+  }
+  if (nrc) {
+    const vt_status st = nrc_finish(ctx, nrc, A, spp, s);
+    if (st != VT_OK) return st;
   }
   scene->samples += spp;
   return VT_OK;
@@ -2757,7 +2800,9 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
     }
   }
   if (flags & VT_NRC_RENDER) {
-    const vt_status st = render_impl(ctx, scene, p, spp, stream, nrc);
+    // MIS primaries through the wavefront integrator; ReSTIR DI's frames through its two passes.
+    const vt_status st = p->sampling_mode == 1u ? wavefront_impl(ctx, scene, p, spp, stream, nrc)
+                                                : render_impl(ctx, scene, p, spp, stream, nrc);
     if (both) {
       VT_CUDA(ctx, cudaEventRecord(nrc->ev_paths, nrc->side));
       VT_CUDA(ctx, cudaStreamWaitEvent(s, nrc->ev_paths, 0));
