@@ -63,11 +63,15 @@ def parse():
                    help="after the training frames, the cache trains on every n-th rendered frame")
     p.add_argument("--nrc-levels", type=int, default=8,
                    help="hash-grid levels of the radiance cache (8 reach the same spp at relMSE 1e-3 on the Cornell box as 16, in cheaper frames)")
+    p.add_argument("--production-size", default="1920x1080", help="production scene's frame size (profiling runs)")
+    p.add_argument("--production-arms", default="restir_di_32,mis,mis_wavefront",
+                   help="production scene's measured arms (profiling runs)")
     p.add_argument("--c5", type=int, default=1, help="1: measure config C5 (the cache on the production scene)")
     p.add_argument("--c5-stride", type=int, default=8, help="pixel stride of C5's FP64 reference and relMSE")
     p.add_argument("--c5-ref-spp", type=int, default=65536, help="spp of C5's FP64 reference")
     p.add_argument("--c5-ref-file", default="", help="resume/save C5's reference accumulation (.npz)")
-    p.add_argument("--c5-max-s", type=float, default=60.0, help="device-time cap per C5 arm, seconds")
+    p.add_argument("--c5-max-s", type=float, default=20.0, help="device-time cap per C5 arm, seconds")
+    p.add_argument("--c5-train-every", type=int, default=1, help="C5's cache trains on every n-th rendered frame")
     p.add_argument("--c5-check", type=int, default=16, help="spp between C5's relMSE checks")
     p.add_argument("--c5-pretrain", type=int, default=32, help="training-only frames of C5's cache, timed")
     p.add_argument("--nrc-records", type=int, default=16384,
@@ -418,15 +422,18 @@ def bench_production(a, ctx, stream) -> dict:
     t0 = time.perf_counter()
     scene = vt.Scene(ctx, mesh, mats, None, tables)
     scene_s = time.perf_counter() - t0
-    W, H, depth = 1920, 1080, 12
+    W, H = (int(v) for v in a.production_size.split("x"))
+    depth = 12
     cs = stream.cuda_stream
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"workload": "production grid scene: %d triangles (displaced subdivision-5 icospheres), %d emissive under a "
                        "light tree, %d material slots (OPENPBR: base colour, roughness, metalness, IOR; spectral uplift), "
-                       "1920x1080, 4 wavelengths, depth 12" % (len(faces), int((faces["tag"] >= 287).sum()), len(mats)),
+                       "%dx%d, 4 wavelengths, depth 12" % (len(faces), int((faces["tag"] >= 287).sum()), len(mats), W, H),
            "triangles": int(len(faces)), "build_ms": info.build_ms, "scene_create_s": scene_s, "generate_s": gen_s}
     for name, mode, cand, wavefront in (("restir_di_32", 0, 32, False), ("mis", 1, 0, False),
                                         ("mis_wavefront", 1, 0, True)):
+        if name not in a.production_arms.split(","):
+            continue
         scene.reset()
         frame = 0
         render = scene.render_wavefront if wavefront else scene.render
@@ -515,12 +522,14 @@ def bench_nrc_c5(a, ctx, stream) -> dict:
             torch.cuda.synchronize()
             total = e0.elapsed_time(e1) / 1e3
         next_check = a.c5_check
+        frames = 0
         while total < a.c5_max_s:
             e0.record(stream)
             while spp_done < next_check:
                 params = vt.make_params(cam, W, H, depth, 1 + spp_done, True, mode, di_candidates=cand)
                 if cache is not None:
-                    cache.render(scene, params, per, stream=cs)
+                    cache.render(scene, params, per, train=frames % max(1, a.c5_train_every) == 0, stream=cs)
+                    frames += 1
                 elif wavefront:
                     scene.render_wavefront(params, per, cs)
                 else:
@@ -599,16 +608,17 @@ def profile_nrc(a) -> int:
 
 
 def profile_production(a) -> int:
-    """The production scene's frames for an ncu launch list: 2 warm-up and `--production-frames`
-    timed frames each of ReSTIR DI (32 candidates) and MIS, as the bench times them, then exit."""
+    """The production scene's frames for ncu: 2 warm-up and `--production-frames` timed frames of each
+    arm in `--production-arms` (ReSTIR DI with 32 candidates, the MIS megakernel, the MIS wavefront
+    integrator) at `--production-size`, as the bench times them, then exit."""
     import torch
 
     import metal_vibe_tracer_b200 as vt
     ctx = vt.Context(0)
     stream = torch.cuda.Stream()
     out = bench_production(a, ctx, stream)
-    print(json.dumps({"profile_production": "ok", "restir_di_32_ms": out["restir_di_32"]["ms_per_frame"],
-                      "mis_ms": out["mis"]["ms_per_frame"]}))
+    print(json.dumps({"profile_production": "ok", **{k: v["ms_per_frame"] for k, v in out.items()
+                                                     if isinstance(v, dict) and "ms_per_frame" in v}}))
     return 0
 
 
