@@ -262,6 +262,10 @@ vt_status vt_accum_restore(vt_ctx *ctx, vt_scene *scene, uint32_t width, uint32_
  * height * 4). M counts the frame's candidates plus the confidence merged from the previous frame
  * (capped at 20, restir_di_merge, main.swift:4686-4699). vt_accum_reset clears the history. */
 vt_status vt_scene_di_weights(vt_ctx *ctx, const vt_scene *scene, float *out, uint32_t n);
+/* The same for the ReSTIR GI reservoirs of the last mode-0 frame (restir_gi_encode, main.swift:
+ * 4797-4806): per pixel (weight sum, M, W, wavelength number); M 0 where no GI reservoir was built
+ * (non-diffuse primaries, depth 1). */
+vt_status vt_scene_gi_weights(vt_ctx *ctx, const vt_scene *scene, float *out, uint32_t n);
 
 /* Per pixel the first draws of one sampling event (vertex, stream) of the pixel's sampler: rand_f,
  * rand_f2 and rand_f3, 6 floats per pixel into the HOST array `out` (width * height * 6). The

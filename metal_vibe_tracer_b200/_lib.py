@@ -150,6 +150,7 @@ SIGNATURES = {
     "vt_scene_emitter_words": (_I32, [_P, _P, _P, _U32, C.POINTER(_U32)]),
     "vt_light_estimate": (_I32, [_P, _P, _P, _U32, _U32, _U32, _P]),
     "vt_scene_di_weights": (_I32, [_P, _P, _P, _U32]),
+    "vt_scene_gi_weights": (_I32, [_P, _P, _P, _U32]),
     "vt_batch_create": (_I32, [_P, _P, _P, _P, _U32, C.POINTER(_P)]),
     "vt_batch_render": (_I32, [_P, _P, _P]),
     "vt_batch_stats": (_I32, [_P, _P, C.POINTER(BatchStats), _P, _U32]),

@@ -96,6 +96,11 @@ struct RenderArgs {
   float4 *gGeo;                  // geometric normal (the shading normal is in gNrm)
   float4 *rPos, *rEmit, *rW;     // (position, light id bits), (emission, pdf), (weight sum, M, W, u)
   const float4 *hPos, *hNrm, *hrPos, *hrEmit, *hrW;
+  // ReSTIR GI (sampling mode 0, diffuse primaries): per pixel the secondary point and its source pdf,
+  // its normal and a validity flag, its outgoing direct radiance per lane, (weight sum, M, W, u); this
+  // frame's and the previous frame's.
+  float4 *giPos, *giNrm, *giRad, *giW;
+  const float4 *hgiPos, *hgiNrm, *hgiRad, *hgiW;
   float3 pcam, pfwd, pright, pup;
   float paspect, pfovScale;
   // Radiance cache (vt_render_nrc): per (sample, pixel) slot the query at vertex nrcVertex, the
@@ -1111,6 +1116,9 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
   int scattering = 0;
   bool emissionOnly = false;
   float spread = 0.0f;  // sum of the vertices' sqrt(d^2 / (p |cos|)) (kNrc)
+  // ReSTIR GI's reservoir estimates the direct light of the secondary diffuse vertex of a path whose
+  // diffuse primary took ReSTIR DI, so that vertex skips NEE (restirGISecondary, main.swift:7801-7803).
+  const bool giPrimary = diPrimary && !kNrc && m.type == VT_MAT_DIFFUSE;
   for (int bounce = 1;; ++bounce) {
     if (scattering >= limit) {
       // BSDF-only paths take one final continuation that may only reach emission.
@@ -1166,7 +1174,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       *queried = true;
       break;
     }
-    if (nee) {
+    if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
       R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
                               seed, stack, false));
@@ -1219,11 +1227,149 @@ __device__ float3 path_sample(const RenderArgs &A, uint32_t x, uint32_t y, uint3
   return c;
 }
 
-// ReSTIR DI pass 1 for frame k (restir_temporal_kernel, main.swift:4842-4960): the primary hit into
-// the primary-surface cache, then at a diffuse hit the initial reservoir (RIS over the frame's
-// candidates, restir_di_initial, main.swift:4638-4668), merged with the previous frame's reservoir
-// of the backprojected pixel when it saw the same surface (restir_di_merge, main.swift:4686-4699,
-// confidence capped at 20), stored with W = wsum / (M p_hat) (restir_di_encode).
+// ---- ReSTIR GI (sampling mode 0): the first indirect diffuse vertex ------------------------------
+// The reference's ReSTIR GI (RESTIRGI2021 in its REFERENCES.md): at a diffuse primary vertex x1, one
+// BSDF sample to a diffuse secondary vertex x2 and one NEE sample there give a reservoir holding x2,
+// its normal and its outgoing direct radiance (restir_gi_initial, main.swift:4718-4770), merged with
+// the previous frame's reservoir of the backprojected pixel (restir_gi_merge, :4775-4795) and, in
+// pass 2, with four compatible neighbours (:7582-7649); the reconnection x1 -> x2 is shaded with the
+// reservoir's weight when visible (:7650-7656). The path's own continuation then skips NEE at its
+// secondary diffuse vertex (main.swift:7801-7803), whose direct light the reservoir estimates.
+struct GISample {
+  float3 pos, nrm;  // x2 and its shading normal
+  float4 rad;       // x2's outgoing direct radiance toward x1 per lane (rgb in RGB transport)
+  float pdf, u;     // source pdf of x2 in area measure; the wavelength number the radiance was traced at
+};
+
+// gi_geometry (main.swift:3201-3207).
+__device__ __forceinline__ float gi_geometry(float3 x1, float3 n1, float3 x2, float3 n2) {
+  const float3 delta = sub(x2, x1);
+  const float d2 = dot3(delta, delta);
+  if (d2 < 1e-10f) return 0.0f;
+  const float3 dir = mul(delta, rsqrtf(d2));
+  return fmaxf(0.0f, dot3(n1, dir)) * fmaxf(0.0f, -dot3(n2, dir)) / d2;
+}
+// restir_gi_jacobian / restir_gi_accepts_shift (main.swift:3213-3226): the reconnection's solid-angle
+// Jacobian must lie in [0.1, 10].
+__device__ __forceinline__ bool gi_accepts_shift(float3 x1r, float3 x1q, float3 x2, float3 n2) {
+  const float3 cur = sub(x1r, x2), src = sub(x1q, x2);
+  const float cd2 = dot3(cur, cur), sd2 = dot3(src, src);
+  if (cd2 < 1e-10f || sd2 < 1e-10f) return false;
+  const float cc = fmaxf(0.0f, dot3(n2, mul(cur, rsqrtf(cd2)))), sc = fmaxf(0.0f, dot3(n2, mul(src, rsqrtf(sd2))));
+  float j = cc * sd2 / (sc * cd2);
+  if (!isfinite(j)) j = 0.0f;
+  return j >= 0.1f && j <= 10.0f;
+}
+// eval_bsdf_with_pdf for DIFFUSE (main.swift:2659-2676) as direct_light evaluates it: f = 1 / pi and
+// the cosine pdf from the shading normal, no light below the geometric surface.
+__device__ __forceinline__ float lambert_eval(float3 n, float3 gn, float3 wo, float3 wi, float &pdf) {
+  const float ni = dot3(n, wi), no = dot3(n, wo);
+  pdf = 0.0f;
+  if (!(no > 0.0f)) return 0.0f;
+  pdf = fmaxf(0.0f, ni) * kInvPi;
+  return ni > 0.0f && fabsf(ni) >= 1e-7f && dot3(wi, gn) > 0.0f ? kInvPi : 0.0f;
+}
+// eval_restir_gi_target (main.swift:3230-3236) at a diffuse x1: |rgb(f(x1 -> x2) L2 G)| in the
+// sample's own wavelengths.
+__device__ __forceinline__ float gi_target(const RenderArgs &A, float3 x1, float3 n1, float3 gn1, float3 rayDir,
+                                           const vt_material &m, const GISample &c) {
+  const float geometry = gi_geometry(x1, n1, c.pos, c.nrm);
+  if (geometry <= 0.0f || !isfinite(c.rad.x) || !isfinite(c.rad.y) || !isfinite(c.rad.z) || !isfinite(c.rad.w))
+    return 0.0f;
+  const float3 dir = normalize3(sub(c.pos, x1));
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, c.u);
+  float pdf;
+  const float f = lambert_eval(n1, gn1, mul(rayDir, -1.0f), dir, pdf);
+  const float3 v = to_rgb(A, L, scale4(mul4(reflectance(A, L, m), c.rad), f * geometry));
+  return sqrtf(dot3(v, v));
+}
+// gi_connection_visible (main.swift:3238-3252): x1 sees x2 (the endpoint tolerance at x2).
+__device__ __forceinline__ bool gi_visible(const RenderArgs &A, float3 x1, float3 n1, float3 x2, float err, int *stack) {
+  float3 delta = sub(x2, x1);
+  const float dist = sqrtf(dot3(delta, delta));
+  if (dist <= 2.0f * ray_eps(A, x1)) return false;
+  const float3 o = ray_origin(A, x1, n1, mul(delta, 1.0f / dist), err);
+  const float3 e = sub(x2, o);
+  const float d = sqrtf(dot3(e, e));
+  const float legacy = 2.0f * ray_eps(A, x2);
+  const float tol = A.imported ? fmaxf(legacy, 1.907349e-6f * (max_abs(o) + max_abs(x2) + d)) : legacy;
+  return !rt_any(A, o, mul(e, 1.0f / d), ray_tmin(A, o), d - tol, stack, A.imported != 0u);
+}
+__device__ __forceinline__ GISample gi_load(const float4 *pos, const float4 *nrm, const float4 *rad, const float4 *w,
+                                            uint32_t j) {
+  GISample s;
+  const float4 p = pos[j], n = nrm[j];
+  s.pos = f3(p.x, p.y, p.z);
+  s.pdf = p.w;
+  s.nrm = f3(n.x, n.y, n.z);
+  s.rad = rad[j];
+  s.u = w[j].w;
+  return s;
+}
+
+// restir_gi_initial (main.swift:4718-4770) at the diffuse primary vertex S (material m), seen along
+// view: (reservoir sample, weight sum); M is 1.
+__device__ GISample gi_initial(const RenderArgs &A, const Surface &S, const vt_material &m, float3 view, float u,
+                               Sampler &seed, int *stack, float &wsum) {
+  GISample r;
+  r.pos = r.nrm = f3(0.0f, 0.0f, 0.0f);
+  r.rad = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  r.pdf = 0.0f;
+  r.u = u;
+  wsum = 0.0f;
+  const int limit = max(0, (int)A.maxDepth - 1);
+  sampler_event(seed, 1u, kZGiBsdf);
+  const float3 rr = rand_f3(seed);  // sample_bsdf's Lambert branch: the direction from the last two
+  const float3 gd = cosine_hemisphere(S.n, rr.y, rr.z);
+  const float bpdf = fmaxf(0.0f, dot3(S.n, gd)) * kInvPi;
+  if (!(bpdf > 0.0f) || !(dot3(gd, S.gn) > 0.0f)) return r;
+  const float3 o = ray_origin(A, S.pos, S.gn, gd, S.err);
+  Hit h;
+  if (!rt_closest(A, o, gd, ray_tmin(A, o), __int_as_float(0x7f800000), h, stack)) return r;
+  const Surface S2 = surface_at(A, h, o, gd);
+  const vt_material m2 = material(A, S2.slot);
+  if (m2.type != VT_MAT_DIFFUSE) return r;
+  Lanes L;
+  if (A.spectral) L = make_lanes(A, u);
+  float4 rad = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  sampler_event(seed, 2u, kZGiNee);
+  const LightSample ls = sample_direct(A, S2.pos, S2.n, seed);
+  if (ls.pdf > 0.0f && light_visible(A, S2.pos, S2.gn, S2.err, ls, stack)) {
+    const float c2 = fmaxf(0.0f, dot3(S2.n, ls.wi));
+    float pdf2;
+    const float f2 = lambert_eval(S2.n, S2.gn, mul(gd, -1.0f), ls.wi, pdf2);
+    // The power heuristic only when a second continuation can sample x2's BSDF
+    // (restir_gi_has_complementary_bsdf, main.swift:3482-3484).
+    const float mis = limit >= 2 ? power_heuristic(ls.pdf, pdf2) : 1.0f;
+    const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
+    rad = scale4(mul4(reflectance(A, L, m2), emission(A, L, le)), f2 * c2 * mis / ls.pdf);
+  }
+  const float3 delta = sub(S2.pos, S.pos);
+  const float d2 = dot3(delta, delta);
+  const float cos2 = fmaxf(0.0f, -dot3(S2.n, gd));
+  const float srcPdf = d2 > 1e-10f ? bpdf * cos2 / d2 : 0.0f;
+  GISample c;
+  c.pos = S2.pos;
+  c.nrm = S2.n;
+  c.rad = rad;
+  c.pdf = srcPdf;
+  c.u = u;
+  const float pHat = gi_target(A, S.pos, S.n, S.gn, view, m, c);
+  if (srcPdf > 0.0f && pHat > 0.0f) {
+    r = c;
+    wsum = pHat / srcPdf;
+  }
+  return r;
+}
+
+// ReSTIR DI pass 1 for frame k (restir_temporal_kernel, main.swift:4842-5005): the primary hit into
+// the primary-surface cache, then at a diffuse (Lambert) hit the initial reservoir (RIS over the
+// frame's candidates, restir_di_initial, main.swift:4638-4668), merged with the previous frame's
+// reservoir of the backprojected pixel when it saw the same surface (restir_di_merge, main.swift:
+// 4686-4699, confidence capped at 20), stored with W = wsum / (M p_hat) (restir_di_encode); then,
+// with a scattering budget, the ReSTIR GI reservoir the same way (restir_gi_initial / _merge /
+// _encode). Other primaries get empty reservoirs and shade with NEE in pass 2 (main.swift:4931-4943).
 template <bool kPbr>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(RenderArgs A, uint32_t k) {
   int stack[kRenderStack];
@@ -1240,6 +1386,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
     A.gPos[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     A.gNrm[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
+    A.giPos[i] = zero; A.giNrm[i] = zero; A.giRad[i] = zero; A.giW[i] = zero;
     return;
   }
   const Surface S = surface_at(A, h, o0, dir0);
@@ -1249,8 +1396,9 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
   A.gNrm[i] = gn;
   A.gGeo[i] = make_float4(S.gn.x, S.gn.y, S.gn.z, 0.0f);
   A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
-  if (m.type != VT_MAT_DIFFUSE && !is_pbr<kPbr>(A, m)) {
+  if (m.type != VT_MAT_DIFFUSE) {
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
+    A.giPos[i] = zero; A.giNrm[i] = zero; A.giRad[i] = zero; A.giW[i] = zero;
     return;
   }
   DIReservoir r;
@@ -1273,8 +1421,9 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
     if (rand_decision(seed) * r.wsum < w) r.s = cand;
   }
   int px, py;
-  if (backproject(A, S.pos, px, py)) {
-    const uint32_t j = (uint32_t)py * A.W + (uint32_t)px;
+  const bool temporal = backproject(A, S.pos, px, py);
+  const uint32_t j = temporal ? (uint32_t)py * A.W + (uint32_t)px : 0u;
+  if (temporal) {
     const float4 hw = A.hrW[j];
     if (same_surface(gp, gn, A.hPos[j], A.hNrm[j]) && hw.y > 0.0f && hw.z > 0.0f) {
       const DISample hs = load_di(A.hrPos, A.hrEmit, A.hrW, j);
@@ -1290,12 +1439,41 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
   A.rPos[i] = make_float4(r.s.pos.x, r.s.pos.y, r.s.pos.z, __uint_as_float(r.s.id));
   A.rEmit[i] = make_float4(r.s.emission.x, r.s.emission.y, r.s.emission.z, r.s.pdf);
   A.rW[i] = make_float4(r.wsum, r.M, W, r.s.u);
+  // ReSTIR GI: depth 1 has no indirect bounce for it (restir_gi_enabled, main.swift:3476-3478).
+  if ((int)A.maxDepth - 1 < 1) {
+    A.giPos[i] = zero; A.giNrm[i] = zero; A.giRad[i] = zero; A.giW[i] = zero;
+    return;
+  }
+  float gwsum, gM = 1.0f;
+  GISample g = gi_initial(A, S, m, dir0, u, seed, stack, gwsum);
+  if (temporal) {
+    const float4 ow = A.hgiW[j], op = A.hgiPos[j], on = A.hgiNrm[j], hp = A.hPos[j];
+    if (same_surface(gp, gn, hp, A.hNrm[j]) && ow.y > 0.0f && ow.z > 0.0f && op.w > 0.0f && on.w > 0.0f) {
+      const GISample hs = gi_load(A.hgiPos, A.hgiNrm, A.hgiRad, A.hgiW, j);
+      if (gi_accepts_shift(S.pos, f3(hp.x, hp.y, hp.z), hs.pos, hs.nrm)) {
+        const float cM = fminf(ow.y, 20.0f);
+        const float w = gi_target(A, S.pos, S.n, S.gn, dir0, m, hs) * ow.z * cM;
+        gM += cM;
+        gwsum += w;
+        if (pcg_rand(seed.state) * gwsum < w) g = hs;
+      }
+    }
+  }
+  const float gHat = gi_target(A, S.pos, S.n, S.gn, dir0, m, g);
+  const float gW = gM > 0.0f && gHat > 0.0f ? gwsum / (gM * gHat) : 0.0f;
+  A.giPos[i] = make_float4(g.pos.x, g.pos.y, g.pos.z, g.pdf);
+  A.giNrm[i] = make_float4(g.nrm.x, g.nrm.y, g.nrm.z, g.pdf > 0.0f ? 1.0f : 0.0f);
+  A.giRad[i] = g.rad;
+  A.giW[i] = make_float4(gwsum, gM, gW, g.u);
 }
 
-// ReSTIR DI pass 2 for frame k (shading_kernel, main.swift:7484-7561): spatial reuse of 4 uniform
-// taps in a 32-pixel box that pass RESTIR2020's compatibility test (uniform_neighbor, main.swift:
-// 5025-5027), the selected sample's contribution W * bsdf * Le * cos * G when visible, then the
-// path's continuation (MIS at later vertices). The sample is added to the FP64 accumulation.
+// ReSTIR DI pass 2 for frame k (shading_kernel, main.swift:7484-7656): at a diffuse primary, spatial
+// reuse of 4 uniform taps in a 32-pixel box that pass RESTIR2020's compatibility test
+// (uniform_neighbor, main.swift:5025-5027), the selected sample's contribution W * bsdf * Le * cos *
+// G when visible; then the same for the GI reservoirs (the reconnection x1 -> x2 shaded with the
+// secondary radiance, W and the area-measure geometry term); other primaries take NEE with MIS
+// (main.swift:7767-7780). Then the path's continuation (MIS at later vertices). The sample is added
+// to the FP64 accumulation.
 template <bool kPbr, bool kNrc = false>
 __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderArgs A, uint32_t k) {
   int stack[kRenderStack];
@@ -1330,6 +1508,13 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
   float3 R;
   if (m.type == VT_MAT_EMISSIVE) {
     R = primary_emission(A, L, S, m);
+  } else if (m.type != VT_MAT_DIFFUSE) {
+    const int limit = max(0, (int)A.maxDepth - 1);
+    const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    sampler_event(seed, 1u, kZNee);
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, seed, stack, true);
+    const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
+    R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, spreadLimit, slot, &queried));
   } else {
     const float4 cw = A.rW[i];
     DISample sel = load_di(A.rPos, A.rEmit, A.rW, i);
@@ -1353,6 +1538,43 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
       R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel), W);
+    // ReSTIR GI (a cache-terminated path's cache covers this light, so the cache's kernel leaves it out).
+    if (!kNrc && (int)A.maxDepth - 1 >= 1) {
+      const float4 cgw = A.giW[i];
+      GISample gsel = gi_load(A.giPos, A.giNrm, A.giRad, A.giW, i);
+      bool gvalid = A.giNrm[i].w > 0.0f;
+      float gwsum = gvalid ? gi_target(A, S.pos, S.n, S.gn, dir0, m, gsel) * cgw.z * cgw.y : 0.0f, gM = cgw.y;
+      for (int t = 0; t < 4; ++t) {
+        const float ox = pcg_rand(seed.state), oy = pcg_rand(seed.state);
+        const int nx = (int)x + (int)((ox * 2.0f - 1.0f) * 16.0f), ny = (int)y + (int)((oy * 2.0f - 1.0f) * 16.0f);
+        if (nx < 0 || nx >= (int)A.W || ny < 0 || ny >= (int)A.H) continue;
+        const uint32_t j = (uint32_t)ny * A.W + (uint32_t)nx;
+        const float4 q = A.gPos[j];
+        if (!compatible(gp, gn, q, A.gNrm[j])) continue;
+        const float4 nw = A.giW[j], np = A.giPos[j], nn = A.giNrm[j];
+        if (nw.y <= 0.0f || nw.z <= 0.0f || np.w <= 0.0f || nn.w <= 0.0f) continue;
+        if (!gi_accepts_shift(S.pos, f3(q.x, q.y, q.z), f3(np.x, np.y, np.z), f3(nn.x, nn.y, nn.z))) continue;
+        const GISample ns = gi_load(A.giPos, A.giNrm, A.giRad, A.giW, j);
+        const float w = gi_target(A, S.pos, S.n, S.gn, dir0, m, ns) * nw.z * nw.y;
+        gwsum += w;
+        gM += nw.y;
+        if (rand_decision(seed) * gwsum < w) {
+          gsel = ns;
+          gvalid = true;
+        }
+      }
+      const float gHat = gvalid ? gi_target(A, S.pos, S.n, S.gn, dir0, m, gsel) : 0.0f;
+      const float gW = gM > 0.0f && gHat > 0.0f ? gwsum / (gM * gHat) : 0.0f;
+      if (gW > 0.0f && gi_visible(A, S.pos, S.gn, gsel.pos, S.err, stack)) {
+        const float3 dir = normalize3(sub(gsel.pos, S.pos));
+        Lanes Ls;
+        if (A.spectral) Ls = make_lanes(A, gsel.u);
+        float pdf;
+        const float f = lambert_eval(S.n, S.gn, mul(dir0, -1.0f), dir, pdf);
+        const float geometry = gi_geometry(S.pos, S.n, gsel.pos, gsel.nrm);
+        R = add(R, to_rgb(A, Ls, scale4(mul4(reflectance(A, Ls, m), gsel.rad), f * geometry * gW)));
+      }
+    }
     const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
     R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, true, spreadLimit, slot, &queried));
   }
@@ -2484,7 +2706,7 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
     if (!scene->d_di || scene->di_width != p->width || scene->di_height != p->height) {
       cudaFree(scene->d_di);
       scene->d_di = nullptr;
-      VT_CUDA(ctx, cudaMalloc(&scene->d_di, 12 * (size_t)npix * sizeof(float4)));
+      VT_CUDA(ctx, cudaMalloc(&scene->d_di, 20 * (size_t)npix * sizeof(float4)));
       scene->di_width = p->width;
       scene->di_height = p->height;
       scene->di_frames = 0;
@@ -2495,17 +2717,23 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
     A.diCandidates = m;
     A.diBits = bits;
     float4 *base = scene->d_di;
-    A.gInfo = reinterpret_cast<uint4 *>(base + 10 * (size_t)npix);
-    A.gGeo = base + 11 * (size_t)npix;
+    // Per frame parity 9 arrays (surface cache 2, DI reservoir 3, GI reservoir 4), then the primary
+    // hit's info and geometric normal.
+    A.gInfo = reinterpret_cast<uint4 *>(base + 18 * (size_t)npix);
+    A.gGeo = base + 19 * (size_t)npix;
     const float cam[14] = {A.cam.x, A.cam.y, A.cam.z, A.fwd.x, A.fwd.y, A.fwd.z, A.right.x, A.right.y, A.right.z,
                            A.up.x, A.up.y, A.up.z, A.aspect, A.fovScale};
     const unsigned blocks = (npix + kRenderBlock - 1) / kRenderBlock;
     for (uint32_t k = 0; k < spp; ++k) {
-      float4 *cur = base + 5 * (size_t)npix * scene->di_parity, *prev = base + 5 * (size_t)npix * (scene->di_parity ^ 1u);
+      float4 *cur = base + 9 * (size_t)npix * scene->di_parity, *prev = base + 9 * (size_t)npix * (scene->di_parity ^ 1u);
       A.gPos = cur; A.gNrm = cur + npix; A.rPos = cur + 2 * (size_t)npix; A.rEmit = cur + 3 * (size_t)npix;
       A.rW = cur + 4 * (size_t)npix;
+      A.giPos = cur + 5 * (size_t)npix; A.giNrm = cur + 6 * (size_t)npix; A.giRad = cur + 7 * (size_t)npix;
+      A.giW = cur + 8 * (size_t)npix;
       A.hPos = prev; A.hNrm = prev + npix; A.hrPos = prev + 2 * (size_t)npix; A.hrEmit = prev + 3 * (size_t)npix;
       A.hrW = prev + 4 * (size_t)npix;
+      A.hgiPos = prev + 5 * (size_t)npix; A.hgiNrm = prev + 6 * (size_t)npix; A.hgiRad = prev + 7 * (size_t)npix;
+      A.hgiW = prev + 8 * (size_t)npix;
       A.history = scene->di_frames > 0 ? 1u : 0u;
       const float *pc = scene->di_cam;
       A.pcam = make_float3(pc[0], pc[1], pc[2]);
@@ -3059,7 +3287,19 @@ vt_status vt_scene_di_weights(vt_ctx *ctx, const vt_scene *scene, float *out, ui
   if (!scene->d_di || scene->di_frames == 0) return vt_fail(ctx, VT_ERR_INVALID, "no ReSTIR DI frame rendered");
   const size_t npix = (size_t)scene->di_width * scene->di_height;
   if (n != 4 * npix) return vt_fail(ctx, VT_ERR_INVALID, "n must equal width * height * 4");
-  const float4 *last = scene->d_di + 5 * npix * (scene->di_parity ^ 1u) + 4 * npix;
+  const float4 *last = scene->d_di + 9 * npix * (scene->di_parity ^ 1u) + 4 * npix;
+  VT_CUDA(ctx, cudaDeviceSynchronize());
+  VT_CUDA(ctx, cudaMemcpy(out, last, npix * sizeof(float4), cudaMemcpyDeviceToHost));
+  return VT_OK;
+}
+
+vt_status vt_scene_gi_weights(vt_ctx *ctx, const vt_scene *scene, float *out, uint32_t n) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene || !out) return vt_fail(ctx, VT_ERR_INVALID, "scene or out is null");
+  if (!scene->d_di || scene->di_frames == 0) return vt_fail(ctx, VT_ERR_INVALID, "no ReSTIR DI frame rendered");
+  const size_t npix = (size_t)scene->di_width * scene->di_height;
+  if (n != 4 * npix) return vt_fail(ctx, VT_ERR_INVALID, "n must equal width * height * 4");
+  const float4 *last = scene->d_di + 9 * npix * (scene->di_parity ^ 1u) + 8 * npix;
   VT_CUDA(ctx, cudaDeviceSynchronize());
   VT_CUDA(ctx, cudaMemcpy(out, last, npix * sizeof(float4), cudaMemcpyDeviceToHost));
   return VT_OK;

@@ -97,7 +97,8 @@ __device__ __forceinline__ uint32_t z_morton(uint32_t x, uint32_t y) {
 }
 
 // Sampling-event streams (main.swift:291-292): 32 dimensions each, 16 per path vertex.
-constexpr uint32_t kZBsdf = 0u, kZNee = 1u, kZRoulette = 2u, kZLens = 3u, kZDi = 4u, kZWavelength = 12u;
+constexpr uint32_t kZBsdf = 0u, kZNee = 1u, kZRoulette = 2u, kZLens = 3u, kZDi = 4u, kZGiBsdf = 5u, kZGiNee = 6u,
+                   kZWavelength = 12u;
 
 struct Sampler {
   uint32_t state, key, dimension, sub, subBits;

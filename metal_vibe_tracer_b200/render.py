@@ -177,6 +177,14 @@ class Scene:
                "vt_scene_di_weights")
         return out
 
+    def gi_weights(self) -> np.ndarray:
+        """(height, width, 4) float32 ReSTIR GI reservoir weights of the last mode-0 frame: weight sum,
+        M, W, wavelength number (M 0 where no GI reservoir was built)."""
+        out = np.empty((self.height, self.width, 4), np.float32)
+        _check(self.ctx.handle, _lib.load().vt_scene_gi_weights(self.ctx.handle, self._p, out.ctypes.data, out.size),
+               "vt_scene_gi_weights")
+        return out
+
     def light_estimate(self, points, per_point: int, samples: int = 64) -> np.ndarray:
         """The reference's lt_estimate check on the device: (npoints * per_point, 8) float32 per
         thread (sum, squares, hits, zero pdfs, max pdf error, back-facing choices, 0, 0)."""

@@ -2126,6 +2126,9 @@ D3 primary_emission_d(const PtContext &C, const PtLanes &L, const PtHit &h, cons
 D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m, D3 dir, ZSampler &seed, bool diPrimary) {
   const int limit = std::max(0, (int)C.p->max_depth - 1);
   const bool nee = C.p->sampling_mode != 3u, mis = C.p->sampling_mode <= 1u;
+  // ReSTIR GI estimates the secondary diffuse vertex's direct light (restirGISecondary,
+  // main.swift:7801-7803).
+  const bool giPrimary = diPrimary && m.type == VT_MAT_DIFFUSE;
   Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
   D3 R{0, 0, 0};
   int scattering = 0;
@@ -2182,7 +2185,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
       break;
     }
     if (emissionOnly) break;
-    if (nee) {
+    if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       seed.event((uint32_t)bounce + 1u, 1u);
       R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, seed,
                        false);
@@ -2201,11 +2204,16 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
 // restir_temporal_kernel (main.swift:4842-4960) and the spatial reuse of shading_kernel
 // (main.swift:7484-7561): per frame, pass 1 over every pixel, then pass 2 over every pixel.
 struct DiS { D3 pos{0, 0, 0}, emission{0, 0, 0}; double pdf = 0, u = 0; uint32_t id = 0; };
+// A ReSTIR GI sample: x2, its normal, its outgoing direct radiance per lane, its source pdf (area
+// measure), the wavelength number, validity (restir_gi_encode's normal flag).
+struct GiS { D3 pos{0, 0, 0}, nrm{0, 0, 0}; Spec4 rad{{0, 0, 0, 0}}; double pdf = 0, u = 0; bool valid = false; };
 struct DiPix {
   double pos[4] = {0, 0, 0, -1}, nrm[4] = {0, 0, 0, -1};
   PtHit hit{};
   DiS s;
   double wsum = 0, M = 0, W = 0;
+  GiS g;
+  double gwsum = 0, gM = 0, gW = 0;
 };
 
 // light_geometry (main.swift:3165-3183).
@@ -2283,6 +2291,104 @@ PtLight light_from_di(const DiS &c, D3 p) {
   return ls;
 }
 
+
+// ---- ReSTIR GI (main.swift:3201-3252, 4718-4806, 7582-7656), FP64 ---------------------------------
+double gi_geometry_d(D3 x1, D3 n1, D3 x2, D3 n2) {
+  const D3 delta = x2 - x1;
+  const double d2 = dot(delta, delta);
+  if (d2 < 1e-10) return 0.0;
+  const D3 dir = delta * (1.0 / std::sqrt(d2));
+  return std::max(0.0, dot(n1, dir)) * std::max(0.0, -dot(n2, dir)) / d2;
+}
+bool gi_accepts_shift_d(D3 x1r, D3 x1q, D3 x2, D3 n2) {
+  const D3 cur = x1r - x2, src = x1q - x2;
+  const double cd2 = dot(cur, cur), sd2 = dot(src, src);
+  if (cd2 < 1e-10 || sd2 < 1e-10) return false;
+  const double cc = std::max(0.0, dot(n2, cur * (1.0 / std::sqrt(cd2)))), sc = std::max(0.0, dot(n2, src * (1.0 / std::sqrt(sd2))));
+  double j = cc * sd2 / (sc * cd2);
+  if (!std::isfinite(j)) j = 0.0;
+  return j >= 0.1 && j <= 10.0;
+}
+double lambert_eval_d(D3 n, D3 gn, D3 wo, D3 wi, double &pdf) {
+  const double ni = dot(n, wi), no = dot(n, wo);
+  pdf = 0.0;
+  if (!(no > 0.0)) return 0.0;
+  pdf = std::max(0.0, ni) / kPi;
+  return ni > 0.0 && std::fabs(ni) >= 1e-7 && dot(wi, gn) > 0.0 ? 1.0 / kPi : 0.0;
+}
+double gi_target_d(const PtContext &C, const PtHit &h, D3 rayDir, const vt_material &m, const GiS &c) {
+  const double geometry = gi_geometry_d(h.pos, h.n, c.pos, c.nrm);
+  bool finite = true;
+  for (double x : c.rad.v) finite = finite && std::isfinite(x);
+  if (geometry <= 0.0 || !finite) return 0.0;
+  const D3 dir = normalize(c.pos - h.pos);
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, c.u);
+  double pdf;
+  const double f = lambert_eval_d(h.n, h.gn, rayDir * -1.0, dir, pdf);
+  const D3 v = to_rgb(C, L, scale(mul(reflectance(C, L, m), c.rad), f * geometry));
+  return std::sqrt(dot(v, v));
+}
+bool gi_visible_d(const PtContext &C, D3 x1, D3 n1, D3 x2, double err) {
+  const D3 delta = x2 - x1;
+  const double dist = std::sqrt(dot(delta, delta));
+  if (dist <= 2.0 * ray_eps_d(C, x1)) return false;
+  const D3 o = ray_origin_d(C, x1, n1, delta * (1.0 / dist), err);
+  const D3 e = x2 - o;
+  const double d = std::sqrt(dot(e, e));
+  const double legacy = 2.0 * ray_eps_d(C, x2);
+  const double tol = C.imported ? std::max(legacy, 1.907349e-6 * (max_abs_d(o) + max_abs_d(x2) + d)) : legacy;
+  return !pt_occluded(C, o, e * (1.0 / d), d - tol);
+}
+// restir_gi_initial (main.swift:4718-4770) at a diffuse primary hit h (material m) seen along view.
+GiS gi_initial_d(const PtContext &C, const PtHit &h, const vt_material &m, D3 view, double u, ZSampler &seed,
+                 double &wsum) {
+  GiS r;
+  r.u = u;
+  wsum = 0.0;
+  const int limit = std::max(0, (int)C.p->max_depth - 1);
+  seed.event(1u, 5u);
+  double r0, r1, r2;
+  seed.f3(r0, r1, r2);
+  const D3 gd = cosine_hemisphere_d(h.n, r1, r2);
+  const double bpdf = std::max(0.0, dot(h.n, gd)) / kPi;
+  if (!(bpdf > 0.0) || !(dot(gd, h.gn) > 0.0)) return r;
+  PtHit h2;
+  if (!pt_closest(C, ray_origin_d(C, h.pos, h.gn, gd, h.err), gd, h2)) return r;
+  const vt_material m2 = pt_material(C, h2.slot);
+  if (m2.type != VT_MAT_DIFFUSE) return r;
+  PtLanes L{};
+  if (C.spectral) L = make_lanes(C, u);
+  Spec4 rad{{0, 0, 0, 0}};
+  seed.event(2u, 6u);
+  const PtLight ls = C.imported ? sample_emitters_d(C, h2.pos, h2.n, seed) : sample_light_d(C, h2.pos, seed);
+  if (ls.pdf > 0.0 && visible_d(C, h2.pos, h2.gn, h2.err, ls)) {
+    const double c2 = std::max(0.0, dot(h2.n, ls.wi));
+    double pdf2;
+    const double f2 = lambert_eval_d(h2.n, h2.gn, gd * -1.0, ls.wi, pdf2);
+    const double mis = limit >= 2 ? power_heuristic_d(ls.pdf, pdf2) : 1.0;
+    const float le[3] = {(float)ls.emission.x, (float)ls.emission.y, (float)ls.emission.z};
+    rad = scale(mul(reflectance(C, L, m2), emission(C, L, le)), f2 * c2 * mis / ls.pdf);
+  }
+  const D3 delta = h2.pos - h.pos;
+  const double d2 = dot(delta, delta);
+  const double cos2 = std::max(0.0, -dot(h2.n, gd));
+  const double src = d2 > 1e-10 ? bpdf * cos2 / d2 : 0.0;
+  GiS c;
+  c.pos = h2.pos;
+  c.nrm = h2.n;
+  c.rad = rad;
+  c.pdf = src;
+  c.u = u;
+  c.valid = src > 0.0;
+  const double pHat = gi_target_d(C, h, view, m, c);
+  if (src > 0.0 && pHat > 0.0) {
+    r = c;
+    wsum = pHat / src;
+  }
+  return r;
+}
+
 void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx, float jy,
                   uint32_t M, uint32_t bits, bool history, const std::vector<DiPix> &prev, DiPix &out) {
   out = DiPix{};
@@ -2297,7 +2403,7 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   const double pos[4] = {h.pos.x, h.pos.y, h.pos.z, h.t}, nrm[4] = {h.n.x, h.n.y, h.n.z, double(m.type)};
   std::memcpy(out.pos, pos, sizeof pos);
   std::memcpy(out.nrm, nrm, sizeof nrm);
-  if (m.type != VT_MAT_DIFFUSE && !pbr_slot(C, m)) return;
+  if (m.type != VT_MAT_DIFFUSE) return;
   out.s.u = u;
   for (uint32_t c = 0; c < M; ++c) {
     seed.candidate(1u, 4u, c, bits);
@@ -2312,7 +2418,8 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
     if (seed.decision() * out.wsum < w) out.s = cand;
   }
   int px, py;
-  if (history && backproject_d(C, h.pos, px, py)) {
+  const bool temporal = history && backproject_d(C, h.pos, px, py);
+  if (temporal) {
     const DiPix &o = prev[(size_t)py * C.p->width + px];
     if (same_surface_d(pos, nrm, o.pos, o.nrm) && o.M > 0.0 && o.W > 0.0) {
       const double cM = std::min(o.M, 20.0);
@@ -2324,6 +2431,25 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   }
   const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, out.s);
   out.W = out.M > 0.0 && pHat > 0.0 ? out.wsum / (out.M * pHat) : 0.0;
+  if ((int)C.p->max_depth - 1 < 1) return;
+  double gwsum, gM = 1.0;
+  GiS g = gi_initial_d(C, h, m, dir0, u, seed, gwsum);
+  if (temporal) {
+    const DiPix &o = prev[(size_t)py * C.p->width + px];
+    if (same_surface_d(pos, nrm, o.pos, o.nrm) && o.gM > 0.0 && o.gW > 0.0 && o.g.pdf > 0.0 && o.g.valid &&
+        gi_accepts_shift_d(h.pos, D3{o.pos[0], o.pos[1], o.pos[2]}, o.g.pos, o.g.nrm)) {
+      const double cM = std::min(o.gM, 20.0);
+      const double w = gi_target_d(C, h, dir0, m, o.g) * o.gW * cM;
+      gM += cM;
+      gwsum += w;
+      if (seed.pcg() * gwsum < w) g = o.g;
+    }
+  }
+  const double gHat = gi_target_d(C, h, dir0, m, g);
+  out.g = g;
+  out.gwsum = gwsum;
+  out.gM = gM;
+  out.gW = gM > 0.0 && gHat > 0.0 ? gwsum / (gM * gHat) : 0.0;
 }
 
 D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t frame, float jx, float jy,
@@ -2339,6 +2465,16 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   const PtHit &h = me.hit;
   const vt_material m = pt_material(C, h.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
+  if (m.type != VT_MAT_DIFFUSE) {
+    // Other primaries: NEE with MIS (main.swift:7767-7780).
+    const int limit = std::max(0, (int)C.p->max_depth - 1);
+    const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
+    seed.event(1u, 1u);
+    D3 R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, seed, true);
+    R = R + continue_path_d(C, L, h, m, dir0, seed, false);
+    if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
+    return R;
+  }
   DiS sel = me.s;
   double wsum = di_target_d(C, h.pos, h.n, h.gn, dir0, m, sel) * me.W * me.M, M = me.M;
   for (int t = 0; t < 4; ++t) {
@@ -2358,6 +2494,38 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   D3 R{0, 0, 0};
   if (W > 0.0 && visible_d(C, h.pos, h.gn, h.err, light_from_di(sel, h.pos)))
     R = di_contribution_d(C, h.pos, h.n, h.gn, dir0, m, sel) * W;
+  if ((int)C.p->max_depth - 1 >= 1) {
+    GiS gs = me.g;
+    bool gvalid = me.g.valid;
+    double gwsum = gvalid ? gi_target_d(C, h, dir0, m, gs) * me.gW * me.gM : 0.0, gM = me.gM;
+    for (int t = 0; t < 4; ++t) {
+      const double ox = seed.pcg(), oy = seed.pcg();
+      const int nx = (int)x + (int)((ox * 2.0 - 1.0) * 16.0), ny = (int)y + (int)((oy * 2.0 - 1.0) * 16.0);
+      if (nx < 0 || nx >= (int)C.p->width || ny < 0 || ny >= (int)C.p->height) continue;
+      const DiPix &n = cur[(size_t)ny * C.p->width + nx];
+      if (!compatible_d(me.pos, me.nrm, n.pos, n.nrm)) continue;
+      if (n.gM <= 0.0 || n.gW <= 0.0 || n.g.pdf <= 0.0 || !n.g.valid) continue;
+      if (!gi_accepts_shift_d(h.pos, D3{n.pos[0], n.pos[1], n.pos[2]}, n.g.pos, n.g.nrm)) continue;
+      const double w = gi_target_d(C, h, dir0, m, n.g) * n.gW * n.gM;
+      gwsum += w;
+      gM += n.gM;
+      if (seed.decision() * gwsum < w) {
+        gs = n.g;
+        gvalid = true;
+      }
+    }
+    const double gHat = gvalid ? gi_target_d(C, h, dir0, m, gs) : 0.0;
+    const double gW = gM > 0.0 && gHat > 0.0 ? gwsum / (gM * gHat) : 0.0;
+    if (gW > 0.0 && gi_visible_d(C, h.pos, h.gn, gs.pos, h.err)) {
+      const D3 dir = normalize(gs.pos - h.pos);
+      PtLanes Ls{};
+      if (C.spectral) Ls = make_lanes(C, gs.u);
+      double pdf;
+      const double f = lambert_eval_d(h.n, h.gn, dir0 * -1.0, dir, pdf);
+      const double geometry = gi_geometry_d(h.pos, h.n, gs.pos, gs.nrm);
+      R = R + to_rgb(C, Ls, scale(mul(reflectance(C, Ls, m), gs.rad), f * geometry * gW));
+    }
+  }
   R = R + continue_path_d(C, L, h, m, dir0, seed, true);
   if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
   return R;

@@ -88,3 +88,25 @@ def test_temporal_reuse_survives_camera_motion_and_cuts_clear_it(ctx, cornell):
     scene.close()
     final = render(ctx, mesh, mats, light, moved, 160, 120, 128, 1)
     assert abs(last.mean() / final.mean() - 1) < 0.15, (last.mean(), final.mean())
+
+
+def test_restir_gi_reservoirs_and_energy(ctx, cornell):
+    """ReSTIR GI (main.swift:4718-4812, 7582-7656): with a scattering budget the diffuse primaries build
+    GI reservoirs (most with a sample after a few frames of temporal reuse), none at depth 1, and the
+    mode-0 image (DI + GI reservoirs, NEE skipped at the secondary diffuse vertex) keeps the MIS
+    image's energy within the reference's 6 % (tests/Fix_integrator.swift:203-205) at depth 8."""
+    faces, verts, mats, light, cam, mesh = cornell
+    scene = vt.Scene(ctx, mesh, mats, light)
+    for k in range(6):
+        scene.render(vt.make_params(cam, 64, 48, 8, 1 + k, False, 0), 1)
+    g = scene.gi_weights()
+    valid = g[..., 1] > 0
+    assert valid.mean() > 0.8, valid.mean()
+    assert (g[valid][:, 1] > 1.5).mean() > 0.5  # merged history
+    scene.reset()
+    scene.render(vt.make_params(cam, 64, 48, 1, 1, False, 0), 1)
+    assert np.all(scene.gi_weights()[..., 1] == 0.0)
+    scene.close()
+    mis = render(ctx, mesh, mats, light, cam, 48, 32, 256, 1, 8).mean()
+    gi = render(ctx, mesh, mats, light, cam, 48, 32, 256, 0, 8).mean()
+    assert abs(gi / mis - 1) < 0.06, (gi, mis)
