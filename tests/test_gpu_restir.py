@@ -101,7 +101,10 @@ def test_restir_gi_reservoirs_and_energy(ctx, cornell):
         scene.render(vt.make_params(cam, 64, 48, 8, 1 + k, False, 0), 1)
     g = scene.gi_weights()
     valid = g[..., 1] > 0
-    assert valid.mean() > 0.8, valid.mean()
+    # Every diffuse primary holds a GI reservoir (M >= 1), as it holds a DI one; misses and the
+    # emitter hold neither.
+    assert np.array_equal(valid, scene.di_weights()[..., 1] > 0)
+    assert valid.mean() > 0.5, valid.mean()
     assert (g[valid][:, 1] > 1.5).mean() > 0.5  # merged history
     scene.reset()
     scene.render(vt.make_params(cam, 64, 48, 1, 1, False, 0), 1)
