@@ -146,6 +146,80 @@ vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays
 vt_status vt_trace_count(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
                          int32_t closest, uint64_t *nodes_visited, uint64_t *tris_tested);
 
+/* ---- two-level hierarchy (instances of meshes) ----------------------------------------------- */
+
+typedef struct vt_tlas vt_tlas;
+
+/* One placed copy of a mesh (MeshLayout.addInstance, Sources/Acceleration.swift:474-516). 64 B. */
+typedef struct vt_instance {
+  float world[12];      /* object -> world transform, row-major 3 x 4 (the rows of MeshInstance.world,
+                           main.swift:1609) */
+  uint32_t mesh;        /* index into vt_tlas_build's mesh array */
+  uint32_t slot_base;   /* added to the mesh's face tags (material slots) by vt_tlas_flatten */
+  uint32_t reserved[2]; /* 0 */
+} vt_instance;
+
+/* An instance as the device holds it (MeshInstance, main.swift:1609; MeshInstanceRecord,
+ * Sources/Acceleration.swift:545-557). 128 B (the reference record without its binding word, which serves scene-graph slots). */
+typedef struct vt_instance_record {
+  float world[12];      /* object -> world, row-major 3 x 4 */
+  float local[12];      /* world -> object: the inverse, computed in double and rounded once */
+  uint32_t mesh;        /* the instance's mesh */
+  uint32_t slot_base;
+  uint32_t rendered_base; /* first rendered triangle: sum of the faces of the instances before it */
+  uint32_t mirrored;    /* 1 when det(world) < 0 (flattening swaps vertices b and c) */
+  float bound[4];       /* max |translation|, infinity norm of the linear part, the mesh's max
+                           |coordinate|, 0 */
+} vt_instance_record;
+
+typedef struct vt_tlas_info {
+  uint32_t instances;   /* instances in the hierarchy */
+  uint32_t meshes;      /* meshes it references */
+  uint32_t nodes;       /* 4-wide TLAS nodes */
+  uint32_t depth;       /* TLAS depth, root = 1 */
+  uint64_t rendered_triangles; /* sum over instances of their mesh's faces */
+  float lo[3], hi[3];   /* world bounds (the union of the instance boxes) */
+  float grow;           /* per-ray TLAS box growth factor 2^-18 (1 + largest condition number of an
+                           instance's linear part) (MeshSceneHeader.lo.w) */
+  float reach;          /* max over instances of |translation| + norm(linear) * mesh max |coordinate|
+                           (MeshSceneHeader.hi.w) */
+  float build_ms;       /* device time of the TLAS build */
+  float pad;
+} vt_tlas_info;
+
+/* Builds the two-level hierarchy: a 4-wide TLAS (leaf size 1) over the instances' world boxes
+ * (the mesh's box corners transformed, enlarged by 2^-20 reach), whose leaves name instances, over
+ * the meshes' own hierarchies (the BLAS). Replaces MeshSceneLayout.sceneBlob (Sources/
+ * Acceleration.swift:519-573). The meshes must outlive the TLAS. Rejects (VT_ERR_INVALID) a mesh
+ * index out of range, a transform with a non-finite entry, a first-column scale outside
+ * [1e-6, 1e6], |det| <= 1e-18 or a reach of 1e8 or more (the reference's "Combined hierarchy scale
+ * exceeds the supported range.", "Singular USD transform.", "Hierarchy transform exceeds the
+ * supported scene extent."). */
+vt_status vt_tlas_build(vt_ctx *ctx, const vt_mesh *const *meshes, uint32_t nmeshes, const vt_instance *instances,
+                        uint32_t ninstances, vt_tlas **out);
+vt_status vt_tlas_destroy(vt_ctx *ctx, vt_tlas *tlas);
+vt_status vt_tlas_get_info(vt_ctx *ctx, const vt_tlas *tlas, vt_tlas_info *out);
+/* The TLAS nodes (leaf children name instances: -(instance + 1), count 1). `n` = info.nodes. */
+vt_status vt_tlas_get_nodes(vt_ctx *ctx, const vt_tlas *tlas, vt_wide_node *nodes, uint32_t n);
+/* The instance records. `n` = info.instances. */
+vt_status vt_tlas_get_instances(vt_ctx *ctx, const vt_tlas *tlas, vt_instance_record *records, uint32_t n);
+/* Closest hit of `n` DEVICE world rays through the two levels (mesh_closest, main.swift:1840-1901):
+ * the TLAS boxes grown per ray by grow * (max|origin| + reach), instances in near-to-far order,
+ * each traced in object space (the ray transformed by `local`, its direction not renormalised, so t
+ * is the world ray's). Hits carry the instance's mesh face (input order); `instances_dev` (may be
+ * NULL) receives the hit instance (0xFFFFFFFF on a miss). */
+vt_status vt_tlas_trace_closest(vt_ctx *ctx, const vt_tlas *tlas, const vt_ray *rays_dev, uint32_t n,
+                                vt_hit *hits_dev, uint32_t *instances_dev, void *stream);
+/* Any hit in [tmin, tmax) through the two levels (mesh_occluded, main.swift:1957-1984), without
+ * endpoint slack. */
+vt_status vt_tlas_trace_any(vt_ctx *ctx, const vt_tlas *tlas, const vt_ray *rays_dev, uint32_t n,
+                            uint8_t *occluded_dev, void *stream);
+/* One world-space mesh of every instance's triangles (SceneGraph.forEachRenderTriangle, as
+ * instance_triangle renders them, main.swift:1645-1668): rendered face rendered_base + f is the
+ * instance's face f with vertices transformed by `world`, normals by the inverse transpose, tag +
+ * slot_base, b and c swapped when mirrored; then built like vt_mesh_build_device. */
+vt_status vt_tlas_flatten(vt_ctx *ctx, const vt_tlas *tlas, const vt_build_options *opts, vt_mesh **out);
+
 /* ---- path tracing (integrator) ------------------------------------------------------------- */
 
 typedef struct vt_scene vt_scene;

@@ -7,10 +7,10 @@ CPU: a missing library raises.
 """
 from ._lib import (FACE_DTYPE, HIT_DTYPE, RAY_DTYPE, VERTEX_DTYPE, WIDE_NODE_DTYPE, LIB_PATH,
                    exported_symbols, load)
-from .accel import Context, MaterialLibraryError, Mesh, WideBVHResult
+from .accel import Context, MaterialLibraryError, Mesh, Tlas, WideBVHResult, instances_array
 from .render import FrameParams, Scene, make_params
 
 __all__ = [
-    "Context", "Mesh", "MaterialLibraryError", "WideBVHResult", "Scene", "FrameParams", "make_params", "FACE_DTYPE", "VERTEX_DTYPE",
+    "Context", "Mesh", "Tlas", "instances_array", "MaterialLibraryError", "WideBVHResult", "Scene", "FrameParams", "make_params", "FACE_DTYPE", "VERTEX_DTYPE",
     "RAY_DTYPE", "HIT_DTYPE", "WIDE_NODE_DTYPE", "LIB_PATH", "exported_symbols", "load",
 ]

@@ -28,6 +28,10 @@ EMITTER_DTYPE = np.dtype([("a", "<f4", 3), ("b", "<f4", 3), ("c", "<f4", 3), ("p
 assert EMITTER_DTYPE.itemsize == 56
 assert FACE_DTYPE.itemsize == 16 and VERTEX_DTYPE.itemsize == 32
 assert WIDE_NODE_DTYPE.itemsize == 128 and RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
+INSTANCE_DTYPE = np.dtype([("world", "<f4", 12), ("mesh", "<u4"), ("slot_base", "<u4"), ("reserved", "<u4", 2)])
+INSTANCE_RECORD_DTYPE = np.dtype([("world", "<f4", 12), ("local", "<f4", 12), ("mesh", "<u4"), ("slot_base", "<u4"),
+                                  ("rendered_base", "<u4"), ("mirrored", "<u4"), ("bound", "<f4", 4)])
+assert INSTANCE_DTYPE.itemsize == 64 and INSTANCE_RECORD_DTYPE.itemsize == 128
 
 
 class BuildOptions(C.Structure):
@@ -39,6 +43,12 @@ class MeshInfo(C.Structure):
     _fields_ = [("faces", C.c_uint32), ("wide_nodes", C.c_uint32), ("binary_nodes", C.c_uint32),
                 ("depth", C.c_uint32), ("sah_cost", C.c_float), ("build_ms", C.c_float),
                 ("lo", C.c_float * 3), ("hi", C.c_float * 3)]
+
+
+class TlasInfo(C.Structure):
+    _fields_ = [("instances", C.c_uint32), ("meshes", C.c_uint32), ("nodes", C.c_uint32), ("depth", C.c_uint32),
+                ("rendered_triangles", C.c_uint64), ("lo", C.c_float * 3), ("hi", C.c_float * 3),
+                ("grow", C.c_float), ("reach", C.c_float), ("build_ms", C.c_float), ("pad", C.c_float)]
 
 
 class LightTreeInfo(C.Structure):
@@ -129,6 +139,14 @@ SIGNATURES = {
     "vt_trace_closest_host": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_trace_any_host": (_I32, [_P, _P, _P, _U32, _P]),
     "vt_trace_count": (_I32, [_P, _P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "vt_tlas_build": (_I32, [_P, _P, _U32, _P, _U32, C.POINTER(_P)]),
+    "vt_tlas_destroy": (_I32, [_P, _P]),
+    "vt_tlas_get_info": (_I32, [_P, _P, C.POINTER(TlasInfo)]),
+    "vt_tlas_get_nodes": (_I32, [_P, _P, _P, _U32]),
+    "vt_tlas_get_instances": (_I32, [_P, _P, _P, _U32]),
+    "vt_tlas_trace_closest": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
+    "vt_tlas_trace_any": (_I32, [_P, _P, _P, _U32, _P, _P]),
+    "vt_tlas_flatten": (_I32, [_P, _P, C.POINTER(BuildOptions), C.POINTER(_P)]),
     "vt_mesh_build_noalloc": (_I32, [_P, _U32, _P, _U32, C.POINTER(BuildOptions), _P, _U32, _P, _P,
                                      C.POINTER(MeshInfo), _P, C.c_char_p, _U32]),
     "vt_scene_create": (_I32, [_P, _P, _P, _U32, _P, _P, C.POINTER(_P)]),

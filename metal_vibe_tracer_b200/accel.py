@@ -19,8 +19,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (FACE_DTYPE, HIT_DTYPE, RAY_DTYPE, VERTEX_DTYPE, WIDE_NODE_DTYPE, BuildOptions,
-                   MeshInfo)
+from ._lib import (FACE_DTYPE, HIT_DTYPE, INSTANCE_DTYPE, INSTANCE_RECORD_DTYPE, RAY_DTYPE, VERTEX_DTYPE,
+                   WIDE_NODE_DTYPE, BuildOptions, MeshInfo, TlasInfo)
 
 
 class MaterialLibraryError(RuntimeError):
@@ -150,6 +150,14 @@ class Mesh:
         _check(ctx.handle, st, "vt_mesh_build")
         self._p = p
 
+    @classmethod
+    def _adopt(cls, ctx: Context, handle: C.c_void_p) -> "Mesh":
+        """Wraps a vt_mesh the library built (vt_tlas_flatten)."""
+        m = cls.__new__(cls)
+        m.ctx = ctx
+        m._p = handle
+        return m
+
     # ---- inspection -------------------------------------------------------------------------
     def info(self) -> MeshInfo:
         out = MeshInfo()
@@ -245,6 +253,105 @@ class Mesh:
     def close(self) -> None:
         if getattr(self, "_p", None) is not None and self.ctx._p is not None:
             _lib.load().vt_mesh_destroy(self.ctx.handle, self._p)
+        self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def instances_array(transforms, meshes, slot_bases=None) -> np.ndarray:
+    """INSTANCE_DTYPE records from (n, 3, 4) object-to-world transforms and per-instance mesh indices."""
+    t = np.asarray(transforms, np.float32).reshape(-1, 12)
+    out = np.zeros(t.shape[0], INSTANCE_DTYPE)
+    out["world"] = t
+    out["mesh"] = np.asarray(meshes, np.uint32)
+    if slot_bases is not None:
+        out["slot_base"] = np.asarray(slot_bases, np.uint32)
+    return out
+
+
+class Tlas:
+    """The two-level hierarchy over instances of meshes (vt_tlas): MeshSceneLayout.sceneBlob's TLAS
+    (Sources/Acceleration.swift:519-573) traversed like mesh_closest / mesh_occluded
+    (main.swift:1840-1984). The meshes must stay open while the TLAS is in use."""
+
+    def __init__(self, ctx: Context, meshes, instances):
+        lib = _lib.load()
+        self.ctx = ctx
+        self.meshes = list(meshes)
+        inst = np.ascontiguousarray(instances, INSTANCE_DTYPE)
+        handles = (C.c_void_p * len(self.meshes))(*[m._p.value for m in self.meshes])
+        p = C.c_void_p()
+        _check(ctx.handle, lib.vt_tlas_build(ctx.handle, handles, len(self.meshes), inst.ctypes.data, inst.shape[0],
+                                             C.byref(p)), "vt_tlas_build")
+        self._p = p
+
+    def info(self) -> TlasInfo:
+        out = TlasInfo()
+        _check(self.ctx.handle, _lib.load().vt_tlas_get_info(self.ctx.handle, self._p, C.byref(out)), "vt_tlas_get_info")
+        return out
+
+    def nodes(self) -> np.ndarray:
+        n = self.info().nodes
+        out = np.empty(n, WIDE_NODE_DTYPE)
+        _check(self.ctx.handle, _lib.load().vt_tlas_get_nodes(self.ctx.handle, self._p, out.ctypes.data, n),
+               "vt_tlas_get_nodes")
+        return out
+
+    def records(self) -> np.ndarray:
+        n = self.info().instances
+        out = np.empty(n, INSTANCE_RECORD_DTYPE)
+        _check(self.ctx.handle, _lib.load().vt_tlas_get_instances(self.ctx.handle, self._p, out.ctypes.data, n),
+               "vt_tlas_get_instances")
+        return out
+
+    def _device_rays(self, rays):
+        import torch
+        if _is_torch_cuda(rays):
+            return rays.contiguous(), False
+        r = as_rays(rays).view(np.float32).reshape(-1, 8)
+        return torch.from_numpy(np.ascontiguousarray(r)).cuda(self.ctx.device), True
+
+    def closest(self, rays):
+        """(hits, instances): numpy rays -> numpy HIT_DTYPE and uint32; CUDA tensor (n, 8) -> CUDA
+        tensors (n, 4) float32 (t, b1, b2, face bits) and (n,) int32 (instance, -1 on a miss)."""
+        import torch
+        r, host = self._device_rays(rays)
+        n = r.shape[0]
+        hits = torch.empty((n, 4), dtype=torch.float32, device=r.device)
+        inst = torch.empty((n,), dtype=torch.int32, device=r.device)
+        stream = torch.cuda.current_stream(r.device).cuda_stream
+        _check(self.ctx.handle, _lib.load().vt_tlas_trace_closest(self.ctx.handle, self._p, r.data_ptr(), n, hits.data_ptr(),
+                                                                  inst.data_ptr(), stream), "vt_tlas_trace_closest")
+        if host:
+            return hits.cpu().numpy().view(HIT_DTYPE).reshape(-1), inst.cpu().numpy().view(np.uint32)
+        return hits, inst
+
+    def occluded(self, rays):
+        """Any hit in [tmin, tmax): uint8 per ray (numpy for numpy rays, else a CUDA tensor)."""
+        import torch
+        r, host = self._device_rays(rays)
+        n = r.shape[0]
+        occ = torch.empty((n,), dtype=torch.uint8, device=r.device)
+        stream = torch.cuda.current_stream(r.device).cuda_stream
+        _check(self.ctx.handle, _lib.load().vt_tlas_trace_any(self.ctx.handle, self._p, r.data_ptr(), n, occ.data_ptr(),
+                                                              stream), "vt_tlas_trace_any")
+        return occ.cpu().numpy() if host else occ
+
+    def flatten(self, *, leaf_size: int = 2, treelet_size: int = 7, refine_rounds: int = 2, max_depth: int = 31) -> Mesh:
+        """One world-space Mesh of all instances' triangles (rendered face = rendered_base + face)."""
+        opts = BuildOptions(leaf_size, treelet_size, refine_rounds, max_depth)
+        p = C.c_void_p()
+        _check(self.ctx.handle, _lib.load().vt_tlas_flatten(self.ctx.handle, self._p, C.byref(opts), C.byref(p)),
+               "vt_tlas_flatten")
+        return Mesh._adopt(self.ctx, p)
+
+    def close(self) -> None:
+        if getattr(self, "_p", None) is not None and self.ctx._p is not None:
+            _lib.load().vt_tlas_destroy(self.ctx.handle, self._p)
         self._p = None
 
     def __del__(self):

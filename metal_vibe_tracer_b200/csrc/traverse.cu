@@ -21,92 +21,6 @@
 namespace {
 using namespace vtd;
 
-// Single-ray traversals in the persistent kernels' order (leaf children pushed as stack entries,
-// near entries popped first), counting node visits and triangle tests when kCount.
-
-template <bool kCount>
-__device__ __forceinline__ bool trace_closest(const float4 *__restrict__ nodes,
-                                              const float4 *__restrict__ tris, float rootMax,
-                                              float4 r0, float4 r1, float &best, float &hb1,
-                                              float &hb2, int &prim, uint32_t &nv, uint32_t &nt) {
-  const WRay wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-  const QRay qr = make_qray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
-  const float tMin = r0.w;
-  float closest = r1.w;
-  bool found = false;
-  int stack[kStack];
-  int top = 0;
-  stack[top++] = 0;
-  while (top > 0) {
-    const int entry = stack[--top];
-    if (entry < 0) {
-      int first, cnt;
-      leaf_range(nodes, entry, first, cnt);
-      for (int q = 0; q < cnt; ++q) {
-        const float4 *tp = tris + 3 * (size_t)(first + q);
-        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
-        float t, b1, b2;
-        if (kCount) ++nt;
-        if (!intersect_tri(wr, a, b, cc, tMin, closest, t, b1, b2)) continue;
-        closest = t; hb1 = b1; hb2 = b2; prim = __float_as_int(a.w); found = true;
-      }
-      continue;
-    }
-    QNode nd;
-    load_qnode(nodes, entry, nd);
-    if (kCount) ++nv;
-    float nearT[4];
-    const int mask = qnode_hits(nd, qr, tMin, closest, nearT);
-    const Sorted4 o = sort_qchildren(nd, mask, nearT);
-#pragma unroll
-    for (int j = 3; j >= 0; --j) {
-      if (j >= o.m || beyond(o.key[j], closest) || top >= kStack) continue;
-      stack[top++] = o.child[j] > 0 ? o.child[j] : leaf_entry_of(entry, (int)(o.key[j] & 3u));
-    }
-  }
-  best = closest;
-  return found;
-}
-
-template <bool kCount>
-__device__ __forceinline__ bool trace_any(const float4 *__restrict__ nodes,
-                                          const float4 *__restrict__ tris, float rootMax, float4 r0,
-                                          float4 r1, uint32_t &nv, uint32_t &nt) {
-  const WRay wr = make_wray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-  const QRay qr = make_qray(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, rootMax);
-  const float tMin = r0.w, tMax = r1.w;
-  int stack[kStack];
-  int top = 0;
-  stack[top++] = 0;
-  while (top > 0) {
-    const int entry = stack[--top];
-    if (entry < 0) {
-      int first, cnt;
-      leaf_range(nodes, entry, first, cnt);
-      for (int q = 0; q < cnt; ++q) {
-        const float4 *tp = tris + 3 * (size_t)(first + q);
-        const float4 a = __ldg(tp), b = __ldg(tp + 1), cc = __ldg(tp + 2);
-        float t, b1, b2;
-        if (kCount) ++nt;
-        if (intersect_tri(wr, a, b, cc, tMin, tMax, t, b1, b2)) return true;
-      }
-      continue;
-    }
-    QNode nd;
-    load_qnode(nodes, entry, nd);
-    if (kCount) ++nv;
-    float nearT[4];
-    const int mask = qnode_hits(nd, qr, tMin, tMax, nearT);
-#pragma unroll
-    for (int k = 3; k >= 0; --k) {
-      if (!(mask >> k & 1) || top >= kStack) continue;
-      const int c = i4(nd.child, k);
-      stack[top++] = c > 0 ? c : leaf_entry_of(entry, k);
-    }
-  }
-  return false;
-}
-
 // ---- persistent traversal -----------------------------------------------------------------------
 // Rays vary a lot in length (65 node visits on average for the incoherent set, with a long tail), so
 // a thread-per-ray grid leaves most lanes of a warp idle while its longest ray finishes.

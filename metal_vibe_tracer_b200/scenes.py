@@ -528,6 +528,70 @@ def production_scene(seed: int = 0, triangles: int = 10_000_000, emitters: int =
     return faces, verts, mats, camera
 
 
+def displaced_sphere_asset(subdivisions: int, seed: int, displace: float = 0.05):
+    """One displaced icosphere in object space (radius 1 before displacement): the grid scenes'
+    displacement (sphere_grid) with the noise seeded by `seed`. Returns faces (tag 0) and vertices."""
+    unit, tri = _unit_icosphere(subdivisions)
+    V = len(unit)
+    scale = 1.0 + displace * (2.0 * _lattice_noise(unit, np.array([seed]))[0] - 1.0)
+    local = unit * scale[:, None]
+    fn = np.cross(local[tri[:, 1]] - local[tri[:, 0]], local[tri[:, 2]] - local[tri[:, 0]])
+    vn = np.zeros_like(local)
+    for c in range(3):
+        for ax in range(3):
+            vn[:, ax] += np.bincount(tri[:, c], weights=fn[:, ax], minlength=V)
+    vn /= np.linalg.norm(vn, axis=1, keepdims=True)
+    verts = np.zeros(V, VERTEX_DTYPE)
+    verts["p"] = local.astype(np.float32)
+    verts["n"] = vn.astype(np.float32)
+    faces = np.zeros(len(tri), FACE_DTYPE)
+    faces["a"], faces["b"], faces["c"] = tri[:, 0], tri[:, 1], tri[:, 2]
+    return faces, verts
+
+
+def instanced_grid(grid: int = 32, assets: int = 16, subdivisions: int = 5, seed: int = 0, displace: float = 0.05,
+                   nmat: int = 287, emissive_every: int = 10, mirrored_fraction: float = 0.1):
+    """The instanced grid scene: a grid x grid lattice of instances of `assets` displaced icospheres
+    (subdivision `subdivisions`, per-vertex noise displacement `displace`), each instance turned by a
+    random angle about y, scaled by 0.4 u (u uniform in [0.8, 1.2]) and, for `mirrored_fraction` of
+    them, mirrored in x; plus a ground quad (its own mesh, one instance). Instance k's faces take slot
+    k % nmat (OPENPBR, as production_scene's), every `emissive_every`-th instance an emissive slot
+    (radiance 4, 8 or 12). Returns (meshes [(faces, verts)], transforms (n, 3, 4), mesh index per
+    instance, slot base per instance, materials, camera)."""
+    rng = np.random.default_rng(seed)
+    meshes = [displaced_sphere_asset(subdivisions, seed * 7919 + a, displace) for a in range(assets)]
+    half = grid / 2.0 + 1.0
+    ground = np.zeros(4, VERTEX_DTYPE)
+    ground["p"] = np.array([(-half, 0.0, -half), (half, 0.0, -half), (half, 0.0, half), (-half, 0.0, half)], np.float32)
+    ground["n"] = (0.0, 1.0, 0.0)
+    gf = np.zeros(2, FACE_DTYPE)
+    gf["a"], gf["b"], gf["c"] = (0, 0), (2, 3), (1, 2)
+    meshes.append((gf, ground))
+    n = grid * grid
+    k = np.arange(n)
+    cx, cz = k // grid - (grid - 1) / 2.0, k % grid - (grid - 1) / 2.0
+    theta = rng.uniform(0.0, 2.0 * np.pi, n)
+    sc = 0.4 * rng.uniform(0.8, 1.2, n)
+    mirror = np.where(rng.random(n) < mirrored_fraction, -1.0, 1.0)
+    c, s_ = np.cos(theta), np.sin(theta)
+    T = np.zeros((n + 1, 3, 4))
+    T[:n, 0, 0], T[:n, 0, 2] = c * sc * mirror, s_ * sc
+    T[:n, 1, 1] = sc
+    T[:n, 2, 0], T[:n, 2, 2] = -s_ * sc * mirror, c * sc
+    T[:n, 0, 3], T[:n, 1, 3], T[:n, 2, 3] = cx, 0.45, cz
+    T[n, 0, 0] = T[n, 1, 1] = T[n, 2, 2] = 1.0
+    mesh_of = np.concatenate([rng.integers(0, assets, n), [assets]]).astype(np.uint32)
+    emissive = (k % max(emissive_every, 1)) == emissive_every // 2
+    slots = np.concatenate([np.where(emissive, nmat + k % 3, k % nmat), [0]]).astype(np.uint32)
+    mats = [{"type": 4, "albedo": tuple(float(x) for x in rng.random(3)), "emission": (0.0, 0.0, 0.0),
+             "roughness": float(rng.random()), "metalness": 1.0 if rng.random() < 0.3 else 0.0,
+             "ior": float(1.3 + 0.5 * rng.random())} for _ in range(nmat)]
+    mats += [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (float(e),) * 3} for e in (4.0, 8.0, 12.0)]
+    d = max(2.0, 0.9 * grid)
+    camera = {"pos": (0.0, 0.8 * d, -1.2 * d), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 45.0}
+    return meshes, T.astype(np.float32), mesh_of, slots, mats, camera
+
+
 def batch_workload(count: int = 64, seed: int = 0, lo: int = 10_000, hi: int = 2_000_000):
     """Config C4's scene list: per scene (triangles log-uniform in [lo, hi], resolution from
     {256, 512, 1024} squared, spp uniform in 4..64), seeded."""

@@ -836,11 +836,13 @@ template <typename T> struct SlabRay {
   bool parallel[3];
 };
 
-template <typename T> SlabRay<T> make_slab(const TraceRay<T> &r, T rootMax) {
+template <typename T> T max_abs_origin(const TraceRay<T> &r) {
+  return std::fmax(std::fmax(std::fabs(r.o[0]), std::fabs(r.o[1])), std::fabs(r.o[2]));
+}
+
+// The slab ray with origin shift e.
+template <typename T> SlabRay<T> make_slab_e(const TraceRay<T> &r, T e) {
   SlabRay<T> s;
-  T om = std::fmax(std::fmax(std::fabs(r.o[0]), std::fabs(r.o[1])), std::fabs(r.o[2]));
-  // fp64 needs no enlargement for its own rounding but keeps the fp32 one (it is conservative).
-  T e = T(1.1920929e-6) * (om + rootMax);
   for (int k = 0; k < 3; ++k) {
     s.low[k] = r.o[k] + e;
     s.high[k] = r.o[k] - e;
@@ -855,6 +857,11 @@ template <typename T> SlabRay<T> make_slab(const TraceRay<T> &r, T rootMax) {
     }
   }
   return s;
+}
+
+template <typename T> SlabRay<T> make_slab(const TraceRay<T> &r, T rootMax) {
+  // fp64 needs no enlargement for its own rounding but keeps the fp32 one (it is conservative).
+  return make_slab_e(r, T(1.1920929e-6) * (max_abs_origin(r) + rootMax));
 }
 
 inline uint32_t ord32(float f) {
@@ -1198,6 +1205,93 @@ bool any_hit(const vto_bvh &h, const TraceRay<T> &r, uint64_t *nodes = nullptr, 
   return false;
 }
 
+// ---- two-level traversal (mesh_closest / mesh_occluded, main.swift:1840-1984) ----------------------
+// The TLAS (128-byte nodes whose leaves name instances: -(instance + 1)) with boxes grown per ray by
+// grow (max|origin| + reach); each instance traced in object space with instance_ray
+// (main.swift:1634-1637), the direction not renormalised. fp32: the CUDA kernel's order and
+// arithmetic (o'_r = fma(l.z, o.z, fma(l.y, o.y, l.x o.x)) + l.w; quantised BLAS nodes); fp64: the
+// reference's form in double on the same float records.
+template <typename T> TraceRay<T> instance_ray(const vt_instance_record &I, const TraceRay<T> &r) {
+  TraceRay<T> o;
+  for (int a = 0; a < 3; ++a) {
+    const float *l = I.local + 4 * a;
+    if constexpr (std::is_same<T, float>::value) {
+      o.o[a] = std::fma(l[2], r.o[2], std::fma(l[1], r.o[1], l[0] * r.o[0])) + l[3];
+      o.d[a] = std::fma(l[2], r.d[2], std::fma(l[1], r.d[1], l[0] * r.d[0]));
+    } else {
+      o.o[a] = T(l[0]) * r.o[0] + T(l[1]) * r.o[1] + T(l[2]) * r.o[2] + T(l[3]);
+      o.d[a] = T(l[0]) * r.d[0] + T(l[1]) * r.d[1] + T(l[2]) * r.d[2];
+    }
+  }
+  o.tmin = r.tmin;
+  o.tmax = r.tmax;
+  return o;
+}
+
+struct TlasView {
+  const vt_wide_node *nodes;
+  const vt_instance_record *inst;
+  const vto_bvh *const *meshes;
+  float grow, reach;
+};
+
+template <typename T>
+bool tlas_closest(const TlasView &V, const TraceRay<T> &r, T &best, int &prim, uint32_t &inst, T &hb1, T &hb2) {
+  const SlabRay<T> s = make_slab_e(r, T(V.grow) * (max_abs_origin(r) + T(V.reach)));
+  T closest = r.tmax;
+  bool found = false;
+  int stack[32];
+  int top = 0;
+  stack[top++] = 0;
+  while (top > 0) {
+    const vt_wide_node &nd = V.nodes[stack[--top]];
+    T nearT[4];
+    const int mask = node_hits(nd, s, r.tmin, closest, nearT);
+    const ChildOrder<T> co(mask, nearT);
+    for (int j = 0; j < co.m; ++j) {
+      const int k = co.order[j];
+      if (nd.child[k] > 0 || co.beyond(j, closest)) continue;
+      const uint32_t i = (uint32_t)(-nd.child[k] - 1);
+      const vt_instance_record &I = V.inst[i];
+      TraceRay<T> lr = instance_ray(I, r);
+      lr.tmax = closest;
+      T t, b1 = 0, b2 = 0;
+      int p = -1;
+      if (closest_hit<T>(*V.meshes[I.mesh], lr, t, p, b1, b2)) {
+        closest = t; prim = p; inst = i; hb1 = b1; hb2 = b2; found = true;
+      }
+    }
+    for (int j = co.m - 1; j >= 0; --j) {
+      const int k = co.order[j];
+      if (nd.child[k] > 0 && !co.beyond(j, closest) && top < 32) stack[top++] = nd.child[k];
+    }
+  }
+  best = closest;
+  return found;
+}
+
+template <typename T> bool tlas_any(const TlasView &V, const TraceRay<T> &r) {
+  const SlabRay<T> s = make_slab_e(r, T(V.grow) * (max_abs_origin(r) + T(V.reach)));
+  int stack[32];
+  int top = 0;
+  stack[top++] = 0;
+  while (top > 0) {
+    const vt_wide_node &nd = V.nodes[stack[--top]];
+    T nearT[4];
+    const int mask = node_hits(nd, s, r.tmin, r.tmax, nearT);
+    for (int k = 0; k < 4; ++k) {
+      if (!(mask >> k & 1)) continue;
+      if (nd.child[k] > 0) {
+        if (top < 32) stack[top++] = nd.child[k];
+        continue;
+      }
+      const vt_instance_record &I = V.inst[-nd.child[k] - 1];
+      if (any_hit<T>(*V.meshes[I.mesh], instance_ray(I, r))) return true;
+    }
+  }
+  return false;
+}
+
 template <typename T> TraceRay<T> load_ray(const vt_ray &r) {
   TraceRay<T> x;
   x.o[0] = r.ox; x.o[1] = r.oy; x.o[2] = r.oz;
@@ -1281,6 +1375,31 @@ void vto_brute_closest(const vt_face *faces, uint32_t nfaces, const vt_vertex *v
       }
     }
     hits[i] = out;
+  });
+}
+
+void vto_tlas_trace(const vt_wide_node *nodes, const vt_instance_record *inst, const vto_bvh *const *meshes,
+                    float grow, float reach, const vt_ray *rays, uint32_t n, vt_hit *hits, uint32_t *instances,
+                    uint8_t *occluded, int32_t closest, int32_t precision, int32_t threads) {
+  const TlasView V{nodes, inst, meshes, grow, reach};
+  parallel_for(n, threads, [&](uint32_t i) {
+    if (!closest) {
+      const bool hit = precision == 64 ? tlas_any<double>(V, load_ray<double>(rays[i])) : tlas_any<float>(V, load_ray<float>(rays[i]));
+      occluded[i] = hit ? 1 : 0;
+      return;
+    }
+    vt_hit out{0.0f, 0.0f, 0.0f, -1};
+    int prim = -1;
+    uint32_t k = 0xffffffffu;
+    if (precision == 64) {
+      double t, b1 = 0, b2 = 0;
+      if (tlas_closest<double>(V, load_ray<double>(rays[i]), t, prim, k, b1, b2)) out = {float(t), float(b1), float(b2), prim};
+    } else {
+      float t, b1 = 0, b2 = 0;
+      if (tlas_closest<float>(V, load_ray<float>(rays[i]), t, prim, k, b1, b2)) out = {t, b1, b2, prim};
+    }
+    hits[i] = out;
+    if (instances) instances[i] = out.prim >= 0 ? k : 0xffffffffu;
   });
 }
 

@@ -68,6 +68,12 @@ void vto_trace_any(const vto_bvh *h, const vt_ray *rays, uint32_t n, uint8_t *oc
 void vto_brute_closest(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
                        const vt_ray *rays, uint32_t n, vt_hit *hits, int32_t precision,
                        int32_t threads);
+/* Two-level traversal (mesh_closest / mesh_occluded, main.swift:1840-1984): TLAS nodes whose leaves
+ * name instances, the instance records and each record's mesh (meshes[record.mesh]); closest = 1
+ * writes hits and (if non-null) instances, 0 writes occluded. precision 32 or 64 as above. */
+void vto_tlas_trace(const vt_wide_node *nodes, const vt_instance_record *inst, const vto_bvh *const *meshes,
+                    float grow, float reach, const vt_ray *rays, uint32_t n, vt_hit *hits, uint32_t *instances,
+                    uint8_t *occluded, int32_t closest, int32_t precision, int32_t threads);
 /* Traversal statistics of closest (1) or any-hit (0) traversal, fp32 order. */
 void vto_trace_count(const vto_bvh *h, const vt_ray *rays, uint32_t n, int32_t closest,
                      uint64_t *nodes_visited, uint64_t *tris_tested, int32_t threads);

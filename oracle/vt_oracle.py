@@ -50,6 +50,7 @@ _SIGS = {
     "vto_trace_any": (None, [_P, _P, _U32, _P, _I32, _I32]),
     "vto_brute_closest": (None, [_P, _U32, _P, _P, _U32, _P, _I32, _I32]),
     "vto_trace_count": (None, [_P, _P, _U32, _I32, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _I32]),
+    "vto_tlas_trace": (None, [_P, _P, _P, C.c_float, C.c_float, _P, _U32, _P, _P, _P, _I32, _I32, _I32]),
 }
 
 _lib = None
@@ -199,6 +200,23 @@ class Bvh:
         load().vto_trace_count(self._h, r.ctypes.data, r.shape[0], 1 if closest else 0, C.byref(a), C.byref(b),
                                nthreads or threads())
         return int(a.value), int(b.value)
+
+
+def tlas_trace(nodes, records, meshes, grow, reach, rays, closest=True, precision=32, nthreads=None):
+    """Two-level traversal over oracle meshes (Bvh), the TLAS nodes and instance records of a vt_tlas:
+    (hits, instances) for closest, else occluded flags."""
+    r = _rays(rays)
+    nodes = np.ascontiguousarray(nodes, WIDE_NODE_DTYPE)
+    records = np.ascontiguousarray(records)
+    handles = (C.c_void_p * len(meshes))(*[m._h for m in meshes])
+    n = r.shape[0]
+    hits = np.empty(n, HIT_DTYPE)
+    inst = np.empty(n, np.uint32)
+    occ = np.empty(n, np.uint8)
+    load().vto_tlas_trace(nodes.ctypes.data, records.ctypes.data, handles, C.c_float(grow), C.c_float(reach),
+                          r.ctypes.data, n, hits.ctypes.data, inst.ctypes.data, occ.ctypes.data, 1 if closest else 0,
+                          precision, nthreads or threads())
+    return (hits, inst) if closest else occ
 
 
 def brute_closest(faces, verts, rays, precision=32, nthreads=None):
