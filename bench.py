@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--production-arms", default="restir_di_32,mis,mis_wavefront",
                    help="production scene's measured arms (profiling runs)")
     p.add_argument("--c5", type=int, default=1, help="1: measure config C5 (the cache on the production scene)")
+    p.add_argument("--instanced-grid", type=int, default=32, help="instances per side of the instanced grid (0: skip)")
     p.add_argument("--c5-stride", type=int, default=8, help="pixel stride of C5's FP64 reference and relMSE")
     p.add_argument("--c5-ref-spp", type=int, default=65536, help="spp of C5's FP64 reference")
     p.add_argument("--c5-ref-file", default="", help="resume/save C5's reference accumulation (.npz)")
@@ -458,6 +459,92 @@ def bench_production(a, ctx, stream) -> dict:
     return out
 
 
+def bench_instanced(a, ctx, stream) -> dict:
+    """The instanced grid: 32 x 32 instances of 16 displaced subdivision-5 icospheres (20,480 triangles
+    each; turned, scaled, 10 % mirrored) and a ground quad, 20.97M rendered triangles from 327,682
+    stored, 5 emissive instances (102,400 emissive triangles). The TLAS build, closest-hit Mrays/s
+    through the two levels and through the flattened mesh (vt_tlas_flatten) on the 1920 x 1080 camera
+    rays and on 4M rays from random points of the grid's bounds in random directions, and one MIS
+    wavefront frame (1080p, spectral, depth 12) of the flattened scene."""
+    import torch
+
+    import metal_vibe_tracer_b200 as vt
+    from metal_vibe_tracer_b200 import scenes, spectral_tables
+
+    g = a.instanced_grid
+    meshes, T, mesh_of, slots, mats, cam = scenes.instanced_grid(grid=g, assets=16, subdivisions=5, seed=0,
+                                                                 emissive_every=max(1, (g * g) // 5))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gm = [vt.Mesh(ctx, f, v) for f, v in meshes]
+    t0 = time.perf_counter()
+    tlas = vt.Tlas(ctx, gm, vt.instances_array(T, mesh_of, slots))
+    tlas_s = time.perf_counter() - t0
+    ti = tlas.info()
+    t0 = time.perf_counter()
+    flat = tlas.flatten()
+    flat_s = time.perf_counter() - t0
+    fi = flat.info()
+    W, H = 1920, 1080
+    cam_rays = scenes.camera_rays_torch(cam, W, H, dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    lo = torch.tensor(list(ti.lo), device=dev)
+    hi = torch.tensor(list(ti.hi), device=dev)
+    n_inc = 1 << 22
+    inc = torch.zeros((n_inc, 8), device=dev)
+    inc[:, 0:3] = lo + (hi - lo) * torch.rand((n_inc, 3), generator=gen, device=dev)
+    d = torch.randn((n_inc, 3), generator=gen, device=dev)
+    inc[:, 4:7] = d / d.norm(dim=1, keepdim=True)
+    inc[:, 7] = float("inf")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hits = torch.empty((max(cam_rays.shape[0], n_inc), 4), device=dev)
+    insts = torch.empty((max(cam_rays.shape[0], n_inc),), dtype=torch.int32, device=dev)
+    lib = vt.load()
+    cs = torch.cuda.current_stream(dev).cuda_stream
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": "instanced grid: %dx%d instances of 16 displaced subdivision-5 icospheres + ground, %d rendered "
+                       "triangles from %d stored" % (g, g, ti.rendered_triangles, sum(len(f) for f, _ in meshes)),
+           "tlas": {"instances": ti.instances, "nodes": ti.nodes, "depth": ti.depth, "build_ms": ti.build_ms,
+                    "build_wall_s": tlas_s},
+           "flattened": {"faces": fi.faces, "wide_nodes": fi.wide_nodes, "build_ms": fi.build_ms, "flatten_wall_s": flat_s}}
+    for name, rays in (("camera_1080p", cam_rays), ("random_4m", inc)):
+        n = rays.shape[0]
+        def two_level():
+            st = lib.vt_tlas_trace_closest(ctx.handle, tlas._p, rays.data_ptr(), n, hits.data_ptr(), insts.data_ptr(), cs)
+            assert st == 0, vt.load().vt_last_error(ctx.handle)
+        ms_tl = timed(two_level)
+        ms_fl = timed(lambda: flat.closest(rays, hits[:n]))
+        out[name] = {"rays": n, "two_level_mrays_s": n / ms_tl / 1e3, "flattened_mrays_s": n / ms_fl / 1e3}
+    # One frame of the flattened scene through the wavefront integrator.
+    scene = vt.Scene(ctx, flat, mats, None, spectral_tables.load())
+    for f in range(2):
+        scene.render_wavefront(vt.make_params(cam, W, H, 12, 1 + f, True, 1), 1, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    frames = 4
+    for f in range(frames):
+        scene.render_wavefront(vt.make_params(cam, W, H, 12, 3 + f, True, 1), 1, stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out["mis_wavefront_ms_per_frame"] = e0.elapsed_time(e1) / frames
+    scene.close()
+    flat.close()
+    tlas.close()
+    for m in gm:
+        m.close()
+    return out
+
+
 def bench_nrc_c5(a, ctx, stream) -> dict:
     """Config C5: the radiance cache on the production scene (9.9M triangles, 102k emitters under a
     light tree, 287 OPENPBR slots) at 1920x1080, spectral, depth 12, against plain MIS path tracing
@@ -816,6 +903,9 @@ def main():
     batched = None
     if world == 1 and not a.no_cornell and a.batch_scenes > 0:
         batched = bench_batch(a, ctx)
+    instanced = None
+    if world == 1 and not a.no_cornell and a.instanced_grid > 0:
+        instanced = bench_instanced(a, ctx, stream)
     c5 = None
     if world == 1 and not a.no_cornell and a.c5:
         c5 = bench_nrc_c5(a, ctx, stream)
@@ -836,6 +926,7 @@ def main():
             "cornell_pt": cornell,
             "production_scene": production,
             "batched_scenes": batched,
+            "instanced_grid": instanced,
             "nrc_c5": c5,
         }
         print(json.dumps(line))

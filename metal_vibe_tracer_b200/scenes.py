@@ -114,6 +114,31 @@ def coherent_rays_torch(width: int, height: int, device, fov_deg: float = 45.0):
     return out
 
 
+def camera_rays_torch(camera: dict, width: int, height: int, device):
+    """Pinhole rays (n, 8) float32 through the pixel centres of a look-at camera dict (pos, target,
+    up, fov in degrees), tmax infinite."""
+    import torch
+    eye = torch.tensor(camera["pos"], dtype=torch.float64, device=device)
+    fwd = torch.tensor(camera["target"], dtype=torch.float64, device=device) - eye
+    fwd = fwd / fwd.norm()
+    right = torch.linalg.cross(fwd, torch.tensor(camera["up"], dtype=torch.float64, device=device))
+    right = right / right.norm()
+    up = torch.linalg.cross(right, fwd)
+    th = math.tan(math.radians(camera["fov"]) * 0.5)
+    ys, xs = torch.meshgrid(torch.arange(height, device=device, dtype=torch.float64),
+                            torch.arange(width, device=device, dtype=torch.float64), indexing="ij")
+    u = ((2.0 * (xs.reshape(-1) + 0.5) / width - 1.0) * th * width / height)[:, None]
+    v = ((1.0 - 2.0 * (ys.reshape(-1) + 0.5) / height) * th)[:, None]
+    d = fwd[None, :] + u * right[None, :] + v * up[None, :]
+    d = d / d.norm(dim=1, keepdim=True)
+    out = torch.empty((d.shape[0], 8), dtype=torch.float32, device=device)
+    out[:, 0:3] = eye.float()
+    out[:, 3] = 0.0
+    out[:, 4:7] = d.float()
+    out[:, 7] = float("inf")
+    return out
+
+
 def incoherent_rays_torch(n: int, device, seed: int = 1):
     import torch
     g = torch.Generator(device=device)
