@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--reference-spp", type=int, default=65536, help="spp of the FP64 reference image")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes in the batched-launch measurement (0: skip)")
     p.add_argument("--batch-passes", type=int, default=2, help="timed batched passes after the tuning passes")
+    p.add_argument("--batch-integrator", choices=["wavefront", "megakernel"], default="wavefront",
+                   help="batched scenes through per-scene wavefront queues or the persistent megakernel")
     p.add_argument("--production-frames", type=int, default=8, help="timed frames of the production scene (0: skip)")
     p.add_argument("--nrc-pretrain", type=int, default=32, help="training-only frames of the radiance cache, timed")
     p.add_argument("--nrc-max-spp", type=int, default=4096, help="spp cap of the radiance cache's relMSE runs")
@@ -362,9 +364,11 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
 
 def bench_batch(a, ctx) -> dict:
     """Batched scenes: `batch_scenes` grid scenes (triangles log-uniform in 10k-2M, resolutions from
-    {256, 512, 1024} squared, 4-64 spp) rendered by one persistent launch per pass. The first six
-    passes try launch shapes (block size x work-grab size); the timed passes replay the captured CUDA
-    graph of the fastest. Reports aggregate paths/s and the per-scene completion latency."""
+    {256, 512, 1024} squared, 4-64 spp). Wavefront (default): each pass runs every scene through its own
+    wavefront queues, the scenes spread over four streams; the first passes try queue size x block size
+    x compaction frequency. Megakernel: one persistent launch per pass; the first six passes try launch
+    shapes, then a captured CUDA graph replays the fastest. Reports aggregate paths/s and the per-scene
+    completion latency."""
     import metal_vibe_tracer_b200 as vt
     from metal_vibe_tracer_b200 import scenes
     from metal_vibe_tracer_b200.render import Batch
@@ -381,21 +385,33 @@ def bench_batch(a, ctx) -> dict:
         spp.append(n)
     setup_s = time.perf_counter() - t0
     batch = Batch(ctx, members, params, spp)
+    wave = a.batch_integrator == "wavefront"
+    run = batch.render_wavefront if wave else batch.render
     tune = []
     while batch.stats()[0].tuned == 0:
-        tune.append(batch.render())
-    timed = [batch.render() for _ in range(a.batch_passes)]
+        tune.append(run())
+    timed = [run() for _ in range(a.batch_passes)]
     st, scene_ms = batch.stats()
     paths = sum(p.width * p.height * n for p, n in zip(params, spp))
     ms = sum(timed) / len(timed)
+    if wave:
+        # Per scene and wavefront pass: generate, (depth + 1) x (extend, shade, shadow), finish.
+        depth = 8
+        launches = sum(-(-n // max(1, st.queue_paths // (p.width * p.height))) * (2 + 3 * (depth + 1))
+                       for p, n in zip(params, spp))
+        chosen = {"integrator": "wavefront", "queue_paths": st.queue_paths, "block": st.block,
+                  "compact_every": st.compact_every, "streams": st.streams}
+    else:
+        launches = 2
+        chosen = {"integrator": "megakernel", "block": st.block, "chunk": st.chunk}
     out = {"workload": "%d grid scenes (displaced icospheres, %.1fM triangles in all, imported emissive-triangle "
                        "lighting under light trees), resolutions 256/512/1024 squared, 4-64 spp, MIS, depth 8, RGB"
                        % (len(work), sum(w[0] for w in work) / 1e6),
            "paths_per_pass": paths, "ms_per_pass": ms, "paths_per_s": paths / (ms / 1e3),
-           "tuning_ms": tune, "chosen": {"block": st.block, "chunk": st.chunk},
+           "tuning_ms": tune, "chosen": chosen,
            "scene_latency_ms": {"median": float(np.median(scene_ms)), "max": float(scene_ms.max()),
                                 "min": float(scene_ms.min())},
-           "gpu_launches_per_pass": 2, "setup_s": setup_s}
+           "gpu_launches_per_pass": launches, "setup_s": setup_s}
     batch.close()
     for sc in members:
         sc.close()

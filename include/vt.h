@@ -373,14 +373,27 @@ typedef struct vt_batch_info {
   uint32_t scenes, passes;
   unsigned long long items;   /* pixels per pass */
   float last_ms;              /* the last pass, device time */
-  uint32_t tuned;             /* 1 once the launch shape is chosen and captured */
-  uint32_t block, chunk;      /* the launch shape of the last pass */
-  uint32_t pad;
+  uint32_t tuned;             /* 1 once the launch shape is chosen (and, for the megakernel, captured) */
+  uint32_t block, chunk;      /* the launch shape of the last pass (chunk: megakernel items per grab) */
+  uint32_t wavefront;         /* 1: the batch renders through vt_batch_render_wavefront */
+  uint32_t queue_paths;       /* wavefront: paths per pass of a scene's queues */
+  uint32_t compact_every;     /* wavefront: the live queue is compacted on every n-th bounce */
+  uint32_t streams;           /* wavefront: streams the scenes are spread over */
 } vt_batch_info;
 vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_params *params, const uint32_t *spp,
                           uint32_t n, vt_batch **out);
 /* One pass; synchronises (it times the pass). */
 vt_status vt_batch_render(vt_ctx *ctx, vt_batch *batch, void *stream);
+/* One pass through the wavefront integrator instead (config C4's per-scene ray queues): each scene's
+ * spp[i] frames run as vt_render_wavefront's stages over its own queues, the scenes spread over four
+ * streams (longest first, each to the least loaded stream, one path-state buffer per stream) and the
+ * camera jitter computed on the device. The first passes try, one each, the queue size (1M or 4M
+ * paths per wavefront pass; only sizes that hold the largest frame), the stage kernels' block size
+ * (128 or 256) and the compaction frequency (every bounce, or every second bounce with ended paths
+ * kept in place); later passes use the fastest. Images equal vt_render's of the same frames (FP64
+ * summation order aside). A batch renders through one integrator: after a wavefront pass
+ * vt_batch_render refuses it, and the other way round. Synchronises (it times the pass). */
+vt_status vt_batch_render_wavefront(vt_ctx *ctx, vt_batch *batch, void *stream);
 /* Statistics of the last pass; scene_ms (n = scene count, may be NULL) receives each scene's
  * completion time from the pass's start, in ms. */
 vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *batch, vt_batch_info *out, double *scene_ms, uint32_t n);

@@ -85,7 +85,8 @@ assert C.sizeof(OpenPBRCase) == 80 and C.sizeof(OpenPBRResult) == 48
 
 class BatchStats(C.Structure):
     _fields_ = [("scenes", C.c_uint32), ("passes", C.c_uint32), ("items", C.c_ulonglong), ("last_ms", C.c_float),
-                ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("pad", C.c_uint32)]
+                ("tuned", C.c_uint32), ("block", C.c_uint32), ("chunk", C.c_uint32), ("wavefront", C.c_uint32),
+                ("queue_paths", C.c_uint32), ("compact_every", C.c_uint32), ("streams", C.c_uint32)]
 
 
 class Environment(C.Structure):
@@ -171,6 +172,7 @@ SIGNATURES = {
     "vt_scene_gi_weights": (_I32, [_P, _P, _P, _U32]),
     "vt_batch_create": (_I32, [_P, _P, _P, _P, _U32, C.POINTER(_P)]),
     "vt_batch_render": (_I32, [_P, _P, _P]),
+    "vt_batch_render_wavefront": (_I32, [_P, _P, _P]),
     "vt_batch_stats": (_I32, [_P, _P, C.POINTER(BatchStats), _P, _U32]),
     "vt_batch_destroy": (_I32, [_P, _P]),
     "vt_spectral_grid_build": (_I32, [_P, _P]),

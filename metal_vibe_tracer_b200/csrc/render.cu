@@ -1613,6 +1613,22 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
   }
 }
 
+// frameJitter on the device, with the host's float operations (no contraction).
+__device__ __forceinline__ float halton_d(uint32_t index, uint32_t base) {
+  uint32_t n = index;
+  float fraction = 1.0f, result = 0.0f;
+  while (n > 0) {
+    fraction = __fdiv_rn(fraction, float(base));
+    result = __fadd_rn(result, __fmul_rn(fraction, float(n % base)));
+    n /= base;
+  }
+  return result;
+}
+__device__ __forceinline__ float2 frame_jitter(uint32_t sampleIndex) {
+  const uint32_t n = (max(1u, sampleIndex) - 1u) % 1024u + 1u;
+  return make_float2(__fsub_rn(halton_d(n, 2u), 0.5f), __fsub_rn(halton_d(n, 3u), 0.5f));
+}
+
 // ---- wavefront integrator (vt_render_wavefront; sampling modes 1-3) ------------------------------
 // The paths of k_render / path_sample taken apart into stage kernels over queues of path indices,
 // with the path's state in HBM between them (WfArgs, structure of arrays). Per bounce b:
@@ -1629,7 +1645,8 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_render(RenderArg
 // entries land contiguously. k_wf_finish adds each path's radiance (primary NEE + continuation,
 // summed in k_render's order) to its pixel's FP64 accumulation.
 constexpr int kWfBlock = 256;
-constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u, kWfQueried = 16u;
+constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u, kWfQueried = 16u,
+                   kWfDead = 32u;
 
 struct WfArgs {
   float4 *T;      // throughput per lane
@@ -1650,6 +1667,9 @@ struct WfArgs {
   uint32_t *outQ, *outCount;      // live paths of the next bounce
   uint32_t *shQ, *shCount;        // shadow rays of this bounce
   uint32_t npix, paths, k0;       // accumulation pixels; paths of the pass; its first sample (of the call)
+  uint32_t compact;               // 1: this bounce compacts the live queue; 0: it keeps every entry in
+                                  // place (ended paths flagged kWfDead, their next ray empty)
+  uint32_t deadFlags;             // 1: some bounce of the pass keeps ended paths queued
 };
 // The cache's query slot of path i: sample k0 + i / npix of pixel i % npix (k_render's slots).
 __device__ __forceinline__ size_t wf_slot(const WfArgs &W, uint32_t i) { return (size_t)W.k0 * W.npix + i; }
@@ -1871,7 +1891,7 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(RenderArgs A, WfArgs W
     const uint32_t x = (p % A.OW) * A.stride, y = (p / A.OW) * A.stride;
     Sampler seed = pixel_sampler(x, y, A.W, A.first + k, A.zSampler != 0u, A.zModel, A.firstFrame + k);
     const float u = A.spectral ? wavelength_numbers(seed).x : 0.0f;
-    float3 dir0 = camera_dir(A, x, y, A.jitter[k]), o0 = A.cam;
+    float3 dir0 = camera_dir(A, x, y, A.jitter ? A.jitter[k] : frame_jitter(A.first + k)), o0 = A.cam;
     lens_ray(A, o0, dir0, seed);
     seed.state = pcg_hash(seed.state ^ 0x27d4eb2fu);  // decorrelate_shading_seed
     wf_set_ray(W.ray, i, o0, ray_tmin(A, o0), dir0, __int_as_float(0x7f800000));
@@ -1895,9 +1915,22 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, u
     uint32_t i = 0;
     if (q < n) {
       i = W.inQ ? W.inQ[q] : q;
-      wf_vertex<kPbr, kNrc>(A, W, i, bounce, next, shadow);
+      const bool dead = W.deadFlags && (W.meta[i].w & kWfDead);
+      if (!dead) {
+        wf_vertex<kPbr, kNrc>(A, W, i, bounce, next, shadow);
+        // A path that ends on a bounce without compaction stays queued: flagged, with an empty ray.
+        if (!next && !W.compact) {
+          W.meta[i].w |= kWfDead;
+          reinterpret_cast<float *>(W.ray + 2 * (size_t)i + 1)[3] = -1.0f;
+        }
+      }
     }
-    wf_push(next, i, W.outQ, W.outCount, sTotal, sBase);
+    if (W.compact) {
+      wf_push(next, i, W.outQ, W.outCount, sTotal, sBase);
+    } else {
+      if (q < n) W.outQ[q] = i;
+      if (q == 0) *W.outCount = n;
+    }
     wf_push(shadow, i, W.shQ, W.shCount, sTotal, sBase);
   }
 }
@@ -2091,22 +2124,6 @@ __global__ void k_nrc_resolve(RenderArgs A, const float4 *__restrict__ pred, uin
 }
 
 // ---- batched scenes: one persistent launch over many scenes (config C4) ---------------------------
-// frameJitter on the device, with the host's float operations (no contraction).
-__device__ __forceinline__ float halton_d(uint32_t index, uint32_t base) {
-  uint32_t n = index;
-  float fraction = 1.0f, result = 0.0f;
-  while (n > 0) {
-    fraction = __fdiv_rn(fraction, float(base));
-    result = __fadd_rn(result, __fmul_rn(fraction, float(n % base)));
-    n /= base;
-  }
-  return result;
-}
-__device__ __forceinline__ float2 frame_jitter(uint32_t sampleIndex) {
-  const uint32_t n = (max(1u, sampleIndex) - 1u) % 1024u + 1u;
-  return make_float2(__fsub_rn(halton_d(n, 2u), 0.5f), __fsub_rn(halton_d(n, 3u), 0.5f));
-}
-
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -2829,10 +2846,22 @@ size_t wf_carve(unsigned char *base, uint32_t cap, WfArgs &W, uint32_t **q0, uin
 
 vt_status nrc_finish(vt_ctx *ctx, vt_nrc *nrc, const RenderArgs &A, uint32_t spp, cudaStream_t s);
 
+// Launch settings of a wavefront render and where its state lives. The defaults are vt_render_wavefront's:
+// the scene's own state, up to 4M paths per pass, 256-thread stage blocks, compaction every bounce and the
+// frame jitter uploaded from the host. Batches give each stream its own state and tune the rest.
+struct WfRun {
+  unsigned char **state = nullptr;  // state buffer (null: the scene's own)
+  uint32_t *stateCap = nullptr;     // its capacity in paths
+  uint32_t maxPaths = kWfMaxPaths;  // queue size: paths per pass
+  int block = kWfBlock;             // stage kernels' block size (at most kWfBlock)
+  uint32_t compactEvery = 1;        // compact the live queue on every n-th bounce
+  bool deviceJitter = false;        // the camera jitter computed in k_wf_generate (no host upload)
+};
+
 // vt_render_wavefront, and with a cache (nrc not null, sampling mode 1) vt_render_nrc's rendering:
 // paths ending where the cache's query rule stops them, then the predictions and the resolve.
 vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, uint32_t spp, void *stream,
-                         vt_nrc *nrc = nullptr) {
+                         vt_nrc *nrc = nullptr, const WfRun &run = WfRun()) {
   if (p->sampling_mode == 0)
     return vt_fail(ctx, VT_ERR_INVALID, "the wavefront integrator renders sampling modes 1-3 (ReSTIR DI frames use vt_render)");
   {
@@ -2847,27 +2876,31 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
     if (st != VT_OK) return st;
   }
   if (spp == 0) return VT_OK;
-  if (spp > scene->jitter_cap) {
-    cudaFree(scene->d_jitter);
-    scene->d_jitter = nullptr;
-    VT_CUDA(ctx, cudaMalloc(&scene->d_jitter, spp * sizeof(float2)));
-    scene->jitter_cap = spp;
+  if (!run.deviceJitter) {
+    if (spp > scene->jitter_cap) {
+      cudaFree(scene->d_jitter);
+      scene->d_jitter = nullptr;
+      VT_CUDA(ctx, cudaMalloc(&scene->d_jitter, spp * sizeof(float2)));
+      scene->jitter_cap = spp;
+    }
+    std::vector<float2> jit(spp);
+    for (uint32_t k = 0; k < spp; ++k) {
+      const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
+      jit[k] = make_float2(halton(n, 2) - 0.5f, halton(n, 3) - 0.5f);
+    }
+    VT_CUDA(ctx, cudaMemcpyAsync(scene->d_jitter, jit.data(), spp * sizeof(float2), cudaMemcpyHostToDevice, s));
   }
-  std::vector<float2> jit(spp);
-  for (uint32_t k = 0; k < spp; ++k) {
-    const uint32_t n = (std::max(1u, p->first_sample + k) - 1u) % 1024u + 1u;
-    jit[k] = make_float2(halton(n, 2) - 0.5f, halton(n, 3) - 0.5f);
-  }
-  VT_CUDA(ctx, cudaMemcpyAsync(scene->d_jitter, jit.data(), spp * sizeof(float2), cudaMemcpyHostToDevice, s));
   if (mesh->nfaces == 0) { scene->samples += spp; return VT_OK; }
 
   RenderArgs A;
   fill_args(scene, p, spp, A);
-  A.jitter = scene->d_jitter;
+  A.jitter = run.deviceJitter ? nullptr : scene->d_jitter;
   A.status = ctx->d_status + 2;
   A.kernelId = 7;
   const uint32_t npix = A.OW * A.OH;
-  if (npix > kWfMaxPaths) return vt_fail(ctx, VT_ERR_LIMIT, "the wavefront integrator takes at most 4M pixels per frame");
+  const uint32_t maxPaths = std::min(run.maxPaths, kWfMaxPaths);
+  if (npix > maxPaths)
+    return vt_fail(ctx, VT_ERR_LIMIT, "the frame has more pixels than the wavefront queue holds (" + std::to_string(maxPaths) + ")");
   if (nrc) {
     const vt_status st = vt_nrc_reserve_queries(ctx, nrc, (size_t)npix * spp);
     if (st != VT_OK) return st;
@@ -2877,39 +2910,45 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
     A.nrcVertex = nrc->cfg.query_vertex;
     A.nrcSpread = nrc->cfg.spread;
   }
-  const uint32_t chunk = std::max(1u, std::min(spp, kWfMaxPaths / npix));
+  const uint32_t chunk = std::max(1u, std::min(spp, maxPaths / npix));
   const uint32_t cap = npix * chunk;
-  if (cap > scene->wf_cap) {
-    cudaFree(scene->d_wf);
-    scene->d_wf = nullptr;
-    scene->wf_cap = 0;
+  unsigned char **state = run.state ? run.state : &scene->d_wf;
+  uint32_t *stateCap = run.state ? run.stateCap : &scene->wf_cap;
+  if (cap > *stateCap) {
+    cudaFree(*state);
+    *state = nullptr;
+    *stateCap = 0;
     WfArgs probe;
     uint32_t *a, *b, *c;
     uint8_t *o;
     int4 *h;
     const size_t bytes = wf_carve(nullptr, cap, probe, &a, &b, &c, &o, &h);
-    VT_CUDA(ctx, cudaMalloc(&scene->d_wf, bytes));
-    scene->wf_cap = cap;
+    VT_CUDA(ctx, cudaMalloc(state, bytes));
+    *stateCap = cap;
   }
   WfArgs W;
   uint32_t *q[2], *counts;
   uint8_t *occ;
   int4 *hit;
-  wf_carve(scene->d_wf, scene->wf_cap, W, &q[0], &q[1], &counts, &occ, &hit);
+  wf_carve(*state, *stateCap, W, &q[0], &q[1], &counts, &occ, &hit);
   W.hit = hit;
   W.occ = occ;
   W.npix = npix;
+  const uint32_t every = std::max(1u, run.compactEvery);
+  W.deadFlags = every > 1u ? 1u : 0u;
+  const int block = std::max(32, std::min(run.block, kWfBlock));
   const bool pbr = A.pbr != nullptr;
-  const uint32_t gridMax = (uint32_t)ctx->sm_count * 8u;
+  const uint32_t gridMax = (uint32_t)ctx->sm_count * (8u * kWfBlock / (uint32_t)block);
   uint32_t *slot = vt_queue_slot(ctx);
   for (uint32_t k0 = 0; k0 < spp; k0 += chunk) {
     const uint32_t P = npix * std::min(chunk, spp - k0);
     W.paths = P;
     W.k0 = k0;
-    const uint32_t grid = std::min<uint32_t>((P + kWfBlock - 1) / kWfBlock, gridMax);
-    k_wf_generate<<<grid, kWfBlock, 0, s>>>(A, W);
+    const uint32_t grid = std::min<uint32_t>((P + block - 1) / block, gridMax);
+    k_wf_generate<<<grid, block, 0, s>>>(A, W);
     VT_CUDA(ctx, cudaGetLastError());
     for (uint32_t b = 0; b <= A.maxDepth; ++b) {
+      W.compact = ((b + 1u) % every == 0u || b == A.maxDepth) ? 1u : 0u;
       // Live queue of bounce b (all paths at b = 0), the next bounce's queue and the shadow queue.
       const uint32_t *inQ = b == 0 ? nullptr : q[b & 1u];
       const uint32_t *inCount = b == 0 ? nullptr : counts + (b & 1u);
@@ -2923,18 +2962,18 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
       vt_launch_closest(mesh, reinterpret_cast<const vt_ray *>(W.ray), P, reinterpret_cast<vt_hit *>(hit), ctx->sm_count,
                         slot, inQ, ctx->d_status + 1, s, inCount, true);
       if (nrc) {
-        if (pbr) k_wf_shade<true, true><<<grid, kWfBlock, 0, s>>>(A, W, b);
-        else k_wf_shade<false, true><<<grid, kWfBlock, 0, s>>>(A, W, b);
+        if (pbr) k_wf_shade<true, true><<<grid, block, 0, s>>>(A, W, b);
+        else k_wf_shade<false, true><<<grid, block, 0, s>>>(A, W, b);
       } else {
-        if (pbr) k_wf_shade<true, false><<<grid, kWfBlock, 0, s>>>(A, W, b);
-        else k_wf_shade<false, false><<<grid, kWfBlock, 0, s>>>(A, W, b);
+        if (pbr) k_wf_shade<true, false><<<grid, block, 0, s>>>(A, W, b);
+        else k_wf_shade<false, false><<<grid, block, 0, s>>>(A, W, b);
       }
       vt_launch_any(mesh, reinterpret_cast<const vt_ray *>(W.sray), P, occ, ctx->sm_count, slot, W.shQ, ctx->d_status + 1, s,
                     W.shCount, A.imported != 0u);
       VT_CUDA(ctx, cudaGetLastError());
     }
-    if (nrc) k_wf_finish<true><<<grid, kWfBlock, 0, s>>>(A, W);
-    else k_wf_finish<false><<<grid, kWfBlock, 0, s>>>(A, W);
+    if (nrc) k_wf_finish<true><<<grid, block, 0, s>>>(A, W);
+    else k_wf_finish<false><<<grid, block, 0, s>>>(A, W);
     VT_CUDA(ctx, cudaGetLastError());
   }
   if (nrc) {
@@ -3066,11 +3105,40 @@ struct vt_batch {
   float last_ms = 0.0f;
   uint32_t passes = 0;
   bool pbr = false;  // some scene has OPENPBR slots: the kernel variant with the OpenPBR code
+  int mode = 0;      // the integrator of the batch's passes: 0 none yet, 1 megakernel, 2 wavefront
+  // Wavefront passes (vt_batch_render_wavefront): per-scene queues on kStreams streams, each stream
+  // with its own path state; the scenes' frame parameters kept on the host and advanced per pass.
+  static constexpr int kStreams = 4;
+  struct WfConfig {
+    uint32_t queue;  // paths per wavefront pass
+    int block;       // stage kernels' block size
+    uint32_t every;  // compaction frequency (bounces)
+    float ms;
+  };
+  std::vector<vt_frame_params> params;
+  std::vector<WfConfig> wfConfigs;
+  size_t wfTried = 0;
+  int wfBest = -1;
+  cudaStream_t streams[kStreams] = {};
+  cudaEvent_t fork = nullptr, join[kStreams] = {};
+  unsigned char *state[kStreams] = {};
+  uint32_t stateCap[kStreams] = {};
+  std::vector<cudaEvent_t> sceneEv;
+  std::vector<int> streamOf;     // stream of each scene (longest-processing-time assignment)
+  std::vector<uint32_t> orderBy; // scenes by decreasing work
+  std::vector<double> sceneMs;   // completion of each scene from the pass's start (wavefront)
 };
 
 namespace {
 
 void batch_free(vt_batch *b) {
+  for (int k = 0; k < vt_batch::kStreams; ++k) {
+    if (b->streams[k]) cudaStreamDestroy(b->streams[k]);
+    if (b->join[k]) cudaEventDestroy(b->join[k]);
+    cudaFree(b->state[k]);
+  }
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (cudaEvent_t e : b->sceneEv) cudaEventDestroy(e);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->e0) cudaEventDestroy(b->e0);
@@ -3144,6 +3212,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     begin[i + 1] = begin[i] + (unsigned long long)params[i].width * params[i].height;
     b->scenes.push_back(scenes[i]);
     b->spp.push_back(spp[i]);
+    b->params.push_back(params[i]);
   }
   b->total = begin[n];
   auto fail = [&](cudaError_t e, const char *what) { batch_free(b); return vt_cuda_fail(ctx, e, what); };
@@ -3168,6 +3237,18 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
   // Launch shapes the first passes try, one each; the fastest is then captured in a graph.
   for (int block : {64, 128, 256})
     for (uint32_t chunk : {1u, 4u}) b->configs.push_back({block, chunk, 0.0f});
+  // Wavefront settings the first wavefront passes try, one each: queue size x block size x
+  // compaction frequency. Queues must hold the largest frame.
+  uint32_t maxPix = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t s = std::max(1u, params[i].pixel_stride);
+    maxPix = std::max(maxPix, ((params[i].width + s - 1) / s) * ((params[i].height + s - 1) / s));
+  }
+  for (uint32_t queue : {1u << 20, 1u << 22})
+    for (int block : {128, 256})
+      for (uint32_t every : {1u, 2u})
+        if (queue >= maxPix) b->wfConfigs.push_back({queue, block, every, 0.0f});
+  if (b->wfConfigs.empty()) b->wfConfigs.push_back({kWfMaxPaths, kWfBlock, 1u, 0.0f});
   *out = b;
   return VT_OK;
 }
@@ -3175,6 +3256,8 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
 vt_status vt_batch_render(vt_ctx *ctx, vt_batch *b, void *stream) {
   if (!ctx) return VT_ERR_INVALID;
   if (!b) return vt_fail(ctx, VT_ERR_INVALID, "batch is null");
+  if (b->mode == 2) return vt_fail(ctx, VT_ERR_INVALID, "this batch renders through the wavefront integrator");
+  b->mode = 1;
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   VT_CUDA(ctx, cudaEventRecord(b->e0, s));
@@ -3209,6 +3292,81 @@ vt_status vt_batch_render(vt_ctx *ctx, vt_batch *b, void *stream) {
   return VT_OK;
 }
 
+vt_status vt_batch_render_wavefront(vt_ctx *ctx, vt_batch *b, void *stream) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!b) return vt_fail(ctx, VT_ERR_INVALID, "batch is null");
+  if (b->mode == 1) return vt_fail(ctx, VT_ERR_INVALID, "this batch renders through the persistent megakernel");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const uint32_t n = (uint32_t)b->scenes.size();
+  if (b->mode == 0) {
+    b->mode = 2;
+    for (int k = 0; k < vt_batch::kStreams; ++k) {
+      VT_CUDA(ctx, cudaStreamCreateWithFlags(&b->streams[k], cudaStreamNonBlocking));
+      VT_CUDA(ctx, cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming));
+    }
+    VT_CUDA(ctx, cudaEventCreate(&b->fork));
+    b->sceneEv.assign(n, nullptr);
+    for (uint32_t i = 0; i < n; ++i) VT_CUDA(ctx, cudaEventCreate(&b->sceneEv[i]));
+    b->sceneMs.assign(n, 0.0);
+    // Longest processing time first: scenes by decreasing paths, each to the least loaded stream.
+    b->orderBy.resize(n);
+    for (uint32_t i = 0; i < n; ++i) b->orderBy[i] = i;
+    auto work = [&](uint32_t i) { return (double)b->params[i].width * b->params[i].height * b->spp[i]; };
+    std::stable_sort(b->orderBy.begin(), b->orderBy.end(), [&](uint32_t x, uint32_t y) { return work(x) > work(y); });
+    b->streamOf.assign(n, 0);
+    double load[vt_batch::kStreams] = {};
+    for (uint32_t i : b->orderBy) {
+      int k = 0;
+      for (int j = 1; j < vt_batch::kStreams; ++j)
+        if (load[j] < load[k]) k = j;
+      b->streamOf[i] = k;
+      load[k] += work(i);
+    }
+  }
+  const vt_batch::WfConfig &c = b->wfConfigs[b->wfBest >= 0 ? (size_t)b->wfBest : b->wfTried];
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  VT_CUDA(ctx, cudaEventRecord(b->fork, s));
+  for (int k = 0; k < vt_batch::kStreams; ++k) VT_CUDA(ctx, cudaStreamWaitEvent(b->streams[k], b->fork, 0));
+  for (uint32_t i : b->orderBy) {
+    const int k = b->streamOf[i];
+    WfRun run;
+    run.state = &b->state[k];
+    run.stateCap = &b->stateCap[k];
+    run.maxPaths = c.queue;
+    run.block = c.block;
+    run.compactEvery = c.every;
+    run.deviceJitter = true;
+    const vt_status st = wavefront_impl(ctx, b->scenes[i], &b->params[i], b->spp[i], b->streams[k], nullptr, run);
+    if (st != VT_OK) return st;
+    VT_CUDA(ctx, cudaEventRecord(b->sceneEv[i], b->streams[k]));
+    vt_frame_params &p = b->params[i];
+    p.first_sample += b->spp[i];
+    if (p.first_frame) p.first_frame += b->spp[i];
+  }
+  for (int k = 0; k < vt_batch::kStreams; ++k) {
+    VT_CUDA(ctx, cudaEventRecord(b->join[k], b->streams[k]));
+    VT_CUDA(ctx, cudaStreamWaitEvent(s, b->join[k], 0));
+  }
+  VT_CUDA(ctx, cudaEventRecord(b->e1, s));
+  VT_CUDA(ctx, cudaEventSynchronize(b->e1));
+  VT_CUDA(ctx, cudaEventElapsedTime(&b->last_ms, b->fork, b->e1));
+  for (uint32_t i = 0; i < n; ++i) {
+    float ms = 0.0f;
+    VT_CUDA(ctx, cudaEventElapsedTime(&ms, b->fork, b->sceneEv[i]));
+    b->sceneMs[i] = ms;
+  }
+  ++b->passes;
+  if (b->wfBest < 0) {
+    b->wfConfigs[b->wfTried].ms = b->last_ms;
+    if (++b->wfTried == b->wfConfigs.size()) {
+      b->wfBest = 0;
+      for (size_t k = 1; k < b->wfConfigs.size(); ++k)
+        if (b->wfConfigs[k].ms < b->wfConfigs[b->wfBest].ms) b->wfBest = (int)k;
+    }
+  }
+  return VT_OK;
+}
+
 vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *b, vt_batch_info *out, double *scene_ms, uint32_t n) {
   if (!ctx) return VT_ERR_INVALID;
   if (!b || !out) return vt_fail(ctx, VT_ERR_INVALID, "null argument");
@@ -3218,6 +3376,18 @@ vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *b, vt_batch_info *out, dou
   out->passes = b->passes;
   out->items = b->total;
   out->last_ms = b->last_ms;
+  if (b->mode == 2) {
+    out->wavefront = 1;
+    out->tuned = b->wfBest >= 0 ? 1u : 0u;
+    const vt_batch::WfConfig &c = b->wfConfigs[b->wfBest >= 0 ? (size_t)b->wfBest : (b->wfTried ? b->wfTried - 1 : 0)];
+    out->block = (uint32_t)c.block;
+    out->queue_paths = c.queue;
+    out->compact_every = c.every;
+    out->streams = vt_batch::kStreams;
+    if (scene_ms && b->passes)
+      for (size_t i = 0; i < b->scenes.size(); ++i) scene_ms[i] = b->sceneMs[i];
+    return VT_OK;
+  }
   out->tuned = b->best >= 0 ? 1u : 0u;
   const vt_batch::Config &c = b->configs[b->best >= 0 ? (size_t)b->best : (b->tried ? b->tried - 1 : 0)];
   out->block = (uint32_t)c.block;

@@ -302,6 +302,13 @@ class Batch:
         _check(self.ctx.handle, _lib.load().vt_batch_render(self.ctx.handle, self._p, stream), "vt_batch_render")
         return self.stats()[0].last_ms
 
+    def render_wavefront(self, stream=None) -> float:
+        """One pass through the wavefront integrator (per-scene queues on four streams); the first
+        passes try queue size x block size x compaction frequency. Returns its device time in ms."""
+        _check(self.ctx.handle, _lib.load().vt_batch_render_wavefront(self.ctx.handle, self._p, stream),
+               "vt_batch_render_wavefront")
+        return self.stats()[0].last_ms
+
     def stats(self):
         """(vt_batch_stats, per-scene completion ms of the last pass)."""
         st = _lib.BatchStats()

@@ -60,6 +60,42 @@ def test_batch_equals_single_renders(ctx):
         m.close()
 
 
+def test_batch_wavefront_equals_single_renders(ctx):
+    """vt_batch_render_wavefront: per-scene queues on four streams; the first eight passes try queue
+    size x block size x compaction frequency (every bounce, every second bounce with ended paths kept
+    in place), and every pass adds exactly the samples vt_render of the same frames adds."""
+    specs, meshes = scene_specs(ctx)
+    batch_scenes = [make() for make, _, _ in specs]
+    batch = Batch(ctx, batch_scenes, [p for _, p, _ in specs], [s for _, _, s in specs])
+    passes = 10
+    seen = set()
+    for k in range(passes):
+        ms_pass = batch.render_wavefront()
+        st, ms = batch.stats()
+        assert st.wavefront == 1 and st.streams == 4 and st.passes == k + 1
+        assert st.tuned == (1 if k >= 7 else 0)
+        seen.add((st.queue_paths, st.block, st.compact_every))
+        assert ms_pass > 0 and np.all(ms > 0) and np.all(ms <= ms_pass * 1.05 + 0.05), (ms, ms_pass)
+    assert len(seen) == 8
+    with pytest.raises(vt.MaterialLibraryError, match="wavefront"):
+        batch.render()
+    for scene, (make, params, spp) in zip(batch_scenes, specs):
+        img, n = scene.readback()
+        assert n == passes * spp
+        ref_scene = make()
+        ref_scene.render(params, passes * spp)
+        ref, m = ref_scene.readback()
+        ref_scene.close()
+        assert m == n
+        assert np.isfinite(img).all() and img.max() > 0
+        np.testing.assert_allclose(img, ref, rtol=1e-12, atol=1e-12)
+    batch.close()
+    for sc in batch_scenes:
+        sc.close()
+    for m in meshes:
+        m.close()
+
+
 def test_batch_rejects_bad_input(ctx):
     faces, verts, mats, light, cam = scenes.cornell_box()
     mesh = vt.Mesh(ctx, faces, verts)
