@@ -92,7 +92,7 @@ def test_temporal_reuse_survives_camera_motion_and_cuts_clear_it(ctx, cornell):
 
 def test_restir_gi_reservoirs_and_energy(ctx, cornell):
     """ReSTIR GI (main.swift:4718-4812, 7582-7656): with a scattering budget the diffuse primaries build
-    GI reservoirs (most with a sample after a few frames of temporal reuse), none at depth 1, and the
+    GI reservoirs (some merged with their history after a few frames of temporal reuse), none at depth 1, and the
     mode-0 image (DI + GI reservoirs, NEE skipped at the secondary diffuse vertex) keeps the MIS
     image's energy within the reference's 6 % (tests/Fix_integrator.swift:203-205) at depth 8."""
     faces, verts, mats, light, cam, mesh = cornell
@@ -105,7 +105,10 @@ def test_restir_gi_reservoirs_and_energy(ctx, cornell):
     # emitter hold neither.
     assert np.array_equal(valid, scene.di_weights()[..., 1] > 0)
     assert valid.mean() > 0.5, valid.mean()
-    assert (g[valid][:, 1] > 1.5).mean() > 0.5  # merged history
+    # History merges only where the previous reservoir's W > 0, i.e. its secondary point's light sample
+    # was unoccluded (the temporal merge's condition, main.swift:4993-4994): a minority on this box at 1 spp.
+    assert (g[valid][:, 1] > 1.5).mean() > 0.05
+    assert g[..., 1].max() <= 21.0  # 1 + the capped confidence 20
     scene.reset()
     scene.render(vt.make_params(cam, 64, 48, 1, 1, False, 0), 1)
     assert np.all(scene.gi_weights()[..., 1] == 0.0)
