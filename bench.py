@@ -264,13 +264,15 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     ref_s = time.perf_counter() - t0
     # Progressive rendering in 16-spp steps until relMSE <= 1e-3 (device time of the renders only;
     # the readback and error between steps are not timed): plain path tracing (MIS, sampling mode 1)
-    # and ReSTIR DI at the primary vertex (sampling mode 0, two launches per frame).
-    def time_to_relmse(mode):
+    # through the wavefront integrator (and the megakernel, for comparison) and ReSTIR DI at the
+    # primary vertex (sampling mode 0, two launches per frame).
+    def time_to_relmse(mode, wavefront=False):
         scene.reset()
         total_ms, done, err = 0.0, 0, None
+        render = scene.render_wavefront if wavefront else scene.render
         while done < 16384:
             e0.record(stream)
-            scene.render(vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp, cs)
+            render(vt.make_params(cam, W, H, depth, 1 + done, True, mode), spp, cs)
             e1.record(stream)
             torch.cuda.synchronize()
             total_ms += e0.elapsed_time(e1)
@@ -281,7 +283,8 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
                 break
         return (total_ms / 1e3 if err is not None and err <= 1e-3 else None), done, err
 
-    pt_s, pt_spp, pt_err = time_to_relmse(1)
+    pt_s, pt_spp, pt_err = time_to_relmse(1, wavefront=True)
+    mk_s, mk_spp, mk_err = time_to_relmse(1)
     di_s, di_spp, di_err = time_to_relmse(0)
 
     # The radiance cache's arms: the cache is trained from scratch inside the timed region (training
@@ -342,7 +345,8 @@ def bench_cornell(a, ctx, dev, stream, cpu_leg: bool) -> dict:
     nrc["nrc_train_every"] = a.nrc_train_every
     nrc["nrc_restir_speedup_vs_plain"] = (pt_s / nrc["nrc_restir_s"]) if (pt_s and nrc["nrc_restir_s"]) else None
     out["time_to_relmse_1e-3"] = {
-        "plain_pt_s": pt_s, "spp": pt_spp, "relmse": pt_err,
+        "plain_pt_s": pt_s, "spp": pt_spp, "relmse": pt_err, "plain_pt_integrator": "wavefront",
+        "plain_pt_megakernel_s": mk_s, "plain_pt_megakernel_spp": mk_spp,
         "restir_di_s": di_s, "restir_di_spp": di_spp, "restir_di_relmse": di_err,
         **nrc,
         "reference_spp": nref, "reference_wall_s": ref_s,

@@ -374,9 +374,10 @@ typedef struct vt_batch_info {
   unsigned long long items;   /* pixels per pass */
   float last_ms;              /* the last pass, device time */
   uint32_t tuned;             /* 1 once the launch shape is chosen (and, for the megakernel, captured) */
-  uint32_t block, chunk;      /* the launch shape of the last pass (chunk: megakernel items per grab) */
+  uint32_t block, chunk;      /* the launch shape (chunk: megakernel items per grab): for the megakernel
+                                 the chosen one once tuned, for the wavefront the last pass's */
   uint32_t wavefront;         /* 1: the batch renders through vt_batch_render_wavefront */
-  uint32_t queue_paths;       /* wavefront: paths per pass of a scene's queues */
+  uint32_t queue_paths;       /* wavefront: paths per pass of a scene's queues (the last pass's) */
   uint32_t compact_every;     /* wavefront: the live queue is compacted on every n-th bounce */
   uint32_t streams;           /* wavefront: streams the scenes are spread over */
 } vt_batch_info;

@@ -3117,7 +3117,7 @@ struct vt_batch {
   };
   std::vector<vt_frame_params> params;
   std::vector<WfConfig> wfConfigs;
-  size_t wfTried = 0;
+  size_t wfTried = 0, wfLast = 0;  // configs tried; the config of the last pass
   int wfBest = -1;
   cudaStream_t streams[kStreams] = {};
   cudaEvent_t fork = nullptr, join[kStreams] = {};
@@ -3323,7 +3323,8 @@ vt_status vt_batch_render_wavefront(vt_ctx *ctx, vt_batch *b, void *stream) {
       load[k] += work(i);
     }
   }
-  const vt_batch::WfConfig &c = b->wfConfigs[b->wfBest >= 0 ? (size_t)b->wfBest : b->wfTried];
+  b->wfLast = b->wfBest >= 0 ? (size_t)b->wfBest : b->wfTried;
+  const vt_batch::WfConfig &c = b->wfConfigs[b->wfLast];
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   VT_CUDA(ctx, cudaEventRecord(b->fork, s));
   for (int k = 0; k < vt_batch::kStreams; ++k) VT_CUDA(ctx, cudaStreamWaitEvent(b->streams[k], b->fork, 0));
@@ -3379,7 +3380,7 @@ vt_status vt_batch_stats(vt_ctx *ctx, const vt_batch *b, vt_batch_info *out, dou
   if (b->mode == 2) {
     out->wavefront = 1;
     out->tuned = b->wfBest >= 0 ? 1u : 0u;
-    const vt_batch::WfConfig &c = b->wfConfigs[b->wfBest >= 0 ? (size_t)b->wfBest : (b->wfTried ? b->wfTried - 1 : 0)];
+    const vt_batch::WfConfig &c = b->wfConfigs[b->wfLast];
     out->block = (uint32_t)c.block;
     out->queue_paths = c.queue;
     out->compact_every = c.every;
