@@ -312,7 +312,8 @@ vt_status vt_render(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *params,
  * state lives in device memory between stage kernels over queues of live paths (camera rays;
  * per bounce the closest-hit traversal of the queue, shading with NEE and the BSDF continuation,
  * the shadow rays' any-hit traversal; then the accumulation), with the megakernel's sampler draws
- * and arithmetic per path, so the image equals vt_render's up to the order of the FP64 sums. The
+ * and arithmetic per path; a path's primary and continuation radiance are summed apart, so the image
+ * equals vt_render's to float rounding (1e-6 relative per pixel). The
  * reference has no wavefront path; its design note proposes the split (docs/KERNEL_SPLIT_DESIGN.md:
  * 72-74). Paths per pass are capped at 4M (whole samples of the frame); the state takes ~250 bytes
  * per path, allocated with the scene on first use. */
@@ -391,8 +392,8 @@ vt_status vt_batch_render(vt_ctx *ctx, vt_batch *batch, void *stream);
  * camera jitter computed on the device. The first passes try, one each, the queue size (1M or 4M
  * paths per wavefront pass; only sizes that hold the largest frame), the stage kernels' block size
  * (128 or 256) and the compaction frequency (every bounce, or every second bounce with ended paths
- * kept in place); later passes use the fastest. Images equal vt_render's of the same frames (FP64
- * summation order aside). A batch renders through one integrator: after a wavefront pass
+ * kept in place); later passes use the fastest. Images equal vt_render_wavefront's of the same
+ * frames (FP64 summation order aside). A batch renders through one integrator: after a wavefront pass
  * vt_batch_render refuses it, and the other way round. Synchronises (it times the pass). */
 vt_status vt_batch_render_wavefront(vt_ctx *ctx, vt_batch *batch, void *stream);
 /* Statistics of the last pass; scene_ms (n = scene count, may be NULL) receives each scene's
@@ -556,6 +557,21 @@ typedef struct vt_environment {
  * accumulation. Sampling modes 1-3 only: ReSTIR DI (mode 0) rejects a scene with an environment, so
  * vt_render_nrc renders one with MIS primaries (mode 1); its training paths see the environment. */
 vt_status vt_scene_set_environment(vt_ctx *ctx, vt_scene *scene, const vt_environment *env);
+/* An equirectangular (lat-long) environment image instead of the procedural sky (MaterialLibrary's
+ * makeEnvironment / environmentImportance, Sources/StudioModel.swift:1300-1436; eval_environment and
+ * its sampling, main.swift:2077-2134, 2918-2950): `rgba` holds width x height linear-sRGB pixels, 4
+ * floats each (alpha ignored, negatives clamped to 0), row 0 at +y; `rotation` (radians) turns it
+ * about +y (Uniforms.environment.y), `intensity` scales it. NEE samples the image's texels from a
+ * compensated table (luminance above the map's mean; used where the vertex's BSDF continuation is
+ * traced) or the original one. Sampling modes 1-3. Restarts the accumulation; NULL or intensity 0
+ * clears the environment. Limits as the reference's: width <= 16384, height <= 8192, at most 2^25
+ * pixels, finite pixels. */
+vt_status vt_scene_set_environment_map(vt_ctx *ctx, vt_scene *scene, const float *rgba, uint32_t width,
+                                       uint32_t height, float intensity, float rotation);
+/* The image's sampling tables as the scene holds them, computed on the host from HOST pixels:
+ * rows[2 y + table] (2 x height marginal CDFs; table 0 compensated, 1 original) and
+ * cols[(table height + y) width + x] (2 x width x height conditional CDFs). For checks. */
+vt_status vt_environment_tables(const float *rgba, uint32_t width, uint32_t height, float *rows, float *cols);
 
 /* ---- neural radiance cache (nrc.cu) -------------------------------------------------------------
  * No counterpart in the reference (it has no radiance cache). A radiance cache after Mueller et al.

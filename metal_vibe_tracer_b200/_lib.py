@@ -185,6 +185,8 @@ SIGNATURES = {
     "vt_openpbr_evaluate": (_I32, [_P, _P, _U32, _P]),
     "vt_scene_set_openpbr": (_I32, [_P, _P, _P, _U32]),
     "vt_scene_set_environment": (_I32, [_P, _P, C.POINTER(Environment)]),
+    "vt_scene_set_environment_map": (_I32, [_P, _P, _P, _U32, _U32, C.c_float, C.c_float]),
+    "vt_environment_tables": (_I32, [_P, _U32, _U32, _P, _P]),
     "vt_nrc_config_default": (_I32, [C.POINTER(NRCConfig)]),
     "vt_nrc_create": (_I32, [_P, C.POINTER(NRCConfig), _P, _P, C.POINTER(_P)]),
     "vt_nrc_destroy": (_I32, [_P, _P]),

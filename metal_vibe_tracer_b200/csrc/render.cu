@@ -83,6 +83,13 @@ struct RenderArgs {
   float envIntensity, sunIntensity;
   float3 sunDir;
   uint32_t skyMode;
+  // Environment image (vt_scene_set_environment_map): linear-sRGB lat-long pixels, the marginal row
+  // CDFs (2 per row: compensated, original) and the conditional column CDFs (the compensated table's
+  // rows first), its size and rotation about +y; envMap = 1 when the image replaces the sky.
+  const float4 *envImg;
+  const float *envRows, *envCols;
+  uint32_t envW, envH, envMap;
+  float envRot;
   float etotal;
   const uint4 *ltNodes;
   const uint32_t *ltLeaves;
@@ -632,9 +639,62 @@ __device__ float3 procedural_sky(const RenderArgs &A, float3 d) {
   }
   return mul(col, gain);
 }
-// eval_environment (main.swift:2127-2134) without an image map or an imported sun.
+// The image's texel lookup as the reference's sampler does it (main.swift:2127-2134: lat-long
+// coordinates u = atan2(z, x) / 2pi + 1/2 + rotation / 2pi, v = acos(y) / pi clamped half a texel in from
+// the poles, bilinear filtering, repeat in u).
+__device__ float3 env_image(const RenderArgs &A, float3 d) {
+  const float W = float(A.envW), H = float(A.envH);
+  const float u = atan2f(d.z, d.x) * (0.5f * kInvPi) + 0.5f + A.envRot * (0.5f * kInvPi);
+  float v = acosf(fminf(fmaxf(d.y, -1.0f), 1.0f)) * kInvPi;
+  v = fminf(fmaxf(v, 0.5f / H), 1.0f - 0.5f / H);
+  const float x = u * W - 0.5f, y = v * H - 0.5f;
+  const float fx = floorf(x), fy = floorf(y), tx = x - fx, ty = y - fy;
+  int x0 = (int)fmodf(fx, W);
+  if (x0 < 0) x0 += (int)A.envW;
+  x0 = min(x0, (int)A.envW - 1);
+  const int x1 = x0 + 1 == (int)A.envW ? 0 : x0 + 1;
+  const int y0 = min(max((int)fy, 0), (int)A.envH - 1), y1 = min(y0 + 1, (int)A.envH - 1);
+  const float4 a = __ldg(A.envImg + (size_t)y0 * A.envW + x0), b = __ldg(A.envImg + (size_t)y0 * A.envW + x1);
+  const float4 c = __ldg(A.envImg + (size_t)y1 * A.envW + x0), e = __ldg(A.envImg + (size_t)y1 * A.envW + x1);
+  const float w00 = (1.0f - tx) * (1.0f - ty), w10 = tx * (1.0f - ty), w01 = (1.0f - tx) * ty, w11 = tx * ty;
+  return f3(w00 * a.x + w10 * b.x + w01 * c.x + w11 * e.x, w00 * a.y + w10 * b.y + w01 * c.y + w11 * e.y,
+            w00 * a.z + w10 * b.z + w01 * c.z + w11 * e.z);
+}
+// eval_environment (main.swift:2127-2134) without an imported sun: the image or the procedural sky,
+// times the intensity.
 __device__ __forceinline__ float3 environment(const RenderArgs &A, float3 d) {
-  return mul(procedural_sky(A, d), A.envIntensity);
+  return mul(A.envMap ? env_image(A, d) : procedural_sky(A, d), A.envIntensity);
+}
+// The environment tables (main.swift:2084-2085): ENV_COMPENSATED samples max(0, L - mean L) and is
+// used where the vertex's BSDF continuation is traced; ENV_ORIGINAL samples L.
+constexpr uint32_t kEnvCompensated = 0u, kEnvOriginal = 1u;
+// environment_cdf_index (main.swift:2089-2097): the first index whose CDF reaches `value`.
+__device__ __forceinline__ uint32_t env_cdf_index(const float *cdf, uint32_t count, uint32_t stride, uint32_t base,
+                                                  float value) {
+  uint32_t low = 0, high = max(1u, count) - 1u;
+  for (uint32_t it = 0; it < 16u && low < high; ++it) {
+    const uint32_t middle = (low + high) / 2u;
+    if (__ldg(cdf + base + (size_t)middle * stride) >= value) high = middle; else low = middle + 1u;
+  }
+  return low;
+}
+// environment_cell_pdf (main.swift:2104-2113): the solid-angle density of texel (x, y) in `table`.
+__device__ __forceinline__ float env_cell_pdf(const RenderArgs &A, uint32_t x, uint32_t y, float sinTheta, uint32_t table) {
+  const float row = __ldg(A.envRows + 2u * y + table);
+  const float prevRow = y == 0u ? 0.0f : __ldg(A.envRows + 2u * (y - 1u) + table);
+  const float *cols = A.envCols + (size_t)(y + table * A.envH) * A.envW;
+  const float col = __ldg(cols + x), prevCol = x == 0u ? 0.0f : __ldg(cols + x - 1u);
+  const float cell = fmaxf(0.0f, row - prevRow) * fmaxf(0.0f, col - prevCol);
+  return cell * float(A.envW * A.envH) / (2.0f * kPiF * kPiF * fmaxf(1e-5f, sinTheta));
+}
+// environment_image_pdf (main.swift:2115-2122).
+__device__ __forceinline__ float env_image_pdf(const RenderArgs &A, float3 wi, uint32_t table) {
+  const float theta = acosf(fminf(fmaxf(wi.y, -1.0f), 1.0f));
+  float u = atan2f(wi.z, wi.x) * (0.5f * kInvPi) + 0.5f + A.envRot * (0.5f * kInvPi);
+  u = u - floorf(u);
+  const float v = fminf(fmaxf(theta * kInvPi, 0.0f), 1.0f - 1e-7f);
+  const uint32_t x = min(A.envW - 1u, (uint32_t)(u * float(A.envW))), y = min(A.envH - 1u, (uint32_t)(v * float(A.envH)));
+  return env_cell_pdf(A, x, y, sinf(theta), table);
 }
 // imported_light_probability (main.swift:2716-2719): emitters and the environment share NEE.
 __device__ __forceinline__ float imported_probability(const RenderArgs &A) {
@@ -644,23 +704,25 @@ __device__ __forceinline__ float imported_probability(const RenderArgs &A) {
 // environment_sun_probability (main.swift:2700-2706) for the procedural sun: 0.6 while the disc is above
 // the horizon.
 __device__ __forceinline__ float sun_probability(const RenderArgs &A) {
-  if (!(A.sunIntensity > 0.0f) || !A.env) return 0.0f;
+  if (!(A.sunIntensity > 0.0f) || !A.env || A.envMap) return 0.0f;
   const float w = sun_one_minus_cos(A.skyMode);
   return A.sunDir.y >= -sqrtf(w * (2.0f - w)) ? 0.60f : 0.0f;
 }
 // eval_environment_pdf (main.swift:2880-2883, environment_mixture_pdf :2707-2712): the sun cone and a
-// cosine lobe about the receiver's normal n, times the environment's share of NEE.
-__device__ __forceinline__ float environment_pdf(const RenderArgs &A, float3 wi, float3 n) {
+// cosine lobe about the receiver's normal n, or the image's density in `table`, times the
+// environment's share of NEE. BSDF continuations that escape weigh against the compensated table.
+__device__ __forceinline__ float environment_pdf(const RenderArgs &A, float3 wi, float3 n, uint32_t table = kEnvCompensated) {
   const float sp = sun_probability(A), w = sun_one_minus_cos(A.skyMode);
   const float sunPdf = in_sun_cone(wi, A.sunDir, w) ? 1.0f / (kTwoPi * w) : 0.0f;
-  const float rest = fmaxf(0.0f, dot3(n, wi)) * kInvPi;
+  const float rest = A.envMap ? env_image_pdf(A, wi, table) : fmaxf(0.0f, dot3(n, wi)) * kInvPi;
   return (1.0f - imported_probability(A)) * (sp * sunPdf + (1.0f - sp) * rest);
 }
 
 // sample_direct_light's imported branch (main.swift:2889-2955): an emitter triangle with probability
-// imported_probability, else the environment (the sun cone with probability sun_probability, else a
-// cosine lobe about n).
-__device__ LightSample sample_emitters(const RenderArgs &A, float3 p, float3 n, Sampler &seed) {
+// imported_probability, else the environment (the sun cone with probability sun_probability, else the
+// image's cell from `table` and a uniform point in it, else a cosine lobe about n). `compensated`:
+// the vertex's BSDF continuation is traced (ENV_COMPENSATED), else ENV_ORIGINAL.
+__device__ LightSample sample_emitters(const RenderArgs &A, float3 p, float3 n, Sampler &seed, bool compensated) {
   LightSample ls;
   ls.pdf = 0.0f;
   ls.face = 0xffffffffu;
@@ -678,6 +740,25 @@ __device__ LightSample sample_emitters(const RenderArgs &A, float3 p, float3 n, 
       float sn, cs;
       sincosf(kTwoPi * q.z, &sn, &cs);
       ls.wi = normalize3(add(add(mul(su, cs * sinTh), mul(sv, sn * sinTh)), mul(A.sunDir, cosTh)));
+    } else if (A.envMap) {
+      const uint32_t table = compensated ? kEnvCompensated : kEnvOriginal;
+      const float2 c = sp > 0.0f ? make_float2(q.y, q.z) : rand_f2(seed);
+      const uint32_t y = env_cdf_index(A.envRows, A.envH, 2u, table, c.x);
+      const uint32_t x = env_cdf_index(A.envCols, A.envW, 1u, (y + table * A.envH) * A.envW, c.y);
+      // The in-texel offset stays inside the chosen cell, and that cell's probability is used.
+      const float W = float(A.envW), H = float(A.envH);
+      const float2 r = rand_f2(seed);
+      const float u = fminf(float(x) / W + r.x / W, nextafterf(float(x + 1u) / W, 0.0f));
+      const float v = fminf(float(y) / H + r.y / H, nextafterf(float(y + 1u) / H, 0.0f));
+      const float theta = v * kPiF, phi = (u - 0.5f - A.envRot * (0.5f * kInvPi)) * kTwoPi;
+      const float sinTheta = sinf(theta);
+      ls.wi = normalize3(f3(sinTheta * cosf(phi), cosf(theta), sinTheta * sinf(phi)));
+      ls.pos = add(p, mul(ls.wi, 1e6f));
+      ls.dist = 1e6f;
+      ls.face = kEnvFace;
+      ls.pdf = (1.0f - ip) * (1.0f - sp) * env_cell_pdf(A, x, y, sinTheta, table);
+      ls.emission = environment(A, ls.wi);
+      return ls;
     } else {
       const float2 r = sp > 0.0f ? make_float2(q.y, q.z) : rand_f2(seed);
       ls.wi = cosine_hemisphere(n, r.x, r.y);
@@ -685,7 +766,7 @@ __device__ LightSample sample_emitters(const RenderArgs &A, float3 p, float3 n, 
     ls.pos = add(p, mul(ls.wi, 1e6f));
     ls.dist = 1e6f;
     ls.face = kEnvFace;
-    ls.pdf = environment_pdf(A, ls.wi, n);
+    ls.pdf = environment_pdf(A, ls.wi, n, compensated ? kEnvCompensated : kEnvOriginal);
     ls.emission = environment(A, ls.wi);
     return ls;
   }
@@ -729,8 +810,9 @@ __device__ __forceinline__ float emitter_pdf(const RenderArgs &A, float3 p, floa
   return g > 1e-12f ? imported_probability(A) * emitter_area_pdf(A, face, p, t) / g : 0.0f;
 }
 
-__device__ __forceinline__ LightSample sample_direct(const RenderArgs &A, float3 p, float3 n, Sampler &seed) {
-  return A.imported ? sample_emitters(A, p, n, seed) : sample_light(A, p, seed);
+__device__ __forceinline__ LightSample sample_direct(const RenderArgs &A, float3 p, float3 n, Sampler &seed,
+                                                     bool compensated) {
+  return A.imported ? sample_emitters(A, p, n, seed, compensated) : sample_light(A, p, seed);
 }
 
 // ray_origin (main.swift:1366-1369): offset along the geometric normal by max(error, epsilon).
@@ -895,9 +977,9 @@ __device__ __forceinline__ float4 nee_lanes(const RenderArgs &A, const Lanes &L,
 template <bool kPbr>
 __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                      float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
-                                                     Sampler &seed, int *stack, bool requirePdf) {
+                                                     bool compensated, Sampler &seed, int *stack, bool requirePdf) {
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  const LightSample ls = sample_direct(A, p, n, seed);
+  const LightSample ls = sample_direct(A, p, n, seed, compensated);
   if (requirePdf && !(ls.pdf > 0.0f)) return zero;
   if (!light_visible(A, p, gn, err, ls, stack)) return zero;
   return nee_lanes<kPbr>(A, L, n, gn, wo, T, m, useMIS, ls);
@@ -906,8 +988,8 @@ __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const 
 template <bool kPbr>
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
                                                float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
-                                               Sampler &seed, int *stack, bool requirePdf) {
-  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, seed, stack, requirePdf));
+                                               bool compensated, Sampler &seed, int *stack, bool requirePdf) {
+  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, compensated, seed, stack, requirePdf));
 }
 
 // ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
@@ -1176,7 +1258,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     }
     if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit,
+      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -1210,7 +1292,7 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, seed,
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, limit > 0, seed,
                      stack, true);
   }
   const float spreadLimit = kNrc ? nrc_spread_limit(A, h.t, S.gn, dir0) : 0.0f;
@@ -1334,7 +1416,7 @@ __device__ GISample gi_initial(const RenderArgs &A, const Surface &S, const vt_m
   if (A.spectral) L = make_lanes(A, u);
   float4 rad = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   sampler_event(seed, 2u, kZGiNee);
-  const LightSample ls = sample_direct(A, S2.pos, S2.n, seed);
+  const LightSample ls = sample_direct(A, S2.pos, S2.n, seed, limit >= 2);
   if (ls.pdf > 0.0f && light_visible(A, S2.pos, S2.gn, S2.err, ls, stack)) {
     const float c2 = fmaxf(0.0f, dot3(S2.n, ls.wi));
     float pdf2;
@@ -1408,7 +1490,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
   r.M = 0.0f;
   for (uint32_t c = 0; c < A.diCandidates; ++c) {
     sampler_candidate(seed, 1u, kZDi, c, A.diBits);
-    const LightSample ls = sample_direct(A, S.pos, S.n, seed);
+    const LightSample ls = sample_direct(A, S.pos, S.n, seed, (int)A.maxDepth - 1 > 0);
     r.M += 1.0f;  // zero-weight candidates still count
     if (!(ls.pdf > 0.0f)) continue;
     DISample cand;
@@ -1512,7 +1594,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, seed, stack, true);
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true);
     const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
     R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, spreadLimit, slot, &queried));
   } else {
@@ -1712,9 +1794,9 @@ __device__ __forceinline__ void wf_push(bool push, uint32_t v, uint32_t *q, uint
 // to trace.
 template <bool kPbr>
 __device__ __forceinline__ bool wf_nee(const RenderArgs &A, const WfArgs &W, uint32_t i, const Lanes &L, const Surface &S,
-                                       float3 wo, float4 T, const vt_material &m, bool useMIS, Sampler &seed,
-                                       bool requirePdf) {
-  const LightSample ls = sample_direct(A, S.pos, S.n, seed);
+                                       float3 wo, float4 T, const vt_material &m, bool useMIS, bool compensated,
+                                       Sampler &seed, bool requirePdf) {
+  const LightSample ls = sample_direct(A, S.pos, S.n, seed, compensated);
   if (requirePdf && !(ls.pdf > 0.0f)) return false;
   float3 o, dir;
   float tmax;
@@ -1778,7 +1860,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         if (kNrc) W.spread[i] = make_float2(0.0f, nrc_spread_limit(A, h.t, S.gn, dir));
         if (A.mode != 3u) {
           sampler_event(seed, 1u, kZNee);
-          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, A.mode == 1u && limit > 0, seed, true)) {
+          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, A.mode == 1u && limit > 0, limit > 0, seed, true)) {
             shadow = true;
             flags |= kWfShadow | kWfShadowPrimary;
           }
@@ -1826,7 +1908,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
       } else {
         if (nee) {
           sampler_event(seed, b + 1u, kZNee);
-          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, mis && scattering < limit, seed, false)) {
+          if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit, seed, false)) {
             shadow = true;
             flags |= kWfShadow;
           }
@@ -2008,7 +2090,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
   }
-  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, seed, stack, true));
+  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true));
   int scattering = 0;
   for (int bounce = 1; scattering < limit; ++bounce) {
     ++scattering;
@@ -2052,7 +2134,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
       ++nrec;
     }
-    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, seed,
+    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, scattering < limit, seed,
                                          stack, false));
     if (bounce > 3) {
       const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
@@ -2218,7 +2300,7 @@ __global__ void k_light_estimate(RenderArgs A, const float4 *__restrict__ points
   seed.key = seed.dimension = seed.sub = seed.subBits = 0u;
   float sum = 0.0f, squares = 0.0f, hits = 0.0f, zero = 0.0f, error = 0.0f, backFacing = 0.0f;
   for (uint32_t i = 0; i < samples; ++i) {
-    const LightSample ls = sample_emitters(A, p, f3(0.0f, 0.0f, 1.0f), seed);
+    const LightSample ls = sample_emitters(A, p, f3(0.0f, 0.0f, 1.0f), seed, true);
     if (ls.face == 0xffffffffu) continue;
     const Tri t = scene_triangle(A, ls.face);
     if (dot3(cross3(sub(t.b, t.a), sub(t.c, t.a)), sub(p, ls.pos)) <= 0.0f) backFacing += 1.0f;
@@ -2309,6 +2391,69 @@ vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *mate
   return VT_OK;
 }
 
+// MaterialLibrary.environmentImportance (Sources/StudioModel.swift:1300-1392), restated: the pixels'
+// luminance (at least 1e-6), dilated by a separable 3 x 3 maximum (wrapping in longitude, clamped in
+// latitude) so that a bright texel's bilinear spill into its neighbours is sampled too; the compensated
+// table weighs max(0, L - mean L) (the mean over solid angle), the original one L, both times sin(theta);
+// a map with nothing above its mean samples L in both. Rows: rows[2 y + table] is the marginal CDF;
+// columns: cols[(table H + y) W + x] the conditional CDF of row y. Float arithmetic as the reference's.
+void environment_tables(const float *px, uint32_t w, uint32_t h, float *rows, float *cols) {
+  const size_t n = (size_t)w * h;
+  const float kPiHost = 3.14159265f;
+  std::vector<float> lum(n), horizontal(n);
+  for (size_t i = 0; i < n; ++i)
+    lum[i] = std::max(1e-6f, 0.2126f * px[4 * i] + 0.7152f * px[4 * i + 1] + 0.0722f * px[4 * i + 2]);
+  for (uint32_t y = 0; y < h; ++y) {
+    const size_t base = (size_t)y * w;
+    for (uint32_t x = 0; x < w; ++x)
+      horizontal[base + x] = std::max(lum[base + x], std::max(lum[base + (x + w - 1) % w], lum[base + (x + 1) % w]));
+  }
+  double meanSum = 0.0, angleSum = 0.0;
+  for (uint32_t y = 0; y < h; ++y) {
+    const double sinTheta = (double)std::max(1e-4f, std::sin((kPiHost * ((float)y + 0.5f)) / (float)h));
+    double row = 0.0;
+    for (uint32_t x = 0; x < w; ++x) row += (double)lum[(size_t)y * w + x];
+    meanSum += row * sinTheta;
+    angleSum += sinTheta * (double)w;
+  }
+  const float mean = (float)(meanSum / angleSum);
+  std::fill(rows, rows + 2 * (size_t)h, 0.0f);
+  float compensatedTotal = 0.0f;
+  for (uint32_t y = 0; y < h; ++y) {
+    const float theta = (kPiHost * ((float)y + 0.5f)) / (float)h;
+    const float sinTheta = std::max(1e-4f, std::sin(theta));
+    const size_t above = (size_t)(y > 0 ? y - 1 : 0) * w, here = (size_t)y * w, below = (size_t)std::min(h - 1, y + 1) * w;
+    for (uint32_t x = 0; x < w; ++x) {
+      const float dilated = std::max(horizontal[above + x], std::max(horizontal[here + x], horizontal[below + x]));
+      const float compensated = std::max(0.0f, dilated - mean) * sinTheta, original = dilated * sinTheta;
+      rows[2 * (size_t)y] += compensated;
+      rows[2 * (size_t)y + 1] += original;
+      cols[here + x] = compensated;
+      cols[n + here + x] = original;
+      compensatedTotal += compensated;
+    }
+  }
+  if (!(compensatedTotal > 0.0f)) {
+    for (uint32_t y = 0; y < h; ++y) rows[2 * (size_t)y] = rows[2 * (size_t)y + 1];
+    for (size_t i = 0; i < n; ++i) cols[i] = cols[n + i];
+  }
+  auto cdf = [](float *weights, size_t count, size_t nrows, size_t stride, size_t step) {
+    for (size_t r = 0; r < nrows; ++r) {
+      const size_t start = r * stride;
+      float total = 0.0f;
+      for (size_t k = 0; k < count; ++k) total += weights[start + k * step];
+      total = std::max(1e-12f, total);
+      float sum = 0.0f;
+      for (size_t k = 0; k < count; ++k) {
+        sum += weights[start + k * step] / total;
+        weights[start + k * step] = k == count - 1 ? 1.0f : sum;
+      }
+    }
+  };
+  cdf(rows, h, 2, 1, 2);
+  cdf(cols, w, 2 * (size_t)h, w, 1);
+}
+
 void scene_free(vt_scene *scene) {
   cudaFree(scene->d_pbr);
   cudaFree(scene->d_slotL);
@@ -2324,6 +2469,9 @@ void scene_free(vt_scene *scene) {
   cudaFree(scene->d_face_pos);
   cudaFree(scene->d_di);
   cudaFree(scene->d_wf);
+  cudaFree(scene->d_env_img);
+  cudaFree(scene->d_env_rows);
+  cudaFree(scene->d_env_cols);
   delete scene;
 }
 
@@ -2654,6 +2802,16 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
     A.sunIntensity = env.sun_intensity;
     A.sunDir = make_float3(env.sun_dir[0], env.sun_dir[1], env.sun_dir[2]);
     A.skyMode = env.sky_mode;
+    if (scene->env_map) {
+      A.envMap = 1u;
+      A.envImg = scene->d_env_img;
+      A.envRows = scene->d_env_rows;
+      A.envCols = scene->d_env_cols;
+      A.envW = scene->env_w;
+      A.envH = scene->env_h;
+      A.envRot = scene->env_rot;
+      A.sunIntensity = 0.0f;
+    }
   }
 }
 
@@ -3177,6 +3335,57 @@ cudaError_t batch_enqueue(vt_ctx *ctx, vt_batch *b, const vt_batch::Config &c, c
 
 extern "C" {
 
+vt_status vt_environment_tables(const float *rgba, uint32_t width, uint32_t height, float *rows, float *cols) {
+  if (!rgba || !rows || !cols || width == 0 || height == 0) return VT_ERR_INVALID;
+  environment_tables(rgba, width, height, rows, cols);
+  return VT_OK;
+}
+
+vt_status vt_scene_set_environment_map(vt_ctx *ctx, vt_scene *scene, const float *rgba, uint32_t width, uint32_t height,
+                                       float intensity, float rotation) {
+  if (!ctx) return VT_ERR_INVALID;
+  if (!scene) return vt_fail(ctx, VT_ERR_INVALID, "scene is null");
+  VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!rgba || !(intensity > 0.0f)) {
+    scene->env_map = false;
+    scene->environment = vt_environment{};
+    return vt_accum_reset(ctx, scene);
+  }
+  if (!scene->imported) return vt_fail(ctx, VT_ERR_INVALID, "an environment needs an imported scene");
+  if (!std::isfinite(intensity) || !std::isfinite(rotation)) return vt_fail(ctx, VT_ERR_INVALID, "intensity and rotation must be finite");
+  if (width == 0 || height == 0 || width > 16384 || height > 8192 || (uint64_t)width * height > 33554432ull)
+    return vt_fail(ctx, VT_ERR_INVALID, "Could not decode the environment image (maximum 16384x8192).");
+  const size_t n = (size_t)width * height;
+  std::vector<float> px(4 * n);
+  for (size_t i = 0; i < 4 * n; ++i) {
+    if (!std::isfinite(rgba[i])) return vt_fail(ctx, VT_ERR_INVALID, "Environment pixels must be finite.");
+    px[i] = rgba[i] < 0.0f ? 0.0f : rgba[i];  // radiance is non-negative
+  }
+  std::vector<float> rows(2 * (size_t)height), cols(2 * n);
+  environment_tables(px.data(), width, height, rows.data(), cols.data());
+  cudaFree(scene->d_env_img);
+  cudaFree(scene->d_env_rows);
+  cudaFree(scene->d_env_cols);
+  scene->d_env_img = nullptr;
+  scene->d_env_rows = scene->d_env_cols = nullptr;
+  scene->env_map = false;
+  VT_CUDA(ctx, cudaMalloc(&scene->d_env_img, n * sizeof(float4)));
+  VT_CUDA(ctx, cudaMalloc(&scene->d_env_rows, rows.size() * sizeof(float)));
+  VT_CUDA(ctx, cudaMalloc(&scene->d_env_cols, cols.size() * sizeof(float)));
+  VT_CUDA(ctx, cudaMemcpy(scene->d_env_img, px.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+  VT_CUDA(ctx, cudaMemcpy(scene->d_env_rows, rows.data(), rows.size() * sizeof(float), cudaMemcpyHostToDevice));
+  VT_CUDA(ctx, cudaMemcpy(scene->d_env_cols, cols.data(), cols.size() * sizeof(float), cudaMemcpyHostToDevice));
+  scene->env_w = width;
+  scene->env_h = height;
+  scene->env_rot = rotation;
+  scene->env_map = true;
+  vt_environment e{};
+  e.intensity = intensity;
+  e.sun_dir[1] = 1.0f;
+  scene->environment = e;
+  return vt_accum_reset(ctx, scene);
+}
+
 vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_params *params, const uint32_t *spp,
                           uint32_t n, vt_batch **out) {
   if (!ctx) return VT_ERR_INVALID;
@@ -3415,6 +3624,7 @@ vt_status vt_batch_destroy(vt_ctx *ctx, vt_batch *b) {
 vt_status vt_scene_set_environment(vt_ctx *ctx, vt_scene *scene, const vt_environment *env) {
   if (!ctx) return VT_ERR_INVALID;
   if (!scene) return vt_fail(ctx, VT_ERR_INVALID, "scene is null");
+  scene->env_map = false;  // the procedural sky replaces an image
   vt_environment e{};
   if (env && env->intensity > 0.0f) {
     if (!scene->imported) return vt_fail(ctx, VT_ERR_INVALID, "an environment needs an imported scene");

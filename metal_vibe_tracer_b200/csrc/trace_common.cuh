@@ -45,6 +45,19 @@ __device__ __forceinline__ void load_node(const float4 *__restrict__ nodes, int 
   n.count = make_int4(__float_as_int(d.x), __float_as_int(d.y), __float_as_int(d.z), __float_as_int(d.w));
 }
 
+// Three-operand max / min (sm_100's max.f32 / min.f32 with three sources): one instruction where two
+// fmaxf / fminf would take two. Exact (the result is one of the inputs), NaN-free inputs here.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 __device__ __forceinline__ float f4(const float4 &v, int k) {
   return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
 }
@@ -173,8 +186,8 @@ __device__ __forceinline__ int node_hits(const Node4 &n, const SlabRay &w, float
     const float ax = __fmul_rn(__fsub_rn(f4(n.lox, k), w.lowx), w.invx), bx = __fmul_rn(__fsub_rn(f4(n.hix, k), w.highx), w.invx);
     const float ay = __fmul_rn(__fsub_rn(f4(n.loy, k), w.lowy), w.invy), by = __fmul_rn(__fsub_rn(f4(n.hiy, k), w.highy), w.invy);
     const float az = __fmul_rn(__fsub_rn(f4(n.loz, k), w.lowz), w.invz), bz = __fmul_rn(__fsub_rn(f4(n.hiz, k), w.highz), w.invz);
-    const float nt = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), tMin));
-    const float ft = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), tMax));
+    const float nt = fmax3(fminf(ax, bx), fminf(ay, by), fmaxf(fminf(az, bz), tMin));
+    const float ft = fmin3(fmaxf(ax, bx), fmaxf(ay, by), fminf(fmaxf(az, bz), tMax));
     nearT[k] = nt;
     mask |= (nt <= ft && i4(n.child, k) != 0) ? (1 << k) : 0;
   }
@@ -326,8 +339,8 @@ __device__ __forceinline__ int qnode_hits(const QNode &n, const QRay &r, float t
     const float nxk = __fmaf_rd(qbyte(x.nw, k), x.d, x.cn), fxk = __fmaf_ru(qbyte(x.fw, k), x.d, x.cf);
     const float nyk = __fmaf_rd(qbyte(y.nw, k), y.d, y.cn), fyk = __fmaf_ru(qbyte(y.fw, k), y.d, y.cf);
     const float nzk = __fmaf_rd(qbyte(z.nw, k), z.d, z.cn), fzk = __fmaf_ru(qbyte(z.fw, k), z.d, z.cf);
-    const float nt = fmaxf(fmaxf(nxk, nyk), fmaxf(nzk, tMin));
-    const float ft = fminf(fminf(fxk, fyk), fminf(fzk, tMax));
+    const float nt = fmaxf(fmax3(nxk, nyk, nzk), tMin);
+    const float ft = fminf(fmin3(fxk, fyk, fzk), tMax);
     nearT[k] = nt;
     mask |= (nt <= ft && i4(n.child, k) != 0) ? (1 << k) : 0;
   }

@@ -88,6 +88,13 @@ struct vt_scene {
   // (emission rgb, selection weight), and face -> BVH position.
   bool imported = false;
   vt_environment environment{};  // procedural sky and sun of an imported scene (intensity 0: none)
+  // Environment image (vt_scene_set_environment_map): pixels, marginal row CDFs (2 x height) and
+  // conditional column CDFs (width x 2 height), its size and rotation; env_map when it is set.
+  float4 *d_env_img = nullptr;
+  float *d_env_rows = nullptr, *d_env_cols = nullptr;
+  uint32_t env_w = 0, env_h = 0;
+  float env_rot = 0.0f;
+  bool env_map = false;
   uint32_t *d_emitters = nullptr;
   std::vector<uint32_t> emitter_words;
   float4 *d_emissions = nullptr;

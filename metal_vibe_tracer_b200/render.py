@@ -158,6 +158,25 @@ class Scene:
         _check(self.ctx.handle, _lib.load().vt_scene_set_environment(self.ctx.handle, self._p, C.byref(e)),
                "vt_scene_set_environment")
 
+    def set_environment_map(self, image, intensity: float = 1.0, rotation: float = 0.0) -> None:
+        """An equirectangular environment image instead of the procedural sky
+        (vt_scene_set_environment_map): `image` is (height, width, 3 or 4) float linear sRGB, row 0
+        toward +y; `rotation` turns it about +y (radians). None removes it. Restarts the accumulation."""
+        lib = _lib.load()
+        if image is None:
+            _check(self.ctx.handle, lib.vt_scene_set_environment_map(self.ctx.handle, self._p, None, 0, 0, 0.0, 0.0),
+                   "vt_scene_set_environment_map")
+            return
+        img = np.asarray(image, np.float32)
+        if img.ndim != 3 or img.shape[2] not in (3, 4):
+            raise ValueError("image must be (height, width, 3 or 4)")
+        if img.shape[2] == 3:
+            img = np.concatenate([img, np.ones(img.shape[:2] + (1,), np.float32)], axis=2)
+        img = np.ascontiguousarray(img)
+        _check(self.ctx.handle, lib.vt_scene_set_environment_map(self.ctx.handle, self._p, img.ctypes.data, img.shape[1],
+                                                                 img.shape[0], float(intensity), float(rotation)),
+               "vt_scene_set_environment_map")
+
     def emitter_words(self) -> np.ndarray:
         """The packed emitter list of an imported scene (uint32 words)."""
         lib = _lib.load()
@@ -401,3 +420,20 @@ def openpbr_evaluate(ctx: Context, cases) -> np.ndarray:
     _check(ctx.handle, _lib.load().vt_openpbr_evaluate(ctx.handle, arr.ctypes.data, arr.shape[0], out.ctypes.data),
            "vt_openpbr_evaluate")
     return out
+
+
+def environment_tables(image):
+    """The environment image's sampling tables as vt_scene_set_environment_map builds them (host code
+    of the library): (rows (height, 2), cols (2, height, width)); table 0 compensated, 1 original."""
+    img = np.asarray(image, np.float32)
+    if img.shape[2] == 3:
+        img = np.concatenate([img, np.ones(img.shape[:2] + (1,), np.float32)], axis=2)
+    img = np.ascontiguousarray(img)
+    h, w = img.shape[:2]
+    rows = np.empty((h, 2), np.float32)
+    cols = np.empty((2, h, w), np.float32)
+    st = _lib.load().vt_environment_tables(img.ctypes.data, w, h, rows.ctypes.data, cols.ctypes.data)
+    if st != _lib.VT_OK:
+        raise ValueError("vt_environment_tables failed")
+    return rows, cols
+

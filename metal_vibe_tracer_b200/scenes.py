@@ -444,6 +444,26 @@ def _lattice_noise(dirs, seeds):
     return noise
 
 
+def environment_image(width: int = 64, height: int = 32, sun=(0.3, 0.28), sun_radiance: float = 40.0):
+    """A synthetic lat-long environment image (height, width, 4) float32, row 0 toward +y: a sky
+    gradient from a blue zenith to a bright horizon, a darker ground below it, and a small bright
+    "sun" patch of `sun_radiance` around the (u, v) position `sun` (2 x 2 texels), so that the
+    compensated sampling table (texels above the mean) differs from the original one."""
+    v = (np.arange(height) + 0.5) / height
+    u = (np.arange(width) + 0.5) / width
+    y = np.cos(np.pi * v)[:, None]                      # +1 at the zenith, -1 at the nadir
+    zenith, horizon, ground = np.array([0.15, 0.35, 0.9]), np.array([1.0, 0.85, 0.7]), np.array([0.25, 0.2, 0.15])
+    up = np.clip(y, 0.0, 1.0)[..., None]
+    sky = horizon * (1 - up ** 0.5) + zenith * up ** 0.5
+    img = np.where(y[..., None] >= 0, sky, ground * (1.0 + y[..., None]) + horizon * 0.2 * (-y[..., None] + 1) * 0.2)
+    img = img * (1.0 + 0.1 * np.sin(2 * np.pi * u)[None, :, None])
+    out = np.ones((height, width, 4), np.float32)
+    out[..., :3] = img
+    cx, cy = int(sun[0] * width), int(sun[1] * height)
+    out[cy:cy + 2, cx:cx + 2, :3] = sun_radiance
+    return out
+
+
 def sky_scene(emitter: bool = True, subdivisions: int = 2):
     """An open scene for the procedural sky and sun (imported-scene lighting): a 10 x 10 ground
     quad, a smooth-shaded icosphere of radius 1 resting on it, a 1 x 1 x 1 box and, with `emitter`,

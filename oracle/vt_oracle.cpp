@@ -1662,6 +1662,13 @@ struct PtContext {
   double envIntensity = 0, sunIntensity = 0;
   D3 sunDir{0, 1, 0};
   uint32_t skyMode = 0;
+  // Environment image: pixels (4 floats each), size, rotation, and its sampling tables built here
+  // (rows[2 y + table], cols[(table H + y) W + x]).
+  bool envMap = false;
+  const float *envImg = nullptr;
+  uint32_t envW = 0, envH = 0;
+  double envRot = 0;
+  std::vector<double> envRows, envCols;
 };
 
 inline double fword(uint32_t w) { float f; std::memcpy(&f, &w, 4); return f; }
@@ -2009,17 +2016,118 @@ D3 procedural_sky_d(const PtContext &C, D3 d) {
   }
   return col * gain;
 }
-D3 environment_d(const PtContext &C, D3 d) { return procedural_sky_d(C, d) * C.envIntensity; }
+// The image lookup (main.swift:2127-2134): lat-long coordinates with the rotation, v clamped half a
+// texel in from the poles, bilinear with repeat in u; in double.
+D3 env_image_d(const PtContext &C, D3 d) {
+  const double W = C.envW, H = C.envH;
+  const double u = std::atan2(d.z, d.x) / (2.0 * kPi) + 0.5 + C.envRot / (2.0 * kPi);
+  double v = std::acos(std::min(1.0, std::max(-1.0, d.y))) / kPi;
+  v = std::min(std::max(v, 0.5 / H), 1.0 - 0.5 / H);
+  const double x = u * W - 0.5, y = v * H - 0.5, fx = std::floor(x), fy = std::floor(y), tx = x - fx, ty = y - fy;
+  long x0 = (long)fx % (long)C.envW;
+  if (x0 < 0) x0 += C.envW;
+  const long x1 = (x0 + 1) % (long)C.envW;
+  const long y0 = std::min<long>(std::max<long>((long)fy, 0), C.envH - 1), y1 = std::min<long>(y0 + 1, C.envH - 1);
+  auto px = [&](long xx, long yy) {
+    const float *q = C.envImg + 4 * ((size_t)yy * C.envW + xx);
+    return D3{q[0], q[1], q[2]};
+  };
+  return px(x0, y0) * ((1 - tx) * (1 - ty)) + px(x1, y0) * (tx * (1 - ty)) + px(x0, y1) * ((1 - tx) * ty) +
+         px(x1, y1) * (tx * ty);
+}
+D3 environment_d(const PtContext &C, D3 d) {
+  return (C.envMap ? env_image_d(C, d) : procedural_sky_d(C, d)) * C.envIntensity;
+}
+// MaterialLibrary.environmentImportance (Sources/StudioModel.swift:1300-1392): dilated luminance, the
+// compensated table max(0, L - mean) sin(theta) and the original L sin(theta), normalised to CDFs.
+void env_tables_d(PtContext &C) {
+  const uint32_t w = C.envW, h = C.envH;
+  const size_t n = (size_t)w * h;
+  std::vector<double> lum(n), hor(n);
+  for (size_t i = 0; i < n; ++i)
+    lum[i] = std::max(1e-6, 0.2126 * C.envImg[4 * i] + 0.7152 * C.envImg[4 * i + 1] + 0.0722 * C.envImg[4 * i + 2]);
+  for (uint32_t y = 0; y < h; ++y)
+    for (uint32_t x = 0; x < w; ++x) {
+      const size_t b = (size_t)y * w;
+      hor[b + x] = std::max(lum[b + x], std::max(lum[b + (x + w - 1) % w], lum[b + (x + 1) % w]));
+    }
+  double meanSum = 0, angleSum = 0;
+  for (uint32_t y = 0; y < h; ++y) {
+    const double st = std::max(1e-4, std::sin(kPi * (y + 0.5) / h));
+    double row = 0;
+    for (uint32_t x = 0; x < w; ++x) row += lum[(size_t)y * w + x];
+    meanSum += row * st;
+    angleSum += st * w;
+  }
+  const double mean = meanSum / angleSum;
+  C.envRows.assign(2 * (size_t)h, 0.0);
+  C.envCols.assign(2 * n, 0.0);
+  double comp = 0;
+  for (uint32_t y = 0; y < h; ++y) {
+    const double st = std::max(1e-4, std::sin(kPi * (y + 0.5) / h));
+    const size_t above = (size_t)(y ? y - 1 : 0) * w, here = (size_t)y * w, below = (size_t)std::min(h - 1, y + 1) * w;
+    for (uint32_t x = 0; x < w; ++x) {
+      const double dil = std::max(hor[above + x], std::max(hor[here + x], hor[below + x]));
+      const double c = std::max(0.0, dil - mean) * st, o = dil * st;
+      C.envRows[2 * (size_t)y] += c;
+      C.envRows[2 * (size_t)y + 1] += o;
+      C.envCols[here + x] = c;
+      C.envCols[n + here + x] = o;
+      comp += c;
+    }
+  }
+  if (!(comp > 0)) {
+    for (uint32_t y = 0; y < h; ++y) C.envRows[2 * (size_t)y] = C.envRows[2 * (size_t)y + 1];
+    for (size_t i = 0; i < n; ++i) C.envCols[i] = C.envCols[n + i];
+  }
+  auto cdf = [](std::vector<double> &wt, size_t count, size_t rows, size_t stride, size_t step) {
+    for (size_t r = 0; r < rows; ++r) {
+      double total = 0;
+      for (size_t k = 0; k < count; ++k) total += wt[r * stride + k * step];
+      total = std::max(1e-12, total);
+      double sum = 0;
+      for (size_t k = 0; k < count; ++k) {
+        sum += wt[r * stride + k * step] / total;
+        wt[r * stride + k * step] = k == count - 1 ? 1.0 : sum;
+      }
+    }
+  };
+  cdf(C.envRows, h, 2, 1, 2);
+  cdf(C.envCols, w, 2 * (size_t)h, w, 1);
+}
+uint32_t env_cdf_index_d(const std::vector<double> &cdf, uint32_t count, size_t stride, size_t base, double value) {
+  uint32_t low = 0, high = std::max(1u, count) - 1;
+  for (int it = 0; it < 16 && low < high; ++it) {
+    const uint32_t mid = (low + high) / 2;
+    if (cdf[base + mid * stride] >= value) high = mid; else low = mid + 1;
+  }
+  return low;
+}
+double env_cell_pdf_d(const PtContext &C, uint32_t x, uint32_t y, double sinTheta, uint32_t table) {
+  const double row = C.envRows[2 * (size_t)y + table], prevRow = y ? C.envRows[2 * (size_t)(y - 1) + table] : 0.0;
+  const size_t b = (size_t)(y + table * C.envH) * C.envW;
+  const double col = C.envCols[b + x], prevCol = x ? C.envCols[b + x - 1] : 0.0;
+  return std::max(0.0, row - prevRow) * std::max(0.0, col - prevCol) * ((double)C.envW * C.envH) /
+         (2.0 * kPi * kPi * std::max(1e-5, sinTheta));
+}
+double env_image_pdf_d(const PtContext &C, D3 wi, uint32_t table) {
+  const double theta = std::acos(std::min(1.0, std::max(-1.0, wi.y)));
+  double u = std::atan2(wi.z, wi.x) / (2.0 * kPi) + 0.5 + C.envRot / (2.0 * kPi);
+  u -= std::floor(u);
+  const double v = std::min(std::max(theta / kPi, 0.0), 1.0 - 1e-7);
+  const uint32_t x = std::min(C.envW - 1, (uint32_t)(u * C.envW)), y = std::min(C.envH - 1, (uint32_t)(v * C.envH));
+  return env_cell_pdf_d(C, x, y, std::sin(theta), table);
+}
 double imported_probability_d(const PtContext &C) { return C.ecount == 0 ? 0.0 : (C.env ? 0.5 : 1.0); }
 double sun_probability_d(const PtContext &C) {
-  if (!(C.sunIntensity > 0.0) || !C.env) return 0.0;
+  if (!(C.sunIntensity > 0.0) || !C.env || C.envMap) return 0.0;
   const double w = sun_omc_d(C.skyMode);
   return C.sunDir.y >= -std::sqrt(w * (2.0 - w)) ? 0.60 : 0.0;
 }
-double environment_pdf_d(const PtContext &C, D3 wi, D3 n) {
+double environment_pdf_d(const PtContext &C, D3 wi, D3 n, uint32_t table = 0) {
   const double sp = sun_probability_d(C), w = sun_omc_d(C.skyMode);
   const double sunPdf = in_sun_cone_d(wi, C.sunDir, w) ? 1.0 / (2.0 * kPi * w) : 0.0;
-  const double rest = std::max(0.0, dot(n, wi)) / kPi;
+  const double rest = C.envMap ? env_image_pdf_d(C, wi, table) : std::max(0.0, dot(n, wi)) / kPi;
   return (1.0 - imported_probability_d(C)) * (sp * sunPdf + (1.0 - sp) * rest);
 }
 D3 cosine_hemisphere_d(D3 n, double r0, double r1) {
@@ -2032,7 +2140,9 @@ D3 cosine_hemisphere_d(D3 n, double r0, double r1) {
 
 // sample_direct_light's imported branch (main.swift:2889-2955): an emitter triangle with probability
 // imported_probability_d, else the environment (sun cone or cosine lobe about n).
-PtLight sample_emitters_d(const PtContext &C, D3 p, D3 n, ZSampler &seed) {
+// `compensated`: the vertex's BSDF continuation is traced, so the image is sampled from the compensated
+// table (main.swift:2077-2085), else from the original one.
+PtLight sample_emitters_d(const PtContext &C, D3 p, D3 n, ZSampler &seed, bool compensated) {
   PtLight ls{};
   ls.face = 0xffffffffu;
   const double ip = imported_probability_d(C);
@@ -2048,6 +2158,23 @@ PtLight sample_emitters_d(const PtContext &C, D3 p, D3 n, ZSampler &seed) {
       make_basis_d(C.sunDir, su, sv);
       const double phi = 2.0 * kPi * qz;
       ls.wi = normalize(su * (std::cos(phi) * sin_th) + sv * (std::sin(phi) * sin_th) + C.sunDir * cos_th);
+    } else if (C.envMap) {
+      const uint32_t table = compensated ? 0u : 1u;
+      double c0 = qy, c1 = qz;
+      if (!(sp > 0.0)) seed.f2(c0, c1);
+      const uint32_t y = env_cdf_index_d(C.envRows, C.envH, 2, table, c0);
+      const uint32_t x = env_cdf_index_d(C.envCols, C.envW, 1, (size_t)(y + table * C.envH) * C.envW, c1);
+      double r0, r1;
+      seed.f2(r0, r1);
+      const double u = (x + r0) / C.envW, v = (y + r1) / C.envH;
+      const double theta = v * kPi, phi = (u - 0.5 - C.envRot / (2.0 * kPi)) * 2.0 * kPi, st = std::sin(theta);
+      ls.wi = normalize(D3{st * std::cos(phi), std::cos(theta), st * std::sin(phi)});
+      ls.pos = p + ls.wi * 1e6;
+      ls.dist = 1e6;
+      ls.face = kEnvFaceD;
+      ls.pdf = (1.0 - ip) * (1.0 - sp) * env_cell_pdf_d(C, x, y, st, table);
+      ls.emission = environment_d(C, ls.wi);
+      return ls;
     } else {
       double r0 = qy, r1 = qz;
       if (!(sp > 0.0)) seed.f2(r0, r1);
@@ -2056,7 +2183,7 @@ PtLight sample_emitters_d(const PtContext &C, D3 p, D3 n, ZSampler &seed) {
     ls.pos = p + ls.wi * 1e6;
     ls.dist = 1e6;
     ls.face = kEnvFaceD;
-    ls.pdf = environment_pdf_d(C, ls.wi, n);
+    ls.pdf = environment_pdf_d(C, ls.wi, n, compensated ? 0u : 1u);
     ls.emission = environment_d(C, ls.wi);
     return ls;
   }
@@ -2184,8 +2311,8 @@ bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material 
 }
 
 D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
-            const vt_material &m, bool useMIS, ZSampler &seed, bool requirePdf) {
-  const PtLight ls = C.imported ? sample_emitters_d(C, p, n, seed) : sample_light_d(C, p, seed);
+            const vt_material &m, bool useMIS, bool compensated, ZSampler &seed, bool requirePdf) {
+  const PtLight ls = C.imported ? sample_emitters_d(C, p, n, seed, compensated) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
   if (!visible_d(C, p, gn, err, ls)) return {0, 0, 0};
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
@@ -2306,7 +2433,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     if (emissionOnly) break;
     if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, seed,
+      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, scattering < limit, seed,
                        false);
     }
     if (bounce > 3) {
@@ -2480,7 +2607,7 @@ GiS gi_initial_d(const PtContext &C, const PtHit &h, const vt_material &m, D3 vi
   if (C.spectral) L = make_lanes(C, u);
   Spec4 rad{{0, 0, 0, 0}};
   seed.event(2u, 6u);
-  const PtLight ls = C.imported ? sample_emitters_d(C, h2.pos, h2.n, seed) : sample_light_d(C, h2.pos, seed);
+  const PtLight ls = C.imported ? sample_emitters_d(C, h2.pos, h2.n, seed, limit >= 2) : sample_light_d(C, h2.pos, seed);
   if (ls.pdf > 0.0 && visible_d(C, h2.pos, h2.gn, h2.err, ls)) {
     const double c2 = std::max(0.0, dot(h2.n, ls.wi));
     double pdf2;
@@ -2526,7 +2653,8 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
   out.s.u = u;
   for (uint32_t c = 0; c < M; ++c) {
     seed.candidate(1u, 4u, c, bits);
-    const PtLight ls = C.imported ? sample_emitters_d(C, h.pos, h.n, seed) : sample_light_d(C, h.pos, seed);
+    const PtLight ls = C.imported ? sample_emitters_d(C, h.pos, h.n, seed, (int)C.p->max_depth - 1 > 0)
+                                  : sample_light_d(C, h.pos, seed);
     out.M += 1.0;
     if (!(ls.pdf > 0.0)) continue;
     const DiS cand = di_from_light(ls, u);
@@ -2589,7 +2717,7 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
     const int limit = std::max(0, (int)C.p->max_depth - 1);
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    D3 R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, seed, true);
+    D3 R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, limit > 0, seed, true);
     R = R + continue_path_d(C, L, h, m, dir0, seed, false);
     if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
     return R;
@@ -2667,7 +2795,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (C.p->sampling_mode != 3u) {
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0,
+    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0, limit > 0,
                  seed, true);
   }
   R = R + continue_path_d(C, L, h, m, dir0, seed, false);
@@ -2718,6 +2846,15 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
     C.sunIntensity = e.sun_intensity;
     C.sunDir = D3{(float)(e.sun_dir[0] / l), (float)(e.sun_dir[1] / l), (float)(e.sun_dir[2] / l)};
     C.skyMode = e.sky_mode;
+    if (in->env_rgba && in->env_w > 0 && in->env_h > 0) {
+      C.envMap = true;
+      C.envImg = in->env_rgba;
+      C.envW = in->env_w;
+      C.envH = in->env_h;
+      C.envRot = in->env_rot;
+      C.sunIntensity = 0.0;
+      env_tables_d(C);
+    }
   }
   if (C.imported) {
     // Per slot (rgb, selection weight max(1e-8, luminance) in float, main.swift:9303-9306).

@@ -127,6 +127,11 @@ typedef struct vto_pt_inputs {
   vto_pbr_sample_fn pbr_sample;
   /* Imported scenes: the procedural sky and sun (intensity 0: none). */
   vt_environment environment;
+  /* An environment image instead of the sky (env_rgba null: none): width x height pixels, 4 floats
+   * each, its rotation about +y in radians; the intensity is environment.intensity. */
+  const float *env_rgba;
+  uint32_t env_w, env_h;
+  float env_rot;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

@@ -259,7 +259,8 @@ class PtInputs(C.Structure):
                 ("emitters", C.c_void_p), ("nemitter_words", C.c_uint32), ("imported", C.c_uint32),
                 ("uplift", C.c_void_p), ("cos_phase", C.c_void_p),
                 ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p),
-                ("environment", Environment)]
+                ("environment", Environment), ("env_rgba", C.c_void_p), ("env_w", C.c_uint32), ("env_h", C.c_uint32),
+                ("env_rot", C.c_float)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -272,7 +273,8 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
 
     light=None renders an imported scene lit by its emissive faces; its emitter list is the
     pure-Python restatement's (oracle/light_tree.py) unless `emitter_words` is given. An imported
-    scene may also have an `environment` (dict: intensity, sun_dir, sun_intensity, sky_mode)."""
+    scene may also have an `environment` (dict: intensity, sun_dir, sun_intensity, sky_mode; or intensity,
+    image (height, width, 4) float32 lat-long pixels and rotation in radians)."""
     lib = load()
     if not hasattr(lib.vto_render, "_typed"):
         lib.vto_render.restype, lib.vto_render.argtypes = _SIGS["vto_render"]
@@ -306,6 +308,11 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         env.sun_dir[:] = [float(x) for x in environment.get("sun_dir", (0.0, 1.0, 0.0))]
         env.sun_intensity = float(environment.get("sun_intensity", 0.0))
         env.sky_mode = int(environment.get("sky_mode", 0))
+        if environment.get("image") is not None:
+            img = np.ascontiguousarray(np.clip(np.asarray(environment["image"], np.float32), 0.0, None))
+            keep.append(img)
+            inp.env_rgba, inp.env_h, inp.env_w = img.ctypes.data, img.shape[0], img.shape[1]
+            inp.env_rot = float(environment.get("rotation", 0.0))
     if light is None:
         if emitter_words is None:
             from . import light_tree as LT

@@ -63,7 +63,8 @@ def test_batch_equals_single_renders(ctx):
 def test_batch_wavefront_equals_single_renders(ctx):
     """vt_batch_render_wavefront: per-scene queues on four streams; the first eight passes try queue
     size x block size x compaction frequency (every bounce, every second bounce with ended paths kept
-    in place), and every pass adds exactly the samples vt_render of the same frames adds."""
+    in place), and every pass adds exactly the samples vt_render_wavefront of the same frames adds (the
+    same paths; only the FP64 summation order of the accumulation differs)."""
     specs, meshes = scene_specs(ctx)
     batch_scenes = [make() for make, _, _ in specs]
     batch = Batch(ctx, batch_scenes, [p for _, p, _ in specs], [s for _, _, s in specs])
@@ -83,7 +84,7 @@ def test_batch_wavefront_equals_single_renders(ctx):
         img, n = scene.readback()
         assert n == passes * spp
         ref_scene = make()
-        ref_scene.render(params, passes * spp)
+        ref_scene.render_wavefront(params, passes * spp)
         ref, m = ref_scene.readback()
         ref_scene.close()
         assert m == n

@@ -1,4 +1,5 @@
-"""The procedural sky and sun of imported scenes (vt_scene_set_environment) against the FP64 oracle,
+"""The procedural sky and sun of imported scenes (vt_scene_set_environment), and an environment image
+(vt_scene_set_environment_map) with its compensated and original sampling tables, against the FP64 oracle,
 which restates the same sky, sun-cone and cosine-lobe sampling and the MIS weights of escaped rays:
 * images within 0.1 % of the oracle's mean radiance, most pixels identical to 1e-4, the per-pixel
   relMSE below a quarter of the estimator's own (as the other integrator parity tests);
@@ -155,5 +156,77 @@ def test_cached_sky_scene_matches_path_tracer(ctx):
     with pytest.raises(vt.MaterialLibraryError, match="sampling mode 0"):
         cache.render(scene, vt.make_params(cam, W, H, 8, 1, True, 0), 1)
     cache.close()
+    scene.close()
+    mesh.close()
+
+
+def render_image_env(ctx, faces, verts, mats, cam, img, w, h, spp, spectral, mode=1, depth=8, wavefront=False,
+                     rotation=0.7):
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, None, spectral_tables.load() if spectral else None)
+    scene.set_environment_map(img, intensity=1.0, rotation=rotation)
+    (scene.render_wavefront if wavefront else scene.render)(vt.make_params(cam, w, h, depth, 1, spectral, mode), spp)
+    out, n = scene.readback()
+    scene.close()
+    mesh.close()
+    assert n == spp and np.isfinite(out).all()
+    return out
+
+
+@pytest.mark.parametrize("emitter,spectral", [(True, True), (False, False)])
+def test_image_environment_matches_oracle(ctx, oracle, emitter, spectral):
+    """The image lookup (bilinear, rotated), the two sampling tables and the escaped rays' MIS weights
+    against the oracle's double restatement (its tables built in double, so cells and densities
+    differ at float rounding: the comparison is the mean and the per-pixel error against the
+    estimator's own)."""
+    faces, verts, mats, cam = scenes.sky_scene(emitter=emitter)
+    img = scenes.environment_image(64, 32)
+    tables = spectral_tables.load() if spectral else None
+    gpu = render_image_env(ctx, faces, verts, mats, cam, img, 96, 96, 16, spectral)
+    env = {"intensity": 1.0, "image": img, "rotation": 0.7}
+    ref = oracle.render(faces, verts, mats, None, cam, 96, 96, 16, spectral=tables, environment=env)
+    other = oracle.render(faces, verts, mats, None, cam, 96, 96, 16, first_sample=1001, spectral=tables,
+                          environment=env)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < 0.5 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+
+
+def test_image_light_and_bsdf_sampling_agree_with_mis(ctx):
+    """Light sampling only (mode 2, the compensated table where a BSDF continuation follows, whose
+    zero-density directions the BSDF hits then carry with full weight) and BSDF sampling only
+    (mode 3) agree with MIS (mode 1) in mean radiance."""
+    faces, verts, mats, cam = scenes.sky_scene(emitter=True)
+    img = scenes.environment_image(64, 32)
+    means = {m: render_image_env(ctx, faces, verts, mats, cam, img, 64, 64, 1024, False, mode=m, depth=2)
+             .reshape(-1, 3).mean(0) for m in (1, 2, 3)}
+    assert np.all(np.abs(means[2] / means[1] - 1) < 0.02), means
+    assert np.all(np.abs(means[3] / means[1] - 1) < 0.03), means
+
+
+def test_image_environment_wavefront_equals_megakernel(ctx):
+    faces, verts, mats, cam = scenes.sky_scene(emitter=True)
+    img = scenes.environment_image(64, 32)
+    mega = render_image_env(ctx, faces, verts, mats, cam, img, 64, 64, 16, True)
+    wave = render_image_env(ctx, faces, verts, mats, cam, img, 64, 64, 16, True, wavefront=True)
+    same = np.all(np.abs(wave - mega) <= 1e-6 * np.maximum(np.abs(mega), 1e-3), axis=-1)
+    assert same.mean() >= 0.995, same.mean()
+
+
+def test_image_environment_rejections(ctx):
+    faces, verts, mats, cam = scenes.sky_scene(emitter=True)
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, None, None)
+    bad = scenes.environment_image(16, 8)
+    bad[3, 4, 0] = np.nan
+    with pytest.raises(vt.MaterialLibraryError, match="finite"):
+        scene.set_environment_map(bad)
+    with pytest.raises(vt.MaterialLibraryError, match="16384"):
+        scene.set_environment_map(np.ones((8193, 1, 4), np.float32))
+    scene.set_environment_map(scenes.environment_image(16, 8))
+    with pytest.raises(vt.MaterialLibraryError, match="sampling mode 0"):
+        scene.render(vt.make_params(cam, 16, 16, 8, 1, False, 0), 1)
+    scene.set_environment_map(None)
+    scene.render(vt.make_params(cam, 16, 16, 8, 1, False, 0), 1)
     scene.close()
     mesh.close()
