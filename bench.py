@@ -380,6 +380,10 @@ def bench_batch(a, ctx) -> dict:
     work = scenes.batch_workload(a.batch_scenes, seed=0)
     t0 = time.perf_counter()
     meshes, members, params, spp = [], [], [], []
+    # Scenes whose oracle times form the CPU baseline: spread over the triangle counts.
+    by_size = sorted(range(len(work)), key=lambda i: work[i][0])
+    cpu_pick = {by_size[int(q * (len(work) - 1))] for q in (0.0, 0.33, 0.67, 1.0)} if len(work) else set()
+    cpu_inputs = {}
     for i, (tris, res, n) in enumerate(work):
         f, v, m, cam = scenes.sphere_grid(tris, seed=i)
         mesh = vt.Mesh(ctx, f, v)
@@ -387,6 +391,8 @@ def bench_batch(a, ctx) -> dict:
         members.append(vt.Scene(ctx, mesh, m, None))
         params.append(vt.make_params(cam, res, res, 8, 1, False, 1))
         spp.append(n)
+        if i in cpu_pick:
+            cpu_inputs[i] = (f, v, m, cam, res)
     setup_s = time.perf_counter() - t0
     batch = Batch(ctx, members, params, spp)
     wave = a.batch_integrator == "wavefront"
@@ -416,6 +422,26 @@ def bench_batch(a, ctx) -> dict:
            "scene_latency_ms": {"median": float(np.median(scene_ms)), "max": float(scene_ms.max()),
                                 "min": float(scene_ms.min())},
            "gpu_launches_per_pass": launches, "setup_s": setup_s}
+    if not a.no_cpu_baseline and cpu_inputs:
+        # The FP64 oracle path tracer per sampled scene (1 spp over every s-th pixel, s = res / 512,
+        # on the device's hierarchy and emitter list), against the scene's share of the GPU pass.
+        from oracle import vt_oracle as O
+        per, tot_paths, tot_s = [], 0, 0.0
+        for i, (f, v, m, cam, res) in sorted(cpu_inputs.items()):
+            ob = O.Bvh.from_arrays(meshes[i].nodes(), meshes[i].order(), f, v, meshes[i].info().depth)
+            stride = max(1, res // 512)
+            t0 = time.perf_counter()
+            img = O.render(f, v, m, None, cam, res, res, 1, max_depth=8, mode=1, emitter_words=members[i].emitter_words(),
+                           pixel_stride=stride, bvh=ob)
+            t = time.perf_counter() - t0
+            npaths = img.shape[0] * img.shape[1]
+            per.append({"scene": i, "triangles": work[i][0], "paths": npaths, "s": t, "paths_per_s": npaths / t})
+            tot_paths += npaths
+            tot_s += t
+        out["cpu_baseline"] = {"value": tot_paths / tot_s, "unit": "paths/s", "cores": O.threads(), "kind": "port",
+                               "sample": "FP64 oracle path tracer on %d of the scenes (smallest to largest), 1 spp "
+                                         "over every (res/512)-th pixel: %d paths in %.1f s" % (len(per), tot_paths, tot_s),
+                               "scenes": per}
     batch.close()
     for sc in members:
         sc.close()
@@ -474,6 +500,24 @@ def bench_production(a, ctx, stream) -> dict:
         # (depth + 1) x (extend, shade, shadow) and the accumulation.
         launches = 2 if mode == 0 else (2 + 3 * (depth + 1) if wavefront else 1)
         out[name] = {"ms_per_frame": ms, "paths_per_s": W * H / (ms / 1e3), "frames": n, "gpu_launches_per_frame": launches}
+    if not a.no_cpu_baseline and not a.profile_production:
+        # The FP64 oracle path tracer on the host cores, on the device's hierarchy and emitter list
+        # (both verified equal to the oracle's own builds elsewhere), over every 2nd pixel in x and y
+        # of one MIS frame: a bounded sample of the same workload (~10 s on the host).
+        from oracle import vt_oracle as O
+        ob = O.Bvh.from_arrays(mesh.nodes(), mesh.order(), faces, verts, info.depth)
+        words = scene.emitter_words()
+        stride = 2
+        t0 = time.perf_counter()
+        img = O.render(faces, verts, mats, None, cam, W, H, 1, max_depth=depth, spectral=tables, mode=1,
+                       emitter_words=words, pixel_stride=stride, bvh=ob)
+        t = time.perf_counter() - t0
+        npaths = img.shape[0] * img.shape[1]
+        out["cpu_baseline"] = {"value": npaths / t, "unit": "paths/s", "cores": O.threads(), "kind": "port",
+                               "sample": "FP64 oracle path tracer (MIS, spectral, depth 12), one frame's every %d-th pixel "
+                                         "in x and y: %d paths in %.1f s" % (stride, npaths, t),
+                               "gpu_mis_wavefront_over_cpu": (out["mis_wavefront"]["paths_per_s"] / (npaths / t)
+                                                              if "mis_wavefront" in out else None)}
     scene.close()
     mesh.close()
     return out

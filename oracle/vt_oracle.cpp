@@ -472,6 +472,20 @@ int32_t vto_intersect_f64(const double *ray, const double *tri, double tmin, dou
   return intersect_tri<double>(w, tri, tri + 3, tri + 6, tmin, tmax, *t, *b1, *b2) ? 1 : 0;
 }
 
+// A hierarchy built elsewhere (the device's: its 4-wide nodes, leaf order and depth) over the same
+// faces and vertices, for traversal and rendering without rebuilding it here.
+vto_bvh *vto_bvh_import(const vt_wide_node *nodes, uint32_t nnodes, const int32_t *order, uint32_t nfaces,
+                        const vt_face *faces, const vt_vertex *verts, uint32_t depth) {
+  vto_bvh *h = new vto_bvh();
+  h->faces = nfaces;
+  h->depth = depth;
+  h->nodes.assign(nodes, nodes + nnodes);
+  h->order.assign(order, order + nfaces);
+  finish_bvh(h, faces, verts);
+  quantize_nodes(*h);
+  return h;
+}
+
 vto_bvh *vto_lbvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
                         uint32_t nverts, int32_t leaf_size, int32_t treelet_size, int32_t rounds) {
   (void)nverts;
@@ -2810,7 +2824,9 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
   PtContext C;
   C.in = in;
   C.p = p;
-  C.bvh = vto_lbvh_build(in->faces, in->nfaces, in->verts, in->nverts, 2, 7, 2);
+  // A prebuilt hierarchy (vto_bvh_import of the device's) skips the build; it stays the caller's.
+  const bool ownBvh = in->bvh == nullptr;
+  C.bvh = ownBvh ? vto_lbvh_build(in->faces, in->nfaces, in->verts, in->nverts, 2, 7, 2) : const_cast<vto_bvh *>(in->bvh);
   C.spectral = p->spectral != 0 && in->cmf_rgb != nullptr;
   C.mats.assign(in->materials, in->materials + in->nmat);
   for (uint32_t i = 0; i < in->nmat; ++i) std::memcpy(&C.mats[i].pad, &i, sizeof i);
@@ -2909,11 +2925,14 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
       });
     }
     for (size_t i = 0; i < sum.size(); ++i) out_rgb[i] = spp ? sum[i] / spp : 0.0;
-    vto_bvh_free(C.bvh);
+    if (ownBvh) vto_bvh_free(C.bvh);
     return;
   }
-  parallel_for(npix, threads, [&](uint32_t i) {
-    const uint32_t x = i % p->width, y = i / p->width;
+  // Pixel stride s (vt_frame_params.pixel_stride, sampling modes 1-3): every s-th pixel in x and y,
+  // each with the full frame's camera ray and its own sample stream; ceil(w / s) x ceil(h / s) out.
+  const uint32_t st = std::max(1u, p->pixel_stride), OW = (p->width + st - 1) / st, OH = (p->height + st - 1) / st;
+  parallel_for(OW * OH, threads, [&](uint32_t i) {
+    const uint32_t x = (i % OW) * st, y = (i / OW) * st;
     double s[3] = {0, 0, 0};
     for (uint32_t k = 0; k < spp; ++k) {
       const D3 c = path_sample_d(C, x, y, p->first_sample + k, std::max(1u, p->first_frame) + k, jx[k], jy[k]);
@@ -2921,5 +2940,5 @@ extern "C" void vto_render(const vto_pt_inputs *in, const vt_frame_params *p, ui
     }
     for (int c = 0; c < 3; ++c) out_rgb[3 * (size_t)i + c] = spp ? s[c] / spp : 0.0;
   });
-  vto_bvh_free(C.bvh);
+  if (ownBvh) vto_bvh_free(C.bvh);
 }

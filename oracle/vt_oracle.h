@@ -52,6 +52,9 @@ vto_bvh *vto_lbvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *
 vto_bvh *vto_widebvh_build(const vt_face *faces, uint32_t nfaces, const vt_vertex *verts,
                            uint32_t nverts, int32_t leaf_size, int32_t max_depth, int32_t threads);
 void vto_bvh_free(vto_bvh *h);
+/* A hierarchy built elsewhere (4-wide nodes, leaf order, depth) over `faces` / `verts`. */
+vto_bvh *vto_bvh_import(const vt_wide_node *nodes, uint32_t nnodes, const int32_t *order, uint32_t nfaces,
+                        const vt_face *faces, const vt_vertex *verts, uint32_t depth);
 void vto_bvh_get_info(const vto_bvh *h, vto_bvh_info *out);
 void vto_bvh_get_nodes(const vto_bvh *h, vt_wide_node *out);
 void vto_bvh_get_order(const vto_bvh *h, int32_t *out);
@@ -132,6 +135,8 @@ typedef struct vto_pt_inputs {
   const float *env_rgba;
   uint32_t env_w, env_h;
   float env_rot;
+  /* A prebuilt hierarchy over these faces (vto_bvh_import); null: the renderer builds its LBVH. */
+  const vto_bvh *bvh;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

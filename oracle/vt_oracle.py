@@ -41,6 +41,7 @@ _SIGS = {
     "vto_lbvh_build": (_P, [_P, _U32, _P, _U32, _I32, _I32, _I32]),
     "vto_widebvh_build": (_P, [_P, _U32, _P, _U32, _I32, _I32, _I32]),
     "vto_bvh_free": (None, [_P]),
+    "vto_bvh_import": (_P, [_P, _U32, _P, _U32, _P, _P, _U32]),
     "vto_bvh_get_info": (None, [_P, C.POINTER(BvhInfo)]),
     "vto_bvh_get_nodes": (None, [_P, _P]),
     "vto_bvh_get_order": (None, [_P, _P]),
@@ -138,6 +139,16 @@ class Bvh:
         f, v = _faces(faces), _verts(verts)
         return cls(load().vto_lbvh_build(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0],
                                          leaf_size, treelet_size, rounds))
+
+    @classmethod
+    def from_arrays(cls, nodes, order, faces, verts, depth):
+        """A hierarchy built elsewhere (the device's 4-wide nodes, leaf order and depth) over the same
+        faces and vertices."""
+        nd = np.ascontiguousarray(nodes, WIDE_NODE_DTYPE)
+        od = np.ascontiguousarray(order, np.int32)
+        f, v = _faces(faces), _verts(verts)
+        return cls(load().vto_bvh_import(nd.ctypes.data, nd.shape[0], od.ctypes.data, od.shape[0], f.ctypes.data,
+                                         v.ctypes.data, int(depth)))
 
     @classmethod
     def widebvh(cls, faces, verts, leaf_size=2, max_depth=20, nthreads=None):
@@ -260,7 +271,7 @@ class PtInputs(C.Structure):
                 ("uplift", C.c_void_p), ("cos_phase", C.c_void_p),
                 ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p),
                 ("environment", Environment), ("env_rgba", C.c_void_p), ("env_w", C.c_uint32), ("env_h", C.c_uint32),
-                ("env_rot", C.c_float)]
+                ("env_rot", C.c_float), ("bvh", C.c_void_p)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -268,8 +279,11 @@ _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32,
 
 def render(faces, verts, materials, light, camera, width, height, spp, max_depth=8, first_sample=1,
            spectral=None, nthreads=None, mode=1, sampler=0, z_temporal=3, first_frame=1, light_tree=True,
-           emitter_words=None, di_candidates=0, aperture=0.0, focus_distance=1.0, environment=None):
-    """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames.
+           emitter_words=None, di_candidates=0, aperture=0.0, focus_distance=1.0, environment=None,
+           pixel_stride=1, bvh=None):
+    """FP64 oracle render: (height, width, 3) mean linear-sRGB radiance over `spp` frames (with a
+    pixel stride s, modes 1-3: (ceil(height / s), ceil(width / s), 3) for every s-th pixel). `bvh`: a
+    prebuilt hierarchy over the faces (Bvh.from_arrays), else the renderer builds its LBVH.
 
     light=None renders an imported scene lit by its emissive faces; its emitter list is the
     pure-Python restatement's (oracle/light_tree.py) unless `emitter_words` is given. An imported
@@ -341,9 +355,15 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
     p.sampler, p.z_temporal, p.first_frame = sampler, z_temporal, first_frame
     p.di_candidates = di_candidates
     p.aperture, p.focus_distance = aperture, focus_distance
-    out = np.empty(3 * width * height, np.float64)
+    stride = max(1, int(pixel_stride))
+    p.pixel_stride = stride
+    if bvh is not None:
+        inp.bvh = bvh._h
+        keep.append(bvh)
+    oh, ow = (height, width) if mode == 0 else (-(-height // stride), -(-width // stride))
+    out = np.empty(3 * ow * oh, np.float64)
     lib.vto_render(C.byref(inp), C.byref(p), spp, out.ctypes.data, nthreads or threads())
-    return out.reshape(height, width, 3)
+    return out.reshape(oh, ow, 3)
 
 
 _SIGS["vto_z_sequences"] = (None, [_U32, _U32, _P, _P])
