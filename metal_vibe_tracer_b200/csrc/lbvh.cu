@@ -238,97 +238,154 @@ __device__ __forceinline__ void refit_node(const TreeView &t, int i) {
 // appended), DP over subsets (partitions p = (p - 1) & s downwards, strict improvement), rebuild
 // only on a strict cost improvement, internal nodes reassigned depth first, left = the side with
 // the lowest leaf bit.
-__device__ void restructure_node(const TreeView &t, int root, int size, uint32_t *status) {
-  int leaves[kMaxTreelet], internals[kMaxTreelet];
-  int nl = 0, ni = 0;
-  internals[ni++] = root;
-  int2 rc = load_child(t, root);
-  leaves[nl++] = rc.x;
-  leaves[nl++] = rc.y;
-  while (nl < size) {
-    int best = -1;
-    float bestA = -1.0f;
-    for (int k = 0; k < nl; ++k) {
-      int c = leaves[k];
-      if (c < 0) continue;
-      Box b = load_box_cg(t.nodeBox, c);
-      float a = box_area(b.lo, b.hi);
-      if (a > bestA) { bestA = a; best = k; }
-    }
-    if (best < 0) break;
-    int c = leaves[best];
-    internals[ni++] = c;
-    int2 cc = load_child(t, c);
-    leaves[best] = cc.x;
-    leaves[nl++] = cc.y;
-  }
-  const int k = nl;
-  if (k < 3) return;
-  const int full = (1 << k) - 1;
-  float area[1 << kMaxTreelet], copt[1 << kMaxTreelet];
+//
+// One warp restructures one treelet (Karras and Aila's warp-wide DP): the subsets' areas are
+// spread over the lanes, and per subset size either the lanes take one subset each (sizes whose
+// partitions are fewer than 32) or all lanes split one subset's partitions and reduce the best
+// (cost, then serial order) with shuffles, so the chosen partition is the serial loop's. Lane 0
+// grows the treelet and rebuilds it. Scratch lives in shared memory, one slice per warp.
+struct TreeletScratch {
+  float area[1 << kMaxTreelet];
+  float copt[1 << kMaxTreelet];
   uint8_t part[1 << kMaxTreelet];
   Box lb[kMaxTreelet];
-  for (int q = 0; q < k; ++q) {
-    lb[q] = child_box(t, leaves[q]);
-    copt[1 << q] = child_cost(t, leaves[q]);
+  int leaves[kMaxTreelet], internals[kMaxTreelet];
+  int k, ni;
+};
+
+// The bits of m deposited into the set bits of s, lowest first (pdep).
+__device__ __forceinline__ int deposit_bits(int m, int s) {
+  int out = 0;
+  for (int r = s; r; r &= r - 1) {
+    if (m & 1) out |= r & -r;
+    m >>= 1;
   }
-  for (int s = 1; s <= full; ++s) {
-    int low = __ffs(s) - 1;
-    Box b = lb[low];
-    for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, lb[__ffs(r) - 1]);
-    area[s] = box_area(b.lo, b.hi);
+  return out;
+}
+
+__device__ void restructure_warp(const TreeView &t, int root, int size, uint32_t *status, TreeletScratch &w) {
+  const unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    int nl = 0, ni = 0;
+    w.internals[ni++] = root;
+    const int2 rc = load_child(t, root);
+    w.leaves[nl++] = rc.x;
+    w.leaves[nl++] = rc.y;
+    while (nl < size) {
+      int best = -1;
+      float bestA = -1.0f;
+      for (int q = 0; q < nl; ++q) {
+        const int c = w.leaves[q];
+        if (c < 0) continue;
+        const Box b = load_box_cg(t.nodeBox, c);
+        const float a = box_area(b.lo, b.hi);
+        if (a > bestA) { bestA = a; best = q; }
+      }
+      if (best < 0) break;
+      const int c = w.leaves[best];
+      w.internals[ni++] = c;
+      const int2 cc = load_child(t, c);
+      w.leaves[best] = cc.x;
+      w.leaves[nl++] = cc.y;
+    }
+    w.k = nl;
+    w.ni = ni;
   }
+  __syncwarp();
+  const int k = w.k;
+  if (k < 3) return;
+  const int full = (1 << k) - 1;
+  if (lane < k) {
+    w.lb[lane] = child_box(t, w.leaves[lane]);
+    w.copt[1 << lane] = child_cost(t, w.leaves[lane]);
+  }
+  __syncwarp();
+  for (int s = lane + 1; s <= full; s += 32) {
+    Box b = w.lb[__ffs(s) - 1];
+    for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, w.lb[__ffs(r) - 1]);
+    w.area[s] = box_area(b.lo, b.hi);
+  }
+  __syncwarp();
   for (int sz = 2; sz <= k; ++sz) {
-    for (int s = 1; s <= full; ++s) {
-      if (__popc(s) != sz) continue;
-      float best = FLT_MAX;
-      int bp = 0;
-      for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
-        float c = __fadd_rn(copt[p], copt[s ^ p]);
-        if (c < best) { best = c; bp = p; }
+    const int np = (1 << sz) - 2;  // partitions of a subset of size sz
+    if (np < 32) {
+      // A subset per lane: the j-th subset of this size (increasing s) goes to lane j mod 32.
+      int rank = 0;
+      for (int s = 1; s <= full; ++s) {
+        if (__popc(s) != sz) continue;
+        if ((rank++ & 31) != lane) continue;
+        float best = FLT_MAX;
+        int bp = 0;
+        for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+          const float c = __fadd_rn(w.copt[p], w.copt[s ^ p]);
+          if (c < best) { best = c; bp = p; }
+        }
+        w.copt[s] = __fadd_rn(__fmul_rn(kCi, w.area[s]), best);
+        w.part[s] = (uint8_t)bp;
       }
-      copt[s] = __fadd_rn(__fmul_rn(kCi, area[s]), best);
-      part[s] = (uint8_t)bp;
-    }
-  }
-  if (!(copt[full] < __ldcg(t.cost + root))) return;
-  int next = 0;
-  int st_s[kMaxTreelet * 2], st_n[kMaxTreelet * 2];
-  int top = 0;
-  st_s[top] = full; st_n[top] = internals[next++]; ++top;
-  while (top) {
-    --top;
-    const int s = st_s[top], node = st_n[top];
-    const int p = part[s], q = s ^ p;
-    const int lowbit = s & -s;
-    const int subs[2] = {(p & lowbit) ? p : q, (p & lowbit) ? q : p};
-    int kids[2];
-    for (int c = 0; c < 2; ++c) {
-      const int x = subs[c];
-      if ((x & (x - 1)) == 0) kids[c] = leaves[__ffs(x) - 1];
-      else {
-        if (next >= ni) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
-        kids[c] = internals[next++];
+    } else {
+      // All lanes on one subset: partition i (serial order, p descending) is deposit(np - i, s).
+      for (int s = 1; s <= full; ++s) {
+        if (__popc(s) != sz) continue;
+        float best = FLT_MAX;
+        int bi = 0x7fffffff;
+        for (int i = lane; i < np; i += 32) {
+          const int p = deposit_bits(np - i, s);
+          const float c = __fadd_rn(w.copt[p], w.copt[s ^ p]);
+          if (c < best) { best = c; bi = i; }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+          const float ob = __shfl_xor_sync(kAll, best, off);
+          const int oi = __shfl_xor_sync(kAll, bi, off);
+          if (ob < best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (lane == 0) {
+          w.copt[s] = __fadd_rn(__fmul_rn(kCi, w.area[s]), best);
+          w.part[s] = (uint8_t)deposit_bits(np - bi, s);
+        }
       }
     }
-    __stcg(t.child + node, make_int2(kids[0], kids[1]));
-    for (int c = 1; c >= 0; --c)
-      if ((subs[c] & (subs[c] - 1)) != 0) { st_s[top] = subs[c]; st_n[top] = kids[c]; ++top; }
+    __syncwarp();
   }
-  for (int i = ni - 1; i >= 0; --i) {
-    const int nd = internals[i];
-    refit_node(t, nd);
-    int2 ch = load_child(t, nd);
-    __stcg(t.parent + (ch.x >= 0 ? ch.x : (t.n - 1 + (-ch.x - 1))), nd);
-    __stcg(t.parent + (ch.y >= 0 ? ch.y : (t.n - 1 + (-ch.y - 1))), nd);
+  if (!(w.copt[full] < __ldcg(t.cost + root))) return;
+  if (lane == 0) {
+    int next = 0;
+    int st_s[kMaxTreelet * 2], st_n[kMaxTreelet * 2];
+    int top = 0;
+    st_s[top] = full; st_n[top] = w.internals[next++]; ++top;
+    while (top) {
+      --top;
+      const int s = st_s[top], node = st_n[top];
+      const int p = w.part[s], q = s ^ p;
+      const int lowbit = s & -s;
+      const int subs[2] = {(p & lowbit) ? p : q, (p & lowbit) ? q : p};
+      int kids[2];
+      for (int c = 0; c < 2; ++c) {
+        const int x = subs[c];
+        if ((x & (x - 1)) == 0) kids[c] = w.leaves[__ffs(x) - 1];
+        else {
+          if (next >= w.ni) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
+          kids[c] = w.internals[next++];
+        }
+      }
+      __stcg(t.child + node, make_int2(kids[0], kids[1]));
+      for (int c = 1; c >= 0; --c)
+        if ((subs[c] & (subs[c] - 1)) != 0) { st_s[top] = subs[c]; st_n[top] = kids[c]; ++top; }
+    }
+    for (int i = w.ni - 1; i >= 0; --i) {
+      const int nd = w.internals[i];
+      refit_node(t, nd);
+      const int2 ch = load_child(t, nd);
+      __stcg(t.parent + (ch.x >= 0 ? ch.x : (t.n - 1 + (-ch.x - 1))), nd);
+      __stcg(t.parent + (ch.y >= 0 ? ch.y : (t.n - 1 + (-ch.y - 1))), nd);
+    }
   }
 }
 
 // One thread per leaf walks to the root; the second thread to reach a node owns it (its two
-// subtrees are final) and refits it (mode 0) or restructures it (mode 1: subtrees with >= size
-// leaves). flags[] must be zero on entry.
-__global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, int mode, int size,
-                                                    uint32_t *status) {
+// subtrees are final) and refits it. flags[] must be zero on entry.
+__global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, uint32_t *status) {
   const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
   if (leaf >= t.n) return;
   int node = __ldcg(t.parent + (t.n - 1 + leaf));
@@ -338,10 +395,47 @@ __global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, 
     __threadfence();
     if (atomicAdd(&flags[node], 1u) == 0u) return;
     __threadfence();
-    if (mode == 0) refit_node(t, node);
-    else if (__ldcg(t.count + node) >= (uint32_t)size) restructure_node(t, node, size, status);
+    refit_node(t, node);
     __threadfence();
     node = __ldcg(t.parent + node);
+  }
+}
+
+// The same walk for restructuring: a node owned by a lane whose subtree has >= size leaves is
+// restructured by the whole warp (restructure_warp), owned nodes in lane order. Nodes owned by
+// lanes of one warp in the same step are disjoint subtrees (an owner's subtrees are final), so
+// restructuring them one after another is what the thread-per-node order gives.
+__global__ void __launch_bounds__(128) k_restructure(TreeView t, uint32_t *flags, int size, uint32_t *status) {
+  __shared__ TreeletScratch scratch[4];
+  TreeletScratch &w = scratch[threadIdx.x >> 5];
+  const unsigned kAll = 0xffffffffu;
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  int node = leaf < t.n ? __ldcg(t.parent + (t.n - 1 + leaf)) : -1;
+  int guard = 0;
+  while (true) {
+    bool own = false;
+    if (node >= 0) {
+      if (guard++ >= t.n) {
+        atomicOr(status, (uint32_t)VT_DEV_TREELET);
+        node = -1;
+      } else {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1u) == 0u) node = -1;
+        else own = true;
+        __threadfence();
+      }
+    }
+    unsigned work = __ballot_sync(kAll, own && __ldcg(t.count + node) >= (uint32_t)size);
+    while (work) {
+      const int src = __ffs(work) - 1;
+      work &= work - 1;
+      const int root = __shfl_sync(kAll, node, src);
+      restructure_warp(t, root, size, status, w);
+      __syncwarp();
+      __threadfence();
+    }
+    if (own) node = __ldcg(t.parent + node);
+    if (!__any_sync(kAll, node >= 0)) break;
   }
 }
 
@@ -567,11 +661,11 @@ vt_status vt_lbvh_build(vt_ctx *ctx, const vt_face *faces, uint32_t nfaces, cons
   if (n >= 2) {
     k_karras<<<blocks(n - 1, 256), 256, 0, s>>>(codes, (int)n, child, parent);
     VT_CUDA(ctx, cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), s));
-    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, flags, 0, 0, ctx->d_status);
+    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, flags, ctx->d_status);
     if (treelet > 0 && n >= 3) {
       for (int r = 0; r < rounds; ++r) {
         VT_CUDA(ctx, cudaMemsetAsync(flags, 0, ni * sizeof(uint32_t), s));
-        k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, flags, 1, treelet, ctx->d_status);
+        k_restructure<<<blocks(n, 128), 128, 0, s>>>(t, flags, treelet, ctx->d_status);
       }
     }
   }
@@ -848,11 +942,11 @@ extern "C" vt_status vt_mesh_build_noalloc(const vt_face *faces, uint32_t nfaces
   if (n >= 2) {
     k_karras<<<blocks(n - 1, 256), 256, 0, s>>>(b.codes, (int)n, b.child, b.parent);
     VT_NA(cudaMemsetAsync(b.flags, 0, ni * sizeof(uint32_t), s));
-    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, 0, 0, b.status);
+    k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, b.status);
     if (treelet > 0 && n >= 3) {
       for (int r = 0; r < rounds; ++r) {
         VT_NA(cudaMemsetAsync(b.flags, 0, ni * sizeof(uint32_t), s));
-        k_bottom_up<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, 1, treelet, b.status);
+        k_restructure<<<blocks(n, 128), 128, 0, s>>>(t, b.flags, treelet, b.status);
       }
     }
   }
