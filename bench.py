@@ -452,7 +452,7 @@ def bench_batch(a, ctx) -> dict:
 
 def bench_production(a, ctx, stream) -> dict:
     """The production-scale scene: ~10M triangles of displaced icospheres, ~100k emissive triangles
-    under a light tree, 287 OPENPBR material slots (thin film left out), at 1920x1080, spectral
+    under a light tree, 287 OPENPBR material slots (10 % with thin films), at 1920x1080, spectral
     (4 wavelengths), depth 12: ReSTIR DI with 32 candidates (temporal + spatial reuse) and plain MIS
     path tracing. Device time per frame."""
     import torch

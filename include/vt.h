@@ -451,6 +451,8 @@ vt_status vt_openpbr_energy_table(vt_ctx *ctx, float *table, float *average);
 typedef struct vt_openpbr_case {
   float base_color[3], metalness, roughness, ior, specular_weight, diffuse_roughness;
   float normal[3], view[3], light[3], rand[3];
+  float thin_film_weight, thin_film_thickness /* micrometres */, thin_film_ior;
+  float lambda[3];      /* the preparation's wavelengths in nm; 0: the upstream RGB wavelengths */
 } vt_openpbr_case;
 /* f |cos| at the light direction and its pdf; the sample: direction, weight f |cos| / pdf, its pdf,
  * and 1 when a sample was produced. 48 bytes. */
@@ -466,6 +468,9 @@ vt_status vt_openpbr_evaluate(vt_ctx *ctx, const vt_openpbr_case *cases, uint32_
  * slots whose type is VT_MAT_OPENPBR. Needs vt_openpbr_tables_set on the context first. */
 typedef struct vt_openpbr_params {
   float roughness, metalness, ior, diffuse_roughness;
+  /* Thin-film iridescence (SpectralMaterial, main.swift:730-735; spectral transport only, as the
+   * reference's adapter): weight in [0, 1], thickness in micrometres, IOR. */
+  float thin_film_weight, thin_film_thickness, thin_film_ior, pad;
 } vt_openpbr_params;
 vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n);
 

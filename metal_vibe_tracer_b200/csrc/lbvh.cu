@@ -239,18 +239,115 @@ __device__ __forceinline__ void refit_node(const TreeView &t, int i) {
 // only on a strict cost improvement, internal nodes reassigned depth first, left = the side with
 // the lowest leaf bit.
 //
-// One warp restructures one treelet (Karras and Aila's warp-wide DP): the subsets' areas are
-// spread over the lanes, and per subset size either the lanes take one subset each (sizes whose
-// partitions are fewer than 32) or all lanes split one subset's partitions and reduce the best
-// (cost, then serial order) with shuffles, so the chosen partition is the serial loop's. Lane 0
-// grows the treelet and rebuilds it. Scratch lives in shared memory, one slice per warp.
+// Two executions of that one algorithm give the same tree. restructure_node is one thread's
+// serial loop. restructure_warp spreads one treelet over a warp (Karras and Aila's warp-wide DP):
+// lane q holds treelet leaf q while the treelet grows (its box, children, cost and leaf count
+// loaded in one round trip, the largest area chosen by a shuffle reduction that keeps the first
+// slot on ties); the subsets are listed by size with ballots (increasing s within a size); per
+// size either each lane takes whole subsets (fewer than 32 partitions) or all lanes split one
+// subset's partitions and reduce (cost, then serial order), so the chosen partition is the
+// serial loop's; the rebuilt nodes' boxes, counts and costs are formed in shared memory in
+// refit_node's order (union of left then right, costs added left + right) and stored by one lane
+// per node. Scratch lives in shared memory, one slice per warp.
+__device__ void restructure_node(const TreeView &t, int root, int size, uint32_t *status) {
+  int leaves[kMaxTreelet], internals[kMaxTreelet];
+  int nl = 0, ni = 0;
+  internals[ni++] = root;
+  int2 rc = load_child(t, root);
+  leaves[nl++] = rc.x;
+  leaves[nl++] = rc.y;
+  while (nl < size) {
+    int best = -1;
+    float bestA = -1.0f;
+    for (int k = 0; k < nl; ++k) {
+      int c = leaves[k];
+      if (c < 0) continue;
+      Box b = load_box_cg(t.nodeBox, c);
+      float a = box_area(b.lo, b.hi);
+      if (a > bestA) { bestA = a; best = k; }
+    }
+    if (best < 0) break;
+    int c = leaves[best];
+    internals[ni++] = c;
+    int2 cc = load_child(t, c);
+    leaves[best] = cc.x;
+    leaves[nl++] = cc.y;
+  }
+  const int k = nl;
+  if (k < 3) return;
+  const int full = (1 << k) - 1;
+  float area[1 << kMaxTreelet], copt[1 << kMaxTreelet];
+  uint8_t part[1 << kMaxTreelet];
+  Box lb[kMaxTreelet];
+  for (int q = 0; q < k; ++q) {
+    lb[q] = child_box(t, leaves[q]);
+    copt[1 << q] = child_cost(t, leaves[q]);
+  }
+  for (int s = 1; s <= full; ++s) {
+    int low = __ffs(s) - 1;
+    Box b = lb[low];
+    for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, lb[__ffs(r) - 1]);
+    area[s] = box_area(b.lo, b.hi);
+  }
+  for (int sz = 2; sz <= k; ++sz) {
+    for (int s = 1; s <= full; ++s) {
+      if (__popc(s) != sz) continue;
+      float best = FLT_MAX;
+      int bp = 0;
+      for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
+        float c = __fadd_rn(copt[p], copt[s ^ p]);
+        if (c < best) { best = c; bp = p; }
+      }
+      copt[s] = __fadd_rn(__fmul_rn(kCi, area[s]), best);
+      part[s] = (uint8_t)bp;
+    }
+  }
+  if (!(copt[full] < __ldcg(t.cost + root))) return;
+  int next = 0;
+  int st_s[kMaxTreelet * 2], st_n[kMaxTreelet * 2];
+  int top = 0;
+  st_s[top] = full; st_n[top] = internals[next++]; ++top;
+  while (top) {
+    --top;
+    const int s = st_s[top], node = st_n[top];
+    const int p = part[s], q = s ^ p;
+    const int lowbit = s & -s;
+    const int subs[2] = {(p & lowbit) ? p : q, (p & lowbit) ? q : p};
+    int kids[2];
+    for (int c = 0; c < 2; ++c) {
+      const int x = subs[c];
+      if ((x & (x - 1)) == 0) kids[c] = leaves[__ffs(x) - 1];
+      else {
+        if (next >= ni) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
+        kids[c] = internals[next++];
+      }
+    }
+    __stcg(t.child + node, make_int2(kids[0], kids[1]));
+    for (int c = 1; c >= 0; --c)
+      if ((subs[c] & (subs[c] - 1)) != 0) { st_s[top] = subs[c]; st_n[top] = kids[c]; ++top; }
+  }
+  for (int i = ni - 1; i >= 0; --i) {
+    const int nd = internals[i];
+    refit_node(t, nd);
+    int2 ch = load_child(t, nd);
+    __stcg(t.parent + (ch.x >= 0 ? ch.x : (t.n - 1 + (-ch.x - 1))), nd);
+    __stcg(t.parent + (ch.y >= 0 ? ch.y : (t.n - 1 + (-ch.y - 1))), nd);
+  }
+}
+
 struct TreeletScratch {
   float area[1 << kMaxTreelet];
   float copt[1 << kMaxTreelet];
   uint8_t part[1 << kMaxTreelet];
-  Box lb[kMaxTreelet];
+  uint8_t list[1 << kMaxTreelet];  // subsets grouped by size, increasing within a size
+  Box lb[kMaxTreelet];             // treelet leaves' boxes
+  Box nb[kMaxTreelet];             // rebuilt internal nodes' boxes (assignment order)
+  float nc[kMaxTreelet];           // and costs
+  uint32_t ncount[kMaxTreelet], lcount[kMaxTreelet];
   int leaves[kMaxTreelet], internals[kMaxTreelet];
-  int k, ni;
+  int2 kid[kMaxTreelet];           // rebuilt node j's children: >= 0 internal index, else -(leaf slot + 1)
+  int start[kMaxTreelet + 2];      // list offset of each subset size
+  int ok;
 };
 
 // The bits of m deposited into the set bits of s, lowest first (pdep).
@@ -266,55 +363,99 @@ __device__ __forceinline__ int deposit_bits(int m, int s) {
 __device__ void restructure_warp(const TreeView &t, int root, int size, uint32_t *status, TreeletScratch &w) {
   const unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  if (lane == 0) {
-    int nl = 0, ni = 0;
-    w.internals[ni++] = root;
-    const int2 rc = load_child(t, root);
-    w.leaves[nl++] = rc.x;
-    w.leaves[nl++] = rc.y;
-    while (nl < size) {
-      int best = -1;
-      float bestA = -1.0f;
-      for (int q = 0; q < nl; ++q) {
-        const int c = w.leaves[q];
-        if (c < 0) continue;
-        const Box b = load_box_cg(t.nodeBox, c);
-        const float a = box_area(b.lo, b.hi);
-        if (a > bestA) { bestA = a; best = q; }
+  const float rootCost = __ldcg(t.cost + root);
+  const int2 rc = load_child(t, root);
+  // Lane q < nl holds treelet leaf q: its node, box, children, cost and leaf count.
+  int myLeaf = lane == 0 ? rc.x : rc.y;
+  bool dirty = lane < 2;
+  Box myBox{};
+  int2 myKids = make_int2(0, 0);
+  float myArea = -INFINITY, myCost = 0.0f;
+  uint32_t myCount = 1u;
+  int myInternal = lane == 0 ? root : -1;
+  int nl = 2, ni = 1;
+  while (true) {
+    if (dirty) {
+      if (myLeaf >= 0) {
+        myBox = load_box_cg(t.nodeBox, myLeaf);
+        myKids = load_child(t, myLeaf);
+        myCost = __ldcg(t.cost + myLeaf);
+        myCount = __ldcg(t.count + myLeaf);
+        myArea = box_area(myBox.lo, myBox.hi);
+      } else {
+        myBox = load_box_cg(t.leafBox, -myLeaf - 1);
+        myCost = __fmul_rn(kCt, box_area(myBox.lo, myBox.hi));
+        myCount = 1u;
+        myArea = -INFINITY;  // a primitive is never opened
       }
-      if (best < 0) break;
-      const int c = w.leaves[best];
-      w.internals[ni++] = c;
-      const int2 cc = load_child(t, c);
-      w.leaves[best] = cc.x;
-      w.leaves[nl++] = cc.y;
+      dirty = false;
     }
-    w.k = nl;
-    w.ni = ni;
+    if (nl >= size) break;
+    float a = lane < nl ? myArea : -INFINITY;
+    int q = lane;
+    for (int off = 16; off > 0; off >>= 1) {
+      const float oa = __shfl_xor_sync(kAll, a, off);
+      const int oq = __shfl_xor_sync(kAll, q, off);
+      if (oa > a || (oa == a && oq < q)) { a = oa; q = oq; }
+    }
+    if (a == -INFINITY) break;  // no internal node left to open
+    const int c = __shfl_sync(kAll, myLeaf, q);
+    const int cx = __shfl_sync(kAll, myKids.x, q), cy = __shfl_sync(kAll, myKids.y, q);
+    if (lane == ni) myInternal = c;
+    if (lane == q) { myLeaf = cx; dirty = true; }
+    if (lane == nl) { myLeaf = cy; dirty = true; }
+    ++ni;
+    ++nl;
   }
-  __syncwarp();
-  const int k = w.k;
+  const int k = nl;
   if (k < 3) return;
   const int full = (1 << k) - 1;
   if (lane < k) {
-    w.lb[lane] = child_box(t, w.leaves[lane]);
-    w.copt[1 << lane] = child_cost(t, w.leaves[lane]);
+    w.leaves[lane] = myLeaf;
+    w.lb[lane] = myBox;
+    w.copt[1 << lane] = myCost;
+    w.lcount[lane] = myCount;
+  }
+  if (lane < ni) w.internals[lane] = myInternal;
+  if (lane == 0) {
+    // Subsets of size j start after those of sizes 2..j-1: C(k, 2) + ... + C(k, j-1).
+    int off = 0, c = k;  // c = C(k, j) for j = 1
+    for (int j = 2; j <= k; ++j) {
+      c = c * (k - j + 1) / j;
+      w.start[j] = off;
+      off += c;
+    }
+    w.start[k + 1] = off;
   }
   __syncwarp();
-  for (int s = lane + 1; s <= full; s += 32) {
-    Box b = w.lb[__ffs(s) - 1];
-    for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, w.lb[__ffs(r) - 1]);
-    w.area[s] = box_area(b.lo, b.hi);
+  // Subset areas and the by-size lists, 32 subsets per step.
+  int fill[kMaxTreelet + 1];
+#pragma unroll
+  for (int j = 0; j <= kMaxTreelet; ++j) fill[j] = 0;
+  for (int base = 0; base < full; base += 32) {
+    const int s = base + lane + 1;
+    const bool valid = s <= full;
+    if (valid) {
+      Box b = w.lb[__ffs(s) - 1];
+      for (int r = s & (s - 1); r; r &= r - 1) b = box_union(b, w.lb[__ffs(r) - 1]);
+      w.area[s] = box_area(b.lo, b.hi);
+    }
+    const int pc = valid ? __popc(s) : 0;
+#pragma unroll
+    for (int j = 2; j <= kMaxTreelet; ++j) {
+      if (j > k) break;
+      const unsigned m = __ballot_sync(kAll, pc == j);
+      if (pc == j) w.list[w.start[j] + fill[j] + __popc(m & ((1u << lane) - 1u))] = (uint8_t)s;
+      fill[j] += __popc(m);
+    }
   }
   __syncwarp();
   for (int sz = 2; sz <= k; ++sz) {
     const int np = (1 << sz) - 2;  // partitions of a subset of size sz
+    const int b0 = w.start[sz], nsub = w.start[sz + 1] - b0;
     if (np < 32) {
-      // A subset per lane: the j-th subset of this size (increasing s) goes to lane j mod 32.
-      int rank = 0;
-      for (int s = 1; s <= full; ++s) {
-        if (__popc(s) != sz) continue;
-        if ((rank++ & 31) != lane) continue;
+      for (int j = lane; j < nsub; j += 32) {
+        const int s = w.list[b0 + j];
         float best = FLT_MAX;
         int bp = 0;
         for (int p = (s - 1) & s; p > 0; p = (p - 1) & s) {
@@ -326,8 +467,8 @@ __device__ void restructure_warp(const TreeView &t, int root, int size, uint32_t
       }
     } else {
       // All lanes on one subset: partition i (serial order, p descending) is deposit(np - i, s).
-      for (int s = 1; s <= full; ++s) {
-        if (__popc(s) != sz) continue;
+      for (int j = 0; j < nsub; ++j) {
+        const int s = w.list[b0 + j];
         float best = FLT_MAX;
         int bi = 0x7fffffff;
         for (int i = lane; i < np; i += 32) {
@@ -348,39 +489,63 @@ __device__ void restructure_warp(const TreeView &t, int root, int size, uint32_t
     }
     __syncwarp();
   }
-  if (!(w.copt[full] < __ldcg(t.cost + root))) return;
+  if (!(w.copt[full] < rootCost)) return;
   if (lane == 0) {
-    int next = 0;
-    int st_s[kMaxTreelet * 2], st_n[kMaxTreelet * 2];
+    // Depth-first assignment of the internal nodes (index j in assignment order), then their
+    // boxes, counts and costs bottom up (children are assigned after their parent).
+    int next = 1;
+    int st_s[kMaxTreelet * 2], st_j[kMaxTreelet * 2];
     int top = 0;
-    st_s[top] = full; st_n[top] = w.internals[next++]; ++top;
+    st_s[top] = full; st_j[top] = 0; ++top;
+    w.ok = 1;
     while (top) {
       --top;
-      const int s = st_s[top], node = st_n[top];
+      const int s = st_s[top], j = st_j[top];
       const int p = w.part[s], q = s ^ p;
       const int lowbit = s & -s;
       const int subs[2] = {(p & lowbit) ? p : q, (p & lowbit) ? q : p};
-      int kids[2];
+      int ref[2];
       for (int c = 0; c < 2; ++c) {
         const int x = subs[c];
-        if ((x & (x - 1)) == 0) kids[c] = w.leaves[__ffs(x) - 1];
+        if ((x & (x - 1)) == 0) ref[c] = -__ffs(x);  // -(leaf slot + 1)
         else {
-          if (next >= w.ni) { atomicOr(status, (uint32_t)VT_DEV_TREELET); return; }
-          kids[c] = w.internals[next++];
+          if (next >= ni) { w.ok = 0; top = 0; break; }
+          ref[c] = next++;
         }
       }
-      __stcg(t.child + node, make_int2(kids[0], kids[1]));
+      if (!w.ok) break;
+      w.kid[j] = make_int2(ref[0], ref[1]);
       for (int c = 1; c >= 0; --c)
-        if ((subs[c] & (subs[c] - 1)) != 0) { st_s[top] = subs[c]; st_n[top] = kids[c]; ++top; }
+        if (ref[c] >= 0) { st_s[top] = subs[c]; st_j[top] = ref[c]; ++top; }
     }
-    for (int i = w.ni - 1; i >= 0; --i) {
-      const int nd = w.internals[i];
-      refit_node(t, nd);
-      const int2 ch = load_child(t, nd);
-      __stcg(t.parent + (ch.x >= 0 ? ch.x : (t.n - 1 + (-ch.x - 1))), nd);
-      __stcg(t.parent + (ch.y >= 0 ? ch.y : (t.n - 1 + (-ch.y - 1))), nd);
+    if (w.ok) {
+      for (int j = ni - 1; j >= 0; --j) {
+        const int2 r = w.kid[j];
+        const Box bx = r.x >= 0 ? w.nb[r.x] : w.lb[-r.x - 1];
+        const Box by = r.y >= 0 ? w.nb[r.y] : w.lb[-r.y - 1];
+        const Box b = box_union(bx, by);
+        const float cx = r.x >= 0 ? w.nc[r.x] : w.copt[1 << (-r.x - 1)];
+        const float cy = r.y >= 0 ? w.nc[r.y] : w.copt[1 << (-r.y - 1)];
+        w.nb[j] = b;
+        w.nc[j] = __fadd_rn(__fmul_rn(kCi, box_area(b.lo, b.hi)), __fadd_rn(cx, cy));
+        w.ncount[j] = (r.x >= 0 ? w.ncount[r.x] : w.lcount[-r.x - 1]) + (r.y >= 0 ? w.ncount[r.y] : w.lcount[-r.y - 1]);
+      }
+    } else {
+      atomicOr(status, (uint32_t)VT_DEV_TREELET);
     }
   }
+  __syncwarp();
+  if (!w.ok || lane >= ni) return;
+  const int node = w.internals[lane];
+  const int2 r = w.kid[lane];
+  const int kx = r.x >= 0 ? w.internals[r.x] : w.leaves[-r.x - 1];
+  const int ky = r.y >= 0 ? w.internals[r.y] : w.leaves[-r.y - 1];
+  __stcg(t.child + node, make_int2(kx, ky));
+  store_box(t.nodeBox, node, w.nb[lane]);
+  __stcg(t.count + node, w.ncount[lane]);
+  __stcg(t.cost + node, w.nc[lane]);
+  __stcg(t.parent + (kx >= 0 ? kx : (t.n - 1 + (-kx - 1))), node);
+  __stcg(t.parent + (ky >= 0 ? ky : (t.n - 1 + (-ky - 1))), node);
 }
 
 // One thread per leaf walks to the root; the second thread to reach a node owns it (its two
@@ -401,10 +566,11 @@ __global__ void __launch_bounds__(128) k_bottom_up(TreeView t, uint32_t *flags, 
   }
 }
 
-// The same walk for restructuring: a node owned by a lane whose subtree has >= size leaves is
-// restructured by the whole warp (restructure_warp), owned nodes in lane order. Nodes owned by
-// lanes of one warp in the same step are disjoint subtrees (an owner's subtrees are final), so
-// restructuring them one after another is what the thread-per-node order gives.
+// The same walk for restructuring. Nodes owned by lanes of one warp in the same step are disjoint
+// subtrees (an owner's subtrees are final), so they may be restructured in any order: when more
+// than kWarpTreelets lanes own a node with >= size leaves, each runs restructure_node on its own;
+// otherwise the whole warp takes them one after another (restructure_warp).
+constexpr int kWarpTreelets = 4;
 __global__ void __launch_bounds__(128) k_restructure(TreeView t, uint32_t *flags, int size, uint32_t *status) {
   __shared__ TreeletScratch scratch[4];
   TreeletScratch &w = scratch[threadIdx.x >> 5];
@@ -425,15 +591,21 @@ __global__ void __launch_bounds__(128) k_restructure(TreeView t, uint32_t *flags
         __threadfence();
       }
     }
-    unsigned work = __ballot_sync(kAll, own && __ldcg(t.count + node) >= (uint32_t)size);
-    while (work) {
-      const int src = __ffs(work) - 1;
-      work &= work - 1;
-      const int root = __shfl_sync(kAll, node, src);
-      restructure_warp(t, root, size, status, w);
-      __syncwarp();
-      __threadfence();
+    const bool mine = own && __ldcg(t.count + node) >= (uint32_t)size;
+    unsigned work = __ballot_sync(kAll, mine);
+    if (__popc(work) > kWarpTreelets) {
+      if (mine) restructure_node(t, node, size, status);
+    } else {
+      while (work) {
+        const int src = __ffs(work) - 1;
+        work &= work - 1;
+        const int root = __shfl_sync(kAll, node, src);
+        restructure_warp(t, root, size, status, w);
+        __syncwarp();
+      }
     }
+    __syncwarp();
+    __threadfence();
     if (own) node = __ldcg(t.parent + node);
     if (!__any_sync(kAll, node >= 0)) break;
   }

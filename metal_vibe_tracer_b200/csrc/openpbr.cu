@@ -48,6 +48,7 @@ __global__ void k_metal_energy(float *__restrict__ table) {
 struct CaseDev {
   float base[3], metal, rough, ior, sw, diffRough;
   float n[3], wo[3], wi[3], rand[3];
+  float tfWeight, tfThickness, tfIor, lambda[3];
 };
 struct ResultDev {
   float fcos[3], pdf, dir[3], weight[3], spdf, ok;
@@ -63,6 +64,11 @@ __device__ __forceinline__ PbrParams case_params(const CaseDev &c) {
   P.ior = fmaxf(1.01f, c.ior);
   P.sw = c.sw;
   P.diffRough = c.diffRough;
+  P.tfWeight = c.tfWeight;
+  P.tfThickness = c.tfThickness;
+  P.tfIor = c.tfIor;
+  // The upstream RGB wavelengths unless the case gives its own (openpbr_bsdf.h: OpenPBR_BaseRgbWavelengths_nm).
+  P.lambda = c.lambda[0] > 0.0f ? pf3(c.lambda[0], c.lambda[1], c.lambda[2]) : pf3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
   return P;
 }
 

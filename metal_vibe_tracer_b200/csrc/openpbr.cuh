@@ -20,8 +20,10 @@
 // reference substitutes it (scripts/prepare_shaders.py:28-39).
 //
 // What the restatement covers: specular_weight, base_color, base_metalness, specular_roughness,
-// specular_ior, base_diffuse_roughness, with coat, fuzz, transmission, subsurface, thin film,
-// anisotropy and dispersion at zero. In that case the upstream coat and fuzz layers pass the base
+// specular_ior, base_diffuse_roughness, and thin-film iridescence (thin_film_weight, _thickness,
+// _ior, at the preparation's three wavelengths; impl/openpbr_thin_film_iridescence_utils.h and
+// openpbr_reflection_coefficient, impl/openpbr_reflection_transmission_coefficient.h:55-125), with
+// coat, fuzz, transmission, subsurface, anisotropy and dispersion at zero. In that case the upstream coat and fuzz layers pass the base
 // through (presence 0), the dielectric multiple-scattering lobe and both thin-wall lobes have zero
 // weight and value, and specular transmission has zero probability; the code below keeps only what
 // is left, in the upstream operation order. The coat and fuzz layers' recomputation of the sample
@@ -43,12 +45,16 @@ constexpr float kPbrMinAlphaEnergyLoss = 0.04f * 0.04f;
 constexpr int kPbrTable = 32;           // the opaque-dielectric energy tables' size per axis
 constexpr float kPbrIorMax = 2.5f;
 constexpr uint32_t kMetalEnergyN = 129;  // the dense metal table: 129 roughness x 129 sqrt-cosine nodes
+// The upstream library's wavelengths for R, G and B (openpbr_constants.h: OpenPBR_BaseRgbWavelengths_nm).
+__device__ constexpr float kPbrRgbNm[3] = {620.0f, 540.0f, 450.0f};
 
 // Per slot: base colour (clamped), metalness, roughness (>= 0.03), IOR (>= 1.01), specular weight,
 // diffuse roughness.
 struct PbrParams {
   float3 base;
   float metal, rough, ior, sw, diffRough;
+  float tfWeight, tfThickness, tfIor;  // thin film: weight, thickness (micrometres), IOR
+  float3 lambda;                       // the preparation's three wavelengths (nm)
 };
 
 struct PbrTables {
@@ -213,6 +219,137 @@ __device__ __forceinline__ float pbr_opaque_average(const PbrTables &T, float io
   return pbr_beyond_ior_max(pmix(v0, v1, ty), ior);
 }
 
+// ---- thin-film iridescence (impl/openpbr_thin_film_iridescence_utils.h) --------------------------
+// An Airy sum over the film between the exterior medium and the base: real Fresnel amplitudes at the
+// exterior-film interface, complex ones (Snell's law with a complex base IOR, the decaying branch) at
+// the film-base interface, the base a dielectric (the weighted specular IOR) or a conductor whose
+// n + i k follow Gulbrandsen's fit from F0 and the F82 tint, the phase 2 pi (2 n_film d cos_t) / lambda
+// per channel; s and p averaged.
+struct PbrCx {
+  float x, y;
+};
+__device__ __forceinline__ PbrCx cx(float x, float y) { return PbrCx{x, y}; }
+__device__ __forceinline__ PbrCx cx_add(PbrCx a, PbrCx b) { return cx(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ PbrCx cx_sub(PbrCx a, PbrCx b) { return cx(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ PbrCx cx_scale(float s, PbrCx a) { return cx(s * a.x, s * a.y); }
+__device__ __forceinline__ PbrCx cx_mul(PbrCx a, PbrCx b) { return cx(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+// z1 / z2, or `fallback` when |z2| is below min_denom.
+__device__ __forceinline__ PbrCx cx_div(PbrCx a, PbrCx b, float minDenom, PbrCx fallback) {
+  const float d = b.x * b.x + b.y * b.y;
+  if (d < minDenom * minDenom) return fallback;
+  const float r = 1.0f / d;
+  return cx((a.x * b.x + a.y * b.y) * r, (a.y * b.x - a.x * b.y) * r);
+}
+__device__ __forceinline__ PbrCx cx_sqrt(PbrCx z) {
+  const float r = sqrtf(z.x * z.x + z.y * z.y);
+  const float a = sqrtf(fmaxf((r + z.x) * 0.5f, 0.0f));
+  const float b = (z.y >= 0.0f ? 1.0f : -1.0f) * sqrtf(fmaxf((r - z.x) * 0.5f, 0.0f));
+  return cx(a, b);
+}
+constexpr float kPbrMinDenom = 1e-9f;
+
+// Complex cos(theta_t) by Snell's law (total internal reflection gives a complex angle), on the branch
+// with Im(eta_t cos_t) >= 0.
+__device__ __forceinline__ PbrCx pbr_snell_cos(float ci, float ei, PbrCx et) {
+  const float si = sqrtf(psat(1.0f - ci * ci));
+  const PbrCx st = cx_scale(si, cx_div(cx(ei, 0.0f), et, kPbrMinDenom, cx(1.0f, 0.0f)));
+  PbrCx ct = cx_sqrt(cx_sub(cx(1.0f, 0.0f), cx_mul(st, st)));
+  if (cx_mul(et, ct).y < 0.0f) ct = cx(-ct.x, -ct.y);
+  return ct;
+}
+// Reflection amplitudes (s, p) into a dielectric or conductor eta_t.
+__device__ __forceinline__ void pbr_fresnel_amp_cx(float ci, float ei, PbrCx et, PbrCx &rs, PbrCx &rp) {
+  const PbrCx ct = pbr_snell_cos(ci, ei, et);
+  const PbrCx eici = cx(ei * ci, 0.0f), etct = cx_mul(et, ct), etci = cx_scale(ci, et), eict = cx_scale(ei, ct);
+  rs = cx_div(cx_sub(eici, etct), cx_add(eici, etct), kPbrMinDenom, cx(1.0f, 0.0f));
+  rp = cx_div(cx_sub(etci, eict), cx_add(etci, eict), kPbrMinDenom, cx(1.0f, 0.0f));
+}
+// Real reflection and transmission amplitudes (s, p) between dielectrics; cos_t 0 under TIR.
+__device__ __forceinline__ void pbr_fresnel_amp(float ci, float ei, float et, float2 &r, float2 &t, float &ct) {
+  const float si = sqrtf(psat(1.0f - ci * ci));
+  const float st = ei / et * si;
+  if (st >= 1.0f) {
+    r = make_float2(1.0f, 1.0f);
+    t = make_float2(0.0f, 0.0f);
+    ct = 0.0f;
+    return;
+  }
+  ct = sqrtf(psat(1.0f - st * st));
+  const float eici = ei * ci, etct = et * ct, etci = et * ci, eict = ei * ct;
+  float ds = eici + etct, dp = etci + eict;
+  if (fabsf(ds) < kPbrMinDenom) ds = ds >= 0.0f ? kPbrMinDenom : -kPbrMinDenom;
+  if (fabsf(dp) < kPbrMinDenom) dp = dp >= 0.0f ? kPbrMinDenom : -kPbrMinDenom;
+  const float rds = 1.0f / ds, rdp = 1.0f / dp;
+  r = make_float2((eici - etct) * rds, (etci - eict) * rdp);
+  t = make_float2((2.0f * eici) * rds, (2.0f * eici) * rdp);
+}
+// Gulbrandsen's n + i k of a conductor from its reflectance r (clamped at 0.99) and edge tint g.
+__device__ __forceinline__ PbrCx pbr_gulbrandsen(float r, float g) {
+  const float c = fminf(fmaxf(r, 0.0f), 0.99f);
+  const float sq = sqrtf(c);
+  const float nmin = (1.0f - c) / (1.0f + c), nmax = (1.0f + sq) / (1.0f - sq);
+  const float n = nmax + (nmin - nmax) * g;
+  const float k2 = (psq(n + 1.0f) * c - psq(n - 1.0f)) / (1.0f - c);
+  return cx(n, sqrtf(fmaxf(k2, 0.0f)));
+}
+// |r12 + t12 t21 r23 e / (1 - r21 r23 e)|^2 with e = exp(i delta_phi).
+__device__ __forceinline__ float pbr_airy(float r12, float t12, float r21, float t21, PbrCx r23, PbrCx e) {
+  const PbrCx re = cx_mul(r23, e);
+  const PbrCx num = cx_scale(t12 * t21, re);
+  const PbrCx den = cx_sub(cx(1.0f, 0.0f), cx_scale(r21, re));
+  const PbrCx r = cx_add(cx(r12, 0.0f), cx_div(num, den, kPbrMinDenom, cx(0.0f, 0.0f)));
+  return r.x * r.x + r.y * r.y;
+}
+__device__ __forceinline__ float pbr_airy_sp(float2 r12, float2 t12, float2 r21, float2 t21, PbrCx r23s, PbrCx r23p, float dphi) {
+  float sn, cs;
+  sincosf(dphi, &sn, &cs);
+  const PbrCx e = cx(cs, sn);
+  return 0.5f * (pbr_airy(r12.x, t12.x, r21.x, t21.x, r23s, e) + pbr_airy(r12.y, t12.y, r21.y, t21.y, r23p, e));
+}
+// openpbr_thin_film_and_base_reflectance: the dielectric base's and the metal base's reflectance per
+// channel at cos ci from the exterior (no dispersion; the metal's F82 tint is white).
+static __device__ void pbr_thin_film(float ci, float eExt, float eFilm, float eBase, float3 f0, bool diel, bool metal, float nm,
+                              float3 lambda, float3 &rd, float3 &rm) {
+  rd = pf3(0.0f, 0.0f, 0.0f);
+  rm = pf3(0.0f, 0.0f, 0.0f);
+  if (!(diel || metal)) return;
+  float2 r12, t12;
+  float ct;
+  pbr_fresnel_amp(ci, eExt, eFilm, r12, t12, ct);
+  if (ct <= 0.0f) {
+    if (diel) rd = pf3(1.0f, 1.0f, 1.0f);
+    if (metal) rm = pf3(1.0f, 1.0f, 1.0f);
+    return;
+  }
+  const float2 r21 = make_float2(-r12.x, -r12.y);
+  const float scale = (eFilm * ct) / (eExt * fmaxf(ci, kPbrMinDenom));
+  const float2 t21 = make_float2(t12.x * scale, t12.y * scale);
+  const float opd = 2.0f * eFilm * nm * ct;
+  const float3 dphi = pf3(2.0f * kPbrPi * opd / lambda.x, 2.0f * kPbrPi * opd / lambda.y, 2.0f * kPbrPi * opd / lambda.z);
+  if (diel) {
+    PbrCx rs, rp;
+    pbr_fresnel_amp_cx(ct, eFilm, cx(eBase, 0.0f), rs, rp);
+    rd = pf3(pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.x), pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.y),
+             pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.z));
+  }
+  if (metal) {
+    const float f[3] = {f0.x, f0.y, f0.z}, d[3] = {dphi.x, dphi.y, dphi.z};
+    float out[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      PbrCx rs, rp;
+      pbr_fresnel_amp_cx(ct, eFilm, pbr_gulbrandsen(f[c], 1.0f), rs, rp);
+      out[c] = pbr_airy_sp(r12, t12, r21, t21, rs, rp, d[c]);
+    }
+    rm = pf3(out[0], out[1], out[2]);
+  }
+}
+// openpbr_thin_film_presence_multiplier: smoothstep from 1e-9 to 30 nm.
+__device__ __forceinline__ float pbr_thin_film_presence(float weight, float nm) {
+  const float t = psat((nm - kPbrMinDenom) / (30.0f - kPbrMinDenom));
+  return weight * (t * t * (3.0f - 2.0f * t));
+}
+
 // ---- the prepared BSDF -----------------------------------------------------------------------
 struct PbrPrepared {
   PbrBasis B;          // face-forwarded shading frame (normal_ff = B.n)
@@ -227,7 +364,29 @@ struct PbrPrepared {
   float3 diffAlbedo;
   float diffRough, diffComp;
   float wSpec, wMetal, wDiff, total;
+  // Thin film: presence (weight x thickness ramp), thickness (nm), the IORs outside, of and under the
+  // film, the wavelengths.
+  float tfPresence, tfNm, tfExt, tfIor, tfInt;
+  float3 lambda;
 };
+
+// Reflection coefficient of the specular lobe at cos c to the half vector (openpbr_reflection_coefficient):
+// the opaque dielectric's Fresnel and the metal's F82 Schlick, blended with the thin film's reflectances
+// by its presence (computed only where it is partial or whole).
+__device__ __forceinline__ float3 pbr_spec_coeff(const PbrPrepared &p, float c) {
+  float3 standard = pf3(0.0f, 0.0f, 0.0f);
+  if (p.tfPresence < 1.0f) {
+    const float F = pbr_fresnel(p.etaOpaque, c);
+    const float3 fm = pbr_metal_fresnel(p.f0, c);
+    standard = padd(pf3(p.scaleOpaque * F, p.scaleOpaque * F, p.scaleOpaque * F), pscale(fm, p.metalAmount));
+  }
+  if (!(p.tfPresence > 0.0f) || c < 0.0f) return standard;
+  float3 rd, rm;
+  pbr_thin_film(c, p.tfExt, p.tfIor, p.tfInt, p.f0, p.scaleOpaque > 0.0f, p.metalAmount > 0.0f, p.tfNm, p.lambda, rd, rm);
+  const float3 film = padd(pscale(rd, p.scaleOpaque), pscale(rm, p.metalAmount));
+  const float t = p.tfPresence;
+  return pf3(standard.x * (1.0f - t) + film.x * t, standard.y * (1.0f - t) + film.y * t, standard.z * (1.0f - t) + film.z * t);
+}
 
 // openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit).
 __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const PbrTables &T, float3 n, float3 wo) {
@@ -254,30 +413,28 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
   p.metalEc = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pbr_metal_energy(T, p.alpha, idotn);
   p.diffAlbedo = pscale(p.f0, p.scaleOpaque);
   p.diffRough = P.diffRough;
+  // Thin film (openpbr_bsdf.h:678-690 with no coat): from outside the film lies between the ambient
+  // medium (1) and the weighted specular IOR; from inside the two swap.
+  p.tfNm = P.tfThickness * 1000.0f;
+  p.tfPresence = pbr_thin_film_presence(P.tfWeight, p.tfNm);
+  p.tfExt = back ? wior : 1.0f;
+  p.tfInt = back ? 1.0f : wior;
+  p.tfIor = P.tfIor;
+  p.lambda = P.lambda;
   {
     const float num = pbr_opaque_energy(T, p.etaOpaque, p.alpha, idotn);
     const float den = pbr_opaque_average(T, p.etaOpaque, p.alpha);
     p.diffComp = num / fmaxf(den, 1e-12f);
   }
   // Lobe weights (estimated contributions with a white throughput).
-  {
-    const float F = pbr_fresnel(p.etaOpaque, idotn);
-    const float3 fm = pbr_metal_fresnel(p.f0, idotn);
-    const float3 refl = padd(pf3(p.scaleOpaque * F, p.scaleOpaque * F, p.scaleOpaque * F), pscale(fm, p.metalAmount));
-    p.wSpec = pmax3(refl);
-  }
+  p.wSpec = pmax3(pbr_spec_coeff(p, idotn));
   p.wMetal = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pmax3(p.metalScale) * p.metalEc;
   p.wDiff = pmax3(pscale(p.diffAlbedo, p.diffComp));
   p.total = ((((p.wSpec + 0.0f) + p.wMetal) + p.wDiff) + 0.0f) + 0.0f;
   return p;
 }
 
-// Reflection coefficient of the specular lobe at |cos| to the half vector.
-__device__ __forceinline__ float3 pbr_spec_coeff(const PbrPrepared &p, float c) {
-  const float F = pbr_fresnel(p.etaOpaque, c);
-  const float3 fm = pbr_metal_fresnel(p.f0, c);
-  return padd(pf3(p.scaleOpaque * F, p.scaleOpaque * F, p.scaleOpaque * F), pscale(fm, p.metalAmount));
-}
+
 
 __device__ __forceinline__ float3 pbr_spec_value(const PbrPrepared &p, float3 wi) {
   const float idotn = pdot(p.B.n, p.wo), odotn = pdot(p.B.n, wi);

@@ -891,8 +891,13 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
 // prepare_bsdf (main.swift:2547-2568): RGB transport evaluates the base colour's three channels; in
 // spectral transport `a` takes the reflectance at lanes 0-2 and `b` lane 3, skipped for a flat
 // (grey) base where lane 3 equals lane 0. Sampling, lobe choice and pdfs are those of `a`.
-__device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_material &m, float3 base) {
-  const float4 q = __ldg(A.pbr + __float_as_uint(m.pad));
+// Per slot two float4: (roughness, metalness, IOR, diffuse roughness) and the thin film (weight,
+// thickness in micrometres, IOR, 0). The thin film is a spectral-transport input
+// (prepare_openpbr_lanes, main.swift:2527-2568; the RGB adapter leaves it at zero), evaluated at the
+// preparation's wavelengths `lambda`.
+__device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_material &m, float3 base, float3 lambda) {
+  const uint32_t slot = __float_as_uint(m.pad);
+  const float4 q = __ldg(A.pbr + 2u * slot);
   PbrParams P;
   P.base = make_float3(psat(base.x), psat(base.y), psat(base.z));
   P.rough = fmaxf(0.03f, q.x);
@@ -900,7 +905,24 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
   P.ior = fmaxf(1.01f, q.z);
   P.sw = 1.0f;
   P.diffRough = q.w;
+  const float4 tf = A.spectral ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+  P.tfWeight = tf.x;
+  P.tfThickness = tf.y;
+  P.tfIor = tf.z;
+  P.lambda = lambda;
   return P;
+}
+// The thin film's weight at slot m (spectral transport only).
+__device__ __forceinline__ bool pbr_thin_film_slot(const RenderArgs &A, const vt_material &m) {
+  return A.spectral && __ldg(A.pbr + 2u * __float_as_uint(m.pad) + 1u).x > 0.0f;
+}
+// Lane k's wavelength lambda_k = F^-1((u + k) / 4) (spectral_lambda, main.swift:795-801).
+__device__ __forceinline__ float lane_lambda(const RenderArgs &A, const Lanes &L, int k) {
+  const float seg = float(A.segments);
+  const float x = (L.u + float(k)) * 0.25f * seg;
+  const uint32_t i = min((uint32_t)x, A.segments - 1u);
+  const float low = __ldg(A.icdf + i), width = __ldg(A.icdf + i + 1) - low;
+  return low + (x - float(i)) * width;
 }
 // kPbr: the kernel variant for scenes with OPENPBR slots; scenes without them run a variant
 // compiled without the OpenPBR code, which keeps its register count (and occupancy) down.
@@ -916,13 +938,19 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   const float cosine = fabsf(dot3(n, wi));
   if (cosine < 1e-7f || dot3(n, wo) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float4 rho = reflectance(A, L, m);
-  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z)), A.pbrT, n, wo);
+  // prepare_bsdf (main.swift:2573-2593): the lanes' wavelengths only with a thin film (else the
+  // upstream RGB ones), and `b` whenever lane 3 can differ from lane 0.
+  const bool film = pbr_thin_film_slot(A, m);
+  const float3 lam = film ? make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2))
+                          : make_float3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo);
   pdf = pbr_pdf(a, wi);
   if (dot3(wi, gn) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float3 fa = pbr_eval(a, A.pbrT, wi);
   float f3w = fa.x;
-  if (A.spectral && rho.w != rho.x) {
-    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w)), A.pbrT, n, wo);
+  if (A.spectral && (rho.w != rho.x || film)) {
+    const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo);
     f3w = pbr_eval(b, A.pbrT, wi).x;
   }
   return make_float4(fa.x / cosine, fa.y / cosine, fa.z / cosine, A.spectral ? f3w / cosine : 0.0f);
@@ -931,13 +959,17 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
 __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 wo,
                                  float3 r, float3 &dir, float4 &weight, float &pdf) {
   const float4 rho = reflectance(A, L, m);
-  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z)), A.pbrT, n, wo);
+  const bool film = pbr_thin_film_slot(A, m);
+  const float3 lam = film ? make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2))
+                          : make_float3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo);
   float3 w;
   if (!pbr_sample(a, A.pbrT, r, dir, w, pdf) || !(pdf > 0.0f)) return false;
   if (dot3(dir, gn) <= 0.0f) return false;
   float w3 = w.x;
-  if (A.spectral && rho.w != rho.x) {
-    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w)), A.pbrT, n, wo);
+  if (A.spectral && (rho.w != rho.x || film)) {
+    const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo);
     w3 = pbr_eval(b, A.pbrT, dir).x / pdf;
   }
   weight = make_float4(w.x, w.y, w.z, A.spectral ? w3 : 0.0f);
@@ -3647,17 +3679,22 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
   if (n != scene->nmat) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the scene's material slot count");
   if (!ctx->pbr_opaque) return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables are not set (vt_openpbr_tables_set)");
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
-  std::vector<float4> q(n);
+  std::vector<float4> q(2 * (size_t)n);
   for (uint32_t i = 0; i < n; ++i) {
     const vt_openpbr_params &p = params[i];
     if (!(p.roughness >= 0.0f && p.roughness <= 1.0f) || !(p.metalness >= 0.0f && p.metalness <= 1.0f) || !(p.ior > 0.0f) ||
         !(p.diffuse_roughness >= 0.0f && p.diffuse_roughness <= 1.0f))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": roughness, metalness and diffuse roughness "
                                           "must lie in [0, 1] and the IOR be positive");
-    q[i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
+    if (!(p.thin_film_weight >= 0.0f && p.thin_film_weight <= 1.0f) || !(p.thin_film_thickness >= 0.0f) ||
+        !std::isfinite(p.thin_film_thickness) || (p.thin_film_weight > 0.0f && !(p.thin_film_ior > 0.0f)))
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": thin-film weight must lie in [0, 1], its "
+                                          "thickness be finite and non-negative and its IOR positive");
+    q[2 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
+    q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f, 0.0f);
   }
-  if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, n * sizeof(float4)));
-  if (n) VT_CUDA(ctx, cudaMemcpy(scene->d_pbr, q.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+  if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, q.size() * sizeof(float4)));
+  if (n) VT_CUDA(ctx, cudaMemcpy(scene->d_pbr, q.data(), q.size() * sizeof(float4), cudaMemcpyHostToDevice));
   scene->pbr_tables = ctx->d_pbr;
   return VT_OK;
 }

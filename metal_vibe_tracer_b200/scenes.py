@@ -561,8 +561,9 @@ def production_scene(seed: int = 0, triangles: int = 10_000_000, emitters: int =
     """The production-scale grid scene: ~`triangles` triangles of displaced subdivision-5 icospheres
     (20,480 triangles each), ~`emitters` emissive triangles (whole emissive spheres), `nmat` OPENPBR
     slots (base colour uniform in [0, 1]^3, roughness uniform in [0, 1], metalness 1 with
-    probability 0.3 else 0, IOR uniform in [1.3, 1.8]; thin film is not supported and left out) and a
-    camera over the grid. Returns faces, vertices, materials, camera."""
+    probability 0.3 else 0, IOR uniform in [1.3, 1.8]; with probability 0.1 a thin film of weight 1,
+    thickness uniform in [200, 800] nm and IOR 1.4) and a camera over the grid. Returns faces,
+    vertices, materials, camera."""
     spheres = max(1, round(triangles / 20480))
     every = max(1, round(spheres / max(1, round(emitters / 20480))))
     faces, verts, mats, camera = sphere_grid(triangles, seed=seed, emissive_every=every, nmat=nmat, coloured=True)
@@ -570,7 +571,17 @@ def production_scene(seed: int = 0, triangles: int = 10_000_000, emitters: int =
     for i in range(nmat):
         mats[i] = dict(mats[i], type=4, roughness=float(rng.random()), metalness=1.0 if rng.random() < 0.3 else 0.0,
                        ior=float(1.3 + 0.5 * rng.random()))
+    _thin_films(mats[:nmat], seed)
     return faces, verts, mats, camera
+
+
+def _thin_films(mats, seed: int, fraction: float = 0.1):
+    """Gives `fraction` of the OPENPBR slots (seeded, own stream) a thin film: weight 1, thickness
+    uniform in [0.2, 0.8] micrometres, IOR 1.4 (OpenPBR's default film IOR)."""
+    rng = np.random.default_rng(seed + 2)
+    for i in range(len(mats)):
+        if rng.random() < fraction:
+            mats[i].update(thin_film_weight=1.0, thin_film_thickness=float(0.2 + 0.6 * rng.random()), thin_film_ior=1.4)
 
 
 def displaced_sphere_asset(subdivisions: int, seed: int, displace: float = 0.05):
@@ -631,6 +642,7 @@ def instanced_grid(grid: int = 32, assets: int = 16, subdivisions: int = 5, seed
     mats = [{"type": 4, "albedo": tuple(float(x) for x in rng.random(3)), "emission": (0.0, 0.0, 0.0),
              "roughness": float(rng.random()), "metalness": 1.0 if rng.random() < 0.3 else 0.0,
              "ior": float(1.3 + 0.5 * rng.random())} for _ in range(nmat)]
+    _thin_films(mats, seed)
     mats += [{"type": 3, "albedo": (0.0, 0.0, 0.0), "emission": (float(e),) * 3} for e in (4.0, 8.0, 12.0)]
     d = max(2.0, 0.9 * grid)
     camera = {"pos": (0.0, 0.8 * d, -1.2 * d), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 45.0}

@@ -38,25 +38,30 @@ def load():
     return _lib
 
 
-def material(base, metalness, roughness, ior, type_=4):
+def material(base, metalness, roughness, ior, type_=4, thin_film=None):
+    """A reference material; `thin_film` = (weight, thickness in micrometres, IOR) or None."""
     m = Material()
     m.type = type_
     m.albedo[:] = [float(x) for x in base]
     m.roughness, m.metalness, m.ior = float(roughness), float(metalness), float(ior)
+    if thin_film is not None:
+        m.thin_film_weight, m.thin_film_thickness, m.thin_film_ior = (float(x) for x in thin_film)
     return m
 
 
-def evaluate(m, n, wo, wi):
-    """(f |cos| (3), pdf) of the reference BSDF."""
+def evaluate(m, n, wo, wi, lambda_nm=None):
+    """(f |cos| (3), pdf) of the reference BSDF (at three wavelengths in nm; None: its RGB ones)."""
     f, pdf = F3(), C.c_float()
-    load().ref_openpbr_eval(C.byref(m), F3(*n), F3(*wo), F3(*wi), None, f, C.byref(pdf))
+    lam = F3(*lambda_nm) if lambda_nm is not None else None
+    load().ref_openpbr_eval(C.byref(m), F3(*n), F3(*wo), F3(*wi), lam, f, C.byref(pdf))
     return np.array(f, np.float32), np.float32(pdf.value)
 
 
-def sample(m, n, wo, rand):
+def sample(m, n, wo, rand, lambda_nm=None):
     """(direction, weight f |cos| / pdf, pdf, lobe type bits) of one reference sample."""
     d, w, pdf, lobe = F3(), F3(), C.c_float(), C.c_int32()
-    load().ref_openpbr_sample(C.byref(m), F3(*n), F3(*wo), F3(*rand), None, d, w, C.byref(pdf), C.byref(lobe))
+    lam = F3(*lambda_nm) if lambda_nm is not None else None
+    load().ref_openpbr_sample(C.byref(m), F3(*n), F3(*wo), F3(*rand), lam, d, w, C.byref(pdf), C.byref(lobe))
     return np.array(d, np.float32), np.array(w, np.float32), np.float32(pdf.value), int(lobe.value)
 
 

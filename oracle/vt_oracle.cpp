@@ -1691,7 +1691,7 @@ inline double max_abs_d(D3 p) { return std::max(std::fabs(p.x), std::max(std::fa
 inline double ray_eps_d(const PtContext &C, D3 p) { return C.imported ? std::max(1e-7, 9.536743e-7 * max_abs_d(p)) : kEpsPt; }
 inline double ray_tmin_d(const PtContext &C, D3 o) { return C.imported ? ray_eps_d(C, o) * 0.25 : kEpsPt; }
 
-struct PtLanes { int bin[4]; double w[4]; };
+struct PtLanes { int bin[4]; double w[4]; double lambda[4]; };
 
 PtLanes make_lanes(const PtContext &C, double u) {
   PtLanes L;
@@ -1702,6 +1702,7 @@ PtLanes make_lanes(const PtContext &C, double u) {
     const double low = C.in->icdf[i], width = double(C.in->icdf[i + 1]) - low;
     L.w[k] = 0.25 * seg * width;
     const double lambda = low + (x - i) * width;
+    L.lambda[k] = lambda;
     const double b = std::min(std::max(lambda - C.in->lambda_min + 0.5, 0.0), double(C.in->nbins - 1u));
     L.bin[k] = (int)std::min((uint32_t)b, C.in->nbins - 1u);
   }
@@ -2269,11 +2270,24 @@ vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double
   q.albedo[0] = (float)b0;
   q.albedo[1] = (float)b1;
   q.albedo[2] = (float)b2;
-  const float *pp = C.in->pbr_params + 4 * (size_t)slot;
+  const float *pp = C.in->pbr_params + 8 * (size_t)slot;
   q.roughness = pp[0];
   q.metalness = pp[1];
   q.ior = pp[2];
+  // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568).
+  if (C.spectral) {
+    q.thin_film_weight = pp[4];
+    q.thin_film_thickness = pp[5];
+    q.thin_film_ior = pp[6];
+  }
   return q;
+}
+// prepare_bsdf (main.swift:2573-2593): with a thin film the lanes' wavelengths (a: lanes 0-2, b: lane
+// 3), else the library's default RGB wavelengths (null).
+bool pbr_film_d(const PtContext &C, const vt_material &m) {
+  uint32_t slot;
+  std::memcpy(&slot, &m.pad, sizeof slot);
+  return C.spectral && C.in->pbr_params[8 * (size_t)slot + 4] > 0.0f;
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706): f (no cosine) per lane, pdf of lanes 0-2.
 Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, D3 wi, double &pdf) {
@@ -2284,15 +2298,18 @@ Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &
   const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
               fi[3] = {(float)wi.x, (float)wi.y, (float)wi.z};
   const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  const bool film = pbr_film_d(C, m);
+  const float la[3] = {(float)L.lambda[0], (float)L.lambda[1], (float)L.lambda[2]};
+  const float lb[3] = {(float)L.lambda[3], (float)L.lambda[3], (float)L.lambda[3]};
   float f[3], q;
-  C.in->pbr_eval(&a, fn, fo, fi, nullptr, f, &q);
+  C.in->pbr_eval(&a, fn, fo, fi, film ? la : nullptr, f, &q);
   pdf = q;
   if (dot(wi, gn) <= 0.0) return {{0, 0, 0, 0}};
   double f3 = f[0];
-  if (C.spectral && rho.v[3] != rho.v[0]) {
+  if (C.spectral && (rho.v[3] != rho.v[0] || film)) {
     const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
     float g[3], qb;
-    C.in->pbr_eval(&b, fn, fo, fi, nullptr, g, &qb);
+    C.in->pbr_eval(&b, fn, fo, fi, film ? lb : nullptr, g, &qb);
     f3 = g[0];
   }
   return {{f[0] / cosine, f[1] / cosine, f[2] / cosine, C.spectral ? f3 / cosine : 0.0}};
@@ -2304,18 +2321,21 @@ bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material 
   const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
               fr[3] = {(float)r[0], (float)r[1], (float)r[2]};
   const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  const bool film = pbr_film_d(C, m);
+  const float la[3] = {(float)L.lambda[0], (float)L.lambda[1], (float)L.lambda[2]};
+  const float lb[3] = {(float)L.lambda[3], (float)L.lambda[3], (float)L.lambda[3]};
   float d[3], ww[3], q;
   int32_t lobe;
-  C.in->pbr_sample(&a, fn, fo, fr, nullptr, d, ww, &q, &lobe);
+  C.in->pbr_sample(&a, fn, fo, fr, film ? la : nullptr, d, ww, &q, &lobe);
   if (!(q > 0.0f)) return false;
   dir = D3{d[0], d[1], d[2]};
   if (dot(dir, gn) <= 0.0) return false;
   pdf = q;
   double w3 = ww[0];
-  if (C.spectral && rho.v[3] != rho.v[0]) {
+  if (C.spectral && (rho.v[3] != rho.v[0] || film)) {
     const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
     float g[3], qb;
-    C.in->pbr_eval(&b, fn, fo, d, nullptr, g, &qb);
+    C.in->pbr_eval(&b, fn, fo, d, film ? lb : nullptr, g, &qb);
     w3 = g[0] / q;
   }
   w = {{ww[0], ww[1], ww[2], C.spectral ? w3 : 0.0}};

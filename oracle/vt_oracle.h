@@ -124,7 +124,8 @@ typedef struct vto_pt_inputs {
    * the warped phase at each of the nbins bins. Needed when spectral. */
   const struct vto_uplift *uplift;
   const float *cos_phase;
-  /* OPENPBR slots (type 4): per slot roughness, metalness, IOR, diffuse roughness, and the BSDF. */
+  /* OPENPBR slots (type 4): per slot 8 floats (roughness, metalness, IOR, diffuse roughness, thin-film
+   * weight, thickness in micrometres and IOR, 0), and the BSDF. */
   const float *pbr_params;
   vto_pbr_eval_fn pbr_eval;
   vto_pbr_sample_fn pbr_sample;

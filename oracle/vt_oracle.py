@@ -311,7 +311,9 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         from . import openpbr_ref
         ref = openpbr_ref.load()
         params = np.array([[float(m.get("roughness", 0.5)), float(m.get("metalness", 0.0)), float(m.get("ior", 1.5)),
-                            float(m.get("diffuse_roughness", 0.0))] for m in materials], np.float32)
+                            float(m.get("diffuse_roughness", 0.0)), float(m.get("thin_film_weight", 0.0)),
+                            float(m.get("thin_film_thickness", 0.0)), float(m.get("thin_film_ior", 1.4)), 0.0]
+                           for m in materials], np.float32)
         keep.append(params)
         inp.pbr_params = params.ctypes.data
         inp.pbr_eval = C.cast(ref.ref_openpbr_eval, C.c_void_p).value

@@ -4,9 +4,9 @@ vendored headers compiled for the CPU) and the FP64 oracle path tracer.
 * the dense GGX energy table, solved on the device, equals Shaders/MetalEnergy.metal's values to
   float summation error;
 * the device BSDF (openpbr.cuh) gives the reference's f |cos|, pdf and samples for 600 seeded
-  opaque materials and directions;
+  opaque materials and directions, and for 300 with thin-film iridescence at given wavelengths;
 * a Cornell box with OPENPBR walls and boxes renders as the oracle does, in RGB and spectral
-  transport.
+  transport, and with thin films on two slots in spectral transport.
 """
 import json
 from pathlib import Path
@@ -32,11 +32,13 @@ def test_energy_table_matches_the_reference(ctx):
     assert t[0].max() == 0.0 and (t >= 0).all() and (t <= 1).all()
 
 
-def test_bsdf_matches_the_reference(ctx):
+@pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json"])
+def test_bsdf_matches_the_reference(ctx, fixture):
     R.openpbr_tables_set(ctx)
-    cases = json.loads((GOLDEN / "openpbr_cases.json").read_text())["cases"]
+    cases = json.loads((GOLDEN / fixture).read_text())["cases"]
+    film = lambda c: c["thin_film"] + c["lambda"] if "thin_film" in c else []
     arr = np.array([c["base"] + [c["metalness"], c["roughness"], c["ior"], 1.0, 0.0] + c["normal"] + c["view"] + c["light"]
-                    + c["rand"] for c in cases], np.float32)
+                    + c["rand"] + film(c) for c in cases], np.float32)
     out = R.openpbr_evaluate(ctx, arr)
     fc = np.float32([c["f_cos"] for c in cases])
     pdf = np.float32([c["pdf"] for c in cases])
@@ -71,6 +73,33 @@ def test_openpbr_cornell_matches_oracle(ctx, oracle, spectral):
     gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
     assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
     assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+
+
+def test_thin_film_cornell_matches_oracle(ctx, oracle):
+    """Spectral transport with thin films on the three dielectric walls (0.45 um, IOR 2.2) and the
+    metal box (0.3 um, IOR 1.6, weight 0.8): the film's reflectance follows each path's wavelengths."""
+    faces, verts, mats, light, cam = scenes.cornell_openpbr()
+    for k in (2, 3, 4):
+        mats[k] = dict(mats[k], thin_film_weight=1.0, thin_film_thickness=0.45, thin_film_ior=2.2)
+    mats[5] = dict(mats[5], thin_film_weight=0.8, thin_film_thickness=0.3, thin_film_ior=1.6)
+    tables = spectral_tables.load()
+    mesh = vt.Mesh(ctx, faces, verts)
+    out = []
+    for m in (mats, [dict(x, thin_film_weight=0.0) for x in mats]):
+        scene = vt.Scene(ctx, mesh, m, light, tables)
+        scene.render(vt.make_params(cam, 96, 96, 6, 1, True), 32)
+        out.append(scene.readback()[0])
+        scene.close()
+    mesh.close()
+    gpu, bare = out
+    ref = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, spectral=tables)
+    other = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, first_sample=1001, spectral=tables)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    # The films change the picture's mean well beyond the noise (by 6-22 % per channel).
+    bm = bare.reshape(-1, 3).mean(0)
+    assert np.abs(bm / rm - 1).max() > 0.03, (bm, rm)
 
 
 def test_openpbr_restir_runs(ctx):

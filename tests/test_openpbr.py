@@ -31,6 +31,34 @@ def test_reference_bsdf_reproduces_the_fixtures():
 
 
 @needs_ref
+def test_reference_thin_film_reproduces_the_fixtures():
+    """The thin-film fixtures (tests/golden/openpbr_thin_film_cases.json): iridescence at the case's
+    three wavelengths (openpbr_thin_film_and_base_reflectance)."""
+    cases = json.loads((GOLDEN / "openpbr_thin_film_cases.json").read_text())["cases"]
+    for c in cases[:150]:
+        m = R.material(c["base"], c["metalness"], c["roughness"], c["ior"], thin_film=c["thin_film"])
+        f, pdf = R.evaluate(m, c["normal"], c["view"], c["light"], c["lambda"])
+        assert np.array_equal(f, np.float32(c["f_cos"])) and pdf == np.float32(c["pdf"])
+        d, w, spdf, lobe = R.sample(m, c["normal"], c["view"], c["rand"], c["lambda"])
+        assert np.array_equal(d, np.float32(c["dir"])) and spdf == np.float32(c["sample_pdf"]) and lobe == c["lobe"]
+
+
+@needs_ref
+def test_reference_thin_film_changes_the_answer():
+    """A film of weight 1 changes f |cos| on most cases; weight 0 gives the film-free answer."""
+    cases = json.loads((GOLDEN / "openpbr_thin_film_cases.json").read_text())["cases"]
+    changed = 0
+    for c in cases[:60]:
+        bare = R.material(c["base"], c["metalness"], c["roughness"], c["ior"])
+        off = R.material(c["base"], c["metalness"], c["roughness"], c["ior"], thin_film=(0.0,) + tuple(c["thin_film"][1:]))
+        f0, _ = R.evaluate(bare, c["normal"], c["view"], c["light"], c["lambda"])
+        f1, _ = R.evaluate(off, c["normal"], c["view"], c["light"], c["lambda"])
+        assert np.array_equal(f0, f1)
+        changed += not np.allclose(f0, np.float32(c["f_cos"]), rtol=1e-2, atol=1e-6)
+    assert changed > 20, changed
+
+
+@needs_ref
 def test_reference_metal_table_is_the_fixture():
     g = json.loads((GOLDEN / "metal_energy.json").read_text())
     t, a = R.metal_energy_table()
