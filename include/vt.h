@@ -224,13 +224,17 @@ vt_status vt_tlas_flatten(vt_ctx *ctx, const vt_tlas *tlas, const vt_build_optio
 
 typedef struct vt_scene vt_scene;
 
-/* Material types: the reference's MaterialType values (main.swift:316-322). */
-enum { VT_MAT_DIFFUSE = 0, VT_MAT_EMISSIVE = 3, VT_MAT_OPENPBR = 4 };
+/* Material types: the reference's MaterialType values (main.swift:316-322). GLOSSY is a metal: an
+ * ideal mirror below roughness 0.02 (Schlick's conductor Fresnel with F0 = albedo), else the OpenPBR
+ * BSDF with metalness 1. DIELECTRIC is ideal glass (Schlick's Fresnel at the slot's IOR, albedo as
+ * the tint). Their roughness and IOR come from the slot's vt_openpbr_params; without them a GLOSSY
+ * slot is a mirror and a DIELECTRIC slot has IOR 1.5. */
+enum { VT_MAT_DIFFUSE = 0, VT_MAT_GLOSSY = 1, VT_MAT_DIELECTRIC = 2, VT_MAT_EMISSIVE = 3, VT_MAT_OPENPBR = 4 };
 
 /* A constant material slot (the role of SurfaceSettings / MaterialResources, main.swift:2253-2263,
  * 628-654, for constant Lambert and emissive surfaces). A face's tag selects its slot. 32 bytes. */
 typedef struct vt_material {
-  int32_t type;        /* VT_MAT_DIFFUSE, VT_MAT_EMISSIVE or VT_MAT_OPENPBR (base colour = albedo) */
+  int32_t type;        /* VT_MAT_*; albedo is the base colour (OPENPBR), F0 (GLOSSY) or the tint (DIELECTRIC) */
   float albedo[3];     /* linear sRGB reflectance (Lambert) */
   float emission[3];   /* linear sRGB radiance (emissive) */
   float pad;
@@ -356,8 +360,9 @@ vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t height, uint32_
  * false, 0.2, 1), (true, true, true, 0, 1), (false, false, false, 0.2, 1); [4] the second PCG draw
  * from seed 890625759; [5] the cosine of the grazing cosine-hemisphere sample drawn from that seed
  * against its normal; [6..7] min and max of 100,000 rand_f draws from seed 17; [8..10]
- * scattering_limit of depths 0, 1, 8. */
-#define VT_KNOWN_ANSWERS 11u
+ * scattering_limit of depths 0, 1, 8; [11..15] the glass total-internal-reflection sample
+ * (GPUChecks.swift:32-34): 1 when it exists, its direction's z, its weight rgb. */
+#define VT_KNOWN_ANSWERS 16u
 vt_status vt_known_answers(vt_ctx *ctx, float *out, uint32_t n);
 
 /* ---- batched scenes ---------------------------------------------------------------------- */
@@ -463,9 +468,10 @@ typedef struct vt_openpbr_result {
 /* openpbr_prepare + openpbr_eval / openpbr_pdf / openpbr_sample for n queries on the device. */
 vt_status vt_openpbr_evaluate(vt_ctx *ctx, const vt_openpbr_case *cases, uint32_t n, vt_openpbr_result *out);
 
-/* A scene's OPENPBR slot parameters (SurfaceSettings surface/detail, main.swift:2253-2263, as
- * resolve_material sets them; base colour is the slot's albedo): one per material slot, read for the
- * slots whose type is VT_MAT_OPENPBR. Needs vt_openpbr_tables_set on the context first. */
+/* A scene's per-slot lobe parameters (SurfaceSettings surface/detail, main.swift:2253-2263, as
+ * resolve_material sets them; base colour is the slot's albedo): one per material slot, read for
+ * OPENPBR slots, for GLOSSY slots (roughness, IOR, thin film) and for DIELECTRIC slots (IOR). Needs
+ * vt_openpbr_tables_set on the context first. */
 typedef struct vt_openpbr_params {
   float roughness, metalness, ior, diffuse_roughness;
   /* Thin-film iridescence (SpectralMaterial, main.swift:730-735; spectral transport only, as the

@@ -203,7 +203,7 @@ SIGNATURES = {
     "vt_render_nrc": (_I32, [_P, _P, _P, _P, _U32, _U32, _P]),
 }
 NOALLOC_MAX_FACES = 32768
-KNOWN_ANSWERS = 11
+KNOWN_ANSWERS = 16
 
 _lib: C.CDLL | None = None
 

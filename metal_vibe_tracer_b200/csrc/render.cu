@@ -58,8 +58,9 @@ struct RenderArgs {
   const float4 *slotL;     // per slot: the albedo's uplift multipliers (L0, L1, L2, flag)
   const float *cosPhase;   // per bin: cos of the warped phase
   const float4 *ebasis;    // per bin: the emission basis (R, G, B, 0), (C, M, Y, 0)
-  const float4 *pbr;       // per slot: OPENPBR roughness, metalness, IOR, diffuse roughness
+  const float4 *pbr;       // per slot: roughness, metalness, IOR, diffuse roughness; thin film
   PbrTables pbrT;          // OpenPBR energy tables
+  uint32_t layered;        // some slot is OPENPBR, GLOSSY or DIELECTRIC (the kPbr kernel variants)
   uint32_t nbins, segments;
   float lambdaMin;
   int spectral;
@@ -887,25 +888,35 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
   return A.spectral ? fmaxf(fmaxf(a.x, a.y), fmaxf(a.z, a.w)) : fmaxf(fmaxf(a.x, a.y), a.z);
 }
 
-// ---- OpenPBR vertices (openpbr.cuh) --------------------------------------------------------------
+// ---- per-slot lobe parameters, OpenPBR vertices (openpbr.cuh) and delta vertices ----------------
+// Per slot two float4 (vt_scene_set_openpbr): (roughness, metalness, IOR, diffuse roughness) and the
+// thin film (weight, thickness in micrometres, IOR, 0). Without a table (or for a slot past it) a
+// slot is ideal: roughness 0, IOR 1.5, no film.
+__device__ __forceinline__ float4 slot_lobe(const RenderArgs &A, const vt_material &m) {
+  const uint32_t slot = __float_as_uint(m.pad);
+  return A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot) : make_float4(0.0f, 0.0f, 1.5f, 0.0f);
+}
+// The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568, and
+// spectral_thin_film_mirror; the RGB adapter leaves it at zero).
+__device__ __forceinline__ float4 slot_film(const RenderArgs &A, const vt_material &m) {
+  const uint32_t slot = __float_as_uint(m.pad);
+  return A.spectral && A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+}
 // prepare_bsdf (main.swift:2547-2568): RGB transport evaluates the base colour's three channels; in
 // spectral transport `a` takes the reflectance at lanes 0-2 and `b` lane 3, skipped for a flat
-// (grey) base where lane 3 equals lane 0. Sampling, lobe choice and pdfs are those of `a`.
-// Per slot two float4: (roughness, metalness, IOR, diffuse roughness) and the thin film (weight,
-// thickness in micrometres, IOR, 0). The thin film is a spectral-transport input
-// (prepare_openpbr_lanes, main.swift:2527-2568; the RGB adapter leaves it at zero), evaluated at the
+// (grey) base where lane 3 equals lane 0. Sampling, lobe choice and pdfs are those of `a`. A GLOSSY
+// slot is the BSDF with metalness 1 (prepare_openpbr, main.swift:2489). The film is evaluated at the
 // preparation's wavelengths `lambda`.
 __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_material &m, float3 base, float3 lambda) {
-  const uint32_t slot = __float_as_uint(m.pad);
-  const float4 q = __ldg(A.pbr + 2u * slot);
+  const float4 q = slot_lobe(A, m);
   PbrParams P;
   P.base = make_float3(psat(base.x), psat(base.y), psat(base.z));
   P.rough = fmaxf(0.03f, q.x);
-  P.metal = q.y;
+  P.metal = m.type == VT_MAT_GLOSSY ? 1.0f : q.y;
   P.ior = fmaxf(1.01f, q.z);
   P.sw = 1.0f;
   P.diffRough = q.w;
-  const float4 tf = A.spectral ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+  const float4 tf = slot_film(A, m);
   P.tfWeight = tf.x;
   P.tfThickness = tf.y;
   P.tfIor = tf.z;
@@ -914,7 +925,7 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
 }
 // The thin film's weight at slot m (spectral transport only).
 __device__ __forceinline__ bool pbr_thin_film_slot(const RenderArgs &A, const vt_material &m) {
-  return A.spectral && __ldg(A.pbr + 2u * __float_as_uint(m.pad) + 1u).x > 0.0f;
+  return slot_film(A, m).x > 0.0f;
 }
 // Lane k's wavelength lambda_k = F^-1((u + k) / 4) (spectral_lambda, main.swift:795-801).
 __device__ __forceinline__ float lane_lambda(const RenderArgs &A, const Lanes &L, int k) {
@@ -924,11 +935,19 @@ __device__ __forceinline__ float lane_lambda(const RenderArgs &A, const Lanes &L
   const float low = __ldg(A.icdf + i), width = __ldg(A.icdf + i + 1) - low;
   return low + (x - float(i)) * width;
 }
-// kPbr: the kernel variant for scenes with OPENPBR slots; scenes without them run a variant
-// compiled without the OpenPBR code, which keeps its register count (and occupancy) down.
+// kPbr: the kernel variant for scenes with OPENPBR, GLOSSY or DIELECTRIC slots; scenes of Lambert and
+// emissive slots run a variant compiled without that code, which keeps its register count (and
+// occupancy) down.
+// is_delta (main.swift:3285-3287): glass, and GLOSSY mirrors smoother than 0.02.
+template <bool kPbr>
+__device__ __forceinline__ bool is_delta(const RenderArgs &A, const vt_material &m) {
+  return kPbr && (m.type == VT_MAT_DIELECTRIC || (m.type == VT_MAT_GLOSSY && slot_lobe(A, m).x < 0.02f));
+}
+// The OpenPBR BSDF: OPENPBR slots and rough GLOSSY ones, given the slot table.
 template <bool kPbr>
 __device__ __forceinline__ bool is_pbr(const RenderArgs &A, const vt_material &m) {
-  return kPbr && m.type == VT_MAT_OPENPBR && A.pbr && __float_as_uint(m.pad) < A.nmat;
+  return kPbr && A.pbr && __float_as_uint(m.pad) < A.nmat &&
+         (m.type == VT_MAT_OPENPBR || (m.type == VT_MAT_GLOSSY && __ldg(A.pbr + 2u * __float_as_uint(m.pad)).x >= 0.02f));
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706) at an OPENPBR vertex: f (without the cosine) per lane
 // and the pdf of `a`.
@@ -975,6 +994,68 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   weight = make_float4(w.x, w.y, w.z, A.spectral ? w3 : 0.0f);
   return isfinite(weight.x) && isfinite(weight.y) && isfinite(weight.z) && isfinite(weight.w) && weight.x >= 0.0f &&
          weight.y >= 0.0f && weight.z >= 0.0f && weight.w >= 0.0f;
+}
+
+// sample_bsdf's delta branches (main.swift:3318-3352): weight = f |cos| / pdf per lane, pdf 0.
+// DIELECTRIC refracts or reflects by Schlick's Fresnel at the slot's IOR (cosine on the less dense
+// side; one draw, none under total internal reflection), tinted by the albedo, eta^2 on refraction;
+// an event that the shading normal sends to the wrong side of the surface is retried once about the
+// geometric normal. A GLOSSY mirror reflects about the shading normal (the geometric one when that
+// reflection would go below the surface) with Schlick's conductor Fresnel of F0 = albedo per lane;
+// in spectral transport a thin film over it mixes in the film-over-metal reflectance by its presence
+// (spectral_thin_film_mirror, main.swift:3272-3283). `front`: the ray meets the outer side.
+__device__ __forceinline__ float3 reflect3(float3 i, float3 n) { return sub(i, mul(n, 2.0f * dot3(n, i))); }
+__device__ __forceinline__ float schlick5(float x) {
+  const float x2 = x * x;
+  return x2 * x2 * x;
+}
+__device__ __forceinline__ bool sample_delta(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 in,
+                             bool front, Sampler &seed, float3 &dir, float4 &weight) {
+  const float4 tint = reflectance(A, L, m);
+  if (m.type == VT_MAT_DIELECTRIC) {
+    const float ior = slot_lobe(A, m).z;
+    const float eta = front ? 1.0f / ior : ior;
+    const float r0 = (1.0f - ior) / (1.0f + ior), f0 = r0 * r0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const float3 mm = attempt == 0 ? n : gn;
+      const float cosI = fminf(fmaxf(-dot3(in, mm), 0.0f), 1.0f);
+      const float sin2T = eta * eta * (1.0f - cosI * cosI);
+      const float cosine = eta > 1.0f && sin2T < 1.0f ? sqrtf(1.0f - sin2T) : cosI;
+      const float fresnel = f0 + (1.0f - f0) * schlick5(1.0f - cosine);
+      const bool reflected = sin2T >= 1.0f || rand_f(seed) < fresnel;
+      if (reflected) {
+        dir = normalize3(reflect3(in, mm));
+        weight = tint;
+      } else {
+        dir = normalize3(add(mul(in, eta), mul(mm, eta * cosI - sqrtf(1.0f - sin2T))));
+        weight = scale4(tint, eta * eta);
+      }
+      if ((dot3(dir, gn) > 0.0f) == reflected) return true;
+    }
+    return false;
+  }
+  const float3 mm = dot3(reflect3(in, n), gn) > 0.0f ? n : gn;
+  dir = normalize3(reflect3(in, mm));
+  const float cosI = fminf(fmaxf(-dot3(in, mm), 0.0f), 1.0f);
+  const float s = schlick5(1.0f - cosI);
+  weight = make_float4(tint.x + (1.0f - tint.x) * s, tint.y + (1.0f - tint.y) * s, tint.z + (1.0f - tint.z) * s,
+                       A.spectral ? tint.w + (1.0f - tint.w) * s : 0.0f);
+  if (A.spectral) {
+    const float4 film = slot_film(A, m);
+    const float nm = film.y * 1000.0f;
+    const float presence = pbr_thin_film_presence(film.x, nm);
+    if (presence > 0.0f) {
+      float3 rd, rm, rm3;
+      pbr_thin_film(cosI, 1.0f, film.z, 1.5f, make_float3(tint.x, tint.y, tint.z), false, true, nm,
+                    make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2)), rd, rm);
+      const float l3 = lane_lambda(A, L, 3);
+      pbr_thin_film(cosI, 1.0f, film.z, 1.5f, make_float3(tint.w, tint.w, tint.w), false, true, nm, make_float3(l3, l3, l3),
+                    rd, rm3);
+      weight = make_float4(weight.x + (rm.x - weight.x) * presence, weight.y + (rm.y - weight.y) * presence,
+                           weight.z + (rm.z - weight.z) * presence, weight.w + (rm3.x - weight.w) * presence);
+    }
+  }
+  return dot3(dir, gn) > 0.0f;
 }
 
 // NEE at a vertex: the contribution per lane (quad: 2 draws; emitters: 4).
@@ -1176,9 +1257,9 @@ __device__ __forceinline__ NrcInput nrc_query(const RenderArgs &A, const Lanes &
   NrcInput q;
   float rough = 1.0f, metal = 0.0f;
   if (is_pbr<kPbr>(A, m)) {
-    const float4 pq = __ldg(A.pbr + __float_as_uint(m.pad));
+    const float4 pq = slot_lobe(A, m);
     rough = pq.x;
-    metal = nrc_sat(pq.y);
+    metal = m.type == VT_MAT_GLOSSY ? 1.0f : nrc_sat(pq.y);
   }
   const float2 w = nrc_sphere(mul(dir, -1.0f)), n = nrc_sphere(S.n);
   q.a = make_float4(S.pos.x, S.pos.y, S.pos.z, rough);
@@ -1233,28 +1314,40 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
   // ReSTIR GI's reservoir estimates the direct light of the secondary diffuse vertex of a path whose
   // diffuse primary took ReSTIR DI, so that vertex skips NEE (restirGISecondary, main.swift:7801-7803).
   const bool giPrimary = diPrimary && !kNrc && m.type == VT_MAT_DIFFUSE;
+  // Ideal reflections and refractions spend no scattering event (main.swift:7716-7723); `delta`
+  // follows the path's current vertex. The cache-terminated form (kNrc: vt_render_nrc's ReSTIR DI
+  // frames) is compiled without glass and mirrors, and the host refuses scenes that have them there.
+  bool delta = !kNrc && is_delta<kPbr>(A, m);
   for (int bounce = 1;; ++bounce) {
-    if (scattering >= limit) {
+    if (!delta && scattering >= limit) {
       // BSDF-only paths take one final continuation that may only reach emission.
       if (nee || emissionOnly) break;
       emissionOnly = true;
     }
-    ++scattering;
+    if (!delta) ++scattering;
     const bool previousMIS = mis && !(diPrimary && bounce == 1);
-    // sample_bsdf, Lambert: one 3D draw (three PCG draws), the direction from the last two.
     sampler_event(seed, (uint32_t)bounce, kZBsdf);
-    const float3 r = rand_f3(seed);
     float3 nd;
     float bpdf;
-    if (is_pbr<kPbr>(A, m)) {  // the prepared OpenPBR sample, from all three numbers
+    if (delta) {  // glass or mirror: its own draws (sample_delta)
       float4 w;
-      if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+      if (!sample_delta(A, L, m, S.n, S.gn, dir, S.front, seed, nd, w)) break;
       T = mul4(T, w);
+      bpdf = 0.0f;
     } else {
-      nd = cosine_hemisphere(S.n, r.y, r.z);
-      bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
-      if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
-      T = mul4(T, reflectance(A, L, m));
+      // One 3D draw (three PCG draws): the prepared OpenPBR sample takes all three, sample_bsdf's
+      // Lambert branch the direction from the last two.
+      const float3 r = rand_f3(seed);
+      if (is_pbr<kPbr>(A, m)) {
+        float4 w;
+        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+        T = mul4(T, w);
+      } else {
+        nd = cosine_hemisphere(S.n, r.y, r.z);
+        bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+        if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
+        T = mul4(T, reflectance(A, L, m));
+      }
     }
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
     const float3 prev = S.pos;
@@ -1266,35 +1359,39 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       // previous vertex (main.swift:7751-7756).
       if (A.env) {
         const float lpdf = nee ? environment_pdf(A, dir, S.n) : 0.0f;
-        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+        const float w = emission_weight(delta, nee, previousMIS, bpdf, lpdf);
         R = add(R, to_rgb(A, L, scale4(mul4(T, emission3(A, L, environment(A, dir))), w)));
       }
       break;
     }
     S = surface_at(A, h, o, dir);
     m = material(A, S.slot);
-    if (kNrc) spread += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
+    if (kNrc && !delta) spread += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
     if (m.type == VT_MAT_EMISSIVE) {
-      // emission_weight (main.swift:3462-3466): 1 without NEE or without a light pdf, else the
-      // power heuristic (MIS) or 0 (light sampling, or a ReSTIR DI vertex).
+      // emission_weight (main.swift:3462-3466): 1 after an ideal bounce, without NEE or without a
+      // light pdf, else the power heuristic (MIS) or 0 (light sampling, or a ReSTIR DI vertex).
       const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
-      const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+      const float w = emission_weight(delta, nee, previousMIS, bpdf, lpdf);
       if (!A.imported || S.front) R = add(R, to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w)));
       break;
     }
     if (emissionOnly) break;
-    if (kNrc && (A.nrcVertex ? (uint32_t)bounce >= A.nrcVertex : spread * spread > spreadLimit)) {
+    // Glass and mirrors take no NEE, and the cache is queried at rough vertices only.
+    const bool nextDelta = !kNrc && is_delta<kPbr>(A, m);
+    delta = nextDelta;
+    if (kNrc && !nextDelta && (A.nrcVertex ? (uint32_t)bounce >= A.nrcVertex : spread * spread > spreadLimit)) {
       nrc_store(A, slot, nrc_query<kPbr>(A, L, S, m, dir), L, T);
       *queried = true;
       break;
     }
-    if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
+    if (nee && !nextDelta && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
       R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
-      const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+      // A higher ceiling at ideal vertices keeps long mirror chains alive (main.swift:7820-7823).
+      const float survival = fminf(fmaxf(max4(A, T), 0.05f), nextDelta ? 0.99f : 0.95f);
       sampler_event(seed, (uint32_t)bounce + 1u, kZRoulette);
       if (rand_f(seed) >= survival) break;
       T = scale4(T, 1.0f / survival);
@@ -1320,7 +1417,7 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
   const vt_material m = material(A, S.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission(A, L, S, m);
   float3 R = f3(0.0f, 0.0f, 0.0f);
-  if (A.mode != 3u) {
+  if (A.mode != 3u && (kNrc || !is_delta<kPbr>(A, m))) {  // no NEE at glass or a mirror (main.swift:7657)
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
@@ -1625,8 +1722,11 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
   } else if (m.type != VT_MAT_DIFFUSE) {
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true);
+    R = f3(0.0f, 0.0f, 0.0f);
+    if (kNrc || !is_delta<kPbr>(A, m)) {  // no NEE at glass or a mirror (main.swift:7657)
+      sampler_event(seed, 1u, kZNee);
+      R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true);
+    }
     const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
     R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, spreadLimit, slot, &queried));
   } else {
@@ -1760,7 +1860,7 @@ __device__ __forceinline__ float2 frame_jitter(uint32_t sampleIndex) {
 // summed in k_render's order) to its pixel's FP64 accumulation.
 constexpr int kWfBlock = 256;
 constexpr uint32_t kWfShadow = 1u, kWfShadowPrimary = 2u, kWfEmissionOnly = 4u, kWfPrevMIS = 8u, kWfQueried = 16u,
-                   kWfDead = 32u;
+                   kWfDead = 32u, kWfPrevDelta = 64u;
 
 struct WfArgs {
   float4 *T;      // throughput per lane
@@ -1890,7 +1990,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
       } else {
         T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         if (kNrc) W.spread[i] = make_float2(0.0f, nrc_spread_limit(A, h.t, S.gn, dir));
-        if (A.mode != 3u) {
+        if (A.mode != 3u && !is_delta<kPbr>(A, m)) {
           sampler_event(seed, 1u, kZNee);
           if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, A.mode == 1u && limit > 0, limit > 0, seed, true)) {
             shadow = true;
@@ -1904,11 +2004,11 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
   } else {  // continue_path after its trace at bounce b
     const float4 pv = W.prev[i];
     const float bpdf = pv.w;
-    const bool previousMIS = (flags & kWfPrevMIS) != 0u;
+    const bool previousMIS = (flags & kWfPrevMIS) != 0u, previousDelta = (flags & kWfPrevDelta) != 0u;
     if (h.pos < 0) {
       if (A.env) {
         const float lpdf = nee ? environment_pdf(A, dir, f3(pn.x, pn.y, pn.z)) : 0.0f;
-        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+        const float w = emission_weight(previousDelta, nee, previousMIS, bpdf, lpdf);
         const float3 c = to_rgb(A, L, scale4(mul4(T, emission3(A, L, environment(A, dir))), w));
         Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
       }
@@ -1920,12 +2020,13 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
       float2 sp = make_float2(0.0f, 0.0f);
       if (kNrc) {
         sp = W.spread[i];
-        sp.x += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
+        if (!previousDelta) sp.x += h.t * rsqrtf(fmaxf(bpdf * fabsf(dot3(S.gn, dir)), 1e-30f));
         W.spread[i] = sp;
       }
+      const bool delta = is_delta<kPbr>(A, m);
       if (m.type == VT_MAT_EMISSIVE) {
         const float lpdf = A.imported ? emitter_pdf(A, prevPos, S.pos, S.face) : light_pdf(A, prevPos, S.pos);
-        const float w = emission_weight(false, nee, previousMIS, bpdf, lpdf);
+        const float w = emission_weight(previousDelta, nee, previousMIS, bpdf, lpdf);
         if (!A.imported || S.front) {
           const float3 c = to_rgb(A, L, scale4(mul4(T, emission(A, L, m.emission)), w));
           Rc = make_float4(Rc.x + c.x, Rc.y + c.y, Rc.z + c.z, 0.0f);
@@ -1933,12 +2034,12 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         alive = false;
       } else if (emissionOnly) {
         alive = false;
-      } else if (kNrc && (A.nrcVertex ? b >= A.nrcVertex : sp.x * sp.x > sp.y)) {
+      } else if (kNrc && !delta && (A.nrcVertex ? b >= A.nrcVertex : sp.x * sp.x > sp.y)) {
         nrc_store(A, wf_slot(W, i), nrc_query<kPbr>(A, L, S, m, dir), L, T);
         flags |= kWfQueried;
         alive = false;
       } else {
-        if (nee) {
+        if (nee && !delta) {
           sampler_event(seed, b + 1u, kZNee);
           if (wf_nee<kPbr>(A, W, i, L, S, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit, seed, false)) {
             shadow = true;
@@ -1946,7 +2047,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
           }
         }
         if (b > 3u) {
-          const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+          const float survival = fminf(fmaxf(max4(A, T), 0.05f), delta ? 0.99f : 0.95f);
           sampler_event(seed, b + 1u, kZRoulette);
           if (rand_f(seed) >= survival) alive = false;
           else T = scale4(T, 1.0f / survival);
@@ -1956,25 +2057,33 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
   }
   if (alive) {  // continue_path's loop head at bounce b + 1: the BSDF continuation
     const uint32_t nb = b + 1u;
-    if (scattering >= limit) {
+    const bool delta = is_delta<kPbr>(A, m);
+    if (!delta && scattering >= limit) {
       if (nee || emissionOnly) alive = false;
       emissionOnly = true;
     }
     if (alive) {
-      ++scattering;
+      if (!delta) ++scattering;
       sampler_event(seed, nb, kZBsdf);
-      const float3 r = rand_f3(seed);
       float3 nd;
       float bpdf;
-      if (is_pbr<kPbr>(A, m)) {
+      if (delta) {
         float4 w;
-        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) alive = false;
+        bpdf = 0.0f;
+        if (!sample_delta(A, L, m, S.n, S.gn, dir, S.front, seed, nd, w)) alive = false;
         else T = mul4(T, w);
       } else {
-        nd = cosine_hemisphere(S.n, r.y, r.z);
-        bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
-        if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) alive = false;
-        else T = mul4(T, reflectance(A, L, m));
+        const float3 r = rand_f3(seed);
+        if (is_pbr<kPbr>(A, m)) {
+          float4 w;
+          if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) alive = false;
+          else T = mul4(T, w);
+        } else {
+          nd = cosine_hemisphere(S.n, r.y, r.z);
+          bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+          if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) alive = false;
+          else T = mul4(T, reflectance(A, L, m));
+        }
       }
       if (alive && (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f))
         alive = false;
@@ -1985,6 +2094,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         W.prevN[i] = make_float4(S.n.x, S.n.y, S.n.z, pn.w);
         W.T[i] = T;
         flags = mis ? (flags | kWfPrevMIS) : (flags & ~kWfPrevMIS);
+        flags = delta ? (flags | kWfPrevDelta) : (flags & ~kWfPrevDelta);
         next = true;
       }
     }
@@ -2019,8 +2129,10 @@ __global__ void __launch_bounds__(kWfBlock) k_wf_generate(RenderArgs A, WfArgs W
   }
 }
 
+// Two blocks of kWfBlock per SM (at most 128 registers): the OpenPBR variant's register demand
+// (with thin films) would otherwise leave one block, and the stage is latency-bound on its loads.
 template <bool kPbr, bool kNrc>
-__global__ void __launch_bounds__(kWfBlock) k_wf_shade(RenderArgs A, WfArgs W, uint32_t bounce) {
+__global__ void __launch_bounds__(kWfBlock, 2) k_wf_shade(RenderArgs A, WfArgs W, uint32_t bounce) {
   __shared__ uint32_t sTotal, sBase;
   const uint32_t n = W.inCount ? min(*W.inCount, W.paths) : W.paths;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -2117,27 +2229,38 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
   }
   float4 *rec = scratch + (size_t)j * kNrcRecords * 5;
   int nrec = 0;
-  {
+  // Records and NEE at rough vertices only; glass and mirrors spend no scattering event.
+  if (!is_delta<kPbr>(A, m)) {
     const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
+    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, limit > 0, seed, stack,
+                                         true));
   }
-  R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true));
   int scattering = 0;
-  for (int bounce = 1; scattering < limit; ++bounce) {
-    ++scattering;
-    const float3 r = rand_f3(seed);
+  for (int bounce = 1;; ++bounce) {
+    const bool delta = is_delta<kPbr>(A, m);
+    if (!delta && scattering >= limit) break;
+    if (!delta) ++scattering;
     float3 nd;
     float bpdf;
-    if (is_pbr<kPbr>(A, m)) {
+    if (delta) {
       float4 w;
-      if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+      if (!sample_delta(A, L, m, S.n, S.gn, dir, S.front, seed, nd, w)) break;
       T = mul4(T, w);
+      bpdf = 0.0f;
     } else {
-      nd = cosine_hemisphere(S.n, r.y, r.z);
-      bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
-      if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
-      T = mul4(T, reflectance(A, L, m));
+      const float3 r = rand_f3(seed);
+      if (is_pbr<kPbr>(A, m)) {
+        float4 w;
+        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+        T = mul4(T, w);
+      } else {
+        nd = cosine_hemisphere(S.n, r.y, r.z);
+        bpdf = fmaxf(0.0f, dot3(S.n, nd)) * kInvPi;
+        if (!(bpdf > 0.0f) || !(dot3(nd, S.gn) > 0.0f)) break;
+        T = mul4(T, reflectance(A, L, m));
+      }
     }
     if (!isfinite(T.x) || !isfinite(T.y) || !isfinite(T.z) || !isfinite(T.w) || max4(A, T) <= 0.0f) break;
     const float3 prev = S.pos;
@@ -2147,7 +2270,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       // An escape sees the environment, weighed against its NEE density at the last vertex.
       if (A.env) {
         const float lpdf = environment_pdf(A, dir, S.n);
-        const float w = emission_weight(false, true, true, bpdf, lpdf);
+        const float w = emission_weight(delta, true, true, bpdf, lpdf);
         R = add4(R, scale4(mul4(T, emission3(A, L, environment(A, dir))), w));
       }
       break;
@@ -2156,20 +2279,23 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     m = material(A, S.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       const float lpdf = A.imported ? emitter_pdf(A, prev, S.pos, S.face) : light_pdf(A, prev, S.pos);
-      const float w = emission_weight(false, true, true, bpdf, lpdf);
+      const float w = emission_weight(delta, true, true, bpdf, lpdf);
       if (!A.imported || S.front) R = add4(R, scale4(mul4(T, emission(A, L, m.emission)), w));
       break;
     }
-    if (nrec < kNrcRecords) {
-      const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
-      float4 *r = rec + 5 * nrec;
-      r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
-      ++nrec;
+    const bool nextDelta = is_delta<kPbr>(A, m);
+    if (!nextDelta) {
+      if (nrec < kNrcRecords) {
+        const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
+        float4 *r = rec + 5 * nrec;
+        r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
+        ++nrec;
+      }
+      R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit,
+                                           scattering < limit, seed, stack, false));
     }
-    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit, scattering < limit, seed,
-                                         stack, false));
     if (bounce > 3) {
-      const float survival = fminf(fmaxf(max4(A, T), 0.05f), 0.95f);
+      const float survival = fminf(fmaxf(max4(A, T), 0.05f), nextDelta ? 0.99f : 0.95f);
       if (rand_f(seed) >= survival) break;
       T = scale4(T, 1.0f / survival);
     }
@@ -2375,6 +2501,13 @@ void host_normalize(float v[3]) {
 namespace {
 
 // Shared by both scene kinds: validation, material slots, spectral tables.
+// Some slot is ideal glass, or a GLOSSY mirror smoother than 0.02 (is_delta on the host).
+static bool scene_has_delta(const vt_scene *sc) {
+  for (size_t i = 0; i < sc->slot_types.size(); ++i)
+    if (sc->slot_types[i] == VT_MAT_DIELECTRIC || (sc->slot_types[i] == VT_MAT_GLOSSY && sc->slot_rough[i] < 0.02f)) return true;
+  return false;
+}
+
 vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *materials, uint32_t nmat,
                        const float *lightEmission, const vt_spectral_tables *tables, vt_scene *sc) {
   (void)lightEmission;
@@ -2385,8 +2518,19 @@ vt_status scene_common(vt_ctx *ctx, const vt_mesh *mesh, const vt_material *mate
     const vt_status st = vt_uplift_ensure(ctx, tables);
     if (st != VT_OK) return st;
   }
+  for (uint32_t i = 0; i < nmat; ++i)
+    if (materials[i].type < VT_MAT_DIFFUSE || materials[i].type > VT_MAT_OPENPBR)
+      return vt_fail(ctx, VT_ERR_INVALID, "material slot " + std::to_string(i) + " has an unknown type");
   sc->mesh = mesh;
   sc->nmat = nmat;
+  sc->layered = false;
+  sc->slot_types.resize(nmat);
+  sc->slot_rough.assign(nmat, 0.0f);
+  for (uint32_t i = 0; i < nmat; ++i) {
+    sc->slot_types[i] = materials[i].type;
+    if (materials[i].type == VT_MAT_GLOSSY || materials[i].type == VT_MAT_DIELECTRIC || materials[i].type == VT_MAT_OPENPBR)
+      sc->layered = true;
+  }
   if (nmat) {
     // The device copy carries each slot's index in `pad` (the key of its uplifted reflectance).
     std::vector<vt_material> mats(materials, materials + nmat);
@@ -2788,6 +2932,7 @@ void fill_args(const vt_scene *scene, const vt_frame_params *p, uint32_t spp, Re
   A.icdf = scene->d_icdf;
   A.slotL = scene->d_slotL;
   A.pbr = scene->d_pbr;
+  A.layered = scene->layered ? 1u : 0u;
   if (scene->pbr_tables) A.pbrT = pbr_tables_at(scene->pbr_tables);
   A.cosPhase = scene->d_cosphase;
   A.ebasis = scene->d_ebasis;
@@ -2949,7 +3094,7 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
       A.pup = make_float3(pc[9], pc[10], pc[11]);
       A.paspect = pc[12];
       A.pfovScale = pc[13];
-      if (A.pbr) {
+      if (A.layered) {
         A.kernelId = 3;
         k_di_primary<true><<<blocks, kRenderBlock, 0, s>>>(A, k);
         A.kernelId = nrc ? 5 : 4;
@@ -2983,14 +3128,14 @@ vt_status render_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p, ui
   const uint32_t grid = (uint32_t)std::min<uint64_t>((items + kRenderBlock - 1) / kRenderBlock, (uint64_t)ctx->sm_count * 32u);
   if (nrc) {
     A.kernelId = 2;
-    if (A.pbr) k_render<true, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    if (A.layered) k_render<true, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     else k_render<false, true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     VT_CUDA(ctx, cudaGetLastError());
     const vt_status st = nrc_finish(ctx, nrc, A, spp, s);
     if (st != VT_OK) return st;
   } else {
     A.kernelId = 1;
-    if (A.pbr) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
+    if (A.layered) k_render<true><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     else k_render<false><<<grid, kRenderBlock, 0, s>>>(A, groups, per);
     VT_CUDA(ctx, cudaGetLastError());
   }
@@ -3127,7 +3272,7 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
   const uint32_t every = std::max(1u, run.compactEvery);
   W.deadFlags = every > 1u ? 1u : 0u;
   const int block = std::max(32, std::min(run.block, kWfBlock));
-  const bool pbr = A.pbr != nullptr;
+  const bool pbr = A.layered != 0u;
   const uint32_t gridMax = (uint32_t)ctx->sm_count * (8u * kWfBlock / (uint32_t)block);
   uint32_t *slot = vt_queue_slot(ctx);
   for (uint32_t k0 = 0; k0 < spp; k0 += chunk) {
@@ -3199,6 +3344,9 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
   if ((p->spectral != 0) != (nrc->cfg.spectral != 0))
     return vt_fail(ctx, VT_ERR_INVALID, "the frame's transport (spectral or rgb) differs from the cache's `spectral` setting");
   if (p->pixel_stride > 1) return vt_fail(ctx, VT_ERR_INVALID, "the cache renders whole frames (pixel_stride 0 or 1)");
+  if ((flags & VT_NRC_RENDER) && p->sampling_mode == 0u && scene_has_delta(scene))
+    return vt_fail(ctx, VT_ERR_INVALID, "the cache's ReSTIR DI frames (sampling mode 0) do not take glass or mirror slots; "
+                                        "render them in sampling mode 1");
   {
     const vt_status st = check_params(ctx, scene, p);
     if (st != VT_OK) return st;
@@ -3242,7 +3390,7 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
       nrc->scratch_cap = scratch;
     }
     const unsigned blocks = (npaths + kRenderBlock - 1) / kRenderBlock;
-    if (A.pbr)
+    if (A.layered)
       k_nrc_paths<true><<<blocks, kRenderBlock, 0, ps>>>(A, npaths, h % npix, stride, si0, cap, nrc->d_scratch,
                                                         nrc->scratch_cap, nrc->d_tin, nrc->d_ttarget, nrc->tcap,
                                                         nrc->d_count);
@@ -3257,7 +3405,8 @@ vt_status vt_render_nrc(vt_ctx *ctx, vt_scene *scene, vt_nrc *nrc, const vt_fram
     }
   }
   if (flags & VT_NRC_RENDER) {
-    // MIS primaries through the wavefront integrator; ReSTIR DI's frames through its two passes.
+    // MIS primaries through the wavefront integrator; ReSTIR DI's frames through its two passes
+    // (compiled without glass and mirrors, see continue_path).
     const vt_status st = p->sampling_mode == 1u ? wavefront_impl(ctx, scene, p, spp, stream, nrc)
                                                 : render_impl(ctx, scene, p, spp, stream, nrc);
     if (both) {
@@ -3448,7 +3597,7 @@ vt_status vt_batch_create(vt_ctx *ctx, vt_scene *const *scenes, const vt_frame_p
     args[i].kernelId = 7;
     args[i].jitter = nullptr;
     first[i] = args[i].first;
-    if (args[i].pbr) b->pbr = true;
+    if (args[i].layered) b->pbr = true;
     frame[i] = args[i].firstFrame;
     begin[i + 1] = begin[i] + (unsigned long long)params[i].width * params[i].height;
     b->scenes.push_back(scenes[i]);
@@ -3691,6 +3840,7 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": thin-film weight must lie in [0, 1], its "
                                           "thickness be finite and non-negative and its IOR positive");
     q[2 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
+    scene->slot_rough[i] = p.roughness;
     q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f, 0.0f);
   }
   if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, q.size() * sizeof(float4)));
@@ -3832,7 +3982,7 @@ extern "C" vt_status vt_sampler_frame(vt_ctx *ctx, uint32_t width, uint32_t heig
 //   out[6..7]  min and max of rand_f over 100,000 draws from seed 17 (expected in [0, 1))
 //   out[8..10] scattering_limit of depths 0, 1 and 8 (main.swift:3471-3473; expected 0, 0, 7)
 namespace {
-__global__ void k_known_answers(float *out) {
+__global__ void k_known_answers(float *out, const float4 *glassParams) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   out[0] = power_heuristic(1e-10f, 1e-10f);
   out[1] = emission_weight(false, true, false, 0.2f, 1.0f);
@@ -3854,6 +4004,29 @@ __global__ void k_known_answers(float *out) {
   out[7] = hi;
   const uint32_t depths[3] = {0u, 1u, 8u};
   for (int k = 0; k < 3; ++k) out[8 + k] = float(max(0, (int)depths[k] - 1));
+  // Glass (IOR 1.52, white) met from inside at normal (0, 0, -1) by normalize(0.9, 0, 0.435): total
+  // internal reflection, so the sample exists, goes to z < 0 and weighs exactly 1 (the shading normal
+  // is the geometric one, as the reference's Material without a geometric normal gives).
+  RenderArgs A = {};
+  A.pbr = glassParams;
+  A.nmat = 1u;
+  vt_material glass;
+  glass.type = VT_MAT_DIELECTRIC;
+  glass.albedo[0] = glass.albedo[1] = glass.albedo[2] = 1.0f;
+  glass.emission[0] = glass.emission[1] = glass.emission[2] = 0.0f;
+  glass.pad = __uint_as_float(0u);
+  Sampler seed = {};
+  seed.state = s;
+  Lanes L = {};
+  const float3 nn = f3(0.0f, 0.0f, -1.0f);
+  float3 dir = f3(0.0f, 0.0f, 0.0f);
+  float4 w = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const bool ok = sample_delta(A, L, glass, nn, nn, normalize3(f3(0.9f, 0.0f, 0.435f)), false, seed, dir, w);
+  out[11] = ok ? 1.0f : 0.0f;
+  out[12] = dir.z;
+  out[13] = w.x;
+  out[14] = w.y;
+  out[15] = w.z;
 }
 }  // namespace
 
@@ -3861,11 +4034,15 @@ extern "C" vt_status vt_known_answers(vt_ctx *ctx, float *out, uint32_t n) {
   if (!ctx) return VT_ERR_INVALID;
   if (!out || n < VT_KNOWN_ANSWERS) return vt_fail(ctx, VT_ERR_INVALID, "out must hold VT_KNOWN_ANSWERS floats");
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
+  // The answers, then the glass slot's parameters (roughness, metalness, IOR 1.52, 0; no film).
   float *d = nullptr;
-  VT_CUDA(ctx, cudaMalloc(&d, VT_KNOWN_ANSWERS * sizeof(float)));
+  VT_CUDA(ctx, cudaMalloc(&d, (VT_KNOWN_ANSWERS + 8) * sizeof(float)));
+  const float glass[8] = {0.0f, 0.0f, 1.52f, 0.0f, 0.0f, 0.0f, 1.4f, 0.0f};
+  float4 *dGlass = reinterpret_cast<float4 *>(d + ((VT_KNOWN_ANSWERS + 3u) & ~3u));
   cudaError_t e = cudaMemsetAsync(d, 0xff, VT_KNOWN_ANSWERS * sizeof(float), ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dGlass, glass, sizeof glass, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) {
-    k_known_answers<<<1, 32, 0, ctx->stream>>>(d);
+    k_known_answers<<<1, 32, 0, ctx->stream>>>(d, dGlass);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, VT_KNOWN_ANSWERS * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);

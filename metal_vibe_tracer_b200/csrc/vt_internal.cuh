@@ -101,6 +101,9 @@ struct vt_scene {
   int32_t *d_face_pos = nullptr;
   vt_material *d_mats = nullptr;
   uint32_t nmat = 0;
+  bool layered = false;  // some slot is OPENPBR, GLOSSY or DIELECTRIC
+  std::vector<int32_t> slot_types;  // host copies: each slot's type and roughness (vt_scene_set_openpbr)
+  std::vector<float> slot_rough;
   vt_quad_light light;
   // Spectral tables: per 1 nm bin (cmf r, g, b, illuminant), the inverse CDF.
   float4 *d_spec = nullptr;

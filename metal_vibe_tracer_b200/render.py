@@ -13,7 +13,7 @@ import numpy as np
 from . import _lib
 from .accel import Context, MaterialLibraryError, Mesh, _check
 
-VT_MAT_DIFFUSE, VT_MAT_EMISSIVE, VT_MAT_OPENPBR = 0, 3, 4
+VT_MAT_DIFFUSE, VT_MAT_GLOSSY, VT_MAT_DIELECTRIC, VT_MAT_EMISSIVE, VT_MAT_OPENPBR = 0, 1, 2, 3, 4
 
 
 class Material(C.Structure):
@@ -133,9 +133,10 @@ class Scene:
             _check(ctx.handle, st, "vt_scene_create")
         self._p = p
         self.width = self.height = 0
-        if any(int(m["type"]) == VT_MAT_OPENPBR for m in materials):
-            # OPENPBR slots: roughness, metalness, IOR and diffuse roughness per slot (the reference's
-            # SurfaceSettings surface.x/y and detail.y; base colour is the albedo).
+        if any(int(m["type"]) in (VT_MAT_GLOSSY, VT_MAT_DIELECTRIC, VT_MAT_OPENPBR) for m in materials):
+            # OPENPBR, GLOSSY and DIELECTRIC slots: roughness, metalness, IOR and diffuse roughness per
+            # slot (the reference's SurfaceSettings surface.x/y and detail.y; base colour is the albedo;
+            # a GLOSSY slot below roughness 0.02 is a mirror, a DIELECTRIC slot ideal glass).
             openpbr_tables_set(ctx)
             params = (_lib.OpenPBRParams * len(materials))()
             for i, m in enumerate(materials):
@@ -296,7 +297,8 @@ def sampler_frame(ctx: Context, width: int, height: int, z: bool, model: int, sa
 def known_answers(ctx: Context) -> np.ndarray:
     """The reference's device known answers (regression_checks, tests/GPUChecks.swift:14-37) as the
     integrator's device functions compute them: power heuristic, emission weights, the grazing
-    cosine sample, rand_f's range and the scattering budget (layout in include/vt.h)."""
+    cosine sample, rand_f's range, the scattering budget and glass total internal reflection
+    (layout in include/vt.h)."""
     out = np.empty(_lib.KNOWN_ANSWERS, np.float32)
     _check(ctx.handle, _lib.load().vt_known_answers(ctx.handle, out.ctypes.data, out.size), "vt_known_answers")
     return out

@@ -271,6 +271,20 @@ def cornell_openpbr(seed: int = 0):
     return faces, verts, materials, light, camera
 
 
+def cornell_delta(seed: int = 0, film: bool = False):
+    """The coloured Cornell box with ideal glass and mirrors (the reference's DIELECTRIC and GLOSSY
+    types): a mirror tall box (GLOSSY, roughness 0, F0 (0.95, 0.9, 0.8); with `film` a 0.45 um film
+    of IOR 1.5 on it), a glass short box (DIELECTRIC, IOR 1.5, tint (0.98, 0.95, 0.9)) and a rough
+    GLOSSY red wall (roughness 0.3, the OpenPBR metal); the rest stays Lambert."""
+    faces, verts, materials, light, camera = cornell_coloured(seed=seed)
+    materials[3] = {"type": 1, "albedo": (0.63, 0.065, 0.05), "emission": (0.0, 0.0, 0.0), "roughness": 0.3, "ior": 1.5}
+    materials[5] = {"type": 1, "albedo": (0.95, 0.9, 0.8), "emission": (0.0, 0.0, 0.0), "roughness": 0.0, "ior": 1.5}
+    if film:
+        materials[5].update(thin_film_weight=1.0, thin_film_thickness=0.45, thin_film_ior=1.5)
+    materials[6] = {"type": 2, "albedo": (0.98, 0.95, 0.9), "emission": (0.0, 0.0, 0.0), "roughness": 0.0, "ior": 1.5}
+    return faces, verts, materials, light, camera
+
+
 def _mesh_from_triangles(tris, tags):
     n = len(tris)
     verts = np.zeros(3 * n, VERTEX_DTYPE)

@@ -112,6 +112,24 @@ void ref_openpbr_sample(const ref_openpbr_material *m, const float *n, const flo
   *lobe = (int32_t)type;
 }
 
+// A thin film over an ideal mirror (spectral_thin_film_mirror, main.swift:3272-3283): the film's
+// presence (weight times the upstream presence ramp at thickness_um * 1000 nm) and, where it is
+// positive, the upstream Airy reflectance of the film over metal at cos_i per wavelength, with the
+// mirror's F0, a white F82 tint, exterior IOR 1 and the unused dielectric base IOR 1.5.
+float ref_thin_film_mirror(float cos_i, float weight, float thickness_um, float film_ior, const float *f0,
+                           const float *lambda, float *reflectance) {
+  const float nm = thickness_um * 1000.0f;
+  const float presence = weight * openpbr_thin_film_presence_multiplier(nm);
+  if (!(presence > 0.0f)) return presence;
+  const OpenPBR_ThinFilmResults r = openpbr_thin_film_and_base_reflectance(
+      cos_i, 1.0f, film_ior, vec3(1.5f), false, vec3(f0[0], f0[1], f0[2]), vec3(1.0f), false, true, nm,
+      vec3(lambda[0], lambda[1], lambda[2]));
+  reflectance[0] = r.reflectance_metal.x;
+  reflectance[1] = r.reflectance_metal.y;
+  reflectance[2] = r.reflectance_metal.z;
+  return presence;
+}
+
 // The dense isotropic GGX energy complement (Shaders/MetalEnergy.metal) and its average.
 float ref_metal_energy(float alpha, float cos_theta) { return vibe_metal_energy(alpha, cos_theta); }
 float ref_metal_average_energy(float alpha) { return vibe_metal_average_energy(alpha); }

@@ -2256,17 +2256,28 @@ bool visible_d(const PtContext &C, D3 p, D3 gn, double err, const PtLight &ls) {
 
 // n: shading normal; gn: geometric normal (eval_bsdf for DIFFUSE, main.swift:2659-2676).
 // ---- OPENPBR vertices: the reference BSDF (float) through vto_pt_inputs ---------------------------
-bool pbr_slot(const PtContext &C, const vt_material &m) {
+// A slot's lobe parameters (8 floats; null without a table or past it).
+const float *slot_params(const PtContext &C, const vt_material &m) {
   uint32_t slot;
   std::memcpy(&slot, &m.pad, sizeof slot);
-  return m.type == 4 && C.in->pbr_params && C.in->pbr_eval && slot < C.in->nmat;
+  return C.in->pbr_params && slot < C.in->nmat ? C.in->pbr_params + 8 * (size_t)slot : nullptr;
+}
+// is_delta (main.swift:3285-3287): glass, and GLOSSY mirrors smoother than 0.02.
+bool is_delta_d(const PtContext &C, const vt_material &m) {
+  const float *pp = slot_params(C, m);
+  return m.type == VT_MAT_DIELECTRIC || (m.type == VT_MAT_GLOSSY && (pp ? pp[0] : 0.0f) < 0.02f);
+}
+// The OpenPBR BSDF: OPENPBR slots and rough GLOSSY ones (metalness 1 in the adapter).
+bool pbr_slot(const PtContext &C, const vt_material &m) {
+  const float *pp = slot_params(C, m);
+  return pp && C.in->pbr_eval && (m.type == VT_MAT_OPENPBR || (m.type == VT_MAT_GLOSSY && pp[0] >= 0.02f));
 }
 vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double b0, double b1, double b2) {
   uint32_t slot;
   std::memcpy(&slot, &m.pad, sizeof slot);
   vto_pbr_material q;
   std::memset(&q, 0, sizeof q);
-  q.type = 4;
+  q.type = m.type;
   q.albedo[0] = (float)b0;
   q.albedo[1] = (float)b1;
   q.albedo[2] = (float)b2;
@@ -2344,6 +2355,61 @@ bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material 
   return true;
 }
 
+// sample_bsdf's delta branches (main.swift:3318-3352), in double: DIELECTRIC refracts or reflects by
+// Schlick's Fresnel at the slot's IOR (the cosine on the less dense side; one draw, none under total
+// internal reflection; tint = albedo, times eta^2 on refraction), retried once about the geometric
+// normal when the event lands on the wrong side; a GLOSSY mirror reflects about the shading normal
+// (the geometric one when that reflection goes below the surface) with Schlick's conductor Fresnel,
+// F0 = albedo, and in spectral transport the reference's film over it (ref_thin_film_mirror) mixed in
+// by its presence. Weight = f |cos| / pdf per lane.
+D3 reflect_d(D3 i, D3 n) { return i - n * (2.0 * dot(n, i)); }
+bool sample_delta_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 in, bool front,
+                    ZSampler &seed, D3 &dir, Spec4 &w) {
+  const Spec4 tint = reflectance(C, L, m);
+  const float *pp = slot_params(C, m);
+  if (m.type == VT_MAT_DIELECTRIC) {
+    const double ior = pp ? pp[2] : 1.5;
+    const double eta = front ? 1.0 / ior : ior;
+    const double r0 = (1.0 - ior) / (1.0 + ior), f0 = r0 * r0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const D3 mm = attempt == 0 ? n : gn;
+      const double cosI = std::min(std::max(-dot(in, mm), 0.0), 1.0);
+      const double sin2T = eta * eta * (1.0 - cosI * cosI);
+      const double cosine = eta > 1.0 && sin2T < 1.0 ? std::sqrt(1.0 - sin2T) : cosI;
+      const double fresnel = f0 + (1.0 - f0) * std::pow(1.0 - cosine, 5.0);
+      const bool reflected = sin2T >= 1.0 || seed.f1() < fresnel;
+      if (reflected) {
+        dir = normalize(reflect_d(in, mm));
+        w = tint;
+      } else {
+        dir = normalize(in * eta + mm * (eta * cosI - std::sqrt(1.0 - sin2T)));
+        w = scale(tint, eta * eta);
+      }
+      if ((dot(dir, gn) > 0.0) == reflected) return true;
+    }
+    return false;
+  }
+  const D3 mm = dot(reflect_d(in, n), gn) > 0.0 ? n : gn;
+  dir = normalize(reflect_d(in, mm));
+  const double cosI = std::min(std::max(-dot(in, mm), 0.0), 1.0);
+  const double s5 = std::pow(1.0 - cosI, 5.0);
+  for (int k = 0; k < 4; ++k) w.v[k] = tint.v[k] + (1.0 - tint.v[k]) * s5;
+  if (!C.spectral) w.v[3] = 0.0;
+  if (C.spectral && pp && C.in->pbr_film_mirror && pp[4] > 0.0f) {
+    const float f0a[3] = {(float)tint.v[0], (float)tint.v[1], (float)tint.v[2]}, f0b[3] = {(float)tint.v[3], (float)tint.v[3], (float)tint.v[3]};
+    const float la[3] = {(float)L.lambda[0], (float)L.lambda[1], (float)L.lambda[2]};
+    const float lb[3] = {(float)L.lambda[3], (float)L.lambda[3], (float)L.lambda[3]};
+    float ra[3], rb[3];
+    const double presence = C.in->pbr_film_mirror((float)cosI, pp[4], pp[5], pp[6], f0a, la, ra);
+    if (presence > 0.0) {
+      C.in->pbr_film_mirror((float)cosI, pp[4], pp[5], pp[6], f0b, lb, rb);
+      const double film[4] = {ra[0], ra[1], ra[2], rb[0]};
+      for (int k = 0; k < 4; ++k) w.v[k] = w.v[k] + (film[k] - w.v[k]) * presence;
+    }
+  }
+  return dot(dir, gn) > 0.0;
+}
+
 D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
             const vt_material &m, bool useMIS, bool compensated, ZSampler &seed, bool requirePdf) {
   const PtLight ls = C.imported ? sample_emitters_d(C, p, n, seed, compensated) : sample_light_d(C, p, seed);
@@ -2414,18 +2480,24 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
   int scattering = 0;
   bool emissionOnly = false;
   for (int bounce = 1;; ++bounce) {
-    if (scattering >= limit) {
+    // Ideal reflections and refractions spend no scattering event (main.swift:7716-7723).
+    const bool delta = is_delta_d(C, m);
+    if (!delta && scattering >= limit) {
       if (nee || emissionOnly) break;
       emissionOnly = true;
     }
-    ++scattering;
+    if (!delta) ++scattering;
     const bool previousMIS = mis && !(diPrimary && bounce == 1);
     seed.event((uint32_t)bounce, 0u);
-    double r0, r1, r2;
-    seed.f3(r0, r1, r2);
     D3 nd;
-    double bpdf;
-    if (pbr_slot(C, m)) {
+    double bpdf = 0.0;
+    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+    if (!delta) seed.f3(r0, r1, r2);
+    if (delta) {
+      Spec4 w;
+      if (!sample_delta_d(C, L, m, h.n, h.gn, dir, h.front, seed, nd, w)) break;
+      T = mul(T, w);
+    } else if (pbr_slot(C, m)) {
       const double r[3] = {r0, r1, r2};
       Spec4 w;
       if (!pbr_sample_lanes_d(C, L, m, h.n, h.gn, dir * -1.0, r, nd, w, bpdf)) break;
@@ -2450,7 +2522,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
       // An escape sees the environment, weighed against its NEE density (main.swift:7751-7756).
       if (C.env) {
         const double lpdf = nee ? environment_pdf_d(C, nd, prevN) : 0.0;
-        const double w = !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
+        const double w = delta || !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
         const D3 e = environment_d(C, nd);
         const float ef[3] = {(float)e.x, (float)e.y, (float)e.z};
         R = R + to_rgb(C, L, scale(mul(T, emission(C, L, ef)), w));
@@ -2460,18 +2532,20 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     m = pt_material(C, h.slot);
     if (m.type == VT_MAT_EMISSIVE) {
       const double lpdf = C.imported ? emitter_pdf_d(C, prev, h.pos, h.face) : light_pdf_d(C, prev, h.pos);
-      const double w = !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
+      const double w = delta || !nee || lpdf <= 0.0 ? 1.0 : (previousMIS ? power_heuristic_d(bpdf, lpdf) : 0.0);
       if (!C.imported || h.front) R = R + to_rgb(C, L, scale(mul(T, emission(C, L, m.emission)), w));
       break;
     }
     if (emissionOnly) break;
-    if (nee && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
+    // No NEE at glass or mirrors (main.swift:7803); the roulette ceiling is 0.99 there (:7820-7823).
+    const bool nextDelta = is_delta_d(C, m);
+    if (nee && !nextDelta && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       seed.event((uint32_t)bounce + 1u, 1u);
       R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, scattering < limit, seed,
                        false);
     }
     if (bounce > 3) {
-      const double survival = std::min(std::max(smax(C, T), 0.05), 0.95);
+      const double survival = std::min(std::max(smax(C, T), 0.05), nextDelta ? 0.99 : 0.95);
       seed.event((uint32_t)bounce + 1u, 2u);
       if (seed.f1() >= survival) break;
       T = scale(T, 1.0 / survival);
@@ -2747,11 +2821,14 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
   const vt_material m = pt_material(C, h.slot);
   if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
   if (m.type != VT_MAT_DIFFUSE) {
-    // Other primaries: NEE with MIS (main.swift:7767-7780).
+    // Other primaries: NEE with MIS (main.swift:7657-7672), none at glass or mirrors.
     const int limit = std::max(0, (int)C.p->max_depth - 1);
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
-    seed.event(1u, 1u);
-    D3 R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, limit > 0, seed, true);
+    D3 R{0, 0, 0};
+    if (!is_delta_d(C, m)) {
+      seed.event(1u, 1u);
+      R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, limit > 0, seed, true);
+    }
     R = R + continue_path_d(C, L, h, m, dir0, seed, false);
     if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
     return R;
@@ -2826,7 +2903,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (m.type == VT_MAT_EMISSIVE) return primary_emission_d(C, L, h, m);
   const int limit = std::max(0, (int)C.p->max_depth - 1);
   D3 R{0, 0, 0};
-  if (C.p->sampling_mode != 3u) {
+  if (C.p->sampling_mode != 3u && !is_delta_d(C, m)) {  // no NEE at glass or mirrors (main.swift:7657)
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
     R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0, limit > 0,

@@ -101,6 +101,10 @@ typedef void (*vto_pbr_eval_fn)(const vto_pbr_material *m, const float *n, const
                                 const float *lambda, float *f_cos, float *pdf);
 typedef void (*vto_pbr_sample_fn)(const vto_pbr_material *m, const float *n, const float *wo, const float *rand,
                                   const float *lambda, float *dir, float *weight, float *pdf, int32_t *lobe);
+/* A thin film over an ideal mirror (spectral_thin_film_mirror): returns the film's presence and,
+ * where it is positive, the film-over-metal reflectance at three wavelengths. */
+typedef float (*vto_pbr_film_mirror_fn)(float cos_i, float weight, float thickness_um, float film_ior, const float *f0,
+                                        const float *lambda, float *reflectance);
 
 typedef struct vto_pt_inputs {
   const vt_face *faces;
@@ -124,8 +128,9 @@ typedef struct vto_pt_inputs {
    * the warped phase at each of the nbins bins. Needed when spectral. */
   const struct vto_uplift *uplift;
   const float *cos_phase;
-  /* OPENPBR slots (type 4): per slot 8 floats (roughness, metalness, IOR, diffuse roughness, thin-film
-   * weight, thickness in micrometres and IOR, 0), and the BSDF. */
+  /* Per-slot lobe parameters, read for OPENPBR, GLOSSY and DIELECTRIC slots (types 4, 1, 2): 8 floats
+   * (roughness, metalness, IOR, diffuse roughness, thin-film weight, thickness in micrometres and IOR,
+   * 0), and the BSDF (null parameters: GLOSSY slots are mirrors, DIELECTRIC slots have IOR 1.5). */
   const float *pbr_params;
   vto_pbr_eval_fn pbr_eval;
   vto_pbr_sample_fn pbr_sample;
@@ -138,6 +143,8 @@ typedef struct vto_pt_inputs {
   float env_rot;
   /* A prebuilt hierarchy over these faces (vto_bvh_import); null: the renderer builds its LBVH. */
   const vto_bvh *bvh;
+  /* The thin film over GLOSSY mirrors in spectral transport (null: none). */
+  vto_pbr_film_mirror_fn pbr_film_mirror;
 } vto_pt_inputs;
 
 /* Z++ sampler primitives (main.swift:122-305): `n` points of the O2m3 and 2D Sobol' sequences

@@ -271,7 +271,7 @@ class PtInputs(C.Structure):
                 ("uplift", C.c_void_p), ("cos_phase", C.c_void_p),
                 ("pbr_params", C.c_void_p), ("pbr_eval", C.c_void_p), ("pbr_sample", C.c_void_p),
                 ("environment", Environment), ("env_rgba", C.c_void_p), ("env_w", C.c_uint32), ("env_h", C.c_uint32),
-                ("env_rot", C.c_float), ("bvh", C.c_void_p)]
+                ("env_rot", C.c_float), ("bvh", C.c_void_p), ("pbr_film_mirror", C.c_void_p)]
 
 
 _SIGS["vto_render"] = (None, [C.POINTER(PtInputs), C.POINTER(FrameParams), _U32, _P, _I32])
@@ -306,8 +306,9 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
     inp = PtInputs(f.ctypes.data, f.shape[0], v.ctypes.data, v.shape[0], C.cast(mats, C.c_void_p), len(materials), q,
                    None, None, None, 0, 0, 0.0, None, 0, 0, None, None, None, None, None)
     keep = []
-    if any(int(m["type"]) == 4 for m in materials):
-        # OPENPBR slots: the reference's own BSDF (oracle/openpbr_ref).
+    if any(int(m["type"]) in (1, 2, 4) for m in materials):
+        # OPENPBR, GLOSSY and DIELECTRIC slots: their lobe parameters, and the reference's own BSDF
+        # and mirror film (oracle/openpbr_ref).
         from . import openpbr_ref
         ref = openpbr_ref.load()
         params = np.array([[float(m.get("roughness", 0.5)), float(m.get("metalness", 0.0)), float(m.get("ior", 1.5)),
@@ -318,6 +319,7 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         inp.pbr_params = params.ctypes.data
         inp.pbr_eval = C.cast(ref.ref_openpbr_eval, C.c_void_p).value
         inp.pbr_sample = C.cast(ref.ref_openpbr_sample, C.c_void_p).value
+        inp.pbr_film_mirror = C.cast(ref.ref_thin_film_mirror, C.c_void_p).value
     if light is None and environment is not None and float(environment.get("intensity", 0.0)) > 0.0:
         env = inp.environment
         env.intensity = float(environment["intensity"])

@@ -1,0 +1,106 @@
+"""Ideal glass and mirrors on the B200: the reference's DIELECTRIC and GLOSSY material types
+(sample_bsdf's delta branches, main.swift:3318-3352; is_delta, :3285-3287) and the bounce loop's rules
+for them (no scattering event spent, no NEE, emission weight 1 after an ideal bounce, roulette ceiling
+0.99; main.swift:7716-7823), against the FP64 oracle drawing the same numbers:
+
+* a Cornell box with a mirror tall box, a glass short box and a rough GLOSSY (OpenPBR metal) wall, in
+  RGB, in spectral transport with a thin film on the mirror, and with the Z++ sampler;
+* the wavefront integrator's images equal the megakernel's;
+* ReSTIR DI (sampling mode 0) renders the scene as the oracle does;
+* the radiance cache renders it in sampling mode 1 and refuses it in mode 0, whose cache-terminated
+  kernels are built without glass and mirrors.
+"""
+import numpy as np
+import pytest
+
+import metal_vibe_tracer_b200 as vt
+from metal_vibe_tracer_b200 import scenes, spectral_tables
+from metal_vibe_tracer_b200.nrc import RadianceCache
+
+pytestmark = pytest.mark.gpu
+
+
+def relmse(a, b):
+    return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
+
+
+def gpu_render(ctx, mesh, mats, light, params, spp, spectral, wavefront=False):
+    scene = vt.Scene(ctx, mesh, mats, light, spectral_tables.load() if spectral else None)
+    (scene.render_wavefront if wavefront else scene.render)(params, spp)
+    img, n = scene.readback()
+    scene.close()
+    assert n == spp and np.isfinite(img).all()
+    return img
+
+
+@pytest.mark.parametrize("spectral,sampler", [(False, 0), (True, 0), (False, 1)])
+def test_delta_cornell_matches_oracle(ctx, oracle, spectral, sampler):
+    faces, verts, mats, light, cam = scenes.cornell_delta(film=spectral)
+    tables = spectral_tables.load() if spectral else None
+    mesh = vt.Mesh(ctx, faces, verts)
+    gpu = gpu_render(ctx, mesh, mats, light, vt.make_params(cam, 96, 96, 8, 1, spectral, 1, sampler=sampler), 32, spectral)
+    mesh.close()
+    kw = dict(max_depth=8, spectral=tables, sampler=sampler)
+    ref = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, **kw)
+    other = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, first_sample=1001, **kw)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    # Glass and mirrors change the picture: with those slots Lambert the box's mean radiance moves by
+    # 3-11 % per channel, beyond the 1-1.5 % between independent sample sets.
+    lam = oracle.render(faces, verts, [dict(m, type=0) if m["type"] in (1, 2) else m for m in mats], light, cam,
+                        96, 96, 32, **kw)
+    assert np.abs(lam.reshape(-1, 3).mean(0) / rm - 1).max() > 0.06
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_delta_wavefront_equals_megakernel(ctx, spectral):
+    faces, verts, mats, light, cam = scenes.cornell_delta(film=spectral)
+    mesh = vt.Mesh(ctx, faces, verts)
+    params = vt.make_params(cam, 96, 64, 8, 1, spectral, 1)
+    mega = gpu_render(ctx, mesh, mats, light, params, 16, spectral)
+    wave = gpu_render(ctx, mesh, mats, light, params, 16, spectral, wavefront=True)
+    mesh.close()
+    same = np.all(np.abs(wave - mega) <= 1e-6 * np.maximum(np.abs(mega), 1e-3), axis=-1)
+    assert same.mean() >= 0.99, same.mean()
+    gm, wm = mega.reshape(-1, 3).mean(0), wave.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(wm / gm - 1) < 2e-3), (wm, gm)
+
+
+def test_delta_restir_matches_oracle(ctx, oracle):
+    faces, verts, mats, light, cam = scenes.cornell_delta()
+    mesh = vt.Mesh(ctx, faces, verts)
+    gpu = gpu_render(ctx, mesh, mats, light, vt.make_params(cam, 64, 64, 8, 1, False, 0), 32, False)
+    mesh.close()
+    ref = oracle.render(faces, verts, mats, light, cam, 64, 64, 32, max_depth=8, mode=0)
+    other = oracle.render(faces, verts, mats, light, cam, 64, 64, 32, max_depth=8, mode=0, first_sample=5001)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+
+
+def test_cache_takes_delta_scenes_in_mode_1_only(ctx):
+    faces, verts, mats, light, cam = scenes.cornell_delta(film=True)
+    mesh = vt.Mesh(ctx, faces, verts)
+    scene = vt.Scene(ctx, mesh, mats, light, spectral_tables.load())
+    info = mesh.info()
+    cache = RadianceCache(ctx, list(info.lo), list(info.hi), train_records=4096, seed=3, spectral=1)
+    for f in range(4):
+        cache.render(scene, vt.make_params(cam, 32, 32, 8, 1 + 4 * f, True, 1), 4)
+    img, n = scene.readback()
+    assert n == 16 and np.isfinite(img).all() and img.mean() > 0.0
+    with pytest.raises(vt.MaterialLibraryError, match="glass or mirror"):
+        cache.render(scene, vt.make_params(cam, 32, 32, 8, 101, True, 0), 1)
+    cache.close()
+    scene.close()
+    mesh.close()
+
+
+def test_unknown_material_type_is_rejected(ctx):
+    faces, verts, mats, light, cam = scenes.cornell_delta()
+    mesh = vt.Mesh(ctx, faces, verts)
+    bad = [dict(m) for m in mats]
+    bad[2]["type"] = 7
+    with pytest.raises(vt.MaterialLibraryError, match="unknown type"):
+        vt.Scene(ctx, mesh, bad, light)
+    mesh.close()

@@ -9,9 +9,9 @@ on the B200 against the integrator's device functions and its traversal.
   turned toward the ray, points along -x; a ray parallel to the box outside misses. The reference
   checks its analytic box primitive; the configs trace triangles, so the same rays are traced
   against a triangulated box.
-* the scattering budget max(0, depth - 1) (scattering_limit, main.swift:3471-3473).
-
-Glass total internal reflection (results[4]) needs the delta dielectric, which this build does not have.
+* the scattering budget max(0, depth - 1) (scattering_limit, main.swift:3471-3473);
+* results[4]: glass (IOR 1.52) met from inside beyond the critical angle reflects totally: the sample
+  exists, goes back to z < 0 and weighs exactly 1 (sample_delta, the delta dielectric).
 """
 import numpy as np
 import pytest
@@ -31,6 +31,9 @@ def test_device_known_answers(ctx):
     assert k[5] > 1e-4, "the grazing cosine sample must stay above the tangent plane"
     assert 0.0 <= k[6] and k[7] < 1.0
     assert list(k[8:11]) == [0.0, 0.0, 7.0]
+    # Glass, IOR 1.52, met from inside beyond the critical angle (GPUChecks.swift:32-34): the sample
+    # exists, reflects to z < 0 and weighs exactly 1.
+    assert k[11] == 1.0 and k[12] < 0.0 and list(k[13:16]) == [1.0, 1.0, 1.0]
 
 
 def _box(lo, hi):
