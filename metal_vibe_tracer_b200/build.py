@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import shutil
 import subprocess
+import time
 import sys
 from pathlib import Path
 
@@ -44,6 +45,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         raise RuntimeError(f"no CUDA sources under {CSRC}")
     newest_header = max((h.stat().st_mtime for h in _headers()), default=0.0)
     objs = []
+    compiled = False
     for src in sources:
         obj = OBJ / (src.stem + ".o")
         objs.append(obj)
@@ -53,12 +55,17 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *(extra or []), "-I", str(INCLUDE), "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
+        started = time.time()
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stdout}\n{res.stderr}")
+        # The object carries the time its compile began, so a source or header edited while it
+        # compiled stays newer and is compiled again next time.
+        os.utime(obj, (started, started))
+        compiled = True
         if verbose and (res.stdout or res.stderr):
             print(res.stdout + res.stderr, file=sys.stderr)
-    if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
+    if force or compiled or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "--cudart", "static", "-o", str(tmp), *map(str, objs)]
         res = subprocess.run(cmd, capture_output=True, text=True)
