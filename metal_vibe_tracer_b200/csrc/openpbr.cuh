@@ -325,24 +325,30 @@ static __device__ void pbr_thin_film(float ci, float eExt, float eFilm, float eB
   const float scale = (eFilm * ct) / (eExt * fmaxf(ci, kPbrMinDenom));
   const float2 t21 = make_float2(t12.x * scale, t12.y * scale);
   const float opd = 2.0f * eFilm * nm * ct;
-  const float3 dphi = pf3(2.0f * kPbrPi * opd / lambda.x, 2.0f * kPbrPi * opd / lambda.y, 2.0f * kPbrPi * opd / lambda.z);
-  if (diel) {
-    PbrCx rs, rp;
-    pbr_fresnel_amp_cx(ct, eFilm, cx(eBase, 0.0f), rs, rp);
-    rd = pf3(pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.x), pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.y),
-             pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi.z));
-  }
-  if (metal) {
-    const float f[3] = {f0.x, f0.y, f0.z}, d[3] = {dphi.x, dphi.y, dphi.z};
-    float out[3];
+  // A preparation at one wavelength with a grey base (the spectral lane-3 preparation) has three equal
+  // channels: the first is computed and copied.
+  const bool mono = lambda.x == lambda.y && lambda.x == lambda.z && (!metal || (f0.x == f0.y && f0.x == f0.z));
+  const float lam[3] = {lambda.x, lambda.y, lambda.z}, f[3] = {f0.x, f0.y, f0.z};
+  PbrCx ds = cx(0.0f, 0.0f), dp = cx(0.0f, 0.0f);
+  if (diel) pbr_fresnel_amp_cx(ct, eFilm, cx(eBase, 0.0f), ds, dp);
+  float od[3] = {0.0f, 0.0f, 0.0f}, om[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
+  for (int c = 0; c < 3; ++c) {
+    if (c > 0 && mono) {
+      od[c] = od[0];
+      om[c] = om[0];
+      continue;
+    }
+    const float dphi = 2.0f * kPbrPi * opd / lam[c];
+    if (diel) od[c] = pbr_airy_sp(r12, t12, r21, t21, ds, dp, dphi);
+    if (metal) {
       PbrCx rs, rp;
       pbr_fresnel_amp_cx(ct, eFilm, pbr_gulbrandsen(f[c], 1.0f), rs, rp);
-      out[c] = pbr_airy_sp(r12, t12, r21, t21, rs, rp, d[c]);
+      om[c] = pbr_airy_sp(r12, t12, r21, t21, rs, rp, dphi);
     }
-    rm = pf3(out[0], out[1], out[2]);
   }
+  if (diel) rd = pf3(od[0], od[1], od[2]);
+  if (metal) rm = pf3(om[0], om[1], om[2]);
 }
 // openpbr_thin_film_presence_multiplier: smoothstep from 1e-9 to 30 nm.
 __device__ __forceinline__ float pbr_thin_film_presence(float weight, float nm) {

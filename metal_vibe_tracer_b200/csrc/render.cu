@@ -3272,7 +3272,7 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
   const uint32_t every = std::max(1u, run.compactEvery);
   W.deadFlags = every > 1u ? 1u : 0u;
   const int block = std::max(32, std::min(run.block, kWfBlock));
-  const bool pbr = A.layered != 0u;
+  const bool pbr = A.layered != 0u, unbounded = scene_has_delta(scene);
   const uint32_t gridMax = (uint32_t)ctx->sm_count * (8u * kWfBlock / (uint32_t)block);
   uint32_t *slot = vt_queue_slot(ctx);
   for (uint32_t k0 = 0; k0 < spp; k0 += chunk) {
@@ -3282,8 +3282,20 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
     const uint32_t grid = std::min<uint32_t>((P + block - 1) / block, gridMax);
     k_wf_generate<<<grid, block, 0, s>>>(A, W);
     VT_CUDA(ctx, cudaGetLastError());
-    for (uint32_t b = 0; b <= A.maxDepth; ++b) {
-      W.compact = ((b + 1u) % every == 0u || b == A.maxDepth) ? 1u : 0u;
+    for (uint32_t b = 0;; ++b) {
+      if (b > A.maxDepth) {
+        // Ideal reflections and refractions spend no scattering event, so paths through glass and
+        // mirrors can outlive the depth (Russian roulette ends them): bounce on while a path lives,
+        // its count read back every 8 bounces (compacted queues from the depth on).
+        if (!unbounded) break;
+        if ((b - A.maxDepth - 1u) % 8u == 0u) {
+          uint32_t live = 0;
+          VT_CUDA(ctx, cudaMemcpyAsync(&live, counts + (b & 1u), sizeof live, cudaMemcpyDeviceToHost, s));
+          VT_CUDA(ctx, cudaStreamSynchronize(s));
+          if (live == 0u) break;
+        }
+      }
+      W.compact = ((b + 1u) % every == 0u || b >= A.maxDepth) ? 1u : 0u;
       // Live queue of bounce b (all paths at b = 0), the next bounce's queue and the shadow queue.
       const uint32_t *inQ = b == 0 ? nullptr : q[b & 1u];
       const uint32_t *inCount = b == 0 ? nullptr : counts + (b & 1u);

@@ -9,6 +9,11 @@ for them (no scattering event spent, no NEE, emission weight 1 after an ideal bo
 * ReSTIR DI (sampling mode 0) renders the scene as the oracle does;
 * the radiance cache renders it in sampling mode 1 and refuses it in mode 0, whose cache-terminated
   kernels are built without glass and mirrors.
+
+The GPU draws the oracle's numbers, so nearly every pixel agrees to 1e-3. Refraction in float and in
+double can still part at a total-internal-reflection or Fresnel threshold, and a path that then reaches
+the light through the glass carries a caustic firefly worth a few percent of the image mean. So means
+and relMSE are compared over the pixels outside the 0.5 % that differ most.
 """
 import numpy as np
 import pytest
@@ -22,6 +27,17 @@ pytestmark = pytest.mark.gpu
 
 def relmse(a, b):
     return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
+
+
+def assert_agrees(gpu, ref, other, frac=0.97, mean_tol=5e-3):
+    """gpu and ref drew the same numbers, other independent ones."""
+    d = np.abs(gpu - ref).sum(-1)
+    rel = d / (ref.sum(-1) + 1e-3)
+    assert (rel < 1e-3).mean() >= frac, (rel < 1e-3).mean()
+    keep = d <= np.quantile(d, 0.995)
+    gm, rm = gpu[keep].mean(0), ref[keep].mean(0)
+    assert np.all(np.abs(gm / rm - 1) < mean_tol), (gm, rm)
+    assert relmse(gpu[keep], ref[keep]) < 0.25 * relmse(other[keep], ref[keep])
 
 
 def gpu_render(ctx, mesh, mats, light, params, spp, spectral, wavefront=False):
@@ -43,13 +59,12 @@ def test_delta_cornell_matches_oracle(ctx, oracle, spectral, sampler):
     kw = dict(max_depth=8, spectral=tables, sampler=sampler)
     ref = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, **kw)
     other = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, first_sample=1001, **kw)
-    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
-    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
-    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    assert_agrees(gpu, ref, other)
     # Glass and mirrors change the picture: with those slots Lambert the box's mean radiance moves by
     # 3-11 % per channel, beyond the 1-1.5 % between independent sample sets.
     lam = oracle.render(faces, verts, [dict(m, type=0) if m["type"] in (1, 2) else m for m in mats], light, cam,
                         96, 96, 32, **kw)
+    rm = ref.reshape(-1, 3).mean(0)
     assert np.abs(lam.reshape(-1, 3).mean(0) / rm - 1).max() > 0.06
 
 
@@ -61,6 +76,7 @@ def test_delta_wavefront_equals_megakernel(ctx, spectral):
     mega = gpu_render(ctx, mesh, mats, light, params, 16, spectral)
     wave = gpu_render(ctx, mesh, mats, light, params, 16, spectral, wavefront=True)
     mesh.close()
+    # Both run the same float arithmetic on the same numbers: the same paths, summed in another order.
     same = np.all(np.abs(wave - mega) <= 1e-6 * np.maximum(np.abs(mega), 1e-3), axis=-1)
     assert same.mean() >= 0.99, same.mean()
     gm, wm = mega.reshape(-1, 3).mean(0), wave.reshape(-1, 3).mean(0)
@@ -74,9 +90,8 @@ def test_delta_restir_matches_oracle(ctx, oracle):
     mesh.close()
     ref = oracle.render(faces, verts, mats, light, cam, 64, 64, 32, max_depth=8, mode=0)
     other = oracle.render(faces, verts, mats, light, cam, 64, 64, 32, max_depth=8, mode=0, first_sample=5001)
-    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
-    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
-    assert relmse(gpu, ref) < relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    # Reservoirs pass samples between pixels, so a parted path moves its neighbours too.
+    assert_agrees(gpu, ref, other, frac=0.9)
 
 
 def test_cache_takes_delta_scenes_in_mode_1_only(ctx):
