@@ -394,8 +394,11 @@ __device__ __forceinline__ float3 pbr_spec_coeff(const PbrPrepared &p, float c) 
   return pf3(standard.x * (1.0f - t) + film.x * t, standard.y * (1.0f - t) + film.y * t, standard.z * (1.0f - t) + film.z * t);
 }
 
-// openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit).
-__device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const PbrTables &T, float3 n, float3 wo) {
+// openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit). Without
+// `weights` the lobe-selection weights (which only pbr_pdf and pbr_sample read) are left at zero: a
+// preparation that is only evaluated skips the specular coefficient at the view.
+__device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const PbrTables &T, float3 n, float3 wo,
+                                                   bool weights = true) {
   PbrPrepared p;
   p.wo = wo;
   p.B = pbr_basis(n);
@@ -433,6 +436,10 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
     p.diffComp = num / fmaxf(den, 1e-12f);
   }
   // Lobe weights (estimated contributions with a white throughput).
+  if (!weights) {
+    p.wSpec = p.wMetal = p.wDiff = p.total = 0.0f;
+    return p;
+  }
   p.wSpec = pmax3(pbr_spec_coeff(p, idotn));
   p.wMetal = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pmax3(p.metalScale) * p.metalEc;
   p.wDiff = pmax3(pscale(p.diffAlbedo, p.diffComp));

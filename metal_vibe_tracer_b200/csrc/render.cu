@@ -969,7 +969,8 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   float f3w = fa.x;
   if (A.spectral && (rho.w != rho.x || film)) {
     const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
-    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo);
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo,
+                                      false);
     f3w = pbr_eval(b, A.pbrT, wi).x;
   }
   return make_float4(fa.x / cosine, fa.y / cosine, fa.z / cosine, A.spectral ? f3w / cosine : 0.0f);
@@ -988,7 +989,8 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   float w3 = w.x;
   if (A.spectral && (rho.w != rho.x || film)) {
     const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
-    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo);
+    const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo,
+                                      false);
     w3 = pbr_eval(b, A.pbrT, dir).x / pdf;
   }
   weight = make_float4(w.x, w.y, w.z, A.spectral ? w3 : 0.0f);
