@@ -275,8 +275,22 @@ def cornell_delta(seed: int = 0, film: bool = False):
     """The coloured Cornell box with ideal glass and mirrors (the reference's DIELECTRIC and GLOSSY
     types): a mirror tall box (GLOSSY, roughness 0, F0 (0.95, 0.9, 0.8); with `film` a 0.45 um film
     of IOR 1.5 on it), a glass short box (DIELECTRIC, IOR 1.5, tint (0.98, 0.95, 0.9)) and a rough
-    GLOSSY red wall (roughness 0.3, the OpenPBR metal); the rest stays Lambert."""
+    GLOSSY red wall (roughness 0.3, the OpenPBR metal); the rest stays Lambert. Glass needs a closed
+    volume: the boxes are wound outward (their `front` side is the outside), and the glass box stands
+    0.02 above the floor, so that no ray leaving it meets the floor and its bottom at the same
+    distance."""
     faces, verts, materials, light, camera = cornell_coloured(seed=seed)
+    p = verts["p"].astype(np.float64)
+    for tag in (5, 6):
+        sel = np.nonzero(faces["tag"] == tag)[0]
+        centre = p[np.concatenate([faces["a"][sel], faces["b"][sel], faces["c"][sel]])].mean(0)
+        for k in sel:
+            a, b, c = p[faces["a"][k]], p[faces["b"][k]], p[faces["c"][k]]
+            if np.dot(np.cross(b - a, c - a), (a + b + c) / 3.0 - centre) < 0.0:
+                faces["b"][k], faces["c"][k] = faces["c"][k], faces["b"][k]
+    glass = np.unique(np.concatenate([faces["a"][faces["tag"] == 6], faces["b"][faces["tag"] == 6],
+                                      faces["c"][faces["tag"] == 6]]))
+    verts["p"][glass, 1] += np.float32(0.02)
     materials[3] = {"type": 1, "albedo": (0.63, 0.065, 0.05), "emission": (0.0, 0.0, 0.0), "roughness": 0.3, "ior": 1.5}
     materials[5] = {"type": 1, "albedo": (0.95, 0.9, 0.8), "emission": (0.0, 0.0, 0.0), "roughness": 0.0, "ior": 1.5}
     if film:
