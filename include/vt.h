@@ -452,12 +452,13 @@ vt_status vt_openpbr_energy_table(vt_ctx *ctx, float *table, float *average);
 
 /* One BSDF query: an OPENPBR material's parameters as the adapter reads them (roughness and IOR are
  * clamped to >= 0.03 and >= 1.01 inside), a unit shading normal, the view (outward) and light
- * directions, and three random numbers for a sample. 80 bytes. */
+ * directions, and three random numbers for a sample. 108 bytes. */
 typedef struct vt_openpbr_case {
   float base_color[3], metalness, roughness, ior, specular_weight, diffuse_roughness;
   float normal[3], view[3], light[3], rand[3];
   float thin_film_weight, thin_film_thickness /* micrometres */, thin_film_ior;
   float lambda[3];      /* the preparation's wavelengths in nm; 0: the upstream RGB wavelengths */
+  float coat;           /* coat weight */
 } vt_openpbr_case;
 /* f |cos| at the light direction and its pdf; the sample: direction, weight f |cos| / pdf, its pdf,
  * and 1 when a sample was produced. 48 bytes. */
@@ -476,7 +477,9 @@ typedef struct vt_openpbr_params {
   float roughness, metalness, ior, diffuse_roughness;
   /* Thin-film iridescence (SpectralMaterial, main.swift:730-735; spectral transport only, as the
    * reference's adapter): weight in [0, 1], thickness in micrometres, IOR. */
-  float thin_film_weight, thin_film_thickness, thin_film_ior, pad;
+  float thin_film_weight, thin_film_thickness, thin_film_ior;
+  /* Coat weight in [0, 1] (main.swift:2494; the adapter's coat: roughness 0.12, IOR 1.6, white). */
+  float coat;
 } vt_openpbr_params;
 vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n);
 

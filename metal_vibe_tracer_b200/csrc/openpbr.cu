@@ -49,6 +49,7 @@ struct CaseDev {
   float base[3], metal, rough, ior, sw, diffRough;
   float n[3], wo[3], wi[3], rand[3];
   float tfWeight, tfThickness, tfIor, lambda[3];
+  float coat;
 };
 struct ResultDev {
   float fcos[3], pdf, dir[3], weight[3], spdf, ok;
@@ -69,6 +70,7 @@ __device__ __forceinline__ PbrParams case_params(const CaseDev &c) {
   P.tfIor = c.tfIor;
   // The upstream RGB wavelengths unless the case gives its own (openpbr_bsdf.h: OpenPBR_BaseRgbWavelengths_nm).
   P.lambda = c.lambda[0] > 0.0f ? pf3(c.lambda[0], c.lambda[1], c.lambda[2]) : pf3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
+  P.coat = c.coat;
   return P;
 }
 

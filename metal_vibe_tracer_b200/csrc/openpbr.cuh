@@ -2,7 +2,7 @@
 // Derivative work of the Adobe OpenPBR BSDF (https://github.com/adobe/openpbr-bsdf, c91aad1d),
 // Copyright 2026 Adobe, licensed under the Apache License, Version 2.0 (LICENSES/Apache-2.0.txt,
 // http://www.apache.org/licenses/LICENSE-2.0); modified as described below and in NOTICE.
-// openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials: a GGX (VNDF-sampled)
+// openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials under an optional coat: a GGX (VNDF-sampled)
 // specular lobe with dielectric Fresnel on the dielectric part and F82-tinted Schlick on the metal
 // part, the metal's microfacet multiple-scattering lobe, and the energy-conserving (EON) diffuse
 // base, combined as one aggregate with lobe selection by estimated contribution.
@@ -20,14 +20,17 @@
 // reference substitutes it (scripts/prepare_shaders.py:28-39).
 //
 // What the restatement covers: specular_weight, base_color, base_metalness, specular_roughness,
-// specular_ior, base_diffuse_roughness, and thin-film iridescence (thin_film_weight, _thickness,
-// _ior, at the preparation's three wavelengths; impl/openpbr_thin_film_iridescence_utils.h and
-// openpbr_reflection_coefficient, impl/openpbr_reflection_transmission_coefficient.h:55-125), with
-// coat, fuzz, transmission, subsurface, anisotropy and dispersion at zero. In that case the upstream coat and fuzz layers pass the base
-// through (presence 0), the dielectric multiple-scattering lobe and both thin-wall lobes have zero
-// weight and value, and specular transmission has zero probability; the code below keeps only what
-// is left, in the upstream operation order. The coat and fuzz layers' recomputation of the sample
-// weight (w pdf / pdf, twice) is kept for the same rounding.
+// specular_ior, base_diffuse_roughness, thin-film iridescence (thin_film_weight, _thickness, _ior, at
+// the preparation's three wavelengths; impl/openpbr_thin_film_iridescence_utils.h and
+// openpbr_reflection_coefficient, impl/openpbr_reflection_transmission_coefficient.h:55-125), and the
+// coat as the reference's adapter sets it (coat_weight; coat_roughness 0.12, coat_ior 1.6, white
+// coat_color, coat_darkening 1; impl/openpbr_coating_lobe.h and the coat's IOR, roughness and
+// darkening terms of openpbr_prepare_lobes), with fuzz, transmission, subsurface, anisotropy and
+// dispersion at zero. In that case the upstream fuzz layer passes the coated base through
+// (presence 0), the dielectric multiple-scattering lobe and both thin-wall lobes have zero weight and
+// value, and specular transmission has zero probability; the code below keeps only what is left, in
+// the upstream operation order. The fuzz layer's recomputation of the sample weight (w pdf / pdf) is
+// kept for the same rounding.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -55,7 +58,13 @@ struct PbrParams {
   float metal, rough, ior, sw, diffRough;
   float tfWeight, tfThickness, tfIor;  // thin film: weight, thickness (micrometres), IOR
   float3 lambda;                       // the preparation's three wavelengths (nm)
+  float coat;                          // coat weight (roughness 0.12, IOR 1.6, white, darkening 1)
 };
+// The reference adapter's coat for materials without a MaterialX graph (prepare_openpbr,
+// main.swift:2494-2495: coat_roughness 0.12) and the upstream default coat IOR
+// (openpbr_make_default_resolved_inputs: coat_ior 1.6).
+constexpr float kPbrCoatRoughness = 0.12f;
+constexpr float kPbrCoatIor = 1.6f;
 
 struct PbrTables {
   const float *metalE;     // 129 x 129
@@ -374,6 +383,14 @@ struct PbrPrepared {
   // film, the wavelengths.
   float tfPresence, tfNm, tfExt, tfIor, tfInt;
   float3 lambda;
+  // Coat (the coating lobe): presence, hit from inside (then only the base counts), relative IOR,
+  // alpha (isotropic and clamped), the share reflected at the view, the base's scale under it
+  // (transmission at the view times the darkening), and the probability of sampling the coat.
+  float coat;
+  bool inside;
+  float coatEta, coatAlpha, coatAx, inRefl;
+  float3 inScale;
+  float coatProb;
 };
 
 // Reflection coefficient of the specular lobe at cos c to the half vector (openpbr_reflection_coefficient):
@@ -394,6 +411,21 @@ __device__ __forceinline__ float3 pbr_spec_coeff(const PbrPrepared &p, float c) 
   return pf3(standard.x * (1.0f - t) + film.x * t, standard.y * (1.0f - t) + film.y * t, standard.z * (1.0f - t) + film.z * t);
 }
 
+// openpbr_average_fresnel: the fitted hemispherical average of the dielectric Fresnel reflectance.
+__device__ __forceinline__ float pbr_average_fresnel(float eta) {
+  if (eta > 1.0f) return (eta - 1.0f) / (4.08567f + 1.00071f * eta);
+  return 0.997118f + 0.1014f * eta - 0.965241f * (eta * eta) - 0.130607f * (eta * eta) * eta;
+}
+__device__ __forceinline__ float pbr_fourth_root(float x) { return sqrtf(sqrtf(x)); }
+__device__ __forceinline__ float pbr_fourth_power(float x) {
+  const float xx = x * x;
+  return xx * xx;
+}
+// openpbr_compute_dielectric_energy_reflected: the share of light a rough dielectric interface reflects.
+__device__ __forceinline__ float pbr_dielectric_energy_reflected(const PbrTables &T, float eta, float alpha, float c) {
+  return alpha == 0.0f ? pbr_fresnel(eta, c) : 1.0f - pbr_opaque_energy(T, eta, alpha, c);
+}
+
 // openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit). Without
 // `weights` the lobe-selection weights (which only pbr_pdf and pbr_sample read) are left at zero: a
 // preparation that is only evaluated skips the specular coefficient at the view.
@@ -408,9 +440,29 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
     p.B.b = pscale(p.B.b, -1.0f);
     p.B.n = pscale(p.B.n, -1.0f);
   }
-  const float wior = 1.0f * pbr_weighted_ior(P.ior / 1.0f, P.sw);
-  p.etaOpaque = back ? wior / 1.0f : wior / 1.0f;
-  p.alpha = psq(P.rough);
+  // IORs (openpbr_bsdf.h:339-409): entering a coated surface, the base sits under the coat (its
+  // relative IOR inverted where that avoids nonphysical total internal reflection); from inside the
+  // coat is ignored.
+  const bool enterCoat = P.coat > 0.0f && !back;
+  const float wcoat = enterCoat ? pmix(1.0f, kPbrCoatIor, P.coat) : 1.0f;
+  const float wior = wcoat * pbr_weighted_ior(P.ior / wcoat, P.sw);
+  float relCoat = 1.0f;
+  if (back) {
+    p.etaOpaque = wior / 1.0f;
+  } else if (enterCoat) {
+    p.etaOpaque = wcoat > wior && wior >= 1.0f ? wcoat / wior : wior / wcoat;
+    relCoat = kPbrCoatIor / 1.0f;
+  } else {
+    p.etaOpaque = wior / 1.0f;
+  }
+  // Roughnesses (openpbr_bsdf.h:424-460): no fuzz, so the coat keeps its roughness; the coat
+  // roughens the base by its presence, the less the closer its IOR is to the exterior's.
+  const float coatRough = kPbrCoatRoughness;
+  const float adjust = pmix(1.0f, 0.0f, relCoat >= 1.0f ? 1.0f / relCoat : relCoat);
+  const float rough = P.coat > 0.0f
+                          ? pmix(P.rough, pbr_fourth_root(fminf(1.0f, pbr_fourth_power(P.rough) + adjust * pbr_fourth_power(coatRough))), P.coat)
+                          : P.rough;
+  p.alpha = psq(rough);
   p.ax = fmaxf(p.alpha, 1e-6f);
   const float dielectric = 1.0f - P.metal;
   p.scaleOpaque = 1.0f * 1.0f * dielectric;
@@ -426,14 +478,40 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
   // medium (1) and the weighted specular IOR; from inside the two swap.
   p.tfNm = P.tfThickness * 1000.0f;
   p.tfPresence = pbr_thin_film_presence(P.tfWeight, p.tfNm);
-  p.tfExt = back ? wior : 1.0f;
-  p.tfInt = back ? 1.0f : wior;
+  p.tfExt = back ? wior : wcoat;
+  p.tfInt = back ? wcoat : wior;
   p.tfIor = P.tfIor;
   p.lambda = P.lambda;
   {
     const float num = pbr_opaque_energy(T, p.etaOpaque, p.alpha, idotn);
     const float den = pbr_opaque_average(T, p.etaOpaque, p.alpha);
     p.diffComp = num / fmaxf(den, 1e-12f);
+  }
+  // The coating lobe (impl/openpbr_coating_lobe.h, white coat colour: no tint on passage). The base
+  // under a coat is darkened by its internal reflections (openpbr_bsdf.h:512-552): K from the coat's
+  // average Fresnel inside and out, blended by the base's effective roughness, and the base albedo
+  // E_b from its metal and opaque-dielectric parts.
+  p.coat = P.coat;
+  p.inside = back;
+  p.coatEta = relCoat;
+  p.coatAlpha = psq(coatRough);
+  p.coatAx = fmaxf(p.coatAlpha, 1e-6f);
+  p.inRefl = 0.0f;
+  p.inScale = pf3(1.0f, 1.0f, 1.0f);
+  p.coatProb = 0.0f;
+  if (P.coat > 0.0f) {
+    const float Ks = pbr_average_fresnel(relCoat);
+    const float Kr = 1.0f - (1.0f - pbr_average_fresnel(relCoat)) / psq(relCoat);
+    const float specOpaque = pbr_average_fresnel(p.etaOpaque);
+    const float specBase = dielectric * specOpaque + P.metal;
+    const float K = pmix(Ks, Kr, pmix(1.0f, rough, specBase));
+    const float3 Eb = padd(pscale(maf, p.metalAmount),
+                           pscale(pf3(pmix(p.f0.x, 1.0f, specOpaque), pmix(p.f0.y, 1.0f, specOpaque), pmix(p.f0.z, 1.0f, specOpaque)),
+                                  dielectric));
+    const float3 delta = pf3((1.0f - K) / (1.0f - Eb.x * K), (1.0f - K) / (1.0f - Eb.y * K), (1.0f - K) / (1.0f - Eb.z * K));
+    const float3 darkening = pf3(pmix(1.0f, delta.x, P.coat), pmix(1.0f, delta.y, P.coat), pmix(1.0f, delta.z, P.coat));
+    p.inRefl = idotn > 0.0f ? pbr_dielectric_energy_reflected(T, relCoat, p.coatAlpha, idotn) * P.coat : 0.0f;
+    p.inScale = pscale(darkening, 1.0f - p.inRefl);
   }
   // Lobe weights (estimated contributions with a white throughput).
   if (!weights) {
@@ -444,6 +522,8 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
   p.wMetal = p.alpha < kPbrMinAlphaEnergyLoss ? 0.0f : pmax3(p.metalScale) * p.metalEc;
   p.wDiff = pmax3(pscale(p.diffAlbedo, p.diffComp));
   p.total = ((((p.wSpec + 0.0f) + p.wMetal) + p.wDiff) + 0.0f) + 0.0f;
+  if (p.coat > 0.0f && !p.inside)
+    p.coatProb = psafe_div(p.inRefl, p.inRefl + p.total * pmax3(p.inScale), 0.5f);
   return p;
 }
 
@@ -569,20 +649,22 @@ __device__ __forceinline__ bool pbr_diffuse_sample(const PbrPrepared &p, const P
 }
 
 // The aggregate: f |cos| and the lobe-weighted pdf.
-__device__ __forceinline__ float3 pbr_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+__device__ __forceinline__ float3 pbr_base_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
   float3 v = pbr_spec_value(p, wi);
   v = padd(v, pbr_metal_value(p, T, wi));
   v = padd(v, pbr_diffuse_value(p, T, wi));
   return v;
 }
-__device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, float3 wi) {
+__device__ __forceinline__ float pbr_base_pdf(const PbrPrepared &p, float3 wi) {
   float sum = p.wSpec * pbr_spec_pdf(p, wi);
   sum += p.wMetal * pbr_metal_pdf(p, wi);
   sum += p.wDiff * pbr_diffuse_pdf(p, wi);
   return p.total > 0.0f ? sum / p.total : 0.0f;
 }
-// One sample from three numbers: direction, weight f |cos| / pdf and pdf; false when none.
-__device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w, float &pdf) {
+// One sample of the base (the aggregate lobe) from three numbers: direction, weight f |cos| / pdf and
+// pdf; false when none.
+__device__ __forceinline__ bool pbr_base_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w,
+                                                float &pdf) {
   if (p.total <= kPbrFloatMin) return false;
   float rx = r.x * p.total;
   int lobe;
@@ -619,10 +701,100 @@ __device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables
   }
   q /= p.total;
   w = pscale(fc, 1.0f / q);
-  // The coat and fuzz layers (presence 0) recompute the weight from f |cos| and the pdf.
-  w = pscale(pscale(w, q), 1.0f / q);
-  w = pscale(pscale(w, q), 1.0f / q);
   pdf = q;
+  return true;
+}
+
+// The coat's reflection (the generic minimal microfacet lobe with the coat's dielectric Fresnel,
+// impl/openpbr_generic_minimal_microfacet_lobe.h): GGX of the coat's alpha about the same normal.
+__device__ __forceinline__ float3 pbr_coat_value(const PbrPrepared &p, float3 wi) {
+  const float idotn = pdot(p.B.n, p.wo), odotn = pdot(p.B.n, wi);
+  if (!(idotn * odotn > 0.0f)) return pf3(0.0f, 0.0f, 0.0f);
+  const float3 h = pnormalize(padd(p.wo, wi));
+  const float idoth = pdot(p.wo, h);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  const float other = 1.0f / (4.0f * idotn);
+  const float F = pbr_fresnel(p.coatEta, fabsf(idoth));
+  const float DoF = F * (D * other);
+  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx) * smith_g1(pbr_to_local(p.B, wi), p.coatAx);
+  return pf3(DoF * G, DoF * G, DoF * G);
+}
+__device__ __forceinline__ float pbr_coat_pdf(const PbrPrepared &p, float3 wi) {
+  const float idotn = pdot(p.B.n, p.wo), odotn = pdot(p.B.n, wi);
+  if (!(idotn * odotn > 0.0f)) return 0.0f;
+  const float3 h = pnormalize(padd(p.wo, wi));
+  const float idoth = pdot(p.wo, h), odoth = pdot(wi, h);
+  if (idoth * odoth < 0.0f) return 0.0f;
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  const float other = idoth / (4.0f * odoth * idotn);
+  return smith_g1(pbr_to_local(p.B, p.wo), p.coatAx) * (D * other);
+}
+__device__ __forceinline__ bool pbr_coat_sample(const PbrPrepared &p, float3 r, float3 &wi, float3 &w, float &pdf) {
+  const float idotn = pdot(p.wo, p.B.n);
+  const float3 h = pbr_to_world(p.B, ggx_sample_vndf(p.coatAx, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y)));
+  const float idoth = pdot(p.wo, h);
+  if (idoth < 0.0f) return false;
+  wi = pnormalize(padd(pscale(p.wo, -1.0f), pscale(h, 2.0f * idoth)));
+  const float odotn = pdot(p.B.n, wi);
+  if (idotn * odotn <= 0.0f) return false;
+  const float odoth = pdot(wi, h);
+  const float F = pbr_fresnel(p.coatEta, idoth);
+  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.coatAx);
+  w = pf3(F * Gs, F * Gs, F * Gs);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  if (D <= 0.0f) return false;
+  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx);
+  pdf = D * Gm * idoth / (4.0f * odoth * idotn);
+  return true;
+}
+
+// The coating layer over the base (impl/openpbr_coating_lobe.h) and the fuzz layer over it (weight 0:
+// it passes the coated base through). Outside: f = coat presence x coat reflection + base x the base's
+// scale at the view (no attenuation on the light's side, OPENPBR_RECIPROCAL_COAT_AND_FUZZ 0); the pdf
+// mixes the coat's and the base's by the coat's sampling probability. From inside only the base
+// counts (a white coat tints nothing). Without a coat the coat's terms vanish and are skipped.
+__device__ __forceinline__ float3 pbr_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  const float3 base = pbr_base_eval(p, T, wi);
+  if (p.inside || !(p.coat > 0.0f)) return base;
+  return padd(pscale(pbr_coat_value(p, wi), p.coat), pmul(base, p.inScale));
+}
+__device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, float3 wi) {
+  const float pb = pbr_base_pdf(p, wi);
+  if (p.inside || !(p.coat > 0.0f)) return pb;
+  return pmix(pb, pbr_coat_pdf(p, wi), p.coatProb);
+}
+// One sample from three numbers: direction, weight f |cos| / pdf and pdf; false when none. Outside,
+// the coat or the base is chosen by r.x against the coat's probability (r.x remapped), and the weight
+// recomputed from both layers' f |cos| and pdfs; the fuzz layer recomputes it once more.
+__device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w, float &pdf) {
+  if (p.inside) {
+    if (!pbr_base_sample(p, T, r, wi, w, pdf)) return false;
+  } else {
+    const float cp = p.coatProb;
+    if (r.x < cp) {
+      const float rx = pclamp_rand(r.x * (1.0f / cp));
+      float3 wc;
+      float pc;
+      if (!pbr_coat_sample(p, pf3(rx, r.y, r.z), wi, wc, pc)) return false;
+      const float3 fc = padd(pscale(pscale(wc, pc), p.coat), pmul(pbr_base_eval(p, T, wi), p.inScale));
+      pdf = pmix(pbr_base_pdf(p, wi), pc, cp);
+      w = pscale(fc, 1.0f / pdf);
+    } else {
+      const float rx = pclamp_rand((r.x - cp) * (1.0f / (1.0f - cp)));
+      float3 wb;
+      float pb;
+      if (!pbr_base_sample(p, T, pf3(rx, r.y, r.z), wi, wb, pb)) return false;
+      float3 fc = pscale(wb, pb);
+      pdf = pb;
+      if (p.coat > 0.0f) {
+        fc = padd(pscale(pbr_coat_value(p, wi), p.coat), pmul(fc, p.inScale));
+        pdf = pmix(pb, pbr_coat_pdf(p, wi), cp);
+      }
+      w = pscale(fc, 1.0f / pdf);
+    }
+  }
+  // The fuzz layer (presence 0) recomputes the weight from f |cos| and the pdf.
+  w = pscale(pscale(w, pdf), 1.0f / pdf);
   return true;
 }
 

@@ -896,11 +896,15 @@ __device__ __forceinline__ float4 slot_lobe(const RenderArgs &A, const vt_materi
   const uint32_t slot = __float_as_uint(m.pad);
   return A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot) : make_float4(0.0f, 0.0f, 1.5f, 0.0f);
 }
+// The slot's second float4: the thin film (weight, thickness in micrometres, IOR) and the coat weight.
+__device__ __forceinline__ float4 slot_extra(const RenderArgs &A, const vt_material &m) {
+  const uint32_t slot = __float_as_uint(m.pad);
+  return A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+}
 // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568, and
 // spectral_thin_film_mirror; the RGB adapter leaves it at zero).
 __device__ __forceinline__ float4 slot_film(const RenderArgs &A, const vt_material &m) {
-  const uint32_t slot = __float_as_uint(m.pad);
-  return A.spectral && A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+  return A.spectral ? slot_extra(A, m) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
 }
 // prepare_bsdf (main.swift:2547-2568): RGB transport evaluates the base colour's three channels; in
 // spectral transport `a` takes the reflectance at lanes 0-2 and `b` lane 3, skipped for a flat
@@ -916,10 +920,11 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
   P.ior = fmaxf(1.01f, q.z);
   P.sw = 1.0f;
   P.diffRough = q.w;
-  const float4 tf = slot_film(A, m);
-  P.tfWeight = tf.x;
-  P.tfThickness = tf.y;
-  P.tfIor = tf.z;
+  const float4 x = slot_extra(A, m);
+  P.tfWeight = A.spectral ? x.x : 0.0f;
+  P.tfThickness = A.spectral ? x.y : 0.0f;
+  P.tfIor = A.spectral ? x.z : 1.4f;
+  P.coat = x.w;  // in both transports (prepare_openpbr and prepare_openpbr_lanes, main.swift:2494, 2537)
   P.lambda = lambda;
   return P;
 }
@@ -3849,13 +3854,16 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
         !(p.diffuse_roughness >= 0.0f && p.diffuse_roughness <= 1.0f))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": roughness, metalness and diffuse roughness "
                                           "must lie in [0, 1] and the IOR be positive");
+    if (!(p.coat >= 0.0f && p.coat <= 1.0f))
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": coat weight must lie in [0, 1]");
     if (!(p.thin_film_weight >= 0.0f && p.thin_film_weight <= 1.0f) || !(p.thin_film_thickness >= 0.0f) ||
         !std::isfinite(p.thin_film_thickness) || (p.thin_film_weight > 0.0f && !(p.thin_film_ior > 0.0f)))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": thin-film weight must lie in [0, 1], its "
                                           "thickness be finite and non-negative and its IOR positive");
     q[2 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
     scene->slot_rough[i] = p.roughness;
-    q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f, 0.0f);
+    q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f,
+                                       p.coat);
   }
   if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, q.size() * sizeof(float4)));
   if (n) VT_CUDA(ctx, cudaMemcpy(scene->d_pbr, q.data(), q.size() * sizeof(float4), cudaMemcpyHostToDevice));

@@ -38,12 +38,14 @@ def load():
     return _lib
 
 
-def material(base, metalness, roughness, ior, type_=4, thin_film=None):
-    """A reference material; `thin_film` = (weight, thickness in micrometres, IOR) or None."""
+def material(base, metalness, roughness, ior, type_=4, thin_film=None, coat=0.0):
+    """A reference material; `thin_film` = (weight, thickness in micrometres, IOR) or None; `coat`:
+    the coat weight (the adapter's coat: roughness 0.12, default IOR and colour)."""
     m = Material()
     m.type = type_
     m.albedo[:] = [float(x) for x in base]
     m.roughness, m.metalness, m.ior = float(roughness), float(metalness), float(ior)
+    m.coat = float(coat)
     if thin_film is not None:
         m.thin_film_weight, m.thin_film_thickness, m.thin_film_ior = (float(x) for x in thin_film)
     return m

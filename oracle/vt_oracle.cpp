@@ -2285,6 +2285,7 @@ vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double
   q.roughness = pp[0];
   q.metalness = pp[1];
   q.ior = pp[2];
+  q.coat = pp[7];  // both transports (prepare_openpbr, main.swift:2494)
   // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568).
   if (C.spectral) {
     q.thin_film_weight = pp[4];

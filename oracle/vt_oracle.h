@@ -130,7 +130,7 @@ typedef struct vto_pt_inputs {
   const float *cos_phase;
   /* Per-slot lobe parameters, read for OPENPBR, GLOSSY and DIELECTRIC slots (types 4, 1, 2): 8 floats
    * (roughness, metalness, IOR, diffuse roughness, thin-film weight, thickness in micrometres and IOR,
-   * 0), and the BSDF (null parameters: GLOSSY slots are mirrors, DIELECTRIC slots have IOR 1.5). */
+   * coat weight), and the BSDF (null parameters: GLOSSY slots are mirrors, DIELECTRIC slots have IOR 1.5). */
   const float *pbr_params;
   vto_pbr_eval_fn pbr_eval;
   vto_pbr_sample_fn pbr_sample;

@@ -4,9 +4,10 @@ vendored headers compiled for the CPU) and the FP64 oracle path tracer.
 * the dense GGX energy table, solved on the device, equals Shaders/MetalEnergy.metal's values to
   float summation error;
 * the device BSDF (openpbr.cuh) gives the reference's f |cos|, pdf and samples for 600 seeded
-  opaque materials and directions, and for 300 with thin-film iridescence at given wavelengths;
+  opaque materials and directions, for 300 with thin-film iridescence at given wavelengths and for 300
+  under the adapter's coat;
 * a Cornell box with OPENPBR walls and boxes renders as the oracle does, in RGB and spectral
-  transport, and with thin films on two slots in spectral transport.
+  transport, with thin films on four slots in spectral transport, and with coats on three slots.
 """
 import json
 from pathlib import Path
@@ -32,13 +33,13 @@ def test_energy_table_matches_the_reference(ctx):
     assert t[0].max() == 0.0 and (t >= 0).all() and (t <= 1).all()
 
 
-@pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json"])
+@pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json", "openpbr_coat_cases.json"])
 def test_bsdf_matches_the_reference(ctx, fixture):
     R.openpbr_tables_set(ctx)
     cases = json.loads((GOLDEN / fixture).read_text())["cases"]
-    film = lambda c: c["thin_film"] + c["lambda"] if "thin_film" in c else []
+    extra = lambda c: (c["thin_film"] + c["lambda"] if "thin_film" in c else [0.0] * 6) + [c.get("coat", 0.0)]
     arr = np.array([c["base"] + [c["metalness"], c["roughness"], c["ior"], 1.0, 0.0] + c["normal"] + c["view"] + c["light"]
-                    + c["rand"] + film(c) for c in cases], np.float32)
+                    + c["rand"] + extra(c) for c in cases], np.float32)
     out = R.openpbr_evaluate(ctx, arr)
     fc = np.float32([c["f_cos"] for c in cases])
     pdf = np.float32([c["pdf"] for c in cases])
@@ -98,6 +99,32 @@ def test_thin_film_cornell_matches_oracle(ctx, oracle):
     assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
     assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
     # The films change the picture's mean well beyond the noise (by 6-22 % per channel).
+    bm = bare.reshape(-1, 3).mean(0)
+    assert np.abs(bm / rm - 1).max() > 0.03, (bm, rm)
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_coated_cornell_matches_oracle(ctx, oracle, spectral):
+    """Coats (weight 1 on the white wall and the metal box, 0.5 on the half-metal box) in RGB and
+    spectral transport."""
+    faces, verts, mats, light, cam = scenes.cornell_openpbr()
+    for k, w in ((2, 1.0), (5, 1.0), (6, 0.5)):
+        mats[k] = dict(mats[k], coat=w)
+    tables = spectral_tables.load() if spectral else None
+    mesh = vt.Mesh(ctx, faces, verts)
+    out = []
+    for m in (mats, [dict(x, coat=0.0) for x in mats]):
+        scene = vt.Scene(ctx, mesh, m, light, tables)
+        scene.render(vt.make_params(cam, 96, 96, 6, 1, spectral), 32)
+        out.append(scene.readback()[0])
+        scene.close()
+    mesh.close()
+    gpu, bare = out
+    ref = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, spectral=tables)
+    other = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, first_sample=1001, spectral=tables)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
     bm = bare.reshape(-1, 3).mean(0)
     assert np.abs(bm / rm - 1).max() > 0.03, (bm, rm)
 

@@ -44,6 +44,20 @@ def test_reference_thin_film_reproduces_the_fixtures():
 
 
 @needs_ref
+def test_reference_coat_reproduces_the_fixtures():
+    """The coated fixtures (tests/golden/openpbr_coat_cases.json): the adapter's coat (roughness 0.12,
+    IOR 1.6) at weights up to 1, some over a thin film, some seen from behind."""
+    cases = json.loads((GOLDEN / "openpbr_coat_cases.json").read_text())["cases"]
+    for c in cases[:150]:
+        film = c["thin_film"] if c["thin_film"][0] > 0.0 else None
+        m = R.material(c["base"], c["metalness"], c["roughness"], c["ior"], thin_film=film, coat=c["coat"])
+        f, pdf = R.evaluate(m, c["normal"], c["view"], c["light"], c["lambda"])
+        assert np.array_equal(f, np.float32(c["f_cos"])) and pdf == np.float32(c["pdf"])
+        d, w, spdf, lobe = R.sample(m, c["normal"], c["view"], c["rand"], c["lambda"])
+        assert np.array_equal(d, np.float32(c["dir"])) and spdf == np.float32(c["sample_pdf"]) and lobe == c["lobe"]
+
+
+@needs_ref
 def test_reference_thin_film_changes_the_answer():
     """A film of weight 1 changes f |cos| on most cases; weight 0 gives the film-free answer."""
     cases = json.loads((GOLDEN / "openpbr_thin_film_cases.json").read_text())["cases"]
