@@ -1887,6 +1887,7 @@ struct WfArgs {
   const uint32_t *inQ, *inCount;  // live paths of this bounce (null: paths 0 .. paths - 1)
   uint32_t *outQ, *outCount;      // live paths of the next bounce
   uint32_t *shQ, *shCount;        // shadow rays of this bounce
+  uint32_t *grpQ;                 // the live queue regrouped by material (k_wf_group)
   uint32_t npix, paths, k0;       // accumulation pixels; paths of the pass; its first sample (of the call)
   uint32_t compact;               // 1: this bounce compacts the live queue; 0: it keeps every entry in
                                   // place (ended paths flagged kWfDead, their next ray empty)
@@ -1926,6 +1927,48 @@ __device__ __forceinline__ void wf_push(bool push, uint32_t v, uint32_t *q, uint
   __syncthreads();
   if (push) q[sBase + w + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
   __syncthreads();  // sTotal and sBase are reused by the next push
+}
+
+// wf_push from the back: the block's entries go to n - 1 - (reserved rank) of queue q.
+__device__ __forceinline__ void wf_push_back(bool push, uint32_t v, uint32_t *q, uint32_t *count, uint32_t n, uint32_t &sTotal,
+                                             uint32_t &sBase) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned m = __ballot_sync(0xffffffffu, push);
+  if (threadIdx.x == 0) sTotal = 0;
+  __syncthreads();
+  uint32_t w = 0;
+  if (lane == 0 && m) w = atomicAdd(&sTotal, (uint32_t)__popc(m));
+  w = __shfl_sync(0xffffffffu, w, 0);
+  __syncthreads();
+  if (threadIdx.x == 0) sBase = sTotal ? atomicAdd(count, sTotal) : 0u;
+  __syncthreads();
+  if (push) q[n - 1u - (sBase + w + (uint32_t)__popc(m & ((1u << lane) - 1u)))] = v;
+  __syncthreads();
+}
+
+// Shading grouped by material: the live queue of a bounce regrouped so that paths whose hit has a
+// thin film (the costly iridescence evaluations of spectral transport) come after all others. With
+// a tenth of the slots filmed nearly every 32-path warp holds a film vertex; grouped, the shade
+// kernel's warps run one kind of vertex. Others fill W.grpQ from the front, film paths from the
+// back; counts[0] and counts[1] must be zero on entry.
+__global__ void __launch_bounds__(kWfBlock) k_wf_group(RenderArgs A, WfArgs W, uint32_t *counts) {
+  __shared__ uint32_t sTotal, sBase;
+  const uint32_t n = W.inCount ? min(*W.inCount, W.paths) : W.paths;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t q = base + threadIdx.x;
+    uint32_t i = 0;
+    bool film = false;
+    if (q < n) {
+      i = W.inQ ? W.inQ[q] : q;
+      const int pos = W.hit[i].w;
+      if (pos >= 0 && (uint32_t)pos < A.faceCount && !(W.deadFlags && (W.meta[i].w & kWfDead))) {
+        const uint32_t slot = __float_as_uint(__ldg(A.tris + 3 * (size_t)pos + 1).w);
+        film = slot < A.nmat && pbr_thin_film_slot(A, material(A, slot));
+      }
+    }
+    wf_push(q < n && !film, i, W.grpQ, counts, sTotal, sBase);
+    wf_push_back(q < n && film, i, W.grpQ, counts + 1, n, sTotal, sBase);
+  }
 }
 
 // The NEE of one vertex up to its visibility: the sample (the draws of direct_light_lanes), its
@@ -3182,6 +3225,7 @@ size_t wf_carve(unsigned char *base, uint32_t cap, WfArgs &W, uint32_t **q0, uin
   *q0 = reinterpret_cast<uint32_t *>(take(4 * n));
   *q1 = reinterpret_cast<uint32_t *>(take(4 * n));
   W.shQ = reinterpret_cast<uint32_t *>(take(4 * n));
+  W.grpQ = reinterpret_cast<uint32_t *>(take(4 * n));
   *counts = reinterpret_cast<uint32_t *>(take(64));
   return off;
 }
@@ -3280,6 +3324,7 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
   W.deadFlags = every > 1u ? 1u : 0u;
   const int block = std::max(32, std::min(run.block, kWfBlock));
   const bool pbr = A.layered != 0u, unbounded = scene_has_delta(scene);
+  const bool group = pbr && A.spectral && scene->has_film;
   const uint32_t gridMax = (uint32_t)ctx->sm_count * (8u * kWfBlock / (uint32_t)block);
   uint32_t *slot = vt_queue_slot(ctx);
   for (uint32_t k0 = 0; k0 < spp; k0 += chunk) {
@@ -3315,6 +3360,11 @@ vt_status wavefront_impl(vt_ctx *ctx, vt_scene *scene, const vt_frame_params *p,
       VT_CUDA(ctx, cudaMemsetAsync(W.shCount, 0, sizeof(uint32_t), s));
       vt_launch_closest(mesh, reinterpret_cast<const vt_ray *>(W.ray), P, reinterpret_cast<vt_hit *>(hit), ctx->sm_count,
                         slot, inQ, ctx->d_status + 1, s, inCount, true);
+      if (group) {
+        VT_CUDA(ctx, cudaMemsetAsync(counts + 3, 0, 2 * sizeof(uint32_t), s));
+        k_wf_group<<<grid, block, 0, s>>>(A, W, counts + 3);
+        W.inQ = W.grpQ;  // the same entries, regrouped (the count stays)
+      }
       if (nrc) {
         if (pbr) k_wf_shade<true, true><<<grid, block, 0, s>>>(A, W, b);
         else k_wf_shade<false, true><<<grid, block, 0, s>>>(A, W, b);
@@ -3848,6 +3898,7 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
   if (!ctx->pbr_opaque) return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables are not set (vt_openpbr_tables_set)");
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
   std::vector<float4> q(2 * (size_t)n);
+  bool film = false;
   for (uint32_t i = 0; i < n; ++i) {
     const vt_openpbr_params &p = params[i];
     if (!(p.roughness >= 0.0f && p.roughness <= 1.0f) || !(p.metalness >= 0.0f && p.metalness <= 1.0f) || !(p.ior > 0.0f) ||
@@ -3862,12 +3913,14 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
                                           "thickness be finite and non-negative and its IOR positive");
     q[2 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
     scene->slot_rough[i] = p.roughness;
+    if (p.thin_film_weight > 0.0f) film = true;
     q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f,
                                        p.coat);
   }
   if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, q.size() * sizeof(float4)));
   if (n) VT_CUDA(ctx, cudaMemcpy(scene->d_pbr, q.data(), q.size() * sizeof(float4), cudaMemcpyHostToDevice));
   scene->pbr_tables = ctx->d_pbr;
+  scene->has_film = film;
   return VT_OK;
 }
 

@@ -104,6 +104,7 @@ struct vt_scene {
   bool layered = false;  // some slot is OPENPBR, GLOSSY or DIELECTRIC
   std::vector<int32_t> slot_types;  // host copies: each slot's type and roughness (vt_scene_set_openpbr)
   std::vector<float> slot_rough;
+  bool has_film = false;  // some slot has a thin film (vt_scene_set_openpbr)
   vt_quad_light light;
   // Spectral tables: per 1 nm bin (cmf r, g, b, illuminant), the inverse CDF.
   float4 *d_spec = nullptr;
