@@ -437,13 +437,15 @@ vt_status vt_spectral_round_trip(vt_ctx *ctx, float *worst, uint32_t *over_half)
 /* ---- OpenPBR materials (openpbr.cu) ------------------------------------------------------------ */
 /* The layered BSDF of the reference's OPENPBR material type (prepare_openpbr, main.swift:2485-2512,
  * around the vendored Adobe openpbr-bsdf) for opaque materials: specular_weight, base colour,
- * metalness, specular roughness and IOR, diffuse roughness; coat, fuzz, transmission, thin film and
- * anisotropy are not supported. Its energy-compensation data: the dense metal table is solved on the
- * device (the reference's Shaders/MetalEnergy.metal); the opaque-dielectric energy complement tables
- * (32^3 and 32^2 unorm16, the upstream library's data) come from the caller, once per context. */
+ * metalness, specular roughness and IOR, diffuse roughness, thin film (spectral transport), coat and
+ * fuzz as the adapter sets them; transmission and anisotropy are not supported. Its data: the dense
+ * metal table is solved on the device (the reference's Shaders/MetalEnergy.metal); the
+ * opaque-dielectric energy complement tables (32^3 and 32^2 unorm16) and the fuzz lobe's LTC table
+ * (32 x 32 x 3 floats), the upstream library's data, come from the caller, once per context. */
 typedef struct vt_openpbr_tables {
   const uint16_t *opaque_energy;   /* 32 x 32 x 32: IOR, sqrt(alpha), cos */
   const uint16_t *opaque_average;  /* 32 x 32: IOR, sqrt(alpha) */
+  const float *ltc;                /* 32 x 32 x 3: the fuzz lobe's LTC fit (a_inv, b_inv, R); rows roughness, columns cos */
 } vt_openpbr_tables;
 vt_status vt_openpbr_tables_set(vt_ctx *ctx, const vt_openpbr_tables *tables);
 /* The dense isotropic GGX energy complement (129 x 129: roughness i/128, sqrt(cos) j/128) and its
@@ -452,13 +454,13 @@ vt_status vt_openpbr_energy_table(vt_ctx *ctx, float *table, float *average);
 
 /* One BSDF query: an OPENPBR material's parameters as the adapter reads them (roughness and IOR are
  * clamped to >= 0.03 and >= 1.01 inside), a unit shading normal, the view (outward) and light
- * directions, and three random numbers for a sample. 108 bytes. */
+ * directions, and three random numbers for a sample. 112 bytes. */
 typedef struct vt_openpbr_case {
   float base_color[3], metalness, roughness, ior, specular_weight, diffuse_roughness;
   float normal[3], view[3], light[3], rand[3];
   float thin_film_weight, thin_film_thickness /* micrometres */, thin_film_ior;
   float lambda[3];      /* the preparation's wavelengths in nm; 0: the upstream RGB wavelengths */
-  float coat;           /* coat weight */
+  float coat, fuzz;     /* coat and fuzz weights */
 } vt_openpbr_case;
 /* f |cos| at the light direction and its pdf; the sample: direction, weight f |cos| / pdf, its pdf,
  * and 1 when a sample was produced. 48 bytes. */
@@ -480,6 +482,9 @@ typedef struct vt_openpbr_params {
   float thin_film_weight, thin_film_thickness, thin_film_ior;
   /* Coat weight in [0, 1] (main.swift:2494; the adapter's coat: roughness 0.12, IOR 1.6, white). */
   float coat;
+  /* Fuzz weight in [0, 1] (main.swift:2497; the upstream default fuzz: roughness 0.5, white). */
+  float fuzz;
+  float pad[3];
 } vt_openpbr_params;
 vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n);
 

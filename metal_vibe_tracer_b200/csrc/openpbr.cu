@@ -49,7 +49,7 @@ struct CaseDev {
   float base[3], metal, rough, ior, sw, diffRough;
   float n[3], wo[3], wi[3], rand[3];
   float tfWeight, tfThickness, tfIor, lambda[3];
-  float coat;
+  float coat, fuzz;
 };
 struct ResultDev {
   float fcos[3], pdf, dir[3], weight[3], spdf, ok;
@@ -71,6 +71,7 @@ __device__ __forceinline__ PbrParams case_params(const CaseDev &c) {
   // The upstream RGB wavelengths unless the case gives its own (openpbr_bsdf.h: OpenPBR_BaseRgbWavelengths_nm).
   P.lambda = c.lambda[0] > 0.0f ? pf3(c.lambda[0], c.lambda[1], c.lambda[2]) : pf3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
   P.coat = c.coat;
+  P.fuzz = c.fuzz;
   return P;
 }
 
@@ -83,7 +84,7 @@ __global__ void k_openpbr_cases(PbrTables T, const CaseDev *__restrict__ cases, 
   const float3 f = pbr_eval(p, T, wi);
   ResultDev r;
   r.fcos[0] = f.x; r.fcos[1] = f.y; r.fcos[2] = f.z;
-  r.pdf = pbr_pdf(p, wi);
+  r.pdf = pbr_pdf(p, T, wi);
   float3 d = pf3(0.0f, 0.0f, 0.0f), w = pf3(0.0f, 0.0f, 0.0f);
   float q = 0.0f;
   const bool ok = pbr_sample(p, T, pf3(c.rand[0], c.rand[1], c.rand[2]), d, w, q);
@@ -100,11 +101,12 @@ __global__ void k_openpbr_cases(PbrTables T, const CaseDev *__restrict__ cases, 
 vt_status vt_openpbr_ensure(vt_ctx *ctx, const vt_openpbr_tables *tables) {
   if (ctx->d_pbr && (!tables || ctx->pbr_opaque)) return VT_OK;
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
-  const size_t nMetal = kMetalEnergyN * kMetalEnergyN, nAvg = kMetalEnergyN, nOpq = 32 * 32 * 32, nOpqAvg = 32 * 32;
+  const size_t nMetal = kMetalEnergyN * kMetalEnergyN, nAvg = kMetalEnergyN, nOpq = 32 * 32 * 32, nOpqAvg = 32 * 32,
+               nLtc = 3 * kPbrLtc * kPbrLtc;
   if (!ctx->d_pbr) {
     float *d = nullptr;
-    VT_CUDA(ctx, cudaMalloc(&d, (nMetal + nAvg + nOpq + nOpqAvg) * sizeof(float)));
-    cudaError_t e = cudaMemsetAsync(d, 0, (nMetal + nAvg + nOpq + nOpqAvg) * sizeof(float), ctx->stream);
+    VT_CUDA(ctx, cudaMalloc(&d, (nMetal + nAvg + nOpq + nOpqAvg + nLtc) * sizeof(float)));
+    cudaError_t e = cudaMemsetAsync(d, 0, (nMetal + nAvg + nOpq + nOpqAvg + nLtc) * sizeof(float), ctx->stream);
     if (e == cudaSuccess) {
       k_metal_energy<<<kMetalEnergyN, kMetalEnergyN, 0, ctx->stream>>>(d);
       e = cudaGetLastError();
@@ -135,12 +137,13 @@ vt_status vt_openpbr_ensure(vt_ctx *ctx, const vt_openpbr_tables *tables) {
     ctx->d_pbr = d;
   }
   if (tables && !ctx->pbr_opaque) {
-    if (!tables->opaque_energy || !tables->opaque_average)
-      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables need the opaque-dielectric energy tables");
+    if (!tables->opaque_energy || !tables->opaque_average || !tables->ltc)
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables need the opaque-dielectric energy tables and the fuzz LTC table");
     std::vector<float> f(nOpq + nOpqAvg);
     for (size_t i = 0; i < nOpq; ++i) f[i] = float(tables->opaque_energy[i]) * (1.0f / 65535.0f);
     for (size_t i = 0; i < nOpqAvg; ++i) f[nOpq + i] = float(tables->opaque_average[i]) * (1.0f / 65535.0f);
     VT_CUDA(ctx, cudaMemcpy(ctx->d_pbr + nMetal + nAvg, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    VT_CUDA(ctx, cudaMemcpy(ctx->d_pbr + nMetal + nAvg + nOpq + nOpqAvg, tables->ltc, nLtc * sizeof(float), cudaMemcpyHostToDevice));
     ctx->pbr_opaque = true;
   }
   return VT_OK;

@@ -2,7 +2,7 @@
 // Derivative work of the Adobe OpenPBR BSDF (https://github.com/adobe/openpbr-bsdf, c91aad1d),
 // Copyright 2026 Adobe, licensed under the Apache License, Version 2.0 (LICENSES/Apache-2.0.txt,
 // http://www.apache.org/licenses/LICENSE-2.0); modified as described below and in NOTICE.
-// openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials under an optional coat: a GGX (VNDF-sampled)
+// openpbr.cuh — the OpenPBR layered BSDF on the device, for opaque materials under optional coat and fuzz: a GGX (VNDF-sampled)
 // specular lobe with dielectric Fresnel on the dielectric part and F82-tinted Schlick on the metal
 // part, the metal's microfacet multiple-scattering lobe, and the energy-conserving (EON) diffuse
 // base, combined as one aggregate with lobe selection by estimated contribution.
@@ -22,15 +22,15 @@
 // What the restatement covers: specular_weight, base_color, base_metalness, specular_roughness,
 // specular_ior, base_diffuse_roughness, thin-film iridescence (thin_film_weight, _thickness, _ior, at
 // the preparation's three wavelengths; impl/openpbr_thin_film_iridescence_utils.h and
-// openpbr_reflection_coefficient, impl/openpbr_reflection_transmission_coefficient.h:55-125), and the
-// coat as the reference's adapter sets it (coat_weight; coat_roughness 0.12, coat_ior 1.6, white
+// openpbr_reflection_coefficient, impl/openpbr_reflection_transmission_coefficient.h:55-125), the coat
+// as the reference's adapter sets it (coat_weight; coat_roughness 0.12, coat_ior 1.6, white
 // coat_color, coat_darkening 1; impl/openpbr_coating_lobe.h and the coat's IOR, roughness and
-// darkening terms of openpbr_prepare_lobes), with fuzz, transmission, subsurface, anisotropy and
-// dispersion at zero. In that case the upstream fuzz layer passes the coated base through
-// (presence 0), the dielectric multiple-scattering lobe and both thin-wall lobes have zero weight and
-// value, and specular transmission has zero probability; the code below keeps only what is left, in
-// the upstream operation order. The fuzz layer's recomputation of the sample weight (w pdf / pdf) is
-// kept for the same rounding.
+// darkening terms of openpbr_prepare_lobes) and the fuzz (fuzz_weight; the default fuzz_roughness 0.5
+// and white fuzz_color; impl/openpbr_fuzz_lobe.h, the LTC sheen fit in the tables), with
+// transmission, subsurface, anisotropy and dispersion at zero. In that case the dielectric
+// multiple-scattering lobe and both thin-wall lobes have zero weight and value, and specular
+// transmission has zero probability; the code below keeps only what is left, in the upstream
+// operation order, including the layers' recomputation of a sample's weight (w pdf / pdf).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -48,6 +48,7 @@ constexpr float kPbrMinAlphaEnergyLoss = 0.04f * 0.04f;
 constexpr int kPbrTable = 32;           // the opaque-dielectric energy tables' size per axis
 constexpr float kPbrIorMax = 2.5f;
 constexpr uint32_t kMetalEnergyN = 129;  // the dense metal table: 129 roughness x 129 sqrt-cosine nodes
+constexpr int kPbrLtc = 32;              // the fuzz LTC table's size per axis
 // The upstream library's wavelengths for R, G and B (openpbr_constants.h: OpenPBR_BaseRgbWavelengths_nm).
 __device__ constexpr float kPbrRgbNm[3] = {620.0f, 540.0f, 450.0f};
 
@@ -59,18 +60,24 @@ struct PbrParams {
   float tfWeight, tfThickness, tfIor;  // thin film: weight, thickness (micrometres), IOR
   float3 lambda;                       // the preparation's three wavelengths (nm)
   float coat;                          // coat weight (roughness 0.12, IOR 1.6, white, darkening 1)
+  float fuzz;                          // fuzz weight (roughness 0.5, white)
 };
 // The reference adapter's coat for materials without a MaterialX graph (prepare_openpbr,
 // main.swift:2494-2495: coat_roughness 0.12) and the upstream default coat IOR
 // (openpbr_make_default_resolved_inputs: coat_ior 1.6).
 constexpr float kPbrCoatRoughness = 0.12f;
 constexpr float kPbrCoatIor = 1.6f;
+// The upstream default fuzz (fuzz_roughness 0.5, white fuzz_color; the adapter sets only the weight,
+// main.swift:2497) and its effect on the coat's roughness (FuzzEffectOnUnderlyingRoughness).
+constexpr float kPbrFuzzRoughness = 0.5f;
+constexpr float kPbrFuzzOnRoughness = 0.005f;
 
 struct PbrTables {
   const float *metalE;     // 129 x 129
   const float *metalAvg;   // 129
   const float *opaqueE;    // 32 x 32 x 32 (ior, alpha, cos)
   const float *opaqueAvg;  // 32 x 32 (ior, alpha)
+  const float *ltc;        // 32 x 32 x 3: the fuzz LTC fit (a_inv, b_inv, R); rows roughness, columns cos
 };
 
 __device__ __forceinline__ float3 pf3(float x, float y, float z) { return make_float3(x, y, z); }
@@ -391,6 +398,12 @@ struct PbrPrepared {
   float coatEta, coatAlpha, coatAx, inRefl;
   float3 inScale;
   float coatProb;
+  // Fuzz (the sheen lobe over the coated base): presence (0 from inside), its basis about the
+  // face-forwarded normal, the view in it, the share it reflects at the view, its probability.
+  float fuzz;
+  PbrBasis FB;
+  float3 fwo;
+  float fuzzRefl, fuzzProb;
 };
 
 // Reflection coefficient of the specular lobe at cos c to the half vector (openpbr_reflection_coefficient):
@@ -426,6 +439,24 @@ __device__ __forceinline__ float pbr_dielectric_energy_reflected(const PbrTables
   return alpha == 0.0f ? pbr_fresnel(eta, c) : 1.0f - pbr_opaque_energy(T, eta, alpha, c);
 }
 
+// The fuzz lobe's LTC coefficients (a_inv, b_inv, R) at roughness alpha and cos c: bilinear over the
+// 32 x 32 table (openpbr_disney_sheen_fetch_coeffs).
+__device__ __forceinline__ float3 pbr_ltc_at(const PbrTables &T, int i, int j) {
+  const float *q = T.ltc + 3 * (i * kPbrLtc + j);
+  return pf3(__ldg(q), __ldg(q + 1), __ldg(q + 2));
+}
+__device__ __forceinline__ float3 pbr_ltc_fetch(const PbrTables &T, float alpha, float c) {
+  const float row = fmaxf(0.0f, fminf(alpha, kPbrBelowOne)) * float(kPbrLtc - 1);
+  const float col = fmaxf(0.0f, fminf(c, kPbrBelowOne)) * float(kPbrLtc - 1);
+  const float r = floorf(row), cc = floorf(col);
+  const float rf = row - r, cf = col - cc;
+  const int ri = int(r), ci = int(cc);
+  const float3 a = pbr_ltc_at(T, ri, ci), b = pbr_ltc_at(T, ri, ci + 1), d = pbr_ltc_at(T, ri + 1, ci), e = pbr_ltc_at(T, ri + 1, ci + 1);
+  const float3 m0 = pf3(pmix(a.x, b.x, cf), pmix(a.y, b.y, cf), pmix(a.z, b.z, cf));
+  const float3 m1 = pf3(pmix(d.x, e.x, cf), pmix(d.y, e.y, cf), pmix(d.z, e.z, cf));
+  return pf3(pmix(m0.x, m1.x, rf), pmix(m0.y, m1.y, rf), pmix(m0.z, m1.z, rf));
+}
+
 // openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit). Without
 // `weights` the lobe-selection weights (which only pbr_pdf and pbr_sample read) are left at zero: a
 // preparation that is only evaluated skips the specular coefficient at the view.
@@ -455,9 +486,12 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
   } else {
     p.etaOpaque = wior / 1.0f;
   }
-  // Roughnesses (openpbr_bsdf.h:424-460): no fuzz, so the coat keeps its roughness; the coat
+  // Roughnesses (openpbr_bsdf.h:424-460): the fuzz roughens the coat a little by its weight; the coat
   // roughens the base by its presence, the less the closer its IOR is to the exterior's.
-  const float coatRough = kPbrCoatRoughness;
+  const float fuzzAdjust = (1.0f + 1.0f + 1.0f) * (1.0f / 3.0f) * kPbrFuzzRoughness * kPbrFuzzOnRoughness;  // average(colour) x roughness x effect
+  const float coatRough =
+      pmix(kPbrCoatRoughness,
+           pbr_fourth_root(fminf(1.0f, pbr_fourth_power(kPbrCoatRoughness) + fuzzAdjust * pbr_fourth_power(kPbrFuzzRoughness))), P.fuzz);
   const float adjust = pmix(1.0f, 0.0f, relCoat >= 1.0f ? 1.0f / relCoat : relCoat);
   const float rough = P.coat > 0.0f
                           ? pmix(P.rough, pbr_fourth_root(fminf(1.0f, pbr_fourth_power(P.rough) + adjust * pbr_fourth_power(coatRough))), P.coat)
@@ -513,6 +547,17 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
     p.inRefl = idotn > 0.0f ? pbr_dielectric_energy_reflected(T, relCoat, p.coatAlpha, idotn) * P.coat : 0.0f;
     p.inScale = pscale(darkening, 1.0f - p.inRefl);
   }
+  // The fuzz layer (impl/openpbr_fuzz_lobe.h, white, roughness 0.5): absent from inside; its basis about
+  // the face-forwarded normal (the base's and the coat's are one), the view in it and the share of
+  // light it reflects there.
+  p.fuzz = back ? 0.0f : P.fuzz;
+  p.fuzzRefl = 0.0f;
+  p.fuzzProb = 0.0f;
+  if (p.fuzz > 0.0f) {
+    p.FB = pbr_basis(pnormalize(p.B.n));
+    p.fwo = pbr_to_local(p.FB, wo);
+    p.fuzzRefl = p.fwo.z <= 0.0f ? 0.0f : p.fuzz * pbr_ltc_fetch(T, kPbrFuzzRoughness, p.fwo.z).z;
+  }
   // Lobe weights (estimated contributions with a white throughput).
   if (!weights) {
     p.wSpec = p.wMetal = p.wDiff = p.total = 0.0f;
@@ -524,6 +569,13 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
   p.total = ((((p.wSpec + 0.0f) + p.wMetal) + p.wDiff) + 0.0f) + 0.0f;
   if (p.coat > 0.0f && !p.inside)
     p.coatProb = psafe_div(p.inRefl, p.inRefl + p.total * pmax3(p.inScale), 0.5f);
+  if (p.fuzz > 0.0f) {
+    // The coated base's estimated contribution: from inside the base's, else the coat's reflected
+    // share plus the base's under the coat.
+    const float coating = p.inside ? p.total : 1.0f * p.inRefl + p.total * pmax3(p.inScale);
+    const float sheen = p.fuzzRefl * 1.0f;
+    p.fuzzProb = psafe_div(sheen, sheen + coating * (1.0f - p.fuzzRefl), 0.5f);
+  }
   return p;
 }
 
@@ -753,12 +805,12 @@ __device__ __forceinline__ bool pbr_coat_sample(const PbrPrepared &p, float3 r, 
 // scale at the view (no attenuation on the light's side, OPENPBR_RECIPROCAL_COAT_AND_FUZZ 0); the pdf
 // mixes the coat's and the base's by the coat's sampling probability. From inside only the base
 // counts (a white coat tints nothing). Without a coat the coat's terms vanish and are skipped.
-__device__ __forceinline__ float3 pbr_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+__device__ __forceinline__ float3 pbr_coating_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
   const float3 base = pbr_base_eval(p, T, wi);
   if (p.inside || !(p.coat > 0.0f)) return base;
   return padd(pscale(pbr_coat_value(p, wi), p.coat), pmul(base, p.inScale));
 }
-__device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, float3 wi) {
+__device__ __forceinline__ float pbr_coating_pdf(const PbrPrepared &p, float3 wi) {
   const float pb = pbr_base_pdf(p, wi);
   if (p.inside || !(p.coat > 0.0f)) return pb;
   return pmix(pb, pbr_coat_pdf(p, wi), p.coatProb);
@@ -766,7 +818,8 @@ __device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, float3 wi) {
 // One sample from three numbers: direction, weight f |cos| / pdf and pdf; false when none. Outside,
 // the coat or the base is chosen by r.x against the coat's probability (r.x remapped), and the weight
 // recomputed from both layers' f |cos| and pdfs; the fuzz layer recomputes it once more.
-__device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w, float &pdf) {
+__device__ __forceinline__ bool pbr_coating_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w,
+                                                   float &pdf) {
   if (p.inside) {
     if (!pbr_base_sample(p, T, r, wi, w, pdf)) return false;
   } else {
@@ -793,7 +846,85 @@ __device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables
       w = pscale(fc, 1.0f / pdf);
     }
   }
-  // The fuzz layer (presence 0) recomputes the weight from f |cos| and the pdf.
+  return true;
+}
+
+// The fuzz (Disney sheen) lobe as linearly transformed cosines (Zeltner, Burley and Chiang 2022;
+// impl/openpbr_fuzz_lobe.h): directions local to the fuzz basis, rotated about the normal so that
+// the view lies in the x-z plane of the fit.
+__device__ __forceinline__ float3 pbr_sheen_rotate(float3 v, float x, float y) {
+  const float r2 = x * x + y * y;
+  if (r2 == 0.0f) return v;
+  const float inv = 1.0f / sqrtf(r2);
+  const float sn = y * inv, cs = x * inv;
+  return pf3(cs * v.x + sn * -v.y, cs * v.y + sn * v.x, v.z);
+}
+__device__ __forceinline__ float pbr_sheen_ltc(float3 wl, float3 k) {
+  const float3 o = pf3(k.x * wl.x + k.y * wl.z, k.x * wl.y, wl.z);
+  const float z = fmaxf(0.0f, wl.z);
+  const float len2 = pdot(o, o);
+  if (len2 == 0.0f || k.x == 0.0f || z == 0.0f) return 0.0f;
+  const float t = k.x / len2;
+  return kPbrRcpPi * (z * t) * t;
+}
+__device__ __forceinline__ float3 pbr_sheen_f(const PbrPrepared &p, const PbrTables &T, float3 wl) {
+  if (p.fwo.z <= 0.0f || wl.z <= 0.0f) return pf3(0.0f, 0.0f, 0.0f);
+  const float3 ws = pbr_sheen_rotate(wl, p.fwo.x, -p.fwo.y);
+  const float3 k = pbr_ltc_fetch(T, kPbrFuzzRoughness, p.fwo.z);
+  const float v = pbr_sheen_ltc(ws, k) * (p.fuzz * k.z * 1.0f);
+  return pf3(v, v, v);
+}
+__device__ __forceinline__ float pbr_sheen_pdf(const PbrPrepared &p, const PbrTables &T, float3 wl) {
+  if (p.fwo.z <= 0.0f || wl.z <= 0.0f) return 0.0f;
+  return pbr_sheen_ltc(pbr_sheen_rotate(wl, p.fwo.x, -p.fwo.y), pbr_ltc_fetch(T, kPbrFuzzRoughness, p.fwo.z));
+}
+__device__ __forceinline__ bool pbr_sheen_sample(const PbrPrepared &p, const PbrTables &T, float2 r, float3 &wl) {
+  if (p.fwo.z <= 0.0f) return false;
+  const float3 k = pbr_ltc_fetch(T, kPbrFuzzRoughness, p.fwo.z);
+  const float phi = kPbrTwoPi * r.x, z = sqrtf(r.y), rr = sqrtf(1.0f - r.y);
+  const float3 o = pf3(cosf(phi) * rr, sinf(phi) * rr, z);
+  const float a = 1.0f / k.x;
+  const float3 ws = pnormalize(pf3(o.x * a - o.z * k.y * a, o.y * a, o.z));
+  wl = pbr_sheen_rotate(ws, p.fwo.x, p.fwo.y);
+  return p.fwo.z * wl.z > 0.0f;
+}
+
+// The fuzz layer over the coated base: f = coated base x (1 - the fuzz's share at the view) + sheen;
+// the pdf mixes the two by the fuzz's sampling probability. Without fuzz the sheen terms vanish and are
+// skipped; the layer still recomputes a sample's weight from f |cos| and the pdf.
+__device__ __forceinline__ float3 pbr_eval(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  const float3 coated = pbr_coating_eval(p, T, wi);
+  if (!(p.fuzz > 0.0f)) return coated;
+  return padd(pscale(coated, 1.0f - p.fuzzRefl), pbr_sheen_f(p, T, pbr_to_local(p.FB, wi)));
+}
+__device__ __forceinline__ float pbr_pdf(const PbrPrepared &p, const PbrTables &T, float3 wi) {
+  const float pc = pbr_coating_pdf(p, wi);
+  if (!(p.fuzz > 0.0f)) return pc;
+  return pmix(pc, pbr_sheen_pdf(p, T, pbr_to_local(p.FB, wi)), p.fuzzProb);
+}
+__device__ __forceinline__ bool pbr_sample(const PbrPrepared &p, const PbrTables &T, float3 r, float3 &wi, float3 &w, float &pdf) {
+  if (p.fuzz > 0.0f) {
+    const float sp = p.fuzzProb, bp = 1.0f - sp;
+    if (r.x < sp) {
+      float3 wl;
+      if (!pbr_sheen_sample(p, T, make_float2(r.y, r.z), wl)) return false;
+      wi = pnormalize(pbr_to_world(p.FB, wl));
+      pdf = pbr_sheen_pdf(p, T, wl) * sp;
+      pdf += pbr_coating_pdf(p, wi) * bp;
+      w = pscale(pbr_eval(p, T, wi), 1.0f / pdf);
+      return true;
+    }
+    const float rx = pclamp_rand((r.x - sp) * (1.0f / bp));
+    if (!pbr_coating_sample(p, T, pf3(rx, r.y, r.z), wi, w, pdf)) return false;
+    const float3 wl = pbr_to_local(p.FB, wi);
+    float3 fc = pscale(pscale(w, pdf), 1.0f - p.fuzzRefl);
+    fc = padd(fc, pbr_sheen_f(p, T, wl));
+    pdf *= bp;
+    pdf += pbr_sheen_pdf(p, T, wl) * sp;
+    w = pscale(fc, 1.0f / pdf);
+    return true;
+  }
+  if (!pbr_coating_sample(p, T, r, wi, w, pdf)) return false;
   w = pscale(pscale(w, pdf), 1.0f / pdf);
   return true;
 }
@@ -808,6 +939,7 @@ inline PbrTables pbr_tables_at(const float *base) {
   T.metalAvg = base + kMetalEnergyN * kMetalEnergyN;
   T.opaqueE = T.metalAvg + kMetalEnergyN;
   T.opaqueAvg = T.opaqueE + kPbrTable * kPbrTable * kPbrTable;
+  T.ltc = T.opaqueAvg + kPbrTable * kPbrTable;
   return T;
 }
 }  // namespace vtd

@@ -889,17 +889,18 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
 }
 
 // ---- per-slot lobe parameters, OpenPBR vertices (openpbr.cuh) and delta vertices ----------------
-// Per slot two float4 (vt_scene_set_openpbr): (roughness, metalness, IOR, diffuse roughness) and the
-// thin film (weight, thickness in micrometres, IOR, 0). Without a table (or for a slot past it) a
-// slot is ideal: roughness 0, IOR 1.5, no film.
+// Per slot kSlotF4 float4 (vt_scene_set_openpbr): (roughness, metalness, IOR, diffuse roughness), the
+// thin film (weight, thickness in micrometres, IOR) with the coat weight, and (fuzz weight, 0, 0, 0).
+// Without a table (or for a slot past it) a slot is ideal: roughness 0, IOR 1.5, no film, coat or fuzz.
+constexpr uint32_t kSlotF4 = 3;
 __device__ __forceinline__ float4 slot_lobe(const RenderArgs &A, const vt_material &m) {
   const uint32_t slot = __float_as_uint(m.pad);
-  return A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot) : make_float4(0.0f, 0.0f, 1.5f, 0.0f);
+  return A.pbr && slot < A.nmat ? __ldg(A.pbr + kSlotF4 * slot) : make_float4(0.0f, 0.0f, 1.5f, 0.0f);
 }
 // The slot's second float4: the thin film (weight, thickness in micrometres, IOR) and the coat weight.
 __device__ __forceinline__ float4 slot_extra(const RenderArgs &A, const vt_material &m) {
   const uint32_t slot = __float_as_uint(m.pad);
-  return A.pbr && slot < A.nmat ? __ldg(A.pbr + 2u * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
+  return A.pbr && slot < A.nmat ? __ldg(A.pbr + kSlotF4 * slot + 1u) : make_float4(0.0f, 0.0f, 1.4f, 0.0f);
 }
 // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568, and
 // spectral_thin_film_mirror; the RGB adapter leaves it at zero).
@@ -925,6 +926,8 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
   P.tfThickness = A.spectral ? x.y : 0.0f;
   P.tfIor = A.spectral ? x.z : 1.4f;
   P.coat = x.w;  // in both transports (prepare_openpbr and prepare_openpbr_lanes, main.swift:2494, 2537)
+  const uint32_t slot = __float_as_uint(m.pad);
+  P.fuzz = A.pbr && slot < A.nmat ? __ldg(A.pbr + kSlotF4 * slot + 2u).x : 0.0f;  // main.swift:2497, 2540
   P.lambda = lambda;
   return P;
 }
@@ -952,7 +955,7 @@ __device__ __forceinline__ bool is_delta(const RenderArgs &A, const vt_material 
 template <bool kPbr>
 __device__ __forceinline__ bool is_pbr(const RenderArgs &A, const vt_material &m) {
   return kPbr && A.pbr && __float_as_uint(m.pad) < A.nmat &&
-         (m.type == VT_MAT_OPENPBR || (m.type == VT_MAT_GLOSSY && __ldg(A.pbr + 2u * __float_as_uint(m.pad)).x >= 0.02f));
+         (m.type == VT_MAT_OPENPBR || (m.type == VT_MAT_GLOSSY && __ldg(A.pbr + kSlotF4 * __float_as_uint(m.pad)).x >= 0.02f));
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706) at an OPENPBR vertex: f (without the cosine) per lane
 // and the pdf of `a`.
@@ -968,7 +971,7 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   const float3 lam = film ? make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2))
                           : make_float3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
   const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo);
-  pdf = pbr_pdf(a, wi);
+  pdf = pbr_pdf(a, A.pbrT, wi);
   if (dot3(wi, gn) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float3 fa = pbr_eval(a, A.pbrT, wi);
   float f3w = fa.x;
@@ -3897,7 +3900,7 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
   if (n != scene->nmat) return vt_fail(ctx, VT_ERR_INVALID, "n must equal the scene's material slot count");
   if (!ctx->pbr_opaque) return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR tables are not set (vt_openpbr_tables_set)");
   VT_CUDA(ctx, cudaSetDevice(ctx->device));
-  std::vector<float4> q(2 * (size_t)n);
+  std::vector<float4> q(kSlotF4 * (size_t)n);
   bool film = false;
   for (uint32_t i = 0; i < n; ++i) {
     const vt_openpbr_params &p = params[i];
@@ -3905,16 +3908,17 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
         !(p.diffuse_roughness >= 0.0f && p.diffuse_roughness <= 1.0f))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": roughness, metalness and diffuse roughness "
                                           "must lie in [0, 1] and the IOR be positive");
-    if (!(p.coat >= 0.0f && p.coat <= 1.0f))
-      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": coat weight must lie in [0, 1]");
+    if (!(p.coat >= 0.0f && p.coat <= 1.0f) || !(p.fuzz >= 0.0f && p.fuzz <= 1.0f))
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": coat and fuzz weights must lie in [0, 1]");
+    q[kSlotF4 * (size_t)i + 2] = make_float4(p.fuzz, 0.0f, 0.0f, 0.0f);
     if (!(p.thin_film_weight >= 0.0f && p.thin_film_weight <= 1.0f) || !(p.thin_film_thickness >= 0.0f) ||
         !std::isfinite(p.thin_film_thickness) || (p.thin_film_weight > 0.0f && !(p.thin_film_ior > 0.0f)))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": thin-film weight must lie in [0, 1], its "
                                           "thickness be finite and non-negative and its IOR positive");
-    q[2 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
+    q[kSlotF4 * (size_t)i] = make_float4(p.roughness, p.metalness, p.ior, p.diffuse_roughness);
     scene->slot_rough[i] = p.roughness;
     if (p.thin_film_weight > 0.0f) film = true;
-    q[2 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f,
+    q[kSlotF4 * (size_t)i + 1] = make_float4(p.thin_film_weight, p.thin_film_thickness, p.thin_film_weight > 0.0f ? p.thin_film_ior : 1.4f,
                                        p.coat);
   }
   if (!scene->d_pbr && n) VT_CUDA(ctx, cudaMalloc(&scene->d_pbr, q.size() * sizeof(float4)));

@@ -1,6 +1,7 @@
-"""OpenPBR energy-compensation data: the opaque-dielectric energy complement tables of the Adobe
-openpbr-bsdf library the reference vendors (Vendor/OpenPBR/impl/data, Apache-2.0), which the
-diffuse base lobe uses (impl/openpbr_diffuse_lobe.h).
+"""OpenPBR data: the opaque-dielectric energy complement tables of the Adobe openpbr-bsdf library
+the reference vendors (Vendor/OpenPBR/impl/data, Apache-2.0), which the diffuse base lobe and the
+coat use (impl/openpbr_diffuse_lobe.h, impl/openpbr_coating_lobe.h), and the fuzz lobe's LTC table
+(openpbr_ltc_data.h: Zeltner, Burley and Chiang's sheen fit, Apache-2.0).
 
 They are library data, not part of this repository: `generate()` reads them at build time from the
 reference's vendored headers (32^3 and 32^2 unorm16 values) and writes
@@ -26,7 +27,7 @@ def reference_data() -> Path | None:
     from .spectral_tables import reference_root
     r = reference_root()
     return r / "Vendor" / "OpenPBR" / "impl" / "data" if r else None
-MAGIC = b"VTPBR001"
+MAGIC = b"VTPBR002"
 N = 32
 
 
@@ -35,17 +36,28 @@ def _read_values(path: Path) -> np.ndarray:
     return np.array([int(v) for v in re.findall(r"\d+", text)], np.uint16)
 
 
+def _read_ltc(path: Path) -> np.ndarray:
+    """The fuzz lobe's LTC table (openpbr_ltc_data.h: 32 x 32 entries of (a_inv, b_inv, R), rows by
+    roughness, columns by cos theta) as float32, each decimal literal rounded as a C++ compiler does
+    (to double, then to float)."""
+    text = "\n".join(line for line in path.read_text().splitlines() if not line.lstrip().startswith("//"))
+    num = r"\s*([-\d.eE+]+)\s*"
+    vals = re.findall(r"vec3\(" + num + "," + num + "," + num + r"\)", text)
+    return np.array([[float(x) for x in v] for v in vals], np.float64).astype(np.float32).reshape(-1)
+
+
 def generate(data_dir: Path | None = None) -> Path:
     data_dir = data_dir or reference_data()
     if data_dir is None:
         raise RuntimeError("OpenPBR data: set VT_REFERENCE_ROOT to the reference checkout")
     energy = _read_values(data_dir / "openpbr_opaque_dielectric_energy_complement_data.h")
     average = _read_values(data_dir / "openpbr_opaque_dielectric_avg_energy_complement_data.h")
-    if energy.size != N ** 3 or average.size != N ** 2:
-        raise RuntimeError(f"unexpected OpenPBR table sizes {energy.size}, {average.size}")
+    ltc = _read_ltc(data_dir / "openpbr_ltc_data.h")
+    if energy.size != N ** 3 or average.size != N ** 2 or ltc.size != 3 * N * N:
+        raise RuntimeError(f"unexpected OpenPBR table sizes {energy.size}, {average.size}, {ltc.size}")
     DATA.parent.mkdir(parents=True, exist_ok=True)
     tmp = DATA.with_suffix(".tmp")
-    tmp.write_bytes(MAGIC + energy.tobytes() + average.tobytes())
+    tmp.write_bytes(MAGIC + energy.tobytes() + average.tobytes() + ltc.tobytes())
     tmp.replace(DATA)
     return DATA
 
@@ -59,4 +71,5 @@ def load() -> dict:
         raise RuntimeError(f"{DATA}: bad header")
     energy = np.frombuffer(b, np.uint16, N ** 3, 8).copy()
     average = np.frombuffer(b, np.uint16, N ** 2, 8 + 2 * N ** 3).copy()
-    return {"opaque_energy": energy, "opaque_average": average}
+    ltc = np.frombuffer(b, np.float32, 3 * N * N, 8 + 2 * N ** 3 + 2 * N ** 2).copy()
+    return {"opaque_energy": energy, "opaque_average": average, "ltc": ltc}

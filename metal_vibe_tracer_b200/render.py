@@ -149,6 +149,7 @@ class Scene:
                 params[i].thin_film_thickness = float(m.get("thin_film_thickness", 0.0))
                 params[i].thin_film_ior = float(m.get("thin_film_ior", 1.4))
                 params[i].coat = float(m.get("coat", 0.0))
+                params[i].fuzz = float(m.get("fuzz", 0.0))
             _check(ctx.handle, lib.vt_scene_set_openpbr(ctx.handle, self._p, params, len(materials)), "vt_scene_set_openpbr")
 
     def set_environment(self, intensity: float = 0.0, sun_dir=(0.0, 1.0, 0.0), sun_intensity: float = 0.0,
@@ -403,8 +404,8 @@ def openpbr_tables_set(ctx: Context) -> None:
         return
     from . import openpbr_tables
     t = openpbr_tables.load()
-    e, a = t["opaque_energy"], t["opaque_average"]
-    s = _lib.OpenPBRTables(e.ctypes.data, a.ctypes.data)
+    e, a, ltc = t["opaque_energy"], t["opaque_average"], t["ltc"]
+    s = _lib.OpenPBRTables(e.ctypes.data, a.ctypes.data, ltc.ctypes.data)
     _check(ctx.handle, _lib.load().vt_openpbr_tables_set(ctx.handle, C.byref(s)), "vt_openpbr_tables_set")
     ctx._pbr_tables_set = True
 
@@ -420,13 +421,14 @@ def openpbr_energy_table(ctx: Context) -> tuple[np.ndarray, np.ndarray]:
 
 def openpbr_evaluate(ctx: Context, cases) -> np.ndarray:
     """BSDF queries on the device: `cases` is an (n, 20) float32 array of the _lib.OpenPBRCase fields
-    up to `rand` (no thin film, the upstream RGB wavelengths, no coat), (n, 26) with the thin film's
-    weight, thickness (micrometres) and IOR and the three wavelengths (nm), or (n, 27) with the coat
-    weight as well; returns (n, 12) float32 results (f_cos, pdf, dir, weight, sample_pdf, ok)."""
+    up to `rand` (no thin film, the upstream RGB wavelengths, no coat or fuzz), (n, 26) with the thin
+    film's weight, thickness (micrometres) and IOR and the three wavelengths (nm), or (n, 28) with the
+    coat and fuzz weights as well; returns (n, 12) float32 results (f_cos, pdf, dir, weight,
+    sample_pdf, ok)."""
     arr = np.asarray(cases, np.float32)
-    if arr.ndim == 2 and arr.shape[1] in (20, 26):
-        arr = np.concatenate([arr, np.zeros((arr.shape[0], 27 - arr.shape[1]), np.float32)], axis=1)
-    arr = np.ascontiguousarray(arr, np.float32).reshape(-1, 27)
+    if arr.ndim == 2 and arr.shape[1] in (20, 26, 27):
+        arr = np.concatenate([arr, np.zeros((arr.shape[0], 28 - arr.shape[1]), np.float32)], axis=1)
+    arr = np.ascontiguousarray(arr, np.float32).reshape(-1, 28)
     out = np.empty((arr.shape[0], 12), np.float32)
     _check(ctx.handle, _lib.load().vt_openpbr_evaluate(ctx.handle, arr.ctypes.data, arr.shape[0], out.ctypes.data),
            "vt_openpbr_evaluate")

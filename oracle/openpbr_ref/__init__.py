@@ -38,14 +38,16 @@ def load():
     return _lib
 
 
-def material(base, metalness, roughness, ior, type_=4, thin_film=None, coat=0.0):
+def material(base, metalness, roughness, ior, type_=4, thin_film=None, coat=0.0, fuzz=0.0):
     """A reference material; `thin_film` = (weight, thickness in micrometres, IOR) or None; `coat`:
-    the coat weight (the adapter's coat: roughness 0.12, default IOR and colour)."""
+    the coat weight (the adapter's coat: roughness 0.12, default IOR and colour); `fuzz`: the fuzz
+    weight (default roughness and colour)."""
     m = Material()
     m.type = type_
     m.albedo[:] = [float(x) for x in base]
     m.roughness, m.metalness, m.ior = float(roughness), float(metalness), float(ior)
     m.coat = float(coat)
+    m.fuzz = float(fuzz)
     if thin_film is not None:
         m.thin_film_weight, m.thin_film_thickness, m.thin_film_ior = (float(x) for x in thin_film)
     return m

@@ -2260,7 +2260,7 @@ bool visible_d(const PtContext &C, D3 p, D3 gn, double err, const PtLight &ls) {
 const float *slot_params(const PtContext &C, const vt_material &m) {
   uint32_t slot;
   std::memcpy(&slot, &m.pad, sizeof slot);
-  return C.in->pbr_params && slot < C.in->nmat ? C.in->pbr_params + 8 * (size_t)slot : nullptr;
+  return C.in->pbr_params && slot < C.in->nmat ? C.in->pbr_params + 12 * (size_t)slot : nullptr;
 }
 // is_delta (main.swift:3285-3287): glass, and GLOSSY mirrors smoother than 0.02.
 bool is_delta_d(const PtContext &C, const vt_material &m) {
@@ -2281,11 +2281,12 @@ vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double
   q.albedo[0] = (float)b0;
   q.albedo[1] = (float)b1;
   q.albedo[2] = (float)b2;
-  const float *pp = C.in->pbr_params + 8 * (size_t)slot;
+  const float *pp = C.in->pbr_params + 12 * (size_t)slot;
   q.roughness = pp[0];
   q.metalness = pp[1];
   q.ior = pp[2];
   q.coat = pp[7];  // both transports (prepare_openpbr, main.swift:2494)
+  q.fuzz = pp[8];  // main.swift:2497
   // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568).
   if (C.spectral) {
     q.thin_film_weight = pp[4];
@@ -2299,7 +2300,7 @@ vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double
 bool pbr_film_d(const PtContext &C, const vt_material &m) {
   uint32_t slot;
   std::memcpy(&slot, &m.pad, sizeof slot);
-  return C.spectral && C.in->pbr_params[8 * (size_t)slot + 4] > 0.0f;
+  return C.spectral && C.in->pbr_params[12 * (size_t)slot + 4] > 0.0f;
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706): f (no cosine) per lane, pdf of lanes 0-2.
 Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, D3 wi, double &pdf) {

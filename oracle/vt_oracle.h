@@ -128,9 +128,9 @@ typedef struct vto_pt_inputs {
    * the warped phase at each of the nbins bins. Needed when spectral. */
   const struct vto_uplift *uplift;
   const float *cos_phase;
-  /* Per-slot lobe parameters, read for OPENPBR, GLOSSY and DIELECTRIC slots (types 4, 1, 2): 8 floats
+  /* Per-slot lobe parameters, read for OPENPBR, GLOSSY and DIELECTRIC slots (types 4, 1, 2): 12 floats
    * (roughness, metalness, IOR, diffuse roughness, thin-film weight, thickness in micrometres and IOR,
-   * coat weight), and the BSDF (null parameters: GLOSSY slots are mirrors, DIELECTRIC slots have IOR 1.5). */
+   * coat weight, fuzz weight, 3 unused), and the BSDF (null parameters: GLOSSY slots are mirrors, DIELECTRIC slots have IOR 1.5). */
   const float *pbr_params;
   vto_pbr_eval_fn pbr_eval;
   vto_pbr_sample_fn pbr_sample;

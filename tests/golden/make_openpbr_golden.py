@@ -10,7 +10,8 @@ at the light direction and its sample (direction, weight, pdf). The metal table:
 the 129 x 129 table and all 129 averages. Thin-film cases (tests/golden/openpbr_thin_film_cases.json): the
 same with thin-film iridescence (weight, thickness, film IOR) at three given wavelengths. Coated cases
 (tests/golden/openpbr_coat_cases.json): the same with the adapter's coat (weight; roughness 0.12, IOR
-1.6), a third of them with a thin film under it.
+1.6), a third of them with a thin film under it. Fuzzed cases (tests/golden/openpbr_fuzz_cases.json): the
+same with the fuzz (weight; roughness 0.5, white), half of them under a coat as well.
 """
 import json
 import sys
@@ -106,7 +107,35 @@ for i in range(300):
                        "view": f32(wo), "light": f32(wi), "rand": f32(r), "thin_film": f32(film) if film else [0.0, 0.0, 1.4],
                        "lambda": lam, "coat": float(np.float32(coat)), "f_cos": f32(f), "pdf": float(pdf), "dir": f32(d),
                        "weight": f32(w), "sample_pdf": float(spdf), "lobe": lobe})
+# Fuzzed cases (their own stream): fuzz weight 1 or uniform, every other one also coated.
+rng = np.random.default_rng(20261206)
+fuzz_cases = []
+for i in range(300):
+    base = rng.random(3)
+    metal = [0.0, 1.0, float(rng.random())][i % 3]
+    rough = float(rng.random())
+    ior = float(1.3 + 0.5 * rng.random())
+    fuzz = 1.0 if i % 4 < 2 else float(rng.random())
+    coat = 0.0 if i % 2 == 0 else float(rng.random())
+    n = unit(rng.normal(size=3))
+    wo = unit(rng.normal(size=3))
+    if (np.dot(wo, n) < 0) != (i % 10 == 9):
+        wo = -wo
+    wi = unit(rng.normal(size=3))
+    if i % 4 != 3 and np.dot(wi, n) < 0:
+        wi = -wi
+    r = rng.random(3).astype(np.float32)
+    f32 = lambda x: [float(v) for v in np.asarray(x, np.float32)]
+    m = R.material(base, metal, rough, ior, coat=coat, fuzz=fuzz)
+    f, pdf = R.evaluate(m, f32(n), f32(wo), f32(wi))
+    d, w, spdf, lobe = R.sample(m, f32(n), f32(wo), f32(r))
+    fuzz_cases.append({"base": f32(base), "metalness": metal, "roughness": rough, "ior": ior, "normal": f32(n),
+                       "view": f32(wo), "light": f32(wi), "rand": f32(r), "coat": float(np.float32(coat)),
+                       "fuzz": float(np.float32(fuzz)), "f_cos": f32(f), "pdf": float(pdf), "dir": f32(d), "weight": f32(w),
+                       "sample_pdf": float(spdf), "lobe": lobe})
 here = Path(__file__).resolve().parent
+(here / "openpbr_fuzz_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF, "
+                                                          "the default fuzz)", "cases": fuzz_cases}) + "\n")
 (here / "openpbr_coat_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF, "
                                                           "the adapter's coat)", "cases": coat_cases}) + "\n")
 (here / "openpbr_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF)",
@@ -118,4 +147,4 @@ t, a = R.metal_energy_table()
 (here / "metal_energy.json").write_text(json.dumps({"source": "Shaders/MetalEnergy.metal via oracle/_ref",
                                                     "step": 8, "table": t[::8, ::8].astype(float).tolist(),
                                                     "average": a.astype(float).tolist()}) + "\n")
-print("wrote", len(cases), "cases,", len(film_cases), "thin-film cases and", len(coat_cases), "coated cases")
+print("wrote", len(cases), "cases,", len(film_cases), "thin-film,", len(coat_cases), "coated and", len(fuzz_cases), "fuzzed cases")

@@ -4,10 +4,10 @@ vendored headers compiled for the CPU) and the FP64 oracle path tracer.
 * the dense GGX energy table, solved on the device, equals Shaders/MetalEnergy.metal's values to
   float summation error;
 * the device BSDF (openpbr.cuh) gives the reference's f |cos|, pdf and samples for 600 seeded
-  opaque materials and directions, for 300 with thin-film iridescence at given wavelengths and for 300
-  under the adapter's coat;
+  opaque materials and directions, for 300 with thin-film iridescence at given wavelengths, for 300
+  under the adapter's coat and for 300 with the default fuzz (half of them coated too);
 * a Cornell box with OPENPBR walls and boxes renders as the oracle does, in RGB and spectral
-  transport, with thin films on four slots in spectral transport, and with coats on three slots.
+  transport, with thin films on four slots in spectral transport, and with coats and fuzz on four slots.
 """
 import json
 from pathlib import Path
@@ -33,11 +33,12 @@ def test_energy_table_matches_the_reference(ctx):
     assert t[0].max() == 0.0 and (t >= 0).all() and (t <= 1).all()
 
 
-@pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json", "openpbr_coat_cases.json"])
+@pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json", "openpbr_coat_cases.json",
+                                     "openpbr_fuzz_cases.json"])
 def test_bsdf_matches_the_reference(ctx, fixture):
     R.openpbr_tables_set(ctx)
     cases = json.loads((GOLDEN / fixture).read_text())["cases"]
-    extra = lambda c: (c["thin_film"] + c["lambda"] if "thin_film" in c else [0.0] * 6) + [c.get("coat", 0.0)]
+    extra = lambda c: (c["thin_film"] + c["lambda"] if "thin_film" in c else [0.0] * 6) + [c.get("coat", 0.0), c.get("fuzz", 0.0)]
     arr = np.array([c["base"] + [c["metalness"], c["roughness"], c["ior"], 1.0, 0.0] + c["normal"] + c["view"] + c["light"]
                     + c["rand"] + extra(c) for c in cases], np.float32)
     out = R.openpbr_evaluate(ctx, arr)
@@ -105,15 +106,17 @@ def test_thin_film_cornell_matches_oracle(ctx, oracle):
 
 @pytest.mark.parametrize("spectral", [False, True])
 def test_coated_cornell_matches_oracle(ctx, oracle, spectral):
-    """Coats (weight 1 on the white wall and the metal box, 0.5 on the half-metal box) in RGB and
-    spectral transport."""
+    """Coats (weight 1 on the white wall and the metal box, 0.5 on the half-metal box) and fuzz (1 on
+    the red wall, 0.7 on the half-metal box) in RGB and spectral transport."""
     faces, verts, mats, light, cam = scenes.cornell_openpbr()
     for k, w in ((2, 1.0), (5, 1.0), (6, 0.5)):
         mats[k] = dict(mats[k], coat=w)
+    for k, w in ((3, 1.0), (6, 0.7)):
+        mats[k] = dict(mats[k], fuzz=w)
     tables = spectral_tables.load() if spectral else None
     mesh = vt.Mesh(ctx, faces, verts)
     out = []
-    for m in (mats, [dict(x, coat=0.0) for x in mats]):
+    for m in (mats, [dict(x, coat=0.0, fuzz=0.0) for x in mats]):
         scene = vt.Scene(ctx, mesh, m, light, tables)
         scene.render(vt.make_params(cam, 96, 96, 6, 1, spectral), 32)
         out.append(scene.readback()[0])

@@ -58,6 +58,19 @@ def test_reference_coat_reproduces_the_fixtures():
 
 
 @needs_ref
+def test_reference_fuzz_reproduces_the_fixtures():
+    """The fuzzed fixtures (tests/golden/openpbr_fuzz_cases.json): the default fuzz (roughness 0.5,
+    white) at weights up to 1, half of them under a coat."""
+    cases = json.loads((GOLDEN / "openpbr_fuzz_cases.json").read_text())["cases"]
+    for c in cases[:150]:
+        m = R.material(c["base"], c["metalness"], c["roughness"], c["ior"], coat=c["coat"], fuzz=c["fuzz"])
+        f, pdf = R.evaluate(m, c["normal"], c["view"], c["light"])
+        assert np.array_equal(f, np.float32(c["f_cos"])) and pdf == np.float32(c["pdf"])
+        d, w, spdf, lobe = R.sample(m, c["normal"], c["view"], c["rand"])
+        assert np.array_equal(d, np.float32(c["dir"])) and spdf == np.float32(c["sample_pdf"]) and lobe == c["lobe"]
+
+
+@needs_ref
 def test_reference_thin_film_changes_the_answer():
     """A film of weight 1 changes f |cos| on most cases; weight 0 gives the film-free answer."""
     cases = json.loads((GOLDEN / "openpbr_thin_film_cases.json").read_text())["cases"]
