@@ -944,6 +944,27 @@ def main():
         # Parity spot check of the host path against the device path.
         torch.cuda.synchronize()
         assert torch.equal(o_i[:4096].view(torch.int32), hits_i[:4096].cpu().view(torch.int32)), "host path differs from device path"
+        # The same calls from ordinary (pageable) host arrays, as a caller passing its own arrays
+        # would: the driver stages those copies, so they do not overlap the traversal.
+        p_coh, p_inc, p_cohs, p_incs = (np.array(as_np(h, vt.RAY_DTYPE)) for h in (h_coh, h_inc, h_cohs, h_incs))
+        po_c, po_i = np.empty(coh.shape[0], vt.HIT_DTYPE), np.empty(inc.shape[0], vt.HIT_DTYPE)
+        poc_c, poc_i = np.empty(coh.shape[0], np.uint8), np.empty(inc.shape[0], np.uint8)
+
+        def pageable_step():
+            mesh.closest(p_coh, po_c)
+            mesh.closest(p_inc, po_i)
+            mesh.occluded(p_cohs, poc_c)
+            mesh.occluded(p_incs, poc_i)
+
+        pageable_step()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(2):
+            pageable_step()
+        torch.cuda.synchronize()
+        pg_s = time.perf_counter() - t
+        e2e["pageable"] = {"value": world * queries * 2 / pg_s / 1e6, "unit": UNIT, "steps": 2,
+                           "note": "pageable host arrays: staged, unoverlapped copies"}
 
     # CPU baseline (rank 0, N = 1 only): the oracle port on the same BVH, bounded sample.
     cpu = None
