@@ -945,7 +945,7 @@ def main():
         torch.cuda.synchronize()
         assert torch.equal(o_i[:4096].view(torch.int32), hits_i[:4096].cpu().view(torch.int32)), "host path differs from device path"
         # The same calls from ordinary (pageable) host arrays, as a caller passing its own arrays
-        # would: the driver stages those copies, so they do not overlap the traversal.
+        # would: the library stages them through its pinned buffers with threaded host copies.
         p_coh, p_inc, p_cohs, p_incs = (np.array(as_np(h, vt.RAY_DTYPE)) for h in (h_coh, h_inc, h_cohs, h_incs))
         po_c, po_i = np.empty(coh.shape[0], vt.HIT_DTYPE), np.empty(inc.shape[0], vt.HIT_DTYPE)
         poc_c, poc_i = np.empty(coh.shape[0], np.uint8), np.empty(inc.shape[0], np.uint8)
@@ -964,7 +964,7 @@ def main():
         torch.cuda.synchronize()
         pg_s = time.perf_counter() - t
         e2e["pageable"] = {"value": world * queries * 2 / pg_s / 1e6, "unit": UNIT, "steps": 2,
-                           "note": "pageable host arrays: staged, unoverlapped copies"}
+                           "note": "pageable host arrays staged through the library's pinned buffers"}
 
     # CPU baseline (rank 0, N = 1 only): the oracle port on the same BVH, bounded sample.
     cpu = None

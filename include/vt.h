@@ -133,8 +133,10 @@ vt_status vt_trace_closest(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_
  * mesh_occluded/blas_any (main.swift:1815-1838, 1902-1984) without endpoint slack. */
 vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev, uint32_t n,
                        uint8_t *occluded_dev, void *stream);
-/* The same from HOST arrays: copies in, traces and copies out in pipelined chunks on the
- * context's streams, then synchronises. Pinned host memory gives overlapped copies. */
+/* The same from HOST arrays: copies in, traces and copies out in pipelined chunks of 2^22 rays on
+ * the context's two streams, then synchronises. Pinned (or registered) buffers are copied directly;
+ * ordinary pageable buffers go through the context's pinned staging buffers (allocated on first
+ * use), filled and drained by up to 8 host threads while the GPU works on the neighbouring chunk. */
 vt_status vt_trace_closest_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
                                 vt_hit *hits);
 vt_status vt_trace_any_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,

@@ -1,6 +1,9 @@
 // vt_api.cu — the C ABI (include/vt.h): contexts, mesh publish, traversal entry points.
+#include <algorithm>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "vt_internal.cuh"
 
@@ -137,6 +140,9 @@ vt_status vt_ctx_destroy(vt_ctx *ctx) {
     cudaFree(ctx->d_chunk_in[k]);
     cudaFree(ctx->d_chunk_out[k]);
     if (ctx->pipe[k]) cudaStreamDestroy(ctx->pipe[k]);
+    cudaFreeHost(ctx->h_stage_in[k]);
+    cudaFreeHost(ctx->h_stage_out[k]);
+    if (ctx->stage_ev[k]) cudaEventDestroy(ctx->stage_ev[k]);
   }
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_counters);
@@ -303,8 +309,63 @@ vt_status vt_trace_any(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays_dev,
   return trace_device(ctx, mesh, rays_dev, n, occluded_dev, false, static_cast<cudaStream_t>(stream), 0);
 }
 
+// Pinned staging buffers for pageable callers (two slots, grown as needed) and their events.
+static vt_status ensure_stage(vt_ctx *ctx, size_t in_bytes, size_t out_bytes) {
+  for (int k = 0; k < 2; ++k)
+    if (!ctx->stage_ev[k]) VT_CUDA(ctx, cudaEventCreateWithFlags(&ctx->stage_ev[k], cudaEventDisableTiming));
+  if (in_bytes > ctx->stage_in_bytes) {
+    for (int k = 0; k < 2; ++k) {
+      cudaFreeHost(ctx->h_stage_in[k]);
+      ctx->h_stage_in[k] = nullptr;
+      VT_CUDA(ctx, cudaMallocHost(&ctx->h_stage_in[k], in_bytes));
+    }
+    ctx->stage_in_bytes = in_bytes;
+  }
+  if (out_bytes > ctx->stage_out_bytes) {
+    for (int k = 0; k < 2; ++k) {
+      cudaFreeHost(ctx->h_stage_out[k]);
+      ctx->h_stage_out[k] = nullptr;
+      VT_CUDA(ctx, cudaMallocHost(&ctx->h_stage_out[k], out_bytes));
+    }
+    ctx->stage_out_bytes = out_bytes;
+  }
+  return VT_OK;
+}
+
+// A host copy split over a few threads: one core's copy bandwidth would otherwise bound a pageable
+// caller's throughput.
+static void copy_parallel(void *dst, const void *src, size_t bytes) {
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t parts = std::min<size_t>(std::min<size_t>(8, hw), std::max<size_t>(1, bytes >> 22));
+  if (parts <= 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t step = (bytes + parts - 1) / parts;
+  std::vector<std::thread> workers;
+  for (size_t p = 1; p < parts; ++p) {
+    const size_t off = p * step;
+    if (off >= bytes) break;
+    workers.emplace_back([=] { std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off, std::min(step, bytes - off)); });
+  }
+  std::memcpy(dst, src, std::min(step, bytes));
+  for (auto &w : workers) w.join();
+}
+
+// Whether a host pointer is ordinary (pageable) memory rather than pinned or registered memory.
+static bool pageable(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
 // Host pipeline: chunk c goes on stream c % 2 as copy-in, trace, copy-out; the two streams let
-// chunk c + 1's copy-in and chunk c - 1's copy-out overlap chunk c's traversal.
+// chunk c + 1's copy-in and chunk c - 1's copy-out overlap chunk c's traversal. Pageable buffers go
+// through pinned staging: while the GPU works on chunk c - 1, the host copies chunk c - 2's hits out
+// and chunk c's rays in (so the driver's synchronous staging never serialises the pipeline).
 static vt_status trace_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays, uint32_t n,
                             void *out, size_t out_stride, bool closest) {
   vt_status st = check_trace_args(ctx, mesh, rays, out, n);
@@ -317,6 +378,38 @@ static vt_status trace_host(vt_ctx *ctx, const vt_mesh *mesh, const vt_ray *rays
   // The previous user of these buffers may still be in flight on the other stream.
   VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[0]));
   VT_CUDA(ctx, cudaStreamSynchronize(ctx->pipe[1]));
+  if (pageable(rays) || pageable(out)) {
+    st = ensure_stage(ctx, (size_t)chunk * sizeof(vt_ray), (size_t)chunk * out_stride);
+    if (st) return st;
+    const uint32_t nchunks = (n + chunk - 1) / chunk;
+    auto copy_out = [&](uint32_t c) -> vt_status {
+      const int k = c & 1;
+      const uint32_t first = c * chunk, m = n - first < chunk ? n - first : chunk;
+      VT_CUDA(ctx, cudaEventSynchronize(ctx->stage_ev[k]));
+      copy_parallel(static_cast<char *>(out) + (size_t)first * out_stride, ctx->h_stage_out[k], (size_t)m * out_stride);
+      return VT_OK;
+    };
+    for (uint32_t c = 0; c < nchunks; ++c) {
+      const int k = c & 1;
+      const uint32_t first = c * chunk, m = n - first < chunk ? n - first : chunk;
+      if (c >= 2) {  // staging slot k held chunk c - 2: its hits out first
+        st = copy_out(c - 2);
+        if (st) return st;
+      }
+      copy_parallel(ctx->h_stage_in[k], rays + first, (size_t)m * sizeof(vt_ray));
+      cudaStream_t s = ctx->pipe[k];
+      VT_CUDA(ctx, cudaMemcpyAsync(ctx->d_chunk_in[k], ctx->h_stage_in[k], (size_t)m * sizeof(vt_ray), cudaMemcpyHostToDevice, s));
+      st = trace_device(ctx, mesh, static_cast<const vt_ray *>(ctx->d_chunk_in[k]), m, ctx->d_chunk_out[k], closest, s, 1 + k);
+      if (st) return st;
+      VT_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage_out[k], ctx->d_chunk_out[k], (size_t)m * out_stride, cudaMemcpyDeviceToHost, s));
+      VT_CUDA(ctx, cudaEventRecord(ctx->stage_ev[k], s));
+    }
+    for (uint32_t c = nchunks >= 2 ? nchunks - 2 : 0; c < nchunks; ++c) {
+      st = copy_out(c);
+      if (st) return st;
+    }
+    return VT_OK;
+  }
   for (uint32_t c = 0, first = 0; first < n; ++c, first += chunk) {
     const uint32_t m = n - first < chunk ? n - first : chunk;
     const int k = c & 1;

@@ -26,6 +26,12 @@ struct vt_ctx {
   void *d_chunk_in[2] = {nullptr, nullptr};
   void *d_chunk_out[2] = {nullptr, nullptr};
   size_t chunk_in_bytes = 0, chunk_out_bytes = 0;
+  // Pinned host staging for callers' pageable buffers (allocated on first use, grown as needed), and
+  // per staging slot the event recorded after its chunk's copy back.
+  void *h_stage_in[2] = {nullptr, nullptr};
+  void *h_stage_out[2] = {nullptr, nullptr};
+  size_t stage_in_bytes = 0, stage_out_bytes = 0;
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   // Ray-ordering scratch (keys, permutation, sort buffers), grown on demand. One per pipeline
   // stream plus one for caller streams, so concurrent launches do not share it.
   uint32_t *d_order[3] = {nullptr, nullptr, nullptr};

@@ -102,13 +102,27 @@ def test_full_size_sample_1m(ctx, oracle):
 def test_host_path_equals_device_path(ctx):
     faces, verts = scenes.triangle_soup(50_000, seed=11, mu=math.log(0.01))
     mesh = vt.Mesh(ctx, faces, verts)
-    # More rays than one pipeline chunk (2^22) so both streams and a ragged tail run.
-    rays = scenes.incoherent_rays_np((1 << 22) + 12345, seed=4)
+    # Three pipeline chunks (2^22 rays each, the last ragged), so both streams and both staging
+    # slots are reused. numpy arrays are pageable: the call stages them through pinned buffers.
+    rays = scenes.incoherent_rays_np((2 << 22) + 12345, seed=4)
     host = mesh.closest(rays)
     dev = gpu_closest(mesh, rays)
     assert_bit_exact(host, dev)
     shadow = scenes.shadow_tmax_np(rays, False)
-    assert np.array_equal(mesh.occluded(shadow), gpu_any(mesh, shadow))
+    occ_dev = gpu_any(mesh, shadow)
+    assert np.array_equal(mesh.occluded(shadow), occ_dev)
+    # Pinned caller buffers take the direct asynchronous copies instead.
+    pin_rays = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).pin_memory()
+    pin_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32).pin_memory()
+    mesh.closest(pin_rays.numpy().view(vt.RAY_DTYPE).reshape(-1), pin_hits.numpy().view(vt.HIT_DTYPE).reshape(-1))
+    assert_bit_exact(pin_hits.numpy().view(vt.HIT_DTYPE).reshape(-1), dev)
+    pin_shadow = torch.from_numpy(np.ascontiguousarray(shadow).view(np.float32).reshape(-1, 8)).pin_memory()
+    pin_occ = torch.empty((rays.shape[0],), dtype=torch.uint8).pin_memory()
+    mesh.occluded(pin_shadow.numpy().view(vt.RAY_DTYPE).reshape(-1), pin_occ.numpy())
+    assert np.array_equal(pin_occ.numpy(), occ_dev)
+    # Mixed: pageable rays into a pinned output.
+    mesh.closest(rays, pin_hits.numpy().view(vt.HIT_DTYPE).reshape(-1))
+    assert_bit_exact(pin_hits.numpy().view(vt.HIT_DTYPE).reshape(-1), dev)
 
 
 def test_edge_cases(ctx, oracle):
