@@ -456,13 +456,16 @@ vt_status vt_openpbr_energy_table(vt_ctx *ctx, float *table, float *average);
 
 /* One BSDF query: an OPENPBR material's parameters as the adapter reads them (roughness and IOR are
  * clamped to >= 0.03 and >= 1.01 inside), a unit shading normal, the view (outward) and light
- * directions, and three random numbers for a sample. 112 bytes. */
+ * directions, and three random numbers for a sample. 128 bytes. */
 typedef struct vt_openpbr_case {
   float base_color[3], metalness, roughness, ior, specular_weight, diffuse_roughness;
   float normal[3], view[3], light[3], rand[3];
   float thin_film_weight, thin_film_thickness /* micrometres */, thin_film_ior;
   float lambda[3];      /* the preparation's wavelengths in nm; 0: the upstream RGB wavelengths */
   float coat, fuzz;     /* coat and fuzz weights */
+  /* specular_roughness_anisotropy in [0, 1] and the unit surface tangent it is oriented by (the
+   * adapter's mat.tangent: used when anisotropy > 0, |tangent|^2 > 0.5 and |tangent . normal| < 0.99) */
+  float anisotropy, tangent[3];
 } vt_openpbr_case;
 /* f |cos| at the light direction and its pdf; the sample: direction, weight f |cos| / pdf, its pdf,
  * and 1 when a sample was produced. 48 bytes. */
@@ -486,7 +489,11 @@ typedef struct vt_openpbr_params {
   float coat;
   /* Fuzz weight in [0, 1] (main.swift:2497; the upstream default fuzz: roughness 0.5, white). */
   float fuzz;
-  float pad[3];
+  /* specular_roughness_anisotropy in [0, 1] (main.swift:2496), oriented by the surface tangent: a mesh
+   * without UVs takes the triangle's first edge b - a made perpendicular to the shading normal
+   * (mesh_hit_attributes, main.swift:1594-1599). */
+  float anisotropy;
+  float pad[2];
 } vt_openpbr_params;
 vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_params *params, uint32_t n);
 

@@ -70,7 +70,8 @@ class OpenPBRCase(C.Structure):
                 ("specular_weight", C.c_float), ("diffuse_roughness", C.c_float), ("normal", C.c_float * 3),
                 ("view", C.c_float * 3), ("light", C.c_float * 3), ("rand", C.c_float * 3),
                 ("thin_film_weight", C.c_float), ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float),
-                ("lambda_nm", C.c_float * 3), ("coat", C.c_float), ("fuzz", C.c_float)]
+                ("lambda_nm", C.c_float * 3), ("coat", C.c_float), ("fuzz", C.c_float),
+                ("anisotropy", C.c_float), ("tangent", C.c_float * 3)]
 
 
 class OpenPBRResult(C.Structure):
@@ -81,10 +82,10 @@ class OpenPBRResult(C.Structure):
 class OpenPBRParams(C.Structure):
     _fields_ = [("roughness", C.c_float), ("metalness", C.c_float), ("ior", C.c_float), ("diffuse_roughness", C.c_float),
                 ("thin_film_weight", C.c_float), ("thin_film_thickness", C.c_float), ("thin_film_ior", C.c_float),
-                ("coat", C.c_float), ("fuzz", C.c_float), ("pad", C.c_float * 3)]
+                ("coat", C.c_float), ("fuzz", C.c_float), ("anisotropy", C.c_float), ("pad", C.c_float * 2)]
 
 
-assert C.sizeof(OpenPBRCase) == 112 and C.sizeof(OpenPBRResult) == 48 and C.sizeof(OpenPBRParams) == 48
+assert C.sizeof(OpenPBRCase) == 128 and C.sizeof(OpenPBRResult) == 48 and C.sizeof(OpenPBRParams) == 48
 
 
 class BatchStats(C.Structure):

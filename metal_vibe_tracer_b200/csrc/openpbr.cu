@@ -36,10 +36,10 @@ __global__ void k_metal_energy(float *__restrict__ table) {
   float sum = 0.0f;
   for (uint32_t s = 0; s < 16384u; ++s) {
     const float2 r = make_float2((float(s) + 0.5f) / 16384.0f, float(__brev(s)) * 2.3283064365386963e-10f);
-    const float3 h = ggx_sample_vndf(alpha, v, r);
+    const float3 h = ggx_sample_vndf(alpha, alpha, v, r);
     const float d = 2.0f * pdot(v, h);
     const float3 l = pf3(h.x * d - v.x, h.y * d - v.y, h.z * d - v.z);  // reflect(-v, h)
-    const float energy = l.z > 0.0f ? smith_g1(l, alpha) : 0.0f;
+    const float energy = l.z > 0.0f ? smith_g1(l, alpha, alpha) : 0.0f;
     sum += 1.0f - energy;
   }
   table[i * kMetalEnergyN + j] = sum / 16384.0f;
@@ -50,6 +50,7 @@ struct CaseDev {
   float n[3], wo[3], wi[3], rand[3];
   float tfWeight, tfThickness, tfIor, lambda[3];
   float coat, fuzz;
+  float aniso, tangent[3];
 };
 struct ResultDev {
   float fcos[3], pdf, dir[3], weight[3], spdf, ok;
@@ -72,6 +73,7 @@ __device__ __forceinline__ PbrParams case_params(const CaseDev &c) {
   P.lambda = c.lambda[0] > 0.0f ? pf3(c.lambda[0], c.lambda[1], c.lambda[2]) : pf3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
   P.coat = c.coat;
   P.fuzz = c.fuzz;
+  P.aniso = c.aniso;
   return P;
 }
 
@@ -79,7 +81,8 @@ __global__ void k_openpbr_cases(PbrTables T, const CaseDev *__restrict__ cases, 
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const CaseDev c = cases[i];
-  const PbrPrepared p = pbr_prepare(case_params(c), T, pf3(c.n[0], c.n[1], c.n[2]), pf3(c.wo[0], c.wo[1], c.wo[2]));
+  const PbrPrepared p = pbr_prepare(case_params(c), T, pf3(c.n[0], c.n[1], c.n[2]), pf3(c.wo[0], c.wo[1], c.wo[2]), true,
+                                    pf3(c.tangent[0], c.tangent[1], c.tangent[2]));
   const float3 wi = pf3(c.wi[0], c.wi[1], c.wi[2]);
   const float3 f = pbr_eval(p, T, wi);
   ResultDev r;

@@ -61,6 +61,7 @@ struct PbrParams {
   float3 lambda;                       // the preparation's three wavelengths (nm)
   float coat;                          // coat weight (roughness 0.12, IOR 1.6, white, darkening 1)
   float fuzz;                          // fuzz weight (roughness 0.5, white)
+  float aniso;                         // specular_roughness_anisotropy in [0, 1]
 };
 // The reference adapter's coat for materials without a MaterialX graph (prepare_openpbr,
 // main.swift:2494-2495: coat_roughness 0.12) and the upstream default coat IOR
@@ -111,23 +112,34 @@ __device__ __forceinline__ PbrBasis pbr_basis(float3 n) {
   B.b = pf3(1.0f + s * n.x * n.x * a, s * b, -s * n.x);
   return B;
 }
+// openpbr_make_basis(normal, tangent, 1): the tangent made perpendicular to the normal, the bitangent
+// their cross product.
+__device__ __forceinline__ PbrBasis pbr_basis_tangent(float3 n, float3 t) {
+  PbrBasis B;
+  B.n = n;
+  B.t = pnormalize(psub(t, pscale(n, pdot(t, n))));
+  B.b = pf3(n.y * B.t.z - n.z * B.t.y, n.z * B.t.x - n.x * B.t.z, n.x * B.t.y - n.y * B.t.x);
+  return B;
+}
 __device__ __forceinline__ float3 pbr_to_local(const PbrBasis &B, float3 d) { return pf3(pdot(d, B.t), pdot(d, B.b), pdot(d, B.n)); }
 __device__ __forceinline__ float3 pbr_to_world(const PbrBasis &B, float3 d) {
   return padd(padd(pscale(B.t, d.x), pscale(B.b, d.y)), pscale(B.n, d.z));
 }
 
-// GGX with Smith masking (isotropic alpha on both axes), local frame.
-__device__ __forceinline__ float ggx_d(float3 h, float ax) {
-  return 1.0f / (kPbrPi * ax * ax * psq(psq(h.x / ax) + psq(h.y / ax) + psq(h.z)));
+// Anisotropic GGX with Smith masking (alpha ax along the tangent, ay along the bitangent), local frame
+// (openpbr_eval_aniso_ggx, openpbr_eval_aniso_smith_g1).
+__device__ __forceinline__ float ggx_d(float3 h, float ax, float ay) {
+  return 1.0f / (kPbrPi * ax * ay * psq(psq(h.x / ax) + psq(h.y / ay) + psq(h.z)));
 }
-__device__ __forceinline__ float smith_g1(float3 v, float ax) {
+__device__ __forceinline__ float smith_g1(float3 v, float ax, float ay) {
   const float vz2 = psq(v.z);
   if (vz2 == 0.0f) return 0.0f;
-  return 2.0f / (1.0f + sqrtf(1.0f + (psq(ax * v.x) + psq(ax * v.y)) / vz2));
+  return 2.0f / (1.0f + sqrtf(1.0f + (psq(ax * v.x) + psq(ay * v.y)) / vz2));
 }
-// Spherical-cap VNDF sampling (Dupuy and Benyoub 2023), local frame.
-__device__ __forceinline__ float3 ggx_sample_vndf(float ax, float3 wi, float2 r) {
-  const float3 ih = pnormalize(pf3(ax * wi.x, ax * wi.y, wi.z));
+// Spherical-cap VNDF sampling (Dupuy and Benyoub 2023), local frame: the view stretched into the
+// hemisphere configuration, a cap sample, and the normal stretched back.
+__device__ __forceinline__ float3 ggx_sample_vndf(float ax, float ay, float3 wi, float2 r) {
+  const float3 ih = pnormalize(pf3(ax * wi.x, ay * wi.y, wi.z));
   const float c = fminf(ih.z, 1.0f);
   const float angle = kPbrTwoPi * r.x;
   const float onePlusCos = 1.0f + c;
@@ -136,7 +148,7 @@ __device__ __forceinline__ float3 ggx_sample_vndf(float ax, float3 wi, float2 r)
   const float onePlusZ = hz + (1.0f - c);
   const float tangent = sqrtf(onePlusZ * oneMinusZ);
   const float3 m = pf3(tangent * cosf(angle) + ih.x, tangent * sinf(angle) + ih.y, hz);
-  return pnormalize(pf3(ax * m.x, ax * m.y, m.z));
+  return pnormalize(pf3(ax * m.x, ay * m.y, m.z));
 }
 
 // Real unpolarised Fresnel reflectance (openpbr_fresnel).
@@ -376,7 +388,8 @@ __device__ __forceinline__ float pbr_thin_film_presence(float weight, float nm) 
 struct PbrPrepared {
   PbrBasis B;          // face-forwarded shading frame (normal_ff = B.n)
   float3 wo;           // view direction (outward)
-  float alpha, ax;     // specular alpha, and the microfacet alpha (clamped at 1e-6)
+  float alpha;         // specular alpha (isotropic: the energy tables' and diffuse lobe's)
+  float ax, ay;        // the microfacet alphas along the basis' tangent and bitangent (clamped at 1e-6)
   float etaOpaque;     // relative IOR of the opaque reflection
   float scaleOpaque;   // opaque dielectric share (specular colour 1)
   float metalAmount;   // darkened metal
@@ -459,12 +472,17 @@ __device__ __forceinline__ float3 pbr_ltc_fetch(const PbrTables &T, float alpha,
 
 // openpbr_prepare for an opaque material seen from `wo` with shading normal n (both unit). Without
 // `weights` the lobe-selection weights (which only pbr_pdf and pbr_sample read) are left at zero: a
-// preparation that is only evaluated skips the specular coefficient at the view.
+// preparation that is only evaluated skips the specular coefficient at the view. `tangent` is the
+// surface's unit tangent (the adapter's mat.tangent); an anisotropic material takes its basis from it
+// when it is usable (prepare_openpbr, main.swift:2510-2511), an isotropic one from the normal alone:
+// the isotropic lobes are symmetric about the normal, so the frame's rotation changes neither their
+// values nor the distribution of their samples.
 __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const PbrTables &T, float3 n, float3 wo,
-                                                   bool weights = true) {
+                                                   bool weights = true, float3 tangent = make_float3(0.0f, 0.0f, 0.0f)) {
   PbrPrepared p;
   p.wo = wo;
-  p.B = pbr_basis(n);
+  p.B = P.aniso > 0.0f && pdot(tangent, tangent) > 0.5f && fabsf(pdot(tangent, n)) < 0.99f ? pbr_basis_tangent(n, tangent)
+                                                                                             : pbr_basis(n);
   const bool back = pdot(wo, n) < 0.0f;
   if (back) {
     p.B.t = pscale(p.B.t, -1.0f);
@@ -497,7 +515,15 @@ __device__ __forceinline__ PbrPrepared pbr_prepare(const PbrParams &P, const Pbr
                           ? pmix(P.rough, pbr_fourth_root(fminf(1.0f, pbr_fourth_power(P.rough) + adjust * pbr_fourth_power(coatRough))), P.coat)
                           : P.rough;
   p.alpha = psq(rough);
-  p.ax = fmaxf(p.alpha, 1e-6f);
+  // openpbr_compute_anisotropic_alpha (impl/openpbr_lobe_utils.h:37-71) with the 1e-6 floor.
+  if (P.aniso > 0.0f) {
+    p.ax = p.alpha * sqrtf(2.0f / (1.0f + psq(1.0f - P.aniso)));
+    p.ay = (1.0f - P.aniso) * p.ax;
+  } else {
+    p.ax = p.ay = p.alpha;
+  }
+  p.ax = fmaxf(p.ax, 1e-6f);
+  p.ay = fmaxf(p.ay, 1e-6f);
   const float dielectric = 1.0f - P.metal;
   p.scaleOpaque = 1.0f * 1.0f * dielectric;
   p.metalAmount = P.metal * P.sw;
@@ -586,11 +612,11 @@ __device__ __forceinline__ float3 pbr_spec_value(const PbrPrepared &p, float3 wi
   if (!(idotn * odotn > 0.0f)) return pf3(0.0f, 0.0f, 0.0f);
   const float3 h = pnormalize(padd(p.wo, wi));
   const float idoth = pdot(p.wo, h);
-  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax, p.ay);
   const float other = 1.0f / (4.0f * idotn);
   const float3 F = pbr_spec_coeff(p, fabsf(idoth));
   const float3 DoF = pscale(F, D * other);
-  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.ax) * smith_g1(pbr_to_local(p.B, wi), p.ax);
+  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.ax, p.ay) * smith_g1(pbr_to_local(p.B, wi), p.ax, p.ay);
   return pscale(DoF, G);
 }
 // The specular lobe's pdf: transmission has zero probability, reflection probability 1 unless the
@@ -601,15 +627,15 @@ __device__ __forceinline__ float pbr_spec_pdf(const PbrPrepared &p, float3 wi) {
   const float3 h = pnormalize(padd(p.wo, wi));
   const float idoth = pdot(p.wo, h), odoth = pdot(wi, h);
   if (idoth * odoth < 0.0f) return 0.0f;
-  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax, p.ay);
   const float other = idoth / (4.0f * odoth * idotn);
   const float rmax = pmax3(pbr_spec_coeff(p, fabsf(idoth)));
   const float Fprob = psafe_div(rmax, rmax + 0.0f, 0.0f);
-  return smith_g1(pbr_to_local(p.B, p.wo), p.ax) * (Fprob * D * other);
+  return smith_g1(pbr_to_local(p.B, p.wo), p.ax, p.ay) * (Fprob * D * other);
 }
 __device__ __forceinline__ bool pbr_spec_sample(const PbrPrepared &p, float3 r, float3 &wi, float3 &w, float &pdf) {
   const float idotn = pdot(p.wo, p.B.n);
-  const float3 hl = ggx_sample_vndf(p.ax, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y));
+  const float3 hl = ggx_sample_vndf(p.ax, p.ay, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y));
   const float3 h = pbr_to_world(p.B, hl);
   const float idoth = pdot(p.wo, h);
   if (idoth < 0.0f) return false;
@@ -621,11 +647,11 @@ __device__ __forceinline__ bool pbr_spec_sample(const PbrPrepared &p, float3 r, 
   const float odotn = pdot(p.B.n, wi);
   if (idotn * odotn <= 0.0f) return false;
   const float odoth = pdot(wi, h);
-  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.ax);
+  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.ax, p.ay);
   w = pscale(pscale(Fr, 1.0f / Prefl), Gs);
-  const float D = ggx_d(pbr_to_local(p.B, h), p.ax);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.ax, p.ay);
   if (D <= 0.0f) return false;
-  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.ax);
+  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.ax, p.ay);
   pdf = Prefl * D * Gm * idoth / (4.0f * odoth * idotn);
   return true;
 }
@@ -764,11 +790,11 @@ __device__ __forceinline__ float3 pbr_coat_value(const PbrPrepared &p, float3 wi
   if (!(idotn * odotn > 0.0f)) return pf3(0.0f, 0.0f, 0.0f);
   const float3 h = pnormalize(padd(p.wo, wi));
   const float idoth = pdot(p.wo, h);
-  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx, p.coatAx);
   const float other = 1.0f / (4.0f * idotn);
   const float F = pbr_fresnel(p.coatEta, fabsf(idoth));
   const float DoF = F * (D * other);
-  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx) * smith_g1(pbr_to_local(p.B, wi), p.coatAx);
+  const float G = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx, p.coatAx) * smith_g1(pbr_to_local(p.B, wi), p.coatAx, p.coatAx);
   return pf3(DoF * G, DoF * G, DoF * G);
 }
 __device__ __forceinline__ float pbr_coat_pdf(const PbrPrepared &p, float3 wi) {
@@ -777,13 +803,13 @@ __device__ __forceinline__ float pbr_coat_pdf(const PbrPrepared &p, float3 wi) {
   const float3 h = pnormalize(padd(p.wo, wi));
   const float idoth = pdot(p.wo, h), odoth = pdot(wi, h);
   if (idoth * odoth < 0.0f) return 0.0f;
-  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx, p.coatAx);
   const float other = idoth / (4.0f * odoth * idotn);
-  return smith_g1(pbr_to_local(p.B, p.wo), p.coatAx) * (D * other);
+  return smith_g1(pbr_to_local(p.B, p.wo), p.coatAx, p.coatAx) * (D * other);
 }
 __device__ __forceinline__ bool pbr_coat_sample(const PbrPrepared &p, float3 r, float3 &wi, float3 &w, float &pdf) {
   const float idotn = pdot(p.wo, p.B.n);
-  const float3 h = pbr_to_world(p.B, ggx_sample_vndf(p.coatAx, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y)));
+  const float3 h = pbr_to_world(p.B, ggx_sample_vndf(p.coatAx, p.coatAx, pbr_to_local(p.B, p.wo), make_float2(r.x, r.y)));
   const float idoth = pdot(p.wo, h);
   if (idoth < 0.0f) return false;
   wi = pnormalize(padd(pscale(p.wo, -1.0f), pscale(h, 2.0f * idoth)));
@@ -791,11 +817,11 @@ __device__ __forceinline__ bool pbr_coat_sample(const PbrPrepared &p, float3 r, 
   if (idotn * odotn <= 0.0f) return false;
   const float odoth = pdot(wi, h);
   const float F = pbr_fresnel(p.coatEta, idoth);
-  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.coatAx);
+  const float Gs = smith_g1(pbr_to_local(p.B, wi), p.coatAx, p.coatAx);
   w = pf3(F * Gs, F * Gs, F * Gs);
-  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx);
+  const float D = ggx_d(pbr_to_local(p.B, h), p.coatAx, p.coatAx);
   if (D <= 0.0f) return false;
-  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx);
+  const float Gm = smith_g1(pbr_to_local(p.B, p.wo), p.coatAx, p.coatAx);
   pdf = D * Gm * idoth / (4.0f * odoth * idotn);
   return true;
 }

@@ -235,6 +235,7 @@ struct Surface {
   float3 n;        // shading normal: the interpolated vertex normals on gn's side, else gn
   float err;       // HitRecord.error: the position's rounding bound
   uint32_t slot, face;
+  uint32_t tri;    // the triangle's position in BVH order (its vertex records)
   bool front;      // the ray meets the side cross(b - a, c - a) points to
 };
 
@@ -261,6 +262,7 @@ __device__ __forceinline__ Surface surface_at(const RenderArgs &A, const Hit &h,
   s.gn = s.front ? ng : mul(ng, -1.0f);
   s.slot = __float_as_uint(b.w);
   s.face = __float_as_uint(a.w);
+  s.tri = (uint32_t)hp;
   const float b0 = 1.0f - h.b1 - h.b2;
   if (A.imported) {
     s.pos = add(add(mul(f3(a.x, a.y, a.z), b0), mul(f3(b.x, b.y, b.z), h.b1)), mul(f3(c.x, c.y, c.z), h.b2));
@@ -890,7 +892,8 @@ __device__ __forceinline__ float max4(const RenderArgs &A, float4 a) {
 
 // ---- per-slot lobe parameters, OpenPBR vertices (openpbr.cuh) and delta vertices ----------------
 // Per slot kSlotF4 float4 (vt_scene_set_openpbr): (roughness, metalness, IOR, diffuse roughness), the
-// thin film (weight, thickness in micrometres, IOR) with the coat weight, and (fuzz weight, 0, 0, 0).
+// thin film (weight, thickness in micrometres, IOR) with the coat weight, and (fuzz weight, anisotropy,
+// 0, 0).
 // Without a table (or for a slot past it) a slot is ideal: roughness 0, IOR 1.5, no film, coat or fuzz.
 constexpr uint32_t kSlotF4 = 3;
 __device__ __forceinline__ float4 slot_lobe(const RenderArgs &A, const vt_material &m) {
@@ -927,9 +930,24 @@ __device__ __forceinline__ PbrParams pbr_params(const RenderArgs &A, const vt_ma
   P.tfIor = A.spectral ? x.z : 1.4f;
   P.coat = x.w;  // in both transports (prepare_openpbr and prepare_openpbr_lanes, main.swift:2494, 2537)
   const uint32_t slot = __float_as_uint(m.pad);
-  P.fuzz = A.pbr && slot < A.nmat ? __ldg(A.pbr + kSlotF4 * slot + 2u).x : 0.0f;  // main.swift:2497, 2540
+  const float4 x3 = A.pbr && slot < A.nmat ? __ldg(A.pbr + kSlotF4 * slot + 2u) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  P.fuzz = x3.x;   // main.swift:2497, 2540
+  P.aniso = x3.y;  // main.swift:2496, 2539
   P.lambda = lambda;
   return P;
+}
+// The adapter's mat.tangent at an anisotropic slot (zero elsewhere): mesh_hit_attributes' tangent
+// for a mesh without UVs (main.swift:1594-1599), the triangle's first edge b - a made perpendicular
+// to the shading normal n, or n x y (n x x near the poles) when the edge runs along n; unit length.
+__device__ __forceinline__ float3 surface_tangent(const RenderArgs &A, const vt_material &m, uint32_t tri, float3 n) {
+  const uint32_t slot = __float_as_uint(m.pad);
+  if (!A.pbr || slot >= A.nmat || tri >= A.faceCount || !(__ldg(A.pbr + kSlotF4 * slot + 2u).y > 0.0f))
+    return f3(0.0f, 0.0f, 0.0f);
+  const float4 a = __ldg(A.tris + 3 * (size_t)tri), b = __ldg(A.tris + 3 * (size_t)tri + 1);
+  const float3 e1 = f3(b.x - a.x, b.y - a.y, b.z - a.z);
+  float3 t = sub(e1, mul(n, dot3(e1, n)));
+  if (dot3(t, t) < 1e-12f) t = cross3(n, fabsf(n.y) < 0.9f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f));
+  return normalize3(t);
 }
 // The thin film's weight at slot m (spectral transport only).
 __device__ __forceinline__ bool pbr_thin_film_slot(const RenderArgs &A, const vt_material &m) {
@@ -959,8 +977,8 @@ __device__ __forceinline__ bool is_pbr(const RenderArgs &A, const vt_material &m
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706) at an OPENPBR vertex: f (without the cosine) per lane
 // and the pdf of `a`.
-__device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 wo,
-                                 float3 wi, float &pdf) {
+__device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, uint32_t tri,
+                                 float3 wo, float3 wi, float &pdf) {
   pdf = 0.0f;
   const float cosine = fabsf(dot3(n, wi));
   if (cosine < 1e-7f || dot3(n, wo) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -970,7 +988,8 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   const bool film = pbr_thin_film_slot(A, m);
   const float3 lam = film ? make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2))
                           : make_float3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
-  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo);
+  const float3 tan = surface_tangent(A, m, tri, n);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo, true, tan);
   pdf = pbr_pdf(a, A.pbrT, wi);
   if (dot3(wi, gn) <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const float3 fa = pbr_eval(a, A.pbrT, wi);
@@ -978,19 +997,20 @@ __device__ float4 pbr_eval_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   if (A.spectral && (rho.w != rho.x || film)) {
     const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
     const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo,
-                                      false);
+                                      false, tan);
     f3w = pbr_eval(b, A.pbrT, wi).x;
   }
   return make_float4(fa.x / cosine, fa.y / cosine, fa.z / cosine, A.spectral ? f3w / cosine : 0.0f);
 }
 // sample_bsdf (main.swift:3359-3366) at an OPENPBR vertex: direction, weight f |cos| / pdf per lane.
-__device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, float3 wo,
-                                 float3 r, float3 &dir, float4 &weight, float &pdf) {
+__device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_material &m, float3 n, float3 gn, uint32_t tri,
+                                 float3 wo, float3 r, float3 &dir, float4 &weight, float &pdf) {
   const float4 rho = reflectance(A, L, m);
   const bool film = pbr_thin_film_slot(A, m);
   const float3 lam = film ? make_float3(lane_lambda(A, L, 0), lane_lambda(A, L, 1), lane_lambda(A, L, 2))
                           : make_float3(kPbrRgbNm[0], kPbrRgbNm[1], kPbrRgbNm[2]);
-  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo);
+  const float3 tan = surface_tangent(A, m, tri, n);
+  const PbrPrepared a = pbr_prepare(pbr_params(A, m, make_float3(rho.x, rho.y, rho.z), lam), A.pbrT, n, wo, true, tan);
   float3 w;
   if (!pbr_sample(a, A.pbrT, r, dir, w, pdf) || !(pdf > 0.0f)) return false;
   if (dot3(dir, gn) <= 0.0f) return false;
@@ -998,7 +1018,7 @@ __device__ bool pbr_sample_lanes(const RenderArgs &A, const Lanes &L, const vt_m
   if (A.spectral && (rho.w != rho.x || film)) {
     const float l3 = film ? lane_lambda(A, L, 3) : kPbrRgbNm[0];
     const PbrPrepared b = pbr_prepare(pbr_params(A, m, make_float3(rho.w, rho.w, rho.w), make_float3(l3, l3, l3)), A.pbrT, n, wo,
-                                      false);
+                                      false, tan);
     w3 = pbr_eval(b, A.pbrT, dir).x / pdf;
   }
   weight = make_float4(w.x, w.y, w.z, A.spectral ? w3 : 0.0f);
@@ -1073,12 +1093,12 @@ __device__ __forceinline__ bool sample_delta(const RenderArgs &A, const Lanes &L
 // The contribution of a visible light sample ls per lane (throughput T, BSDF, emission, cosine,
 // MIS weight against the BSDF pdf when useMIS, over the light pdf).
 template <bool kPbr>
-__device__ __forceinline__ float4 nee_lanes(const RenderArgs &A, const Lanes &L, float3 n, float3 gn, float3 wo, float4 T,
+__device__ __forceinline__ float4 nee_lanes(const RenderArgs &A, const Lanes &L, float3 n, float3 gn, uint32_t tri, float3 wo, float4 T,
                                             const vt_material &m, bool useMIS, const LightSample &ls) {
   const float cosine = fabsf(dot3(n, ls.wi));
   if (is_pbr<kPbr>(A, m)) {
     float bpdf;
-    const float4 f = pbr_eval_lanes(A, L, m, n, gn, wo, ls.wi, bpdf);
+    const float4 f = pbr_eval_lanes(A, L, m, n, gn, tri, wo, ls.wi, bpdf);
     const float weight = useMIS ? power_heuristic(ls.pdf, bpdf) : 1.0f;
     const float le[3] = {ls.emission.x, ls.emission.y, ls.emission.z};
     return scale4(mul4(mul4(T, f), emission(A, L, le)), cosine * weight / ls.pdf);
@@ -1099,20 +1119,20 @@ __device__ __forceinline__ float4 nee_lanes(const RenderArgs &A, const Lanes &L,
 }
 template <bool kPbr>
 __device__ __forceinline__ float4 direct_light_lanes(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
-                                                     float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
+                                                     uint32_t tri, float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                      bool compensated, Sampler &seed, int *stack, bool requirePdf) {
   const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   const LightSample ls = sample_direct(A, p, n, seed, compensated);
   if (requirePdf && !(ls.pdf > 0.0f)) return zero;
   if (!light_visible(A, p, gn, err, ls, stack)) return zero;
-  return nee_lanes<kPbr>(A, L, n, gn, wo, T, m, useMIS, ls);
+  return nee_lanes<kPbr>(A, L, n, gn, tri, wo, T, m, useMIS, ls);
 }
 // The same as rgb.
 template <bool kPbr>
 __device__ __forceinline__ float3 direct_light(const RenderArgs &A, const Lanes &L, float3 p, float3 n, float3 gn,
-                                               float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
+                                               uint32_t tri, float err, float3 wo, float4 T, const vt_material &m, bool useMIS,
                                                bool compensated, Sampler &seed, int *stack, bool requirePdf) {
-  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, err, wo, T, m, useMIS, compensated, seed, stack, requirePdf));
+  return to_rgb(A, L, direct_light_lanes<kPbr>(A, L, p, n, gn, tri, err, wo, T, m, useMIS, compensated, seed, stack, requirePdf));
 }
 
 // ---- ReSTIR DI (sampling mode 0): reservoirs at the primary vertex --------------------------------
@@ -1145,7 +1165,7 @@ __device__ __forceinline__ float lambert_f(float3 n, float3 gn, float3 wo, float
 // The sample's contribution at the shading point before its weight: bsdf * Le * cos * G, in the
 // sample's own wavelengths (u), as linear sRGB.
 template <bool kPbr>
-__device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
+__device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p, float3 n, float3 gn, uint32_t tri, float3 view,
                                                   const vt_material &m, const DISample &c) {
   const float3 dir = normalize3(sub(c.pos, p));
   const float cos_th = fmaxf(0.0f, dot3(n, dir));
@@ -1155,7 +1175,7 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
   const float e[3] = {c.emission.x, c.emission.y, c.emission.z};
   if (is_pbr<kPbr>(A, m)) {
     float pdf;
-    const float4 f = pbr_eval_lanes(A, L, m, n, gn, mul(view, -1.0f), dir, pdf);
+    const float4 f = pbr_eval_lanes(A, L, m, n, gn, tri, mul(view, -1.0f), dir, pdf);
     return mul(to_rgb(A, L, scale4(mul4(f, emission(A, L, e)), cos_th)), light_geometry(A, p, c));
   }
   const float f = lambert_f(n, gn, mul(view, -1.0f), dir);
@@ -1165,10 +1185,10 @@ __device__ __forceinline__ float3 di_contribution(const RenderArgs &A, float3 p,
 
 // eval_restir_target_pdf (main.swift:3187-3197): the length of that contribution.
 template <bool kPbr>
-__device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 gn, float3 view,
+__device__ __forceinline__ float di_target(const RenderArgs &A, float3 p, float3 n, float3 gn, uint32_t tri, float3 view,
                                            const vt_material &m, const DISample &c) {
   if (c.pdf <= 0.0f) return 0.0f;
-  const float3 v = di_contribution<kPbr>(A, p, n, gn, view, m, c);
+  const float3 v = di_contribution<kPbr>(A, p, n, gn, tri, view, m, c);
   return sqrtf(dot3(v, v));
 }
 
@@ -1350,7 +1370,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
       const float3 r = rand_f3(seed);
       if (is_pbr<kPbr>(A, m)) {
         float4 w;
-        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, S.tri, mul(dir, -1.0f), r, nd, w, bpdf)) break;
         T = mul4(T, w);
       } else {
         nd = cosine_hemisphere(S.n, r.y, r.z);
@@ -1396,7 +1416,7 @@ __device__ float3 continue_path(const RenderArgs &A, const Lanes &L, Surface S, 
     }
     if (nee && !nextDelta && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       sampler_event(seed, (uint32_t)bounce + 1u, kZNee);
-      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit,
+      R = add(R, direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.tri, S.err, mul(dir, -1.0f), T, m, mis && scattering < limit, scattering < limit,
                               seed, stack, false));
     }
     if (bounce > 3) {
@@ -1431,7 +1451,7 @@ __device__ __forceinline__ float3 path_sample_body(const RenderArgs &A, uint32_t
     const int limit = max(0, (int)A.maxDepth - 1);
     const float4 T = A.spectral ? make_float4(1.0f, 1.0f, 1.0f, 1.0f) : make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     sampler_event(seed, 1u, kZNee);
-    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, limit > 0, seed,
+    R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.tri, S.err, mul(dir0, -1.0f), T, m, A.mode == 1u && limit > 0, limit > 0, seed,
                      stack, true);
   }
   const float spreadLimit = kNrc ? nrc_spread_limit(A, h.t, S.gn, dir0) : 0.0f;
@@ -1616,7 +1636,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
   A.gPos[i] = gp;
   A.gNrm[i] = gn;
   A.gGeo[i] = make_float4(S.gn.x, S.gn.y, S.gn.z, 0.0f);
-  A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), 0u);
+  A.gInfo[i] = make_uint4(S.face, S.slot | (S.front ? 0x80000000u : 0u), __float_as_uint(S.err), S.tri);
   if (m.type != VT_MAT_DIFFUSE) {
     A.rPos[i] = zero; A.rEmit[i] = zero; A.rW[i] = zero;
     A.giPos[i] = zero; A.giNrm[i] = zero; A.giRad[i] = zero; A.giW[i] = zero;
@@ -1635,7 +1655,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
     DISample cand;
     cand.pos = ls.pos; cand.emission = ls.emission; cand.pdf = ls.pdf; cand.u = u;
     cand.id = ls.face == 0xffffffffu ? 0u : ls.face + 2u;
-    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, cand);
+    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, cand);
     const float proposal = cand.pdf * light_geometry(A, S.pos, cand);
     const float w = proposal > 0.0f ? pHat / proposal : 0.0f;
     r.wsum += w;
@@ -1649,13 +1669,13 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_primary(Rende
     if (same_surface(gp, gn, A.hPos[j], A.hNrm[j]) && hw.y > 0.0f && hw.z > 0.0f) {
       const DISample hs = load_di(A.hrPos, A.hrEmit, A.hrW, j);
       const float cM = fminf(hw.y, 20.0f);
-      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, hs) * hw.z * cM;
+      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, hs) * hw.z * cM;
       r.M += cM;
       r.wsum += w;
       if (rand_decision(seed) * r.wsum < w) r.s = hs;
     }
   }
-  const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, r.s);
+  const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, r.s);
   const float W = r.M > 0.0f && pHat > 0.0f ? r.wsum / (r.M * pHat) : 0.0f;
   A.rPos[i] = make_float4(r.s.pos.x, r.s.pos.y, r.s.pos.z, __uint_as_float(r.s.id));
   A.rEmit[i] = make_float4(r.s.emission.x, r.s.emission.y, r.s.emission.z, r.s.pdf);
@@ -1725,6 +1745,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
   S.slot = gi.y & 0x7fffffffu;
   S.front = (gi.y >> 31) != 0u;
   S.err = __uint_as_float(gi.z);
+  S.tri = gi.w;
   const vt_material m = material(A, S.slot);
   float3 R;
   if (m.type == VT_MAT_EMISSIVE) {
@@ -1735,14 +1756,14 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
     R = f3(0.0f, 0.0f, 0.0f);
     if (kNrc || !is_delta<kPbr>(A, m)) {  // no NEE at glass or a mirror (main.swift:7657)
       sampler_event(seed, 1u, kZNee);
-      R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir0, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true);
+      R = direct_light<kPbr>(A, L, S.pos, S.n, S.gn, S.tri, S.err, mul(dir0, -1.0f), T, m, limit > 0, limit > 0, seed, stack, true);
     }
     const float spreadLimit = kNrc ? nrc_spread_limit(A, gp.w, S.gn, dir0) : 0.0f;
     R = add(R, continue_path<kPbr, kNrc>(A, L, S, m, dir0, seed, stack, false, spreadLimit, slot, &queried));
   } else {
     const float4 cw = A.rW[i];
     DISample sel = load_di(A.rPos, A.rEmit, A.rW, i);
-    float wsum = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel) * cw.z * cw.y, M = cw.y;
+    float wsum = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, sel) * cw.z * cw.y, M = cw.y;
     for (int t = 0; t < 4; ++t) {
       const float ox = pcg_rand(seed.state), oy = pcg_rand(seed.state);
       const int nx = (int)x + (int)((ox * 2.0f - 1.0f) * 16.0f), ny = (int)y + (int)((oy * 2.0f - 1.0f) * 16.0f);
@@ -1752,16 +1773,16 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4) k_di_shade(RenderA
       const float4 nw = A.rW[j];
       if (!(nw.y > 0.0f && nw.z > 0.0f)) continue;
       const DISample ns = load_di(A.rPos, A.rEmit, A.rW, j);
-      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, ns) * nw.z * nw.y;
+      const float w = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, ns) * nw.z * nw.y;
       wsum += w;
       M += nw.y;
       if (rand_decision(seed) * wsum < w) sel = ns;
     }
-    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel);
+    const float pHat = di_target<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, sel);
     const float W = M > 0.0f && pHat > 0.0f ? wsum / (M * pHat) : 0.0f;
     R = f3(0.0f, 0.0f, 0.0f);
     if (W > 0.0f && light_visible(A, S.pos, S.gn, S.err, di_light_sample(sel, S.pos), stack))
-      R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, dir0, m, sel), W);
+      R = mul(di_contribution<kPbr>(A, S.pos, S.n, S.gn, S.tri, dir0, m, sel), W);
     // ReSTIR GI (a cache-terminated path's cache covers this light, so the cache's kernel leaves it out).
     if (!kNrc && (int)A.maxDepth - 1 >= 1) {
       const float4 cgw = A.giW[i];
@@ -1986,7 +2007,7 @@ __device__ __forceinline__ bool wf_nee(const RenderArgs &A, const WfArgs &W, uin
   float3 o, dir;
   float tmax;
   if (!shadow_ray(A, S.pos, S.gn, S.err, ls, o, dir, tmax)) return false;
-  const float3 c = to_rgb(A, L, nee_lanes<kPbr>(A, L, S.n, S.gn, wo, T, m, useMIS, ls));
+  const float3 c = to_rgb(A, L, nee_lanes<kPbr>(A, L, S.n, S.gn, S.tri, wo, T, m, useMIS, ls));
   W.scon[i] = make_float4(c.x, c.y, c.z, 0.0f);
   wf_set_ray(W.sray, i, o, ray_tmin(A, o), dir, tmax);
   return true;
@@ -2129,7 +2150,7 @@ __device__ __forceinline__ void wf_vertex(const RenderArgs &A, const WfArgs &W, 
         const float3 r = rand_f3(seed);
         if (is_pbr<kPbr>(A, m)) {
           float4 w;
-          if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) alive = false;
+          if (!pbr_sample_lanes(A, L, m, S.n, S.gn, S.tri, mul(dir, -1.0f), r, nd, w, bpdf)) alive = false;
           else T = mul4(T, w);
         } else {
           nd = cosine_hemisphere(S.n, r.y, r.z);
@@ -2287,7 +2308,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
     const NrcInput q = nrc_query<kPbr>(A, L, S, m, dir);
     rec[0] = q.a; rec[1] = q.b; rec[2] = q.c; rec[3] = T; rec[4] = R;
     nrec = 1;
-    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, limit > 0, limit > 0, seed, stack,
+    R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.tri, S.err, mul(dir, -1.0f), T, m, limit > 0, limit > 0, seed, stack,
                                          true));
   }
   int scattering = 0;
@@ -2306,7 +2327,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
       const float3 r = rand_f3(seed);
       if (is_pbr<kPbr>(A, m)) {
         float4 w;
-        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, mul(dir, -1.0f), r, nd, w, bpdf)) break;
+        if (!pbr_sample_lanes(A, L, m, S.n, S.gn, S.tri, mul(dir, -1.0f), r, nd, w, bpdf)) break;
         T = mul4(T, w);
       } else {
         nd = cosine_hemisphere(S.n, r.y, r.z);
@@ -2344,7 +2365,7 @@ __global__ void __launch_bounds__(kRenderBlock, kPbr ? 3 : 4)
         r[0] = q.a; r[1] = q.b; r[2] = q.c; r[3] = T; r[4] = R;
         ++nrec;
       }
-      R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.err, mul(dir, -1.0f), T, m, scattering < limit,
+      R = add4(R, direct_light_lanes<kPbr>(A, L, S.pos, S.n, S.gn, S.tri, S.err, mul(dir, -1.0f), T, m, scattering < limit,
                                            scattering < limit, seed, stack, false));
     }
     if (bounce > 3) {
@@ -3908,9 +3929,10 @@ vt_status vt_scene_set_openpbr(vt_ctx *ctx, vt_scene *scene, const vt_openpbr_pa
         !(p.diffuse_roughness >= 0.0f && p.diffuse_roughness <= 1.0f))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": roughness, metalness and diffuse roughness "
                                           "must lie in [0, 1] and the IOR be positive");
-    if (!(p.coat >= 0.0f && p.coat <= 1.0f) || !(p.fuzz >= 0.0f && p.fuzz <= 1.0f))
-      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": coat and fuzz weights must lie in [0, 1]");
-    q[kSlotF4 * (size_t)i + 2] = make_float4(p.fuzz, 0.0f, 0.0f, 0.0f);
+    if (!(p.coat >= 0.0f && p.coat <= 1.0f) || !(p.fuzz >= 0.0f && p.fuzz <= 1.0f) || !(p.anisotropy >= 0.0f && p.anisotropy <= 1.0f))
+      return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": coat and fuzz weights and the anisotropy must lie "
+                                          "in [0, 1]");
+    q[kSlotF4 * (size_t)i + 2] = make_float4(p.fuzz, p.anisotropy, 0.0f, 0.0f);
     if (!(p.thin_film_weight >= 0.0f && p.thin_film_weight <= 1.0f) || !(p.thin_film_thickness >= 0.0f) ||
         !std::isfinite(p.thin_film_thickness) || (p.thin_film_weight > 0.0f && !(p.thin_film_ior > 0.0f)))
       return vt_fail(ctx, VT_ERR_INVALID, "OpenPBR slot " + std::to_string(i) + ": thin-film weight must lie in [0, 1], its "

@@ -150,6 +150,7 @@ class Scene:
                 params[i].thin_film_ior = float(m.get("thin_film_ior", 1.4))
                 params[i].coat = float(m.get("coat", 0.0))
                 params[i].fuzz = float(m.get("fuzz", 0.0))
+                params[i].anisotropy = float(m.get("anisotropy", 0.0))
             _check(ctx.handle, lib.vt_scene_set_openpbr(ctx.handle, self._p, params, len(materials)), "vt_scene_set_openpbr")
 
     def set_environment(self, intensity: float = 0.0, sun_dir=(0.0, 1.0, 0.0), sun_intensity: float = 0.0,
@@ -422,13 +423,13 @@ def openpbr_energy_table(ctx: Context) -> tuple[np.ndarray, np.ndarray]:
 def openpbr_evaluate(ctx: Context, cases) -> np.ndarray:
     """BSDF queries on the device: `cases` is an (n, 20) float32 array of the _lib.OpenPBRCase fields
     up to `rand` (no thin film, the upstream RGB wavelengths, no coat or fuzz), (n, 26) with the thin
-    film's weight, thickness (micrometres) and IOR and the three wavelengths (nm), or (n, 28) with the
-    coat and fuzz weights as well; returns (n, 12) float32 results (f_cos, pdf, dir, weight,
-    sample_pdf, ok)."""
+    film's weight, thickness (micrometres) and IOR and the three wavelengths (nm), (n, 28) with the
+    coat and fuzz weights as well, or (n, 32) with the anisotropy and the unit tangent; returns (n, 12)
+    float32 results (f_cos, pdf, dir, weight, sample_pdf, ok)."""
     arr = np.asarray(cases, np.float32)
-    if arr.ndim == 2 and arr.shape[1] in (20, 26, 27):
-        arr = np.concatenate([arr, np.zeros((arr.shape[0], 28 - arr.shape[1]), np.float32)], axis=1)
-    arr = np.ascontiguousarray(arr, np.float32).reshape(-1, 28)
+    if arr.ndim == 2 and arr.shape[1] in (20, 26, 27, 28):
+        arr = np.concatenate([arr, np.zeros((arr.shape[0], 32 - arr.shape[1]), np.float32)], axis=1)
+    arr = np.ascontiguousarray(arr, np.float32).reshape(-1, 32)
     out = np.empty((arr.shape[0], 12), np.float32)
     _check(ctx.handle, _lib.load().vt_openpbr_evaluate(ctx.handle, arr.ctypes.data, arr.shape[0], out.ctypes.data),
            "vt_openpbr_evaluate")

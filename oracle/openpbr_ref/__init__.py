@@ -38,16 +38,20 @@ def load():
     return _lib
 
 
-def material(base, metalness, roughness, ior, type_=4, thin_film=None, coat=0.0, fuzz=0.0):
+def material(base, metalness, roughness, ior, type_=4, thin_film=None, coat=0.0, fuzz=0.0, anisotropy=0.0, tangent=None):
     """A reference material; `thin_film` = (weight, thickness in micrometres, IOR) or None; `coat`:
     the coat weight (the adapter's coat: roughness 0.12, default IOR and colour); `fuzz`: the fuzz
-    weight (default roughness and colour)."""
+    weight (default roughness and colour); `anisotropy`: specular_roughness_anisotropy, oriented by the
+    unit `tangent` (the adapter's mat.tangent; None: the basis from the normal alone)."""
     m = Material()
     m.type = type_
     m.albedo[:] = [float(x) for x in base]
     m.roughness, m.metalness, m.ior = float(roughness), float(metalness), float(ior)
     m.coat = float(coat)
     m.fuzz = float(fuzz)
+    m.anisotropy = float(anisotropy)
+    if tangent is not None:
+        m.tangent[:] = [float(x) for x in tangent]
     if thin_film is not None:
         m.thin_film_weight, m.thin_film_thickness, m.thin_film_ior = (float(x) for x in thin_film)
     return m

@@ -1754,7 +1754,7 @@ inline double smax(const PtContext &C, const Spec4 &a) {
   return C.spectral ? std::max(m, a.v[3]) : m;
 }
 
-struct PtHit { D3 pos, gn, n; double err, t; uint32_t slot, face; bool front; };
+struct PtHit { D3 pos, gn, n, e1; double err, t; uint32_t slot, face; bool front; };  // e1: the edge b - a
 
 struct PtTri { D3 a, b, c; uint32_t slot; };
 PtTri pt_triangle(const PtContext &C, uint32_t face) {
@@ -1779,6 +1779,7 @@ bool pt_closest(const PtContext &C, D3 o, D3 d, PtHit &h) {
   const D3 ng = normalize(cross(tri.b - tri.a, tri.c - tri.a));
   h.front = dot(ng, d) < 0.0;
   h.gn = h.front ? ng : ng * -1.0;
+  h.e1 = tri.b - tri.a;
   h.slot = tri.slot;
   h.face = (uint32_t)prim;
   h.t = t;
@@ -2272,7 +2273,11 @@ bool pbr_slot(const PtContext &C, const vt_material &m) {
   const float *pp = slot_params(C, m);
   return pp && C.in->pbr_eval && (m.type == VT_MAT_OPENPBR || (m.type == VT_MAT_GLOSSY && pp[0] >= 0.02f));
 }
-vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double b0, double b1, double b2) {
+// The adapter's mat.tangent for an anisotropic slot: mesh_hit_attributes' tangent of a mesh without UVs
+// (main.swift:1594-1599), the edge e1 = b - a made perpendicular to the shading normal n (n x y, or
+// n x x near the poles, when e1 runs along n), unit length. Isotropic slots keep the basis from the
+// normal alone, as the device does: their lobes are symmetric about it.
+vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double b0, double b1, double b2, D3 n, D3 e1) {
   uint32_t slot;
   std::memcpy(&slot, &m.pad, sizeof slot);
   vto_pbr_material q;
@@ -2287,6 +2292,15 @@ vto_pbr_material pbr_material_d(const PtContext &C, const vt_material &m, double
   q.ior = pp[2];
   q.coat = pp[7];  // both transports (prepare_openpbr, main.swift:2494)
   q.fuzz = pp[8];  // main.swift:2497
+  q.anisotropy = pp[9];  // main.swift:2496
+  if (q.anisotropy > 0.0f) {
+    D3 t = e1 - n * dot(e1, n);
+    if (dot(t, t) < 1e-12) t = cross(n, std::fabs(n.y) < 0.9 ? D3{0, 1, 0} : D3{1, 0, 0});
+    t = normalize(t);
+    q.tangent[0] = (float)t.x;
+    q.tangent[1] = (float)t.y;
+    q.tangent[2] = (float)t.z;
+  }
   // The thin film is a spectral-transport input (prepare_openpbr_lanes, main.swift:2527-2568).
   if (C.spectral) {
     q.thin_film_weight = pp[4];
@@ -2303,14 +2317,14 @@ bool pbr_film_d(const PtContext &C, const vt_material &m) {
   return C.spectral && C.in->pbr_params[12 * (size_t)slot + 4] > 0.0f;
 }
 // eval_bsdf_with_pdf (main.swift:2695-2706): f (no cosine) per lane, pdf of lanes 0-2.
-Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, D3 wi, double &pdf) {
+Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 e1, D3 wo, D3 wi, double &pdf) {
   pdf = 0.0;
   const double cosine = std::fabs(dot(n, wi));
   if (cosine < 1e-7 || dot(n, wo) <= 0.0) return {{0, 0, 0, 0}};
   const Spec4 rho = reflectance(C, L, m);
   const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
               fi[3] = {(float)wi.x, (float)wi.y, (float)wi.z};
-  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2], n, e1);
   const bool film = pbr_film_d(C, m);
   const float la[3] = {(float)L.lambda[0], (float)L.lambda[1], (float)L.lambda[2]};
   const float lb[3] = {(float)L.lambda[3], (float)L.lambda[3], (float)L.lambda[3]};
@@ -2320,7 +2334,7 @@ Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &
   if (dot(wi, gn) <= 0.0) return {{0, 0, 0, 0}};
   double f3 = f[0];
   if (C.spectral && (rho.v[3] != rho.v[0] || film)) {
-    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
+    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3], n, e1);
     float g[3], qb;
     C.in->pbr_eval(&b, fn, fo, fi, film ? lb : nullptr, g, &qb);
     f3 = g[0];
@@ -2328,12 +2342,12 @@ Spec4 pbr_eval_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &
   return {{f[0] / cosine, f[1] / cosine, f[2] / cosine, C.spectral ? f3 / cosine : 0.0}};
 }
 // sample_bsdf (main.swift:3359-3366): direction, f |cos| / pdf per lane, pdf.
-bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 wo, const double r[3],
+bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material &m, D3 n, D3 gn, D3 e1, D3 wo, const double r[3],
                         D3 &dir, Spec4 &w, double &pdf) {
   const Spec4 rho = reflectance(C, L, m);
   const float fn[3] = {(float)n.x, (float)n.y, (float)n.z}, fo[3] = {(float)wo.x, (float)wo.y, (float)wo.z},
               fr[3] = {(float)r[0], (float)r[1], (float)r[2]};
-  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2]);
+  const vto_pbr_material a = pbr_material_d(C, m, rho.v[0], rho.v[1], rho.v[2], n, e1);
   const bool film = pbr_film_d(C, m);
   const float la[3] = {(float)L.lambda[0], (float)L.lambda[1], (float)L.lambda[2]};
   const float lb[3] = {(float)L.lambda[3], (float)L.lambda[3], (float)L.lambda[3]};
@@ -2346,7 +2360,7 @@ bool pbr_sample_lanes_d(const PtContext &C, const PtLanes &L, const vt_material 
   pdf = q;
   double w3 = ww[0];
   if (C.spectral && (rho.v[3] != rho.v[0] || film)) {
-    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3]);
+    const vto_pbr_material b = pbr_material_d(C, m, rho.v[3], rho.v[3], rho.v[3], n, e1);
     float g[3], qb;
     C.in->pbr_eval(&b, fn, fo, d, film ? lb : nullptr, g, &qb);
     w3 = g[0] / q;
@@ -2412,7 +2426,7 @@ bool sample_delta_d(const PtContext &C, const PtLanes &L, const vt_material &m, 
   return dot(dir, gn) > 0.0;
 }
 
-D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err, D3 wo, const Spec4 &T,
+D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, D3 e1, double err, D3 wo, const Spec4 &T,
             const vt_material &m, bool useMIS, bool compensated, ZSampler &seed, bool requirePdf) {
   const PtLight ls = C.imported ? sample_emitters_d(C, p, n, seed, compensated) : sample_light_d(C, p, seed);
   if (requirePdf && !(ls.pdf > 0.0)) return {0, 0, 0};
@@ -2420,7 +2434,7 @@ D3 direct_d(const PtContext &C, const PtLanes &L, D3 p, D3 n, D3 gn, double err,
   const double cosine = std::fabs(dot(n, ls.wi)), ni = dot(n, ls.wi), no = dot(n, wo);
   if (pbr_slot(C, m)) {
     double bpdf;
-    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, wo, ls.wi, bpdf);
+    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, e1, wo, ls.wi, bpdf);
     const double w = useMIS ? power_heuristic_d(ls.pdf, bpdf) : 1.0;
     const float le[3] = {(float)ls.emission.x, (float)ls.emission.y, (float)ls.emission.z};
     return to_rgb(C, L, scale(mul(mul(T, f), emission(C, L, le)), cosine * w / ls.pdf));
@@ -2502,7 +2516,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     } else if (pbr_slot(C, m)) {
       const double r[3] = {r0, r1, r2};
       Spec4 w;
-      if (!pbr_sample_lanes_d(C, L, m, h.n, h.gn, dir * -1.0, r, nd, w, bpdf)) break;
+      if (!pbr_sample_lanes_d(C, L, m, h.n, h.gn, h.e1, dir * -1.0, r, nd, w, bpdf)) break;
       T = mul(T, w);
     } else {
       const double phi = 2.0 * kPi * r1, cos_th = std::sqrt(r2 + 0.5 / 16777216.0);
@@ -2543,7 +2557,7 @@ D3 continue_path_d(const PtContext &C, const PtLanes &L, PtHit h, vt_material m,
     const bool nextDelta = is_delta_d(C, m);
     if (nee && !nextDelta && !(giPrimary && bounce == 1 && m.type == VT_MAT_DIFFUSE)) {
       seed.event((uint32_t)bounce + 1u, 1u);
-      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.err, nd * -1.0, T, m, mis && scattering < limit, scattering < limit, seed,
+      R = R + direct_d(C, L, h.pos, h.n, h.gn, h.e1, h.err, nd * -1.0, T, m, mis && scattering < limit, scattering < limit, seed,
                        false);
     }
     if (bounce > 3) {
@@ -2581,7 +2595,7 @@ double light_geometry_d(const PtContext &C, D3 p, const DiS &c) {
   return std::max(0.0, dot(d3(C.in->light.normal), delta * (-1.0 / std::sqrt(d2)))) / d2;
 }
 
-D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_material &m, const DiS &c) {
+D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 e1, D3 view, const vt_material &m, const DiS &c) {
   const D3 dir = normalize(c.pos - p);
   const double cos_th = std::max(0.0, dot(n, dir));
   if (cos_th <= 0.0) return {0, 0, 0};
@@ -2590,7 +2604,7 @@ D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_ma
   const float e[3] = {(float)c.emission.x, (float)c.emission.y, (float)c.emission.z};
   if (pbr_slot(C, m)) {
     double pdf;
-    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, view * -1.0, dir, pdf);
+    const Spec4 f = pbr_eval_lanes_d(C, L, m, n, gn, e1, view * -1.0, dir, pdf);
     return to_rgb(C, L, scale(mul(f, emission(C, L, e)), cos_th)) * light_geometry_d(C, p, c);
   }
   const double ni = dot(n, dir), no = -dot(n, view);
@@ -2599,9 +2613,9 @@ D3 di_contribution_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_ma
 }
 
 // eval_restir_target_pdf (main.swift:3187-3197).
-double di_target_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 view, const vt_material &m, const DiS &c) {
+double di_target_d(const PtContext &C, D3 p, D3 n, D3 gn, D3 e1, D3 view, const vt_material &m, const DiS &c) {
   if (c.pdf <= 0.0) return 0.0;
-  const D3 v = di_contribution_d(C, p, n, gn, view, m, c);
+  const D3 v = di_contribution_d(C, p, n, gn, e1, view, m, c);
   return std::sqrt(dot(v, v));
 }
 
@@ -2768,7 +2782,7 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
     out.M += 1.0;
     if (!(ls.pdf > 0.0)) continue;
     const DiS cand = di_from_light(ls, u);
-    const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, cand);
+    const double pHat = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, cand);
     const double proposal = cand.pdf * light_geometry_d(C, h.pos, cand);
     const double w = proposal > 0.0 ? pHat / proposal : 0.0;
     out.wsum += w;
@@ -2780,13 +2794,13 @@ void di_primary_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint3
     const DiPix &o = prev[(size_t)py * C.p->width + px];
     if (same_surface_d(pos, nrm, o.pos, o.nrm) && o.M > 0.0 && o.W > 0.0) {
       const double cM = std::min(o.M, 20.0);
-      const double w = di_target_d(C, h.pos, h.n, h.gn, dir0, m, o.s) * o.W * cM;
+      const double w = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, o.s) * o.W * cM;
       out.M += cM;
       out.wsum += w;
       if (seed.decision() * out.wsum < w) out.s = o.s;
     }
   }
-  const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, out.s);
+  const double pHat = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, out.s);
   out.W = out.M > 0.0 && pHat > 0.0 ? out.wsum / (out.M * pHat) : 0.0;
   if ((int)C.p->max_depth - 1 < 1) return;
   double gwsum, gM = 1.0;
@@ -2829,14 +2843,14 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
     D3 R{0, 0, 0};
     if (!is_delta_d(C, m)) {
       seed.event(1u, 1u);
-      R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, limit > 0, limit > 0, seed, true);
+      R = direct_d(C, L, h.pos, h.n, h.gn, h.e1, h.err, dir0 * -1.0, T, m, limit > 0, limit > 0, seed, true);
     }
     R = R + continue_path_d(C, L, h, m, dir0, seed, false);
     if (!std::isfinite(R.x) || !std::isfinite(R.y) || !std::isfinite(R.z)) R = {0, 0, 0};
     return R;
   }
   DiS sel = me.s;
-  double wsum = di_target_d(C, h.pos, h.n, h.gn, dir0, m, sel) * me.W * me.M, M = me.M;
+  double wsum = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, sel) * me.W * me.M, M = me.M;
   for (int t = 0; t < 4; ++t) {
     const double ox = seed.pcg(), oy = seed.pcg();
     const int nx = (int)x + (int)((ox * 2.0 - 1.0) * 16.0), ny = (int)y + (int)((oy * 2.0 - 1.0) * 16.0);
@@ -2844,16 +2858,16 @@ D3 di_shade_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32_t 
     const DiPix &n = cur[(size_t)ny * C.p->width + nx];
     if (!compatible_d(me.pos, me.nrm, n.pos, n.nrm)) continue;
     if (!(n.M > 0.0 && n.W > 0.0)) continue;
-    const double w = di_target_d(C, h.pos, h.n, h.gn, dir0, m, n.s) * n.W * n.M;
+    const double w = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, n.s) * n.W * n.M;
     wsum += w;
     M += n.M;
     if (seed.decision() * wsum < w) sel = n.s;
   }
-  const double pHat = di_target_d(C, h.pos, h.n, h.gn, dir0, m, sel);
+  const double pHat = di_target_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, sel);
   const double W = M > 0.0 && pHat > 0.0 ? wsum / (M * pHat) : 0.0;
   D3 R{0, 0, 0};
   if (W > 0.0 && visible_d(C, h.pos, h.gn, h.err, light_from_di(sel, h.pos)))
-    R = di_contribution_d(C, h.pos, h.n, h.gn, dir0, m, sel) * W;
+    R = di_contribution_d(C, h.pos, h.n, h.gn, h.e1, dir0, m, sel) * W;
   if ((int)C.p->max_depth - 1 >= 1) {
     GiS gs = me.g;
     bool gvalid = me.g.valid;
@@ -2908,7 +2922,7 @@ D3 path_sample_d(const PtContext &C, uint32_t x, uint32_t y, uint32_t si, uint32
   if (C.p->sampling_mode != 3u && !is_delta_d(C, m)) {  // no NEE at glass or mirrors (main.swift:7657)
     const Spec4 T = C.spectral ? Spec4{{1, 1, 1, 1}} : Spec4{{1, 1, 1, 0}};
     seed.event(1u, 1u);
-    R = direct_d(C, L, h.pos, h.n, h.gn, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0, limit > 0,
+    R = direct_d(C, L, h.pos, h.n, h.gn, h.e1, h.err, dir0 * -1.0, T, m, C.p->sampling_mode == 1u && limit > 0, limit > 0,
                  seed, true);
   }
   R = R + continue_path_d(C, L, h, m, dir0, seed, false);

@@ -314,7 +314,7 @@ def render(faces, verts, materials, light, camera, width, height, spp, max_depth
         params = np.array([[float(m.get("roughness", 0.5)), float(m.get("metalness", 0.0)), float(m.get("ior", 1.5)),
                             float(m.get("diffuse_roughness", 0.0)), float(m.get("thin_film_weight", 0.0)),
                             float(m.get("thin_film_thickness", 0.0)), float(m.get("thin_film_ior", 1.4)), float(m.get("coat", 0.0)),
-                            float(m.get("fuzz", 0.0)), 0.0, 0.0, 0.0]
+                            float(m.get("fuzz", 0.0)), float(m.get("anisotropy", 0.0)), 0.0, 0.0]
                            for m in materials], np.float32)
         keep.append(params)
         inp.pbr_params = params.ctypes.data

@@ -11,7 +11,10 @@ the 129 x 129 table and all 129 averages. Thin-film cases (tests/golden/openpbr_
 same with thin-film iridescence (weight, thickness, film IOR) at three given wavelengths. Coated cases
 (tests/golden/openpbr_coat_cases.json): the same with the adapter's coat (weight; roughness 0.12, IOR
 1.6), a third of them with a thin film under it. Fuzzed cases (tests/golden/openpbr_fuzz_cases.json): the
-same with the fuzz (weight; roughness 0.5, white), half of them under a coat as well.
+same with the fuzz (weight; roughness 0.5, white), half of them under a coat as well. Anisotropic
+cases (tests/golden/openpbr_aniso_cases.json): the same with specular_roughness_anisotropy in (0, 1]
+about a unit tangent perpendicular to the normal (as the adapter's mat.tangent is), a third of them
+coated and a sixth fuzzed.
 """
 import json
 import sys
@@ -133,7 +136,39 @@ for i in range(300):
                        "view": f32(wo), "light": f32(wi), "rand": f32(r), "coat": float(np.float32(coat)),
                        "fuzz": float(np.float32(fuzz)), "f_cos": f32(f), "pdf": float(pdf), "dir": f32(d), "weight": f32(w),
                        "sample_pdf": float(spdf), "lobe": lobe})
+# Anisotropic cases (their own stream): anisotropy 1 or uniform, a tangent perpendicular to the normal.
+rng = np.random.default_rng(20261207)
+aniso_cases = []
+for i in range(300):
+    base = rng.random(3)
+    metal = [0.0, 1.0, float(rng.random())][i % 3]
+    rough = float(rng.random())
+    ior = float(1.3 + 0.5 * rng.random())
+    aniso = 1.0 if i % 5 == 0 else float(rng.random())
+    coat = float(rng.random()) if i % 3 == 1 else 0.0
+    fuzz = float(rng.random()) if i % 6 == 2 else 0.0
+    n = unit(rng.normal(size=3))
+    t = rng.normal(size=3)
+    t = unit(t - n * np.dot(t, n))
+    wo = unit(rng.normal(size=3))
+    if (np.dot(wo, n) < 0) != (i % 10 == 9):
+        wo = -wo
+    wi = unit(rng.normal(size=3))
+    if i % 4 != 3 and np.dot(wi, n) < 0:
+        wi = -wi
+    r = rng.random(3).astype(np.float32)
+    f32 = lambda x: [float(v) for v in np.asarray(x, np.float32)]
+    m = R.material(base, metal, rough, ior, coat=coat, fuzz=fuzz, anisotropy=aniso, tangent=f32(t))
+    f, pdf = R.evaluate(m, f32(n), f32(wo), f32(wi))
+    d, w, spdf, lobe = R.sample(m, f32(n), f32(wo), f32(r))
+    aniso_cases.append({"base": f32(base), "metalness": metal, "roughness": rough, "ior": ior, "normal": f32(n),
+                        "view": f32(wo), "light": f32(wi), "rand": f32(r), "coat": float(np.float32(coat)),
+                        "fuzz": float(np.float32(fuzz)), "anisotropy": float(np.float32(aniso)), "tangent": f32(t),
+                        "f_cos": f32(f), "pdf": float(pdf), "dir": f32(d), "weight": f32(w), "sample_pdf": float(spdf),
+                        "lobe": lobe})
 here = Path(__file__).resolve().parent
+(here / "openpbr_aniso_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF, "
+                                                           "specular anisotropy about a tangent)", "cases": aniso_cases}) + "\n")
 (here / "openpbr_fuzz_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF, "
                                                           "the default fuzz)", "cases": fuzz_cases}) + "\n")
 (here / "openpbr_coat_cases.json").write_text(json.dumps({"source": "oracle/_ref/libopenpbr_ref.so (reference OpenPBR BSDF, "
@@ -147,4 +182,5 @@ t, a = R.metal_energy_table()
 (here / "metal_energy.json").write_text(json.dumps({"source": "Shaders/MetalEnergy.metal via oracle/_ref",
                                                     "step": 8, "table": t[::8, ::8].astype(float).tolist(),
                                                     "average": a.astype(float).tolist()}) + "\n")
-print("wrote", len(cases), "cases,", len(film_cases), "thin-film,", len(coat_cases), "coated and", len(fuzz_cases), "fuzzed cases")
+print("wrote", len(cases), "cases,", len(film_cases), "thin-film,", len(coat_cases), "coated,", len(fuzz_cases), "fuzzed and",
+      len(aniso_cases), "anisotropic cases")

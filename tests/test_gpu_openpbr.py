@@ -34,11 +34,12 @@ def test_energy_table_matches_the_reference(ctx):
 
 
 @pytest.mark.parametrize("fixture", ["openpbr_cases.json", "openpbr_thin_film_cases.json", "openpbr_coat_cases.json",
-                                     "openpbr_fuzz_cases.json"])
+                                     "openpbr_fuzz_cases.json", "openpbr_aniso_cases.json"])
 def test_bsdf_matches_the_reference(ctx, fixture):
     R.openpbr_tables_set(ctx)
     cases = json.loads((GOLDEN / fixture).read_text())["cases"]
-    extra = lambda c: (c["thin_film"] + c["lambda"] if "thin_film" in c else [0.0] * 6) + [c.get("coat", 0.0), c.get("fuzz", 0.0)]
+    extra = lambda c: ((c["thin_film"] + c["lambda"] if "thin_film" in c else [0.0] * 6) + [c.get("coat", 0.0), c.get("fuzz", 0.0)]
+                       + [c.get("anisotropy", 0.0)] + c.get("tangent", [0.0, 0.0, 0.0]))
     arr = np.array([c["base"] + [c["metalness"], c["roughness"], c["ior"], 1.0, 0.0] + c["normal"] + c["view"] + c["light"]
                     + c["rand"] + extra(c) for c in cases], np.float32)
     out = R.openpbr_evaluate(ctx, arr)
@@ -53,7 +54,12 @@ def test_bsdf_matches_the_reference(ctx, fixture):
     w = np.float32([c["weight"] for c in cases])
     sp = np.float32([c["sample_pdf"] for c in cases])
     assert np.abs(out[ok, 4:7] - d[ok]).max() < 1e-4
-    assert rel(out[ok, 7:10], w[ok]).max() < 2e-3 and rel(out[ok, 10], sp[ok]).max() < 2e-3
+    assert rel(out[ok, 7:10], w[ok]).max() < 2e-3
+    # At anisotropy 1 the bitangent alpha sits on the 1e-6 floor: the pdf of a half-vector sampled on
+    # that line hangs on the last bits of its bitangent component (f |cos| / pdf stays well conditioned
+    # and is held to 2e-3 above), so those sample pdfs get 0.1.
+    tol = np.where(np.float32([c.get("anisotropy", 0.0) for c in cases]) >= 1.0, 0.1, 2e-3)
+    assert (rel(out[ok, 10], sp[ok]) < tol[ok]).all(), rel(out[ok, 10], sp[ok]).max()
 
 
 def relmse(a, b):
@@ -130,6 +136,34 @@ def test_coated_cornell_matches_oracle(ctx, oracle, spectral):
     assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
     bm = bare.reshape(-1, 3).mean(0)
     assert np.abs(bm / rm - 1).max() > 0.03, (bm, rm)
+
+
+@pytest.mark.parametrize("spectral", [False, True])
+def test_anisotropic_cornell_matches_oracle(ctx, oracle, spectral):
+    """Specular anisotropy (1 on the three OPENPBR walls and the metal box, 0.8 on the half-metal box
+    under a coat), oriented by each triangle's first edge, in RGB and spectral transport. The same
+    samples without anisotropy move the image's mean by about 1 % (the oracle: 1.1 % in blue)."""
+    faces, verts, mats, light, cam = scenes.cornell_openpbr()
+    for k, a in ((2, 1.0), (3, 1.0), (4, 1.0), (5, 1.0), (6, 0.8)):
+        mats[k] = dict(mats[k], anisotropy=a)
+    mats[6] = dict(mats[6], coat=0.5)
+    tables = spectral_tables.load() if spectral else None
+    mesh = vt.Mesh(ctx, faces, verts)
+    out = []
+    for m in (mats, [dict(x, anisotropy=0.0) for x in mats]):
+        scene = vt.Scene(ctx, mesh, m, light, tables)
+        scene.render(vt.make_params(cam, 96, 96, 6, 1, spectral), 32)
+        out.append(scene.readback()[0])
+        scene.close()
+    mesh.close()
+    gpu, iso = out
+    ref = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, spectral=tables)
+    other = oracle.render(faces, verts, mats, light, cam, 96, 96, 32, max_depth=6, first_sample=1001, spectral=tables)
+    gm, rm = gpu.reshape(-1, 3).mean(0), ref.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(gm / rm - 1) < 5e-3), (gm, rm)
+    assert relmse(gpu, ref) < 0.25 * relmse(other, ref), (relmse(gpu, ref), relmse(other, ref))
+    im = iso.reshape(-1, 3).mean(0)
+    assert np.abs(im / gm - 1).max() > 0.006, (im, gm)
 
 
 def test_openpbr_restir_runs(ctx):
