@@ -26,8 +26,11 @@
 // as the reference's adapter sets it (coat_weight; coat_roughness 0.12, coat_ior 1.6, white
 // coat_color, coat_darkening 1; impl/openpbr_coating_lobe.h and the coat's IOR, roughness and
 // darkening terms of openpbr_prepare_lobes) and the fuzz (fuzz_weight; the default fuzz_roughness 0.5
-// and white fuzz_color; impl/openpbr_fuzz_lobe.h, the LTC sheen fit in the tables), with
-// transmission, subsurface, anisotropy and dispersion at zero. In that case the dielectric
+// and white fuzz_color; impl/openpbr_fuzz_lobe.h, the LTC sheen fit in the tables) and the specular
+// roughness anisotropy (specular_roughness_anisotropy about the basis from the adapter's tangent;
+// openpbr_compute_anisotropic_alpha and the anisotropic GGX of impl/openpbr_lobe_utils.h; the coat
+// stays isotropic, as the adapter leaves coat_roughness_anisotropy at 0), with transmission,
+// subsurface and dispersion at zero. In that case the dielectric
 // multiple-scattering lobe and both thin-wall lobes have zero weight and value, and specular
 // transmission has zero probability; the code below keeps only what is left, in the upstream
 // operation order, including the layers' recomputation of a sample's weight (w pdf / pdf).
