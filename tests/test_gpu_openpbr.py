@@ -5,9 +5,11 @@ vendored headers compiled for the CPU) and the FP64 oracle path tracer.
   float summation error;
 * the device BSDF (openpbr.cuh) gives the reference's f |cos|, pdf and samples for 600 seeded
   opaque materials and directions, for 300 with thin-film iridescence at given wavelengths, for 300
-  under the adapter's coat and for 300 with the default fuzz (half of them coated too);
+  under the adapter's coat, for 300 with the default fuzz (half of them coated too) and for 300 with
+  specular anisotropy about a given tangent;
 * a Cornell box with OPENPBR walls and boxes renders as the oracle does, in RGB and spectral
-  transport, with thin films on four slots in spectral transport, and with coats and fuzz on four slots.
+  transport, with thin films on four slots in spectral transport, with coats and fuzz on four slots,
+  and with anisotropy on five slots (tangents from each triangle's first edge).
 """
 import json
 from pathlib import Path
